@@ -1,0 +1,26 @@
+#include "common.hpp"
+
+#include "../../include/germaine_gpu.h"
+
+namespace gm {
+
+std::string &last_error() {
+    static thread_local std::string msg;
+    return msg;
+}
+
+int fail(int code, const char *fmt, ...) {
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    last_error() = buf;
+    return code;
+}
+
+}  // namespace gm
+
+extern "C" const char *gm_last_error(void) { return gm::last_error().c_str(); }
+
+extern "C" int gm_version(void) { return 100; }

@@ -1,0 +1,177 @@
+/*
+ * germaine_gpu.h -- C-ABI of the B200 per-frequency forward/adjoint engine
+ * (libgermaine_gpu.so).  Plain pointers and sizes only; every entry point
+ * returns an int status (GM_OK = 0, GM_WARNING_* > 0, GM_ERROR_* < 0) that
+ * mirrors UMFPACK's convention, and gm_last_error() returns the message of
+ * the last failure on the calling thread.
+ *
+ * Pointer arguments named h_* are host memory; d_* are device memory of the
+ * engine's GPU; plain names accept either (copies use unified addressing).
+ * Grid arrays are flat row-major [NY][NX] over the FULL grid including the
+ * PML frame: grid point (i, j) of the reference (1-based, src/util.c:177
+ * NR matrices) is element (j-1)*NX + (i-1).  Complex vectors are
+ * interleaved (re, im).  One engine per GPU stream; an engine is not
+ * re-entrant.  Every call is synchronous on return unless noted.
+ */
+#ifndef GERMAINE_GPU_H
+#define GERMAINE_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status codes (UMFPACK_OK / _WARNING_singular_matrix / _ERROR_*) ---- */
+#define GM_OK                     0
+#define GM_WARNING_PERTURBED      1  /* static pivots were perturbed (tiny or zero pivot) */
+#define GM_WARNING_NOT_CONVERGED  2  /* refinement stopped above the residual target */
+#define GM_ERROR_OUT_OF_MEMORY   -1
+#define GM_ERROR_INVALID         -2  /* bad argument */
+#define GM_ERROR_STATE           -3  /* call out of order (e.g. solve before factor) */
+#define GM_ERROR_CUDA            -4
+#define GM_ERROR_NONFINITE       -5  /* NaN/Inf in the factors or the solution */
+#define GM_ERROR_PATTERN         -6  /* matrix is not a 9-point grid pattern (UMFPACK shim) */
+
+/* ---- physics (the reference's PHYSICS, src/germaine.c:86-140) ---- */
+#define GM_PHYS_AC 1   /* acoustic pressure: material 0 = vp [m/s], 1 = rho [kg/m^3] */
+#define GM_PHYS_SH 2   /* elastic SH: 0 = vs [m/s], 1 = rho [kg/m^3] */
+#define GM_PHYS_TE 4   /* EM TE mode: 0 = epsilon [F/m] (absolute), 1 = sigma [S/m] */
+
+/* ---- factor precision ---- */
+#define GM_PREC_FP64    0  /* complex128 fronts, FP64 substitution (the drop-in) */
+#define GM_PREC_C64_IR  1  /* complex64 fronts + FP64 residual/update refinement */
+
+/* ---- operator orientation ---- */
+#define GM_OP_REF   0  /* M = A^T: what UMFPACK factorises after the value
+                          overwrite at src/AC/forward_shot_AC.c:41-48 */
+#define GM_OP_EXACT 1  /* M = A: the assembled stencil rows */
+
+/* ---- solve system (umfpack_zi_solve sys argument) ---- */
+#define GM_SYS_A   0   /* M x = b   (UMFPACK_A)   */
+#define GM_SYS_AT  1   /* M^T x = b (UMFPACK_Aat, non-conjugate transpose) */
+
+typedef struct gm_engine gm_engine;
+
+/* Grid and discretisation parameters: the reference's .inp globals after
+ * forward_AC.c:41-47 (NX, NY already include 2*NPML and NPML+FSSHIFT). */
+typedef struct {
+    int32_t nx, ny;          /* full grid incl. PML frame */
+    float dh;                /* DH [m] */
+    int32_t npml;            /* NPML */
+    int32_t free_surf;       /* FREE_SURF (FSSHIFT = free_surf ? 0 : npml) */
+    float a0_pml;            /* A0_PML */
+    float s;                 /* S, Laplace damping */
+    int32_t physics;         /* GM_PHYS_* */
+    int32_t precision;       /* GM_PREC_* */
+    int32_t op_mode;         /* GM_OP_* */
+    int32_t leaf_max;        /* nested-dissection leaf size (0 = default 64) */
+    double ir_tol;           /* refinement target on max_k ||b_k - M x_k|| / ||b_k|| (0 = 1e-10) */
+    int32_t ir_max_iter;     /* refinement iteration cap (0 = default 10) */
+} gm_config;
+
+/* Statistics of the last factor/solve (host-side copy). */
+typedef struct {
+    int64_t n;                  /* unknowns per frequency (NX*NY) */
+    int64_t nonzero;            /* NONZERO (src/calc_nonzero.c) */
+    int32_t nnodes, nlevels, max_front, max_piv;
+    int64_t front_entries;      /* sum nfront^2 per frequency */
+    int64_t factor_entries;     /* stored L+U entries per frequency */
+    double factor_flops;        /* real flops per frequency (complex FMA = 8) */
+    double solve_flops_per_rhs; /* real flops per right-hand side (fwd + bwd) */
+    int64_t perturbed_pivots;   /* static pivots replaced since the last factor */
+    int32_t ir_iterations;      /* refinement sweeps of the last solve */
+    double ir_residual;         /* max relative residual after the last solve */
+    double ms_assemble, ms_factor, ms_solve, ms_refine;  /* device time of the last calls */
+} gm_stats;
+
+const char *gm_last_error(void);
+int gm_version(void);
+
+/* Create / destroy an engine on CUDA device `device`.  Replaces the
+ * per-frequency set-up of forward_shot_AC (src/AC/forward_shot_AC.c:30-35)
+ * and umfpack_zi_symbolic (:58): the nested-dissection symbolic analysis
+ * of the NX x NY 9-point grid is done once here, on the host, and uploaded. */
+int gm_engine_create(int device, const gm_config *cfg, gm_engine **out);
+int gm_engine_destroy(gm_engine *e);
+int gm_engine_stats(const gm_engine *e, gm_stats *out);
+
+/* Material model [NY][NX] (two float arrays, meaning per physics).
+ * Replaces readmod()/init_mat_AC (src/AC/init_mat_AC.c:10) input handling. */
+int gm_set_model(gm_engine *e, const float *mat0, const float *mat1);
+
+/* Assemble and factorise the impedance matrices of nfreq frequencies as one
+ * batch: init_A_{AC,SH,TE}_9p_pml (src/AC/init_A_AC_9p_pml.c:17) +
+ * umfpack_zi_numeric (src/AC/forward_shot_AC.c:61), all frequencies at once.
+ * Returns GM_WARNING_PERTURBED if static pivots had to be replaced. */
+int gm_factor(gm_engine *e, int nfreq, const float *h_freqs);
+
+/* Copy the assembled matrix of frequency ifreq out in the reference's
+ * triplet layout (row-major, ascending columns; waveAC.Ar/Ai/irow/icol of
+ * src/AC/init_A_AC_9p_pml.c:75-80).  Any of the four outputs may be NULL. */
+int gm_get_triplets(gm_engine *e, int ifreq, double *Ar, double *Ai, int32_t *irow, int32_t *icol);
+
+/* Solve sys (GM_SYS_A / GM_SYS_AT) for nrhs right-hand sides per frequency
+ * with the current factors, followed by FP64 iterative refinement to
+ * cfg.ir_tol: umfpack_zi_solve (src/AC/forward_shot_AC.c:88) over a block
+ * of right-hand sides.  b and x are [nfreq][N][nrhs] complex128 (interleaved
+ * re/im doubles, right-hand side fastest); x may alias nothing.  Returns
+ * GM_WARNING_NOT_CONVERGED if the target was not met. */
+int gm_solve(gm_engine *e, int sys, int nrhs, const double *b, double *x);
+
+/* Forward modelling of all shots of all factorised frequencies
+ * (forward_shot_AC, src/AC/forward_shot_AC.c:77-109):
+ *   src_x/src_y   [nshots] source coordinates in metres inside the model
+ *                 (srcpos[1]/[2], src/sources.c:74-75);
+ *   rec_x/rec_y   [ntr] receiver grid indices without the PML offset
+ *                 (recpos[1]/[2], src/receiver.c:59-60);
+ *   seis          [nfreq][nshots][ntr] complex64 seismograms (precr/preci
+ *                 index i + ntr*(ishot-1) + ntr*nshots*(nfreq-1)); may be NULL;
+ *   field         [nfreq][nshots][N] complex64 wavefields in the reference's
+ *                 vec2mat layout (src/vec2mat.c:19-26, one-slot shift); may be NULL.
+ * Sources are spikes of amplitude 1 (AC/SH) or -i*Omega*mu0 (TE) over DH^2. */
+int gm_forward(gm_engine *e, int nshots, const float *src_x, const float *src_y,
+               int ntr, const int32_t *rec_x, const int32_t *rec_y,
+               float *seis, float *field);
+
+/* FWI objective + gradient of all factorised frequencies (grad_obj_AC,
+ * src/AC/grad_obj_AC.c:10-194; grad_obj_TE for GM_PHYS_TE): forward solve,
+ * residual (calc_res_AC, MISFIT 1/2/3, optional Wiener source estimate
+ * STF_INV), adjoint source, adjoint solve with the same factors
+ * (GM_SYS_A for AC as at grad_obj_AC.c:147, GM_SYS_AT for TE as at
+ * grad_obj_TE.c:149), gradient stack (ass_grad_AC / ass_grad_TE) and the
+ * PML frame taper (cp_grad_frame).
+ *   pobs          [nfreq][nshots][ntr] complex64 observed data;
+ *   grad0         [NY][NX] AC: vp gradient; TE: sigma gradient (overwritten);
+ *   grad1         [NY][NX] TE: epsilon gradient (NULL for AC);
+ *   l2            0.5 * sum |res|^2 (the reference's returned L2);
+ *   seis          optional modelled seismograms, as in gm_forward. */
+int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y,
+                int ntr, const int32_t *rec_x, const int32_t *rec_y,
+                const float *pobs, int stf_inv, int misfit,
+                float *grad0, float *grad1, float *l2, float *seis);
+
+/* Objective only (obj_AC, src/AC/obj_AC.c:10-145). */
+int gm_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y,
+           int ntr, const int32_t *rec_x, const int32_t *rec_y,
+           const float *pobs, int stf_inv, int misfit, float *l2);
+
+/* ---- symbolic-analysis introspection (host only, no GPU needed) ---- */
+typedef struct gm_symbolic gm_symbolic;
+int gm_symbolic_create(int nx, int ny, int leaf_max, gm_symbolic **out);
+int gm_symbolic_destroy(gm_symbolic *s);
+/* sizes[0..15]: n, nnodes, nlevels, nvars, front_total, ninv, nent, rhs_total,
+ * factor_entries, max_front, max_piv, 0... */
+int gm_symbolic_sizes(const gm_symbolic *s, int64_t *sizes);
+/* what: 0 perm, 1 iperm, 2 npiv, 3 nfront, 4 parent, 5 height, 6 child0,
+ * 7 child1, 8 var_off(int64), 9 vars, 10 front_off(int64), 11 inv_off(int64),
+ * 12 inv, 13 ent_off(int64), 14 ent_pos, 15 ent_id, 16 rhs_off(int64),
+ * 17 lvl_off, 18 lvl_nodes */
+int gm_symbolic_export(const gm_symbolic *s, int what, void *dst);
+double gm_symbolic_flops(const gm_symbolic *s, int which /* 0 factor, 1 solve per rhs */);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

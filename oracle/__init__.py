@@ -1,0 +1,272 @@
+"""TEST ORACLE for the GERMAINE per-frequency hot path.
+
+Test infrastructure only: tests/, ``__graft_entry__.smoke()`` and the
+``cpu_baseline`` / ``--impl reference`` legs of bench.py may import this
+package, and only as the checker or the timed CPU baseline.  The product
+(``germaine_b200``) never imports it.
+
+Two CPU implementations live here:
+
+* ``port``  -- liboracle_port.so, this project's plain-C restatement
+  (oracle/port.c) of the reference's assembly, PML, source, receiver,
+  residual and gradient arithmetic, bit-faithful in float/double;
+* ``ref``   -- oracle/_ref/libgermaine_ref.so, the reference's own C sources
+  compiled in place by oracle/Makefile (only where the reference tree is
+  present; the built library travels with the repository snapshot).
+
+The sparse direct solve (UMFPACK in the reference, an un-vendored
+SuiteSparse dependency with no pinned version) is restated with SciPy's
+SuperLU in complex128 on the operator UMFPACK actually factorises
+(oracle/sparse.py).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+PORT_SO = os.path.join(HERE, "liboracle_port.so")
+REF_SO = os.path.join(HERE, "_ref", "libgermaine_ref.so")
+
+PHYS_AC, PHYS_SH, PHYS_TE = 1, 2, 4
+
+_f32p = np.ctypeslib.ndpointer(np.float32, flags="C_CONTIGUOUS")
+_f64p = np.ctypeslib.ndpointer(np.float64, flags="C_CONTIGUOUS")
+_i32p = np.ctypeslib.ndpointer(np.int32, flags="C_CONTIGUOUS")
+
+
+@dataclass(frozen=True)
+class Grid:
+    """Full modelling grid INCLUDING the PML frame (NX, NY after
+    forward_AC.c:44-45), spacing DH [m], PML width NPML, FREE_SURF, A0_PML
+    and the Laplace damping S."""
+
+    nx: int
+    ny: int
+    dh: float
+    npml: int
+    free_surf: int = 0
+    a0_pml: float = 90.0
+    s: float = 0.0
+
+    @property
+    def fsshift(self) -> int:
+        return 0 if self.free_surf else self.npml
+
+    @property
+    def n(self) -> int:
+        return self.nx * self.ny
+
+    @property
+    def nonzero(self) -> int:
+        return 9 * self.nx * self.ny - 6 * self.nx - 6 * self.ny + 4
+
+
+class _PortGrid(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int), ("ny", ctypes.c_int), ("npml", ctypes.c_int),
+                ("free_surf", ctypes.c_int), ("fsshift", ctypes.c_int),
+                ("dh", ctypes.c_float), ("a0_pml", ctypes.c_float), ("s", ctypes.c_float)]
+
+
+def _pg(g: Grid) -> _PortGrid:
+    return _PortGrid(g.nx, g.ny, g.npml, g.free_surf, g.fsshift, g.dh, g.a0_pml, g.s)
+
+
+_port_lib = None
+_ref_lib = None
+
+
+def load_port():
+    global _port_lib
+    if _port_lib is None:
+        if not os.path.exists(PORT_SO):
+            raise RuntimeError(f"{PORT_SO} missing: run `make -C oracle port`")
+        lib = ctypes.CDLL(PORT_SO)
+        P = ctypes.POINTER(_PortGrid)
+        lib.port_pml.argtypes = [P, ctypes.c_float, _f32p]
+        lib.port_assemble.argtypes = [P, ctypes.c_int, ctypes.c_float, _f32p, _f32p, _f64p, _f64p, _i32p, _i32p]
+        lib.port_assemble.restype = ctypes.c_int
+        lib.port_rhs_source.argtypes = [P, ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f64p, _f64p]
+        lib.port_vec2mat.argtypes = [ctypes.c_int, _f64p, _f64p, _f32p, _f32p]
+        lib.port_calc_seis.argtypes = [P, _f32p, _f32p, ctypes.c_int, _i32p, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p]
+        lib.port_calc_res.argtypes = [_f32p, _f32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p]
+        lib.port_calc_res.restype = ctypes.c_float
+        lib.port_rhs_adj.argtypes = [P, _f32p, _f32p, ctypes.c_int, _i32p, _i32p, _f64p, _f64p]
+        lib.port_ass_grad_ac.argtypes = [P, ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
+        lib.port_ass_grad_te.argtypes = [P, ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
+        lib.port_grad_frame_coeff.argtypes = [P, _f32p]
+        lib.port_cp_grad_frame.argtypes = [P, _f32p]
+        _port_lib = lib
+    return _port_lib
+
+
+def ref_available() -> bool:
+    return os.path.exists(REF_SO)
+
+
+def load_ref():
+    global _ref_lib
+    if _ref_lib is None:
+        if not ref_available():
+            raise RuntimeError(f"{REF_SO} missing: run `make -C oracle ref` where the reference tree exists")
+        lib = ctypes.CDLL(REF_SO)
+        lib.ref_set_grid.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_float]
+        lib.ref_nonzero.restype = ctypes.c_int
+        lib.ref_pml.argtypes = [ctypes.c_float, _f32p]
+        lib.ref_assemble.argtypes = [ctypes.c_int, ctypes.c_float, _f32p, _f32p, _f64p, _f64p, _i32p, _i32p]
+        lib.ref_assemble.restype = ctypes.c_int
+        lib.ref_rhs_source.argtypes = [ctypes.c_int, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f64p, _f64p]
+        lib.ref_vec2mat.argtypes = [_f64p, _f64p, _f32p, _f32p]
+        lib.ref_calc_seis.argtypes = [_f32p, _f32p, ctypes.c_int, _i32p, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p]
+        lib.ref_calc_res.argtypes = [_f32p, _f32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p]
+        lib.ref_calc_res.restype = ctypes.c_float
+        lib.ref_rhs_adj.argtypes = [_f32p, _f32p, ctypes.c_int, _i32p, _i32p, _f64p, _f64p]
+        lib.ref_ass_grad_ac.argtypes = [ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
+        lib.ref_ass_grad_te.argtypes = [ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
+        lib.ref_cp_grad_frame.argtypes = [_f32p]
+        _ref_lib = lib
+    return _ref_lib
+
+
+def _f32(a):
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+# --------------------------------------------------------------- port API
+class Port:
+    """Restated hot-path arithmetic (oracle/port.c) on flat row-major
+    [NY][NX] arrays (grid point (i, j), 1-based, is index (j-1)*NX+(i-1))."""
+
+    def __init__(self, g: Grid):
+        self.g = g
+        self.lib = load_port()
+        self._pg = _pg(g)
+
+    def pml(self, freq: float) -> np.ndarray:
+        out = np.zeros(4 * (self.g.nx + 2) + 4 * (self.g.ny + 2), np.float32)
+        self.lib.port_pml(ctypes.byref(self._pg), freq, out)
+        return out
+
+    def assemble(self, physics: int, freq: float, m0, m1):
+        nz = self.g.nonzero
+        ar = np.zeros(nz); ai = np.zeros(nz)
+        ir = np.zeros(nz, np.int32); ic = np.zeros(nz, np.int32)
+        c = self.lib.port_assemble(ctypes.byref(self._pg), physics, freq, _f32(m0).ravel(), _f32(m1).ravel(), ar, ai, ir, ic)
+        if c != nz:
+            raise RuntimeError(f"port_assemble wrote {c} triplets, expected {nz}")
+        return ar, ai, ir, ic
+
+    def rhs_source(self, physics, freq, xsrc, ysrc):
+        rr = np.zeros(self.g.n); ri = np.zeros(self.g.n)
+        self.lib.port_rhs_source(ctypes.byref(self._pg), physics, freq, xsrc, ysrc, rr, ri)
+        return rr, ri
+
+    def vec2mat(self, x: np.ndarray):
+        n = self.g.n
+        xr = np.zeros(n + 1); xi = np.zeros(n + 1)
+        xr[:n] = x.real; xi[:n] = x.imag
+        pr = np.zeros(n, np.float32); pi = np.zeros(n, np.float32)
+        self.lib.port_vec2mat(n, xr, xi, pr, pi)
+        return pr, pi
+
+    def calc_seis(self, pr, pi, recx, recy, ishot, nshots, nfreq, sr, si):
+        self.lib.port_calc_seis(ctypes.byref(self._pg), _f32(pr), _f32(pi), len(recx),
+                                np.asarray(recx, np.int32), np.asarray(recy, np.int32),
+                                ishot, nshots, nfreq, sr, si)
+
+    def calc_res(self, calr, cali, obsr, obsi, stf_inv=0, invmat=1, misfit=1):
+        ntr = len(calr)
+        rr = np.zeros(ntr, np.float32); ri = np.zeros(ntr, np.float32); stf = np.zeros(2, np.float32)
+        l2 = self.lib.port_calc_res(_f32(calr), _f32(cali), _f32(obsr), _f32(obsi), ntr, stf_inv, invmat, misfit, rr, ri, stf)
+        return float(l2), rr, ri, stf
+
+    def rhs_adj(self, resr, resi, recx, recy):
+        rr = np.zeros(self.g.n); ri = np.zeros(self.g.n)
+        self.lib.port_rhs_adj(ctypes.byref(self._pg), _f32(resr), _f32(resi), len(recx),
+                              np.asarray(recx, np.int32), np.asarray(recy, np.int32), rr, ri)
+        return rr, ri
+
+    def ass_grad_ac(self, freq, stf, fr, fi, lr, li, vp, rho, grad):
+        self.lib.port_ass_grad_ac(ctypes.byref(self._pg), freq, _f32(stf), _f32(fr), _f32(fi),
+                                  _f32(lr), _f32(li), _f32(vp), _f32(rho), grad)
+
+    def ass_grad_te(self, freq, stf, fr, fi, lr, li, gsig, geps):
+        self.lib.port_ass_grad_te(ctypes.byref(self._pg), freq, _f32(stf), _f32(fr), _f32(fi),
+                                  _f32(lr), _f32(li), gsig, geps)
+
+    def grad_frame_coeff(self):
+        c = np.zeros(self.g.n, np.float32)
+        self.lib.port_grad_frame_coeff(ctypes.byref(self._pg), c)
+        return c
+
+    def cp_grad_frame(self, grad):
+        self.lib.port_cp_grad_frame(ctypes.byref(self._pg), grad)
+
+
+class Ref:
+    """The reference's own sources (compiled into oracle/_ref); same call
+    shapes as :class:`Port`.  Holds process-global reference state, so only
+    one grid is active at a time."""
+
+    def __init__(self, g: Grid):
+        self.g = g
+        self.lib = load_ref()
+        self.lib.ref_set_grid(g.nx, g.ny, g.dh, g.npml, g.free_surf, g.a0_pml, g.s)
+
+    def nonzero(self):
+        return self.lib.ref_nonzero()
+
+    def pml(self, freq):
+        out = np.zeros(4 * (self.g.nx + 2) + 4 * (self.g.ny + 2), np.float32)
+        self.lib.ref_pml(freq, out)
+        return out
+
+    def assemble(self, physics, freq, m0, m1):
+        nz = self.g.nonzero
+        ar = np.zeros(nz); ai = np.zeros(nz)
+        ir = np.zeros(nz, np.int32); ic = np.zeros(nz, np.int32)
+        if self.lib.ref_assemble(physics, freq, _f32(m0).ravel(), _f32(m1).ravel(), ar, ai, ir, ic) != 0:
+            raise RuntimeError("ref_assemble failed")
+        return ar, ai, ir, ic
+
+    def rhs_source(self, physics, freq, xsrc, ysrc):
+        rr = np.zeros(self.g.n); ri = np.zeros(self.g.n)
+        self.lib.ref_rhs_source(physics, freq, xsrc, ysrc, rr, ri)
+        return rr, ri
+
+    def vec2mat(self, x):
+        n = self.g.n
+        xr = np.zeros(n + 1); xi = np.zeros(n + 1)
+        xr[:n] = x.real; xi[:n] = x.imag
+        pr = np.zeros(n, np.float32); pi = np.zeros(n, np.float32)
+        self.lib.ref_vec2mat(xr, xi, pr, pi)
+        return pr, pi
+
+    def calc_seis(self, pr, pi, recx, recy, ishot, nshots, nfreq, sr, si, nf):
+        self.lib.ref_calc_seis(_f32(pr), _f32(pi), len(recx), np.asarray(recx, np.int32),
+                               np.asarray(recy, np.int32), ishot, nshots, nf, nfreq, sr, si)
+
+    def calc_res(self, calr, cali, obsr, obsi, stf_inv=0, invmat=1, misfit=1):
+        ntr = len(calr)
+        rr = np.zeros(ntr, np.float32); ri = np.zeros(ntr, np.float32); stf = np.zeros(2, np.float32)
+        l2 = self.lib.ref_calc_res(_f32(calr), _f32(cali), _f32(obsr), _f32(obsi), ntr, 1, 1, 1, 1,
+                                   stf_inv, invmat, misfit, rr, ri, stf)
+        return float(l2), rr, ri, stf
+
+    def rhs_adj(self, resr, resi, recx, recy):
+        rr = np.zeros(self.g.n); ri = np.zeros(self.g.n)
+        self.lib.ref_rhs_adj(_f32(resr), _f32(resi), len(recx), np.asarray(recx, np.int32),
+                             np.asarray(recy, np.int32), rr, ri)
+        return rr, ri
+
+    def ass_grad_ac(self, freq, stf, fr, fi, lr, li, vp, rho, grad):
+        self.lib.ref_ass_grad_ac(freq, _f32(stf), _f32(fr), _f32(fi), _f32(lr), _f32(li), _f32(vp), _f32(rho), grad)
+
+    def ass_grad_te(self, freq, stf, fr, fi, lr, li, gsig, geps):
+        self.lib.ref_ass_grad_te(freq, _f32(stf), _f32(fr), _f32(fi), _f32(lr), _f32(li), gsig, geps)
+
+    def cp_grad_frame(self, grad):
+        self.lib.ref_cp_grad_frame(grad)

@@ -1,0 +1,258 @@
+/*
+ * oracle/ref_harness.c -- TEST INFRASTRUCTURE ONLY (never shipped, never
+ * measured as the product).
+ *
+ * Flat-pointer entry points around the reference's OWN hot-path C sources,
+ * which oracle/Makefile compiles straight from the reference tree into
+ * oracle/_ref/libgermaine_ref.so.  This file contains no reference code: it
+ * sets the reference's globals (include/globvar.h), fills the reference's
+ * NR-style 1-based arrays (src/util.c matrix()/vector()) from flat row-major
+ * buffers, calls the reference function and copies the result out.
+ *
+ * Wrapped reference functions (file:line in the reference project):
+ *   calc_nonzero         src/calc_nonzero.c:10
+ *   pml_pro              src/pml_pro.c:20
+ *   init_mat_AC          src/AC/init_mat_AC.c:10   (+ av_rho src/av_rho.c:10)
+ *   init_A_AC_9p_pml     src/AC/init_A_AC_9p_pml.c:17
+ *   init_A_SH_9p_pml     src/SH/init_A_SH_9p_pml.c:17 (+ init_mat_SH, av_mu)
+ *   init_A_TE_9p_pml     src/TE/init_A_TE_9p_pml.c:21
+ *   RHS_source_AC        src/AC/RHS_source_AC.c:11
+ *   RHS_source_TE        src/TE/RHS_source_TE.c:11
+ *   RHS_source_AC_adj    src/AC/RHS_source_AC_adj.c:10
+ *   vec2mat              src/vec2mat.c:10
+ *   calc_seis_AC         src/AC/calc_seis_AC.c:10
+ *   calc_res_AC          src/AC/calc_res_AC.c:10
+ *   ass_grad_AC          src/AC/ass_grad_AC.c:11
+ *   ass_grad_TE          src/TE/ass_grad_TE.c:11
+ *   cp_grad_frame        src/cp_grad_frame.c:10
+ */
+#include "fd.h"
+#include "globvar.h"
+
+/* reference prototypes not declared in fd.h */
+void calc_nonzero(void);
+void pml_pro(struct PML_AC *PML_AC, struct waveAC *waveAC);
+void vec2mat(float **pr, float **pi, double *xr, double *xi);
+void cp_grad_frame(float **A);
+
+/* grid set-up: NX/NY INCLUDE the PML frame, as after forward_AC.c:44-45 */
+void ref_set_grid(int nx, int ny, float dh, int npml, int free_surf, float a0_pml, float s)
+{
+    NX = nx; NY = ny; NXNY = nx * ny; DH = dh; NPML = npml; FREE_SURF = free_surf;
+    FSSHIFT = free_surf ? 0 : npml; A0_PML = a0_pml; S = s;
+    NX0 = NX - 2 * NPML; NY0 = NY - NPML - FSSHIFT;
+    MYID = 0; READ_WAVELET = 0; SWS_TAPER_CIRCULAR_PER_SHOT = 0;
+    calc_nonzero();
+}
+
+int ref_nonzero(void) { return NONZERO; }
+
+static void alloc_pml(struct PML_AC *p)
+{
+    p->dampxr = vector(0, NX + 1); p->dampxi = vector(0, NX + 1);
+    p->dampxhr = vector(0, NX + 1); p->dampxhi = vector(0, NX + 1);
+    p->dampyr = vector(0, NY + 1); p->dampyi = vector(0, NY + 1);
+    p->dampyhr = vector(0, NY + 1); p->dampyhi = vector(0, NY + 1);
+}
+
+static void free_pml(struct PML_AC *p)
+{
+    free_vector(p->dampxr, 0, NX + 1); free_vector(p->dampxi, 0, NX + 1);
+    free_vector(p->dampxhr, 0, NX + 1); free_vector(p->dampxhi, 0, NX + 1);
+    free_vector(p->dampyr, 0, NY + 1); free_vector(p->dampyi, 0, NY + 1);
+    free_vector(p->dampyhr, 0, NY + 1); free_vector(p->dampyhi, 0, NY + 1);
+}
+
+/* out: 4*(NX+2) x-profiles (r, i, half r, half i) then 4*(NY+2) y-profiles */
+void ref_pml(float freq, float *out)
+{
+    struct PML_AC p; struct waveAC w;
+    int i, o = 0;
+    alloc_pml(&p);
+    w.freq = freq;
+    pml_pro(&p, &w);
+    for (i = 0; i <= NX + 1; i++) out[o++] = p.dampxr[i];
+    for (i = 0; i <= NX + 1; i++) out[o++] = p.dampxi[i];
+    for (i = 0; i <= NX + 1; i++) out[o++] = p.dampxhr[i];
+    for (i = 0; i <= NX + 1; i++) out[o++] = p.dampxhi[i];
+    for (i = 0; i <= NY + 1; i++) out[o++] = p.dampyr[i];
+    for (i = 0; i <= NY + 1; i++) out[o++] = p.dampyi[i];
+    for (i = 0; i <= NY + 1; i++) out[o++] = p.dampyhr[i];
+    for (i = 0; i <= NY + 1; i++) out[o++] = p.dampyhi[i];
+    free_pml(&p);
+}
+
+static float **to_nr(const float *flat)
+{
+    float **m = matrix(0, NY + 1, 0, NX + 1);
+    int i, j;
+    for (j = 1; j <= NY; j++)
+        for (i = 1; i <= NX; i++) m[j][i] = flat[(j - 1) * NX + (i - 1)];
+    return m;
+}
+
+static void from_nr(float **m, float *flat)
+{
+    int i, j;
+    for (j = 1; j <= NY; j++)
+        for (i = 1; i <= NX; i++) flat[(j - 1) * NX + (i - 1)] = m[j][i];
+}
+
+/* physics 1 = AC (m0 = vp, m1 = rho), 2 = SH (m0 = vs, m1 = rho),
+ * 4 = TE (m0 = epsilon [F/m], m1 = sigma [S/m]); material arrays are
+ * row-major [NY][NX] over the full grid including the PML frame. */
+int ref_assemble(int physics, float freq, const float *m0, const float *m1,
+                 double *Ar, double *Ai, int *irow, int *icol)
+{
+    struct PML_AC p; struct waveAC w;
+    alloc_pml(&p);
+    w.freq = freq;
+    w.Ar = Ar; w.Ai = Ai; w.irow = irow; w.icol = icol;
+    pml_pro(&p, &w);
+    if (physics == 1) {
+        struct matAC m;
+        m.vp = to_nr(m0); m.rho = to_nr(m1);
+        m.ivp2 = matrix(0, NY + 1, 0, NX + 1); m.b = matrix(0, NY + 1, 0, NX + 1);
+        init_mat_AC(&w, &m);
+        init_A_AC_9p_pml(&p, &m, &w);
+        free_matrix(m.vp, 0, NY + 1, 0, NX + 1); free_matrix(m.rho, 0, NY + 1, 0, NX + 1);
+        free_matrix(m.ivp2, 0, NY + 1, 0, NX + 1); free_matrix(m.b, 0, NY + 1, 0, NX + 1);
+    } else if (physics == 2) {
+        struct matSH m;
+        m.vs = to_nr(m0); m.rho = to_nr(m1); m.mu = matrix(0, NY + 1, 0, NX + 1);
+        init_A_SH_9p_pml(&p, &m, &w);
+        free_matrix(m.vs, 0, NY + 1, 0, NX + 1); free_matrix(m.rho, 0, NY + 1, 0, NX + 1);
+        free_matrix(m.mu, 0, NY + 1, 0, NX + 1);
+    } else if (physics == 4) {
+        struct matTE m;
+        m.epsilon = to_nr(m0); m.sigma = to_nr(m1);
+        init_A_TE_9p_pml(&p, &m, &w);
+        free_matrix(m.epsilon, 0, NY + 1, 0, NX + 1); free_matrix(m.sigma, 0, NY + 1, 0, NX + 1);
+    } else {
+        free_pml(&p);
+        return -1;
+    }
+    free_pml(&p);
+    return 0;
+}
+
+/* srcpos in metres (x, y = depth); ishot is 1-based as in the reference */
+void ref_rhs_source(int physics, float freq, float xsrc, float ysrc, double *RHSr, double *RHSi)
+{
+    struct waveAC w;
+    float **srcpos = matrix(1, 8, 1, 1);
+    srcpos[1][1] = xsrc; srcpos[2][1] = ysrc;
+    w.freq = freq; w.RHSr = RHSr; w.RHSi = RHSi;
+    if (physics == 4) RHS_source_TE(&w, srcpos, 1);
+    else RHS_source_AC(&w, srcpos, 1);
+    free_matrix(srcpos, 1, 8, 1, 1);
+}
+
+/* x must hold NXNY+1 entries (the reference reads x[NXNY]) */
+void ref_vec2mat(double *xr, double *xi, float *pr, float *pi)
+{
+    float **r = matrix(1, NY, 1, NX), **i = matrix(1, NY, 1, NX);
+    vec2mat(r, i, xr, xi);
+    { int a, b; for (b = 1; b <= NY; b++) for (a = 1; a <= NX; a++) {
+        pr[(b - 1) * NX + a - 1] = r[b][a]; pi[(b - 1) * NX + a - 1] = i[b][a]; } }
+    free_matrix(r, 1, NY, 1, NX); free_matrix(i, 1, NY, 1, NX);
+}
+
+static int **recpos_nr(int ntr, const int *recx, const int *recy)
+{
+    int **rp = imatrix(1, 3, 1, ntr), t;
+    for (t = 1; t <= ntr; t++) { rp[1][t] = recx[t - 1]; rp[2][t] = recy[t - 1]; rp[3][t] = 0; }
+    return rp;
+}
+
+/* receiver grid indices recx/recy are the reference's recpos[1]/[2]
+ * (iround(x/DH), iround(y/DH), without the PML offset); precr/preci are
+ * flat arrays of ntr*nshots*nf entries indexed from 0 (reference index - 1). */
+void ref_calc_seis(const float *pr, const float *pi, int ntr, const int *recx, const int *recy,
+                   int ishot, int nshots, int nf, int nfreq, float *precr, float *preci)
+{
+    struct waveAC w;
+    int **rp = recpos_nr(ntr, recx, recy);
+    NF = nf;
+    w.pr = to_nr(pr); w.pi = to_nr(pi);
+    w.precr = precr - 1; w.preci = preci - 1;
+    calc_seis_AC(&w, rp, ntr, ishot, nshots, nfreq);
+    free_matrix(w.pr, 0, NY + 1, 0, NX + 1); free_matrix(w.pi, 0, NY + 1, 0, NX + 1);
+    free_imatrix(rp, 1, 3, 1, ntr);
+}
+
+/* residual of one shot; presr/presi are ntr long (0-based here).  The
+ * reference leaves its local l2 uninitialised when STF_INV==0
+ * (calc_res_AC.c:18,23,88), so callers compare the returned misfit only
+ * for stf_inv == 1; the residual vectors are compared in both cases. */
+float ref_calc_res(const float *precr, const float *preci, const float *pobsr, const float *pobsi,
+                   int ntr, int ishot, int nshots, int nf, int nfreq, int stf_inv, int invmat,
+                   int misfit, float *presr, float *presi, float *stf)
+{
+    struct waveAC w;
+    float l2;
+    NF = nf; NSHOTS = nshots; STF_INV = stf_inv; INVMAT = invmat; MISFIT = misfit;
+    w.precr = (float *)precr - 1; w.preci = (float *)preci - 1;
+    w.pobsr = (float *)pobsr - 1; w.pobsi = (float *)pobsi - 1;
+    w.presr = presr - 1; w.presi = presi - 1;
+    l2 = calc_res_AC(&w, ntr, ishot, 1, nfreq);
+    stf[0] = w.stfr; stf[1] = w.stfi;
+    return l2;
+}
+
+void ref_rhs_adj(const float *presr, const float *presi, int ntr, const int *recx, const int *recy,
+                 double *RHSr, double *RHSi)
+{
+    struct waveAC w;
+    int **rp = recpos_nr(ntr, recx, recy);
+    w.presr = (float *)presr - 1; w.presi = (float *)presi - 1;
+    w.RHSr = RHSr; w.RHSi = RHSi;
+    RHS_source_AC_adj(&w, rp, ntr);
+    free_imatrix(rp, 1, 3, 1, ntr);
+}
+
+/* grad (in/out) accumulates one shot like ass_grad_AC; fwd = stored forward
+ * field (float), adj = adjoint field (float), both [NY][NX] row-major. */
+void ref_ass_grad_ac(float freq, const float *stf, const float *fwdr, const float *fwdi,
+                     const float *adjr, const float *adji, const float *vp, const float *rho,
+                     float *grad)
+{
+    struct fwiAC f; struct waveAC w; struct matAC m;
+    float **gs = matrix(1, NY, 1, NX);
+    w.freq = freq; w.stfr = stf[0]; w.stfi = stf[1];
+    f.forwardr = to_nr(fwdr); f.forwardi = to_nr(fwdi); f.grad = to_nr(grad);
+    w.pr = to_nr(adjr); w.pi = to_nr(adji);
+    m.vp = to_nr(vp); m.rho = to_nr(rho);
+    ass_grad_AC(&f, &w, &m, gs, NULL, 0, NULL, 0, 1);
+    from_nr(f.grad, grad);
+    free_matrix(gs, 1, NY, 1, NX);
+    free_matrix(f.forwardr, 0, NY + 1, 0, NX + 1); free_matrix(f.forwardi, 0, NY + 1, 0, NX + 1);
+    free_matrix(f.grad, 0, NY + 1, 0, NX + 1);
+    free_matrix(w.pr, 0, NY + 1, 0, NX + 1); free_matrix(w.pi, 0, NY + 1, 0, NX + 1);
+    free_matrix(m.vp, 0, NY + 1, 0, NX + 1); free_matrix(m.rho, 0, NY + 1, 0, NX + 1);
+}
+
+void ref_ass_grad_te(float freq, const float *stf, const float *fwdr, const float *fwdi,
+                     const float *adjr, const float *adji, float *grad_sigma, float *grad_eps)
+{
+    struct fwiTE f; struct waveAC w;
+    float **gs = matrix(1, NY, 1, NX), **ge = matrix(1, NY, 1, NX);
+    w.freq = freq; w.stfr = stf[0]; w.stfi = stf[1];
+    f.forwardr = to_nr(fwdr); f.forwardi = to_nr(fwdi);
+    f.grad_sigma = to_nr(grad_sigma); f.grad_epsilon = to_nr(grad_eps);
+    w.pr = to_nr(adjr); w.pi = to_nr(adji);
+    ass_grad_TE(&f, &w, NULL, gs, ge, NULL, 0, NULL, 0, 1);
+    from_nr(f.grad_sigma, grad_sigma); from_nr(f.grad_epsilon, grad_eps);
+    free_matrix(gs, 1, NY, 1, NX); free_matrix(ge, 1, NY, 1, NX);
+    free_matrix(f.forwardr, 0, NY + 1, 0, NX + 1); free_matrix(f.forwardi, 0, NY + 1, 0, NX + 1);
+    free_matrix(f.grad_sigma, 0, NY + 1, 0, NX + 1); free_matrix(f.grad_epsilon, 0, NY + 1, 0, NX + 1);
+    free_matrix(w.pr, 0, NY + 1, 0, NX + 1); free_matrix(w.pi, 0, NY + 1, 0, NX + 1);
+}
+
+void ref_cp_grad_frame(float *grad)
+{
+    float **g = to_nr(grad);
+    cp_grad_frame(g);
+    from_nr(g, grad);
+    free_matrix(g, 0, NY + 1, 0, NX + 1);
+}
