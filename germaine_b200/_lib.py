@@ -1,0 +1,118 @@
+"""ctypes binding of libgermaine_gpu.so (the C-ABI in include/germaine_gpu.h).
+
+The library is built in-tree by germaine_b200/build.py.  There is no CPU
+fallback: if the shared library is missing or a call fails, an exception is
+raised.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libgermaine_gpu.so")
+
+GM_OK = 0
+GM_WARNING_PERTURBED = 1
+GM_WARNING_NOT_CONVERGED = 2
+GM_ERROR_OUT_OF_MEMORY = -1
+GM_ERROR_INVALID = -2
+GM_ERROR_STATE = -3
+GM_ERROR_CUDA = -4
+GM_ERROR_NONFINITE = -5
+GM_ERROR_PATTERN = -6
+
+GM_PHYS_AC, GM_PHYS_SH, GM_PHYS_TE = 1, 2, 4
+GM_PREC_FP64, GM_PREC_C64_IR = 0, 1
+GM_OP_REF, GM_OP_EXACT = 0, 1
+GM_SYS_A, GM_SYS_AT = 0, 1
+
+
+class GmConfig(ctypes.Structure):
+    _fields_ = [("nx", ctypes.c_int32), ("ny", ctypes.c_int32), ("dh", ctypes.c_float),
+                ("npml", ctypes.c_int32), ("free_surf", ctypes.c_int32), ("a0_pml", ctypes.c_float),
+                ("s", ctypes.c_float), ("physics", ctypes.c_int32), ("precision", ctypes.c_int32),
+                ("op_mode", ctypes.c_int32), ("leaf_max", ctypes.c_int32), ("ir_tol", ctypes.c_double),
+                ("ir_max_iter", ctypes.c_int32)]
+
+
+class GmStats(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int64), ("nonzero", ctypes.c_int64), ("nnodes", ctypes.c_int32),
+                ("nlevels", ctypes.c_int32), ("max_front", ctypes.c_int32), ("max_piv", ctypes.c_int32),
+                ("front_entries", ctypes.c_int64), ("factor_entries", ctypes.c_int64),
+                ("factor_flops", ctypes.c_double), ("solve_flops_per_rhs", ctypes.c_double),
+                ("perturbed_pivots", ctypes.c_int64), ("ir_iterations", ctypes.c_int32),
+                ("ir_residual", ctypes.c_double), ("ms_assemble", ctypes.c_double),
+                ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double), ("ms_refine", ctypes.c_double)]
+
+    def as_dict(self) -> dict:
+        return {k: getattr(self, k) for k, _ in self._fields_}
+
+
+# every C-ABI symbol declared in include/germaine_gpu.h
+EXPORTS = [
+    "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats",
+    "gm_set_model", "gm_factor", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
+    "gm_get_gradient_fp64",
+    "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
+    "gm_symbolic_flops",
+]
+
+_lib = None
+
+
+class GmError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"germaine_gpu error {code}: {msg}")
+        self.code = code
+
+
+def load() -> ctypes.CDLL:
+    """Load the in-tree library (raises if it was not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python germaine_b200/build.py` "
+                           "(there is no CPU fallback)")
+    lib = ctypes.CDLL(LIB_PATH)
+    vp = ctypes.c_void_p
+    i32, f64 = ctypes.c_int, ctypes.c_double
+    lib.gm_last_error.restype = ctypes.c_char_p
+    lib.gm_version.restype = i32
+    lib.gm_engine_create.argtypes = [i32, ctypes.POINTER(GmConfig), ctypes.POINTER(vp)]
+    lib.gm_engine_destroy.argtypes = [vp]
+    lib.gm_engine_stats.argtypes = [vp, ctypes.POINTER(GmStats)]
+    lib.gm_set_model.argtypes = [vp, vp, vp]
+    lib.gm_factor.argtypes = [vp, i32, vp]
+    lib.gm_get_triplets.argtypes = [vp, i32, vp, vp, vp, vp]
+    lib.gm_solve.argtypes = [vp, i32, i32, vp, vp]
+    lib.gm_forward.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, vp]
+    lib.gm_grad_obj.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, i32, i32, vp, vp, vp, vp]
+    lib.gm_obj.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, i32, i32, vp]
+    lib.gm_get_gradient_fp64.argtypes = [vp, vp, vp]
+    lib.gm_symbolic_create.argtypes = [i32, i32, i32, ctypes.POINTER(vp)]
+    lib.gm_symbolic_destroy.argtypes = [vp]
+    lib.gm_symbolic_sizes.argtypes = [vp, vp]
+    lib.gm_symbolic_export.argtypes = [vp, i32, vp]
+    lib.gm_symbolic_flops.argtypes = [vp, i32]
+    lib.gm_symbolic_flops.restype = f64
+    _lib = lib
+    return lib
+
+
+def check(rc: int, allow_warning: bool = True) -> int:
+    """Raise GmError for negative status codes (and for warnings unless allowed)."""
+    if rc < 0 or (rc > 0 and not allow_warning):
+        msg = load().gm_last_error().decode(errors="replace")
+        raise GmError(rc, msg)
+    return rc
+
+
+def ptr(a) -> ctypes.c_void_p:
+    """Address of a numpy array (host) or a torch tensor (host or device); None -> NULL."""
+    if a is None:
+        return ctypes.c_void_p(0)
+    if hasattr(a, "data_ptr"):
+        return ctypes.c_void_p(a.data_ptr())
+    return ctypes.c_void_p(a.ctypes.data)

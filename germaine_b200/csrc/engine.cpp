@@ -1,0 +1,430 @@
+// gm_engine: the C-ABI of the per-frequency engine (include/germaine_gpu.h).
+//
+// Memory plan (HBM, per engine):
+//   symbolic structure        ~ 40 B per grid point (uploaded once)
+//   A      [nf][9][n] c128    assembled stencils of the frequency batch
+//   fronts [nf][sum f^2]      c128 (GM_PREC_FP64) or c64 (GM_PREC_C64_IR)
+//   x, b, r[nf][n][nrhs] c128 solution, right-hand side, residual
+//   t      [nf][n][nrhs]      working precision copy for the substitution
+//   w      [nf][sum f][nrhs]  front-vector workspace of the substitution
+// At 841 x 227 (n = 190,907) with 10 frequencies x 100 shots this is about
+// 8 GB of fronts in FP64 plus 12 GB of vectors -- resident in one B200.
+#include "engine.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <new>
+
+#include "host_setup.h"
+
+using gm::fail;
+
+#define GM_CUDA(call)                                                                                       \
+    do {                                                                                                    \
+        cudaError_t err_ = (call);                                                                          \
+        if (err_ != cudaSuccess)                                                                            \
+            return fail(GM_ERROR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(err_), __FILE__, \
+                        __LINE__);                                                                          \
+    } while (0)
+
+#define GM_ALLOC(buf, nbytes)                                                                                   \
+    do {                                                                                                        \
+        cudaError_t err_ = (buf).ensure(nbytes);                                                                \
+        if (err_ != cudaSuccess)                                                                                \
+            return fail(err_ == cudaErrorMemoryAllocation ? GM_ERROR_OUT_OF_MEMORY : GM_ERROR_CUDA,             \
+                        "device allocation of %zu bytes failed: %s", (size_t)(nbytes), cudaGetErrorString(err_)); \
+    } while (0)
+
+namespace {
+
+template <class T>
+int upload(gm::DevBuf &buf, const std::vector<T> &v, cudaStream_t st) {
+    GM_ALLOC(buf, v.size() * sizeof(T));
+    if (!v.empty()) GM_CUDA(cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return GM_OK;
+}
+
+int check_config(const gm_config *c) {
+    if (!c) return fail(GM_ERROR_INVALID, "null config");
+    if (c->nx < 3 || c->ny < 3) return fail(GM_ERROR_INVALID, "grid must be at least 3 x 3 (got %d x %d)", c->nx, c->ny);
+    if ((int64_t)c->nx * c->ny > (int64_t)1 << 27) return fail(GM_ERROR_INVALID, "grid too large");
+    if (!(c->dh > 0.f)) return fail(GM_ERROR_INVALID, "DH must be positive");
+    if (c->npml < 0 || 2 * c->npml >= c->nx || 2 * c->npml >= c->ny)
+        return fail(GM_ERROR_INVALID, "NPML %d does not fit the %d x %d grid", c->npml, c->nx, c->ny);
+    if (c->physics != GM_PHYS_AC && c->physics != GM_PHYS_SH && c->physics != GM_PHYS_TE)
+        return fail(GM_ERROR_INVALID, "unknown physics %d", c->physics);
+    if (c->precision != GM_PREC_FP64 && c->precision != GM_PREC_C64_IR)
+        return fail(GM_ERROR_INVALID, "unknown precision %d", c->precision);
+    if (c->op_mode != GM_OP_REF && c->op_mode != GM_OP_EXACT) return fail(GM_ERROR_INVALID, "unknown op_mode %d", c->op_mode);
+    return GM_OK;
+}
+
+}  // namespace
+
+extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **out) {
+    if (!out) return fail(GM_ERROR_INVALID, "gm_engine_create: null output");
+    *out = nullptr;
+    int rc = check_config(cfg);
+    if (rc) return rc;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+        return fail(GM_ERROR_CUDA, "no CUDA device available: the engine has no CPU path");
+    if (device < 0 || device >= ndev) return fail(GM_ERROR_INVALID, "device %d out of range (%d devices)", device, ndev);
+    GM_CUDA(cudaSetDevice(device));
+
+    gm_engine *e = nullptr;
+    try {
+        e = new gm_engine();
+        e->cfg = *cfg;
+        if (e->cfg.leaf_max <= 0) e->cfg.leaf_max = 64;
+        if (!(e->cfg.ir_tol > 0)) e->cfg.ir_tol = 1e-10;
+        if (e->cfg.ir_max_iter <= 0) e->cfg.ir_max_iter = 10;
+        e->device = device;
+        e->fsshift = cfg->free_surf ? 0 : cfg->npml;
+        e->n = cfg->nx * cfg->ny;
+        gm::build_symbolic(cfg->nx, cfg->ny, e->cfg.leaf_max, e->sym);
+    } catch (const std::bad_alloc &) {
+        delete e;
+        return fail(GM_ERROR_OUT_OF_MEMORY, "host allocation failed in gm_engine_create");
+    } catch (const std::exception &ex) {
+        delete e;
+        return fail(GM_ERROR_INVALID, "symbolic analysis failed: %s", ex.what());
+    }
+    std::unique_ptr<gm_engine> guard(e);
+    GM_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
+    GM_CUDA(cudaEventCreate(&e->ev0));
+    GM_CUDA(cudaEventCreate(&e->ev1));
+
+    const gm::Symbolic &s = e->sym;
+    // level-ordered entry lists in the configured operator orientation
+    std::vector<int64_t> ent_dst;
+    std::vector<int> ent_src;
+    ent_dst.reserve(s.ent_pos.size());
+    ent_src.reserve(s.ent_pos.size());
+    e->levels.resize(s.nlevels);
+    for (int h = 0; h < s.nlevels; ++h) {
+        gm::LevelInfo &L = e->levels[h];
+        L.first = s.lvl_off[h];
+        L.count = s.lvl_off[h + 1] - s.lvl_off[h];
+        L.max_front = s.lvl_max_front[h];
+        L.max_piv = s.lvl_max_piv[h];
+        L.ent_first = (int64_t)ent_dst.size();
+        for (int t = L.first; t < L.first + L.count; ++t) {
+            const int v = s.lvl_nodes[t];
+            for (int64_t q = s.ent_off[v]; q < s.ent_off[v + 1]; ++q) {
+                ent_dst.push_back(s.front_off[v] + s.ent_pos[q]);
+                int id = s.ent_id[q];
+                if (e->cfg.op_mode == GM_OP_EXACT) {   // M = A: entry (r, c) reads A[r][c]
+                    const int dir = id / s.n, c = id % s.n;
+                    const int r = c + gm::stencil_di(dir) + gm::stencil_dj(dir) * s.nx;
+                    id = (8 - dir) * s.n + r;
+                }
+                ent_src.push_back(id);
+            }
+        }
+        L.ent_count = (int64_t)ent_dst.size() - L.ent_first;
+    }
+    int rc2;
+    if ((rc2 = upload(e->d_npiv, s.npiv, e->st)) || (rc2 = upload(e->d_nfront, s.nfront, e->st)) ||
+        (rc2 = upload(e->d_child0, s.child0, e->st)) || (rc2 = upload(e->d_child1, s.child1, e->st)) ||
+        (rc2 = upload(e->d_vars, s.vars, e->st)) || (rc2 = upload(e->d_inv, s.inv, e->st)) ||
+        (rc2 = upload(e->d_lvl_nodes, s.lvl_nodes, e->st)) || (rc2 = upload(e->d_front_off, s.front_off, e->st)) ||
+        (rc2 = upload(e->d_var_off, s.var_off, e->st)) || (rc2 = upload(e->d_inv_off, s.inv_off, e->st)) ||
+        (rc2 = upload(e->d_rhs_off, s.rhs_off, e->st)) || (rc2 = upload(e->d_ent_dst, ent_dst, e->st)) ||
+        (rc2 = upload(e->d_ent_src, ent_src, e->st)))
+        return rc2;
+    GM_CUDA(cudaStreamSynchronize(e->st));
+    gm::DevSym &d = e->dsym;
+    d.n = s.n; d.nnodes = s.nnodes;
+    d.npiv = e->d_npiv.as<int>(); d.nfront = e->d_nfront.as<int>();
+    d.child0 = e->d_child0.as<int>(); d.child1 = e->d_child1.as<int>();
+    d.vars = e->d_vars.as<int>(); d.inv = e->d_inv.as<int>(); d.lvl_nodes = e->d_lvl_nodes.as<int>();
+    d.front_off = e->d_front_off.as<int64_t>(); d.var_off = e->d_var_off.as<int64_t>();
+    d.inv_off = e->d_inv_off.as<int64_t>(); d.rhs_off = e->d_rhs_off.as<int64_t>();
+    d.front_total = s.front_total; d.rhs_total = s.rhs_total;
+
+    gm_stats &st = e->stats;
+    st.n = s.n;
+    st.nonzero = 9LL * cfg->nx * cfg->ny - 6LL * cfg->nx - 6LL * cfg->ny + 4;
+    st.nnodes = s.nnodes; st.nlevels = s.nlevels;
+    st.max_front = *std::max_element(s.nfront.begin(), s.nfront.end());
+    st.max_piv = *std::max_element(s.npiv.begin(), s.npiv.end());
+    st.front_entries = s.front_total;
+    st.factor_entries = s.factor_entries;
+    st.factor_flops = s.factor_flops;
+    st.solve_flops_per_rhs = s.solve_flops_per_rhs;
+    *out = guard.release();
+    return GM_OK;
+}
+
+extern "C" int gm_engine_destroy(gm_engine *e) {
+    if (!e) return GM_OK;
+    cudaSetDevice(e->device);
+    if (e->st) cudaStreamSynchronize(e->st);
+    delete e;  // releases the stream, the events and every device buffer
+    return GM_OK;
+}
+
+extern "C" int gm_engine_stats(const gm_engine *e, gm_stats *out) {
+    if (!e || !out) return fail(GM_ERROR_INVALID, "gm_engine_stats: null argument");
+    *out = e->stats;
+    return GM_OK;
+}
+
+extern "C" int gm_set_model(gm_engine *e, const float *mat0, const float *mat1) {
+    if (!e || !mat0 || !mat1) return fail(GM_ERROR_INVALID, "gm_set_model: null argument");
+    GM_CUDA(cudaSetDevice(e->device));
+    const size_t nb = (size_t)e->n * sizeof(float);
+    GM_ALLOC(e->d_m0, nb);
+    GM_ALLOC(e->d_m1, nb);
+    GM_ALLOC(e->d_stiff, nb);
+    GM_CUDA(cudaMemcpyAsync(e->d_m0.p, mat0, nb, cudaMemcpyDefault, e->st));
+    GM_CUDA(cudaMemcpyAsync(e->d_m1.p, mat1, nb, cudaMemcpyDefault, e->st));
+    GM_CUDA(cudaStreamSynchronize(e->st));
+    e->have_model = true;
+    e->factored = false;
+    return GM_OK;
+}
+
+namespace gm {
+
+// Assemble all frequencies of the batch into e->d_A (device, asynchronous).
+static int assemble_batch(gm_engine *e) {
+    const gm_config &c = e->cfg;
+    const int n = e->n, nf = e->nf;
+    const int pml_stride = 4 * (c.nx + 2) + 4 * (c.ny + 2);
+    std::vector<float> pml((size_t)nf * pml_stride);
+    std::vector<AsmFreq> fq(nf);
+    for (int f = 0; f < nf; ++f) {
+        gmh_pml(c.nx, c.ny, c.dh, c.npml, c.free_surf, c.a0_pml, c.s, e->freqs[f], pml.data() + (size_t)f * pml_stride);
+        float om2[2], om[2], om2mu0[2];
+        gmh_assembly_scalars(c.physics, e->freqs[f], c.s, om2, om, om2mu0);
+        fq[f].om2 = make_float2(om2[0], om2[1]);
+        fq[f].om = make_float2(om[0], om[1]);
+        fq[f].om2mu0 = make_float2(om2mu0[0], om2mu0[1]);
+    }
+    GM_ALLOC(e->d_A, (size_t)nf * 9 * n * sizeof(double2));
+    GM_ALLOC(e->d_mass, (size_t)nf * n * sizeof(float2));
+    GM_ALLOC(e->d_pml, pml.size() * sizeof(float));
+    GM_ALLOC(e->d_fq, fq.size() * sizeof(AsmFreq));
+    GM_CUDA(cudaMemcpyAsync(e->d_pml.p, pml.data(), pml.size() * sizeof(float), cudaMemcpyHostToDevice, e->st));
+    GM_CUDA(cudaMemcpyAsync(e->d_fq.p, fq.data(), fq.size() * sizeof(AsmFreq), cudaMemcpyHostToDevice, e->st));
+    AsmArgs a{};
+    a.nx = c.nx; a.ny = c.ny; a.n = n; a.nf = nf; a.physics = c.physics;
+    gmh_fd_weights(c.dh, a.w);
+    a.pml = e->d_pml.as<float>();
+    a.pml_stride = pml_stride;
+    a.stiff = e->d_stiff.as<float>();
+    a.mass = e->d_mass.as<float2>();
+    a.A = e->d_A.as<double2>();
+    launch_assemble(a, e->d_m0.as<float>(), e->d_m1.as<float>(), e->d_fq.as<AsmFreq>(), e->d_stiff.as<float>(), e->st);
+    GM_CUDA(cudaGetLastError());
+    return GM_OK;
+}
+
+template <class R>
+static int factor_batch(gm_engine *e, R pivtol) {
+    FactorArgs<R> a{};
+    a.s = e->dsym;
+    a.front = e->d_front.p;
+    a.A = e->d_A.as<double2>();
+    a.ent_dst = e->d_ent_dst.as<int64_t>();
+    a.ent_src = e->d_ent_src.as<int>();
+    a.nf = e->nf;
+    a.pivtol = pivtol;
+    a.npert = e->d_npert.as<unsigned long long>();
+    for (const LevelInfo &L : e->levels) launch_factor_level<R>(a, L, e->st);
+    GM_CUDA(cudaGetLastError());
+    return GM_OK;
+}
+
+}  // namespace gm
+
+extern "C" int gm_factor(gm_engine *e, int nfreq, const float *h_freqs) {
+    if (!e || nfreq <= 0 || !h_freqs) return fail(GM_ERROR_INVALID, "gm_factor: bad argument");
+    if (!e->have_model) return fail(GM_ERROR_STATE, "gm_factor: no model set (gm_set_model)");
+    for (int f = 0; f < nfreq; ++f)
+        if (!(h_freqs[f] > 0.f) || !std::isfinite(h_freqs[f])) return fail(GM_ERROR_INVALID, "frequency %d is not positive", f);
+    GM_CUDA(cudaSetDevice(e->device));
+    e->factored = false;
+    e->nf = nfreq;
+    e->freqs.assign(h_freqs, h_freqs + nfreq);
+
+    GM_CUDA(cudaEventRecord(e->ev0, e->st));
+    int rc = gm::assemble_batch(e);
+    if (rc) return rc;
+    GM_CUDA(cudaEventRecord(e->ev1, e->st));
+    GM_CUDA(cudaEventSynchronize(e->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    e->stats.ms_assemble = ms;
+
+    // static-pivot threshold relative to the largest operator entry
+    std::vector<double2> tmp;
+    double amax = 0;
+    {
+        // centre coefficients dominate the stencil; sample all nine directions of a few rows per frequency
+        const int n = e->n;
+        tmp.resize(9);
+        const int rows[3] = {n / 2, n / 3, (2 * n) / 3};
+        for (int f = 0; f < nfreq; ++f)
+            for (int r : rows) {
+                for (int q = 0; q < 9; ++q)
+                    GM_CUDA(cudaMemcpy(&tmp[q], e->d_A.as<double2>() + (size_t)f * 9 * n + (size_t)q * n + r, sizeof(double2),
+                                       cudaMemcpyDeviceToHost));
+                for (int q = 0; q < 9; ++q) amax = std::max(amax, std::hypot(tmp[q].x, tmp[q].y));
+            }
+    }
+    const bool fp64 = e->cfg.precision == GM_PREC_FP64;
+    const size_t fbytes = (size_t)nfreq * e->sym.front_total * e->csize();
+    GM_ALLOC(e->d_front, fbytes);
+    GM_ALLOC(e->d_npert, sizeof(unsigned long long));
+    GM_CUDA(cudaMemsetAsync(e->d_npert.p, 0, sizeof(unsigned long long), e->st));
+    GM_CUDA(cudaEventRecord(e->ev0, e->st));
+    rc = fp64 ? gm::factor_batch<double>(e, 1e-13 * amax) : gm::factor_batch<float>(e, (float)(1e-6 * amax));
+    if (rc) return rc;
+    GM_CUDA(cudaEventRecord(e->ev1, e->st));
+    GM_CUDA(cudaEventSynchronize(e->ev1));
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    e->stats.ms_factor = ms;
+    unsigned long long np = 0;
+    GM_CUDA(cudaMemcpy(&np, e->d_npert.p, sizeof np, cudaMemcpyDeviceToHost));
+    e->stats.perturbed_pivots = (int64_t)np;
+    e->factored = true;
+    return np ? GM_WARNING_PERTURBED : GM_OK;
+}
+
+extern "C" int gm_get_triplets(gm_engine *e, int ifreq, double *Ar, double *Ai, int32_t *irow, int32_t *icol) {
+    if (!e || ifreq < 0 || ifreq >= e->nf || !e->d_A.p) return fail(GM_ERROR_STATE, "gm_get_triplets: no assembled frequency %d", ifreq);
+    GM_CUDA(cudaSetDevice(e->device));
+    const int n = e->n, nx = e->cfg.nx, ny = e->cfg.ny;
+    std::vector<double2> h((size_t)9 * n);
+    GM_CUDA(cudaMemcpy(h.data(), e->d_A.as<double2>() + (size_t)ifreq * 9 * n, h.size() * sizeof(double2),
+                       cudaMemcpyDeviceToHost));
+    size_t c = 0;
+    for (int k = 0; k < n; ++k) {
+        const int x = k % nx, y = k / nx;
+        for (int q = 0; q < 9; ++q) {
+            const int xx = x + gm::stencil_di(q), yy = y + gm::stencil_dj(q);
+            if (xx < 0 || xx >= nx || yy < 0 || yy >= ny) continue;
+            const double2 v = h[(size_t)q * n + k];
+            if (Ar) Ar[c] = v.x;
+            if (Ai) Ai[c] = v.y;
+            if (irow) irow[c] = k;
+            if (icol) icol[c] = yy * nx + xx;
+            ++c;
+        }
+    }
+    return GM_OK;
+}
+
+namespace gm {
+
+template <class R>
+static void substitute(gm_engine *e, void *xT, int nrhs, int trans) {
+    SolveArgs<R> a{};
+    a.s = e->dsym;
+    a.front = e->d_front.p;
+    a.x = xT;
+    a.w = e->d_w.p;
+    a.nf = e->nf;
+    a.nrhs = nrhs;
+    a.ldr = nrhs;
+    a.trans = trans;
+    for (int h = 0; h < (int)e->levels.size(); ++h) launch_solve_forward_level<R>(a, e->levels[h], e->st);
+    for (int h = (int)e->levels.size() - 1; h >= 0; --h) launch_solve_backward_level<R>(a, e->levels[h], e->st);
+}
+
+// x (device, [nf][n][nrhs] c128) = M'^{-1} b with FP64 refinement; b, x device.
+int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const double2 *d_b) {
+    const size_t cnt = (size_t)e->nf * e->n * nrhs;
+    const bool fp64 = e->cfg.precision == GM_PREC_FP64;
+    GM_ALLOC(e->d_t, cnt * e->csize());
+    GM_ALLOC(e->d_w, (size_t)e->nf * e->sym.rhs_total * nrhs * e->csize());
+    GM_ALLOC(e->d_r, cnt * sizeof(double2));
+    const int nblk_max = (e->n + 63) / 64;
+    GM_ALLOC(e->d_part, (size_t)nblk_max * e->nf * nrhs * 2 * sizeof(double));
+    GM_ALLOC(e->d_norm, (size_t)e->nf * nrhs * 2 * sizeof(double));
+
+    cudaEvent_t t0 = e->ev0, t1 = e->ev1;
+    GM_CUDA(cudaEventRecord(t0, e->st));
+    // initial solve in working precision
+    if (fp64) launch_convert_down<double>(d_b, e->d_t.p, cnt, e->st);
+    else launch_convert_down<float>(d_b, e->d_t.p, cnt, e->st);
+    GM_CUDA(cudaMemsetAsync(d_x, 0, cnt * sizeof(double2), e->st));
+    if (fp64) substitute<double>(e, e->d_t.p, nrhs, sys);
+    else substitute<float>(e, e->d_t.p, nrhs, sys);
+    if (fp64) launch_add_up<double>(d_x, e->d_t.p, cnt, e->st);
+    else launch_add_up<float>(d_x, e->d_t.p, cnt, e->st);
+    GM_CUDA(cudaGetLastError());
+    GM_CUDA(cudaEventRecord(t1, e->st));
+    GM_CUDA(cudaEventSynchronize(t1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, t0, t1);
+    e->stats.ms_solve = ms;
+
+    // refinement: r = b - M' x (FP64), x += M'^{-1} r (working precision)
+    ResidArgs ra{};
+    ra.nx = e->cfg.nx; ra.ny = e->cfg.ny; ra.n = e->n; ra.nf = e->nf; ra.nrhs = nrhs; ra.ldr = nrhs;
+    ra.A = e->d_A.as<double2>(); ra.x = d_x; ra.b = d_b; ra.r = e->d_r.as<double2>();
+    ra.op_mode = e->cfg.op_mode; ra.trans = sys;
+    const int cntn = e->nf * nrhs * 2;
+    std::vector<double> norms(cntn);
+    double worst = 0;
+    int it = 0;
+    GM_CUDA(cudaEventRecord(t0, e->st));
+    for (;; ++it) {
+        const int nblk = launch_residual(ra, e->d_part.as<double>(), nblk_max, e->st);
+        launch_reduce_norms(e->d_part.as<double>(), nblk, cntn, e->d_norm.as<double>(), e->st);
+        GM_CUDA(cudaGetLastError());
+        GM_CUDA(cudaMemcpyAsync(norms.data(), e->d_norm.p, cntn * sizeof(double), cudaMemcpyDeviceToHost, e->st));
+        GM_CUDA(cudaStreamSynchronize(e->st));
+        worst = 0;
+        bool finite = true;
+        for (int c = 0; c < e->nf * nrhs; ++c) {
+            const double rr = norms[2 * c], bb = norms[2 * c + 1];
+            if (!std::isfinite(rr)) finite = false;
+            const double rel = bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);
+            worst = std::max(worst, rel);
+        }
+        if (!finite) {
+            e->stats.ir_iterations = it;
+            e->stats.ir_residual = NAN;
+            return fail(GM_ERROR_NONFINITE, "non-finite residual after %d refinement sweeps", it);
+        }
+        if (worst <= e->cfg.ir_tol || it >= e->cfg.ir_max_iter) break;
+        if (fp64) launch_convert_down<double>(e->d_r.as<double2>(), e->d_t.p, cnt, e->st);
+        else launch_convert_down<float>(e->d_r.as<double2>(), e->d_t.p, cnt, e->st);
+        if (fp64) substitute<double>(e, e->d_t.p, nrhs, sys);
+        else substitute<float>(e, e->d_t.p, nrhs, sys);
+        if (fp64) launch_add_up<double>(d_x, e->d_t.p, cnt, e->st);
+        else launch_add_up<float>(d_x, e->d_t.p, cnt, e->st);
+    }
+    GM_CUDA(cudaEventRecord(t1, e->st));
+    GM_CUDA(cudaEventSynchronize(t1));
+    cudaEventElapsedTime(&ms, t0, t1);
+    e->stats.ms_refine = ms;
+    e->stats.ir_iterations = it;
+    e->stats.ir_residual = worst;
+    return worst <= e->cfg.ir_tol ? GM_OK : GM_WARNING_NOT_CONVERGED;
+}
+
+}  // namespace gm
+
+extern "C" int gm_solve(gm_engine *e, int sys, int nrhs, const double *b, double *x) {
+    if (!e || !b || !x || nrhs <= 0) return fail(GM_ERROR_INVALID, "gm_solve: bad argument");
+    if (sys != GM_SYS_A && sys != GM_SYS_AT) return fail(GM_ERROR_INVALID, "gm_solve: unknown sys %d", sys);
+    if (!e->factored) return fail(GM_ERROR_STATE, "gm_solve: no factorisation (gm_factor)");
+    GM_CUDA(cudaSetDevice(e->device));
+    const size_t cnt = (size_t)e->nf * e->n * nrhs;
+    GM_ALLOC(e->d_b, cnt * sizeof(double2));
+    GM_ALLOC(e->d_x, cnt * sizeof(double2));
+    GM_CUDA(cudaMemcpyAsync(e->d_b.p, b, cnt * sizeof(double2), cudaMemcpyDefault, e->st));
+    int rc = gm::engine_solve_device(e, sys, nrhs, e->d_x.as<double2>(), e->d_b.as<double2>());
+    if (rc < 0) return rc;
+    GM_CUDA(cudaMemcpyAsync(x, e->d_x.p, cnt * sizeof(double2), cudaMemcpyDefault, e->st));
+    GM_CUDA(cudaStreamSynchronize(e->st));
+    return rc;
+}

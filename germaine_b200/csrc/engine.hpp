@@ -1,0 +1,93 @@
+// Engine state behind the gm_engine handle.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/germaine_gpu.h"
+#include "common.hpp"
+#include "kernels.cuh"
+#include "symbolic.hpp"
+
+namespace gm {
+
+// Owning device allocation.
+struct DevBuf {
+    void *p = nullptr;
+    size_t bytes = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        bytes = 0;
+    }
+    cudaError_t ensure(size_t nb) {  // grow-only
+        if (nb <= bytes && p) return cudaSuccess;
+        release();
+        cudaError_t e = cudaMalloc(&p, nb ? nb : 16);
+        if (e == cudaSuccess) bytes = nb;
+        else p = nullptr;
+        return e;
+    }
+    template <class T> T *as() const { return reinterpret_cast<T *>(p); }
+};
+
+}  // namespace gm
+
+struct gm_engine {
+    int device = 0;
+    cudaStream_t st = nullptr;
+    gm_config cfg{};
+    int fsshift = 0;
+    int n = 0;
+    gm::Symbolic sym;
+
+    // device copy of the symbolic structure
+    gm::DevBuf d_npiv, d_nfront, d_child0, d_child1, d_vars, d_inv, d_lvl_nodes;
+    gm::DevBuf d_front_off, d_var_off, d_inv_off, d_rhs_off;
+    gm::DevBuf d_ent_dst, d_ent_src;
+    std::vector<gm::LevelInfo> levels;
+    gm::DevSym dsym{};
+
+    // model
+    gm::DevBuf d_m0, d_m1, d_stiff;
+    bool have_model = false;
+
+    // factorisation of the current frequency batch
+    int nf = 0;
+    std::vector<float> freqs;
+    gm::DevBuf d_A, d_mass, d_pml, d_fq, d_front, d_npert;
+    bool factored = false;
+
+    // solve workspaces
+    gm::DevBuf d_x, d_b, d_r, d_t, d_w, d_part, d_norm;
+
+    // epilogue state
+    gm::DevBuf d_src_k, d_rec_k, d_seis, d_field, d_res, d_grad, d_frame, d_frame_pass, d_misc;
+    gm::DevBuf d_xf, d_xa;   // forward / adjoint solutions kept for the gradient
+    std::vector<double> last_grad0, last_grad1;
+
+    gm_stats stats{};
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+
+    gm_engine() = default;
+    gm_engine(const gm_engine &) = delete;
+    gm_engine &operator=(const gm_engine &) = delete;
+    ~gm_engine() {
+        if (ev0) cudaEventDestroy(ev0);
+        if (ev1) cudaEventDestroy(ev1);
+        if (st) cudaStreamDestroy(st);
+    }
+
+    size_t csize() const { return cfg.precision == GM_PREC_FP64 ? sizeof(double2) : sizeof(float2); }
+};
+
+namespace gm {
+// internal entry points shared between translation units
+int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x_out, const double2 *d_b_in);
+}

@@ -1,0 +1,284 @@
+// gm_forward / gm_grad_obj / gm_obj: the per-frequency drivers of the
+// reference (forward_shot_AC, grad_obj_AC, obj_AC and their TE/SH twins)
+// over every shot and every frequency of the factorised batch at once.
+#include <cmath>
+#include <cstring>
+#include <vector>
+
+#include "engine.hpp"
+#include "host_setup.h"
+#include "kernels_epi.cuh"
+
+using gm::fail;
+
+#define GM_CUDA(call)                                                                                       \
+    do {                                                                                                    \
+        cudaError_t err_ = (call);                                                                          \
+        if (err_ != cudaSuccess)                                                                            \
+            return fail(GM_ERROR_CUDA, "%s failed: %s (%s:%d)", #call, cudaGetErrorString(err_), __FILE__, \
+                        __LINE__);                                                                          \
+    } while (0)
+
+#define GM_ALLOC(buf, nbytes)                                                                                   \
+    do {                                                                                                        \
+        cudaError_t err_ = (buf).ensure(nbytes);                                                                \
+        if (err_ != cudaSuccess)                                                                                \
+            return fail(err_ == cudaErrorMemoryAllocation ? GM_ERROR_OUT_OF_MEMORY : GM_ERROR_CUDA,             \
+                        "device allocation of %zu bytes failed: %s", (size_t)(nbytes), cudaGetErrorString(err_)); \
+    } while (0)
+
+namespace {
+
+// iround of fd.h:20 applied to a float quotient, as sources()/receiver() do
+int iround_div(float x, float dh) {
+    const float q = x / dh;
+    return (int)std::floor((double)q + 0.5);
+}
+
+struct Geometry {
+    std::vector<int> ksrc;   // RHS index of each shot (RHS_source_AC.c:32)
+    std::vector<int> krec;   // grid index read for each receiver before the vec2mat shift
+    std::vector<int> kadj;   // RHS index of each adjoint source (RHS_source_AC_adj.c:28)
+};
+
+int make_geometry(const gm_engine *e, int ns, const float *sx, const float *sy, int ntr, const int32_t *rx,
+                  const int32_t *ry, Geometry &g) {
+    const gm_config &c = e->cfg;
+    const int n = e->n;
+    g.ksrc.resize(ns);
+    for (int s = 0; s < ns; ++s) {
+        const int nxs = iround_div(sx[s], c.dh) + c.npml;
+        const int nys = iround_div(sy[s], c.dh) + e->fsshift;
+        const long k = (long)nxs + (long)(nys - 1) * c.nx;
+        if (k < 0 || k >= n)
+            return fail(GM_ERROR_INVALID, "shot %d at (%g, %g) m falls outside the %d x %d grid", s, sx[s], sy[s], c.nx, c.ny);
+        g.ksrc[s] = (int)k;
+    }
+    g.krec.resize(ntr);
+    g.kadj.resize(ntr);
+    for (int t = 0; t < ntr; ++t) {
+        const long kr = (long)(ry[t] + e->fsshift - 1) * c.nx + (rx[t] + c.npml - 1);
+        const long ka = (long)(rx[t] + c.npml) + (long)(ry[t] + e->fsshift - 1) * c.nx;
+        if (kr < 0 || kr >= n || ka < 0 || ka >= n)
+            return fail(GM_ERROR_INVALID, "receiver %d at grid (%d, %d) falls outside the grid", t, rx[t], ry[t]);
+        g.krec[t] = (int)kr;
+        g.kadj[t] = (int)ka;
+    }
+    return GM_OK;
+}
+
+template <class T>
+int upload(gm::DevBuf &buf, const std::vector<T> &v, cudaStream_t st) {
+    GM_ALLOC(buf, v.size() * sizeof(T) + 16);
+    if (!v.empty()) GM_CUDA(cudaMemcpyAsync(buf.p, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice, st));
+    return GM_OK;
+}
+
+// spike right-hand sides of every shot and frequency into e->d_b, forward solve into xout
+int forward_solve(gm_engine *e, int ns, const Geometry &g, double2 *xout) {
+    const int nf = e->nf, n = e->n;
+    std::vector<double2> amp(nf);
+    for (int f = 0; f < nf; ++f) {
+        double a[2];
+        gmh_source_amp(e->cfg.physics, e->freqs[f], e->cfg.s, e->cfg.dh, a);
+        amp[f] = make_double2(a[0], a[1]);
+    }
+    int rc;
+    if ((rc = upload(e->d_src_k, g.ksrc, e->st))) return rc;
+    gm::DevBuf amp_buf;
+    if ((rc = upload(amp_buf, amp, e->st))) return rc;
+    GM_ALLOC(e->d_b, (size_t)nf * n * ns * sizeof(double2));
+    gm::launch_spikes(e->d_b.as<double2>(), n, nf, ns, e->d_src_k.as<int>(), amp_buf.as<double2>(), e->st);
+    GM_CUDA(cudaGetLastError());
+    rc = gm::engine_solve_device(e, GM_SYS_A, ns, xout, e->d_b.as<double2>());
+    GM_CUDA(cudaStreamSynchronize(e->st));  // amp_buf is released on return
+    return rc;
+}
+
+int check_ready(const gm_engine *e, int ns, int ntr) {
+    if (!e) return fail(GM_ERROR_INVALID, "null engine");
+    if (!e->factored) return fail(GM_ERROR_STATE, "no factorisation (call gm_factor first)");
+    if (ns <= 0 || ntr < 0) return fail(GM_ERROR_INVALID, "need at least one shot (nshots=%d, ntr=%d)", ns, ntr);
+    return GM_OK;
+}
+
+// forward + seismograms (cal kept in e->d_res as complex128) ; returns solve status
+int forward_and_seis(gm_engine *e, int ns, const Geometry &g, int ntr, float *seis_out) {
+    const int nf = e->nf, n = e->n;
+    GM_ALLOC(e->d_xf, (size_t)nf * n * ns * sizeof(double2));
+    const int rc = forward_solve(e, ns, g, e->d_xf.as<double2>());
+    if (rc < 0) return rc;
+    if (ntr > 0) {
+        int rc2;
+        if ((rc2 = upload(e->d_rec_k, g.krec, e->st))) return rc2;
+        const size_t cnt = (size_t)nf * ns * ntr;
+        GM_ALLOC(e->d_res, 2 * cnt * sizeof(double2));   // cal | res
+        GM_ALLOC(e->d_seis, cnt * sizeof(float2));
+        gm::launch_gather_seis(e->d_xf.as<double2>(), n, nf, ns, ntr, e->d_rec_k.as<int>(), e->d_seis.as<float2>(),
+                               e->d_res.as<double2>(), e->st);
+        GM_CUDA(cudaGetLastError());
+        if (seis_out) GM_CUDA(cudaMemcpyAsync(seis_out, e->d_seis.p, cnt * sizeof(float2), cudaMemcpyDefault, e->st));
+    }
+    return rc;
+}
+
+// residuals and misfit; leaves res in the second half of e->d_res and the
+// source estimates w/|w| on the host
+int residuals(gm_engine *e, int ns, int ntr, const float *pobs, int stf_inv, int misfit, double &l2,
+              std::vector<double2> &stfu) {
+    const int nf = e->nf;
+    const size_t cnt = (size_t)nf * ns * ntr;
+    const int nfs = nf * ns;
+    GM_ALLOC(e->d_misc, cnt * sizeof(float2) + (size_t)nfs * (sizeof(double) + sizeof(double2)) + 64);
+    float2 *obs = e->d_misc.as<float2>();
+    double *l2p = reinterpret_cast<double *>(obs + cnt);
+    double2 *stf = reinterpret_cast<double2 *>(l2p + nfs + (nfs & 1));
+    GM_CUDA(cudaMemcpyAsync(obs, pobs, cnt * sizeof(float2), cudaMemcpyDefault, e->st));
+    double2 *cal = e->d_res.as<double2>(), *res = cal + cnt;
+    gm::launch_residual_shot(cal, obs, nfs, ntr, stf_inv, misfit, res, l2p, stf, e->st);
+    GM_CUDA(cudaGetLastError());
+    std::vector<double> l2h(nfs);
+    std::vector<double2> stfh(nfs);
+    GM_CUDA(cudaMemcpyAsync(l2h.data(), l2p, nfs * sizeof(double), cudaMemcpyDeviceToHost, e->st));
+    GM_CUDA(cudaMemcpyAsync(stfh.data(), stf, nfs * sizeof(double2), cudaMemcpyDeviceToHost, e->st));
+    GM_CUDA(cudaStreamSynchronize(e->st));
+    l2 = 0;
+    for (double v : l2h) l2 += v;
+    stfu.resize(nfs);
+    for (int i = 0; i < nfs; ++i) {
+        const double a = std::hypot(stfh[i].x, stfh[i].y);
+        stfu[i] = a > 0 ? make_double2(stfh[i].x / a, stfh[i].y / a) : make_double2(1.0, 0.0);
+    }
+    return GM_OK;
+}
+
+}  // namespace
+
+extern "C" int gm_forward(gm_engine *e, int nshots, const float *src_x, const float *src_y, int ntr,
+                          const int32_t *rec_x, const int32_t *rec_y, float *seis, float *field) {
+    int rc = check_ready(e, nshots, ntr);
+    if (rc) return rc;
+    if (!src_x || !src_y || (ntr > 0 && (!rec_x || !rec_y))) return fail(GM_ERROR_INVALID, "gm_forward: null geometry");
+    GM_CUDA(cudaSetDevice(e->device));
+    Geometry g;
+    if ((rc = make_geometry(e, nshots, src_x, src_y, ntr, rec_x, rec_y, g))) return rc;
+    const int solve_rc = forward_and_seis(e, nshots, g, ntr, seis);
+    if (solve_rc < 0) return solve_rc;
+    if (field) {
+        const size_t cnt = (size_t)e->nf * nshots * e->n;
+        GM_ALLOC(e->d_field, cnt * sizeof(float2));
+        gm::launch_field(e->d_xf.as<double2>(), e->n, e->nf, nshots, e->d_field.as<float2>(), e->st);
+        GM_CUDA(cudaGetLastError());
+        GM_CUDA(cudaMemcpyAsync(field, e->d_field.p, cnt * sizeof(float2), cudaMemcpyDefault, e->st));
+    }
+    GM_CUDA(cudaStreamSynchronize(e->st));
+    return solve_rc;
+}
+
+extern "C" int gm_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y, int ntr,
+                      const int32_t *rec_x, const int32_t *rec_y, const float *pobs, int stf_inv, int misfit,
+                      float *l2_out) {
+    int rc = check_ready(e, nshots, ntr);
+    if (rc) return rc;
+    if (!pobs || !l2_out || ntr <= 0) return fail(GM_ERROR_INVALID, "gm_obj: need observed data, receivers and an output");
+    if (misfit < 1 || misfit > 3) return fail(GM_ERROR_INVALID, "gm_obj: MISFIT must be 1, 2 or 3");
+    GM_CUDA(cudaSetDevice(e->device));
+    Geometry g;
+    if ((rc = make_geometry(e, nshots, src_x, src_y, ntr, rec_x, rec_y, g))) return rc;
+    const int solve_rc = forward_and_seis(e, nshots, g, ntr, nullptr);
+    if (solve_rc < 0) return solve_rc;
+    double l2 = 0;
+    std::vector<double2> stfu;
+    if ((rc = residuals(e, nshots, ntr, pobs, stf_inv, misfit, l2, stfu))) return rc;
+    *l2_out = (float)(0.5 * l2);
+    return solve_rc;
+}
+
+extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y, int ntr,
+                           const int32_t *rec_x, const int32_t *rec_y, const float *pobs, int stf_inv, int misfit,
+                           float *grad0, float *grad1, float *l2_out, float *seis) {
+    int rc = check_ready(e, nshots, ntr);
+    if (rc) return rc;
+    if (!pobs || ntr <= 0) return fail(GM_ERROR_INVALID, "gm_grad_obj: need observed data and receivers");
+    if (misfit < 1 || misfit > 3) return fail(GM_ERROR_INVALID, "gm_grad_obj: MISFIT must be 1, 2 or 3");
+    const bool te = e->cfg.physics == GM_PHYS_TE;
+    GM_CUDA(cudaSetDevice(e->device));
+    Geometry g;
+    if ((rc = make_geometry(e, nshots, src_x, src_y, ntr, rec_x, rec_y, g))) return rc;
+    const int nf = e->nf, n = e->n;
+    int worst = forward_and_seis(e, nshots, g, ntr, seis);
+    if (worst < 0) return worst;
+    double l2 = 0;
+    std::vector<double2> stfu;
+    if ((rc = residuals(e, nshots, ntr, pobs, stf_inv, misfit, l2, stfu))) return rc;
+
+    // adjoint sources and the adjoint solve with the same factors
+    if ((rc = upload(e->d_rec_k, g.kadj, e->st))) return rc;
+    const size_t cnt = (size_t)nf * nshots * ntr;
+    const double dh2 = (double)(e->cfg.dh * e->cfg.dh);
+    GM_ALLOC(e->d_b, (size_t)nf * n * nshots * sizeof(double2));
+    gm::launch_adjoint_src(e->d_b.as<double2>(), n, nf, nshots, ntr, e->d_rec_k.as<int>(), e->d_res.as<double2>() + cnt,
+                           dh2, e->st);
+    GM_CUDA(cudaGetLastError());
+    GM_ALLOC(e->d_xa, (size_t)nf * n * nshots * sizeof(double2));
+    const int sys = te ? GM_SYS_AT : GM_SYS_A;   // grad_obj_TE.c:149 vs grad_obj_AC.c:147
+    const int arc = gm::engine_solve_device(e, sys, nshots, e->d_xa.as<double2>(), e->d_b.as<double2>());
+    if (arc < 0) return arc;
+    if (arc > worst) worst = arc;
+
+    // gradient stack + PML frame taper
+    if (!e->d_frame.p) {
+        std::vector<float> coef(n);
+        std::vector<unsigned char> passes(n);
+        gmh_grad_frame(e->cfg.nx, e->cfg.ny, e->cfg.npml, e->cfg.free_surf, coef.data(), passes.data());
+        if ((rc = upload(e->d_frame, coef, e->st))) return rc;
+        if ((rc = upload(e->d_frame_pass, passes, e->st))) return rc;
+    }
+    std::vector<double2> om2(nf), om(nf);
+    for (int f = 0; f < nf; ++f) {
+        float a[2], b[2];
+        gmh_gradient_scalars(e->cfg.physics, e->freqs[f], e->cfg.s, a, b);
+        om2[f] = make_double2(a[0], a[1]);
+        om[f] = make_double2(b[0], b[1]);
+    }
+    gm::DevBuf scal;
+    std::vector<double2> sc;
+    sc.insert(sc.end(), stfu.begin(), stfu.end());
+    sc.insert(sc.end(), om2.begin(), om2.end());
+    sc.insert(sc.end(), om.begin(), om.end());
+    if ((rc = upload(scal, sc, e->st))) return rc;
+    GM_ALLOC(e->d_grad, 2 * (size_t)n * sizeof(double));
+    gm::GradArgs ga{};
+    ga.n = n; ga.nf = nf; ga.ns = nshots; ga.te = te;
+    ga.xf = e->d_xf.as<double2>(); ga.xa = e->d_xa.as<double2>();
+    ga.stfu = scal.as<double2>(); ga.om2 = ga.stfu + stfu.size(); ga.om = ga.om2 + nf;
+    ga.m0 = e->d_m0.as<float>(); ga.m1 = e->d_m1.as<float>();
+    ga.frame = e->d_frame.as<float>(); ga.passes = e->d_frame_pass.as<unsigned char>();
+    ga.g0 = e->d_grad.as<double>(); ga.g1 = ga.g0 + n;
+    gm::launch_gradient(ga, e->st);
+    GM_CUDA(cudaGetLastError());
+    e->last_grad0.resize(n);
+    e->last_grad1.assign(te ? n : 0, 0.0);
+    GM_CUDA(cudaMemcpyAsync(e->last_grad0.data(), ga.g0, n * sizeof(double), cudaMemcpyDeviceToHost, e->st));
+    if (te) GM_CUDA(cudaMemcpyAsync(e->last_grad1.data(), ga.g1, n * sizeof(double), cudaMemcpyDeviceToHost, e->st));
+    GM_CUDA(cudaStreamSynchronize(e->st));
+    std::vector<float> tmp(n);
+    if (grad0) {
+        for (int k = 0; k < n; ++k) tmp[k] = (float)e->last_grad0[k];
+        GM_CUDA(cudaMemcpy(grad0, tmp.data(), n * sizeof(float), cudaMemcpyDefault));
+    }
+    if (grad1 && te) {
+        for (int k = 0; k < n; ++k) tmp[k] = (float)e->last_grad1[k];
+        GM_CUDA(cudaMemcpy(grad1, tmp.data(), n * sizeof(float), cudaMemcpyDefault));
+    }
+    if (l2_out) *l2_out = (float)(0.5 * l2);
+    return worst;
+}
+
+extern "C" int gm_get_gradient_fp64(gm_engine *e, double *g0, double *g1) {
+    if (!e) return fail(GM_ERROR_INVALID, "null engine");
+    if (e->last_grad0.empty()) return fail(GM_ERROR_STATE, "no gradient computed yet");
+    if (g0) std::memcpy(g0, e->last_grad0.data(), e->last_grad0.size() * sizeof(double));
+    if (g1 && !e->last_grad1.empty()) std::memcpy(g1, e->last_grad1.data(), e->last_grad1.size() * sizeof(double));
+    return GM_OK;
+}

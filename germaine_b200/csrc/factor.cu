@@ -1,0 +1,285 @@
+// K2-K4: numeric multifrontal LU of one elimination-tree level, batched
+// over every front of the level and every frequency (the replacement of
+// umfpack_zi_numeric, src/AC/forward_shot_AC.c:61).
+//
+// Fronts live in HBM as dense column-major nfront x nfront complex blocks
+// (one block per node per frequency).  A level is processed by
+//   K2 gather   -- each front pulls its children's contribution blocks
+//                  (extend-add by inverse maps: deterministic, no atomics),
+//   K2 scatter  -- adds the operator entries owned by the front,
+//   K3 panel    -- per NB-wide pivot block: LU of the diagonal block with
+//                  static pivoting (each CTA factors it redundantly in shared
+//                  memory) and the triangular solves of the L and U panels,
+//   K4 update   -- rank-NB Schur update of the trailing front, 64x64 tiles.
+// K3/K4 alternate ceil(max_piv/NB) times per level.  After the last step a
+// front holds L (unit lower) and U in its first npiv rows/columns and its
+// Schur complement (the contribution block) in the trailing block.
+#include "kernels.cuh"
+#include "cplx.cuh"
+
+namespace gm {
+
+constexpr int NB = 32;       // pivot block width
+constexpr int TILE = 64;     // Schur-update tile
+constexpr int PCHUNK = 128;  // panel rows / columns per CTA
+
+template <class R>
+__global__ void k_front_gather(FactorArgs<R> a, int lvl_first) {
+    using C = cplx<R>;
+    const int node = a.s.lvl_nodes[lvl_first + blockIdx.y];
+    const int f = a.s.nfront[node];
+    const int j = blockIdx.x;
+    if (j >= f) return;
+    C *base = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.z * a.s.front_total;
+    C *F = base + a.s.front_off[node];
+    const int *inv = a.s.inv + a.s.inv_off[node];
+    const int c0 = a.s.child0[node], c1 = a.s.child1[node];
+    const int b0 = c0 >= 0 ? inv[j] : -1;
+    const int b1 = c1 >= 0 ? inv[f + j] : -1;
+    const C *cb0 = nullptr, *cb1 = nullptr;
+    int f0 = 0, f1 = 0;
+    if (b0 >= 0) {
+        const int s0 = a.s.npiv[c0]; f0 = a.s.nfront[c0];
+        cb0 = base + a.s.front_off[c0] + s0 + (size_t)(s0 + b0) * f0;
+    }
+    if (b1 >= 0) {
+        const int s1 = a.s.npiv[c1]; f1 = a.s.nfront[c1];
+        cb1 = base + a.s.front_off[c1] + s1 + (size_t)(s1 + b1) * f1;
+    }
+    for (int i = threadIdx.x; i < f; i += blockDim.x) {
+        C v = czero<C>();
+        if (cb0) { const int r = inv[i]; if (r >= 0) v = cadd(v, cb0[r]); }
+        if (cb1) { const int r = inv[f + i]; if (r >= 0) v = cadd(v, cb1[r]); }
+        F[i + (size_t)j * f] = v;
+    }
+}
+
+template <class R>
+__global__ void k_entry_scatter(FactorArgs<R> a, int64_t e0, int64_t cnt) {
+    using C = cplx<R>;
+    const int64_t e = e0 + (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (e >= e0 + cnt) return;
+    C *F = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.y * a.s.front_total;
+    const double2 v = a.A[(size_t)blockIdx.y * 9 * a.s.n + a.ent_src[e]];
+    C &d = F[a.ent_dst[e]];
+    d = cadd(d, cconv<C>(v));
+}
+
+// Factor the kb x kb diagonal block D (shared memory, column stride NB+1)
+// in place: unit-lower L and upper U, static pivoting.  Returns (through
+// shared memory) the reciprocals of the pivots.
+template <class R>
+__device__ void diag_lu(cplx<R> (*D)[NB + 1], cplx<R> *rdiag, int kb, R pivtol, int *nperturbed) {
+    using C = cplx<R>;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int p = 0; p < kb; ++p) {
+        if (tid == 0) {
+            C piv = D[p][p];
+            const R mag = sqrt(cabs2(piv));
+            if (!(mag >= pivtol)) {   // also catches NaN
+                if (mag > R(0)) {
+                    const R sc = pivtol / mag;
+                    piv = mk(piv.x * sc, piv.y * sc);
+                } else {
+                    piv = mk(pivtol, R(0));
+                }
+                D[p][p] = piv;
+                ++*nperturbed;
+            }
+            rdiag[p] = crcp(piv);
+        }
+        __syncthreads();
+        const C rp = rdiag[p];
+        for (int r = p + 1 + tid; r < kb; r += nt) D[r][p] = cmul(D[r][p], rp);
+        __syncthreads();
+        const int m = kb - p - 1;
+        for (int t = tid; t < m * m; t += nt) {
+            const int r = p + 1 + t % m, c = p + 1 + t / m;
+            cfms(D[r][c], D[r][p], D[p][c]);
+        }
+        __syncthreads();
+    }
+}
+
+template <class R>
+__global__ void __launch_bounds__(PCHUNK) k_panel(FactorArgs<R> a, int lvl_first, int k0) {
+    using C = cplx<R>;
+    const int node = a.s.lvl_nodes[lvl_first + blockIdx.y];
+    const int s = a.s.npiv[node];
+    if (k0 >= s) return;
+    const int f = a.s.nfront[node];
+    const int kb = min(NB, s - k0);
+    const int i0 = k0 + kb;            // first trailing index
+    const int m = f - i0;              // trailing size
+    const int nchunk = (m + PCHUNK - 1) / PCHUNK;
+    const int bx = blockIdx.x;
+    if (bx >= 2 * nchunk) return;
+    C *F = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.z * a.s.front_total + a.s.front_off[node];
+
+    // Every CTA factors the diagonal block redundantly from the unmodified
+    // front; the factored block is written back by k_update's last CTA, after
+    // this kernel has finished reading it.
+    __shared__ C D[NB][NB + 1];
+    __shared__ C rdiag[NB];
+    __shared__ int npert;
+    if (threadIdx.x == 0) npert = 0;
+    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+        const int r = t % kb, c = t / kb;
+        D[r][c] = F[(k0 + r) + (size_t)(k0 + c) * f];
+    }
+    __syncthreads();
+    diag_lu<R>(D, rdiag, kb, a.pivtol, &npert);
+
+    if (bx < nchunk) {
+        // L panel: row i solves x U = a  (U = upper triangle of D incl. diagonal)
+        const int i = i0 + bx * PCHUNK + threadIdx.x;
+        if (i < f) {
+            C x[NB];
+#pragma unroll
+            for (int c = 0; c < NB; ++c) x[c] = c < kb ? F[i + (size_t)(k0 + c) * f] : czero<C>();
+#pragma unroll
+            for (int c = 0; c < NB; ++c) {
+                if (c < kb) {
+                    C acc = x[c];
+#pragma unroll
+                    for (int l = 0; l < c; ++l) cfms(acc, x[l], D[l][c]);
+                    x[c] = cmul(acc, rdiag[c]);
+                }
+            }
+#pragma unroll
+            for (int c = 0; c < NB; ++c)
+                if (c < kb) F[i + (size_t)(k0 + c) * f] = x[c];
+        }
+    } else if (bx < 2 * nchunk) {
+        // U panel: column j solves L y = a (unit lower triangle of D)
+        const int j = i0 + (bx - nchunk) * PCHUNK + threadIdx.x;
+        if (j < f) {
+            C y[NB];
+            C *col = F + (size_t)j * f + k0;
+#pragma unroll
+            for (int r = 0; r < NB; ++r) y[r] = r < kb ? col[r] : czero<C>();
+#pragma unroll
+            for (int r = 0; r < NB; ++r) {
+                if (r < kb) {
+                    C acc = y[r];
+#pragma unroll
+                    for (int l = 0; l < r; ++l) cfms(acc, D[r][l], y[l]);
+                    y[r] = acc;
+                }
+            }
+#pragma unroll
+            for (int r = 0; r < NB; ++r)
+                if (r < kb) col[r] = y[r];
+        }
+    }
+}
+
+// Trailing update C -= Lp * Up on one TILE x TILE tile; 256 threads, each
+// owns a 4 x 4 complex sub-tile with rows tx + 16a and columns ty + 16b.
+template <class R>
+__global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, int k0, int ntmax) {
+    using C = cplx<R>;
+    const int node = a.s.lvl_nodes[lvl_first + blockIdx.y];
+    const int s = a.s.npiv[node];
+    if (k0 >= s) return;
+    const int f = a.s.nfront[node];
+    const int kb = min(NB, s - k0);
+    const int i0 = k0 + kb, m = f - i0;
+    const int nt = (m + TILE - 1) / TILE;
+    C *F = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.z * a.s.front_total + a.s.front_off[node];
+    if (blockIdx.x == (unsigned)(ntmax * ntmax)) {
+        // write back the factored diagonal block of this step (k_panel only
+        // read it); the tiles of this kernel never touch that block.
+        __shared__ C D[NB][NB + 1];
+        __shared__ C rdiag[NB];
+        __shared__ int npert;
+        if (threadIdx.x == 0) npert = 0;
+        for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+            const int r = t % kb, c = t / kb;
+            D[r][c] = F[(k0 + r) + (size_t)(k0 + c) * f];
+        }
+        __syncthreads();
+        diag_lu<R>(D, rdiag, kb, a.pivtol, &npert);
+        for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
+            const int r = t % kb, c = t / kb;
+            F[(k0 + r) + (size_t)(k0 + c) * f] = D[r][c];
+        }
+        if (threadIdx.x == 0 && npert) atomicAdd(a.npert, (unsigned long long)npert);
+        return;
+    }
+    const int ti = blockIdx.x / ntmax, tj = blockIdx.x % ntmax;
+    if (ti >= nt || tj >= nt) return;
+
+    extern __shared__ unsigned char smem_raw[];
+    C *Ls = reinterpret_cast<C *>(smem_raw);   // [NB][TILE]: Ls[c*TILE + r]
+    C *Us = Ls + NB * TILE;                    // [NB][TILE]: Us[c*TILE + col]
+    const int r0 = i0 + ti * TILE, c0 = i0 + tj * TILE;
+    for (int t = threadIdx.x; t < NB * TILE; t += blockDim.x) {
+        const int r = t % TILE, c = t / TILE;
+        Ls[t] = (c < kb && r0 + r < f) ? F[(r0 + r) + (size_t)(k0 + c) * f] : czero<C>();
+        const int col = t / NB, cc = t % NB;   // U: contiguous along the pivot index
+        Us[cc * TILE + col] = (cc < kb && c0 + col < f) ? F[(k0 + cc) + (size_t)(c0 + col) * f] : czero<C>();
+    }
+    __syncthreads();
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    C acc[4][4];
+#pragma unroll
+    for (int p = 0; p < 4; ++p)
+#pragma unroll
+        for (int q = 0; q < 4; ++q) acc[p][q] = czero<C>();
+    for (int c = 0; c < kb; ++c) {
+        C lv[4], uv[4];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) lv[p] = Ls[c * TILE + tx + 16 * p];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) uv[q] = Us[c * TILE + ty + 16 * q];
+#pragma unroll
+        for (int p = 0; p < 4; ++p)
+#pragma unroll
+            for (int q = 0; q < 4; ++q) cfma(acc[p][q], lv[p], uv[q]);
+    }
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        const int col = c0 + ty + 16 * q;
+        if (col >= f) continue;
+#pragma unroll
+        for (int p = 0; p < 4; ++p) {
+            const int row = r0 + tx + 16 * p;
+            if (row < f) {
+                C &d = F[row + (size_t)col * f];
+                d = csub(d, acc[p][q]);
+            }
+        }
+    }
+}
+
+template <class R>
+void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
+    using C = cplx<R>;
+    if (L.count == 0) return;
+    k_front_gather<R><<<dim3(L.max_front, L.count, a.nf), 128, 0, st>>>(a, L.first);
+    if (L.ent_count > 0) {
+        const int tpb = 256;
+        k_entry_scatter<R><<<dim3((unsigned)((L.ent_count + tpb - 1) / tpb), a.nf), tpb, 0, st>>>(a, L.ent_first,
+                                                                                                  L.ent_count);
+    }
+    const size_t smem = 2 * NB * TILE * sizeof(C);
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set = true;
+    }
+    for (int k0 = 0; k0 < L.max_piv; k0 += NB) {
+        const int mmax = L.max_front - k0 - 1;   // largest trailing size (kb >= 1)
+        const int nchunk = mmax > 0 ? (mmax + PCHUNK - 1) / PCHUNK : 0;
+        if (nchunk > 0)
+            k_panel<R><<<dim3(2 * nchunk, L.count, a.nf), PCHUNK, 0, st>>>(a, L.first, k0);
+        const int ntmax = mmax > 0 ? (mmax + TILE - 1) / TILE : 0;
+        k_update<R><<<dim3(ntmax * ntmax + 1, L.count, a.nf), 256, smem, st>>>(a, L.first, k0, ntmax);
+    }
+}
+
+template void launch_factor_level<double>(const FactorArgs<double> &, const LevelInfo &, cudaStream_t);
+template void launch_factor_level<float>(const FactorArgs<float> &, const LevelInfo &, cudaStream_t);
+
+}  // namespace gm

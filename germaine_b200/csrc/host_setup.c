@@ -1,0 +1,174 @@
+/*
+ * Host-side per-frequency set-up scalars and 1-D profiles of the engine.
+ *
+ * These are O(1) or O(NX+NY) per frequency, computed on the host exactly as
+ * the reference computes them (same C99 complex types, gcc, no FMA) and
+ * uploaded to the device; all O(NX*NY) work runs in the CUDA kernels.  The
+ * file is C, not C++, because the roundings of C99 complex float/double
+ * arithmetic (complex float division, promotion of complex float to complex
+ * double next to a double literal, glibc cpowf) are part of the reference's
+ * numerics that the assembly kernel must reproduce bit for bit.
+ */
+#include <complex.h>
+#include <math.h>
+#include <string.h>
+
+#include "host_setup.h"
+
+#ifndef M_PI
+#define M_PI 3.14159265358979323846
+#endif
+
+/* mixed-grid weights a, b, c, d, e and 1/DH^2: src/AC/init_A_AC_9p_pml.c:34-43 */
+void gmh_fd_weights(float dh, float w[6])
+{
+    float a = 0.6287326, b = 0.3712667, c, d, e, idh2;
+    c = 1 - a - b;
+    b = 0.25 * b;
+    c = 0.25 * c;
+    d = 0.4382634;
+    e = 1 - d;
+    idh2 = 1.0 / (dh * dh);
+    w[0] = a; w[1] = b; w[2] = c; w[3] = d; w[4] = e; w[5] = idh2;
+}
+
+/* 1-D PML stretch profiles, src/pml_pro.c:20-160.  out holds 4 x-arrays of
+ * NX+2 (node r/i, half-node r/i) followed by 4 y-arrays of NY+2. */
+void gmh_pml(int nx, int ny, float dh, int npml, int free_surf, float a0_pml, float s,
+             float freq, float *out)
+{
+    const int nxa = nx + 2, nya = ny + 2;
+    float *xr = out, *xi = out + nxa, *xhr = out + 2 * nxa, *xhi = out + 3 * nxa;
+    float *yr = out + 4 * nxa, *yi = yr + nya, *yhr = yi + nya, *yhi = yhr + nya;
+    const float half_pi = M_PI / 2.0;
+    const complex float ci = 0.0 + 1.0 * I;
+    const float width = npml * dh;
+    const complex float omega = 2.0 * M_PI * (freq - I * s);
+    int k;
+    for (k = 0; k < nxa; k++) { xr[k] = 1.0f; xi[k] = 0.0f; xhr[k] = 1.0f; xhi[k] = 0.0f; }
+    for (k = 0; k < nya; k++) { yr[k] = 1.0f; yi[k] = 0.0f; yhr[k] = 1.0f; yhi[k] = 0.0f; }
+    for (k = 1; k <= npml; k++) {
+        const float x = k * dh;
+        const float xh = x + 0.5 * dh;
+        const float damp = a0_pml * (1.0 - cos((width - x) * half_pi / width));
+        const float damph = a0_pml * (1.0 - cos((width - xh) * half_pi / width));
+        const complex double node = 1.0 / (1.0 + damp / (ci * omega));
+        const complex double half = 1.0 / (1.0 + damph / (ci * omega));
+        xr[k] = creal(node); xi[k] = cimag(node);
+        xhr[k] = creal(half); xhi[k] = cimag(half);
+        yr[k] = xr[k]; yi[k] = xi[k]; yhr[k] = xhr[k]; yhi[k] = xhi[k];
+        xr[nx - k + 1] = xr[k]; xi[nx - k + 1] = xi[k];
+        xhr[nx - k + 1] = xhr[k]; xhi[nx - k + 1] = xhi[k];
+        yr[ny - k + 1] = xr[k]; yi[ny - k + 1] = xi[k];
+        yhr[ny - k + 1] = xhr[k]; yhi[ny - k + 1] = xhi[k];
+        if (free_surf == 1) { yr[k] = 1.0f; yi[k] = 0.0f; yhr[k] = 1.0f; yhi[k] = 0.0f; }
+    }
+    xr[0] = xr[1]; xi[0] = xi[1]; xhr[0] = xhr[1]; xhi[0] = xhi[1];
+    xr[nx + 1] = xr[nx]; xi[nx + 1] = xi[nx]; xhr[nx + 1] = xhr[nx]; xhi[nx + 1] = xhi[nx];
+    yr[0] = yr[1]; yi[0] = yi[1]; yhr[0] = yhr[1]; yhi[0] = yhi[1];
+    yr[ny + 1] = yr[ny]; yi[ny + 1] = yi[ny]; yhr[ny + 1] = yhr[ny]; yhi[ny + 1] = yhi[ny];
+}
+
+/* Per-frequency scalars of the assembly:
+ *   om2    = Omega^2 via glibc cpowf, AC: (2 pi (f - iS))^2
+ *            (init_A_AC_9p_pml.c:50), SH/TE: (2 pi (f + iS))^2
+ *            (init_A_SH_9p_pml.c:50, init_A_TE_9p_pml.c:55);
+ *   om     = TE Omega = 2 pi (f + iS) (init_A_TE_9p_pml.c:54);
+ *   om2mu0 = TE Omega^2 * mu0, mu0 = 4 pi 1e-7 (init_A_TE_9p_pml.c:58). */
+void gmh_assembly_scalars(int physics, float freq, float s, float om2[2], float om[2], float om2mu0[2])
+{
+    complex float o2, o = 0.0f, o2m;
+    const float mu0 = 4.0 * M_PI * 1e-7;
+    if (physics == 1) {
+        o2 = cpowf(2.0 * M_PI * (freq - s * I), 2.0);
+    } else {
+        o2 = cpowf(2.0 * M_PI * (freq + s * I), 2.0);
+        o = 2.0 * M_PI * (freq + s * I);
+    }
+    o2m = o2 * mu0;
+    om2[0] = crealf(o2); om2[1] = cimagf(o2);
+    om[0] = crealf(o); om[1] = cimagf(o);
+    om2mu0[0] = crealf(o2m); om2mu0[1] = cimagf(o2m);
+}
+
+/* Spike-source amplitude over DH^2 as stored into the double RHS:
+ * AC/SH src/AC/RHS_source_AC.c:48-53 (amp 1), TE src/TE/RHS_source_TE.c:40-55
+ * (amp = -i Omega mu0). */
+void gmh_source_amp(int physics, float freq, float s, float dh, double amp[2])
+{
+    float ar = 1.0f, ai = 0.0f;
+    if (physics == 4) {
+        const complex float omega = 2.0 * M_PI * (freq + s * I);
+        const float mu0 = 4.0 * M_PI * 1e-7;
+        ar = -creal((omega * mu0 * I) * (1.0 + 0.0 * I));
+        ai = -cimag((omega * mu0 * I) * (1.0 + 0.0 * I));
+    }
+    amp[0] = ar / (dh * dh);
+    amp[1] = ai / (dh * dh);
+}
+
+/* Gradient scalars: AC Omega^2 = cpowf((2 pi f) - iS, 2) (ass_grad_AC.c:22);
+ * TE Omega = 2 pi (f + iS), Omega^2 = cpowf(2 pi (f + iS), 2)
+ * (ass_grad_TE.c:22-23). */
+void gmh_gradient_scalars(int physics, float freq, float s, float om2[2], float om[2])
+{
+    complex float o2, o = 0.0f;
+    if (physics == 4) {
+        o = 2.0 * M_PI * (freq + (I * s));
+        o2 = cpowf(2.0 * M_PI * (freq + (I * s)), 2.0);
+    } else {
+        o2 = cpowf(((2.0 * M_PI * freq) - (I * s)), 2.0);
+    }
+    om2[0] = crealf(o2); om2[1] = cimagf(o2);
+    om[0] = crealf(o); om[1] = cimagf(o);
+}
+
+/* |w| and w/|w| of the source-wavelet estimate, as ass_grad_AC forms
+ * (wien/cabsf(wien)) (src/AC/ass_grad_AC.c:30). */
+void gmh_stf_unit(const float stf[2], float unit[2])
+{
+    const complex float w = stf[0] + stf[1] * I;
+    const complex float u = w / cabsf(w);
+    unit[0] = crealf(u); unit[1] = cimagf(u);
+}
+
+/* Wiener source estimate from accumulated sums, src/AC/calc_res_AC.c:40:
+ * wien = num / den in complex float. */
+void gmh_wiener(const float num[2], const float den[2], float wien[2])
+{
+    const complex float a = num[0] + num[1] * I, b = den[0] + den[1] * I;
+    const complex float w = a / b;
+    wien[0] = crealf(w); wien[1] = cimagf(w);
+}
+
+/* PML taper of cp_grad_frame (PML_grad = 3), src/cp_grad_frame.c:108-170:
+ * coefficient field [NY][NX] and per-point multiplicity (how many of the
+ * reference's left/right/top/bottom passes multiply the point). */
+void gmh_grad_frame(int nx, int ny, int npml, int free_surf, float *coef, unsigned char *passes)
+{
+    const int fsshift = free_surf ? 0 : npml;
+    const int nx0 = nx - 2 * npml, ny0 = ny - npml - fsshift;
+    float c[1024];
+    float damping = 60.0, amp = 1.0 - damping / 100.0, a;
+    int p, i, j;
+    if (npml < 2 || npml > 1023) {
+        for (i = 0; i < nx * ny; i++) { coef[i] = 1.0f; passes[i] = 0; }
+        return;
+    }
+    a = sqrt(-log(amp) / ((npml - 1) * (npml - 1)));
+    for (p = 1; p <= npml; p++) c[p] = exp(-(a * a * (npml - p) * (npml - p)));
+    for (i = 0; i < nx * ny; i++) { coef[i] = 1.0f; passes[i] = 0; }
+#define COEF(jj, ii) coef[((jj) - 1) * nx + (ii) - 1]
+#define PASS(jj, ii) passes[((jj) - 1) * nx + (ii) - 1]
+    for (p = 1; p <= npml; p++) for (j = p; j <= ny - p + 1; j++) COEF(j, p) = c[p];
+    for (p = 1; p <= npml; p++) for (j = p; j <= ny - p + 1; j++) COEF(j, nx - p + 1) = c[p];
+    if (free_surf == 0)
+        for (p = 1; p <= npml; p++) for (i = p; i <= nx - p + 1; i++) COEF(p, i) = c[p];
+    for (p = 1; p <= npml; p++) for (i = p; i <= nx - p + 1; i++) COEF(ny - p + 1, i) = c[p];
+    for (i = 1; i <= npml; i++) for (j = 1; j <= ny; j++) PASS(j, i)++;
+    for (i = npml + nx0 + 1; i <= nx; i++) for (j = 1; j <= ny; j++) PASS(j, i)++;
+    if (free_surf == 0) for (i = 1; i <= nx; i++) for (j = 1; j <= npml; j++) PASS(j, i)++;
+    for (i = 1; i <= nx; i++) for (j = fsshift + ny0 + 1; j <= ny; j++) PASS(j, i)++;
+#undef COEF
+#undef PASS
+}

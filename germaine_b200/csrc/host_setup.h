@@ -1,0 +1,19 @@
+/* Host-side per-frequency set-up (see host_setup.c). */
+#ifndef GM_HOST_SETUP_H
+#define GM_HOST_SETUP_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+void gmh_fd_weights(float dh, float w[6]);
+void gmh_pml(int nx, int ny, float dh, int npml, int free_surf, float a0_pml, float s,
+             float freq, float *out);
+void gmh_assembly_scalars(int physics, float freq, float s, float om2[2], float om[2], float om2mu0[2]);
+void gmh_source_amp(int physics, float freq, float s, float dh, double amp[2]);
+void gmh_gradient_scalars(int physics, float freq, float s, float om2[2], float om[2]);
+void gmh_stf_unit(const float stf[2], float unit[2]);
+void gmh_wiener(const float num[2], const float den[2], float wien[2]);
+void gmh_grad_frame(int nx, int ny, int npml, int free_surf, float *coef, unsigned char *passes);
+#ifdef __cplusplus
+}
+#endif
+#endif

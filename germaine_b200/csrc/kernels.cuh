@@ -1,0 +1,98 @@
+// Device-side argument blocks and launch wrappers shared by the engine.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/germaine_gpu.h"
+
+namespace gm {
+
+// ---------------- K1 assembly ----------------
+struct AsmFreq {
+    float2 om2;     // Omega^2 of the assembly
+    float2 om;      // TE Omega
+    float2 om2mu0;  // TE Omega^2 * mu0
+};
+
+struct AsmArgs {
+    int nx, ny, n, nf, physics;
+    float w[6];               // a, b, c, d, e, idh2
+    const float *pml;         // [nf][pml_stride]
+    int pml_stride;           // 4*(nx+2) + 4*(ny+2)
+    const float *stiff;       // [n]  b (AC) or mu (SH)
+    float2 *mass;             // [nf][n]
+    double2 *A;               // [nf][9][n]
+};
+
+void launch_assemble(const AsmArgs &a, const float *m0, const float *m1, const AsmFreq *fq, float *stiff,
+                     cudaStream_t st);
+
+// ---------------- symbolic structure on the device ----------------
+struct DevSym {
+    int n, nnodes;
+    const int *npiv, *nfront, *child0, *child1, *vars, *inv, *lvl_nodes;
+    const int64_t *front_off, *var_off, *inv_off, *rhs_off;
+    int64_t front_total, rhs_total;
+};
+
+// ---------------- K2-K4 numeric factorisation ----------------
+struct LevelInfo {
+    int first;      // offset into lvl_nodes
+    int count;      // nodes in the level
+    int max_front, max_piv;
+    int64_t ent_first, ent_count;  // level's entry range in ent_dst/ent_src
+};
+
+template <class R>
+struct FactorArgs {
+    DevSym s;
+    void *front;              // cplx<R> [nf][front_total]
+    const double2 *A;         // [nf][9][n] assembled stencil values
+    const int64_t *ent_dst;   // per entry: front_off + position
+    const int *ent_src;       // per entry: q*n + k into A (operator orientation applied)
+    int nf;
+    R pivtol;                 // |pivot| below this is replaced (static pivoting)
+    unsigned long long *npert;  // perturbed-pivot counter
+};
+
+template <class R>
+void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st);
+
+// ---------------- K5 multi-RHS substitution ----------------
+template <class R>
+struct SolveArgs {
+    DevSym s;
+    const void *front;        // cplx<R> factors [nf][front_total]
+    void *x;                  // cplx<R> [nf][n][ldr], rhs in, solution out
+    void *w;                  // cplx<R> [nf][rhs_total][ldr] front-vector workspace
+    int nf, nrhs, ldr;
+    int trans;                // 0: M x = b, 1: M^T x = b
+};
+
+template <class R>
+void launch_solve_forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st);
+template <class R>
+void launch_solve_backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st);
+
+// ---------------- K6 FP64 residual / refinement ----------------
+struct ResidArgs {
+    int nx, ny, n, nf, nrhs, ldr;
+    const double2 *A;   // [nf][9][n]
+    const double2 *x;   // [nf][n][ldr]
+    const double2 *b;   // [nf][n][ldr]
+    double2 *r;         // [nf][n][ldr] out: b - M x
+    int op_mode;        // GM_OP_REF: M = A^T, GM_OP_EXACT: M = A
+    int trans;          // 0: M, 1: M^T
+};
+// r = b - M x and per-(freq, rhs) partial sums of |r|^2 and |b|^2 into
+// part[nblk][nf][nrhs][2]; returns nblk.
+int launch_residual(const ResidArgs &a, double *part, int max_blocks, cudaStream_t st);
+void launch_reduce_norms(const double *part, int nblk, int cnt, double *out, cudaStream_t st);
+
+// y(T) <- x(double) and x(double) += d(T) over [nf][n][ldr]
+template <class R>
+void launch_convert_down(const double2 *src, void *dst, size_t count, cudaStream_t st);
+template <class R>
+void launch_add_up(double2 *x, const void *d, size_t count, cudaStream_t st);
+
+}  // namespace gm

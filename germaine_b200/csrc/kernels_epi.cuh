@@ -1,0 +1,28 @@
+// Launch wrappers of the per-shot epilogue kernels (epilogue.cu).
+#pragma once
+#include <cuda_runtime.h>
+
+namespace gm {
+
+struct GradArgs {
+    int n, nf, ns, te;
+    const double2 *xf, *xa;     // forward / adjoint solutions [nf][n][ns]
+    const double2 *stfu;        // w/|w| per (f, s)
+    const double2 *om2, *om;    // per frequency
+    const float *m0, *m1;       // vp, rho (AC)
+    const float *frame;         // PML taper coefficient per grid point
+    const unsigned char *passes;
+    double *g0, *g1;            // [n] outputs (FP64)
+};
+
+void launch_spikes(double2 *b, int n, int nf, int ns, const int *ksrc, const double2 *amp, cudaStream_t st);
+void launch_gather_seis(const double2 *x, int n, int nf, int ns, int ntr, const int *krec, float2 *seis, double2 *cal,
+                        cudaStream_t st);
+void launch_field(const double2 *x, int n, int nf, int ns, float2 *field, cudaStream_t st);
+void launch_residual_shot(const double2 *cal, const float2 *obs, int nfs, int ntr, int stf_inv, int misfit,
+                          double2 *res, double *l2, double2 *stf, cudaStream_t st);
+void launch_adjoint_src(double2 *b, int n, int nf, int ns, int ntr, const int *kadj, const double2 *res, double dh2,
+                        cudaStream_t st);
+void launch_gradient(const GradArgs &a, cudaStream_t st);
+
+}  // namespace gm

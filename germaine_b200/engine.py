@@ -1,0 +1,173 @@
+"""Host-side mirror of GERMAINE's per-frequency engine over the C-ABI.
+
+The reference drives one frequency at a time through
+``forward_shot_AC`` (src/AC/forward_shot_AC.c:10), ``grad_obj_AC``
+(src/AC/grad_obj_AC.c:10) and ``obj_AC`` (src/AC/obj_AC.c:10) (TE/SH twins
+alike), each of which assembles the impedance matrix, factorises it with
+UMFPACK and loops over the shots.  :class:`Engine` exposes the same steps
+over libgermaine_gpu.so, batched over frequencies and shots: ``factor``
+(assembly + numeric LU of every frequency of a stage), then ``forward`` /
+``grad_obj`` / ``obj`` over all shots at once, and ``solve`` for arbitrary
+right-hand sides (the ``umfpack_zi_solve`` level).
+
+Argument meaning follows the reference: grids are the full NX x NY grid with
+the PML frame (forward_AC.c:44-45), source positions are in metres
+(srcpos[1]/[2]), receiver positions are grid indices without the PML offset
+(recpos[1]/[2]), seismograms use the reference's flat index
+``i + ntr*(ishot-1) + ntr*nshots*(nfreq-1)``.  Errors raise
+:class:`~germaine_b200._lib.GmError`; there is no CPU path.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from ._lib import (GM_OP_EXACT, GM_OP_REF, GM_PHYS_AC, GM_PHYS_SH, GM_PHYS_TE, GM_PREC_C64_IR, GM_PREC_FP64,
+                   GM_SYS_A, GM_SYS_AT, GmConfig, GmStats, check, ptr)
+
+__all__ = ["Engine", "GM_PHYS_AC", "GM_PHYS_SH", "GM_PHYS_TE", "GM_PREC_FP64", "GM_PREC_C64_IR",
+           "GM_OP_REF", "GM_OP_EXACT", "GM_SYS_A", "GM_SYS_AT", "nonzero"]
+
+
+def nonzero(nx: int, ny: int) -> int:
+    """NONZERO of the 9-point pattern (src/calc_nonzero.c:10-52)."""
+    return 9 * nx * ny - 6 * nx - 6 * ny + 4
+
+
+def _c(a, dtype):
+    return np.ascontiguousarray(a, dtype=dtype)
+
+
+class Engine:
+    """One GPU engine for one NX x NY grid and one physics."""
+
+    def __init__(self, nx: int, ny: int, dh: float, npml: int, physics: int = GM_PHYS_AC,
+                 precision: int = GM_PREC_FP64, op_mode: int = GM_OP_REF, free_surf: int = 0,
+                 a0_pml: float = 90.0, s: float = 0.0, device: int = 0, leaf_max: int = 64,
+                 ir_tol: float = 1e-10, ir_max_iter: int = 10):
+        self.lib = _lib.load()
+        self.cfg = GmConfig(nx, ny, dh, npml, free_surf, a0_pml, s, physics, precision, op_mode, leaf_max,
+                            ir_tol, ir_max_iter)
+        self.nx, self.ny, self.n = nx, ny, nx * ny
+        self.physics = physics
+        self._h = ctypes.c_void_p()
+        check(self.lib.gm_engine_create(device, ctypes.byref(self.cfg), ctypes.byref(self._h)))
+        self.nf = 0
+        self.freqs = None
+        self.last_status = 0
+
+    # -- lifetime --
+    def close(self):
+        if self._h:
+            self.lib.gm_engine_destroy(self._h)
+            self._h = ctypes.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    # -- set-up --
+    def set_model(self, mat0, mat1):
+        """Material arrays [NY][NX] (AC: vp, rho; SH: vs, rho; TE: epsilon, sigma)."""
+        m0 = _c(mat0, np.float32).reshape(-1)
+        m1 = _c(mat1, np.float32).reshape(-1)
+        if m0.size != self.n or m1.size != self.n:
+            raise ValueError(f"material arrays must have {self.n} entries")
+        self._m = (m0, m1)
+        check(self.lib.gm_set_model(self._h, ptr(m0), ptr(m1)))
+
+    def factor(self, freqs) -> int:
+        f = _c(np.atleast_1d(freqs), np.float32)
+        self.last_status = check(self.lib.gm_factor(self._h, int(f.size), ptr(f)))
+        self.nf = int(f.size)
+        self.freqs = f
+        return self.last_status
+
+    def stats(self) -> dict:
+        s = GmStats()
+        check(self.lib.gm_engine_stats(self._h, ctypes.byref(s)))
+        return s.as_dict()
+
+    def triplets(self, ifreq: int = 0):
+        nz = nonzero(self.nx, self.ny)
+        ar = np.zeros(nz); ai = np.zeros(nz)
+        ir = np.zeros(nz, np.int32); ic = np.zeros(nz, np.int32)
+        check(self.lib.gm_get_triplets(self._h, ifreq, ptr(ar), ptr(ai), ptr(ir), ptr(ic)))
+        return ar, ai, ir, ic
+
+    # -- solves --
+    def solve(self, b, sys: int = GM_SYS_A):
+        """b: complex array [nf][n][nrhs] (or [n][nrhs] / [n] for nf == 1)."""
+        b = np.asarray(b)
+        squeeze = b.ndim
+        if b.ndim == 1:
+            b = b[None, :, None]
+        elif b.ndim == 2:
+            b = b[None]
+        if b.shape[0] != self.nf or b.shape[1] != self.n:
+            raise ValueError(f"b must be [{self.nf}][{self.n}][nrhs]")
+        bb = _c(b, np.complex128)
+        x = np.empty_like(bb)
+        self.last_status = check(self.lib.gm_solve(self._h, sys, int(bb.shape[2]), ptr(bb), ptr(x)))
+        if squeeze == 1:
+            return x[0, :, 0]
+        if squeeze == 2:
+            return x[0]
+        return x
+
+    def forward(self, src_x, src_y, rec_x=None, rec_y=None, want_seis: bool = True, want_field: bool = False):
+        """All shots of all factorised frequencies.  Returns (seis, field):
+        seis [nf][nshots][ntr] complex64, field [nf][nshots][NY*NX] complex64
+        in the reference's vec2mat layout (either may be None)."""
+        sx = _c(src_x, np.float32); sy = _c(src_y, np.float32)
+        ns = sx.size
+        rx = _c(rec_x if rec_x is not None else [], np.int32)
+        ry = _c(rec_y if rec_y is not None else [], np.int32)
+        ntr = rx.size
+        seis = np.empty((self.nf, ns, ntr), np.complex64) if (want_seis and ntr) else None
+        field = np.empty((self.nf, ns, self.n), np.complex64) if want_field else None
+        self.last_status = check(self.lib.gm_forward(self._h, ns, ptr(sx), ptr(sy), ntr, ptr(rx), ptr(ry),
+                                                     ptr(seis), ptr(field)))
+        return seis, field
+
+    def grad_obj(self, src_x, src_y, rec_x, rec_y, pobs, stf_inv: int = 0, misfit: int = 1, want_seis=False):
+        """Misfit and gradient(s).  Returns (grad0, grad1, l2, seis); grad1 is
+        None for AC (the reference's fwiAC.grad) and the epsilon gradient for
+        TE (grad0 = sigma gradient)."""
+        sx = _c(src_x, np.float32); sy = _c(src_y, np.float32)
+        rx = _c(rec_x, np.int32); ry = _c(rec_y, np.int32)
+        ns, ntr = sx.size, rx.size
+        obs = _c(pobs, np.complex64).reshape(self.nf, ns, ntr)
+        g0 = np.zeros(self.n, np.float32)
+        g1 = np.zeros(self.n, np.float32) if self.physics == GM_PHYS_TE else None
+        l2 = ctypes.c_float(0.0)
+        seis = np.empty((self.nf, ns, ntr), np.complex64) if want_seis else None
+        self.last_status = check(self.lib.gm_grad_obj(self._h, ns, ptr(sx), ptr(sy), ntr, ptr(rx), ptr(ry), ptr(obs),
+                                                      stf_inv, misfit, ptr(g0), ptr(g1), ctypes.byref(l2),
+                                                      ptr(seis)))
+        return g0, g1, float(l2.value), seis
+
+    def gradient_fp64(self):
+        g0 = np.zeros(self.n)
+        g1 = np.zeros(self.n) if self.physics == GM_PHYS_TE else None
+        check(self.lib.gm_get_gradient_fp64(self._h, ptr(g0), ptr(g1)))
+        return g0, g1
+
+    def obj(self, src_x, src_y, rec_x, rec_y, pobs, stf_inv: int = 0, misfit: int = 1) -> float:
+        sx = _c(src_x, np.float32); sy = _c(src_y, np.float32)
+        rx = _c(rec_x, np.int32); ry = _c(rec_y, np.int32)
+        obs = _c(pobs, np.complex64).reshape(self.nf, sx.size, rx.size)
+        l2 = ctypes.c_float(0.0)
+        self.last_status = check(self.lib.gm_obj(self._h, sx.size, ptr(sx), ptr(sy), rx.size, ptr(rx), ptr(ry),
+                                                 ptr(obs), stf_inv, misfit, ctypes.byref(l2)))
+        return float(l2.value)

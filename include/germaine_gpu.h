@@ -116,7 +116,7 @@ int gm_get_triplets(gm_engine *e, int ifreq, double *Ar, double *Ai, int32_t *ir
  * with the current factors, followed by FP64 iterative refinement to
  * cfg.ir_tol: umfpack_zi_solve (src/AC/forward_shot_AC.c:88) over a block
  * of right-hand sides.  b and x are [nfreq][N][nrhs] complex128 (interleaved
- * re/im doubles, right-hand side fastest); x may alias nothing.  Returns
+ * re/im doubles, right-hand side fastest) and must not overlap.  Returns
  * GM_WARNING_NOT_CONVERGED if the target was not met. */
 int gm_solve(gm_engine *e, int sys, int nrhs, const double *b, double *x);
 
@@ -151,6 +151,10 @@ int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y
                 int ntr, const int32_t *rec_x, const int32_t *rec_y,
                 const float *pobs, int stf_inv, int misfit,
                 float *grad0, float *grad1, float *l2, float *seis);
+
+/* The last gm_grad_obj gradients before rounding to float, in FP64
+ * ([NY][NX] each; g1 ignored for AC).  Either pointer may be NULL. */
+int gm_get_gradient_fp64(gm_engine *e, double *g0, double *g1);
 
 /* Objective only (obj_AC, src/AC/obj_AC.c:10-145). */
 int gm_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y,

@@ -99,6 +99,7 @@ def load_port():
         lib.port_ass_grad_te.argtypes = [P, ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
         lib.port_grad_frame_coeff.argtypes = [P, _f32p]
         lib.port_cp_grad_frame.argtypes = [P, _f32p]
+        lib.port_gradient_scalars.argtypes = [P, ctypes.c_int, ctypes.c_float, _f32p, _f32p]
         _port_lib = lib
     return _port_lib
 
@@ -204,6 +205,12 @@ class Port:
 
     def cp_grad_frame(self, grad):
         self.lib.port_cp_grad_frame(ctypes.byref(self._pg), grad)
+
+    def gradient_scalars(self, physics, freq):
+        """(Omega^2, Omega) of ass_grad_AC / ass_grad_TE as complex64 values."""
+        a = np.zeros(2, np.float32); b = np.zeros(2, np.float32)
+        self.lib.port_gradient_scalars(ctypes.byref(self._pg), physics, freq, a, b)
+        return complex(a[0], a[1]), complex(b[0], b[1])
 
 
 class Ref:

@@ -403,3 +403,18 @@ void port_cp_grad_frame(const port_grid *g, float *grad)
 #undef C
     free(coef);
 }
+
+/* Gradient scalars: AC Omega^2 = cpowf((2 pi f) - iS, 2) (ass_grad_AC.c:22);
+ * TE Omega = 2 pi (f + iS), Omega^2 = cpowf(2 pi (f + iS), 2) (ass_grad_TE.c:22-23). */
+void port_gradient_scalars(const port_grid *g, int physics, float freq, float *om2, float *om)
+{
+    complex float o2, o = 0.0f;
+    if (physics == 4) {
+        o = 2.0 * M_PI * (freq + (I * g->s));
+        o2 = cpowf(2.0 * M_PI * (freq + (I * g->s)), 2.0);
+    } else {
+        o2 = cpowf(((2.0 * M_PI * freq) - (I * g->s)), 2.0);
+    }
+    om2[0] = crealf(o2); om2[1] = cimagf(o2);
+    om[0] = crealf(o); om[1] = cimagf(o);
+}

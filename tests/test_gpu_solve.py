@@ -1,0 +1,86 @@
+"""Multifrontal factor + multi-RHS solve on the GPU vs SuperLU (FP64) on the
+operator UMFPACK factorises (M = A^T, or A in EXACT mode)."""
+import numpy as np
+import pytest
+
+import oracle as O
+from oracle import sparse as OS
+from germaine_b200 import (GM_OP_EXACT, GM_OP_REF, GM_PHYS_AC, GM_PHYS_TE, GM_PREC_C64_IR, GM_PREC_FP64, GM_SYS_A,
+                           GM_SYS_AT, Engine)
+from tests.models import inclusion_ac, random_smooth, te_model
+
+pytestmark = pytest.mark.gpu
+
+
+def _setup(nx, ny, dh, npml, physics=GM_PHYS_AC, seed=0):
+    if physics == GM_PHYS_TE:
+        return te_model(nx, ny, seed)
+    vp, rho = inclusion_ac(nx, ny, dh, npml)
+    return vp * random_smooth(nx, ny, 0.85, 1.15, seed), rho
+
+
+def _rel(a, b):
+    return np.linalg.norm(a - b) / np.linalg.norm(b)
+
+
+@pytest.mark.parametrize("precision", [GM_PREC_FP64, GM_PREC_C64_IR], ids=["fp64", "c64ir"])
+@pytest.mark.parametrize("op_mode", [GM_OP_REF, GM_OP_EXACT], ids=["ref", "exact"])
+@pytest.mark.parametrize("sys_", [GM_SYS_A, GM_SYS_AT], ids=["A", "At"])
+def test_solve_matches_superlu(precision, op_mode, sys_):
+    nx, ny, dh, npml = 71, 53, 10.0, 10
+    freqs = [12.0, 25.0]
+    g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml)
+    m0, m1 = _setup(nx, ny, dh, npml, seed=3)
+    rng = np.random.default_rng(11)
+    nrhs = 13
+    b = rng.standard_normal((len(freqs), g.n, nrhs)) + 1j * rng.standard_normal((len(freqs), g.n, nrhs))
+    with Engine(nx, ny, dh, npml, precision=precision, op_mode=op_mode, leaf_max=24) as e:
+        e.set_model(m0, m1)
+        e.factor(freqs)
+        x = e.solve(b, sys=sys_)
+        st = e.stats()
+    port = O.Port(g)
+    for i, f in enumerate(freqs):
+        A = OS.assembled_matrix(g, *port.assemble(1, f, m0, m1))
+        ds = OS.DirectSolver(OS.operator(A, op_mode))
+        xr = ds.solve(b[i], trans=(sys_ == GM_SYS_AT))
+        err = _rel(x[i], xr)
+        Mop = ds.M.T if sys_ == GM_SYS_AT else ds.M
+        res = max(np.linalg.norm(Mop @ x[i][:, k] - b[i][:, k]) / np.linalg.norm(b[i][:, k]) for k in range(nrhs))
+        assert res <= 1e-10, f"relative residual {res:.3e} (freq {f})"
+        tol = 1e-10 if precision == GM_PREC_FP64 else 1e-8
+        assert err <= tol, f"relative L2 error vs SuperLU {err:.3e} (freq {f})"
+    assert st["ir_residual"] <= 1e-10
+
+
+@pytest.mark.parametrize("shape", [(5, 5, 1), (9, 4, 1), (60, 9, 2), (13, 77, 3), (128, 31, 5)])
+def test_solve_grid_shapes(shape):
+    """Tiny, skinny and tall grids (ND leaves, single-front trees, uneven cuts)."""
+    nx, ny, npml = shape
+    dh = 20.0
+    g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml)
+    m0, m1 = random_smooth(nx, ny, 1500.0, 3500.0, 5), random_smooth(nx, ny, 1000.0, 2500.0, 6)
+    rng = np.random.default_rng(1)
+    b = rng.standard_normal((1, g.n, 3)) + 1j * rng.standard_normal((1, g.n, 3))
+    with Engine(nx, ny, dh, npml, leaf_max=16) as e:
+        e.set_model(m0, m1)
+        e.factor([7.0])
+        x = e.solve(b)
+    A = OS.assembled_matrix(g, *O.Port(g).assemble(1, 7.0, m0, m1))
+    xr = OS.DirectSolver(OS.operator(A)).solve(b[0])
+    assert _rel(x[0], xr) <= 1e-10
+
+
+def test_te_transpose_solve():
+    nx, ny, dh, npml = 48, 40, 0.025, 8
+    g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml)
+    m0, m1 = _setup(nx, ny, dh, npml, physics=GM_PHYS_TE, seed=2)
+    rng = np.random.default_rng(4)
+    b = rng.standard_normal((1, g.n, 4)) + 1j * rng.standard_normal((1, g.n, 4))
+    with Engine(nx, ny, dh, npml, physics=GM_PHYS_TE, leaf_max=32) as e:
+        e.set_model(m0, m1)
+        e.factor([2e8])
+        x = e.solve(b, sys=GM_SYS_AT)
+    A = OS.assembled_matrix(g, *O.Port(g).assemble(4, 2e8, m0, m1))
+    xr = OS.DirectSolver(OS.operator(A)).solve(b[0], trans=True)
+    assert _rel(x[0], xr) <= 1e-10

@@ -1,0 +1,120 @@
+"""Pins the oracle: the C restatement (oracle/port.c) against the reference's
+own sources compiled into oracle/_ref, and both against the committed golden
+fixtures (tests/golden/, made by tests/golden/make_golden.py)."""
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+from tests.models import inclusion_ac, random_smooth, te_model
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+
+
+def _bits(a):
+    a = np.asarray(a)
+    return a.view(np.uint64 if a.dtype == np.float64 else np.uint32)
+
+
+def _materials(physics, g, seed):
+    if physics == O.PHYS_AC:
+        vp, rho = inclusion_ac(g.nx, g.ny, g.dh, g.npml)
+        return vp * random_smooth(g.nx, g.ny, 0.9, 1.1, seed), rho
+    if physics == O.PHYS_SH:
+        return random_smooth(g.nx, g.ny, 800, 2500, seed), random_smooth(g.nx, g.ny, 1500, 2600, seed + 1)
+    return te_model(g.nx, g.ny, seed)
+
+
+needs_ref = pytest.mark.skipif(not O.ref_available(), reason="oracle/_ref not built (reference tree absent)")
+
+
+@needs_ref
+@pytest.mark.parametrize("physics,freq", [(1, 15.0), (2, 7.0), (4, 2e8)])
+@pytest.mark.parametrize("s,fs", [(0.0, 0), (1.3, 1)])
+def test_port_assembly_equals_reference(physics, freq, s, fs):
+    g = O.Grid(nx=45, ny=33, dh=10.0 if physics != 4 else 0.025, npml=8, free_surf=fs, s=s)
+    m0, m1 = _materials(physics, g, 5)
+    a = O.Port(g).assemble(physics, freq, m0, m1)
+    b = O.Ref(g).assemble(physics, freq, m0, m1)
+    for x, y in zip(a, b):
+        assert np.array_equal(_bits(x), _bits(y))
+    assert np.array_equal(_bits(O.Port(g).pml(freq)), _bits(O.Ref(g).pml(freq)))
+
+
+@needs_ref
+def test_port_nonzero_equals_reference():
+    for nx, ny in [(241, 141), (3, 3), (10, 4)]:
+        g = O.Grid(nx=nx, ny=ny, dh=10.0, npml=1)
+        assert O.Ref(g).nonzero() == g.nonzero
+    assert O.Grid(nx=241, ny=141, dh=10.0, npml=20).nonzero == 303541
+
+
+@needs_ref
+@pytest.mark.parametrize("physics", [1, 4])
+def test_port_shot_arithmetic_equals_reference(physics):
+    g = O.Grid(nx=40, ny=30, dh=10.0, npml=6, s=0.4)
+    P, R = O.Port(g), O.Ref(g)
+    f = 9.0 if physics == 1 else 1.5e8
+    for xs, ys in [(55.0, 30.0), (104.9, 25.1), (0.0, 0.0)]:
+        a, b = P.rhs_source(physics, f, xs, ys), R.rhs_source(physics, f, xs, ys)
+        assert np.array_equal(_bits(a[0]), _bits(b[0])) and np.array_equal(_bits(a[1]), _bits(b[1]))
+    rng = np.random.default_rng(2)
+    x = rng.standard_normal(g.n) + 1j * rng.standard_normal(g.n)
+    pa, pb = P.vec2mat(x), R.vec2mat(x)
+    assert np.array_equal(pa[0], pb[0]) and np.array_equal(pa[1], pb[1])
+    rx = np.arange(1, 25, dtype=np.int32); ry = np.full(rx.size, 2, np.int32)
+    sa = np.zeros(rx.size, np.float32); sb = np.zeros(rx.size, np.float32)
+    sa2 = np.zeros(rx.size, np.float32); sb2 = np.zeros(rx.size, np.float32)
+    P.calc_seis(pa[0], pa[1], rx, ry, 1, 1, 1, sa, sa2)
+    R.calc_seis(pb[0], pb[1], rx, ry, 1, 1, 1, sb, sb2, 1)
+    assert np.array_equal(sa, sb) and np.array_equal(sa2, sb2)
+    obs_r = rng.standard_normal(rx.size).astype(np.float32)
+    obs_i = rng.standard_normal(rx.size).astype(np.float32)
+    for stf_inv in (0, 1):
+        for misfit in (1, 2, 3):
+            la, ra, ia, wa = P.calc_res(sa, sa2, obs_r, obs_i, stf_inv, 1, misfit)
+            lb, rb, ib, wb = R.calc_res(sb, sb2, obs_r, obs_i, stf_inv, 1, misfit)
+            assert np.array_equal(ra, rb) and np.array_equal(ia, ib) and np.array_equal(wa, wb)
+            if stf_inv == 1:
+                assert la == lb
+    ad, bd = P.rhs_adj(ra, ia, rx, ry), R.rhs_adj(rb, ib, rx, ry)
+    assert np.array_equal(ad[0], bd[0]) and np.array_equal(ad[1], bd[1])
+    stf = np.array([0.7, -0.3], np.float32)
+    vp = random_smooth(g.nx, g.ny, 1500, 3000, 1); rho = random_smooth(g.nx, g.ny, 1000, 2000, 2)
+    fr, fi, lr, li = (rng.standard_normal(g.n).astype(np.float32) for _ in range(4))
+    if physics == 1:
+        ga = np.zeros(g.n, np.float32); gb = np.zeros(g.n, np.float32)
+        P.ass_grad_ac(f, stf, fr, fi, lr, li, vp, rho, ga)
+        R.ass_grad_ac(f, stf, fr, fi, lr, li, vp, rho, gb)
+        assert np.array_equal(ga, gb)
+        P.cp_grad_frame(ga); R.cp_grad_frame(gb)
+        assert np.array_equal(ga, gb)
+    else:
+        ga = np.zeros(g.n, np.float32); gb = np.zeros(g.n, np.float32)
+        ea = np.zeros(g.n, np.float32); eb = np.zeros(g.n, np.float32)
+        P.ass_grad_te(f, stf, fr, fi, lr, li, ga, ea)
+        R.ass_grad_te(f, stf, fr, fi, lr, li, gb, eb)
+        assert np.array_equal(ga, gb) and np.array_equal(ea, eb)
+
+
+def _golden_files():
+    return sorted(f for f in os.listdir(GOLDEN) if f.endswith(".npz")) if os.path.isdir(GOLDEN) else []
+
+
+@pytest.mark.parametrize("fname", _golden_files())
+def test_port_against_golden(fname):
+    """Fixtures generated from the reference's own compiled sources."""
+    d = np.load(os.path.join(GOLDEN, fname))
+    g = O.Grid(nx=int(d["nx"]), ny=int(d["ny"]), dh=float(d["dh"]), npml=int(d["npml"]),
+               free_surf=int(d["free_surf"]), a0_pml=float(d["a0_pml"]), s=float(d["s"]))
+    physics, freq = int(d["physics"]), float(d["freq"])
+    a = O.Port(g).assemble(physics, freq, d["m0"], d["m1"])
+    assert np.array_equal(_bits(a[0]), _bits(d["Ar"])) and np.array_equal(_bits(a[1]), _bits(d["Ai"]))
+    assert np.array_equal(a[2], d["irow"]) and np.array_equal(a[3], d["icol"])
+    assert np.array_equal(_bits(O.Port(g).pml(freq)), _bits(d["pml"]))
+    if "x" in d:
+        from oracle import sparse as OS
+        M = OS.operator(OS.assembled_matrix(g, *a))
+        x = OS.DirectSolver(M).solve(d["b"])
+        assert np.linalg.norm(x - d["x"]) / np.linalg.norm(d["x"]) < 1e-12
