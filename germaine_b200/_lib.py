@@ -43,7 +43,8 @@ class GmStats(ctypes.Structure):
                 ("factor_flops", ctypes.c_double), ("solve_flops_per_rhs", ctypes.c_double),
                 ("perturbed_pivots", ctypes.c_int64), ("ir_iterations", ctypes.c_int32),
                 ("ir_residual", ctypes.c_double), ("ms_assemble", ctypes.c_double),
-                ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double), ("ms_refine", ctypes.c_double)]
+                ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double), ("ms_refine", ctypes.c_double),
+                ("ms_subst", ctypes.c_double), ("n_subst", ctypes.c_int32), ("kernel_launches", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -51,7 +52,7 @@ class GmStats(ctypes.Structure):
 
 # every C-ABI symbol declared in include/germaine_gpu.h
 EXPORTS = [
-    "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats",
+    "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats", "gm_engine_stream",
     "gm_set_model", "gm_factor", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
     "gm_get_gradient_fp64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
@@ -83,6 +84,7 @@ def load() -> ctypes.CDLL:
     lib.gm_engine_create.argtypes = [i32, ctypes.POINTER(GmConfig), ctypes.POINTER(vp)]
     lib.gm_engine_destroy.argtypes = [vp]
     lib.gm_engine_stats.argtypes = [vp, ctypes.POINTER(GmStats)]
+    lib.gm_engine_stream.argtypes = [vp, ctypes.POINTER(vp)]
     lib.gm_set_model.argtypes = [vp, vp, vp]
     lib.gm_factor.argtypes = [vp, i32, vp]
     lib.gm_get_triplets.argtypes = [vp, i32, vp, vp, vp, vp]

@@ -192,8 +192,8 @@ void launch_assemble(const AsmArgs &a, const float *m0, const float *m1, const A
                      cudaStream_t st) {
     const int tpb = 256;
     dim3 grid((a.n + tpb - 1) / tpb, a.nf);
-    k_cells<<<grid, tpb, 0, st>>>(a.physics, a.n, m0, m1, fq, a.mass, stiff);
-    k_stencil<<<grid, tpb, 0, st>>>(a);
+    (k_cells<<<grid, tpb, 0, st>>>(a.physics, a.n, m0, m1, fq, a.mass, stiff), note_launch());
+    (k_stencil<<<grid, tpb, 0, st>>>(a), note_launch());
 }
 
 }  // namespace gm

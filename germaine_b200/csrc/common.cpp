@@ -1,5 +1,7 @@
 #include "common.hpp"
 
+#include <atomic>
+
 #include "../../include/germaine_gpu.h"
 
 namespace gm {
@@ -18,6 +20,10 @@ int fail(int code, const char *fmt, ...) {
     last_error() = buf;
     return code;
 }
+
+static std::atomic<long long> g_launches{0};
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+long long launch_count() { return g_launches.load(std::memory_order_relaxed); }
 
 }  // namespace gm
 

@@ -96,6 +96,8 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
     GM_CUDA(cudaStreamCreateWithFlags(&e->st, cudaStreamNonBlocking));
     GM_CUDA(cudaEventCreate(&e->ev0));
     GM_CUDA(cudaEventCreate(&e->ev1));
+    GM_CUDA(cudaEventCreate(&e->ev_s0));
+    GM_CUDA(cudaEventCreate(&e->ev_s1));
 
     const gm::Symbolic &s = e->sym;
     // level-ordered entry lists in the configured operator orientation
@@ -170,6 +172,13 @@ extern "C" int gm_engine_destroy(gm_engine *e) {
 extern "C" int gm_engine_stats(const gm_engine *e, gm_stats *out) {
     if (!e || !out) return fail(GM_ERROR_INVALID, "gm_engine_stats: null argument");
     *out = e->stats;
+    out->kernel_launches = gm::launch_count();
+    return GM_OK;
+}
+
+extern "C" int gm_engine_stream(const gm_engine *e, void **stream) {
+    if (!e || !stream) return fail(GM_ERROR_INVALID, "gm_engine_stream: null argument");
+    *stream = (void *)e->st;
     return GM_OK;
 }
 
@@ -324,6 +333,7 @@ namespace gm {
 
 template <class R>
 static void substitute(gm_engine *e, void *xT, int nrhs, int trans) {
+    cudaEventRecord(e->ev_s0, e->st);
     SolveArgs<R> a{};
     a.s = e->dsym;
     a.front = e->d_front.p;
@@ -332,9 +342,17 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans) {
     a.nf = e->nf;
     a.nrhs = nrhs;
     a.ldr = nrhs;
+    const int nchunk = (nrhs + 31) / 32;
+    a.rch = (nrhs + nchunk - 1) / nchunk;
     a.trans = trans;
     for (int h = 0; h < (int)e->levels.size(); ++h) launch_solve_forward_level<R>(a, e->levels[h], e->st);
     for (int h = (int)e->levels.size() - 1; h >= 0; --h) launch_solve_backward_level<R>(a, e->levels[h], e->st);
+    cudaEventRecord(e->ev_s1, e->st);
+    cudaEventSynchronize(e->ev_s1);
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev_s0, e->ev_s1);
+    e->stats.ms_subst += ms;
+    e->stats.n_subst += 1;
 }
 
 // x (device, [nf][n][nrhs] c128) = M'^{-1} b with FP64 refinement; b, x device.
@@ -349,6 +367,8 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     GM_ALLOC(e->d_norm, (size_t)e->nf * nrhs * 2 * sizeof(double));
 
     cudaEvent_t t0 = e->ev0, t1 = e->ev1;
+    e->stats.ms_subst = 0;
+    e->stats.n_subst = 0;
     GM_CUDA(cudaEventRecord(t0, e->st));
     // initial solve in working precision
     if (fp64) launch_convert_down<double>(d_b, e->d_t.p, cnt, e->st);

@@ -73,7 +73,7 @@ struct gm_engine {
     std::vector<double> last_grad0, last_grad1;
 
     gm_stats stats{};
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_s0 = nullptr, ev_s1 = nullptr;
 
     gm_engine() = default;
     gm_engine(const gm_engine &) = delete;
@@ -81,6 +81,8 @@ struct gm_engine {
     ~gm_engine() {
         if (ev0) cudaEventDestroy(ev0);
         if (ev1) cudaEventDestroy(ev1);
+        if (ev_s0) cudaEventDestroy(ev_s0);
+        if (ev_s1) cudaEventDestroy(ev_s1);
         if (st) cudaStreamDestroy(st);
     }
 

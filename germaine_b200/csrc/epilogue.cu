@@ -23,7 +23,7 @@ __global__ void k_spikes(double2 *b, int n, int nf, int ns, const int *ksrc, con
 
 void launch_spikes(double2 *b, int n, int nf, int ns, const int *ksrc, const double2 *amp, cudaStream_t st) {
     cudaMemsetAsync(b, 0, (size_t)nf * n * ns * sizeof(double2), st);
-    k_spikes<<<(nf * ns + 255) / 256, 256, 0, st>>>(b, n, nf, ns, ksrc, amp);
+    (k_spikes<<<(nf * ns + 255) / 256, 256, 0, st>>>(b, n, nf, ns, ksrc, amp), note_launch());
 }
 
 __device__ __forceinline__ double2 shifted(const double2 *x, int n, int ns, int k, int s) {
@@ -49,7 +49,7 @@ void launch_gather_seis(const double2 *x, int n, int nf, int ns, int ntr, const 
                         cudaStream_t st) {
     const size_t tot = (size_t)nf * ns * ntr;
     if (!tot) return;
-    k_gather_seis<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(x, n, nf, ns, ntr, krec, seis, cal);
+    (k_gather_seis<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(x, n, nf, ns, ntr, krec, seis, cal), note_launch());
 }
 
 // field[f][s][k] = (complex64) x[f][k+1][s]: 32 x 32 tiles through shared memory
@@ -75,7 +75,7 @@ __global__ void k_field(const double2 *x, int n, int ns, float2 *field) {
 
 void launch_field(const double2 *x, int n, int nf, int ns, float2 *field, cudaStream_t st) {
     dim3 grid((n + 31) / 32, (ns + 31) / 32, nf);
-    k_field<<<grid, dim3(32, 8), 0, st>>>(x, n, ns, field);
+    (k_field<<<grid, dim3(32, 8), 0, st>>>(x, n, ns, field), note_launch());
 }
 
 // Residuals of one (frequency, shot) per CTA: optional Wiener source
@@ -143,7 +143,7 @@ __global__ void k_residual_shot(const double2 *cal, const float2 *obs, int ntr, 
 
 void launch_residual_shot(const double2 *cal, const float2 *obs, int nfs, int ntr, int stf_inv, int misfit,
                           double2 *res, double *l2, double2 *stf, cudaStream_t st) {
-    k_residual_shot<<<nfs, 256, 0, st>>>(cal, obs, ntr, stf_inv, misfit, res, l2, stf);
+    (k_residual_shot<<<nfs, 256, 0, st>>>(cal, obs, ntr, stf_inv, misfit, res, l2, stf), note_launch());
 }
 
 // Adjoint sources conj(res)/DH^2 at the receivers; receivers sharing a grid
@@ -162,7 +162,7 @@ __global__ void k_adjoint_src(double2 *b, int n, int nf, int ns, int ntr, const 
 void launch_adjoint_src(double2 *b, int n, int nf, int ns, int ntr, const int *kadj, const double2 *res, double dh2,
                         cudaStream_t st) {
     cudaMemsetAsync(b, 0, (size_t)nf * n * ns * sizeof(double2), st);
-    k_adjoint_src<<<(nf * ns + 127) / 128, 128, 0, st>>>(b, n, nf, ns, ntr, kadj, res, dh2);
+    (k_adjoint_src<<<(nf * ns + 127) / 128, 128, 0, st>>>(b, n, nf, ns, ntr, kadj, res, dh2), note_launch());
 }
 
 // Gradient stack over all frequencies and shots, one thread per grid point,
@@ -203,7 +203,7 @@ __global__ void k_gradient(GradArgs a) {
 }
 
 void launch_gradient(const GradArgs &a, cudaStream_t st) {
-    k_gradient<<<(a.n + 127) / 128, 128, 0, st>>>(a);
+    (k_gradient<<<(a.n + 127) / 128, 128, 0, st>>>(a), note_launch());
 }
 
 }  // namespace gm

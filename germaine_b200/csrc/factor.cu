@@ -257,11 +257,11 @@ template <class R>
 void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
     using C = cplx<R>;
     if (L.count == 0) return;
-    k_front_gather<R><<<dim3(L.max_front, L.count, a.nf), 128, 0, st>>>(a, L.first);
+    (k_front_gather<R><<<dim3(L.max_front, L.count, a.nf), 128, 0, st>>>(a, L.first), note_launch());
     if (L.ent_count > 0) {
         const int tpb = 256;
-        k_entry_scatter<R><<<dim3((unsigned)((L.ent_count + tpb - 1) / tpb), a.nf), tpb, 0, st>>>(a, L.ent_first,
-                                                                                                  L.ent_count);
+        (k_entry_scatter<R><<<dim3((unsigned)((L.ent_count + tpb - 1) / tpb), a.nf), tpb, 0, st>>>(a, L.ent_first,
+                                                                                                  L.ent_count), note_launch());
     }
     const size_t smem = 2 * NB * TILE * sizeof(C);
     static bool attr_set = false;
@@ -273,9 +273,9 @@ void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
         const int mmax = L.max_front - k0 - 1;   // largest trailing size (kb >= 1)
         const int nchunk = mmax > 0 ? (mmax + PCHUNK - 1) / PCHUNK : 0;
         if (nchunk > 0)
-            k_panel<R><<<dim3(2 * nchunk, L.count, a.nf), PCHUNK, 0, st>>>(a, L.first, k0);
+            (k_panel<R><<<dim3(2 * nchunk, L.count, a.nf), PCHUNK, 0, st>>>(a, L.first, k0), note_launch());
         const int ntmax = mmax > 0 ? (mmax + TILE - 1) / TILE : 0;
-        k_update<R><<<dim3(ntmax * ntmax + 1, L.count, a.nf), 256, smem, st>>>(a, L.first, k0, ntmax);
+        (k_update<R><<<dim3(ntmax * ntmax + 1, L.count, a.nf), 256, smem, st>>>(a, L.first, k0, ntmax), note_launch());
     }
 }
 

@@ -7,6 +7,10 @@
 
 namespace gm {
 
+// Counts kernel launches of this library (reported in gm_stats).
+void note_launch();
+long long launch_count();
+
 // ---------------- K1 assembly ----------------
 struct AsmFreq {
     float2 om2;     // Omega^2 of the assembly
@@ -66,6 +70,7 @@ struct SolveArgs {
     void *x;                  // cplx<R> [nf][n][ldr], rhs in, solution out
     void *w;                  // cplx<R> [nf][rhs_total][ldr] front-vector workspace
     int nf, nrhs, ldr;
+    int rch;                  // right-hand sides per CTA (<= 32)
     int trans;                // 0: M x = b, 1: M^T x = b
 };
 

@@ -2,6 +2,8 @@
 #pragma once
 #include <cuda_runtime.h>
 
+#include "kernels.cuh"
+
 namespace gm {
 
 struct GradArgs {

@@ -51,7 +51,7 @@ __global__ void __launch_bounds__(128) k_residual(ResidArgs a, double *part) {
 int launch_residual(const ResidArgs &a, double *part, int max_blocks, cudaStream_t st) {
     const int nblk = (a.n + RROWS - 1) / RROWS;
     if (nblk > max_blocks) return -1;
-    k_residual<<<dim3(nblk, a.nf), 128, 0, st>>>(a, part);
+    (k_residual<<<dim3(nblk, a.nf), 128, 0, st>>>(a, part), note_launch());
     return nblk;
 }
 
@@ -65,7 +65,7 @@ __global__ void k_reduce_norms(const double *part, int nblk, int cnt, double *ou
 }
 
 void launch_reduce_norms(const double *part, int nblk, int cnt, double *out, cudaStream_t st) {
-    k_reduce_norms<<<(cnt + 255) / 256, 256, 0, st>>>(part, nblk, cnt, out);
+    (k_reduce_norms<<<(cnt + 255) / 256, 256, 0, st>>>(part, nblk, cnt, out), note_launch());
 }
 
 template <class R>
@@ -87,13 +87,13 @@ __global__ void k_add_up(double2 *x, const cplx<R> *d, size_t count) {
 template <class R>
 void launch_convert_down(const double2 *src, void *dst, size_t count, cudaStream_t st) {
     if (!count) return;
-    k_convert_down<R><<<(unsigned)((count + 255) / 256), 256, 0, st>>>(src, reinterpret_cast<cplx<R> *>(dst), count);
+    (k_convert_down<R><<<(unsigned)((count + 255) / 256), 256, 0, st>>>(src, reinterpret_cast<cplx<R> *>(dst), count), note_launch());
 }
 
 template <class R>
 void launch_add_up(double2 *x, const void *d, size_t count, cudaStream_t st) {
     if (!count) return;
-    k_add_up<R><<<(unsigned)((count + 255) / 256), 256, 0, st>>>(x, reinterpret_cast<const cplx<R> *>(d), count);
+    (k_add_up<R><<<(unsigned)((count + 255) / 256), 256, 0, st>>>(x, reinterpret_cast<const cplx<R> *>(d), count), note_launch());
 }
 
 template void launch_convert_down<double>(const double2 *, void *, size_t, cudaStream_t);

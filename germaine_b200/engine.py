@@ -78,7 +78,14 @@ class Engine:
 
     # -- set-up --
     def set_model(self, mat0, mat1):
-        """Material arrays [NY][NX] (AC: vp, rho; SH: vs, rho; TE: epsilon, sigma)."""
+        """Material arrays [NY][NX] (AC: vp, rho; SH: vs, rho; TE: epsilon,
+        sigma): numpy arrays or torch float32 tensors (host or device)."""
+        if hasattr(mat0, "data_ptr"):
+            if mat0.numel() != self.n or mat1.numel() != self.n:
+                raise ValueError(f"material arrays must have {self.n} entries")
+            self._m = (mat0, mat1)
+            check(self.lib.gm_set_model(self._h, ptr(mat0), ptr(mat1)))
+            return
         m0 = _c(mat0, np.float32).reshape(-1)
         m1 = _c(mat1, np.float32).reshape(-1)
         if m0.size != self.n or m1.size != self.n:
@@ -125,20 +132,33 @@ class Engine:
             return x[0]
         return x
 
-    def forward(self, src_x, src_y, rec_x=None, rec_y=None, want_seis: bool = True, want_field: bool = False):
+    def forward(self, src_x, src_y, rec_x=None, rec_y=None, want_seis: bool = True, want_field: bool = False,
+                seis_out=None, field_out=None):
         """All shots of all factorised frequencies.  Returns (seis, field):
         seis [nf][nshots][ntr] complex64, field [nf][nshots][NY*NX] complex64
-        in the reference's vec2mat layout (either may be None)."""
+        in the reference's vec2mat layout (either may be None).  seis_out /
+        field_out may be preallocated outputs (numpy arrays or torch tensors,
+        host or device) of those shapes."""
         sx = _c(src_x, np.float32); sy = _c(src_y, np.float32)
         ns = sx.size
         rx = _c(rec_x if rec_x is not None else [], np.int32)
         ry = _c(rec_y if rec_y is not None else [], np.int32)
         ntr = rx.size
-        seis = np.empty((self.nf, ns, ntr), np.complex64) if (want_seis and ntr) else None
-        field = np.empty((self.nf, ns, self.n), np.complex64) if want_field else None
+        seis = seis_out
+        if seis is None and want_seis and ntr:
+            seis = np.empty((self.nf, ns, ntr), np.complex64)
+        field = field_out
+        if field is None and want_field:
+            field = np.empty((self.nf, ns, self.n), np.complex64)
         self.last_status = check(self.lib.gm_forward(self._h, ns, ptr(sx), ptr(sy), ntr, ptr(rx), ptr(ry),
                                                      ptr(seis), ptr(field)))
         return seis, field
+
+    def stream(self) -> int:
+        """Address of the CUDA stream the engine issues its work on."""
+        s = ctypes.c_void_p()
+        check(self.lib.gm_engine_stream(self._h, ctypes.byref(s)))
+        return int(s.value or 0)
 
     def grad_obj(self, src_x, src_y, rec_x, rec_y, pobs, stf_inv: int = 0, misfit: int = 1, want_seis=False):
         """Misfit and gradient(s).  Returns (grad0, grad1, l2, seis); grad1 is

@@ -84,6 +84,9 @@ typedef struct {
     int32_t ir_iterations;      /* refinement sweeps of the last solve */
     double ir_residual;         /* max relative residual after the last solve */
     double ms_assemble, ms_factor, ms_solve, ms_refine;  /* device time of the last calls */
+    double ms_subst;            /* device time of the substitutions of the last solve */
+    int32_t n_subst;            /* substitutions (initial + refinement) of the last solve */
+    int64_t kernel_launches;    /* kernels launched by this library in this process */
 } gm_stats;
 
 const char *gm_last_error(void);
@@ -96,6 +99,9 @@ int gm_version(void);
 int gm_engine_create(int device, const gm_config *cfg, gm_engine **out);
 int gm_engine_destroy(gm_engine *e);
 int gm_engine_stats(const gm_engine *e, gm_stats *out);
+/* The CUDA stream (cudaStream_t) all of the engine's work is issued on, for
+ * callers that time or order work against it. */
+int gm_engine_stream(const gm_engine *e, void **stream);
 
 /* Material model [NY][NX] (two float arrays, meaning per physics).
  * Replaces readmod()/init_mat_AC (src/AC/init_mat_AC.c:10) input handling. */
