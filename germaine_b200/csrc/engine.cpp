@@ -112,6 +112,11 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
         L.count = s.lvl_off[h + 1] - s.lvl_off[h];
         L.max_front = s.lvl_max_front[h];
         L.max_piv = s.lvl_max_piv[h];
+        L.max_ring = 0;
+        for (int t = L.first; t < L.first + L.count; ++t) {
+            const int v = s.lvl_nodes[t];
+            L.max_ring = std::max(L.max_ring, s.nfront[v] - s.npiv[v]);
+        }
         L.ent_first = (int64_t)ent_dst.size();
         for (int t = L.first; t < L.first + L.count; ++t) {
             const int v = s.lvl_nodes[t];

@@ -12,8 +12,10 @@
 //                  memory) and the triangular solves of the L and U panels,
 //   K4 update   -- rank-NB Schur update of the trailing front, 64x64 tiles.
 // K3/K4 alternate ceil(max_piv/NB) times per level.  After the last step a
-// front holds L (unit lower) and U in its first npiv rows/columns and its
-// Schur complement (the contribution block) in the trailing block.
+// front holds L (unit lower) and U in its first npiv rows/columns -- except
+// that each NB x NB diagonal block holds the INVERSES of its two triangles
+// (what the substitution multiplies by) -- and its Schur complement (the
+// contribution block) in the trailing block.
 #include "kernels.cuh"
 #include "cplx.cuh"
 
@@ -200,9 +202,32 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
         }
         __syncthreads();
         diag_lu<R>(D, rdiag, kb, a.pivtol, &npert);
-        for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-            const int r = t % kb, c = t / kb;
-            F[(k0 + r) + (size_t)(k0 + c) * f] = D[r][c];
+        // The substitution only needs the inverses of the block's triangles:
+        // store L^-1 (strict lower part; unit diagonal implied) and U^-1
+        // (upper part with diagonal) in place of L and U.  Thread c < kb
+        // inverts column c of L, thread 32 + c column c of U.
+        __shared__ C Dinv[NB][NB + 1];
+        const int t = threadIdx.x;
+        if (t < kb) {   // the unit diagonal of L^-1 is implied: only U^-1 owns Dinv[c][c]
+            const int c = t;
+            for (int r = c + 1; r < kb; ++r) {
+                C acc = D[r][c];
+                for (int q = c + 1; q < r; ++q) cfma(acc, D[r][q], Dinv[q][c]);
+                Dinv[r][c] = mk(-acc.x, -acc.y);
+            }
+        } else if (t >= 32 && t < 32 + kb) {
+            const int c = t - 32;
+            Dinv[c][c] = rdiag[c];
+            for (int r = c - 1; r >= 0; --r) {
+                C acc = czero<C>();
+                for (int q = r + 1; q <= c; ++q) cfma(acc, D[r][q], Dinv[q][c]);
+                Dinv[r][c] = cmul(mk(-acc.x, -acc.y), rdiag[r]);
+            }
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kb * kb; i += blockDim.x) {
+            const int r = i % kb, c = i / kb;
+            F[(k0 + r) + (size_t)(k0 + c) * f] = Dinv[r][c];
         }
         if (threadIdx.x == 0 && npert) atomicAdd(a.npert, (unsigned long long)npert);
         return;

@@ -43,7 +43,7 @@ struct DevSym {
 struct LevelInfo {
     int first;      // offset into lvl_nodes
     int count;      // nodes in the level
-    int max_front, max_piv;
+    int max_front, max_piv, max_ring;
     int64_t ent_first, ent_count;  // level's entry range in ent_dst/ent_src
 };
 

@@ -4,275 +4,377 @@
 // every frequency).
 //
 // Right-hand sides / solutions are [nf][n][ldr] complex, right-hand side
-// fastest.  One CTA (8 warps) owns one (front, frequency, slice of up to 32
-// right-hand sides); lane l of every warp works on right-hand side l, so all
-// vector traffic is a coalesced row of the slice.
-//   forward (leaves -> root): gather the front vector (own rows of x plus
-//     the children's update vectors, by the same inverse maps as the
-//     extend-add), then for each 32-pivot block: triangular solve of the
-//     block -- one warp per right-hand side, lane p holding unknown p, the
-//     eliminated value broadcast by warp shuffle (no block barrier inside
-//     the block) -- and a rank-32 update of the rows below from 64-row tiles
-//     of L staged in shared memory; y goes back to x at the pivots, the
-//     trailing rows stay in the front-vector workspace as this front's update
-//     for its parent;
-//   backward (root -> leaves): t = y - U12 x2 (x2 = final values of the
-//     ancestors' variables), then blocked back substitution with U11.
-// trans = 1 solves M^T x = b with the same factors: M^T = U^T L^T, so the
-// forward pass runs with U^T (non-unit diagonal) and the backward pass with
-// L^T (unit diagonal); only the indexing of the factor changes.
+// fastest.  Work units are (front, frequency, slice of TC = 32 right-hand
+// sides).  The factorisation stores, in every 32 x 32 diagonal block, the
+// inverses of the block's triangles, so every step below is a small GEMM on
+// CUDA cores: 128 threads, each owning a 4 x 4 complex register tile of a
+// 64-row x 32-right-hand-side output tile, operands staged in shared memory.
+//
+// Per elimination-tree level:
+//   forward  (leaves -> root)
+//     k_fwd_piv   gather the front vector w (own rows of x + the children's
+//                 update vectors, by the extend-add inverse maps), then per
+//                 32-pivot block: y_b = L_bb^-1 w_b, w_rest -= L_rb y_b over
+//                 the remaining pivot rows; y goes back to x at the pivots;
+//     k_fwd_ring  w_ring -= L_ring,piv * y over 64-row tiles of the ring
+//                 (many CTAs per front: the wide part of the level), leaving
+//                 this front's update vector for its parent;
+//   backward (root -> leaves)
+//     k_bwd_ring  t = y - U_piv,ring * x_ring (x_ring = final values of the
+//                 ancestors' variables), 64-row tiles of the pivot rows;
+//     k_bwd_piv   per block from the last: x_b = U_bb^-1 t_b, scatter to x,
+//                 t_above -= U_ab x_b.
+// trans = 1 solves M^T x = b with the same factors: M^T = U^T L^T, the
+// forward pass runs with U^T and the backward pass with L^T; only the
+// factor indexing and which stored inverse is used change.
 #include "kernels.cuh"
 #include "cplx.cuh"
 
 namespace gm {
 
-constexpr int SNB = 32;    // pivot block
-constexpr int RT = 64;     // row tile of the updates
-constexpr int NWARP = 8;
-
-template <class C, bool TRANS>
-__device__ __forceinline__ C lower_el(const C *F, int f, int i, int c) {
-    // forward-pass factor L'(i, c), i >= c
-    return TRANS ? F[c + (size_t)i * f] : F[i + (size_t)c * f];
-}
-template <class C, bool TRANS>
-__device__ __forceinline__ C upper_el(const C *F, int f, int i, int c) {
-    // backward-pass factor U'(i, c), i <= c
-    return TRANS ? F[c + (size_t)i * f] : F[i + (size_t)c * f];
-}
-
-__device__ __forceinline__ double2 shfl(double2 v, int src) {
-    return make_double2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
-}
-__device__ __forceinline__ float2 shfl(float2 v, int src) {
-    return make_float2(__shfl_sync(0xffffffffu, v.x, src), __shfl_sync(0xffffffffu, v.y, src));
-}
+constexpr int SNB = 32;   // pivot block (= factorisation block)
+constexpr int RT = 64;    // output rows per tile
+constexpr int TC = 32;    // right-hand sides per CTA
+constexpr int NT = 128;   // threads per CTA
 
 template <class C>
 struct SolveSmem {
-    C D[SNB][SNB + 1];   // diagonal block of the current pivot block
-    C Y[SNB][SNB + 1];   // solved block [pivot][rhs], or a ring block of x
-    C L[RT][SNB + 1];    // factor tile [row][pivot]
+    C L[SNB][RT];    // factor tile, [pivot q][row]
+    C Y[SNB][TC];    // right operand, [pivot q][rhs]
 };
 
-// Stage the factor tile T[row][q] = (lower ? L' : U')(i0 + row, c0 + q),
-// row < rows, q < qb, coalesced along the factor's contiguous index.
+// factor element M'(i, c) of the forward (L') or backward (U') factor:
+// F[i + c f] for M x = b, F[c + i f] for M^T x = b
 template <class C, bool TRANS>
-__device__ __forceinline__ void stage_tile(C (*T)[SNB + 1], const C *F, int f, int i0, int rows, int c0, int qb) {
-    if (!TRANS) {   // column-major: contiguous along the row index
-        for (int t = threadIdx.x; t < RT * SNB; t += blockDim.x) {
+__device__ __forceinline__ C elem(const C *F, int f, int i, int c) {
+    return TRANS ? F[c + (size_t)i * f] : F[i + (size_t)c * f];
+}
+
+// sm.L[q][row] = M'(i0 + row, c0 + q) for row < rows, q < qb; zeros elsewhere
+template <class C, bool TRANS>
+__device__ __forceinline__ void stage_factor(SolveSmem<C> &sm, const C *F, int f, int i0, int rows, int c0, int qb) {
+    if (!TRANS) {
+        for (int t = threadIdx.x; t < RT * SNB; t += NT) {
             const int row = t % RT, q = t / RT;
-            if (row < rows && q < qb) T[row][q] = F[(i0 + row) + (size_t)(c0 + q) * f];
+            sm.L[q][row] = (row < rows && q < qb) ? F[(i0 + row) + (size_t)(c0 + q) * f] : czero<C>();
         }
-    } else {        // transposed access: contiguous along the pivot index
-        for (int t = threadIdx.x; t < RT * SNB; t += blockDim.x) {
+    } else {
+        for (int t = threadIdx.x; t < RT * SNB; t += NT) {
             const int q = t % SNB, row = t / SNB;
-            if (row < rows && q < qb) T[row][q] = F[(c0 + q) + (size_t)(i0 + row) * f];
+            sm.L[q][row] = (row < rows && q < qb) ? F[(c0 + q) + (size_t)(i0 + row) * f] : czero<C>();
         }
     }
 }
 
-// V[i0 + row][lane] -= sum_q T[row][q] * Y[q][lane] over the staged tile;
-// warp w owns rows w + 8j.
-template <class C>
-__device__ __forceinline__ void tile_update(const C (*T)[SNB + 1], const C (*Y)[SNB + 1], int qb, C *V, int ldr,
-                                            int i0, int rows, int rn) {
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    C acc[RT / NWARP];
-#pragma unroll
-    for (int j = 0; j < RT / NWARP; ++j) acc[j] = czero<C>();
-    for (int q = 0; q < qb; ++q) {
-        const C y = Y[q][lane];
-#pragma unroll
-        for (int j = 0; j < RT / NWARP; ++j) cfma(acc[j], T[warp + NWARP * j][q], y);
-    }
-    if (lane < rn) {
-#pragma unroll
-        for (int j = 0; j < RT / NWARP; ++j) {
-            const int row = warp + NWARP * j;
-            if (row < rows) {
-                C &d = V[(size_t)(i0 + row) * ldr + lane];
-                d = csub(d, acc[j]);
+// sm.L[q][p] = the inverse diagonal-block operator of pivot block k0:
+//   FWD && !TRANS: L^-1        FWD && TRANS: (U^-1)^T
+//   !FWD && !TRANS: U^-1       !FWD && TRANS: (L^-1)^T
+// The stored block holds L^-1 strictly below the diagonal (unit diagonal
+// implied) and U^-1 on and above it.
+template <class C, bool FWD, bool TRANS>
+__device__ __forceinline__ void stage_dinv(SolveSmem<C> &sm, const C *F, int f, int k0, int kb) {
+    for (int t = threadIdx.x; t < SNB * SNB; t += NT) {
+        const int p = t % SNB, q = t / SNB;   // operator entry (p, q) -> sm.L[q][p]
+        C v = czero<C>();
+        if (p < kb && q < kb) {
+            const bool lower_src = FWD != TRANS;         // L^-1 (or its transpose) wanted
+            const int r = TRANS ? q : p, c = TRANS ? p : q;  // position in the stored block
+            if (lower_src) {
+                if (r > c) v = F[(k0 + r) + (size_t)(k0 + c) * f];
+                else if (r == c) v = mk(decltype(v.x)(1), decltype(v.x)(0));
+            } else if (r <= c) {
+                v = F[(k0 + r) + (size_t)(k0 + c) * f];
             }
         }
+        sm.L[q][p] = v;
     }
+}
+
+// acc[a][b] += sum_q sm.L[q][tr + 16a] * sm.Y[q][tc + 8b]
+template <class C>
+__device__ __forceinline__ void tile_mma(const SolveSmem<C> &sm, int qb, C (&acc)[4][4], int tr, int tc) {
+#pragma unroll 4
+    for (int q = 0; q < qb; ++q) {
+        C l[4], y[4];
+#pragma unroll
+        for (int a = 0; a < 4; ++a) l[a] = sm.L[q][tr + 16 * a];
+#pragma unroll
+        for (int b = 0; b < 4; ++b) y[b] = sm.Y[q][tc + 8 * b];
+#pragma unroll
+        for (int a = 0; a < 4; ++a)
+#pragma unroll
+            for (int b = 0; b < 4; ++b) cfma(acc[a][b], l[a], y[b]);
+    }
+}
+
+template <class C>
+__device__ __forceinline__ void zero_acc(C (&acc)[4][4]) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a)
+#pragma unroll
+        for (int b = 0; b < 4; ++b) acc[a][b] = czero<C>();
+}
+
+// V[(i0 + row) * ldr + col] -= acc for the thread's rows/columns
+template <class C>
+__device__ __forceinline__ void sub_acc(C *V, int ldr, int i0, int rows, int rn, const C (&acc)[4][4], int tr, int tc) {
+#pragma unroll
+    for (int a = 0; a < 4; ++a) {
+        const int row = tr + 16 * a;
+        if (row >= rows) continue;
+        C *v = V + (size_t)(i0 + row) * ldr;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int col = tc + 8 * b;
+            if (col < rn) v[col] = csub(v[col], acc[a][b]);
+        }
+    }
+}
+
+template <class R>
+struct Ctx {
+    using C = cplx<R>;
+    int node, f, s, rn;
+    const C *F;
+    C *X, *W;
+};
+
+template <class R>
+__device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first, int chunk) {
+    using C = cplx<R>;
+    Ctx<R> c;
+    c.node = a.s.lvl_nodes[lvl_first + blockIdx.y];
+    c.f = a.s.nfront[c.node];
+    c.s = a.s.npiv[c.node];
+    const int r0 = chunk * TC;
+    c.rn = min(TC, a.nrhs - r0);
+    const size_t fz = blockIdx.z;
+    c.F = reinterpret_cast<const C *>(a.front) + fz * a.s.front_total + a.s.front_off[c.node];
+    c.X = reinterpret_cast<C *>(a.x) + fz * (size_t)a.s.n * a.ldr + r0;
+    c.W = reinterpret_cast<C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + r0 + (size_t)a.s.rhs_off[c.node] * a.ldr;
+    return c;
 }
 
 template <class R, bool TRANS>
-__global__ void __launch_bounds__(256) k_fwd(SolveArgs<R> a, int lvl_first) {
+__global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first) {
     using C = cplx<R>;
-    extern __shared__ unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     SolveSmem<C> &sm = *reinterpret_cast<SolveSmem<C> *>(smem_raw);
-    const int node = a.s.lvl_nodes[lvl_first + blockIdx.y];
-    const int f = a.s.nfront[node], s = a.s.npiv[node];
-    const int r0 = blockIdx.x * a.rch;
-    const int rn = min(a.rch, a.nrhs - r0);
-    if (rn <= 0) return;
+    const Ctx<R> c = make_ctx(a, lvl_first, blockIdx.x);
+    if (c.rn <= 0) return;
+    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int *vars = a.s.vars + a.s.var_off[c.node];
+    const int *inv = a.s.inv + a.s.inv_off[c.node];
     const size_t fz = blockIdx.z;
-    const C *F = reinterpret_cast<const C *>(a.front) + fz * a.s.front_total + a.s.front_off[node];
-    C *X = reinterpret_cast<C *>(a.x) + fz * (size_t)a.s.n * a.ldr + r0;
-    C *Wall = reinterpret_cast<C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + r0;
-    C *W = Wall + (size_t)a.s.rhs_off[node] * a.ldr;
-    const int *vars = a.s.vars + a.s.var_off[node];
-    const int *inv = a.s.inv + a.s.inv_off[node];
-    const int c0 = a.s.child0[node], c1 = a.s.child1[node];
+    const C *Wall = reinterpret_cast<const C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + blockIdx.x * TC;
+    const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
     const C *W0 = c0 >= 0 ? Wall + (size_t)(a.s.rhs_off[c0] + a.s.npiv[c0]) * a.ldr : nullptr;
     const C *W1 = c1 >= 0 ? Wall + (size_t)(a.s.rhs_off[c1] + a.s.npiv[c1]) * a.ldr : nullptr;
 
-    // gather the front vector (warp per row, lane per right-hand side)
-    for (int i = warp; i < f; i += NWARP) {
-        if (lane < rn) {
-            C v = i < s ? X[(size_t)vars[i] * a.ldr + lane] : czero<C>();
+    // gather the front vector: warp per row, lane per right-hand side
+    for (int i = warp; i < c.f; i += NT / 32) {
+        if (lane < c.rn) {
+            C v = i < c.s ? c.X[(size_t)vars[i] * a.ldr + lane] : czero<C>();
             if (W0) { const int q = inv[i]; if (q >= 0) v = cadd(v, W0[(size_t)q * a.ldr + lane]); }
-            if (W1) { const int q = inv[f + i]; if (q >= 0) v = cadd(v, W1[(size_t)q * a.ldr + lane]); }
-            W[(size_t)i * a.ldr + lane] = v;
+            if (W1) { const int q = inv[c.f + i]; if (q >= 0) v = cadd(v, W1[(size_t)q * a.ldr + lane]); }
+            c.W[(size_t)i * a.ldr + lane] = v;
         }
     }
+    __syncthreads();
 
-    for (int k0 = 0; k0 < s; k0 += SNB) {
-        const int kb = min(SNB, s - k0);
-        if (!TRANS) {
-            for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-                const int p = t % kb, q = t / kb;
-                if (p >= q) sm.D[p][q] = F[(k0 + p) + (size_t)(k0 + q) * f];
-            }
-        } else {
-            for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-                const int q = t % kb, p = t / kb;
-                if (p >= q) sm.D[p][q] = F[(k0 + q) + (size_t)(k0 + p) * f];
-            }
-        }
-        __syncthreads();   // D staged; W rows of this block final
-        for (int r = warp; r < rn; r += NWARP) {
-            C y = lane < kb ? W[(size_t)(k0 + lane) * a.ldr + r] : czero<C>();
-            for (int p = 0; p < kb; ++p) {
-                if (TRANS && lane == p) y = cmul(y, crcp(sm.D[p][p]));
-                const C yp = shfl(y, p);
-                if (lane > p && lane < kb) cfms(y, sm.D[lane][p], yp);
-            }
-            if (lane < kb) sm.Y[lane][r] = y;
+    C acc[4][4];
+    for (int k0 = 0; k0 < c.s; k0 += SNB) {
+        const int kb = min(SNB, c.s - k0);
+        stage_dinv<C, true, TRANS>(sm, c.F, c.f, k0, kb);
+        for (int t = threadIdx.x; t < SNB * TC; t += NT) {
+            const int q = t / TC, r = t % TC;
+            sm.Y[q][r] = (q < kb && r < c.rn) ? c.W[(size_t)(k0 + q) * a.ldr + r] : czero<C>();
         }
         __syncthreads();
-        for (int q = warp; q < kb; q += NWARP) {
-            if (lane < rn) {
-                const C y = sm.Y[q][lane];
-                W[(size_t)(k0 + q) * a.ldr + lane] = y;
-                X[(size_t)vars[k0 + q] * a.ldr + lane] = y;
+        zero_acc(acc);
+        tile_mma(sm, kb, acc, tr, tc);   // y_b = Dinv w_b (rows tr + 16a < 32 valid)
+        __syncthreads();
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2) {
+            const int p = tr + 16 * a2;
+#pragma unroll
+            for (int b = 0; b < 4; ++b) sm.Y[p][tc + 8 * b] = acc[a2][b];
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < kb * TC; t += NT) {
+            const int q = t / TC, r = t % TC;
+            if (r < c.rn) {
+                const C y = sm.Y[q][r];
+                c.W[(size_t)(k0 + q) * a.ldr + r] = y;
+                c.X[(size_t)vars[k0 + q] * a.ldr + r] = y;
             }
         }
-        for (int i0 = k0 + kb; i0 < f; i0 += RT) {
-            const int rows = min(RT, f - i0);
-            stage_tile<C, TRANS>(sm.L, F, f, i0, rows, k0, kb);
+        // remaining pivot rows of this front (the ring is k_fwd_ring's)
+        for (int i0 = k0 + kb; i0 < c.s; i0 += RT) {
+            const int rows = min(RT, c.s - i0);
+            stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, k0, kb);
             __syncthreads();
-            tile_update<C>(sm.L, sm.Y, kb, W, a.ldr, i0, rows, rn);
+            zero_acc(acc);
+            tile_mma(sm, kb, acc, tr, tc);
+            sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
             __syncthreads();
         }
     }
 }
 
+// blockIdx.x = chunk + nchunk * tile
 template <class R, bool TRANS>
-__global__ void __launch_bounds__(256) k_bwd(SolveArgs<R> a, int lvl_first) {
+__global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, int nchunk) {
     using C = cplx<R>;
-    extern __shared__ unsigned char smem_raw[];
+    extern __shared__ __align__(16) unsigned char smem_raw[];
     SolveSmem<C> &sm = *reinterpret_cast<SolveSmem<C> *>(smem_raw);
-    const int node = a.s.lvl_nodes[lvl_first + blockIdx.y];
-    const int f = a.s.nfront[node], s = a.s.npiv[node];
-    const int r0 = blockIdx.x * a.rch;
-    const int rn = min(a.rch, a.nrhs - r0);
-    if (rn <= 0) return;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const size_t fz = blockIdx.z;
-    const C *F = reinterpret_cast<const C *>(a.front) + fz * a.s.front_total + a.s.front_off[node];
-    C *X = reinterpret_cast<C *>(a.x) + fz * (size_t)a.s.n * a.ldr + r0;
-    C *T = reinterpret_cast<C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + r0 +
-           (size_t)a.s.rhs_off[node] * a.ldr;   // rows 0..s-1 hold y from the forward pass
-    const int *vars = a.s.vars + a.s.var_off[node];
-
-    // t = y - U'12 x2: 64-row tiles of t, ring in blocks of 32
-    for (int i0 = 0; i0 < s; i0 += RT) {
-        const int rows = min(RT, s - i0);
-        for (int j0 = s; j0 < f; j0 += SNB) {
-            const int jb = min(SNB, f - j0);
-            for (int q = warp; q < jb; q += NWARP)
-                sm.Y[q][lane] = lane < rn ? X[(size_t)vars[j0 + q] * a.ldr + lane] : czero<C>();
-            stage_tile<C, TRANS>(sm.L, F, f, i0, rows, j0, jb);
-            __syncthreads();
-            tile_update<C>(sm.L, sm.Y, jb, T, a.ldr, i0, rows, rn);
-            __syncthreads();
+    const int chunk = blockIdx.x % nchunk, tile = blockIdx.x / nchunk;
+    const Ctx<R> c = make_ctx(a, lvl_first, chunk);
+    const int i0 = c.s + tile * RT;
+    if (c.rn <= 0 || i0 >= c.f) return;
+    const int rows = min(RT, c.f - i0);
+    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
+    C acc[4][4];
+    zero_acc(acc);
+    for (int q0 = 0; q0 < c.s; q0 += SNB) {
+        const int qb = min(SNB, c.s - q0);
+        stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, q0, qb);
+        for (int t = threadIdx.x; t < SNB * TC; t += NT) {
+            const int q = t / TC, r = t % TC;
+            sm.Y[q][r] = (q < qb && r < c.rn) ? c.W[(size_t)(q0 + q) * a.ldr + r] : czero<C>();
         }
+        __syncthreads();
+        tile_mma(sm, qb, acc, tr, tc);
+        __syncthreads();
     }
-    // blocked back substitution with U'11, last block first
-    const int nblk = (s + SNB - 1) / SNB;
+    sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
+}
+
+// t -= U'(pivot rows, ring) x_ring ; blockIdx.x = chunk + nchunk * tile
+template <class R, bool TRANS>
+__global__ void __launch_bounds__(NT) k_bwd_ring(SolveArgs<R> a, int lvl_first, int nchunk) {
+    using C = cplx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SolveSmem<C> &sm = *reinterpret_cast<SolveSmem<C> *>(smem_raw);
+    const int chunk = blockIdx.x % nchunk, tile = blockIdx.x / nchunk;
+    const Ctx<R> c = make_ctx(a, lvl_first, chunk);
+    const int i0 = tile * RT;
+    if (c.rn <= 0 || i0 >= c.s || c.f == c.s) return;
+    const int rows = min(RT, c.s - i0);
+    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
+    const int *vars = a.s.vars + a.s.var_off[c.node];
+    C acc[4][4];
+    zero_acc(acc);
+    for (int j0 = c.s; j0 < c.f; j0 += SNB) {
+        const int jb = min(SNB, c.f - j0);
+        stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, j0, jb);
+        for (int t = threadIdx.x; t < SNB * TC; t += NT) {
+            const int q = t / TC, r = t % TC;
+            sm.Y[q][r] = (q < jb && r < c.rn) ? c.X[(size_t)vars[j0 + q] * a.ldr + r] : czero<C>();
+        }
+        __syncthreads();
+        tile_mma(sm, jb, acc, tr, tc);
+        __syncthreads();
+    }
+    sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
+}
+
+template <class R, bool TRANS>
+__global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first) {
+    using C = cplx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SolveSmem<C> &sm = *reinterpret_cast<SolveSmem<C> *>(smem_raw);
+    const Ctx<R> c = make_ctx(a, lvl_first, blockIdx.x);
+    if (c.rn <= 0) return;
+    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
+    const int *vars = a.s.vars + a.s.var_off[c.node];
+    C acc[4][4];
+    const int nblk = (c.s + SNB - 1) / SNB;
     for (int b = nblk - 1; b >= 0; --b) {
-        const int k0 = b * SNB, kb = min(SNB, s - k0);
-        if (!TRANS) {
-            for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-                const int p = t % kb, q = t / kb;
-                if (p <= q) sm.D[p][q] = F[(k0 + p) + (size_t)(k0 + q) * f];
-            }
-        } else {
-            for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-                const int q = t % kb, p = t / kb;
-                if (p <= q) sm.D[p][q] = F[(k0 + q) + (size_t)(k0 + p) * f];
-            }
+        const int k0 = b * SNB, kb = min(SNB, c.s - k0);
+        stage_dinv<C, false, TRANS>(sm, c.F, c.f, k0, kb);
+        for (int t = threadIdx.x; t < SNB * TC; t += NT) {
+            const int q = t / TC, r = t % TC;
+            sm.Y[q][r] = (q < kb && r < c.rn) ? c.W[(size_t)(k0 + q) * a.ldr + r] : czero<C>();
         }
         __syncthreads();
-        for (int r = warp; r < rn; r += NWARP) {
-            C t = lane < kb ? T[(size_t)(k0 + lane) * a.ldr + r] : czero<C>();
-            for (int p = kb - 1; p >= 0; --p) {
-                if (!TRANS && lane == p) t = cmul(t, crcp(sm.D[p][p]));
-                const C xp = shfl(t, p);
-                if (lane < p) cfms(t, sm.D[lane][p], xp);
-            }
-            if (lane < kb) sm.Y[lane][r] = t;
+        zero_acc(acc);
+        tile_mma(sm, kb, acc, tr, tc);   // x_b = Dinv t_b
+        __syncthreads();
+#pragma unroll
+        for (int a2 = 0; a2 < 2; ++a2) {
+            const int p = tr + 16 * a2;
+#pragma unroll
+            for (int bb = 0; bb < 4; ++bb) sm.Y[p][tc + 8 * bb] = acc[a2][bb];
         }
         __syncthreads();
-        for (int q = warp; q < kb; q += NWARP)
-            if (lane < rn) X[(size_t)vars[k0 + q] * a.ldr + lane] = sm.Y[q][lane];
+        for (int t = threadIdx.x; t < kb * TC; t += NT) {
+            const int q = t / TC, r = t % TC;
+            if (r < c.rn) c.X[(size_t)vars[k0 + q] * a.ldr + r] = sm.Y[q][r];
+        }
         for (int i0 = 0; i0 < k0; i0 += RT) {
             const int rows = min(RT, k0 - i0);
-            stage_tile<C, TRANS>(sm.L, F, f, i0, rows, k0, kb);
+            stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, k0, kb);
             __syncthreads();
-            tile_update<C>(sm.L, sm.Y, kb, T, a.ldr, i0, rows, rn);
+            zero_acc(acc);
+            tile_mma(sm, kb, acc, tr, tc);
+            sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
             __syncthreads();
         }
     }
 }
 
 template <class R>
-static void set_smem(const void *fn) {
-    cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(SolveSmem<cplx<R>>));
+static size_t solve_smem() { return sizeof(SolveSmem<cplx<R>>); }
+
+template <class R>
+static void set_attrs() {
+    static bool done = false;
+    if (done) return;
+    const int sm = (int)solve_smem<R>();
+    cudaFuncSetAttribute((const void *)k_fwd_piv<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_fwd_piv<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_fwd_ring<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_fwd_ring<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_bwd_ring<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_bwd_ring<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_bwd_piv<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_bwd_piv<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    done = true;
 }
 
 template <class R>
 void launch_solve_forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
     if (L.count == 0) return;
-    static bool attr = false;
-    if (!attr) {
-        set_smem<R>((const void *)k_fwd<R, false>);
-        set_smem<R>((const void *)k_fwd<R, true>);
-        attr = true;
+    set_attrs<R>();
+    const size_t smem = solve_smem<R>();
+    const int nchunk = (a.nrhs + TC - 1) / TC;
+    dim3 g1(nchunk, L.count, a.nf);
+    if (a.trans) (k_fwd_piv<R, true><<<g1, NT, smem, st>>>(a, L.first), note_launch());
+    else (k_fwd_piv<R, false><<<g1, NT, smem, st>>>(a, L.first), note_launch());
+    const int ring_max = L.max_ring;
+    if (ring_max > 0) {
+        dim3 g2(nchunk * ((ring_max + RT - 1) / RT), L.count, a.nf);
+        if (a.trans) (k_fwd_ring<R, true><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
+        else (k_fwd_ring<R, false><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
     }
-    const size_t smem = sizeof(SolveSmem<cplx<R>>);
-    dim3 grid((a.nrhs + a.rch - 1) / a.rch, L.count, a.nf);
-    if (a.trans) (k_fwd<R, true><<<grid, 32 * NWARP, smem, st>>>(a, L.first), note_launch());
-    else (k_fwd<R, false><<<grid, 32 * NWARP, smem, st>>>(a, L.first), note_launch());
 }
 
 template <class R>
 void launch_solve_backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
     if (L.count == 0) return;
-    static bool attr = false;
-    if (!attr) {
-        set_smem<R>((const void *)k_bwd<R, false>);
-        set_smem<R>((const void *)k_bwd<R, true>);
-        attr = true;
+    set_attrs<R>();
+    const size_t smem = solve_smem<R>();
+    const int nchunk = (a.nrhs + TC - 1) / TC;
+    if (L.max_ring > 0) {
+        dim3 g1(nchunk * ((L.max_piv + RT - 1) / RT), L.count, a.nf);
+        if (a.trans) (k_bwd_ring<R, true><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
+        else (k_bwd_ring<R, false><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
     }
-    const size_t smem = sizeof(SolveSmem<cplx<R>>);
-    dim3 grid((a.nrhs + a.rch - 1) / a.rch, L.count, a.nf);
-    if (a.trans) (k_bwd<R, true><<<grid, 32 * NWARP, smem, st>>>(a, L.first), note_launch());
-    else (k_bwd<R, false><<<grid, 32 * NWARP, smem, st>>>(a, L.first), note_launch());
+    dim3 g2(nchunk, L.count, a.nf);
+    if (a.trans) (k_bwd_piv<R, true><<<g2, NT, smem, st>>>(a, L.first), note_launch());
+    else (k_bwd_piv<R, false><<<g2, NT, smem, st>>>(a, L.first), note_launch());
 }
 
 template void launch_solve_forward_level<double>(const SolveArgs<double> &, const LevelInfo &, cudaStream_t);
