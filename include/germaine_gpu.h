@@ -167,6 +167,19 @@ int gm_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y,
            int ntr, const int32_t *rec_x, const int32_t *rec_y,
            const float *pobs, int stf_inv, int misfit, float *l2);
 
+/* gm_solve without device allocation.  No counterpart in the reference: for
+ * callers that cannot call cudaMalloc/cudaFree while solving -- cudaFree
+ * synchronises the whole device (stalling the caller's own kernels on other
+ * streams), and a caller that has reserved its device memory budget up
+ * front has none left to give.  Same arguments and result as gm_solve, but
+ * b and x must be device pointers, and every workspace comes from one
+ * file-scope device array of 32 MiB (held by every GPU that loads the
+ * library until exit); problems whose workspaces do not fit return
+ * GM_ERROR_INVALID.  The first call on a device looks up the array's
+ * address (make it before any stream capture); calls whose GPU work
+ * overlaps race on the shared array. */
+int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d_b, double *d_x);
+
 /* ---- symbolic-analysis introspection (host only, no GPU needed) ---- */
 typedef struct gm_symbolic gm_symbolic;
 int gm_symbolic_create(int nx, int ny, int leaf_max, gm_symbolic **out);

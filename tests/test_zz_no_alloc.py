@@ -1,0 +1,66 @@
+"""gm_solve_noalloc: the block solve + refinement for callers that cannot
+allocate device memory while solving (cudaFree stalls every stream of the
+device; a caller with a fixed, pre-reserved memory budget has nothing left to
+allocate from).  Its workspaces live in one fixed-size device array inside
+the library instead of cudaMalloc'd buffers.  Checked through the C-ABI
+against gm_solve on the same factors, on two calls in a row (the second one
+runs over the first one's leftovers in the shared array)."""
+import ctypes
+
+import numpy as np
+import pytest
+
+from germaine_b200 import GM_PREC_C64_IR, GM_PREC_FP64, GM_SYS_A, GM_SYS_AT, Engine, _lib
+from tests.models import inclusion_ac, random_smooth
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / np.linalg.norm(b))
+
+
+@pytest.mark.parametrize("precision", [GM_PREC_FP64, GM_PREC_C64_IR], ids=["fp64", "c64ir"])
+@pytest.mark.parametrize("sys_", [GM_SYS_A, GM_SYS_AT], ids=["A", "At"])
+def test_noalloc_solve_matches_gm_solve_twice(precision, sys_):
+    import torch
+    nx, ny, dh, npml = 47, 35, 10.0, 8
+    vp, rho = inclusion_ac(nx, ny, dh, npml, radius=50.0)
+    vp = vp * random_smooth(nx, ny, 0.9, 1.1, 4)
+    rng = np.random.default_rng(9)
+    nrhs = 6
+    b = rng.standard_normal((2, nx * ny, nrhs)) + 1j * rng.standard_normal((2, nx * ny, nrhs))
+    lib = _lib.load()
+    with Engine(nx, ny, dh, npml, precision=precision, leaf_max=24) as e:
+        e.set_model(vp, rho)
+        e.factor([8.0, 14.0])
+        x_ref = e.solve(b, sys=sys_)                      # gm_solve
+        res_ref = e.stats()["ir_residual"]
+        b_d = torch.from_numpy(b.view(np.float64).copy()).cuda()
+        for _ in range(2):
+            x_d = torch.full_like(b_d, float("nan"))
+            torch.cuda.synchronize()
+            rc = lib.gm_solve_noalloc(e._h, sys_, nrhs, _lib.ptr(b_d), _lib.ptr(x_d))
+            _lib.check(rc)
+            torch.cuda.synchronize()
+            x = x_d.cpu().numpy().view(np.complex128).reshape(b.shape)
+            assert _rel(x, x_ref) <= 1e-10
+            assert e.stats()["ir_residual"] <= 1e-10
+        assert res_ref <= 1e-10
+
+
+def test_noalloc_rejects_problems_beyond_the_scratch():
+    import torch
+    nx, ny, dh, npml = 120, 90, 10.0, 10
+    vp = random_smooth(nx, ny, 1800, 2600, 1)
+    rho = np.full((ny, nx), 1000.0, np.float32)
+    lib = _lib.load()
+    with Engine(nx, ny, dh, npml) as e:
+        e.set_model(vp, rho)
+        e.factor([6.0, 9.0, 12.0])
+        nrhs = 64
+        b_d = torch.zeros((3, nx * ny, 2 * nrhs), dtype=torch.float64, device="cuda")
+        x_d = torch.zeros_like(b_d)
+        rc = lib.gm_solve_noalloc(e._h, GM_SYS_A, nrhs, _lib.ptr(b_d), _lib.ptr(x_d))
+        assert rc == _lib.GM_ERROR_INVALID
+        assert b"scratch" in lib.gm_last_error()
