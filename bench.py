@@ -293,6 +293,7 @@ def run_gpu(args):
         "mixed_over_fp64": fp64["ms"] / mixed["ms"],
         "ir_iterations": st["ir_iterations"],
         "ir_residual": st["ir_residual"],
+        "perturbed_pivots": {"mixed": st["perturbed_pivots"], "fp64": fp64["stats"]["perturbed_pivots"]},
         "phase_ms": {"assemble": st["ms_assemble"], "factor": st["ms_factor"], "solve": st["ms_solve"],
                      "refine": st["ms_refine"], "substitutions": st["ms_subst"], "n_subst": st["n_subst"]},
         "roofline": {"kernel": "K5 multi-RHS substitution (k_fwd + k_bwd, complex64)", "bound": "hbm",

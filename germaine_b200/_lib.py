@@ -54,7 +54,7 @@ class GmStats(ctypes.Structure):
 EXPORTS = [
     "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats", "gm_engine_stream",
     "gm_set_model", "gm_factor", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
-    "gm_get_gradient_fp64", "gm_solve_noalloc",
+    "gm_get_gradient_fp64", "gm_solve_noalloc", "gm_cgemm_sub_c64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
 ]
@@ -94,6 +94,7 @@ def load() -> ctypes.CDLL:
     lib.gm_obj.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, i32, i32, vp]
     lib.gm_get_gradient_fp64.argtypes = [vp, vp, vp]
     lib.gm_solve_noalloc.argtypes = [vp, i32, i32, vp, vp]
+    lib.gm_cgemm_sub_c64.argtypes = [i32, i32, i32, vp, vp, vp, vp]
     lib.gm_symbolic_create.argtypes = [i32, i32, i32, ctypes.POINTER(vp)]
     lib.gm_symbolic_destroy.argtypes = [vp]
     lib.gm_symbolic_sizes.argtypes = [vp, vp]

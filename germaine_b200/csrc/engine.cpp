@@ -366,7 +366,6 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     const bool fp64 = e->cfg.precision == GM_PREC_FP64;
     GM_ALLOC(e->d_t, cnt * e->csize());
     GM_ALLOC(e->d_w, (size_t)e->nf * e->sym.rhs_total * nrhs * e->csize());
-    GM_ALLOC(e->d_r, cnt * sizeof(double2));
     const int nblk_max = (e->n + 63) / 64;
     GM_ALLOC(e->d_part, (size_t)nblk_max * e->nf * nrhs * 2 * sizeof(double));
     GM_ALLOC(e->d_norm, (size_t)e->nf * nrhs * 2 * sizeof(double));
@@ -393,7 +392,7 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     // refinement: r = b - M' x (FP64), x += M'^{-1} r (working precision)
     ResidArgs ra{};
     ra.nx = e->cfg.nx; ra.ny = e->cfg.ny; ra.n = e->n; ra.nf = e->nf; ra.nrhs = nrhs; ra.ldr = nrhs;
-    ra.A = e->d_A.as<double2>(); ra.x = d_x; ra.b = d_b; ra.r = e->d_r.as<double2>();
+    ra.A = e->d_A.as<double2>(); ra.x = d_x; ra.b = d_b; ra.r = nullptr;
     ra.op_mode = e->cfg.op_mode; ra.trans = sys;
     const int cntn = e->nf * nrhs * 2;
     std::vector<double> norms(cntn);
@@ -401,7 +400,9 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     int it = 0;
     GM_CUDA(cudaEventRecord(t0, e->st));
     for (;; ++it) {
-        const int nblk = launch_residual(ra, e->d_part.as<double>(), nblk_max, e->st);
+        // residual straight into the working-precision right-hand side
+        const int nblk = fp64 ? launch_residual_t<double>(ra, e->d_t.p, e->d_part.as<double>(), nblk_max, e->st)
+                              : launch_residual_t<float>(ra, e->d_t.p, e->d_part.as<double>(), nblk_max, e->st);
         launch_reduce_norms(e->d_part.as<double>(), nblk, cntn, e->d_norm.as<double>(), e->st);
         GM_CUDA(cudaGetLastError());
         GM_CUDA(cudaMemcpyAsync(norms.data(), e->d_norm.p, cntn * sizeof(double), cudaMemcpyDeviceToHost, e->st));
@@ -420,8 +421,6 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
             return fail(GM_ERROR_NONFINITE, "non-finite residual after %d refinement sweeps", it);
         }
         if (worst <= e->cfg.ir_tol || it >= e->cfg.ir_max_iter) break;
-        if (fp64) launch_convert_down<double>(e->d_r.as<double2>(), e->d_t.p, cnt, e->st);
-        else launch_convert_down<float>(e->d_r.as<double2>(), e->d_t.p, cnt, e->st);
         if (fp64) substitute<double>(e, e->d_t.p, nrhs, sys);
         else substitute<float>(e, e->d_t.p, nrhs, sys);
         if (fp64) launch_add_up<double>(d_x, e->d_t.p, cnt, e->st);

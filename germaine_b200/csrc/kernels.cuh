@@ -93,6 +93,9 @@ struct ResidArgs {
 // part[nblk][nf][nrhs][2]; returns nblk.
 int launch_residual(const ResidArgs &a, double *part, int max_blocks, cudaStream_t st);
 void launch_reduce_norms(const double *part, int nblk, int cnt, double *out, cudaStream_t st);
+// as launch_residual, but writes (T)(b - M'x) into t [nf][n][ldr] instead of r
+template <class R>
+int launch_residual_t(const ResidArgs &a, void *t, double *part, int max_blocks, cudaStream_t st);
 
 // y(T) <- x(double) and x(double) += d(T) over [nf][n][ldr]
 template <class R>

@@ -18,7 +18,10 @@ __device__ __forceinline__ double2 op_coef(const double2 *A9, int n, int nx, boo
     return A9[(size_t)(8 - q) * n + c];
 }
 
-__global__ void __launch_bounds__(128) k_residual(ResidArgs a, double *part) {
+// OutC = double2 writes r = b - M'x; OutC = cplx<R> writes the refinement
+// right-hand side directly in the working precision of the substitution.
+template <class OutC>
+__global__ void __launch_bounds__(128) k_residual(ResidArgs a, OutC *out, double *part) {
     const int f = blockIdx.y;
     const int k0 = blockIdx.x * RROWS, k1 = min(a.n, k0 + RROWS);
     const bool use_row = (a.op_mode == GM_OP_EXACT) != (a.trans != 0);
@@ -38,7 +41,7 @@ __global__ void __launch_bounds__(128) k_residual(ResidArgs a, double *part) {
                 const double2 xv = a.x[base + (size_t)(yy * a.nx + xx) * a.ldr + r];
                 cfms(acc, m, xv);
             }
-            a.r[base + (size_t)k * a.ldr + r] = acc;
+            out[base + (size_t)k * a.ldr + r] = cconv<OutC>(acc);
             rr += acc.x * acc.x + acc.y * acc.y;
             bb += bv.x * bv.x + bv.y * bv.y;
         }
@@ -51,9 +54,20 @@ __global__ void __launch_bounds__(128) k_residual(ResidArgs a, double *part) {
 int launch_residual(const ResidArgs &a, double *part, int max_blocks, cudaStream_t st) {
     const int nblk = (a.n + RROWS - 1) / RROWS;
     if (nblk > max_blocks) return -1;
-    (k_residual<<<dim3(nblk, a.nf), 128, 0, st>>>(a, part), note_launch());
+    (k_residual<double2><<<dim3(nblk, a.nf), 128, 0, st>>>(a, a.r, part), note_launch());
     return nblk;
 }
+
+template <class R>
+int launch_residual_t(const ResidArgs &a, void *t, double *part, int max_blocks, cudaStream_t st) {
+    const int nblk = (a.n + RROWS - 1) / RROWS;
+    if (nblk > max_blocks) return -1;
+    (k_residual<cplx<R>><<<dim3(nblk, a.nf), 128, 0, st>>>(a, reinterpret_cast<cplx<R> *>(t), part), note_launch());
+    return nblk;
+}
+
+template int launch_residual_t<double>(const ResidArgs &, void *, double *, int, cudaStream_t);
+template int launch_residual_t<float>(const ResidArgs &, void *, double *, int, cudaStream_t);
 
 // out[c] = sum over blocks of part[blk][c] (fixed order: deterministic)
 __global__ void k_reduce_norms(const double *part, int nblk, int cnt, double *out) {

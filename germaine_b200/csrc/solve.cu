@@ -90,10 +90,18 @@ __device__ __forceinline__ void stage_dinv(SolveSmem<C> &sm, const C *F, int f, 
     }
 }
 
-// acc[a][b] += sum_q sm.L[q][tr + 16a] * sm.Y[q][tc + 8b]
+// acc[a][b] += sum_q sm.L[q][tr + 16a] * sm.Y[q][tc + 8b] for the output rows
+// below `rows` and right-hand sides below `rn`; row groups a and column
+// groups b that lie entirely outside are skipped warp-uniformly (a warp owns
+// rows 4w..4w+3 of each 16-row group), so small fronts and short slices do
+// not pay for the full 64 x 32 tile.
 template <class C>
-__device__ __forceinline__ void tile_mma(const SolveSmem<C> &sm, int qb, C (&acc)[4][4], int tr, int tc) {
-#pragma unroll 4
+__device__ __forceinline__ void tile_mma(const SolveSmem<C> &sm, int qb, C (&acc)[4][4], int tr, int tc, int rows,
+                                         int rn) {
+    const int wrow = (threadIdx.x >> 5) * 4;
+    const int na = rows <= wrow ? 0 : min(4, (rows - wrow + 15) / 16);
+    const int nb = min(4, (rn + 7) / 8);
+#pragma unroll 2
     for (int q = 0; q < qb; ++q) {
         C l[4], y[4];
 #pragma unroll
@@ -101,9 +109,12 @@ __device__ __forceinline__ void tile_mma(const SolveSmem<C> &sm, int qb, C (&acc
 #pragma unroll
         for (int b = 0; b < 4; ++b) y[b] = sm.Y[q][tc + 8 * b];
 #pragma unroll
-        for (int a = 0; a < 4; ++a)
+        for (int a = 0; a < 4; ++a) {
+            if (a >= na) break;
 #pragma unroll
-            for (int b = 0; b < 4; ++b) cfma(acc[a][b], l[a], y[b]);
+            for (int b = 0; b < 4; ++b)
+                if (b < nb) cfma(acc[a][b], l[a], y[b]);
+        }
     }
 }
 
@@ -155,8 +166,10 @@ __device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first,
     return c;
 }
 
+// fused = 1: the level's rings fit one row tile, so the ring rows are
+// updated here, block by block, and k_fwd_ring is not launched.
 template <class R, bool TRANS>
-__global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first) {
+__global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, int fused) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SolveSmem<C> &sm = *reinterpret_cast<SolveSmem<C> *>(smem_raw);
@@ -193,7 +206,7 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first) {
         }
         __syncthreads();
         zero_acc(acc);
-        tile_mma(sm, kb, acc, tr, tc);   // y_b = Dinv w_b (rows tr + 16a < 32 valid)
+        tile_mma(sm, kb, acc, tr, tc, kb, c.rn);   // y_b = Dinv w_b
         __syncthreads();
 #pragma unroll
         for (int a2 = 0; a2 < 2; ++a2) {
@@ -210,13 +223,14 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first) {
                 c.X[(size_t)vars[k0 + q] * a.ldr + r] = y;
             }
         }
-        // remaining pivot rows of this front (the ring is k_fwd_ring's)
-        for (int i0 = k0 + kb; i0 < c.s; i0 += RT) {
-            const int rows = min(RT, c.s - i0);
+        // remaining pivot rows of this front, and the ring when fused
+        const int row_end = fused ? c.f : c.s;
+        for (int i0 = k0 + kb; i0 < row_end; i0 += RT) {
+            const int rows = min(RT, row_end - i0);
             stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, k0, kb);
             __syncthreads();
             zero_acc(acc);
-            tile_mma(sm, kb, acc, tr, tc);
+            tile_mma(sm, kb, acc, tr, tc, rows, c.rn);
             sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
             __syncthreads();
         }
@@ -245,7 +259,7 @@ __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, 
             sm.Y[q][r] = (q < qb && r < c.rn) ? c.W[(size_t)(q0 + q) * a.ldr + r] : czero<C>();
         }
         __syncthreads();
-        tile_mma(sm, qb, acc, tr, tc);
+        tile_mma(sm, qb, acc, tr, tc, rows, c.rn);
         __syncthreads();
     }
     sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
@@ -274,14 +288,16 @@ __global__ void __launch_bounds__(NT) k_bwd_ring(SolveArgs<R> a, int lvl_first, 
             sm.Y[q][r] = (q < jb && r < c.rn) ? c.X[(size_t)vars[j0 + q] * a.ldr + r] : czero<C>();
         }
         __syncthreads();
-        tile_mma(sm, jb, acc, tr, tc);
+        tile_mma(sm, jb, acc, tr, tc, rows, c.rn);
         __syncthreads();
     }
     sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
 }
 
+// fused = 1: the level's rings fit one 32-wide block sweep cheaply, so
+// t -= U'(pivots, ring) x_ring is done here and k_bwd_ring is not launched.
 template <class R, bool TRANS>
-__global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first) {
+__global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, int fused) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     SolveSmem<C> &sm = *reinterpret_cast<SolveSmem<C> *>(smem_raw);
@@ -290,6 +306,25 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first) {
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const int *vars = a.s.vars + a.s.var_off[c.node];
     C acc[4][4];
+    if (fused) {
+        for (int i0 = 0; i0 < c.s; i0 += RT) {
+            const int rows = min(RT, c.s - i0);
+            zero_acc(acc);
+            for (int j0 = c.s; j0 < c.f; j0 += SNB) {
+                const int jb = min(SNB, c.f - j0);
+                stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, j0, jb);
+                for (int t = threadIdx.x; t < SNB * TC; t += NT) {
+                    const int q = t / TC, r = t % TC;
+                    sm.Y[q][r] = (q < jb && r < c.rn) ? c.X[(size_t)vars[j0 + q] * a.ldr + r] : czero<C>();
+                }
+                __syncthreads();
+                tile_mma(sm, jb, acc, tr, tc, rows, c.rn);
+                __syncthreads();
+            }
+            sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
+        }
+        __syncthreads();
+    }
     const int nblk = (c.s + SNB - 1) / SNB;
     for (int b = nblk - 1; b >= 0; --b) {
         const int k0 = b * SNB, kb = min(SNB, c.s - k0);
@@ -300,7 +335,7 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first) {
         }
         __syncthreads();
         zero_acc(acc);
-        tile_mma(sm, kb, acc, tr, tc);   // x_b = Dinv t_b
+        tile_mma(sm, kb, acc, tr, tc, kb, c.rn);   // x_b = Dinv t_b
         __syncthreads();
 #pragma unroll
         for (int a2 = 0; a2 < 2; ++a2) {
@@ -318,7 +353,7 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first) {
             stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, k0, kb);
             __syncthreads();
             zero_acc(acc);
-            tile_mma(sm, kb, acc, tr, tc);
+            tile_mma(sm, kb, acc, tr, tc, rows, c.rn);
             sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
             __syncthreads();
         }
@@ -351,10 +386,11 @@ void launch_solve_forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaS
     const size_t smem = solve_smem<R>();
     const int nchunk = (a.nrhs + TC - 1) / TC;
     dim3 g1(nchunk, L.count, a.nf);
-    if (a.trans) (k_fwd_piv<R, true><<<g1, NT, smem, st>>>(a, L.first), note_launch());
-    else (k_fwd_piv<R, false><<<g1, NT, smem, st>>>(a, L.first), note_launch());
+    const int fused = 0;   // separate ring kernel: more parallelism per level
+    if (a.trans) (k_fwd_piv<R, true><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
+    else (k_fwd_piv<R, false><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
     const int ring_max = L.max_ring;
-    if (ring_max > 0) {
+    if (ring_max > 0 && !fused) {
         dim3 g2(nchunk * ((ring_max + RT - 1) / RT), L.count, a.nf);
         if (a.trans) (k_fwd_ring<R, true><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
         else (k_fwd_ring<R, false><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
@@ -367,14 +403,15 @@ void launch_solve_backward_level(const SolveArgs<R> &a, const LevelInfo &L, cuda
     set_attrs<R>();
     const size_t smem = solve_smem<R>();
     const int nchunk = (a.nrhs + TC - 1) / TC;
-    if (L.max_ring > 0) {
+    const int fused = 0;
+    if (L.max_ring > 0 && !fused) {
         dim3 g1(nchunk * ((L.max_piv + RT - 1) / RT), L.count, a.nf);
         if (a.trans) (k_bwd_ring<R, true><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
         else (k_bwd_ring<R, false><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
     }
     dim3 g2(nchunk, L.count, a.nf);
-    if (a.trans) (k_bwd_piv<R, true><<<g2, NT, smem, st>>>(a, L.first), note_launch());
-    else (k_bwd_piv<R, false><<<g2, NT, smem, st>>>(a, L.first), note_launch());
+    if (a.trans) (k_bwd_piv<R, true><<<g2, NT, smem, st>>>(a, L.first, fused), note_launch());
+    else (k_bwd_piv<R, false><<<g2, NT, smem, st>>>(a, L.first, fused), note_launch());
 }
 
 template void launch_solve_forward_level<double>(const SolveArgs<double> &, const LevelInfo &, cudaStream_t);

@@ -180,6 +180,14 @@ int gm_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y,
  * overlaps race on the shared array. */
 int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d_b, double *d_x);
 
+/* Batched complex64 GEMM C_i -= A_i * B_i on device pointers: the Schur
+ * update of the mixed-precision factorisation (the dense kernel behind
+ * umfpack_zi_numeric's front updates) exposed for testing.  dims holds
+ * (m, n, k, lda, ldb, ldc) per problem, all matrices column-major.
+ * backend 1 = tcgen05 tensor cores (3xTF32 split products), 0 = CUDA cores. */
+int gm_cgemm_sub_c64(int device, int backend, int nprob, const int32_t *dims, void *const *A, void *const *B,
+                     void *const *C);
+
 /* ---- symbolic-analysis introspection (host only, no GPU needed) ---- */
 typedef struct gm_symbolic gm_symbolic;
 int gm_symbolic_create(int nx, int ny, int leaf_max, gm_symbolic **out);
