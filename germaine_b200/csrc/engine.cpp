@@ -13,11 +13,14 @@
 
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <new>
 
 #include "host_setup.h"
+#include "kernels_tc.cuh"
 
 using gm::fail;
 
@@ -238,6 +241,67 @@ static int assemble_batch(gm_engine *e) {
     return GM_OK;
 }
 
+// Builds the per-level list of contribution-block products
+// C[s:f, s:f] -= L21 * U12 (K = npiv) over every front and frequency, and
+// their output tiles: tcgen05 tiles (128 x 64) for the complex64 path on
+// levels whose blocks are large enough to fill them, CUDA-core tiles
+// (64 x 64) otherwise.
+template <class R>
+static int build_cb_plan(gm_engine *e) {
+    using C = cplx_any<R>;
+    const Symbolic &s = e->sym;
+    const bool c64 = e->cfg.precision == GM_PREC_C64_IR;
+    // Smallest contribution block routed to the tcgen05 kernel.  Off by
+    // default: the kernel's accumulation keeps a ~1e-7 relative bias on
+    // same-sign sums (truncation inside each MMA) that costs the refinement
+    // two extra sweeps on the 841 x 227 benchmark, while the block GEMM is a
+    // small part of the factorisation time; GM_TC_MIN_BLOCK=<rows> enables it.
+    int kTcMinBlock = 1 << 30;
+    if (const char *v = std::getenv("GM_TC_MIN_BLOCK")) kTcMinBlock = std::atoi(v);
+    std::vector<GemmProb<R>> probs;
+    std::vector<int4> tiles;
+    e->cb_plan.assign(e->levels.size(), {});
+    C *base = e->d_front.as<C>();
+    for (size_t h = 0; h < e->levels.size(); ++h) {
+        const LevelInfo &L = e->levels[h];
+        int max_cb = 0;
+        for (int t = L.first; t < L.first + L.count; ++t) {
+            const int v = s.lvl_nodes[t];
+            max_cb = std::max(max_cb, s.nfront[v] - s.npiv[v]);
+        }
+        const int backend = (c64 && max_cb >= kTcMinBlock) ? 1 : 0;
+        const int tr = backend ? cgemm_tile_rows() : kGemmTileCC, tc = backend ? cgemm_tile_cols() : kGemmTileCC;
+        auto &pl = e->cb_plan[h];
+        pl.backend = backend;
+        pl.prob_off = (int64_t)probs.size();
+        pl.tile_off = (int64_t)tiles.size();
+        for (int f = 0; f < e->nf; ++f)
+            for (int t = L.first; t < L.first + L.count; ++t) {
+                const int v = s.lvl_nodes[t];
+                const int fr = s.nfront[v], sp = s.npiv[v], m = fr - sp;
+                if (sp == 0 || m == 0) continue;
+                C *F = base + (size_t)f * s.front_total + s.front_off[v];
+                GemmProb<R> p{F + sp, F + (size_t)sp * fr, F + sp + (size_t)sp * fr, fr, fr, fr, m, m, sp};
+                const int id = (int)(probs.size() - pl.prob_off);
+                probs.push_back(p);
+                for (int a = 0; a < (m + tr - 1) / tr; ++a)
+                    for (int b = 0; b < (m + tc - 1) / tc; ++b) tiles.push_back(make_int4(id, a, b, 0));
+            }
+        pl.ntiles = (int)(tiles.size() - pl.tile_off);
+    }
+    GM_ALLOC(e->d_cb_probs, probs.size() * sizeof(GemmProb<R>) + 16);
+    GM_ALLOC(e->d_cb_tiles, tiles.size() * sizeof(int4) + 16);
+    GM_ALLOC(e->d_tcerr, sizeof(int));
+    if (!probs.empty())
+        GM_CUDA(cudaMemcpyAsync(e->d_cb_probs.p, probs.data(), probs.size() * sizeof(GemmProb<R>), cudaMemcpyHostToDevice, e->st));
+    if (!tiles.empty())
+        GM_CUDA(cudaMemcpyAsync(e->d_cb_tiles.p, tiles.data(), tiles.size() * sizeof(int4), cudaMemcpyHostToDevice, e->st));
+    GM_CUDA(cudaStreamSynchronize(e->st));
+    e->cb_plan_base = e->d_front.p;
+    e->cb_plan_nf = e->nf;
+    return GM_OK;
+}
+
 template <class R>
 static int factor_batch(gm_engine *e, R pivtol) {
     FactorArgs<R> a{};
@@ -249,7 +313,22 @@ static int factor_batch(gm_engine *e, R pivtol) {
     a.nf = e->nf;
     a.pivtol = pivtol;
     a.npert = e->d_npert.as<unsigned long long>();
-    for (const LevelInfo &L : e->levels) launch_factor_level<R>(a, L, e->st);
+    if (e->cb_plan_base != e->d_front.p || e->cb_plan_nf != e->nf) {
+        const int rc = build_cb_plan<R>(e);
+        if (rc) return rc;
+    }
+    GM_CUDA(cudaMemsetAsync(e->d_tcerr.p, 0, sizeof(int), e->st));
+    const GemmProb<R> *probs = e->d_cb_probs.as<GemmProb<R>>();
+    const int4 *tiles = e->d_cb_tiles.as<int4>();
+    for (size_t h = 0; h < e->levels.size(); ++h) {
+        launch_factor_level<R>(a, e->levels[h], e->st);
+        const auto &pl = e->cb_plan[h];
+        if (pl.backend == 1)
+            launch_cgemm_sub(1, reinterpret_cast<const CgemmProb *>(probs + pl.prob_off), tiles + pl.tile_off,
+                             pl.ntiles, e->d_tcerr.as<int>(), e->st);
+        else
+            launch_gemm_sub_cc<R>(probs + pl.prob_off, tiles + pl.tile_off, pl.ntiles, e->st);
+    }
     GM_CUDA(cudaGetLastError());
     return GM_OK;
 }
@@ -305,6 +384,9 @@ extern "C" int gm_factor(gm_engine *e, int nfreq, const float *h_freqs) {
     e->stats.ms_factor = ms;
     unsigned long long np = 0;
     GM_CUDA(cudaMemcpy(&np, e->d_npert.p, sizeof np, cudaMemcpyDeviceToHost));
+    int tcerr = 0;
+    GM_CUDA(cudaMemcpy(&tcerr, e->d_tcerr.p, sizeof tcerr, cudaMemcpyDeviceToHost));
+    if (tcerr) return fail(GM_ERROR_CUDA, "gm_factor: a tensor-core wait timed out in the contribution-block update");
     e->stats.perturbed_pivots = (int64_t)np;
     e->factored = true;
     return np ? GM_WARNING_PERTURBED : GM_OK;
@@ -420,6 +502,7 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
             e->stats.ir_residual = NAN;
             return fail(GM_ERROR_NONFINITE, "non-finite residual after %d refinement sweeps", it);
         }
+        if (std::getenv("GM_TRACE_REFINEMENT")) std::fprintf(stderr, "refinement sweep %d: max relative residual %.3e\n", it, worst);
         if (worst <= e->cfg.ir_tol || it >= e->cfg.ir_max_iter) break;
         if (fp64) substitute<double>(e, e->d_t.p, nrhs, sys);
         else substitute<float>(e, e->d_t.p, nrhs, sys);

@@ -64,6 +64,14 @@ struct gm_engine {
     gm::DevBuf d_A, d_mass, d_pml, d_fq, d_front, d_npert;
     bool factored = false;
 
+    // contribution-block GEMM plan per level (rebuilt when the front
+    // storage moves or the batch size changes)
+    struct CbPlan { int backend; int64_t prob_off, tile_off; int ntiles; };
+    std::vector<CbPlan> cb_plan;
+    gm::DevBuf d_cb_probs, d_cb_tiles, d_tcerr;
+    const void *cb_plan_base = nullptr;
+    int cb_plan_nf = 0;
+
     // solve workspaces
     gm::DevBuf d_x, d_b, d_r, d_t, d_w, d_part, d_norm;
 

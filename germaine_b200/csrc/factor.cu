@@ -178,6 +178,10 @@ __global__ void __launch_bounds__(PCHUNK) k_panel(FactorArgs<R> a, int lvl_first
 
 // Trailing update C -= Lp * Up on one TILE x TILE tile; 256 threads, each
 // owns a 4 x 4 complex sub-tile with rows tx + 16a and columns ty + 16b.
+// Only the part of the trailing matrix that still belongs to pivot rows or
+// pivot columns is updated here; the contribution block (rows and columns
+// >= npiv) receives all pivot steps at once in one K = npiv GEMM at the end
+// of the level (launch_cb_gemm).
 template <class R>
 __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, int k0, int ntmax) {
     using C = cplx<R>;
@@ -234,6 +238,7 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
     }
     const int ti = blockIdx.x / ntmax, tj = blockIdx.x % ntmax;
     if (ti >= nt || tj >= nt) return;
+    if (i0 + ti * TILE >= s && i0 + tj * TILE >= s) return;   // tile inside the contribution block
 
     extern __shared__ unsigned char smem_raw[];
     C *Ls = reinterpret_cast<C *>(smem_raw);   // [NB][TILE]: Ls[c*TILE + r]
@@ -270,13 +275,85 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
 #pragma unroll
         for (int p = 0; p < 4; ++p) {
             const int row = r0 + tx + 16 * p;
-            if (row < f) {
+            if (row < f && (row < s || col < s)) {
                 C &d = F[row + (size_t)col * f];
                 d = csub(d, acc[p][q]);
             }
         }
     }
 }
+
+// Batched C -= A * B on CUDA cores (64 x 64 output tiles, K in chunks of NB
+// staged through shared memory, 4 x 4 complex register tile per thread):
+// the contribution-block update of every front of a level in one launch.
+template <class R>
+__global__ void __launch_bounds__(256) k_gemm_sub_cc(const GemmProb<R> *__restrict__ probs,
+                                                     const int4 *__restrict__ tiles) {
+    using C = cplx<R>;
+    const int4 tl = tiles[blockIdx.x];
+    const GemmProb<R> p = probs[tl.x];
+    const int r0 = tl.y * TILE, c0 = tl.z * TILE;
+    extern __shared__ unsigned char smem_raw[];
+    C *As = reinterpret_cast<C *>(smem_raw);   // [NB][TILE]
+    C *Bs = As + NB * TILE;                    // [NB][TILE]
+    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    C acc[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+        for (int j = 0; j < 4; ++j) acc[i][j] = czero<C>();
+    for (int k0 = 0; k0 < p.k; k0 += NB) {
+        const int kb = min(NB, p.k - k0);
+        for (int t = threadIdx.x; t < NB * TILE; t += blockDim.x) {
+            const int r = t % TILE, c = t / TILE;
+            As[t] = (c < kb && r0 + r < p.m) ? p.A[(size_t)(r0 + r) + (size_t)(k0 + c) * p.lda] : czero<C>();
+            const int col = t / NB, cc = t % NB;
+            Bs[cc * TILE + col] = (cc < kb && c0 + col < p.n) ? p.B[(size_t)(k0 + cc) + (size_t)(c0 + col) * p.ldb]
+                                                              : czero<C>();
+        }
+        __syncthreads();
+        for (int c = 0; c < kb; ++c) {
+            C lv[4], uv[4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) lv[i] = As[c * TILE + tx + 16 * i];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) uv[j] = Bs[c * TILE + ty + 16 * j];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int j = 0; j < 4; ++j) cfma(acc[i][j], lv[i], uv[j]);
+        }
+        __syncthreads();
+    }
+#pragma unroll
+    for (int j = 0; j < 4; ++j) {
+        const int col = c0 + ty + 16 * j;
+        if (col >= p.n) continue;
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            const int row = r0 + tx + 16 * i;
+            if (row < p.m) {
+                C &d = p.C[(size_t)row + (size_t)col * p.ldc];
+                d = csub(d, acc[i][j]);
+            }
+        }
+    }
+}
+
+template <class R>
+void launch_gemm_sub_cc(const GemmProb<R> *d_probs, const int4 *d_tiles, int ntiles, cudaStream_t st) {
+    if (ntiles <= 0) return;
+    const size_t smem = 2 * NB * TILE * sizeof(cplx<R>);
+    static bool attr = false;
+    if (!attr) {
+        cudaFuncSetAttribute(k_gemm_sub_cc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr = true;
+    }
+    (k_gemm_sub_cc<R><<<ntiles, 256, smem, st>>>(d_probs, d_tiles), note_launch());
+}
+
+template void launch_gemm_sub_cc<double>(const GemmProb<double> *, const int4 *, int, cudaStream_t);
+template void launch_gemm_sub_cc<float>(const GemmProb<float> *, const int4 *, int, cudaStream_t);
 
 template <class R>
 void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {

@@ -7,6 +7,11 @@
 
 namespace gm {
 
+template <class R> struct cplx_any_t;
+template <> struct cplx_any_t<double> { using type = double2; };
+template <> struct cplx_any_t<float> { using type = float2; };
+template <class R> using cplx_any = typename cplx_any_t<R>::type;
+
 // Counts kernel launches of this library (reported in gm_stats).
 void note_launch();
 long long launch_count();
@@ -61,6 +66,19 @@ struct FactorArgs {
 
 template <class R>
 void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st);
+
+// one dense product C -= A * B (column-major, complex<R>)
+template <class R>
+struct GemmProb {
+    const cplx_any<R> *A;
+    const cplx_any<R> *B;
+    cplx_any<R> *C;
+    int lda, ldb, ldc, m, n, k;
+};
+// CUDA-core batched GEMM over 64 x 64 tiles: tiles[t] = (problem, tile row, tile col)
+template <class R>
+void launch_gemm_sub_cc(const GemmProb<R> *d_probs, const int4 *d_tiles, int ntiles, cudaStream_t st);
+constexpr int kGemmTileCC = 64;
 
 // ---------------- K5 multi-RHS substitution ----------------
 template <class R>

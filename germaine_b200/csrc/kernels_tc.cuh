@@ -6,12 +6,8 @@
 
 namespace gm {
 
-struct CgemmProb {
-    const float2 *A;   // m x k, column-major, leading dimension lda
-    const float2 *B;   // k x n, column-major, ldb
-    float2 *C;         // m x n, column-major, ldc
-    int lda, ldb, ldc, m, n, k;
-};
+// A: m x k, B: k x n, C: m x n, column-major with leading dimensions lda/ldb/ldc
+using CgemmProb = GemmProb<float>;
 
 // tiles[t] = (problem, tile row, tile column) of a 128 x 64 output tile;
 // backend 1 = tcgen05 (3xTF32), 0 = CUDA cores.  *d_err is set to 1 if a

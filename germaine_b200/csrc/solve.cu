@@ -10,20 +10,22 @@
 // CUDA cores: 128 threads, each owning a 4 x 4 complex register tile of a
 // 64-row x 32-right-hand-side output tile, operands staged in shared memory.
 //
-// Per elimination-tree level:
+// Pivot rows are solved in place in x (their rows of x hold the right-hand
+// side, then y, then the solution); the workspace w holds only each front's
+// update vector for its parent (its ring rows).  Per elimination-tree level:
 //   forward  (leaves -> root)
-//     k_fwd_piv   gather the front vector w (own rows of x + the children's
-//                 update vectors, by the extend-add inverse maps), then per
-//                 32-pivot block: y_b = L_bb^-1 w_b, w_rest -= L_rb y_b over
-//                 the remaining pivot rows; y goes back to x at the pivots;
+//     k_fwd_piv   add the children's update vectors (by the extend-add
+//                 inverse maps) into x at the pivots and into the front's own
+//                 update vector at the ring rows, then per 32-pivot block:
+//                 y_b = L_bb^-1 x_b, x_rest -= L_rb y_b over the remaining
+//                 pivot rows;
 //     k_fwd_ring  w_ring -= L_ring,piv * y over 64-row tiles of the ring
-//                 (many CTAs per front: the wide part of the level), leaving
-//                 this front's update vector for its parent;
+//                 (many CTAs per front: the wide part of the level);
 //   backward (root -> leaves)
-//     k_bwd_ring  t = y - U_piv,ring * x_ring (x_ring = final values of the
+//     k_bwd_ring  x_piv -= U_piv,ring * x_ring (x_ring = final values of the
 //                 ancestors' variables), 64-row tiles of the pivot rows;
-//     k_bwd_piv   per block from the last: x_b = U_bb^-1 t_b, scatter to x,
-//                 t_above -= U_ab x_b.
+//     k_bwd_piv   per block from the last: x_b = U_bb^-1 x_b,
+//                 x_above -= U_ab x_b.
 // trans = 1 solves M^T x = b with the same factors: M^T = U^T L^T, the
 // forward pass runs with U^T and the backward pass with L^T; only the
 // factor indexing and which stored inverse is used change.
@@ -126,14 +128,14 @@ __device__ __forceinline__ void zero_acc(C (&acc)[4][4]) {
         for (int b = 0; b < 4; ++b) acc[a][b] = czero<C>();
 }
 
-// V[(i0 + row) * ldr + col] -= acc for the thread's rows/columns
-template <class C>
-__device__ __forceinline__ void sub_acc(C *V, int ldr, int i0, int rows, int rn, const C (&acc)[4][4], int tr, int tc) {
+// row_ptr(row)[col] -= acc for the thread's rows (< rows) and columns (< rn)
+template <class C, class RowPtr>
+__device__ __forceinline__ void sub_acc(RowPtr row_ptr, int rows, int rn, const C (&acc)[4][4], int tr, int tc) {
 #pragma unroll
     for (int a = 0; a < 4; ++a) {
         const int row = tr + 16 * a;
         if (row >= rows) continue;
-        C *v = V + (size_t)(i0 + row) * ldr;
+        C *v = row_ptr(row);
 #pragma unroll
         for (int b = 0; b < 4; ++b) {
             const int col = tc + 8 * b;
@@ -142,12 +144,23 @@ __device__ __forceinline__ void sub_acc(C *V, int ldr, int i0, int rows, int rn,
     }
 }
 
+// sm.Y[q][r] = row_ptr(q)[r] for q < qb, r < rn; zeros elsewhere
+template <class C, class RowPtr>
+__device__ __forceinline__ void stage_rows(SolveSmem<C> &sm, RowPtr row_ptr, int qb, int rn) {
+    for (int t = threadIdx.x; t < SNB * TC; t += NT) {
+        const int q = t / TC, r = t % TC;
+        sm.Y[q][r] = (q < qb && r < rn) ? row_ptr(q)[r] : czero<C>();
+    }
+}
+
 template <class R>
 struct Ctx {
     using C = cplx<R>;
     int node, f, s, rn;
     const C *F;
-    C *X, *W;
+    const int *vars;
+    C *X;   // this slice of x; pivot rows are solved in place here
+    C *W;   // this node's update vector: ring row i (front position s + i)
 };
 
 template <class R>
@@ -161,13 +174,16 @@ __device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first,
     c.rn = min(TC, a.nrhs - r0);
     const size_t fz = blockIdx.z;
     c.F = reinterpret_cast<const C *>(a.front) + fz * a.s.front_total + a.s.front_off[c.node];
+    c.vars = a.s.vars + a.s.var_off[c.node];
     c.X = reinterpret_cast<C *>(a.x) + fz * (size_t)a.s.n * a.ldr + r0;
     c.W = reinterpret_cast<C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + r0 + (size_t)a.s.rhs_off[c.node] * a.ldr;
     return c;
 }
 
-// fused = 1: the level's rings fit one row tile, so the ring rows are
-// updated here, block by block, and k_fwd_ring is not launched.
+// Forward pass, pivot part: add the children's update vectors (gathered by
+// the extend-add inverse maps) into x at this front's pivots and into this
+// front's own update vector at its ring rows, then solve the pivot rows in
+// place in x, 32-pivot block by block.
 template <class R, bool TRANS>
 __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, int fused) {
     using C = cplx<R>;
@@ -175,35 +191,40 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
     SolveSmem<C> &sm = *reinterpret_cast<SolveSmem<C> *>(smem_raw);
     const Ctx<R> c = make_ctx(a, lvl_first, blockIdx.x);
     if (c.rn <= 0) return;
+    (void)fused;
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int *vars = a.s.vars + a.s.var_off[c.node];
     const int *inv = a.s.inv + a.s.inv_off[c.node];
     const size_t fz = blockIdx.z;
     const C *Wall = reinterpret_cast<const C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + blockIdx.x * TC;
     const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
-    const C *W0 = c0 >= 0 ? Wall + (size_t)(a.s.rhs_off[c0] + a.s.npiv[c0]) * a.ldr : nullptr;
-    const C *W1 = c1 >= 0 ? Wall + (size_t)(a.s.rhs_off[c1] + a.s.npiv[c1]) * a.ldr : nullptr;
+    const C *W0 = c0 >= 0 ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
+    const C *W1 = c1 >= 0 ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
+    const size_t ldr = a.ldr;
 
-    // gather the front vector: warp per row, lane per right-hand side
     for (int i = warp; i < c.f; i += NT / 32) {
-        if (lane < c.rn) {
-            C v = i < c.s ? c.X[(size_t)vars[i] * a.ldr + lane] : czero<C>();
-            if (W0) { const int q = inv[i]; if (q >= 0) v = cadd(v, W0[(size_t)q * a.ldr + lane]); }
-            if (W1) { const int q = inv[c.f + i]; if (q >= 0) v = cadd(v, W1[(size_t)q * a.ldr + lane]); }
-            c.W[(size_t)i * a.ldr + lane] = v;
+        if (lane >= c.rn) continue;
+        const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
+        C v = czero<C>();
+        if (q0 >= 0) v = cadd(v, W0[(size_t)q0 * ldr + lane]);
+        if (q1 >= 0) v = cadd(v, W1[(size_t)q1 * ldr + lane]);
+        if (i < c.s) {
+            if (q0 >= 0 || q1 >= 0) {
+                C &x = c.X[(size_t)c.vars[i] * ldr + lane];
+                x = cadd(x, v);
+            }
+        } else {
+            c.W[(size_t)(i - c.s) * ldr + lane] = v;
         }
     }
     __syncthreads();
 
+    auto xrow = [&](int k) { return c.X + (size_t)c.vars[k] * ldr; };
     C acc[4][4];
     for (int k0 = 0; k0 < c.s; k0 += SNB) {
         const int kb = min(SNB, c.s - k0);
         stage_dinv<C, true, TRANS>(sm, c.F, c.f, k0, kb);
-        for (int t = threadIdx.x; t < SNB * TC; t += NT) {
-            const int q = t / TC, r = t % TC;
-            sm.Y[q][r] = (q < kb && r < c.rn) ? c.W[(size_t)(k0 + q) * a.ldr + r] : czero<C>();
-        }
+        stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
         __syncthreads();
         zero_acc(acc);
         tile_mma(sm, kb, acc, tr, tc, kb, c.rn);   // y_b = Dinv w_b
@@ -217,27 +238,23 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
         __syncthreads();
         for (int t = threadIdx.x; t < kb * TC; t += NT) {
             const int q = t / TC, r = t % TC;
-            if (r < c.rn) {
-                const C y = sm.Y[q][r];
-                c.W[(size_t)(k0 + q) * a.ldr + r] = y;
-                c.X[(size_t)vars[k0 + q] * a.ldr + r] = y;
-            }
+            if (r < c.rn) xrow(k0 + q)[r] = sm.Y[q][r];
         }
-        // remaining pivot rows of this front, and the ring when fused
-        const int row_end = fused ? c.f : c.s;
-        for (int i0 = k0 + kb; i0 < row_end; i0 += RT) {
-            const int rows = min(RT, row_end - i0);
+        for (int i0 = k0 + kb; i0 < c.s; i0 += RT) {
+            const int rows = min(RT, c.s - i0);
             stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, k0, kb);
             __syncthreads();
             zero_acc(acc);
             tile_mma(sm, kb, acc, tr, tc, rows, c.rn);
-            sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
+            sub_acc(
+                [&](int row) { return xrow(i0 + row); }, rows, c.rn, acc, tr, tc);
             __syncthreads();
         }
     }
 }
 
-// blockIdx.x = chunk + nchunk * tile
+// Forward pass, ring part: update vector -= L'(ring, pivots) y, 64-row tiles
+// of the ring over many CTAs; blockIdx.x = chunk + nchunk * tile
 template <class R, bool TRANS>
 __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, int nchunk) {
     using C = cplx<R>;
@@ -249,23 +266,22 @@ __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, 
     if (c.rn <= 0 || i0 >= c.f) return;
     const int rows = min(RT, c.f - i0);
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
+    const size_t ldr = a.ldr;
     C acc[4][4];
     zero_acc(acc);
     for (int q0 = 0; q0 < c.s; q0 += SNB) {
         const int qb = min(SNB, c.s - q0);
         stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, q0, qb);
-        for (int t = threadIdx.x; t < SNB * TC; t += NT) {
-            const int q = t / TC, r = t % TC;
-            sm.Y[q][r] = (q < qb && r < c.rn) ? c.W[(size_t)(q0 + q) * a.ldr + r] : czero<C>();
-        }
+        stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q0 + q] * ldr; }, qb, c.rn);
         __syncthreads();
         tile_mma(sm, qb, acc, tr, tc, rows, c.rn);
         __syncthreads();
     }
-    sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
+    sub_acc([&](int row) { return c.W + (size_t)(i0 - c.s + row) * ldr; }, rows, c.rn, acc, tr, tc);
 }
 
-// t -= U'(pivot rows, ring) x_ring ; blockIdx.x = chunk + nchunk * tile
+// Backward pass, ring part: x[pivots] -= U'(pivots, ring) x[ring]
+// (final values of the ancestors' variables); blockIdx.x = chunk + nchunk * tile
 template <class R, bool TRANS>
 __global__ void __launch_bounds__(NT) k_bwd_ring(SolveArgs<R> a, int lvl_first, int nchunk) {
     using C = cplx<R>;
@@ -277,25 +293,22 @@ __global__ void __launch_bounds__(NT) k_bwd_ring(SolveArgs<R> a, int lvl_first, 
     if (c.rn <= 0 || i0 >= c.s || c.f == c.s) return;
     const int rows = min(RT, c.s - i0);
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
-    const int *vars = a.s.vars + a.s.var_off[c.node];
+    const size_t ldr = a.ldr;
     C acc[4][4];
     zero_acc(acc);
     for (int j0 = c.s; j0 < c.f; j0 += SNB) {
         const int jb = min(SNB, c.f - j0);
         stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, j0, jb);
-        for (int t = threadIdx.x; t < SNB * TC; t += NT) {
-            const int q = t / TC, r = t % TC;
-            sm.Y[q][r] = (q < jb && r < c.rn) ? c.X[(size_t)vars[j0 + q] * a.ldr + r] : czero<C>();
-        }
+        stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[j0 + q] * ldr; }, jb, c.rn);
         __syncthreads();
         tile_mma(sm, jb, acc, tr, tc, rows, c.rn);
         __syncthreads();
     }
-    sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
+    sub_acc([&](int row) { return c.X + (size_t)c.vars[i0 + row] * ldr; }, rows, c.rn, acc, tr, tc);
 }
 
-// fused = 1: the level's rings fit one 32-wide block sweep cheaply, so
-// t -= U'(pivots, ring) x_ring is done here and k_bwd_ring is not launched.
+// Backward pass, pivot part: block by block from the last, x_b = Dinv t_b in
+// place in x, then t_above -= U'(above, b) x_b.
 template <class R, bool TRANS>
 __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, int fused) {
     using C = cplx<R>;
@@ -303,36 +316,16 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
     SolveSmem<C> &sm = *reinterpret_cast<SolveSmem<C> *>(smem_raw);
     const Ctx<R> c = make_ctx(a, lvl_first, blockIdx.x);
     if (c.rn <= 0) return;
+    (void)fused;
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
-    const int *vars = a.s.vars + a.s.var_off[c.node];
+    const size_t ldr = a.ldr;
+    auto xrow = [&](int k) { return c.X + (size_t)c.vars[k] * ldr; };
     C acc[4][4];
-    if (fused) {
-        for (int i0 = 0; i0 < c.s; i0 += RT) {
-            const int rows = min(RT, c.s - i0);
-            zero_acc(acc);
-            for (int j0 = c.s; j0 < c.f; j0 += SNB) {
-                const int jb = min(SNB, c.f - j0);
-                stage_factor<C, TRANS>(sm, c.F, c.f, i0, rows, j0, jb);
-                for (int t = threadIdx.x; t < SNB * TC; t += NT) {
-                    const int q = t / TC, r = t % TC;
-                    sm.Y[q][r] = (q < jb && r < c.rn) ? c.X[(size_t)vars[j0 + q] * a.ldr + r] : czero<C>();
-                }
-                __syncthreads();
-                tile_mma(sm, jb, acc, tr, tc, rows, c.rn);
-                __syncthreads();
-            }
-            sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
-        }
-        __syncthreads();
-    }
     const int nblk = (c.s + SNB - 1) / SNB;
     for (int b = nblk - 1; b >= 0; --b) {
         const int k0 = b * SNB, kb = min(SNB, c.s - k0);
         stage_dinv<C, false, TRANS>(sm, c.F, c.f, k0, kb);
-        for (int t = threadIdx.x; t < SNB * TC; t += NT) {
-            const int q = t / TC, r = t % TC;
-            sm.Y[q][r] = (q < kb && r < c.rn) ? c.W[(size_t)(k0 + q) * a.ldr + r] : czero<C>();
-        }
+        stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
         __syncthreads();
         zero_acc(acc);
         tile_mma(sm, kb, acc, tr, tc, kb, c.rn);   // x_b = Dinv t_b
@@ -346,7 +339,7 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
         __syncthreads();
         for (int t = threadIdx.x; t < kb * TC; t += NT) {
             const int q = t / TC, r = t % TC;
-            if (r < c.rn) c.X[(size_t)vars[k0 + q] * a.ldr + r] = sm.Y[q][r];
+            if (r < c.rn) xrow(k0 + q)[r] = sm.Y[q][r];
         }
         for (int i0 = 0; i0 < k0; i0 += RT) {
             const int rows = min(RT, k0 - i0);
@@ -354,7 +347,7 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
             __syncthreads();
             zero_acc(acc);
             tile_mma(sm, kb, acc, tr, tc, rows, c.rn);
-            sub_acc(c.W, a.ldr, i0, rows, c.rn, acc, tr, tc);
+            sub_acc([&](int row) { return xrow(i0 + row); }, rows, c.rn, acc, tr, tc);
             __syncthreads();
         }
     }

@@ -111,7 +111,7 @@ void build_symbolic(int nx, int ny, int leaf_max, Symbolic &s) {
     int64_t fo = 0, ro = 0;
     for (int v = 0; v < nn; ++v) {
         s.front_off[v] = fo; fo += (int64_t)s.nfront[v] * s.nfront[v];
-        s.rhs_off[v] = ro; ro += s.nfront[v];
+        s.rhs_off[v] = ro; ro += s.nfront[v] - s.npiv[v];
     }
     s.front_total = fo; s.rhs_total = ro;
 

@@ -35,7 +35,7 @@ struct Symbolic {
     int64_t front_total = 0;         // sum nfront^2 (elements per frequency)
     std::vector<int64_t> inv_off;    // inv[inv_off[v] + t*nfront[v] + i], t = child slot 0/1
     std::vector<int> inv;            // child contribution-block index feeding front position i, or -1
-    std::vector<int64_t> rhs_off;    // per-node offset in the front-vector workspace (sum nfront)
+    std::vector<int64_t> rhs_off;    // per-node offset of its update vector (the ring rows, sum nfront - npiv)
     int64_t rhs_total = 0;
 
     // matrix entries of the REF operator M = A^T scattered into fronts:

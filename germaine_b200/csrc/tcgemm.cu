@@ -12,18 +12,28 @@
 //       [Pr | Pi] = [Ar | Ai] * [[Br, Bi]; [-Bi, Br]]
 //     i.e. real A' (128 x 2k), real B' (128 x 2k, rows 0..63 give Re P,
 //     rows 64..127 give Im P), D = A' B'^T (M = 128, N = 128);
-//   * each real operand is split x = hi + lo with hi, lo TF32 (round to
-//     nearest), and D accumulates hi*hi + hi*lo + lo*hi (three MMAs per
-//     k-step) in FP32 in TMEM: close to FP32 accuracy at tensor-core rate;
+//   * each real operand is split into three TF32 pieces x = x1 + x2 + x3
+//     (round to nearest, ~33 significant bits in total) and D accumulates
+//     the six products of order <= 2 (x1y1, x1y2, x2y1, x1y3, x2y2, x3y1)
+//     in FP32 in TMEM: more accurate than an FP32 FMA (a two-piece split,
+//     ~22 bits, roughly doubled the refinement sweeps of the
+//     mixed-precision solve), still at tensor-core rate;
 //   * operands are staged per 16-complex K chunk into shared memory in the
 //     canonical K-major, no-swizzle layout (8-row x 16-byte core matrices:
 //     leading byte offset = 128 rows x 16 B between the two 16-B K halves
 //     of one MMA, stride byte offset = 128 B between 8-row groups);
-//   * one elected thread issues the 12 MMAs of a chunk and commits them to
-//     an mbarrier; all threads wait (bounded: on timeout an error flag is
-//     set and the kernel winds down) before the shared memory is reused;
-//   * epilogue: tcgen05.ld 32x32b (warp w owns accumulator lanes 32w..32w+31
-//     = rows of the tile), C -= D with coalesced column-major stores.
+//   * one elected thread issues the 24 MMAs of a chunk (smallest products
+//     first) and commits them to an mbarrier; all threads wait (bounded: on
+//     timeout an error flag is set and the kernel winds down) before the
+//     shared memory is reused;
+//   * the tensor core's FP32 accumulation is not round-to-nearest: its error
+//     grows linearly with the number of accumulated products (measured: at
+//     K = 454 real terms of one sign, 30x the error of FP32 FMA chains, all
+//     of it bias).  So TMEM accumulates one K chunk only; after each chunk
+//     every thread moves its accumulator row to registers (tcgen05.ld
+//     32x32b: warp w owns lanes 32w..32w+31 = rows of the tile) and adds it
+//     to an FP32 register accumulator with ordinary round-to-nearest adds;
+//   * epilogue: C -= accumulator with coalesced column-major stores.
 #include "kernels_tc.cuh"
 #include "cplx.cuh"
 
@@ -36,15 +46,15 @@ constexpr int TN = 64;           // complex tile columns (N of the MMA = 2 TN)
 constexpr int KC = 16;           // complex K per staged chunk -> 2 KC = 32 real
 constexpr int KR = 2 * KC;       // real K per chunk
 constexpr int NCHUNK16 = KR / 4; // 16-byte K chunks per operand row
-constexpr int OPER_BYTES = NCHUNK16 * 128 * 16;   // one operand (hi or lo): 16 KB
+constexpr int OPER_BYTES = NCHUNK16 * 128 * 16;   // one operand piece: 16 KB
 constexpr uint32_t TMEM_COLS = 128;
 constexpr long long WAIT_LIMIT = 1ll << 26;       // mbarrier polls before giving up
 
+constexpr int NSPLIT = 3;
+
 struct __align__(1024) TcSmem {
-    unsigned char a_hi[OPER_BYTES];
-    unsigned char a_lo[OPER_BYTES];
-    unsigned char b_hi[OPER_BYTES];
-    unsigned char b_lo[OPER_BYTES];
+    unsigned char a[NSPLIT][OPER_BYTES];
+    unsigned char b[NSPLIT][OPER_BYTES];
     unsigned long long mbar;
     uint32_t tmem_addr;
 };
@@ -57,6 +67,14 @@ __device__ __forceinline__ float tf32_rna(float x) {
     uint32_t r;
     asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
     return __uint_as_float(r);
+}
+
+// x -> three TF32 pieces (round to nearest each); x - p1 and r1 - p2 are exact
+__device__ __forceinline__ void split3(float x, float &p1, float &p2, float &p3) {
+    p1 = tf32_rna(x);
+    const float r1 = x - p1;
+    p2 = tf32_rna(r1);
+    p3 = tf32_rna(r1 - p2);
 }
 
 // shared-memory matrix descriptor, K-major, no swizzle (layout type 0),
@@ -99,6 +117,19 @@ __device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
     return false;
 }
 
+// 32 consecutive accumulator columns of this thread's lane
+__device__ __forceinline__ void tmem_ld32(uint32_t addr, uint32_t (&v)[32]) {
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
+        "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
+        "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
+        : "=r"(v[0]), "=r"(v[1]), "=r"(v[2]), "=r"(v[3]), "=r"(v[4]), "=r"(v[5]), "=r"(v[6]), "=r"(v[7]),
+          "=r"(v[8]), "=r"(v[9]), "=r"(v[10]), "=r"(v[11]), "=r"(v[12]), "=r"(v[13]), "=r"(v[14]), "=r"(v[15]),
+          "=r"(v[16]), "=r"(v[17]), "=r"(v[18]), "=r"(v[19]), "=r"(v[20]), "=r"(v[21]), "=r"(v[22]), "=r"(v[23]),
+          "=r"(v[24]), "=r"(v[25]), "=r"(v[26]), "=r"(v[27]), "=r"(v[28]), "=r"(v[29]), "=r"(v[30]), "=r"(v[31])
+        : "r"(addr));
+}
+
 // row r (0..127), real K index kr (0..31) -> byte offset in an operand
 __device__ __forceinline__ int oper_off(int r, int chunk16) { return chunk16 * (128 * 16) + r * 16; }
 
@@ -130,6 +161,10 @@ __global__ void __launch_bounds__(128) k_cgemm_tc(const CgemmProb *__restrict__ 
     bool ok = true;
 
     const int nk = (p.k + KC - 1) / KC;
+    float accr[TN], acci[TN];   // this thread's tile row: Re, Im of the product
+#pragma unroll
+    for (int q = 0; q < TN; ++q) { accr[q] = 0.f; acci[q] = 0.f; }
+    const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
     for (int kc = 0; kc < nk && ok; ++kc) {
         const int k0 = kc * KC;
         // ---- stage A': row i = tid, K' = [Re A(i, k0..k0+15) | Im A(i, ...)] ----
@@ -145,16 +180,15 @@ __global__ void __launch_bounds__(128) k_cgemm_tc(const CgemmProb *__restrict__ 
             }
 #pragma unroll
             for (int c = 0; c < NCHUNK16; ++c) {
-                float h[4], l[4];
+                float q1[4], q2[4], q3[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int kr = 4 * c + e;
-                    const float x = kr < KC ? re[kr] : im[kr - KC];
-                    h[e] = tf32_rna(x);
-                    l[e] = tf32_rna(x - h[e]);
+                    split3(kr < KC ? re[kr] : im[kr - KC], q1[e], q2[e], q3[e]);
                 }
-                *reinterpret_cast<float4 *>(sm.a_hi + oper_off(tid, c)) = make_float4(h[0], h[1], h[2], h[3]);
-                *reinterpret_cast<float4 *>(sm.a_lo + oper_off(tid, c)) = make_float4(l[0], l[1], l[2], l[3]);
+                *reinterpret_cast<float4 *>(sm.a[0] + oper_off(tid, c)) = make_float4(q1[0], q1[1], q1[2], q1[3]);
+                *reinterpret_cast<float4 *>(sm.a[1] + oper_off(tid, c)) = make_float4(q2[0], q2[1], q2[2], q2[3]);
+                *reinterpret_cast<float4 *>(sm.a[2] + oper_off(tid, c)) = make_float4(q3[0], q3[1], q3[2], q3[3]);
             }
         }
         // ---- stage B': row j' = tid; j' < 64: [Re B(:, j) ; -Im B(:, j)], j' >= 64: [Im B(:, j) ; Re B(:, j)] ----
@@ -170,18 +204,18 @@ __global__ void __launch_bounds__(128) k_cgemm_tc(const CgemmProb *__restrict__ 
             }
 #pragma unroll
             for (int c = 0; c < NCHUNK16; ++c) {
-                float h[4], l[4];
+                float q1[4], q2[4], q3[4];
 #pragma unroll
                 for (int e = 0; e < 4; ++e) {
                     const int kr = 4 * c + e;
                     float x;
                     if (half == 0) x = kr < KC ? re[kr] : -im[kr - KC];
                     else x = kr < KC ? im[kr] : re[kr - KC];
-                    h[e] = tf32_rna(x);
-                    l[e] = tf32_rna(x - h[e]);
+                    split3(x, q1[e], q2[e], q3[e]);
                 }
-                *reinterpret_cast<float4 *>(sm.b_hi + oper_off(tid, c)) = make_float4(h[0], h[1], h[2], h[3]);
-                *reinterpret_cast<float4 *>(sm.b_lo + oper_off(tid, c)) = make_float4(l[0], l[1], l[2], l[3]);
+                *reinterpret_cast<float4 *>(sm.b[0] + oper_off(tid, c)) = make_float4(q1[0], q1[1], q1[2], q1[3]);
+                *reinterpret_cast<float4 *>(sm.b[1] + oper_off(tid, c)) = make_float4(q2[0], q2[1], q2[2], q2[3]);
+                *reinterpret_cast<float4 *>(sm.b[2] + oper_off(tid, c)) = make_float4(q3[0], q3[1], q3[2], q3[3]);
             }
         }
         // generic-proxy shared-memory writes -> visible to the tensor core (async proxy)
@@ -190,62 +224,54 @@ __global__ void __launch_bounds__(128) k_cgemm_tc(const CgemmProb *__restrict__ 
         if (tid == 0) {
             asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
             const uint32_t lbo = 128 * 16, sbo = 128;
-            const uint32_t ahi = smem_u32(sm.a_hi), alo = smem_u32(sm.a_lo);
-            const uint32_t bhi = smem_u32(sm.b_hi), blo = smem_u32(sm.b_lo);
+            uint32_t ab[NSPLIT], bb[NSPLIT];
 #pragma unroll
-            for (int t = 0; t < KR / 8; ++t) {
-                const uint32_t off = (uint32_t)t * 2u * (128u * 16u);   // two 16-B K chunks per MMA (K = 8)
-                const uint32_t acc0 = (kc > 0 || t > 0) ? 1u : 0u;
-                mma_tf32(tmem, smem_desc(ahi + off, lbo, sbo), smem_desc(bhi + off, lbo, sbo), acc0);
-                mma_tf32(tmem, smem_desc(ahi + off, lbo, sbo), smem_desc(blo + off, lbo, sbo), 1u);
-                mma_tf32(tmem, smem_desc(alo + off, lbo, sbo), smem_desc(bhi + off, lbo, sbo), 1u);
+            for (int q = 0; q < NSPLIT; ++q) { ab[q] = smem_u32(sm.a[q]); bb[q] = smem_u32(sm.b[q]); }
+            // products of order <= 2, smallest first, each over the chunk's K;
+            // the chunk starts from a zero accumulator
+            const int pa[6] = {0, 1, 2, 0, 1, 0}, pb[6] = {2, 1, 0, 1, 0, 0};
+#pragma unroll
+            for (int u = 0; u < 6; ++u) {
+#pragma unroll
+                for (int t = 0; t < KR / 8; ++t) {
+                    const uint32_t off = (uint32_t)t * 2u * (128u * 16u);   // two 16-B K chunks per MMA (K = 8)
+                    const uint32_t acc = (t > 0 || u > 0) ? 1u : 0u;
+                    mma_tf32(tmem, smem_desc(ab[pa[u]] + off, lbo, sbo), smem_desc(bb[pb[u]] + off, lbo, sbo), acc);
+                }
             }
             asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
                          :: "r"(mbar) : "memory");
         }
         ok = mbar_wait(mbar, (uint32_t)(kc & 1));
         asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory");
-        if (!__syncthreads_and(ok)) ok = false;
+        if (!__syncthreads_and(ok)) { ok = false; break; }
+        // flush the chunk's accumulator into the register accumulator
+#pragma unroll
+        for (int js = 0; js < TN; js += 32) {
+            uint32_t vr[32], vi[32];
+            tmem_ld32(lane_base + (uint32_t)js, vr);
+            tmem_ld32(lane_base + (uint32_t)(TN + js), vi);
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+            for (int q = 0; q < 32; ++q) {
+                accr[js + q] += __uint_as_float(vr[q]);
+                acci[js + q] += __uint_as_float(vi[q]);
+            }
+        }
+        asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory");
     }
     if (!ok) {
         if (tid == 0) atomicExch(err, 1);
     } else if (nk > 0) {
-        // ---- epilogue: C -= D; thread owns tile row i, columns in slices of 32 ----
         const int i = m0 + warp * 32 + lane;
-        const uint32_t lane_base = tmem + ((uint32_t)(warp * 32) << 16);
-#pragma unroll 1
-        for (int js = 0; js < TN; js += 32) {
-            uint32_t vr[32], vi[32];
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                : "=r"(vr[0]), "=r"(vr[1]), "=r"(vr[2]), "=r"(vr[3]), "=r"(vr[4]), "=r"(vr[5]), "=r"(vr[6]),
-                  "=r"(vr[7]), "=r"(vr[8]), "=r"(vr[9]), "=r"(vr[10]), "=r"(vr[11]), "=r"(vr[12]), "=r"(vr[13]),
-                  "=r"(vr[14]), "=r"(vr[15]), "=r"(vr[16]), "=r"(vr[17]), "=r"(vr[18]), "=r"(vr[19]), "=r"(vr[20]),
-                  "=r"(vr[21]), "=r"(vr[22]), "=r"(vr[23]), "=r"(vr[24]), "=r"(vr[25]), "=r"(vr[26]), "=r"(vr[27]),
-                  "=r"(vr[28]), "=r"(vr[29]), "=r"(vr[30]), "=r"(vr[31])
-                : "r"(lane_base + (uint32_t)js));
-            asm volatile(
-                "tcgen05.ld.sync.aligned.32x32b.x32.b32 "
-                "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"
-                "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];"
-                : "=r"(vi[0]), "=r"(vi[1]), "=r"(vi[2]), "=r"(vi[3]), "=r"(vi[4]), "=r"(vi[5]), "=r"(vi[6]),
-                  "=r"(vi[7]), "=r"(vi[8]), "=r"(vi[9]), "=r"(vi[10]), "=r"(vi[11]), "=r"(vi[12]), "=r"(vi[13]),
-                  "=r"(vi[14]), "=r"(vi[15]), "=r"(vi[16]), "=r"(vi[17]), "=r"(vi[18]), "=r"(vi[19]), "=r"(vi[20]),
-                  "=r"(vi[21]), "=r"(vi[22]), "=r"(vi[23]), "=r"(vi[24]), "=r"(vi[25]), "=r"(vi[26]), "=r"(vi[27]),
-                  "=r"(vi[28]), "=r"(vi[29]), "=r"(vi[30]), "=r"(vi[31])
-                : "r"(lane_base + (uint32_t)(TN + js)));
-            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-            if (i < p.m) {
+        if (i < p.m) {
 #pragma unroll
-                for (int q = 0; q < 32; ++q) {
-                    const int j = n0 + js + q;
-                    if (j < p.n) {
-                        float2 &c = p.C[(size_t)i + (size_t)j * p.ldc];
-                        c.x -= __uint_as_float(vr[q]);
-                        c.y -= __uint_as_float(vi[q]);
-                    }
+            for (int q = 0; q < TN; ++q) {
+                const int j = n0 + q;
+                if (j < p.n) {
+                    float2 &c = p.C[(size_t)i + (size_t)j * p.ldc];
+                    c.x -= accr[q];
+                    c.y -= acci[q];
                 }
             }
         }

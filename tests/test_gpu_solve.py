@@ -84,3 +84,28 @@ def test_te_transpose_solve():
     A = OS.assembled_matrix(g, *O.Port(g).assemble(4, 2e8, m0, m1))
     xr = OS.DirectSolver(OS.operator(A)).solve(b[0], trans=True)
     assert _rel(x[0], xr) <= 1e-10
+
+
+@pytest.mark.parametrize("precision", [GM_PREC_FP64, GM_PREC_C64_IR], ids=["fp64", "c64ir"])
+def test_solve_large_fronts(precision):
+    """A grid whose upper fronts have contribution blocks above 96 rows, so
+    the complex64 path runs its contribution-block updates on tcgen05."""
+    nx, ny, dh, npml = 230, 170, 10.0, 12
+    g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml)
+    m0, m1 = _setup(nx, ny, dh, npml, seed=8)
+    rng = np.random.default_rng(12)
+    b = rng.standard_normal((1, g.n, 6)) + 1j * rng.standard_normal((1, g.n, 6))
+    with Engine(nx, ny, dh, npml, precision=precision) as e:
+        e.set_model(m0, m1)
+        e.factor([18.0])
+        x = e.solve(b)
+        st = e.stats()
+    A = OS.assembled_matrix(g, *O.Port(g).assemble(1, 18.0, m0, m1))
+    ds = OS.DirectSolver(OS.operator(A))
+    xr = ds.solve(b[0])
+    assert st["max_front"] > 200
+    res = max(np.linalg.norm(ds.M @ x[0][:, k] - b[0][:, k]) / np.linalg.norm(b[0][:, k]) for k in range(6))
+    assert res <= 1e-10
+    assert _rel(x[0], xr) <= (1e-10 if precision == GM_PREC_FP64 else 1e-8)
+    if precision == GM_PREC_C64_IR:
+        assert st["ir_iterations"] <= 4
