@@ -40,17 +40,29 @@ import numpy as np
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-NX0, NY0, DH, NPML = 801, 187, 25.0, 20
-FREQS = [float(f) for f in range(2, 12)]
-NSHOTS, ROW = 100, 2
+DH, NPML, ROW = 25.0, 20, 2
 METRIC = "shot-solves/s (factor+solve) mixed vs FP64 on B200 at resid<=1e-10; %roofline"
-WORKLOAD = "thrust 801x187 h=25m pml20 (841x227, N=190907), 10 freqs 2-11 Hz x 100 shots, 800 receivers, AC"
+
+# the benchmark workload; --nx0/--ny0/--nfreq/--nshots shrink it for
+# profiling captures (the bench line then names the smaller workload)
+W = {"nx0": 801, "ny0": 187, "nfreq": 10, "nshots": 100}
+
+
+def freqs_hz() -> list[float]:
+    return [float(f) for f in range(2, 2 + W["nfreq"])]
+
+
+def workload_name() -> str:
+    nx, ny = W["nx0"] + 2 * NPML, W["ny0"] + 2 * NPML
+    f = freqs_hz()
+    return (f"thrust {W['nx0']}x{W['ny0']} h=25m pml20 ({nx}x{ny}, N={nx * ny}), "
+            f"{len(f)} freqs {f[0]:g}-{f[-1]:g} Hz x {W['nshots']} shots, {W['nx0'] - 1} receivers, AC")
 
 
 def workload(seed: int = 2024):
     from germaine_b200.synthetic import line_acquisition, thrust_model
-    vp, rho = thrust_model(NX0, NY0, DH, NPML, seed=seed)
-    xs, ys, rx, ry = line_acquisition(NX0, DH, NSHOTS, ROW)
+    vp, rho = thrust_model(W["nx0"], W["ny0"], DH, NPML, seed=seed)
+    xs, ys, rx, ry = line_acquisition(W["nx0"], DH, W["nshots"], ROW)
     return vp, rho, xs, ys, rx, ry
 
 
@@ -58,11 +70,12 @@ def workload(seed: int = 2024):
 def _cpu_one_frequency(args):
     """One process of the CPU reference path: assemble (reference sources),
     SuperLU factorisation of M = A^T, all shots of the frequency."""
-    freq, nshots, seed = args
+    freq, nshots, seed, dims = args
+    W.update(dims)
     import oracle as O
     from oracle import sparse as OS
     vp, rho, xs, ys, rx, ry = workload(seed)
-    g = O.Grid(nx=NX0 + 2 * NPML, ny=NY0 + 2 * NPML, dh=DH, npml=NPML)
+    g = O.Grid(nx=W["nx0"] + 2 * NPML, ny=W["ny0"] + 2 * NPML, dh=DH, npml=NPML)
     asm = O.Ref(g) if O.ref_available() else O.Port(g)
     t0 = time.perf_counter()
     trip = asm.assemble(1, freq, vp, rho)
@@ -74,11 +87,13 @@ def _cpu_one_frequency(args):
     return time.perf_counter() - t0
 
 
-def cpu_reference_step(nproc: int, nshots: int = NSHOTS, seed: int = 2024):
+def cpu_reference_step(nproc: int, nshots: int | None = None, seed: int = 2024):
     """One bounded sample: nproc processes, each one frequency with nshots
     shots.  Returns (shot-solves/s, wall seconds, frequencies done)."""
+    nshots = nshots or W["nshots"]
     ctx = mp.get_context("spawn")
-    freqs = [FREQS[i % len(FREQS)] for i in range(nproc)]
+    fl = freqs_hz()
+    freqs = [fl[i % len(fl)] for i in range(nproc)]
     # one BLAS thread per process: each process is one "rank" of the
     # reference's MPI layout (and several multi-threaded OpenBLAS pools in
     # sibling processes oversubscribe the cores)
@@ -88,7 +103,7 @@ def cpu_reference_step(nproc: int, nshots: int = NSHOTS, seed: int = 2024):
     try:
         t0 = time.perf_counter()
         with ctx.Pool(nproc) as pool:
-            pool.map(_cpu_one_frequency, [(f, nshots, seed) for f in freqs])
+            pool.map(_cpu_one_frequency, [(f, nshots, seed, dict(W)) for f in freqs])
         wall = time.perf_counter() - t0
     finally:
         for k, v in saved.items():
@@ -101,7 +116,7 @@ def cpu_reference_step(nproc: int, nshots: int = NSHOTS, seed: int = 2024):
 
 def cpu_procs() -> int:
     n = os.cpu_count() or 1
-    return max(1, min(n, len(FREQS)))
+    return max(1, min(n, W["nfreq"]))
 
 
 # ----------------------------------------------------------------- clocks
@@ -217,13 +232,13 @@ def run_gpu(args):
         nproc = cpu_procs()
         rate, wall, nfq = cpu_reference_step(nproc)
         cpu = {"value": rate, "unit": "shot-solves/s", "cores": nproc, "kind": "port",
-               "sample": f"{nfq} frequencies x {NSHOTS} shots of the same workload, one process per frequency "
+               "sample": f"{nfq} frequencies x {W['nshots']} shots of the same workload, one process per frequency "
                          f"(reference assembly + SciPy SuperLU standing in for UMFPACK), wall {wall:.1f} s"}
 
     vp, rho, xs, ys, rx, ry = workload(args.seed + rank)
-    nx, ny = NX0 + 2 * NPML, NY0 + 2 * NPML
-    freqs = np.array(FREQS, np.float32)
-    nf, ns, ntr = len(FREQS), NSHOTS, rx.size
+    nx, ny = W["nx0"] + 2 * NPML, W["ny0"] + 2 * NPML
+    freqs = np.array(freqs_hz(), np.float32)
+    nf, ns, ntr = len(freqs), W["nshots"], rx.size
     dev = torch.device("cuda", local)
     vp_d = torch.from_numpy(vp.reshape(-1)).to(dev)
     rho_d = torch.from_numpy(rho.reshape(-1)).to(dev)
@@ -283,7 +298,7 @@ def run_gpu(args):
         "vs_baseline": None,
         "dtype": "c64 fronts + f64 refinement",
         "data": "synthetic (seeded thrust model; no public dataset)",
-        "config": {"workload": WORKLOAD, "frequencies": nf, "shots_per_frequency": ns, "receivers": ntr,
+        "config": {"workload": workload_name(), "frequencies": nf, "shots_per_frequency": ns, "receivers": ntr,
                    "residual_target": 1e-10, "l2": "inputs larger than L2 (fronts 4-8 GB per step)",
                    "parallelism": f"replicas{world}" if world > 1 else "single"},
         "e2e": {"value": units / (mixed["ms_e2e"] * 1e-3), "unit": "shot-solves/s",
@@ -317,7 +332,7 @@ def run_reference(args):
         return
     nproc = cpu_procs()
     for _ in range(args.warmup):
-        cpu_reference_step(nproc, nshots=min(NSHOTS, 10))
+        cpu_reference_step(nproc, nshots=min(W["nshots"], 10))
     rates, walls = [], []
     for _ in range(args.steps):
         r, w, _ = cpu_reference_step(nproc)
@@ -329,10 +344,10 @@ def run_reference(args):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": float(np.median(walls)) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "c128",
         "data": "synthetic (seeded thrust model; no public dataset)",
-        "config": {"workload": WORKLOAD, "frequencies_per_step": nproc, "shots_per_frequency": NSHOTS},
+        "config": {"workload": workload_name(), "frequencies_per_step": nproc, "shots_per_frequency": W["nshots"]},
         "impl": "reference",
         "cpu_baseline": {"value": value, "unit": "shot-solves/s", "cores": nproc, "kind": "port",
-                         "sample": f"{nproc} frequencies x {NSHOTS} shots per step, one process per frequency "
+                         "sample": f"{nproc} frequencies x {W['nshots']} shots per step, one process per frequency "
                                    "(reference assembly + SciPy SuperLU standing in for UMFPACK)"},
         "e2e": {"value": value, "unit": "shot-solves/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -348,7 +363,12 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--leaf", type=int, default=64)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--nx0", type=int, default=W["nx0"], help="model width without PML (profiling cases)")
+    ap.add_argument("--ny0", type=int, default=W["ny0"], help="model depth without PML (profiling cases)")
+    ap.add_argument("--nfreq", type=int, default=W["nfreq"], help="frequencies 2, 3, ... Hz (profiling cases)")
+    ap.add_argument("--nshots", type=int, default=W["nshots"], help="shots per frequency (profiling cases)")
     args = ap.parse_args()
+    W.update(nx0=args.nx0, ny0=args.ny0, nfreq=args.nfreq, nshots=args.nshots)
     if args.impl == "reference":
         run_reference(args)
     else:

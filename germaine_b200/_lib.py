@@ -11,6 +11,7 @@ import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libgermaine_gpu.so")
+UMFPACK_LIB_PATH = os.path.join(HERE, "libgermaine_umfpack.so")
 
 GM_OK = 0
 GM_WARNING_PERTURBED = 1
@@ -53,11 +54,20 @@ class GmStats(ctypes.Structure):
 # every C-ABI symbol declared in include/germaine_gpu.h
 EXPORTS = [
     "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats", "gm_engine_stream",
-    "gm_set_model", "gm_factor", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
+    "gm_set_model", "gm_factor", "gm_factor_values", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
     "gm_get_gradient_fp64", "gm_solve_noalloc", "gm_cgemm_sub_c64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
 ]
+
+# every symbol declared in include/germaine_umfpack.h (libgermaine_umfpack.so)
+UMFPACK_EXPORTS = [
+    "umfpack_zi_triplet_to_col", "umfpack_zi_symbolic", "umfpack_zi_numeric", "umfpack_zi_solve",
+    "umfpack_zi_free_symbolic", "umfpack_zi_free_numeric", "gm_umfpack_last_error",
+]
+UMFPACK_A, UMFPACK_At, UMFPACK_Aat = 0, 1, 2
+UMFPACK_OK, UMFPACK_WARNING_singular_matrix = 0, 1
+UMFPACK_ERROR_invalid_matrix, UMFPACK_ERROR_different_pattern, UMFPACK_ERROR_invalid_system = -8, -11, -13
 
 _lib = None
 
@@ -87,6 +97,7 @@ def load() -> ctypes.CDLL:
     lib.gm_engine_stream.argtypes = [vp, ctypes.POINTER(vp)]
     lib.gm_set_model.argtypes = [vp, vp, vp]
     lib.gm_factor.argtypes = [vp, i32, vp]
+    lib.gm_factor_values.argtypes = [vp, i32, vp, vp]
     lib.gm_get_triplets.argtypes = [vp, i32, vp, vp, vp, vp]
     lib.gm_solve.argtypes = [vp, i32, i32, vp, vp]
     lib.gm_forward.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, vp]
@@ -102,6 +113,32 @@ def load() -> ctypes.CDLL:
     lib.gm_symbolic_flops.argtypes = [vp, i32]
     lib.gm_symbolic_flops.restype = f64
     _lib = lib
+    return lib
+
+
+_umf = None
+
+
+def load_umfpack() -> ctypes.CDLL:
+    """Load the in-tree UMFPACK-API shim (raises if it was not built)."""
+    global _umf
+    if _umf is not None:
+        return _umf
+    load()
+    if not os.path.exists(UMFPACK_LIB_PATH):
+        raise RuntimeError(f"{UMFPACK_LIB_PATH} is missing: build it with `python germaine_b200/build.py`")
+    lib = ctypes.CDLL(UMFPACK_LIB_PATH)
+    vp, i32 = ctypes.c_void_p, ctypes.c_int
+    lib.umfpack_zi_triplet_to_col.argtypes = [i32, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.umfpack_zi_symbolic.argtypes = [i32, i32, vp, vp, vp, vp, ctypes.POINTER(vp), vp, vp]
+    lib.umfpack_zi_numeric.argtypes = [vp, vp, vp, vp, vp, ctypes.POINTER(vp), vp, vp]
+    lib.umfpack_zi_solve.argtypes = [i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.umfpack_zi_free_symbolic.argtypes = [ctypes.POINTER(vp)]
+    lib.umfpack_zi_free_symbolic.restype = None
+    lib.umfpack_zi_free_numeric.argtypes = [ctypes.POINTER(vp)]
+    lib.umfpack_zi_free_numeric.restype = None
+    lib.gm_umfpack_last_error.restype = ctypes.c_char_p
+    _umf = lib
     return lib
 
 

@@ -1,4 +1,6 @@
-"""In-tree build of libgermaine_gpu.so (sm_100a) -- the product library.
+"""In-tree build of libgermaine_gpu.so (sm_100a) -- the product library --
+and of libgermaine_umfpack.so, the UMFPACK-API shim over it (host C++ only,
+csrc/umfpack/).
 
 CUDA sources are compiled by nvcc for ``-gencode arch=compute_100a,code=sm_100a``
 with ``-lineinfo``; C++ host sources by nvcc's host compiler; the C host
@@ -21,6 +23,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 BUILD = os.path.join(HERE, "_build")
 LIB = os.path.join(HERE, "libgermaine_gpu.so")
+UMF_LIB = os.path.join(HERE, "libgermaine_umfpack.so")
 INCLUDE = os.path.join(os.path.dirname(HERE), "include")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
@@ -80,7 +83,22 @@ def build(verbose: bool = False, jobs: int = 8) -> str:
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"link failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
+    _build_umfpack_shim(hdr_time, verbose)
     return LIB
+
+
+def _build_umfpack_shim(hdr_time: float, verbose: bool) -> None:
+    srcs = sorted(glob.glob(os.path.join(CSRC, "umfpack", "*.cpp")))
+    newest = max([hdr_time, os.path.getmtime(LIB)] + [os.path.getmtime(s) for s in srcs])
+    if os.path.exists(UMF_LIB) and os.path.getmtime(UMF_LIB) >= newest:
+        return
+    cmd = ["g++", "-O2", "-std=c++17", "-fPIC", "-Wall", "-shared", "-I", INCLUDE, *srcs, "-o", UMF_LIB,
+           "-L", HERE, "-lgermaine_gpu", "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        raise RuntimeError(f"shim build failed: {' '.join(cmd)}\n{r.stdout}\n{r.stderr}")
 
 
 if __name__ == "__main__":

@@ -303,7 +303,7 @@ static int build_cb_plan(gm_engine *e) {
 }
 
 template <class R>
-static int factor_batch(gm_engine *e, R pivtol) {
+static int factor_batch(gm_engine *e, double pivscale) {
     FactorArgs<R> a{};
     a.s = e->dsym;
     a.front = e->d_front.p;
@@ -311,7 +311,8 @@ static int factor_batch(gm_engine *e, R pivtol) {
     a.ent_dst = e->d_ent_dst.as<int64_t>();
     a.ent_src = e->d_ent_src.as<int>();
     a.nf = e->nf;
-    a.pivtol = pivtol;
+    a.amax = e->d_amax.as<unsigned long long>();
+    a.pivscale = pivscale;
     a.npert = e->d_npert.as<unsigned long long>();
     if (e->cb_plan_base != e->d_front.p || e->cb_plan_nf != e->nf) {
         const int rc = build_cb_plan<R>(e);
@@ -335,6 +336,40 @@ static int factor_batch(gm_engine *e, R pivtol) {
 
 }  // namespace gm
 
+namespace gm {
+
+// Numeric factorisation of the nf operators in e->d_A (assembled or given
+// by value).  The static-pivot threshold is relative to max |A| over the
+// whole batch, reduced on the device.
+static int factor_assembled(gm_engine *e) {
+    const bool fp64 = e->cfg.precision == GM_PREC_FP64;
+    const size_t fbytes = (size_t)e->nf * e->sym.front_total * e->csize();
+    GM_ALLOC(e->d_front, fbytes);
+    GM_ALLOC(e->d_npert, sizeof(unsigned long long));
+    GM_ALLOC(e->d_amax, sizeof(unsigned long long));
+    GM_CUDA(cudaEventRecord(e->ev0, e->st));
+    GM_CUDA(cudaMemsetAsync(e->d_npert.p, 0, sizeof(unsigned long long), e->st));
+    GM_CUDA(cudaMemsetAsync(e->d_amax.p, 0, sizeof(unsigned long long), e->st));
+    launch_amax(e->d_A.as<double2>(), (size_t)e->nf * 9 * e->n, e->d_amax.as<unsigned long long>(), e->st);
+    const int rc = fp64 ? factor_batch<double>(e, 1e-13) : factor_batch<float>(e, 1e-6);
+    if (rc) return rc;
+    GM_CUDA(cudaEventRecord(e->ev1, e->st));
+    GM_CUDA(cudaEventSynchronize(e->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    e->stats.ms_factor = ms;
+    unsigned long long np = 0;
+    GM_CUDA(cudaMemcpy(&np, e->d_npert.p, sizeof np, cudaMemcpyDeviceToHost));
+    int tcerr = 0;
+    GM_CUDA(cudaMemcpy(&tcerr, e->d_tcerr.p, sizeof tcerr, cudaMemcpyDeviceToHost));
+    if (tcerr) return fail(GM_ERROR_CUDA, "factor: a tensor-core wait timed out in the contribution-block update");
+    e->stats.perturbed_pivots = (int64_t)np;
+    e->factored = true;
+    return np ? GM_WARNING_PERTURBED : GM_OK;
+}
+
+}  // namespace gm
+
 extern "C" int gm_factor(gm_engine *e, int nfreq, const float *h_freqs) {
     if (!e || nfreq <= 0 || !h_freqs) return fail(GM_ERROR_INVALID, "gm_factor: bad argument");
     if (!e->have_model) return fail(GM_ERROR_STATE, "gm_factor: no model set (gm_set_model)");
@@ -342,6 +377,7 @@ extern "C" int gm_factor(gm_engine *e, int nfreq, const float *h_freqs) {
         if (!(h_freqs[f] > 0.f) || !std::isfinite(h_freqs[f])) return fail(GM_ERROR_INVALID, "frequency %d is not positive", f);
     GM_CUDA(cudaSetDevice(e->device));
     e->factored = false;
+    e->values_only = false;
     e->nf = nfreq;
     e->freqs.assign(h_freqs, h_freqs + nfreq);
 
@@ -353,43 +389,31 @@ extern "C" int gm_factor(gm_engine *e, int nfreq, const float *h_freqs) {
     float ms = 0;
     cudaEventElapsedTime(&ms, e->ev0, e->ev1);
     e->stats.ms_assemble = ms;
+    return gm::factor_assembled(e);
+}
 
-    // static-pivot threshold relative to the largest operator entry
-    std::vector<double2> tmp;
-    double amax = 0;
-    {
-        // centre coefficients dominate the stencil; sample all nine directions of a few rows per frequency
-        const int n = e->n;
-        tmp.resize(9);
-        const int rows[3] = {n / 2, n / 3, (2 * n) / 3};
-        for (int f = 0; f < nfreq; ++f)
-            for (int r : rows) {
-                for (int q = 0; q < 9; ++q)
-                    GM_CUDA(cudaMemcpy(&tmp[q], e->d_A.as<double2>() + (size_t)f * 9 * n + (size_t)q * n + r, sizeof(double2),
-                                       cudaMemcpyDeviceToHost));
-                for (int q = 0; q < 9; ++q) amax = std::max(amax, std::hypot(tmp[q].x, tmp[q].y));
-            }
-    }
-    const bool fp64 = e->cfg.precision == GM_PREC_FP64;
-    const size_t fbytes = (size_t)nfreq * e->sym.front_total * e->csize();
-    GM_ALLOC(e->d_front, fbytes);
-    GM_ALLOC(e->d_npert, sizeof(unsigned long long));
-    GM_CUDA(cudaMemsetAsync(e->d_npert.p, 0, sizeof(unsigned long long), e->st));
+extern "C" int gm_factor_values(gm_engine *e, int nmat, const double *re, const double *im) {
+    if (!e || nmat <= 0 || !re || !im) return fail(GM_ERROR_INVALID, "gm_factor_values: bad argument");
+    GM_CUDA(cudaSetDevice(e->device));
+    e->factored = false;
+    e->values_only = true;
+    e->nf = nmat;
+    e->freqs.assign(nmat, 0.f);
+    const size_t cnt = (size_t)nmat * 9 * e->n;
+    GM_ALLOC(e->d_A, cnt * sizeof(double2));
+    // split inputs staged in the (grow-only) residual workspace
+    GM_ALLOC(e->d_r, 2 * cnt * sizeof(double));
+    double *dre = e->d_r.as<double>(), *dim = dre + cnt;
     GM_CUDA(cudaEventRecord(e->ev0, e->st));
-    rc = fp64 ? gm::factor_batch<double>(e, 1e-13 * amax) : gm::factor_batch<float>(e, (float)(1e-6 * amax));
-    if (rc) return rc;
+    GM_CUDA(cudaMemcpyAsync(dre, re, cnt * sizeof(double), cudaMemcpyDefault, e->st));
+    GM_CUDA(cudaMemcpyAsync(dim, im, cnt * sizeof(double), cudaMemcpyDefault, e->st));
+    gm::launch_pack_split(e->d_A.as<double2>(), dre, dim, cnt, e->st);
     GM_CUDA(cudaEventRecord(e->ev1, e->st));
     GM_CUDA(cudaEventSynchronize(e->ev1));
+    float ms = 0;
     cudaEventElapsedTime(&ms, e->ev0, e->ev1);
-    e->stats.ms_factor = ms;
-    unsigned long long np = 0;
-    GM_CUDA(cudaMemcpy(&np, e->d_npert.p, sizeof np, cudaMemcpyDeviceToHost));
-    int tcerr = 0;
-    GM_CUDA(cudaMemcpy(&tcerr, e->d_tcerr.p, sizeof tcerr, cudaMemcpyDeviceToHost));
-    if (tcerr) return fail(GM_ERROR_CUDA, "gm_factor: a tensor-core wait timed out in the contribution-block update");
-    e->stats.perturbed_pivots = (int64_t)np;
-    e->factored = true;
-    return np ? GM_WARNING_PERTURBED : GM_OK;
+    e->stats.ms_assemble = ms;
+    return gm::factor_assembled(e);
 }
 
 extern "C" int gm_get_triplets(gm_engine *e, int ifreq, double *Ar, double *Ai, int32_t *irow, int32_t *icol) {
@@ -502,7 +526,18 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
             e->stats.ir_residual = NAN;
             return fail(GM_ERROR_NONFINITE, "non-finite residual after %d refinement sweeps", it);
         }
-        if (std::getenv("GM_TRACE_REFINEMENT")) std::fprintf(stderr, "refinement sweep %d: max relative residual %.3e\n", it, worst);
+        if (std::getenv("GM_TRACE_REFINEMENT")) {
+            std::fprintf(stderr, "refinement sweep %d: max relative residual %.3e; per frequency", it, worst);
+            for (int f = 0; f < e->nf; ++f) {
+                double wf = 0;
+                for (int r = 0; r < nrhs; ++r) {
+                    const double rr = norms[2 * (f * nrhs + r)], bb = norms[2 * (f * nrhs + r) + 1];
+                    wf = std::max(wf, bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr));
+                }
+                std::fprintf(stderr, " %.1e", wf);
+            }
+            std::fprintf(stderr, "\n");
+        }
         if (worst <= e->cfg.ir_tol || it >= e->cfg.ir_max_iter) break;
         if (fp64) substitute<double>(e, e->d_t.p, nrhs, sys);
         else substitute<float>(e, e->d_t.p, nrhs, sys);

@@ -61,8 +61,9 @@ struct gm_engine {
     // factorisation of the current frequency batch
     int nf = 0;
     std::vector<float> freqs;
-    gm::DevBuf d_A, d_mass, d_pml, d_fq, d_front, d_npert;
+    gm::DevBuf d_A, d_mass, d_pml, d_fq, d_front, d_npert, d_amax;
     bool factored = false;
+    bool values_only = false;   // operator given by gm_factor_values (no frequencies / model)
 
     // contribution-block GEMM plan per level (rebuilt when the front
     // storage moves or the batch size changes)

@@ -98,6 +98,8 @@ int forward_solve(gm_engine *e, int ns, const Geometry &g, double2 *xout) {
 int check_ready(const gm_engine *e, int ns, int ntr) {
     if (!e) return fail(GM_ERROR_INVALID, "null engine");
     if (!e->factored) return fail(GM_ERROR_STATE, "no factorisation (call gm_factor first)");
+    if (e->values_only)
+        return fail(GM_ERROR_STATE, "the factors come from gm_factor_values: no frequencies or model to model shots with");
     if (ns <= 0 || ntr < 0) return fail(GM_ERROR_INVALID, "need at least one shot (nshots=%d, ntr=%d)", ns, ntr);
     return GM_OK;
 }

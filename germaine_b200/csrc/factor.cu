@@ -130,7 +130,7 @@ __global__ void __launch_bounds__(PCHUNK) k_panel(FactorArgs<R> a, int lvl_first
         D[r][c] = F[(k0 + r) + (size_t)(k0 + c) * f];
     }
     __syncthreads();
-    diag_lu<R>(D, rdiag, kb, a.pivtol, &npert);
+    diag_lu<R>(D, rdiag, kb, (R)(a.pivscale * __longlong_as_double((long long)*a.amax)), &npert);
 
     if (bx < nchunk) {
         // L panel: row i solves x U = a  (U = upper triangle of D incl. diagonal)
@@ -205,7 +205,7 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
             D[r][c] = F[(k0 + r) + (size_t)(k0 + c) * f];
         }
         __syncthreads();
-        diag_lu<R>(D, rdiag, kb, a.pivtol, &npert);
+        diag_lu<R>(D, rdiag, kb, (R)(a.pivscale * __longlong_as_double((long long)*a.amax)), &npert);
         // The substitution only needs the inverses of the block's triangles:
         // store L^-1 (strict lower part; unit diagonal implied) and U^-1
         // (upper part with diagonal) in place of L and U.  Thread c < kb
@@ -383,5 +383,33 @@ void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
 
 template void launch_factor_level<double>(const FactorArgs<double> &, const LevelInfo &, cudaStream_t);
 template void launch_factor_level<float>(const FactorArgs<float> &, const LevelInfo &, cudaStream_t);
+
+// Grid-stride max of |A| with one atomicMax per warp.  Non-negative doubles
+// order like their bit patterns read as unsigned integers.
+__global__ void __launch_bounds__(256) k_amax(const double2 *A, size_t cnt, unsigned long long *out) {
+    double m = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x) {
+        const double2 v = A[i];
+        const double a = hypot(v.x, v.y);
+        m = a > m ? a : m;   // NaN entries are skipped here; they surface as non-finite factors
+    }
+    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
+}
+
+void launch_amax(const double2 *A, size_t cnt, unsigned long long *out, cudaStream_t st) {
+    note_launch();
+    k_amax<<<148 * 8, 256, 0, st>>>(A, cnt, out);
+}
+
+__global__ void k_pack_split(double2 *dst, const double *re, const double *im, size_t cnt) {
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x)
+        dst[i] = make_double2(re[i], im[i]);
+}
+
+void launch_pack_split(double2 *dst, const double *re, const double *im, size_t cnt, cudaStream_t st) {
+    note_launch();
+    k_pack_split<<<148 * 8, 256, 0, st>>>(dst, re, im, cnt);
+}
 
 }  // namespace gm

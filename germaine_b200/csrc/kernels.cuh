@@ -60,12 +60,23 @@ struct FactorArgs {
     const int64_t *ent_dst;   // per entry: front_off + position
     const int *ent_src;       // per entry: q*n + k into A (operator orientation applied)
     int nf;
-    R pivtol;                 // |pivot| below this is replaced (static pivoting)
+    // static pivoting: |pivot| below pivscale * max|A| is replaced; max|A|
+    // is a device scalar (bits of a non-negative double) written by
+    // launch_amax, so the threshold never round-trips through the host
+    const unsigned long long *amax;
+    double pivscale;
     unsigned long long *npert;  // perturbed-pivot counter
 };
 
+// max |A| over cnt complex entries into *out (bits of a double; *out must
+// be zeroed first)
+void launch_amax(const double2 *A, size_t cnt, unsigned long long *out, cudaStream_t st);
+// dst[i] = (re[i], im[i])
+void launch_pack_split(double2 *dst, const double *re, const double *im, size_t cnt, cudaStream_t st);
+
 template <class R>
 void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st);
+
 
 // one dense product C -= A * B (column-major, complex<R>)
 template <class R>
@@ -86,7 +97,7 @@ struct SolveArgs {
     DevSym s;
     const void *front;        // cplx<R> factors [nf][front_total]
     void *x;                  // cplx<R> [nf][n][ldr], rhs in, solution out
-    void *w;                  // cplx<R> [nf][rhs_total][ldr] front-vector workspace
+    void *w;                  // cplx<R> [nf][rhs_total][ldr] update vectors (ring rows)
     int nf, nrhs, ldr;
     int rch;                  // right-hand sides per CTA (<= 32)
     int trans;                // 0: M x = b, 1: M^T x = b

@@ -83,18 +83,20 @@ void launch_reduce_norms(const double *part, int nblk, int cnt, double *out, cud
 }
 
 template <class R>
-__global__ void k_convert_down(const double2 *src, cplx<R> *dst, size_t count) {
+__global__ void k_convert_down(const double2 *__restrict__ src, cplx<R> *__restrict__ dst, size_t count) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < count) dst[i] = cconv<cplx<R>>(src[i]);
 }
 
 template <class R>
-__global__ void k_add_up(double2 *x, const cplx<R> *d, size_t count) {
+__global__ void k_add_up(double2 *__restrict__ x, const cplx<R> *__restrict__ d, size_t count) {
     const size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < count) {
         const double2 v = cto_d(d[i]);
-        x[i].x += v.x;
-        x[i].y += v.y;
+        double2 u = x[i];
+        u.x += v.x;
+        u.y += v.y;
+        x[i] = u;
     }
 }
 

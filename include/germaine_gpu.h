@@ -113,6 +113,19 @@ int gm_set_model(gm_engine *e, const float *mat0, const float *mat1);
  * Returns GM_WARNING_PERTURBED if static pivots had to be replaced. */
 int gm_factor(gm_engine *e, int nfreq, const float *h_freqs);
 
+/* Factorise nmat operators given by value instead of assembled from a model:
+ * umfpack_zi_numeric (src/AC/forward_shot_AC.c:61) on matrices that arrive
+ * as numbers (the UMFPACK shim, libgermaine_umfpack.so, calls this).
+ * re/im are [nmat][9][NX*NY] doubles, direction-major in the stencil order
+ * NW, N, NE, W, C, E, SW, S, SE (direction q = (di+1) + 3*(dj+1)):
+ * entry [m][q][c] is the coefficient that couples grid point c with its
+ * neighbour c + di + dj*NX, read in the engine's op_mode -- under GM_OP_REF
+ * it is M[c + di + dj*NX][c] (column c of the factorised matrix M), under
+ * GM_OP_EXACT M[c][c + di + dj*NX].  Entries whose neighbour lies outside
+ * the grid are ignored.  Afterwards gm_solve works as after gm_factor;
+ * gm_forward, gm_grad_obj and gm_obj return GM_ERROR_STATE (no model). */
+int gm_factor_values(gm_engine *e, int nmat, const double *re, const double *im);
+
 /* Copy the assembled matrix of frequency ifreq out in the reference's
  * triplet layout (row-major, ascending columns; waveAC.Ar/Ai/irow/icol of
  * src/AC/init_A_AC_9p_pml.c:75-80).  Any of the four outputs may be NULL. */

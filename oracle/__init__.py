@@ -12,7 +12,12 @@ Two CPU implementations live here:
   residual and gradient arithmetic, bit-faithful in float/double;
 * ``ref``   -- oracle/_ref/libgermaine_ref.so, the reference's own C sources
   compiled in place by oracle/Makefile (only where the reference tree is
-  present; the built library travels with the repository snapshot).
+  present; the built library travels with the repository snapshot);
+* ``dropin`` -- oracle/_ref/libgermaine_ref_dropin.so, the reference's
+  unmodified drivers forward_shot_AC / grad_obj_AC linked against the
+  product's UMFPACK shim (libgermaine_umfpack.so): not a checker but the
+  object under test of tests/test_gpu_dropin.py, run against the checkers
+  above.
 
 The sparse direct solve (UMFPACK in the reference, an un-vendored
 SuiteSparse dependency with no pinned version) is restated with SciPy's
@@ -30,6 +35,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 PORT_SO = os.path.join(HERE, "liboracle_port.so")
 REF_SO = os.path.join(HERE, "_ref", "libgermaine_ref.so")
+DROPIN_SO = os.path.join(HERE, "_ref", "libgermaine_ref_dropin.so")
 
 PHYS_AC, PHYS_SH, PHYS_TE = 1, 2, 4
 
@@ -277,3 +283,46 @@ class Ref:
 
     def cp_grad_frame(self, grad):
         self.lib.ref_cp_grad_frame(grad)
+
+
+def dropin_available() -> bool:
+    return os.path.exists(DROPIN_SO)
+
+
+class RefDropin:
+    """The reference's own drivers running their UMFPACK calls on the GPU
+    (oracle/ref_dropin.c).  Holds process-global reference state."""
+
+    def __init__(self, g: Grid):
+        if not dropin_available():
+            raise RuntimeError(f"{DROPIN_SO} missing: run `make -C oracle dropin` where the reference tree exists")
+        self.g = g
+        lib = ctypes.CDLL(DROPIN_SO)
+        lib.ref_set_grid.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_float, ctypes.c_int, ctypes.c_int,
+                                     ctypes.c_float, ctypes.c_float]
+        lib.dropin_forward_shot_ac.argtypes = [ctypes.c_float, _f32p, _f32p, ctypes.c_int, _f32p, _f32p, ctypes.c_int,
+                                               _i32p, _i32p, _f32p, _f32p]
+        lib.dropin_grad_obj_ac.argtypes = [ctypes.c_int, _f32p, _f32p, _f32p, ctypes.c_int, _f32p, _f32p, ctypes.c_int,
+                                           _i32p, _i32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int, _f32p]
+        lib.dropin_grad_obj_ac.restype = ctypes.c_float
+        self.lib = lib
+        lib.ref_set_grid(g.nx, g.ny, g.dh, g.npml, g.free_surf, g.a0_pml, g.s)
+
+    def forward_shot_ac(self, freq, vp, rho, xs, ys, rx, ry):
+        """Seismograms [nshots][ntr] complex64 of forward_shot_AC."""
+        ns, ntr = len(xs), len(rx)
+        sr = np.zeros(ns * ntr, np.float32); si = np.zeros(ns * ntr, np.float32)
+        self.lib.dropin_forward_shot_ac(freq, _f32(vp).ravel(), _f32(rho).ravel(), ns, _f32(xs), _f32(ys), ntr,
+                                        np.ascontiguousarray(rx, np.int32), np.ascontiguousarray(ry, np.int32), sr, si)
+        return (sr + 1j * si).reshape(ns, ntr).astype(np.complex64)
+
+    def grad_obj_ac(self, freqs, vp, rho, xs, ys, rx, ry, obs, stf_inv=0, misfit=1):
+        """(gradient [NY][NX] float32, L2) of grad_obj_AC over one stage."""
+        nf, ns, ntr = len(freqs), len(xs), len(rx)
+        obs = np.asarray(obs, np.complex64).reshape(nf, ns, ntr)
+        grad = np.zeros(self.g.n, np.float32)
+        l2 = self.lib.dropin_grad_obj_ac(nf, _f32(freqs), _f32(vp).ravel(), _f32(rho).ravel(), ns, _f32(xs),
+                                         _f32(ys), ntr, np.ascontiguousarray(rx, np.int32),
+                                         np.ascontiguousarray(ry, np.int32), _f32(obs.real).ravel(),
+                                         _f32(obs.imag).ravel(), stf_inv, misfit, grad)
+        return grad.reshape(self.g.ny, self.g.nx), float(l2)

@@ -1,5 +1,6 @@
-"""The C-ABI library loads without a GPU and exports every function that
-include/*.h declares; the engine refuses to run without a device."""
+"""The C-ABI libraries load without a GPU and export every function that
+include/*.h declares (germaine_gpu.h: libgermaine_gpu.so, germaine_umfpack.h:
+libgermaine_umfpack.so); the engine refuses to run without a device."""
 import ctypes
 import glob
 import os
@@ -12,9 +13,15 @@ from germaine_b200 import _lib
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
-def declared_functions():
+HEADER_LIB = {"germaine_gpu.h": (_lib.load, _lib.LIB_PATH, _lib.EXPORTS),
+              "germaine_umfpack.h": (_lib.load_umfpack, _lib.UMFPACK_LIB_PATH, _lib.UMFPACK_EXPORTS)}
+
+
+def declared_functions(header=None):
     names = set()
     for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        if header is not None and os.path.basename(h) != header:
+            continue
         text = re.sub(r"/\*.*?\*/", "", open(h).read(), flags=re.S)
         for m in re.finditer(r"^\s*(?:const\s+)?[A-Za-z_][\w\s\*]*?\b(\w+)\s*\(", text, flags=re.M):
             name = m.group(1)
@@ -25,18 +32,25 @@ def declared_functions():
 
 def test_header_declares_something():
     names = declared_functions()
-    assert "gm_factor" in names and "gm_solve" in names
+    assert "gm_factor" in names and "gm_solve" in names and "umfpack_zi_numeric" in names
 
 
-@pytest.mark.parametrize("name", declared_functions())
-def test_symbol_exported(name):
-    lib = _lib.load()
-    assert hasattr(lib, name), f"{name} declared in include/ but not exported by {_lib.LIB_PATH}"
+def test_every_header_has_a_library():
+    headers = {os.path.basename(h) for h in glob.glob(os.path.join(ROOT, "include", "*.h"))}
+    assert headers == set(HEADER_LIB)
 
 
-def test_python_binding_lists_every_symbol():
-    missing = set(declared_functions()) - set(_lib.EXPORTS)
-    assert not missing, f"declared but not bound in germaine_b200/_lib.py: {sorted(missing)}" 
+@pytest.mark.parametrize("header,name", [(h, n) for h in sorted(HEADER_LIB) for n in declared_functions(h)])
+def test_symbol_exported(header, name):
+    load, path, _ = HEADER_LIB[header]
+    lib = load()
+    assert hasattr(lib, name), f"{name} declared in include/{header} but not exported by {path}"
+
+
+@pytest.mark.parametrize("header", sorted(HEADER_LIB))
+def test_python_binding_lists_every_symbol(header):
+    missing = set(declared_functions(header)) - set(HEADER_LIB[header][2])
+    assert not missing, f"declared but not bound in germaine_b200/_lib.py: {sorted(missing)}"
 
 
 def test_no_device_no_cpu_path():
