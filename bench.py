@@ -279,12 +279,17 @@ def run_gpu(args):
     units = nf * ns * world
     value = units / (mixed["ms"] * 1e-3)
     st = mixed["stats"]
-    # roofline of the substitution (K5): factor entries read once per
-    # substitution + right-hand sides read and written, complex64
+    # roofline of the substitution (K5, the dominant kernel group): factor
+    # entries read once per substitution + right-hand sides read and
+    # written, complex64, over the device time of one substitution
     csize = 8
     subst_bytes = nf * (st["factor_entries"] * csize + 2 * st["n"] * ns * csize)
     subst_ms = st["ms_subst"] / max(1, st["n_subst"])
     achieved = subst_bytes / (subst_ms * 1e-3) / 1e9
+    # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
+    # complex64 substitution from an ncu capture of the first 50 K5 launches
+    # of this workload on 4 frequencies (9.697 GB), scaled by frequency count
+    traffic = 9.697e9 / 4 * nf if (W["nx0"], W["ny0"], W["nshots"], args.leaf) == (801, 187, 100, 64) else None
     line = {
         "metric": METRIC,
         "value": value,
@@ -313,9 +318,10 @@ def run_gpu(args):
                      "refine": st["ms_refine"], "substitutions": st["ms_subst"], "n_subst": st["n_subst"]},
         "roofline": {"kernel": "K5 multi-RHS substitution (k_fwd + k_bwd, complex64)", "bound": "hbm",
                      "achieved": achieved, "peak": peak_hbm, "unit": "GB/s", "frac": achieved / peak_hbm,
-                     "peak_kind": peak_kind, "traffic": None,
+                     "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": subst_bytes, "ms_per_launch_group": subst_ms},
-        "gpu_launches": mixed["launches"],
+        "gpu_launches": mixed["launches"] * args.steps,
+        "gpu_launches_per_step": mixed["launches"],
         "clocks": mixed["clocks"],
         "cpu_baseline": cpu,
     }
