@@ -1,0 +1,147 @@
+"""Frequency sharding with one gradient all-reduce (germaine_b200/sharding.py):
+the rank shares follow init_MPIfreq (src/init_MPIfreq.c:20-31), and the
+sharded misfit / FP64 gradient over gloo ranks on CPU equals the
+single-process result.  The per-rank evaluation in the CPU tests is the FP64
+oracle (SuperLU + FP64 restatements); on the GPU it is the engine, with the
+all-reduce over NCCL."""
+import os
+import socket
+import tempfile
+
+import numpy as np
+import pytest
+
+from germaine_b200.sharding import frequency_range, local_frequencies, sharded_grad_obj
+
+
+def init_mpifreq(nf, nprocfreq, myid_shot):
+    """NFREQ1, NFREQ2 (1-based, half-open) as src/init_MPIfreq.c:20-31 computes them."""
+    nfreq1 = (nf // nprocfreq) * myid_shot
+    if nf % nprocfreq > myid_shot:
+        nfreq1 += myid_shot
+        nfreq2 = nfreq1 + nf // nprocfreq + 1
+    else:
+        nfreq1 += nf % nprocfreq
+        nfreq2 = nfreq1 + nf // nprocfreq
+    return nfreq1 + 1, nfreq2 + 1
+
+
+@pytest.mark.parametrize("nf", [1, 2, 3, 7, 10, 16, 32])
+@pytest.mark.parametrize("nproc", [1, 2, 3, 4, 8])
+def test_frequency_range_is_init_mpifreq(nf, nproc):
+    seen = []
+    for rank in range(nproc):
+        lo, hi = frequency_range(nf, nproc, rank)
+        n1, n2 = init_mpifreq(nf, nproc, rank)
+        assert (lo, hi) == (n1 - 1, n2 - 1)
+        seen += list(range(lo, hi))
+    assert seen == list(range(nf))
+
+
+def test_frequency_range_rejects_bad_rank():
+    with pytest.raises(ValueError):
+        frequency_range(4, 2, 2)
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _case():
+    from tests.models import inclusion_ac, random_smooth
+    import oracle as O
+    nx, ny, dh, npml = 40, 30, 10.0, 6
+    vp, rho = inclusion_ac(nx, ny, dh, npml, radius=50.0)
+    vp = vp * random_smooth(nx, ny, 0.9, 1.1, 4)
+    g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml)
+    nx0 = nx - 2 * npml
+    xs = np.linspace(2 * dh, (nx0 - 3) * dh, 3).astype(np.float32)
+    ys = np.full(3, 3 * dh, np.float32)
+    rx = np.arange(1, nx0 - 1, dtype=np.int32)
+    ry = np.full(rx.size, 3, np.int32)
+    freqs = [6.0, 9.0, 13.0]
+    return g, vp, rho, xs, ys, rx, ry, freqs
+
+
+def _oracle_local(g, vp, rho, xs, ys, rx, ry, obs_by_freq):
+    from tests.test_gpu_forward_grad import oracle_grad
+
+    def run(local):
+        if not local:
+            return np.zeros(g.n), None, 0.0
+        obs = np.stack([obs_by_freq[f] for f in local])
+        g0, _, l2 = oracle_grad(g, 1, vp, rho, local, xs, ys, rx, ry, obs, 0, 1)
+        return g0, None, l2
+    return run
+
+
+def _observed(g, vp, rho, xs, ys, rx, ry, freqs):
+    from tests.test_gpu_forward_grad import _observed as obs_fn
+    obs = obs_fn(g, 1, vp, rho, freqs, xs, ys, rx, ry)
+    return {f: obs[i] for i, f in enumerate(freqs)}
+
+
+def _worker(rank, world, port, out_dir):
+    import torch.distributed as dist
+    import datetime
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        g, vp, rho, xs, ys, rx, ry, freqs = _case()
+        obs = _observed(g, vp, rho, xs, ys, rx, ry, freqs)
+        g0, _, l2 = sharded_grad_obj(freqs, _oracle_local(g, vp, rho, xs, ys, rx, ry, obs), dist)
+        np.save(os.path.join(out_dir, f"g{rank}.npy"), np.append(g0, l2))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_sharded_gradient_gloo_equals_single_process(world):
+    """world 2: shares of 2 and 1 frequencies; world 4: one rank has none."""
+    import torch.multiprocessing as tmp
+    with tempfile.TemporaryDirectory() as d:
+        tmp.spawn(_worker, args=(world, _free_port(), d), nprocs=world, join=True)
+        res = [np.load(os.path.join(d, f"g{r}.npy")) for r in range(world)]
+    g, vp, rho, xs, ys, rx, ry, freqs = _case()
+    obs = _observed(g, vp, rho, xs, ys, rx, ry, freqs)
+    g_all, _, l2_all = _oracle_local(g, vp, rho, xs, ys, rx, ry, obs)(freqs)
+    for r in res:   # every rank holds the same total
+        assert np.array_equal(r, res[0])
+    assert np.linalg.norm(res[0][:-1] - g_all) <= 1e-12 * np.linalg.norm(g_all)
+    assert abs(res[0][-1] - l2_all) <= 1e-12 * abs(l2_all)
+
+
+def test_local_frequencies_slices():
+    f = [2.0, 3.0, 4.0, 5.0, 6.0]
+    assert local_frequencies(f, 2, 0) == [2.0, 3.0, 4.0]
+    assert local_frequencies(f, 2, 1) == [5.0, 6.0]
+    assert local_frequencies(f, 8, 7) == []
+
+
+@pytest.mark.gpu
+def test_sharded_engine_gradient_over_nccl():
+    """One rank over NCCL on cuda:0: the all-reduce of the engine's FP64
+    gradient (device buffer) returns it unchanged and equals the oracle."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from germaine_b200 import Engine
+    from germaine_b200.sharding import engine_grad_obj
+    g, vp, rho, xs, ys, rx, ry, freqs = _case()
+    obs = _observed(g, vp, rho, xs, ys, rx, ry, freqs)
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(_free_port())
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        with Engine(g.nx, g.ny, g.dh, g.npml, leaf_max=32) as e:
+            e.set_model(vp, rho)
+            g0, _, l2 = sharded_grad_obj(freqs, engine_grad_obj(e, xs, ys, rx, ry, obs), dist,
+                                         device=torch.device("cuda", 0))
+    finally:
+        dist.destroy_process_group()
+    r0, _, rl2 = _oracle_local(g, vp, rho, xs, ys, rx, ry, obs)(freqs)
+    assert np.linalg.norm(g0 - r0) <= 1e-8 * np.linalg.norm(r0)
+    assert abs(l2 - rl2) <= 2e-6 * abs(rl2)
