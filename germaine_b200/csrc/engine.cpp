@@ -106,6 +106,7 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
     // level-ordered entry lists in the configured operator orientation
     std::vector<int64_t> ent_dst;
     std::vector<int> ent_src;
+    std::vector<int64_t> ent_lvl_off(s.nnodes + 1, 0);
     ent_dst.reserve(s.ent_pos.size());
     ent_src.reserve(s.ent_pos.size());
     e->levels.resize(s.nlevels);
@@ -123,6 +124,7 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
         L.ent_first = (int64_t)ent_dst.size();
         for (int t = L.first; t < L.first + L.count; ++t) {
             const int v = s.lvl_nodes[t];
+            ent_lvl_off[t] = (int64_t)ent_dst.size();
             for (int64_t q = s.ent_off[v]; q < s.ent_off[v + 1]; ++q) {
                 ent_dst.push_back(s.front_off[v] + s.ent_pos[q]);
                 int id = s.ent_id[q];
@@ -136,6 +138,7 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
         }
         L.ent_count = (int64_t)ent_dst.size() - L.ent_first;
     }
+    ent_lvl_off[s.nnodes] = (int64_t)ent_dst.size();
     int rc2;
     if ((rc2 = upload(e->d_npiv, s.npiv, e->st)) || (rc2 = upload(e->d_nfront, s.nfront, e->st)) ||
         (rc2 = upload(e->d_child0, s.child0, e->st)) || (rc2 = upload(e->d_child1, s.child1, e->st)) ||
@@ -143,7 +146,7 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
         (rc2 = upload(e->d_lvl_nodes, s.lvl_nodes, e->st)) || (rc2 = upload(e->d_front_off, s.front_off, e->st)) ||
         (rc2 = upload(e->d_var_off, s.var_off, e->st)) || (rc2 = upload(e->d_inv_off, s.inv_off, e->st)) ||
         (rc2 = upload(e->d_rhs_off, s.rhs_off, e->st)) || (rc2 = upload(e->d_ent_dst, ent_dst, e->st)) ||
-        (rc2 = upload(e->d_ent_src, ent_src, e->st)))
+        (rc2 = upload(e->d_ent_src, ent_src, e->st)) || (rc2 = upload(e->d_ent_lvl_off, ent_lvl_off, e->st)))
         return rc2;
     GM_CUDA(cudaStreamSynchronize(e->st));
     gm::DevSym &d = e->dsym;
@@ -275,6 +278,10 @@ static int build_cb_plan(gm_engine *e) {
         pl.backend = backend;
         pl.prob_off = (int64_t)probs.size();
         pl.tile_off = (int64_t)tiles.size();
+        if (small_factor_level<R>(L)) {   // fused small-front kernel forms the Schur complement itself
+            pl.ntiles = 0;
+            continue;
+        }
         for (int f = 0; f < e->nf; ++f)
             for (int t = L.first; t < L.first + L.count; ++t) {
                 const int v = s.lvl_nodes[t];
@@ -310,6 +317,7 @@ static int factor_batch(gm_engine *e, double pivscale) {
     a.A = e->d_A.as<double2>();
     a.ent_dst = e->d_ent_dst.as<int64_t>();
     a.ent_src = e->d_ent_src.as<int>();
+    a.ent_lvl_off = e->d_ent_lvl_off.as<int64_t>();
     a.nf = e->nf;
     a.amax = e->d_amax.as<unsigned long long>();
     a.pivscale = pivscale;
@@ -322,6 +330,10 @@ static int factor_batch(gm_engine *e, double pivscale) {
     const GemmProb<R> *probs = e->d_cb_probs.as<GemmProb<R>>();
     const int4 *tiles = e->d_cb_tiles.as<int4>();
     for (size_t h = 0; h < e->levels.size(); ++h) {
+        if (small_factor_level<R>(e->levels[h])) {
+            launch_factor_small<R>(a, e->levels[h], e->st);
+            continue;
+        }
         launch_factor_level<R>(a, e->levels[h], e->st);
         const auto &pl = e->cb_plan[h];
         if (pl.backend == 1)

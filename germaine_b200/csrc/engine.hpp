@@ -50,7 +50,7 @@ struct gm_engine {
     // device copy of the symbolic structure
     gm::DevBuf d_npiv, d_nfront, d_child0, d_child1, d_vars, d_inv, d_lvl_nodes;
     gm::DevBuf d_front_off, d_var_off, d_inv_off, d_rhs_off;
-    gm::DevBuf d_ent_dst, d_ent_src;
+    gm::DevBuf d_ent_dst, d_ent_src, d_ent_lvl_off;
     std::vector<gm::LevelInfo> levels;
     gm::DevSym dsym{};
 

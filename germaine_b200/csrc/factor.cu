@@ -384,6 +384,163 @@ void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
 template void launch_factor_level<double>(const FactorArgs<double> &, const LevelInfo &, cudaStream_t);
 template void launch_factor_level<float>(const FactorArgs<float> &, const LevelInfo &, cudaStream_t);
 
+// ---------------------------------------------------------------------
+// Small fronts (the lower levels of the tree): one CTA assembles and
+// factorises a whole front in shared memory -- extend-add of the children's
+// contribution blocks, the operator entries, right-looking LU of the npiv
+// pivot columns with the same static pivoting as diag_lu, the Schur
+// complement of the contribution block, and the inverses of the NB x NB
+// diagonal blocks -- and writes the front back once.  The result has the
+// layout the blocked path leaves (L below, U above, diagonal-block inverses,
+// contribution block), in one launch per level instead of the
+// gather / scatter / ceil(npiv/NB) x (panel + update) / contribution GEMM
+// sequence.  S[i + j * ld] holds front entry (i, j).
+// ---------------------------------------------------------------------
+constexpr int SMALL_FT = 256;   // threads per CTA
+
+template <class R>
+__global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int lvl_first, int ld) {
+    using C = cplx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C *S = reinterpret_cast<C *>(smem_raw);
+    __shared__ C Dinv[NB][NB + 1];
+    __shared__ int npert;
+    const int pos = lvl_first + blockIdx.x;
+    const int node = a.s.lvl_nodes[pos];
+    const int f = a.s.nfront[node], s = a.s.npiv[node];
+    C *rd = S + (size_t)ld * f;   // reciprocal pivots
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = SMALL_FT / 32;
+    const size_t fz = blockIdx.y;
+    C *base = reinterpret_cast<C *>(a.front) + fz * a.s.front_total;
+    C *F = base + a.s.front_off[node];
+
+    // extend-add of the children's contribution blocks (zero for leaves)
+    const int *inv = a.s.inv + a.s.inv_off[node];
+    const int c0 = a.s.child0[node], c1 = a.s.child1[node];
+    const C *cb0 = nullptr, *cb1 = nullptr;
+    int f0 = 0, f1 = 0;
+    if (c0 >= 0) { const int s0 = a.s.npiv[c0]; f0 = a.s.nfront[c0]; cb0 = base + a.s.front_off[c0] + s0 + (size_t)s0 * f0; }
+    if (c1 >= 0) { const int s1 = a.s.npiv[c1]; f1 = a.s.nfront[c1]; cb1 = base + a.s.front_off[c1] + s1 + (size_t)s1 * f1; }
+    for (int j = warp; j < f; j += nw) {
+        const int j0 = cb0 ? inv[j] : -1, j1 = cb1 ? inv[f + j] : -1;
+        for (int i = lane; i < f; i += 32) {
+            C v = czero<C>();
+            if (j0 >= 0) { const int r = inv[i]; if (r >= 0) v = cadd(v, cb0[r + (size_t)j0 * f0]); }
+            if (j1 >= 0) { const int r = inv[f + i]; if (r >= 0) v = cadd(v, cb1[r + (size_t)j1 * f1]); }
+            S[i + j * ld] = v;
+        }
+    }
+    if (tid == 0) npert = 0;
+    __syncthreads();
+    // operator entries owned by the front (positions are distinct)
+    {
+        const int64_t e0 = a.ent_lvl_off[pos], e1 = a.ent_lvl_off[pos + 1];
+        const int64_t fo = a.s.front_off[node];
+        const double2 *A = a.A + fz * 9 * (size_t)a.s.n;
+        for (int64_t e = e0 + tid; e < e1; e += SMALL_FT) {
+            const int p = (int)(a.ent_dst[e] - fo);
+            const int i = p % f, j = p / f;
+            C &d = S[i + j * ld];
+            d = cadd(d, cconv<C>(A[a.ent_src[e]]));
+        }
+    }
+    __syncthreads();
+
+    // right-looking LU of the pivot columns; the trailing update covers the
+    // contribution block too (its Schur complement)
+    const R pivtol = (R)(a.pivscale * __longlong_as_double((long long)*a.amax));
+    for (int k = 0; k < s; ++k) {
+        if (tid == 0) {
+            C piv = S[k + k * ld];
+            const R mag = sqrt(cabs2(piv));
+            if (!(mag >= pivtol)) {   // also catches NaN
+                if (mag > R(0)) {
+                    const R sc = pivtol / mag;
+                    piv = mk(piv.x * sc, piv.y * sc);
+                } else {
+                    piv = mk(pivtol, R(0));
+                }
+                S[k + k * ld] = piv;
+                ++npert;
+            }
+            rd[k] = crcp(piv);
+        }
+        __syncthreads();
+        const C rk = rd[k];
+        for (int i = k + 1 + tid; i < f; i += SMALL_FT) S[i + k * ld] = cmul(S[i + k * ld], rk);
+        __syncthreads();
+        const int m = f - k - 1;
+        for (int jj = warp; jj < m; jj += nw) {
+            C *col = S + (k + 1 + jj) * ld;
+            const C u = col[k];
+            for (int ii = lane; ii < m; ii += 32) cfms(col[k + 1 + ii], S[k + 1 + ii + k * ld], u);
+        }
+        __syncthreads();
+    }
+
+    // inverses of the NB x NB diagonal blocks: L^-1 strictly below the
+    // diagonal (unit diagonal implied), U^-1 on and above it
+    for (int k0 = 0; k0 < s; k0 += NB) {
+        const int kb = min(NB, s - k0);
+        auto D = [&](int r, int q) { return S[(k0 + r) + (k0 + q) * ld]; };
+        if (tid < kb) {
+            const int c = tid;
+            for (int r = c + 1; r < kb; ++r) {
+                C acc = D(r, c);
+                for (int q = c + 1; q < r; ++q) cfma(acc, D(r, q), Dinv[q][c]);
+                Dinv[r][c] = mk(-acc.x, -acc.y);
+            }
+        } else if (tid >= 32 && tid < 32 + kb) {
+            const int c = tid - 32;
+            Dinv[c][c] = rd[k0 + c];
+            for (int r = c - 1; r >= 0; --r) {
+                C acc = czero<C>();
+                for (int q = r + 1; q <= c; ++q) cfma(acc, D(r, q), Dinv[q][c]);
+                Dinv[r][c] = cmul(mk(-acc.x, -acc.y), rd[k0 + r]);
+            }
+        }
+        __syncthreads();
+        for (int t = tid; t < kb * kb; t += SMALL_FT) {
+            const int r = t % kb, c = t / kb;
+            S[(k0 + r) + (k0 + c) * ld] = Dinv[r][c];
+        }
+        __syncthreads();
+    }
+
+    for (int j = warp; j < f; j += nw)
+        for (int i = lane; i < f; i += 32) F[i + (size_t)j * f] = S[i + j * ld];
+    if (tid == 0 && npert) atomicAdd(a.npert, (unsigned long long)npert);
+}
+
+constexpr size_t SMALL_FACTOR_SMEM = 100 << 10;
+
+template <class R>
+static size_t small_factor_smem(int fmax) {
+    const int ld = fmax + 1;
+    return ((size_t)ld * fmax + fmax) * sizeof(cplx<R>);
+}
+
+template <class R>
+bool small_factor_level(const LevelInfo &L) {
+    return L.count > 0 && small_factor_smem<R>(L.max_front) <= SMALL_FACTOR_SMEM;
+}
+
+template <class R>
+void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_factor_small<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
+        attr_set = true;
+    }
+    const size_t smem = small_factor_smem<R>(L.max_front);
+    (k_factor_small<R><<<dim3(L.count, a.nf), SMALL_FT, smem, st>>>(a, L.first, L.max_front + 1), note_launch());
+}
+
+template bool small_factor_level<double>(const LevelInfo &);
+template bool small_factor_level<float>(const LevelInfo &);
+template void launch_factor_small<double>(const FactorArgs<double> &, const LevelInfo &, cudaStream_t);
+template void launch_factor_small<float>(const FactorArgs<float> &, const LevelInfo &, cudaStream_t);
+
 // Grid-stride max of |A| with one atomicMax per warp.  Non-negative doubles
 // order like their bit patterns read as unsigned integers.
 __global__ void __launch_bounds__(256) k_amax(const double2 *A, size_t cnt, unsigned long long *out) {

@@ -66,6 +66,8 @@ struct FactorArgs {
     const unsigned long long *amax;
     double pivscale;
     unsigned long long *npert;  // perturbed-pivot counter
+    const int64_t *ent_lvl_off; // entries of level position t (index into lvl_nodes):
+                                // ent_dst/ent_src[ent_lvl_off[t] .. ent_lvl_off[t + 1])
 };
 
 // max |A| over cnt complex entries into *out (bits of a double; *out must
@@ -76,6 +78,13 @@ void launch_pack_split(double2 *dst, const double *re, const double *im, size_t 
 
 template <class R>
 void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st);
+// Small fronts: the whole front of every node of the level assembled and
+// factorised in shared memory by one CTA (replaces launch_factor_level and
+// the level's contribution-block GEMM) when small_factor_level(L).
+template <class R>
+bool small_factor_level(const LevelInfo &L);
+template <class R>
+void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st);
 
 
 // one dense product C -= A * B (column-major, complex<R>)
