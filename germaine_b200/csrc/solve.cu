@@ -15,12 +15,12 @@
 // update vector for its parent (its ring rows).  Per elimination-tree level:
 //   forward  (leaves -> root)
 //     k_fwd_piv   add the children's update vectors (by the extend-add
-//                 inverse maps) into x at the pivots and into the front's own
-//                 update vector at the ring rows, then per 32-pivot block:
+//                 inverse maps) into x at the pivots, then per 32-pivot block:
 //                 y_b = L_bb^-1 x_b, x_rest -= L_rb y_b over the remaining
 //                 pivot rows;
-//     k_fwd_ring  w_ring -= L_ring,piv * y over 64-row tiles of the ring
-//                 (many CTAs per front: the wide part of the level);
+//     k_fwd_ring  w_ring = (children's update vectors at the ring rows)
+//                 - L_ring,piv * y over 64-row tiles of the ring (many CTAs
+//                 per front: the wide part of the level);
 //   backward (root -> leaves)
 //     k_bwd_ring  x_piv -= U_piv,ring * x_ring (x_ring = final values of the
 //                 ancestors' variables), 64-row tiles of the pivot rows;
@@ -52,18 +52,21 @@ __device__ __forceinline__ C elem(const C *F, int f, int i, int c) {
     return TRANS ? F[c + (size_t)i * f] : F[i + (size_t)c * f];
 }
 
-// sm.L[q][row] = M'(i0 + row, c0 + q) for row < rows, q < qb; zeros elsewhere
+// sm.L[q][row] = M'(i0 + row, c0 + q) for row < rows, q < qb.  Entries
+// outside are left as they are: tile_mma reads only q < qb, and rows >= rows
+// (or right-hand sides >= rn) only feed accumulators that are never stored,
+// so partial tiles stage only what they use.
 template <class C, bool TRANS>
 __device__ __forceinline__ void stage_factor(SolveSmem<C> &sm, const C *F, int f, int i0, int rows, int c0, int qb) {
     if (!TRANS) {
-        for (int t = threadIdx.x; t < RT * SNB; t += NT) {
+        for (int t = threadIdx.x; t < RT * qb; t += NT) {
             const int row = t % RT, q = t / RT;
-            sm.L[q][row] = (row < rows && q < qb) ? F[(i0 + row) + (size_t)(c0 + q) * f] : czero<C>();
+            if (row < rows) sm.L[q][row] = F[(i0 + row) + (size_t)(c0 + q) * f];
         }
     } else {
-        for (int t = threadIdx.x; t < RT * SNB; t += NT) {
+        for (int t = threadIdx.x; t < SNB * rows; t += NT) {
             const int q = t % SNB, row = t / SNB;
-            sm.L[q][row] = (row < rows && q < qb) ? F[(c0 + q) + (size_t)(i0 + row) * f] : czero<C>();
+            if (q < qb) sm.L[q][row] = F[(c0 + q) + (size_t)(i0 + row) * f];
         }
     }
 }
@@ -75,18 +78,17 @@ __device__ __forceinline__ void stage_factor(SolveSmem<C> &sm, const C *F, int f
 // implied) and U^-1 on and above it.
 template <class C, bool FWD, bool TRANS>
 __device__ __forceinline__ void stage_dinv(SolveSmem<C> &sm, const C *F, int f, int k0, int kb) {
-    for (int t = threadIdx.x; t < SNB * SNB; t += NT) {
-        const int p = t % SNB, q = t / SNB;   // operator entry (p, q) -> sm.L[q][p]
+    for (int t = threadIdx.x; t < SNB * kb; t += NT) {
+        const int p = t % SNB, q = t / SNB;   // operator entry (p, q) -> sm.L[q][p], q < kb
+        if (p >= kb) continue;
         C v = czero<C>();
-        if (p < kb && q < kb) {
-            const bool lower_src = FWD != TRANS;         // L^-1 (or its transpose) wanted
-            const int r = TRANS ? q : p, c = TRANS ? p : q;  // position in the stored block
-            if (lower_src) {
-                if (r > c) v = F[(k0 + r) + (size_t)(k0 + c) * f];
-                else if (r == c) v = mk(decltype(v.x)(1), decltype(v.x)(0));
-            } else if (r <= c) {
-                v = F[(k0 + r) + (size_t)(k0 + c) * f];
-            }
+        const bool lower_src = FWD != TRANS;         // L^-1 (or its transpose) wanted
+        const int r = TRANS ? q : p, c = TRANS ? p : q;  // position in the stored block
+        if (lower_src) {
+            if (r > c) v = F[(k0 + r) + (size_t)(k0 + c) * f];
+            else if (r == c) v = mk(decltype(v.x)(1), decltype(v.x)(0));
+        } else if (r <= c) {
+            v = F[(k0 + r) + (size_t)(k0 + c) * f];
         }
         sm.L[q][p] = v;
     }
@@ -103,13 +105,14 @@ __device__ __forceinline__ void tile_mma(const SolveSmem<C> &sm, int qb, C (&acc
     const int wrow = (threadIdx.x >> 5) * 4;
     const int na = rows <= wrow ? 0 : min(4, (rows - wrow + 15) / 16);
     const int nb = min(4, (rn + 7) / 8);
+    if (na == 0) return;   // warp-uniform: this warp owns no row of the tile
 #pragma unroll 2
     for (int q = 0; q < qb; ++q) {
         C l[4], y[4];
 #pragma unroll
-        for (int a = 0; a < 4; ++a) l[a] = sm.L[q][tr + 16 * a];
+        for (int a = 0; a < 4; ++a) l[a] = a < na ? sm.L[q][tr + 16 * a] : czero<C>();
 #pragma unroll
-        for (int b = 0; b < 4; ++b) y[b] = sm.Y[q][tc + 8 * b];
+        for (int b = 0; b < 4; ++b) y[b] = b < nb ? sm.Y[q][tc + 8 * b] : czero<C>();
 #pragma unroll
         for (int a = 0; a < 4; ++a) {
             if (a >= na) break;
@@ -144,12 +147,12 @@ __device__ __forceinline__ void sub_acc(RowPtr row_ptr, int rows, int rn, const 
     }
 }
 
-// sm.Y[q][r] = row_ptr(q)[r] for q < qb, r < rn; zeros elsewhere
+// sm.Y[q][r] = row_ptr(q)[r] for q < qb, r < rn (entries outside: as above)
 template <class C, class RowPtr>
 __device__ __forceinline__ void stage_rows(SolveSmem<C> &sm, RowPtr row_ptr, int qb, int rn) {
-    for (int t = threadIdx.x; t < SNB * TC; t += NT) {
+    for (int t = threadIdx.x; t < qb * TC; t += NT) {
         const int q = t / TC, r = t % TC;
-        sm.Y[q][r] = (q < qb && r < rn) ? row_ptr(q)[r] : czero<C>();
+        if (r < rn) sm.Y[q][r] = row_ptr(q)[r];
     }
 }
 
@@ -181,9 +184,8 @@ __device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first,
 }
 
 // Forward pass, pivot part: add the children's update vectors (gathered by
-// the extend-add inverse maps) into x at this front's pivots and into this
-// front's own update vector at its ring rows, then solve the pivot rows in
-// place in x, 32-pivot block by block.
+// the extend-add inverse maps) into x at this front's pivots, then solve the
+// pivot rows in place in x, 32-pivot block by block.
 template <class R, bool TRANS>
 __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, int fused) {
     using C = cplx<R>;
@@ -202,22 +204,19 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
     const C *W1 = c1 >= 0 ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
     const size_t ldr = a.ldr;
 
-    for (int i = warp; i < c.f; i += NT / 32) {
-        if (lane >= c.rn) continue;
-        const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
-        C v = czero<C>();
-        if (q0 >= 0) v = cadd(v, W0[(size_t)q0 * ldr + lane]);
-        if (q1 >= 0) v = cadd(v, W1[(size_t)q1 * ldr + lane]);
-        if (i < c.s) {
-            if (q0 >= 0 || q1 >= 0) {
-                C &x = c.X[(size_t)c.vars[i] * ldr + lane];
-                x = cadd(x, v);
-            }
-        } else {
-            c.W[(size_t)(i - c.s) * ldr + lane] = v;
+    if (W0 || W1) {   // children's update vectors at the pivots (the ring part is k_fwd_ring's)
+        for (int i = warp; i < c.s; i += NT / 32) {
+            if (lane >= c.rn) continue;
+            const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
+            if (q0 < 0 && q1 < 0) continue;
+            C v = czero<C>();
+            if (q0 >= 0) v = cadd(v, W0[(size_t)q0 * ldr + lane]);
+            if (q1 >= 0) v = cadd(v, W1[(size_t)q1 * ldr + lane]);
+            C &x = c.X[(size_t)c.vars[i] * ldr + lane];
+            x = cadd(x, v);
         }
+        __syncthreads();
     }
-    __syncthreads();
 
     auto xrow = [&](int k) { return c.X + (size_t)c.vars[k] * ldr; };
     C acc[4][4];
@@ -253,8 +252,9 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
     }
 }
 
-// Forward pass, ring part: update vector -= L'(ring, pivots) y, 64-row tiles
-// of the ring over many CTAs; blockIdx.x = chunk + nchunk * tile
+// Forward pass, ring part: update vector = children's update vectors at the
+// ring rows - L'(ring, pivots) y, 64-row tiles of the ring over many CTAs;
+// blockIdx.x = chunk + nchunk * tile
 template <class R, bool TRANS>
 __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, int nchunk) {
     using C = cplx<R>;
@@ -277,7 +277,29 @@ __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, 
         tile_mma(sm, qb, acc, tr, tc, rows, c.rn);
         __syncthreads();
     }
-    sub_acc([&](int row) { return c.W + (size_t)(i0 - c.s + row) * ldr; }, rows, c.rn, acc, tr, tc);
+    // w = (children's update vectors at the ring rows) - L'(ring, piv) y
+    const int *inv = a.s.inv + a.s.inv_off[c.node];
+    const C *Wall = reinterpret_cast<const C *>(a.w) + (size_t)blockIdx.z * a.s.rhs_total * a.ldr + chunk * TC;
+    const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
+    const C *W0 = c0 >= 0 ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
+    const C *W1 = c1 >= 0 ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
+#pragma unroll
+    for (int p = 0; p < 4; ++p) {
+        const int row = tr + 16 * p;
+        if (row >= rows) continue;
+        const int i = i0 + row;
+        const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
+        C *w = c.W + (size_t)(i - c.s) * ldr;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int r = tc + 8 * b;
+            if (r >= c.rn) continue;
+            C g = czero<C>();
+            if (q0 >= 0) g = cadd(g, W0[(size_t)q0 * ldr + r]);
+            if (q1 >= 0) g = cadd(g, W1[(size_t)q1 * ldr + r]);
+            w[r] = csub(g, acc[p][b]);
+        }
+    }
 }
 
 // Backward pass, ring part: x[pivots] -= U'(pivots, ring) x[ring]
