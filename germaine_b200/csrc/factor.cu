@@ -447,10 +447,13 @@ __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int 
     __syncthreads();
 
     // right-looking LU of the pivot columns; the trailing update covers the
-    // contribution block too (its Schur complement)
+    // contribution block too (its Schur complement).  Warp 0 updates column
+    // k + 1 first in step k, so it can take the next pivot (static pivoting
+    // as in diag_lu) and scale the next L column while the other warps are
+    // still updating: one barrier per pivot.
     const R pivtol = (R)(a.pivscale * __longlong_as_double((long long)*a.amax));
-    for (int k = 0; k < s; ++k) {
-        if (tid == 0) {
+    auto take_pivot = [&](int k) {   // warp 0 only: pivot k, reciprocal, L column k scaled
+        if (lane == 0) {
             C piv = S[k + k * ld];
             const R mag = sqrt(cabs2(piv));
             if (!(mag >= pivtol)) {   // also catches NaN
@@ -465,15 +468,23 @@ __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int 
             }
             rd[k] = crcp(piv);
         }
-        __syncthreads();
+        __syncwarp();
         const C rk = rd[k];
-        for (int i = k + 1 + tid; i < f; i += SMALL_FT) S[i + k * ld] = cmul(S[i + k * ld], rk);
-        __syncthreads();
+        for (int i = k + 1 + lane; i < f; i += 32) S[i + k * ld] = cmul(S[i + k * ld], rk);
+        __syncwarp();
+    };
+    if (warp == 0 && s > 0) take_pivot(0);
+    __syncthreads();
+    for (int k = 0; k < s; ++k) {
         const int m = f - k - 1;
         for (int jj = warp; jj < m; jj += nw) {
             C *col = S + (k + 1 + jj) * ld;
             const C u = col[k];
             for (int ii = lane; ii < m; ii += 32) cfms(col[k + 1 + ii], S[k + 1 + ii + k * ld], u);
+            if (jj == 0 && k + 1 < s) {   // warp 0 just finished column k + 1
+                __syncwarp();
+                take_pivot(k + 1);
+            }
         }
         __syncthreads();
     }
