@@ -7,13 +7,18 @@ One step = assemble + factorise all 10 frequencies + solve all 100 shots of
 every frequency (1,000 shot-solves) with FP64 iterative refinement to a
 relative residual <= 1e-10, and gather the seismograms.
 
-  value  -- mixed precision (complex64 fronts + FP64 refinement), inputs and
-            outputs resident in HBM, device time from CUDA events on the
-            engine's stream;
-  e2e    -- the same step through the public C-ABI with host buffers: the
-            model is copied in from pinned host memory and the seismograms
-            copied back every step, inside the timed region;
-  fp64   -- the plain FP64 drop-in path, same step, for the mixed/FP64 ratio.
+Both paths are run on the same step:
+  fp64   -- the drop-in: complex128 fronts and substitution, one FP64
+            residual check (refinement only if it is above the target);
+  mixed  -- complex64 fronts and substitution with FP64 iterative
+            refinement (residual and update in FP64) to the same target.
+
+  value  -- the faster of the two (config.path names it), inputs and outputs
+            resident in HBM, device time from CUDA events on the engine's
+            stream; `paths` reports both, `mixed_over_fp64` their ratio;
+  e2e    -- the same path and step through the public C-ABI with host
+            buffers: the model is copied in from pinned host memory and the
+            seismograms copied back every step, inside the timed region.
 
 `--impl reference` times the reference's CPU path on the host cores: the
 reference's own assembly (oracle/_ref, else the C restatement) and SciPy
@@ -42,6 +47,9 @@ sys.path.insert(0, ROOT)
 
 DH, NPML, ROW = 25.0, 20, 2
 METRIC = "shot-solves/s (factor+solve) mixed vs FP64 on B200 at resid<=1e-10; %roofline"
+# DRAM bytes of one complex128 substitution on 4 frequencies (first 50 K5
+# launches of the FP64 engine, ncu dram__bytes_read.sum + write.sum)
+SUBST_TRAFFIC_FP64_4FREQ = 15.221e9
 
 # the benchmark workload; --nx0/--ny0/--nfreq/--nshots shrink it for
 # profiling captures (the bench line then names the smaller workload)
@@ -263,13 +271,13 @@ def run_gpu(args):
         ck = clocks.stop()
         st = e.stats()
         r = {"ms": ms, "launches": launches, "stats": st, "clocks": ck}
-        if name == "mixed":
-            def step_e2e():
-                e.set_model(vp_h, rho_h)
-                e.factor(freqs)
-                e.forward(xs, ys, rx, ry, seis_out=seis_h)
-            ms_e2e, _ = time_steps(torch, e, step_e2e, max(1, args.steps // 2), 1, dist)
-            r["ms_e2e"] = ms_e2e
+
+        def step_e2e():
+            e.set_model(vp_h, rho_h)
+            e.factor(freqs)
+            e.forward(xs, ys, rx, ry, seis_out=seis_h)
+        ms_e2e, _ = time_steps(torch, e, step_e2e, max(1, args.steps // 2), 1, dist)
+        r["ms_e2e"] = ms_e2e
         results[name] = r
         e.close()
         del e
@@ -277,19 +285,25 @@ def run_gpu(args):
 
     mixed, fp64 = results["mixed"], results["fp64"]
     units = nf * ns * world
-    value = units / (mixed["ms"] * 1e-3)
-    st = mixed["stats"]
+    # headline: the faster of the two paths (both refine to the residual
+    # target); the other is reported beside it
+    head_name = "fp64" if fp64["ms"] <= mixed["ms"] else "mixed"
+    head = results[head_name]
+    value = units / (head["ms"] * 1e-3)
+    st = head["stats"]
     # roofline of the substitution (K5, the dominant kernel group): factor
     # entries read once per substitution + right-hand sides read and
-    # written, complex64, over the device time of one substitution
-    csize = 8
+    # written, over the device time of one substitution
+    csize = 16 if head_name == "fp64" else 8
     subst_bytes = nf * (st["factor_entries"] * csize + 2 * st["n"] * ns * csize)
     subst_ms = st["ms_subst"] / max(1, st["n_subst"])
     achieved = subst_bytes / (subst_ms * 1e-3) / 1e9
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
-    # complex64 substitution from an ncu capture of the first 50 K5 launches
-    # of this workload on 4 frequencies (9.697 GB), scaled by frequency count
-    traffic = 9.697e9 / 4 * nf if (W["nx0"], W["ny0"], W["nshots"], args.leaf) == (801, 187, 100, 64) else None
+    # substitution from ncu captures of this workload on 4 frequencies (the
+    # first 50 K5 launches of each engine), scaled by frequency count
+    per4 = {"mixed": 9.697e9, "fp64": SUBST_TRAFFIC_FP64_4FREQ}[head_name]
+    traffic = (per4 / 4 * nf if per4 and (W["nx0"], W["ny0"], W["nshots"], args.leaf) == (801, 187, 100, 64)
+               else None)
     line = {
         "metric": METRIC,
         "value": value,
@@ -297,32 +311,39 @@ def run_gpu(args):
         "n_gpus": world,
         "steps": args.steps,
         "warmup": args.warmup,
-        "ms_per_step": mixed["ms"],
+        "ms_per_step": head["ms"],
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
-        "dtype": "c64 fronts + f64 refinement",
+        "dtype": "c128" if head_name == "fp64" else "c64 fronts + f64 refinement",
         "data": "synthetic (seeded thrust model; no public dataset)",
         "config": {"workload": workload_name(), "frequencies": nf, "shots_per_frequency": ns, "receivers": ntr,
+                   "path": {"fp64": "FP64 drop-in (complex128 factors and substitution, FP64 residual check)",
+                            "mixed": "complex64 factors + FP64 iterative refinement"}[head_name],
                    "residual_target": 1e-10, "l2": "inputs larger than L2 (fronts 4-8 GB per step)",
                    "parallelism": f"replicas{world}" if world > 1 else "single"},
-        "e2e": {"value": units / (mixed["ms_e2e"] * 1e-3), "unit": "shot-solves/s",
+        "e2e": {"value": units / (head["ms_e2e"] * 1e-3), "unit": "shot-solves/s",
                 "h2d_bytes_per_step": int(2 * vp.size * 4), "d2h_bytes_per_step": int(nf * ns * ntr * 8)},
-        "fp64": {"value": units / (fp64["ms"] * 1e-3), "ms_per_step": fp64["ms"],
-                 "ir_iterations": fp64["stats"]["ir_iterations"], "ir_residual": fp64["stats"]["ir_residual"]},
+        "paths": {n: {"value": units / (results[n]["ms"] * 1e-3), "ms_per_step": results[n]["ms"],
+                      "e2e_value": units / (results[n]["ms_e2e"] * 1e-3),
+                      "ir_iterations": results[n]["stats"]["ir_iterations"],
+                      "ir_residual": results[n]["stats"]["ir_residual"],
+                      "perturbed_pivots": results[n]["stats"]["perturbed_pivots"],
+                      "phase_ms": {"assemble": results[n]["stats"]["ms_assemble"],
+                                   "factor": results[n]["stats"]["ms_factor"],
+                                   "solve": results[n]["stats"]["ms_solve"],
+                                   "refine": results[n]["stats"]["ms_refine"],
+                                   "substitutions": results[n]["stats"]["ms_subst"],
+                                   "n_subst": results[n]["stats"]["n_subst"]},
+                      "gpu_launches_per_step": results[n]["launches"]}
+                  for n in ("fp64", "mixed")},
         "mixed_over_fp64": fp64["ms"] / mixed["ms"],
-        "ir_iterations": st["ir_iterations"],
-        "ir_residual": st["ir_residual"],
-        "perturbed_pivots": {"mixed": st["perturbed_pivots"], "fp64": fp64["stats"]["perturbed_pivots"]},
-        "phase_ms": {"assemble": st["ms_assemble"], "factor": st["ms_factor"], "solve": st["ms_solve"],
-                     "refine": st["ms_refine"], "substitutions": st["ms_subst"], "n_subst": st["n_subst"]},
-        "roofline": {"kernel": "K5 multi-RHS substitution (k_fwd + k_bwd, complex64)", "bound": "hbm",
-                     "achieved": achieved, "peak": peak_hbm, "unit": "GB/s", "frac": achieved / peak_hbm,
-                     "peak_kind": peak_kind, "traffic": traffic,
+        "roofline": {"kernel": "K5 multi-RHS substitution (k_fwd + k_bwd, %s)" % ("complex128" if csize == 16 else "complex64"),
+                     "bound": "hbm", "achieved": achieved, "peak": peak_hbm, "unit": "GB/s",
+                     "frac": achieved / peak_hbm, "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": subst_bytes, "ms_per_launch_group": subst_ms},
-        "gpu_launches": mixed["launches"] * args.steps,
-        "gpu_launches_per_step": mixed["launches"],
-        "clocks": mixed["clocks"],
+        "gpu_launches": head["launches"] * args.steps,
+        "clocks": head["clocks"],
         "cpu_baseline": cpu,
     }
     if rank == 0:
