@@ -9,5 +9,5 @@ ctypes binding (``_lib``) and the host-side mirror of the reference's
 per-frequency drivers (``engine.Engine``).
 """
 from .engine import (GM_OP_EXACT, GM_OP_REF, GM_PHYS_AC, GM_PHYS_SH, GM_PHYS_TE, GM_PREC_C64_IR,  # noqa: F401
-                     GM_PREC_FP64, GM_SYS_A, GM_SYS_AT, Engine, nonzero)
+                     GM_PREC_FP64, GM_SYS_A, GM_SYS_AT, Engine, gauss_filt, nonzero)
 from ._lib import GmError  # noqa: F401

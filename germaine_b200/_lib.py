@@ -55,7 +55,7 @@ class GmStats(ctypes.Structure):
 EXPORTS = [
     "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats", "gm_engine_stream",
     "gm_set_model", "gm_factor", "gm_factor_values", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
-    "gm_get_gradient_fp64", "gm_solve_noalloc", "gm_cgemm_sub_c64",
+    "gm_get_gradient_fp64", "gm_gauss_filt", "gm_solve_noalloc", "gm_cgemm_sub_c64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
 ]
@@ -104,6 +104,8 @@ def load() -> ctypes.CDLL:
     lib.gm_grad_obj.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, i32, i32, vp, vp, vp, vp]
     lib.gm_obj.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, i32, i32, vp]
     lib.gm_get_gradient_fp64.argtypes = [vp, vp, vp]
+    f32 = ctypes.c_float
+    lib.gm_gauss_filt.argtypes = [i32, i32, i32, f32, f32, f32, f32, f32, vp, vp]
     lib.gm_solve_noalloc.argtypes = [vp, i32, i32, vp, vp]
     lib.gm_cgemm_sub_c64.argtypes = [i32, i32, i32, vp, vp, vp, vp]
     lib.gm_symbolic_create.argtypes = [i32, i32, i32, ctypes.POINTER(vp)]

@@ -11,6 +11,7 @@
  */
 #include <complex.h>
 #include <math.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include "host_setup.h"
@@ -171,4 +172,43 @@ void gmh_grad_frame(int nx, int ny, int npml, int free_surf, float *coef, unsign
     for (i = 1; i <= nx; i++) for (j = fsshift + ny0 + 1; j <= ny; j++) PASS(j, i)++;
 #undef COEF
 #undef PASS
+}
+
+/* Gaussian gradient filter of gauss_filt (src/gauss_filt.c:27-118): half
+ * widths hfs[0] (x), hfs[1] (y) and the normalised (2 hfs[1] + 1) x
+ * (2 hfs[0] + 1) weights w[(jj + hfsy) * (2 hfsx + 1) + ii + hfsx], in the
+ * reference's float / double arithmetic and summation order.  Returns 0 when
+ * the filter is off (a zero size), else the number of weights; at most
+ * wmax weights are written (-1 if more are needed). */
+int gmh_gauss_kernel(float dh, float vref, float fc_low, float fsg, float fsg1, int hfs[2], float *w, int wmax)
+{
+    float lam = vref / fc_low;
+    int fsx = round((fsg * lam) / dh), fsy = round((fsg1 * lam) / dh);
+    int hfsx, hfsy, ii, jj, nwx, nwy;
+    float sigmax, sigmay, sx, sy, sum = 0.0;
+    if (fsx == 0 || fsy == 0) return 0;
+    if (!(fsx % 2)) fsx += fsx > 0 ? 1 : -1;
+    if (!(fsy % 2)) fsy += fsy > 0 ? 1 : -1;
+    hfsx = abs(fsx) / 2;
+    sigmax = hfsx / 2;
+    sx = 2.0 * sigmax * sigmax;
+    hfsy = abs(fsy) / 2;
+    sigmay = hfsy / 2;
+    sy = 2.0 * sigmay * sigmay;
+    nwx = 2 * hfsx + 1;
+    nwy = 2 * hfsy + 1;
+    if (nwx * nwy > wmax) return -1;
+    hfs[0] = hfsx;
+    hfs[1] = hfsy;
+    for (ii = -hfsx; ii <= hfsx; ii++)
+        for (jj = -hfsy; jj <= hfsy; jj++) {
+            float *k = &w[(jj + hfsy) * nwx + ii + hfsx];
+            *k = exp(-((ii * ii) / sx) - ((jj * jj) / sy));
+            sum += *k;
+        }
+    /* the reference normalises over i <= filt_size_x, j <= filt_size_y: a
+     * negative size leaves the weights unnormalised */
+    if (fsx > 0 && fsy > 0)
+        for (ii = 0; ii < nwx * nwy; ii++) w[ii] /= sum;
+    return nwx * nwy;
 }

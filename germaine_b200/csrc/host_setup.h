@@ -13,6 +13,7 @@ void gmh_gradient_scalars(int physics, float freq, float s, float om2[2], float 
 void gmh_stf_unit(const float stf[2], float unit[2]);
 void gmh_wiener(const float num[2], const float den[2], float wien[2]);
 void gmh_grad_frame(int nx, int ny, int npml, int free_surf, float *coef, unsigned char *passes);
+int gmh_gauss_kernel(float dh, float vref, float fc_low, float fsg, float fsg1, int hfs[2], float *w, int wmax);
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,78 @@
+// Gradient post-processing on the device: the Gaussian smoothing of the
+// gradient that precond() applies before the l-BFGS step when SPATFILTER = 1
+// (src/precond.c:18, src/gauss_filt.c:10-141).  The filter weights are built
+// on the host with the reference's own float / double arithmetic
+// (host_setup.c: gmh_gauss_kernel); the device convolution accumulates in
+// float in the reference's order (taps along x outer, along y inner) with
+// separately rounded products and sums, so the result is bit-identical.
+// HBM-bound: the gradient is read through L1 (each value is reused by every
+// output cell whose window covers it), one float per cell written.
+#include <vector>
+
+#include "common.hpp"
+#include "host_setup.h"
+#include "kernels.cuh"
+
+namespace gm {
+
+constexpr int GAUSS_WMAX = 12288;   // weights held in shared memory (48 KB)
+
+__global__ void __launch_bounds__(256) k_gauss_filt(const float *__restrict__ in, float *__restrict__ out, int nx,
+                                                    int ny, const float *__restrict__ wg, int hfsx, int hfsy) {
+    extern __shared__ float w[];
+    const int nwx = 2 * hfsx + 1, nw = nwx * (2 * hfsy + 1);
+    for (int t = threadIdx.x; t < nw; t += blockDim.x) w[t] = wg[t];
+    __syncthreads();
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nx * ny) return;
+    const int i = k % nx, j = k / nx;
+    float conv = 0.0f;
+    for (int ii = -hfsx; ii <= hfsx; ++ii) {
+        const int xi = min(max(i + ii, 0), nx - 1);   // the edge extension of gauss_filt.c:72-100
+        for (int jj = -hfsy; jj <= hfsy; ++jj) {
+            const int yj = min(max(j + jj, 0), ny - 1);
+            conv = __fadd_rn(conv, __fmul_rn(__ldg(in + (size_t)yj * nx + xi), w[(jj + hfsy) * nwx + ii + hfsx]));
+        }
+    }
+    out[k] = conv;
+}
+
+}  // namespace gm
+
+extern "C" int gm_gauss_filt(int device, int nx, int ny, float dh, float vref, float fc_low, float filt_size_grad,
+                             float filt_size_grad1, const float *grad, float *out) {
+    if (nx <= 0 || ny <= 0 || !grad || !out || !(dh > 0.f) || !(fc_low > 0.f))
+        return gm::fail(GM_ERROR_INVALID, "gm_gauss_filt: bad argument");
+    if (cudaSetDevice(device) != cudaSuccess) return gm::fail(GM_ERROR_CUDA, "gm_gauss_filt: bad device %d", device);
+    const size_t n = (size_t)nx * ny;
+    std::vector<float> w(gm::GAUSS_WMAX);
+    int hfs[2] = {0, 0};
+    const int nw = gmh_gauss_kernel(dh, vref, fc_low, filt_size_grad, filt_size_grad1, hfs, w.data(), gm::GAUSS_WMAX);
+    if (nw < 0) return gm::fail(GM_ERROR_INVALID, "gm_gauss_filt: filter window larger than %d taps", gm::GAUSS_WMAX);
+    if (nw == 0) {   // filter size 0: gauss_filt returns without touching the gradient
+        if (out != grad && cudaMemcpy(out, grad, n * sizeof(float), cudaMemcpyDefault) != cudaSuccess)
+            return gm::fail(GM_ERROR_CUDA, "gm_gauss_filt: copy failed");
+        return GM_OK;
+    }
+    float *din = nullptr, *dout = nullptr, *dw = nullptr;
+    int rc = GM_OK;
+    if (cudaMalloc(&din, n * sizeof(float)) != cudaSuccess || cudaMalloc(&dout, n * sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&dw, nw * sizeof(float)) != cudaSuccess) {
+        rc = gm::fail(GM_ERROR_OUT_OF_MEMORY, "gm_gauss_filt: device allocation failed");
+    } else if (cudaMemcpy(din, grad, n * sizeof(float), cudaMemcpyDefault) != cudaSuccess ||
+               cudaMemcpy(dw, w.data(), nw * sizeof(float), cudaMemcpyHostToDevice) != cudaSuccess) {
+        rc = gm::fail(GM_ERROR_CUDA, "gm_gauss_filt: upload failed");
+    } else {
+        const int tpb = 256;
+        gm::k_gauss_filt<<<(unsigned)((n + tpb - 1) / tpb), tpb, nw * sizeof(float)>>>(din, dout, nx, ny, dw, hfs[0],
+                                                                                      hfs[1]);
+        gm::note_launch();
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(out, dout, n * sizeof(float), cudaMemcpyDefault);
+        if (e != cudaSuccess) rc = gm::fail(GM_ERROR_CUDA, "gm_gauss_filt: %s", cudaGetErrorString(e));
+    }
+    cudaFree(din);
+    cudaFree(dout);
+    cudaFree(dw);
+    return rc;
+}

@@ -27,7 +27,7 @@ from . import _lib
 from ._lib import (GM_OP_EXACT, GM_OP_REF, GM_PHYS_AC, GM_PHYS_SH, GM_PHYS_TE, GM_PREC_C64_IR, GM_PREC_FP64,
                    GM_SYS_A, GM_SYS_AT, GmConfig, GmStats, check, ptr)
 
-__all__ = ["Engine", "GM_PHYS_AC", "GM_PHYS_SH", "GM_PHYS_TE", "GM_PREC_FP64", "GM_PREC_C64_IR",
+__all__ = ["Engine", "gauss_filt", "GM_PHYS_AC", "GM_PHYS_SH", "GM_PHYS_TE", "GM_PREC_FP64", "GM_PREC_C64_IR",
            "GM_OP_REF", "GM_OP_EXACT", "GM_SYS_A", "GM_SYS_AT", "nonzero"]
 
 
@@ -191,3 +191,15 @@ class Engine:
         self.last_status = check(self.lib.gm_obj(self._h, sx.size, ptr(sx), ptr(sy), rx.size, ptr(rx), ptr(ry),
                                                  ptr(obs), stf_inv, misfit, ctypes.byref(l2)))
         return float(l2.value)
+
+
+def gauss_filt(grad, dh: float, vref: float, fc_low: float, filt_size_grad: float, filt_size_grad1: float,
+               device: int = 0) -> np.ndarray:
+    """Gaussian smoothing of a [NY][NX] gradient on the GPU (gm_gauss_filt:
+    gauss_filt, src/gauss_filt.c:10-141, bit-identical)."""
+    g = _c(grad, np.float32)
+    ny, nx = g.shape
+    out = np.empty_like(g)
+    check(_lib.load().gm_gauss_filt(device, nx, ny, dh, vref, fc_low, filt_size_grad, filt_size_grad1, ptr(g),
+                                    ptr(out)))
+    return out

@@ -180,6 +180,16 @@ int gm_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y,
            int ntr, const int32_t *rec_x, const int32_t *rec_y,
            const float *pobs, int stf_inv, int misfit, float *l2);
 
+/* Gaussian smoothing of a gradient on the device: gauss_filt
+ * (src/gauss_filt.c:10-141), applied by precond() when SPATFILTER = 1
+ * (src/precond.c:18).  grad and out are [NY][NX] floats (host or device; out
+ * may equal grad); the window follows from VREF, FC_low, FILT_SIZE_GRAD,
+ * FILT_SIZE_GRAD1 and DH as in the reference (a size of 0 leaves the
+ * gradient unchanged), edges extended by their last value.  Bit-identical
+ * to the reference's float result. */
+int gm_gauss_filt(int device, int nx, int ny, float dh, float vref, float fc_low, float filt_size_grad,
+                  float filt_size_grad1, const float *grad, float *out);
+
 /* gm_solve without device allocation.  No counterpart in the reference: for
  * callers that cannot call cudaMalloc/cudaFree while solving -- cudaFree
  * synchronises the whole device (stalling the caller's own kernels on other

@@ -106,6 +106,7 @@ def load_port():
         lib.port_grad_frame_coeff.argtypes = [P, _f32p]
         lib.port_cp_grad_frame.argtypes = [P, _f32p]
         lib.port_gradient_scalars.argtypes = [P, ctypes.c_int, ctypes.c_float, _f32p, _f32p]
+        lib.port_gauss_filt.argtypes = [P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f32p]
         _port_lib = lib
     return _port_lib
 
@@ -134,6 +135,7 @@ def load_ref():
         lib.ref_ass_grad_ac.argtypes = [ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
         lib.ref_ass_grad_te.argtypes = [ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
         lib.ref_cp_grad_frame.argtypes = [_f32p]
+        lib.ref_gauss_filt.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f32p]
         _ref_lib = lib
     return _ref_lib
 
@@ -212,6 +214,12 @@ class Port:
     def cp_grad_frame(self, grad):
         self.lib.port_cp_grad_frame(ctypes.byref(self._pg), grad)
 
+    def gauss_filt(self, grad, vref, fc_low, fsg, fsg1):
+        """Filtered copy of a [NY][NX] gradient (gauss_filt)."""
+        out = np.ascontiguousarray(grad, np.float32).copy()
+        self.lib.port_gauss_filt(ctypes.byref(self._pg), vref, fc_low, fsg, fsg1, out.reshape(-1))
+        return out
+
     def gradient_scalars(self, physics, freq):
         """(Omega^2, Omega) of ass_grad_AC / ass_grad_TE as complex64 values."""
         a = np.zeros(2, np.float32); b = np.zeros(2, np.float32)
@@ -283,6 +291,11 @@ class Ref:
 
     def cp_grad_frame(self, grad):
         self.lib.ref_cp_grad_frame(grad)
+
+    def gauss_filt(self, grad, vref, fc_low, fsg, fsg1):
+        out = np.ascontiguousarray(grad, np.float32).copy()
+        self.lib.ref_gauss_filt(vref, fc_low, fsg, fsg1, out.reshape(-1))
+        return out
 
 
 def dropin_available() -> bool:

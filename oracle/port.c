@@ -418,3 +418,53 @@ void port_gradient_scalars(const port_grid *g, int physics, float freq, float *o
     om2[0] = crealf(o2); om2[1] = cimagf(o2);
     om[0] = crealf(o); om[1] = cimagf(o);
 }
+
+/* Gaussian smoothing of the gradient, src/gauss_filt.c:10-141 (SPATFILTER=1
+ * in precond(), src/precond.c:18).  grad [NY][NX] is filtered in place;
+ * window and weights in the reference's float / double arithmetic, edges
+ * extended by their last value (gauss_filt.c:72-100), float accumulation
+ * with taps along x outer and along y inner. */
+void port_gauss_filt(const port_grid *g, float vref, float fc_low, float fsg, float fsg1, float *grad)
+{
+    const int nx = g->nx, ny = g->ny;
+    const float lam = vref / fc_low;
+    int fx = round((fsg * lam) / g->dh), fy = round((fsg1 * lam) / g->dh);
+    int hx, hy, ii, jj, i, j, nwx;
+    float sgx, sgy, sx, sy, total = 0.0, *wt, *src;
+    if (fx == 0 || fy == 0) return;
+    if (fx % 2 == 0) fx += (fx > 0) ? 1 : -1;
+    if (fy % 2 == 0) fy += (fy > 0) ? 1 : -1;
+    hx = abs(fx) / 2; hy = abs(fy) / 2;
+    sgx = hx / 2; sgy = hy / 2;
+    sx = 2.0 * sgx * sgx; sy = 2.0 * sgy * sgy;
+    nwx = 2 * hx + 1;
+    wt = malloc(sizeof(float) * (size_t)nwx * (2 * hy + 1));
+    src = malloc(sizeof(float) * (size_t)nx * ny);
+    for (ii = -hx; ii <= hx; ii++)
+        for (jj = -hy; jj <= hy; jj++) {
+            float v = exp(-((ii * ii) / sx) - ((jj * jj) / sy));
+            wt[(jj + hy) * nwx + ii + hx] = v;
+            total += v;
+        }
+    /* gauss_filt.c:114-120 normalises over i <= filt_size_x, j <= filt_size_y:
+     * with a negative size the loop is empty and the weights stay raw */
+    if (fx > 0 && fy > 0)
+        for (i = 0; i < nwx * (2 * hy + 1); i++) wt[i] /= total;
+    memcpy(src, grad, sizeof(float) * (size_t)nx * ny);
+    for (j = 0; j < ny; j++)
+        for (i = 0; i < nx; i++) {
+            float acc = 0.0;
+            for (ii = -hx; ii <= hx; ii++) {
+                int x = i + ii;
+                x = x < 0 ? 0 : (x >= nx ? nx - 1 : x);
+                for (jj = -hy; jj <= hy; jj++) {
+                    int y = j + jj;
+                    y = y < 0 ? 0 : (y >= ny ? ny - 1 : y);
+                    acc += src[y * nx + x] * wt[(jj + hy) * nwx + ii + hx];
+                }
+            }
+            grad[j * nx + i] = acc;
+        }
+    free(wt);
+    free(src);
+}

@@ -256,3 +256,14 @@ void ref_cp_grad_frame(float *grad)
     from_nr(g, grad);
     free_matrix(g, 0, NY + 1, 0, NX + 1);
 }
+
+/* gauss_filt (src/gauss_filt.c:10) on a flat [NY][NX] gradient, in place */
+void ref_gauss_filt(float vref, float fc_low, float fsg, float fsg1, float *grad)
+{
+    extern float VREF, FC_low, FILT_SIZE_GRAD, FILT_SIZE_GRAD1;
+    float **gr = to_nr(grad);
+    VREF = vref; FC_low = fc_low; FILT_SIZE_GRAD = fsg; FILT_SIZE_GRAD1 = fsg1;
+    gauss_filt(gr);
+    from_nr(gr, grad);
+    free_matrix(gr, 0, NY + 1, 0, NX + 1);
+}

@@ -50,6 +50,32 @@ def main():
             d["x"] = OS.DirectSolver(M).solve(b)
         np.savez_compressed(os.path.join(out, name + ".npz"), **d)
         print("wrote", name)
+    gauss_filt_fixture(out)
+
+
+# gauss_filt (src/gauss_filt.c) cases: grid, VREF, FC_low, FILT_SIZE_GRAD, FILT_SIZE_GRAD1
+GAUSS_CASES = [
+    (61, 41, 10.0, 2000.0, 5.0, 0.5, 0.5),
+    (61, 41, 10.0, 2000.0, 5.0, 0.3, 0.7),
+    (45, 33, 25.0, 3000.0, 2.0, 0.2, 0.35),
+    (61, 41, 10.0, 2000.0, 5.0, -0.4, 0.4),   # negative size: weights left unnormalised
+    (61, 41, 10.0, 2000.0, 5.0, 0.0, 0.5),    # size 0: filter off
+]
+
+
+def gauss_filt_fixture(out):
+    """postproc_gauss_filt.npz: seeded gradients and the reference's
+    gauss_filt of each (case k in arrays with suffix _k)."""
+    d = {"ncases": len(GAUSS_CASES)}
+    rng = np.random.default_rng(11)
+    for k, (nx, ny, dh, vref, fc, fs0, fs1) in enumerate(GAUSS_CASES):
+        g = O.Grid(nx=nx, ny=ny, dh=dh, npml=6)
+        grad = (rng.standard_normal((ny, nx)) * 1e-3).astype(np.float32)
+        d[f"case_{k}"] = np.array([nx, ny, dh, vref, fc, fs0, fs1])
+        d[f"grad_{k}"] = grad
+        d[f"out_{k}"] = O.Ref(g).gauss_filt(grad, vref, fc, fs0, fs1)
+    np.savez_compressed(os.path.join(out, "postproc_gauss_filt.npz"), **d)
+    print("wrote postproc_gauss_filt")
 
 
 if __name__ == "__main__":

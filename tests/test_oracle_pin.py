@@ -99,7 +99,9 @@ def test_port_shot_arithmetic_equals_reference(physics):
 
 
 def _golden_files():
-    return sorted(f for f in os.listdir(GOLDEN) if f.endswith(".npz")) if os.path.isdir(GOLDEN) else []
+    """assembly / solve fixtures (the post-processing fixtures have their own tests)"""
+    return (sorted(f for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("postproc_"))
+            if os.path.isdir(GOLDEN) else [])
 
 
 @pytest.mark.parametrize("fname", _golden_files())
@@ -118,3 +120,32 @@ def test_port_against_golden(fname):
         M = OS.operator(OS.assembled_matrix(g, *a))
         x = OS.DirectSolver(M).solve(d["b"])
         assert np.linalg.norm(x - d["x"]) / np.linalg.norm(d["x"]) < 1e-12
+
+
+def gauss_cases():
+    d = np.load(os.path.join(GOLDEN, "postproc_gauss_filt.npz"))
+    out = []
+    for k in range(int(d["ncases"])):
+        nx, ny, dh, vref, fc, fs0, fs1 = d[f"case_{k}"]
+        out.append((int(nx), int(ny), float(dh), float(vref), float(fc), float(fs0), float(fs1), d[f"grad_{k}"],
+                    d[f"out_{k}"]))
+    return out
+
+
+def test_port_gauss_filt_against_golden():
+    """gauss_filt (src/gauss_filt.c:10-141): the restatement is bit-identical
+    to the reference's output stored in the fixture, including the filter-off
+    and unnormalised (negative size) cases."""
+    for nx, ny, dh, vref, fc, fs0, fs1, grad, ref in gauss_cases():
+        g = O.Grid(nx=nx, ny=ny, dh=dh, npml=6)
+        assert np.array_equal(_bits(O.Port(g).gauss_filt(grad, vref, fc, fs0, fs1)), _bits(ref))
+
+
+@needs_ref
+@pytest.mark.parametrize("fs0,fs1", [(0.5, 0.5), (0.25, 0.6), (1.1, 0.15), (-0.3, 0.3), (0.4, -0.2)])
+def test_port_gauss_filt_equals_reference(fs0, fs1):
+    g = O.Grid(nx=57, ny=43, dh=12.5, npml=6)
+    grad = np.random.default_rng(3).standard_normal((43, 57)).astype(np.float32)
+    a = O.Port(g).gauss_filt(grad, 2500.0, 4.0, fs0, fs1)
+    b = O.Ref(g).gauss_filt(grad, 2500.0, 4.0, fs0, fs1)
+    assert np.array_equal(_bits(a), _bits(b))
