@@ -54,8 +54,8 @@ class GmStats(ctypes.Structure):
 # every C-ABI symbol declared in include/germaine_gpu.h
 EXPORTS = [
     "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats", "gm_engine_stream",
-    "gm_set_model", "gm_factor", "gm_factor_values", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
-    "gm_get_gradient_fp64", "gm_gauss_filt", "gm_solve_noalloc", "gm_cgemm_sub_c64",
+    "gm_set_model", "gm_set_models", "gm_factor", "gm_factor_models", "gm_factor_values", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
+    "gm_get_gradient_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_cgemm_sub_c64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
 ]
@@ -97,6 +97,9 @@ def load() -> ctypes.CDLL:
     lib.gm_engine_stream.argtypes = [vp, ctypes.POINTER(vp)]
     lib.gm_set_model.argtypes = [vp, vp, vp]
     lib.gm_factor.argtypes = [vp, i32, vp]
+    lib.gm_set_models.argtypes = [vp, i32, vp, vp]
+    lib.gm_factor_models.argtypes = [vp, i32, vp, vp]
+    lib.gm_obj_each.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, i32, i32, vp]
     lib.gm_factor_values.argtypes = [vp, i32, vp, vp]
     lib.gm_get_triplets.argtypes = [vp, i32, vp, vp, vp, vp]
     lib.gm_solve.argtypes = [vp, i32, i32, vp, vp]

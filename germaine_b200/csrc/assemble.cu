@@ -17,8 +17,8 @@
 
 namespace gm {
 
-// Per-cell, per-frequency mass factor (complex float) and per-cell
-// stiffness (float):
+// Per-cell, per-matrix mass factor (complex float) and stiffness (float),
+// from the material model of the matrix:
 //   AC: mass = Omega^2 * ivp2, ivp2 = 1/(rho vp^2)   (init_mat_AC.c:21, :71)
 //       stiff = b = 1/rho                          (init_mat_AC.c:24)
 //   SH: mass = Omega^2 * rho, stiff = mu = rho vs^2 (init_mat_SH.c:21)
@@ -28,16 +28,17 @@ __global__ void k_cells(int physics, int n, const float *__restrict__ m0, const 
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
     const int f = blockIdx.y;
     if (k >= n) return;
-    const float a = m0[k], b = m1[k];
     const AsmFreq p = fq[f];
+    const size_t mo = (size_t)p.model * n;
+    const float a = m0[mo + k], b = m1[mo + k];
     float2 m;
     if (physics == GM_PHYS_AC) {
         const float ivp2 = __double2float_rn(__ddiv_rn(1.0, (double)__fmul_rn(__fmul_rn(b, a), a)));
         m = rn_scale(ivp2, p.om2);
-        if (f == 0) stiff[k] = __double2float_rn(__ddiv_rn(1.0, (double)b));
+        stiff[(size_t)f * n + k] = __double2float_rn(__ddiv_rn(1.0, (double)b));
     } else if (physics == GM_PHYS_SH) {
         m = rn_scale(b, p.om2);
-        if (f == 0) stiff[k] = __fmul_rn(__fmul_rn(b, a), a);
+        stiff[(size_t)f * n + k] = __fmul_rn(__fmul_rn(b, a), a);
     } else {
         const float2 q = rn_real_div_cf(b, p.om);
         // (q) * I as gcc lowers complex-float multiplication by (0 + 1i)
@@ -83,14 +84,15 @@ __global__ void k_stencil(AsmArgs a) {
     const float2 dyp = make_float2(pyhr[j], pyhi[j]), dym = make_float2(pyhr[j - 1], pyhi[j - 1]);
 
     BVals b;
+    const float *stiff = a.stiff + (size_t)f * a.n;
     if (a.physics == GM_PHYS_AC) {           // pointwise buoyancy, av_rho.c:32-48
-        const float v = a.stiff[k];
+        const float v = stiff[k];
         b.pm = b.mp = b.pp = b.mm = b.p0 = b.m0 = b.zp = b.zm = v;
     } else if (a.physics == GM_PHYS_SH) {    // averaged shear modulus, av_mu.c:12-28
         auto mu = [&](int jj, int ii) {
             jj = jj < 1 ? 1 : (jj > ny ? ny : jj);
             ii = ii < 1 ? 1 : (ii > nx ? nx : ii);
-            return a.stiff[(jj - 1) * nx + (ii - 1)];
+            return stiff[(jj - 1) * nx + (ii - 1)];
         };
         auto q4 = [](float s0, float s1, float s2, float s3) {
             return __double2float_rn(__dmul_rn(0.25, (double)__fadd_rn(__fadd_rn(__fadd_rn(s0, s1), s2), s3)));

@@ -193,19 +193,24 @@ extern "C" int gm_engine_stream(const gm_engine *e, void **stream) {
     return GM_OK;
 }
 
-extern "C" int gm_set_model(gm_engine *e, const float *mat0, const float *mat1) {
-    if (!e || !mat0 || !mat1) return fail(GM_ERROR_INVALID, "gm_set_model: null argument");
+extern "C" int gm_set_models(gm_engine *e, int nmod, const float *mat0, const float *mat1) {
+    if (!e || nmod <= 0 || !mat0 || !mat1) return fail(GM_ERROR_INVALID, "gm_set_models: bad argument");
     GM_CUDA(cudaSetDevice(e->device));
-    const size_t nb = (size_t)e->n * sizeof(float);
+    const size_t nb = (size_t)nmod * e->n * sizeof(float);
     GM_ALLOC(e->d_m0, nb);
     GM_ALLOC(e->d_m1, nb);
-    GM_ALLOC(e->d_stiff, nb);
     GM_CUDA(cudaMemcpyAsync(e->d_m0.p, mat0, nb, cudaMemcpyDefault, e->st));
     GM_CUDA(cudaMemcpyAsync(e->d_m1.p, mat1, nb, cudaMemcpyDefault, e->st));
     GM_CUDA(cudaStreamSynchronize(e->st));
+    e->nmod = nmod;
     e->have_model = true;
     e->factored = false;
     return GM_OK;
+}
+
+extern "C" int gm_set_model(gm_engine *e, const float *mat0, const float *mat1) {
+    if (!e || !mat0 || !mat1) return fail(GM_ERROR_INVALID, "gm_set_model: null argument");
+    return gm_set_models(e, 1, mat0, mat1);
 }
 
 namespace gm {
@@ -224,9 +229,12 @@ static int assemble_batch(gm_engine *e) {
         fq[f].om2 = make_float2(om2[0], om2[1]);
         fq[f].om = make_float2(om[0], om[1]);
         fq[f].om2mu0 = make_float2(om2mu0[0], om2mu0[1]);
+        fq[f].model = e->models[f];
+        fq[f].pad = 0;
     }
     GM_ALLOC(e->d_A, (size_t)nf * 9 * n * sizeof(double2));
     GM_ALLOC(e->d_mass, (size_t)nf * n * sizeof(float2));
+    GM_ALLOC(e->d_stiff, (size_t)nf * n * sizeof(float));
     GM_ALLOC(e->d_pml, pml.size() * sizeof(float));
     GM_ALLOC(e->d_fq, fq.size() * sizeof(AsmFreq));
     GM_CUDA(cudaMemcpyAsync(e->d_pml.p, pml.data(), pml.size() * sizeof(float), cudaMemcpyHostToDevice, e->st));
@@ -382,16 +390,21 @@ static int factor_assembled(gm_engine *e) {
 
 }  // namespace gm
 
-extern "C" int gm_factor(gm_engine *e, int nfreq, const float *h_freqs) {
-    if (!e || nfreq <= 0 || !h_freqs) return fail(GM_ERROR_INVALID, "gm_factor: bad argument");
+extern "C" int gm_factor_models(gm_engine *e, int nmat, const float *h_freqs, const int32_t *h_models) {
+    if (!e || nmat <= 0 || !h_freqs) return fail(GM_ERROR_INVALID, "gm_factor: bad argument");
     if (!e->have_model) return fail(GM_ERROR_STATE, "gm_factor: no model set (gm_set_model)");
-    for (int f = 0; f < nfreq; ++f)
+    for (int f = 0; f < nmat; ++f) {
         if (!(h_freqs[f] > 0.f) || !std::isfinite(h_freqs[f])) return fail(GM_ERROR_INVALID, "frequency %d is not positive", f);
+        if (h_models && (h_models[f] < 0 || h_models[f] >= e->nmod))
+            return fail(GM_ERROR_INVALID, "matrix %d: model %d out of range (%d models)", f, h_models[f], e->nmod);
+    }
     GM_CUDA(cudaSetDevice(e->device));
     e->factored = false;
     e->values_only = false;
-    e->nf = nfreq;
-    e->freqs.assign(h_freqs, h_freqs + nfreq);
+    e->nf = nmat;
+    e->freqs.assign(h_freqs, h_freqs + nmat);
+    if (h_models) e->models.assign(h_models, h_models + nmat);
+    else e->models.assign(nmat, 0);
 
     GM_CUDA(cudaEventRecord(e->ev0, e->st));
     int rc = gm::assemble_batch(e);
@@ -404,6 +417,10 @@ extern "C" int gm_factor(gm_engine *e, int nfreq, const float *h_freqs) {
     return gm::factor_assembled(e);
 }
 
+extern "C" int gm_factor(gm_engine *e, int nfreq, const float *h_freqs) {
+    return gm_factor_models(e, nfreq, h_freqs, nullptr);
+}
+
 extern "C" int gm_factor_values(gm_engine *e, int nmat, const double *re, const double *im) {
     if (!e || nmat <= 0 || !re || !im) return fail(GM_ERROR_INVALID, "gm_factor_values: bad argument");
     GM_CUDA(cudaSetDevice(e->device));
@@ -411,6 +428,7 @@ extern "C" int gm_factor_values(gm_engine *e, int nmat, const double *re, const 
     e->values_only = true;
     e->nf = nmat;
     e->freqs.assign(nmat, 0.f);
+    e->models.assign(nmat, 0);
     const size_t cnt = (size_t)nmat * 9 * e->n;
     GM_ALLOC(e->d_A, cnt * sizeof(double2));
     // split inputs staged in the (grow-only) residual workspace

@@ -55,12 +55,14 @@ struct gm_engine {
     gm::DevSym dsym{};
 
     // model
-    gm::DevBuf d_m0, d_m1, d_stiff;
+    gm::DevBuf d_m0, d_m1, d_stiff;  // models [nmod][n]; stiffness per matrix [nf][n]
+    int nmod = 0;
     bool have_model = false;
 
     // factorisation of the current frequency batch
     int nf = 0;
     std::vector<float> freqs;
+    std::vector<int> models;    // material model of each matrix of the batch
     gm::DevBuf d_A, d_mass, d_pml, d_fq, d_front, d_npert, d_amax;
     bool factored = false;
     bool values_only = false;   // operator given by gm_factor_values (no frequencies / model)

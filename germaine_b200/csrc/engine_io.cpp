@@ -127,7 +127,7 @@ int forward_and_seis(gm_engine *e, int ns, const Geometry &g, int ntr, float *se
 // residuals and misfit; leaves res in the second half of e->d_res and the
 // source estimates w/|w| on the host
 int residuals(gm_engine *e, int ns, int ntr, const float *pobs, int stf_inv, int misfit, double &l2,
-              std::vector<double2> &stfu) {
+              std::vector<double2> &stfu, std::vector<double> *l2_each = nullptr) {
     const int nf = e->nf;
     const size_t cnt = (size_t)nf * ns * ntr;
     const int nfs = nf * ns;
@@ -146,6 +146,10 @@ int residuals(gm_engine *e, int ns, int ntr, const float *pobs, int stf_inv, int
     GM_CUDA(cudaStreamSynchronize(e->st));
     l2 = 0;
     for (double v : l2h) l2 += v;
+    if (l2_each) {
+        l2_each->assign(nf, 0.0);
+        for (int i = 0; i < nfs; ++i) (*l2_each)[i / ns] += l2h[i];
+    }
     stfu.resize(nfs);
     for (int i = 0; i < nfs; ++i) {
         const double a = std::hypot(stfh[i].x, stfh[i].y);
@@ -196,6 +200,26 @@ extern "C" int gm_obj(gm_engine *e, int nshots, const float *src_x, const float 
     return solve_rc;
 }
 
+extern "C" int gm_obj_each(gm_engine *e, int nshots, const float *src_x, const float *src_y, int ntr,
+                           const int32_t *rec_x, const int32_t *rec_y, const float *pobs, int stf_inv, int misfit,
+                           float *l2_each) {
+    int rc = check_ready(e, nshots, ntr);
+    if (rc) return rc;
+    if (!pobs || !l2_each || ntr <= 0) return fail(GM_ERROR_INVALID, "gm_obj_each: need observed data, receivers and an output");
+    if (misfit < 1 || misfit > 3) return fail(GM_ERROR_INVALID, "gm_obj_each: MISFIT must be 1, 2 or 3");
+    GM_CUDA(cudaSetDevice(e->device));
+    Geometry g;
+    if ((rc = make_geometry(e, nshots, src_x, src_y, ntr, rec_x, rec_y, g))) return rc;
+    const int solve_rc = forward_and_seis(e, nshots, g, ntr, nullptr);
+    if (solve_rc < 0) return solve_rc;
+    double l2 = 0;
+    std::vector<double2> stfu;
+    std::vector<double> each;
+    if ((rc = residuals(e, nshots, ntr, pobs, stf_inv, misfit, l2, stfu, &each))) return rc;
+    for (int f = 0; f < e->nf; ++f) l2_each[f] = (float)(0.5 * each[f]);
+    return solve_rc;
+}
+
 extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y, int ntr,
                            const int32_t *rec_x, const int32_t *rec_y, const float *pobs, int stf_inv, int misfit,
                            float *grad0, float *grad1, float *l2_out, float *seis) {
@@ -203,6 +227,9 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     if (rc) return rc;
     if (!pobs || ntr <= 0) return fail(GM_ERROR_INVALID, "gm_grad_obj: need observed data and receivers");
     if (misfit < 1 || misfit > 3) return fail(GM_ERROR_INVALID, "gm_grad_obj: MISFIT must be 1, 2 or 3");
+    for (int m : e->models)   // one gradient: every matrix of the batch from the same model
+        if (m != e->models[0])
+            return fail(GM_ERROR_STATE, "gm_grad_obj: the factorised matrices come from different models");
     const bool te = e->cfg.physics == GM_PHYS_TE;
     GM_CUDA(cudaSetDevice(e->device));
     Geometry g;
@@ -254,7 +281,7 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     ga.n = n; ga.nf = nf; ga.ns = nshots; ga.te = te;
     ga.xf = e->d_xf.as<double2>(); ga.xa = e->d_xa.as<double2>();
     ga.stfu = scal.as<double2>(); ga.om2 = ga.stfu + stfu.size(); ga.om = ga.om2 + nf;
-    ga.m0 = e->d_m0.as<float>(); ga.m1 = e->d_m1.as<float>();
+    ga.m0 = e->d_m0.as<float>() + (size_t)e->models[0] * n; ga.m1 = e->d_m1.as<float>() + (size_t)e->models[0] * n;
     ga.frame = e->d_frame.as<float>(); ga.passes = e->d_frame_pass.as<unsigned char>();
     ga.g0 = e->d_grad.as<double>(); ga.g1 = ga.g0 + n;
     gm::launch_gradient(ga, e->st);

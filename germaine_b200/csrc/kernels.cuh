@@ -21,6 +21,8 @@ struct AsmFreq {
     float2 om2;     // Omega^2 of the assembly
     float2 om;      // TE Omega
     float2 om2mu0;  // TE Omega^2 * mu0
+    int model;      // material model of this matrix (index into [nmod][n])
+    int pad;
 };
 
 struct AsmArgs {
@@ -28,7 +30,7 @@ struct AsmArgs {
     float w[6];               // a, b, c, d, e, idh2
     const float *pml;         // [nf][pml_stride]
     int pml_stride;           // 4*(nx+2) + 4*(ny+2)
-    const float *stiff;       // [n]  b (AC) or mu (SH)
+    const float *stiff;       // [nf][n]  b (AC) or mu (SH) of each matrix's model
     float2 *mass;             // [nf][n]
     double2 *A;               // [nf][9][n]
 };

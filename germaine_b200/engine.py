@@ -93,6 +93,36 @@ class Engine:
         self._m = (m0, m1)
         check(self.lib.gm_set_model(self._h, ptr(m0), ptr(m1)))
 
+    def set_models(self, mat0, mat1):
+        """Several material models [nmod][NY][NX] for gm_factor_models
+        (line-search trial models)."""
+        m0 = _c(mat0, np.float32)
+        m1 = _c(mat1, np.float32)
+        if m0.shape != m1.shape or m0.size % self.n:
+            raise ValueError("models must be [nmod][ny][nx] pairs")
+        check(self.lib.gm_set_models(self._h, m0.size // self.n, ptr(m0), ptr(m1)))
+
+    def factor_models(self, freqs, models) -> int:
+        """Factorise matrix m at freqs[m] from model models[m] (one batch)."""
+        f = _c(freqs, np.float32)
+        mi = _c(models, np.int32)
+        if f.size != mi.size:
+            raise ValueError("one model index per matrix")
+        self.last_status = check(self.lib.gm_factor_models(self._h, f.size, ptr(f), ptr(mi)))
+        self.nf = f.size
+        self.freqs = f
+        return self.last_status
+
+    def obj_each(self, src_x, src_y, rec_x, rec_y, pobs, stf_inv: int = 0, misfit: int = 1) -> np.ndarray:
+        """Misfit (0.5 L2) of every factorised matrix."""
+        sx = _c(src_x, np.float32); sy = _c(src_y, np.float32)
+        rx = _c(rec_x, np.int32); ry = _c(rec_y, np.int32)
+        obs = _c(pobs, np.complex64).reshape(self.nf, sx.size, rx.size)
+        out = np.zeros(self.nf, np.float32)
+        self.last_status = check(self.lib.gm_obj_each(self._h, sx.size, ptr(sx), ptr(sy), rx.size, ptr(rx), ptr(ry),
+                                                      ptr(obs), stf_inv, misfit, ptr(out)))
+        return out
+
     def factor(self, freqs) -> int:
         f = _c(np.atleast_1d(freqs), np.float32)
         self.last_status = check(self.lib.gm_factor(self._h, int(f.size), ptr(f)))

@@ -107,11 +107,26 @@ int gm_engine_stream(const gm_engine *e, void **stream);
  * Replaces readmod()/init_mat_AC (src/AC/init_mat_AC.c:10) input handling. */
 int gm_set_model(gm_engine *e, const float *mat0, const float *mat1);
 
+/* nmod material models at once (mat0, mat1: [nmod][NY][NX]) for a batch of
+ * matrices from different models: the trial models of a line search, which
+ * obj_AC re-assembles and re-factorises one at a time
+ * (src/AC/obj_AC.c:10-145, called per trial step by
+ * src/AC/parabolicls_AC.c and src/AC/wolfels_AC.c).  gm_set_model is
+ * gm_set_models with nmod = 1. */
+int gm_set_models(gm_engine *e, int nmod, const float *mat0, const float *mat1);
+
 /* Assemble and factorise the impedance matrices of nfreq frequencies as one
  * batch: init_A_{AC,SH,TE}_9p_pml (src/AC/init_A_AC_9p_pml.c:17) +
  * umfpack_zi_numeric (src/AC/forward_shot_AC.c:61), all frequencies at once.
  * Returns GM_WARNING_PERTURBED if static pivots had to be replaced. */
 int gm_factor(gm_engine *e, int nfreq, const float *h_freqs);
+
+/* gm_factor over nmat matrices, matrix m assembled at frequency h_freqs[m]
+ * from model h_models[m] (NULL: model 0 for all): one level-batched
+ * factorisation for every (trial model, frequency) pair.  gm_forward,
+ * gm_obj and gm_obj_each then run over all of them; gm_grad_obj requires
+ * one model for the whole batch. */
+int gm_factor_models(gm_engine *e, int nmat, const float *h_freqs, const int32_t *h_models);
 
 /* Factorise nmat operators given by value instead of assembled from a model:
  * umfpack_zi_numeric (src/AC/forward_shot_AC.c:61) on matrices that arrive
@@ -179,6 +194,14 @@ int gm_get_gradient_fp64(gm_engine *e, double *g0, double *g1);
 int gm_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y,
            int ntr, const int32_t *rec_x, const int32_t *rec_y,
            const float *pobs, int stf_inv, int misfit, float *l2);
+
+/* gm_obj with one misfit per factorised matrix: l2_each[m] = 0.5 * the
+ * misfit sum of matrix m over its shots (calc_res_AC, src/AC/calc_res_AC.c:
+ * 10-95, and the 0.5 L2 of obj_AC, src/AC/obj_AC.c), so that one batched
+ * call scores every trial model of a line search.  pobs as for gm_obj,
+ * [nmat][nshots][ntr]. */
+int gm_obj_each(gm_engine *e, int nshots, const float *src_x, const float *src_y, int ntr, const int32_t *rec_x,
+                const int32_t *rec_y, const float *pobs, int stf_inv, int misfit, float *l2_each);
 
 /* Gaussian smoothing of a gradient on the device: gauss_filt
  * (src/gauss_filt.c:10-141), applied by precond() when SPATFILTER = 1
