@@ -6,8 +6,10 @@ impedance-matrix assembly, nested-dissection multifrontal LU, multi-RHS
 substitution with FP64 refinement, and the adjoint-state gradient stack, all
 as CUDA kernels.  This package holds its in-tree build (``build.py``), the
 ctypes binding (``_lib``) and the host-side mirror of the reference's
-per-frequency drivers (``engine.Engine``).
+per-frequency drivers (``engine.Engine``) and of the reference's file
+formats (``files``).
 """
 from .engine import (GM_OP_EXACT, GM_OP_REF, GM_PHYS_AC, GM_PHYS_SH, GM_PHYS_TE, GM_PREC_C64_IR,  # noqa: F401
                      GM_PREC_FP64, GM_SYS_A, GM_SYS_AT, Engine, gauss_filt, nonzero)
 from ._lib import GmError  # noqa: F401
+from . import files  # noqa: F401

@@ -18,6 +18,7 @@ GM_WARNING_PERTURBED = 1
 GM_WARNING_NOT_CONVERGED = 2
 GM_ERROR_OUT_OF_MEMORY = -1
 GM_ERROR_INVALID = -2
+GM_SEIS_KEEP_LAST = 1
 GM_ERROR_STATE = -3
 GM_ERROR_CUDA = -4
 GM_ERROR_NONFINITE = -5
@@ -55,7 +56,8 @@ class GmStats(ctypes.Structure):
 EXPORTS = [
     "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats", "gm_engine_stream",
     "gm_set_model", "gm_set_models", "gm_factor", "gm_factor_models", "gm_factor_values", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
-    "gm_get_gradient_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_cgemm_sub_c64",
+    "gm_get_gradient_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc",
+    "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_cgemm_sub_c64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
 ]
@@ -109,6 +111,12 @@ def load() -> ctypes.CDLL:
     lib.gm_get_gradient_fp64.argtypes = [vp, vp, vp]
     f32 = ctypes.c_float
     lib.gm_gauss_filt.argtypes = [i32, i32, i32, f32, f32, f32, f32, f32, vp, vp]
+    cp = ctypes.c_char_p
+    lib.gm_write_seis.argtypes = [cp, i32, i32, i32, i32, vp]
+    lib.gm_read_seis.argtypes = [cp, i32, i32, i32, vp]
+    lib.gm_write_model_true.argtypes = [cp, i32, i32, i32, i32, i32, i32, vp]
+    lib.gm_write_model.argtypes = [cp, i32, i32, i32, i32, vp]
+    lib.gm_read_model.argtypes = [cp, i32, i32, i32, i32, vp]
     lib.gm_solve_noalloc.argtypes = [vp, i32, i32, vp, vp]
     lib.gm_cgemm_sub_c64.argtypes = [i32, i32, i32, vp, vp, vp, vp]
     lib.gm_symbolic_create.argtypes = [i32, i32, i32, ctypes.POINTER(vp)]

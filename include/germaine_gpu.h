@@ -213,6 +213,32 @@ int gm_obj_each(gm_engine *e, int nshots, const float *src_x, const float *src_y
 int gm_gauss_filt(int device, int nx, int ny, float dh, float vref, float fc_low, float filt_size_grad,
                   float filt_size_grad1, const float *grad, float *out);
 
+/* ---- the reference's file formats (host stdio, no GPU needed) ---- */
+#define GM_SEIS_KEEP_LAST 1  /* gm_write_seis: write the last sample as given */
+
+/* Seismogram file <PICKS_FILE>_p_stage_<n>.bin of write_seis_AC
+ * (src/AC/write_seis_AC.c:53-67): float (re, im) pairs, frequency outer,
+ * shot, receiver inner -- the [nf][nshots][ntr] layout gm_forward returns.
+ * write_seis_AC's gather (src/AC/write_seis_AC.c:43-44) reduces its
+ * 1-based arrays from element 0, so the reference always writes the file's
+ * LAST sample as 0 + 0i; flags 0 does the same (byte-identical files),
+ * GM_SEIS_KEEP_LAST writes that sample as given. */
+int gm_write_seis(const char *path, int nf, int nshots, int ntr, int flags, const float *seis);
+/* Observed seismograms as read_seis_AC reads them (src/AC/read_seis_AC.c:24-37). */
+int gm_read_seis(const char *path, int nf, int nshots, int ntr, float *seis);
+/* A [NY][NX] grid without its PML frame, as writemod_true writes models and
+ * snapshots (src/writemod_true.c:26-34): interior floats, x outer, every
+ * idx-th column and idy-th row (the reference's IDX, IDY). */
+int gm_write_model_true(const char *path, int nx, int ny, int npml, int free_surf, int idx, int idy,
+                        const float *grid);
+/* The full [NY][NX] grid as writemod writes it in binary format 3
+ * (src/writemod.c:24-30, src/writedsk.c:32-40): x outer, subsampled. */
+int gm_write_model(const char *path, int nx, int ny, int idx, int idy, const float *grid);
+/* One material file as readmod reads it (src/readmod.c:43-104; readmod_SH
+ * and readmod_TE alike): interior floats, x outer, placed into the [NY][NX]
+ * grid and extended into the PML frame by the nearest interior value. */
+int gm_read_model(const char *path, int nx, int ny, int npml, int free_surf, float *grid);
+
 /* gm_solve without device allocation.  No counterpart in the reference: for
  * callers that cannot call cudaMalloc/cudaFree while solving -- cudaFree
  * synchronises the whole device (stalling the caller's own kernels on other

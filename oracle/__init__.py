@@ -136,6 +136,12 @@ def load_ref():
         lib.ref_ass_grad_te.argtypes = [ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
         lib.ref_cp_grad_frame.argtypes = [_f32p]
         lib.ref_gauss_filt.argtypes = [ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f32p]
+        cp, i = ctypes.c_char_p, ctypes.c_int
+        lib.ref_write_seis.argtypes = [cp, i, i, i, i, _f32p, _f32p]
+        lib.ref_read_seis.argtypes = [cp, i, i, i, i, _f32p, _f32p]
+        lib.ref_writemod_true.argtypes = [cp, i, i, _f32p]
+        lib.ref_writemod.argtypes = [cp, i, i, _f32p]
+        lib.ref_readmod.argtypes = [cp, _f32p, _f32p]
         _ref_lib = lib
     return _ref_lib
 
@@ -220,6 +226,35 @@ class Port:
         self.lib.port_gauss_filt(ctypes.byref(self._pg), vref, fc_low, fsg, fsg1, out.reshape(-1))
         return out
 
+    # ---- file formats (numpy restatement) ----
+    def seis_bytes(self, seis, keep_last=False):
+        """write_seis_AC (src/AC/write_seis_AC.c:53-67): (re, im) float pairs,
+        frequency outer, shot, receiver inner.  Its gather
+        (src/AC/write_seis_AC.c:43-44) reduces the 1-based arrays from
+        element 0, so element n never arrives and the last sample is 0."""
+        s = np.array(seis, np.complex64).reshape(-1)
+        if not keep_last:
+            s[-1] = 0
+        return s.tobytes()
+
+    def model_true_bytes(self, grid, idx=1, idy=1):
+        """writemod_true (src/writemod_true.c:26-34): interior columns, x outer."""
+        g, fs = self.g, self.g.fsshift
+        inner = np.asarray(grid, np.float32)[fs:g.ny - g.npml, g.npml:g.nx - g.npml]
+        return np.ascontiguousarray(inner[::idy, ::idx].T).tobytes()
+
+    def model_bytes(self, grid, idx=1, idy=1):
+        """writemod format 3 (src/writemod.c:24-30): full grid, x outer."""
+        return np.ascontiguousarray(np.asarray(grid, np.float32)[::idy, ::idx].T).tobytes()
+
+    def model_from_bytes(self, data):
+        """readmod (src/readmod.c:43-104): interior read x outer, then the
+        frame filled with the nearest interior value."""
+        g, fs = self.g, self.g.fsshift
+        nx0, ny0 = g.nx - 2 * g.npml, g.ny - g.npml - fs
+        inner = np.frombuffer(data, np.float32, nx0 * ny0).reshape(nx0, ny0).T
+        return np.pad(inner, ((fs, g.npml), (g.npml, g.npml)), mode="edge")
+
     def gradient_scalars(self, physics, freq):
         """(Omega^2, Omega) of ass_grad_AC / ass_grad_TE as complex64 values."""
         a = np.zeros(2, np.float32); b = np.zeros(2, np.float32)
@@ -296,6 +331,31 @@ class Ref:
         out = np.ascontiguousarray(grad, np.float32).copy()
         self.lib.ref_gauss_filt(vref, fc_low, fsg, fsg1, out.reshape(-1))
         return out
+
+    # ---- file formats: the reference writes / reads the files itself ----
+    def write_seis(self, prefix, stage, seis):
+        """write_seis_AC: <prefix>_p_stage_<stage>.bin from complex [nf][nshots][ntr]."""
+        nf, ns, ntr = seis.shape
+        self.lib.ref_write_seis(os.fsencode(prefix), stage, nf, ns, ntr, _f32(seis.real).ravel(),
+                                _f32(seis.imag).ravel())
+
+    def read_seis(self, prefix, stage, nf, nshots, ntr):
+        """read_seis_AC of <prefix>_p_stage_<stage>.bin."""
+        re = np.zeros(nf * nshots * ntr, np.float32); im = np.zeros_like(re)
+        self.lib.ref_read_seis(os.fsencode(prefix), stage, nf, nshots, ntr, re, im)
+        return (re + 1j * im).astype(np.complex64).reshape(nf, nshots, ntr)
+
+    def writemod_true(self, path, grid, idx=1, idy=1):
+        self.lib.ref_writemod_true(os.fsencode(path), idx, idy, _f32(grid).ravel())
+
+    def writemod(self, path, grid, idx=1, idy=1):
+        self.lib.ref_writemod(os.fsencode(path), idx, idy, _f32(grid).ravel())
+
+    def readmod(self, mfile):
+        """readmod of <mfile>.vp / <mfile>.rho -> (vp, rho) [NY][NX] with the frame."""
+        vp = np.zeros(self.g.n, np.float32); rho = np.zeros_like(vp)
+        self.lib.ref_readmod(os.fsencode(mfile), vp, rho)
+        return vp.reshape(self.g.ny, self.g.nx), rho.reshape(self.g.ny, self.g.nx)
 
 
 def dropin_available() -> bool:

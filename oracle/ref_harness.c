@@ -25,6 +25,12 @@
  *   ass_grad_AC          src/AC/ass_grad_AC.c:11
  *   ass_grad_TE          src/TE/ass_grad_TE.c:11
  *   cp_grad_frame        src/cp_grad_frame.c:10
+ *   gauss_filt           src/gauss_filt.c:10
+ *   write_seis_AC        src/AC/write_seis_AC.c:10
+ *   read_seis_AC         src/AC/read_seis_AC.c:10
+ *   writemod_true        src/writemod_true.c:12
+ *   writemod             src/writemod.c:11   (format 3 via writedsk)
+ *   readmod              src/readmod.c:10
  */
 #include "fd.h"
 #include "globvar.h"
@@ -266,4 +272,75 @@ void ref_gauss_filt(float vref, float fc_low, float fsg, float fsg1, float *grad
     gauss_filt(gr);
     from_nr(gr, grad);
     free_matrix(gr, 0, NY + 1, 0, NX + 1);
+}
+
+/* write_seis_AC (src/AC/write_seis_AC.c:10): the file <prefix>_p_stage_<stage>.bin
+ * from flat [nf][nshots][ntr] real / imaginary parts */
+void ref_write_seis(const char *prefix, int stage, int nf, int nshots, int ntr, const float *re, const float *im)
+{
+    struct waveAC w;
+    int i, n = nf * nshots * ntr;
+    NF = nf; MYID = 0; INFO = 0;
+    snprintf(PICKS_FILE, STRING_SIZE, "%s", prefix);
+    w.precr = vector(1, n); w.preci = vector(1, n);
+    for (i = 1; i <= n; i++) { w.precr[i] = re[i - 1]; w.preci[i] = im[i - 1]; }
+    write_seis_AC(&w, nshots, ntr, stage);
+    free_vector(w.precr, 1, n); free_vector(w.preci, 1, n);
+}
+
+/* read_seis_AC (src/AC/read_seis_AC.c:10): the observed data of one stage */
+void ref_read_seis(const char *prefix, int stage, int nf, int nshots, int ntr, float *re, float *im)
+{
+    struct waveAC w;
+    int i, n = nf * nshots * ntr;
+    NF = nf; MYID = 1; INFO = 0;   /* MYID != 0 keeps the progress line off stdout */
+    snprintf(DATA_DIR, STRING_SIZE, "%s", prefix);
+    w.pobsr = vector(1, n); w.pobsi = vector(1, n);
+    read_seis_AC(&w, nshots, ntr, stage);
+    for (i = 1; i <= n; i++) { re[i - 1] = w.pobsr[i]; im[i - 1] = w.pobsi[i]; }
+    free_vector(w.pobsr, 1, n); free_vector(w.pobsi, 1, n);
+    MYID = 0;
+}
+
+/* writemod_true (src/writemod_true.c:12) of a flat [NY][NX] grid */
+void ref_writemod_true(const char *path, int idx, int idy, const float *grid)
+{
+    float **g = to_nr(grid);
+    char file[STRING_SIZE];
+    snprintf(file, STRING_SIZE, "%s", path);
+    IDX = idx; IDY = idy; MYID = 1;
+    writemod_true(file, g, 3);
+    MYID = 0;
+    free_matrix(g, 0, NY + 1, 0, NX + 1);
+}
+
+/* writemod (src/writemod.c:11) in binary format 3 */
+void ref_writemod(const char *path, int idx, int idy, const float *grid)
+{
+    float **g = to_nr(grid);
+    char file[STRING_SIZE];
+    snprintf(file, STRING_SIZE, "%s", path);
+    IDX = idx; IDY = idy; MYID = 1;
+    writemod(file, g, 3);
+    MYID = 0;
+    free_matrix(g, 0, NY + 1, 0, NX + 1);
+}
+
+/* readmod (src/readmod.c:10): <mfile>.vp and <mfile>.rho into flat [NY][NX]
+ * grids with the PML frame filled; readmod also writes <mfile>.germaine.vp
+ * and <mfile>.germaine.rho (full grids, writemod format 3) beside them. */
+void ref_readmod(const char *mfile, float *vp, float *rho)
+{
+    struct matAC m;
+    FILE *log = fopen("/dev/null", "w");
+    m.vp = matrix(0, NY + 1, 0, NX + 1);
+    m.rho = matrix(0, NY + 1, 0, NX + 1);
+    snprintf(MFILE, STRING_SIZE, "%s", mfile);
+    FP = log ? log : stderr; IDX = 1; IDY = 1; MYID = 1;
+    readmod(&m);
+    MYID = 0;
+    if (log) fclose(log);
+    from_nr(m.vp, vp); from_nr(m.rho, rho);
+    free_matrix(m.vp, 0, NY + 1, 0, NX + 1);
+    free_matrix(m.rho, 0, NY + 1, 0, NX + 1);
 }

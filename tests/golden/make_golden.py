@@ -4,8 +4,12 @@ present).  Each fixture holds one small seeded model, the reference's PML
 profiles and assembled triplets (init_A_*_9p_pml) and, for the acoustic
 cases, a right-hand side with its FP64 sparse solution on the operator
 UMFPACK factorises (M = A^T; solved with SciPy SuperLU because UMFPACK is
-not part of the reference tree).  Run:  python tests/golden/make_golden.py
+not part of the reference tree); postproc_gauss_filt.npz holds gauss_filt
+cases and files_formats.npz the bytes of the reference's seismogram and
+model files.  Run:  python tests/golden/make_golden.py [assembly] [gauss] [files]
+(no argument: all).
 """
+import tempfile
 import os
 import sys
 
@@ -29,6 +33,16 @@ CASES = [
 
 def main():
     out = os.path.dirname(os.path.abspath(__file__))
+    which = set(sys.argv[1:]) or {"assembly", "gauss", "files"}
+    if "assembly" in which:
+        assembly_fixtures(out)
+    if "gauss" in which:
+        gauss_filt_fixture(out)
+    if "files" in which:
+        files_fixture(out)
+
+
+def assembly_fixtures(out):
     for name, physics, nx, ny, dh, npml, fs, s, freq in CASES:
         g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml, free_surf=fs, s=s)
         if physics == 1:
@@ -50,7 +64,6 @@ def main():
             d["x"] = OS.DirectSolver(M).solve(b)
         np.savez_compressed(os.path.join(out, name + ".npz"), **d)
         print("wrote", name)
-    gauss_filt_fixture(out)
 
 
 # gauss_filt (src/gauss_filt.c) cases: grid, VREF, FC_low, FILT_SIZE_GRAD, FILT_SIZE_GRAD1
@@ -76,6 +89,49 @@ def gauss_filt_fixture(out):
         d[f"out_{k}"] = O.Ref(g).gauss_filt(grad, vref, fc, fs0, fs1)
     np.savez_compressed(os.path.join(out, "postproc_gauss_filt.npz"), **d)
     print("wrote postproc_gauss_filt")
+
+
+# file-format cases: grid nx, ny, npml, free_surf
+FILE_GRIDS = [(30, 22, 5, 0), (27, 19, 4, 1)]
+
+
+def files_fixture(out):
+    """files_formats.npz: for each grid k, seeded inputs (seis_k: seismograms
+    [nf][nshots][ntr]; grid_k: a full [NY][NX] float grid; vp_k, rho_k: the
+    interiors of a material file pair, x outer) and the files the reference
+    writes or the arrays it reads from them: seis_file_k (write_seis_AC),
+    true_file_k and true2_file_k (writemod_true, IDX = IDY = 1 and IDX = 2,
+    IDY = 3), full_file_k (writemod format 3), readmod_vp_k / readmod_rho_k
+    (readmod)."""
+    rng = np.random.default_rng(23)
+    d = {"ngrids": len(FILE_GRIDS)}
+    with tempfile.TemporaryDirectory() as tmp:
+        def rd(f):
+            with open(os.path.join(tmp, f), "rb") as fh:
+                return np.frombuffer(fh.read(), np.uint8)
+        for k, (nx, ny, npml, fs) in enumerate(FILE_GRIDS):
+            g = O.Grid(nx=nx, ny=ny, dh=10.0, npml=npml, free_surf=fs)
+            ref = O.Ref(g)
+            nf, ns, ntr = 3, 4, nx - 2 * npml
+            seis = (rng.standard_normal((nf, ns, ntr)) + 1j * rng.standard_normal((nf, ns, ntr))).astype(np.complex64)
+            grid = rng.standard_normal((ny, nx)).astype(np.float32)
+            nx0, ny0 = nx - 2 * npml, ny - npml - g.fsshift
+            vp = rng.uniform(1500, 4500, (nx0, ny0)).astype(np.float32)
+            rho = rng.uniform(1000, 2600, (nx0, ny0)).astype(np.float32)
+            ref.write_seis(os.path.join(tmp, f"picks{k}"), 2, seis)
+            ref.writemod_true(os.path.join(tmp, "t1"), grid)
+            ref.writemod_true(os.path.join(tmp, "t2"), grid, 2, 3)
+            ref.writemod(os.path.join(tmp, "f1"), grid)
+            mfile = os.path.join(tmp, f"model{k}")
+            vp.tofile(mfile + ".vp")
+            rho.tofile(mfile + ".rho")
+            rvp, rrho = ref.readmod(mfile)
+            d.update({f"case_{k}": np.array([nx, ny, npml, fs]), f"seis_{k}": seis, f"grid_{k}": grid,
+                      f"vp_{k}": vp, f"rho_{k}": rho, f"seis_file_{k}": rd(f"picks{k}_p_stage_2.bin"),
+                      f"true_file_{k}": rd("t1"), f"true2_file_{k}": rd("t2"), f"full_file_{k}": rd("f1"),
+                      f"readmod_vp_{k}": rvp, f"readmod_rho_{k}": rrho})
+    np.savez_compressed(os.path.join(out, "files_formats.npz"), **d)
+    print("wrote files_formats")
 
 
 if __name__ == "__main__":

@@ -99,8 +99,9 @@ def test_port_shot_arithmetic_equals_reference(physics):
 
 
 def _golden_files():
-    """assembly / solve fixtures (the post-processing fixtures have their own tests)"""
-    return (sorted(f for f in os.listdir(GOLDEN) if f.endswith(".npz") and not f.startswith("postproc_"))
+    """assembly / solve fixtures (the post-processing and file-format fixtures have their own tests)"""
+    return (sorted(f for f in os.listdir(GOLDEN)
+                   if f.endswith(".npz") and not f.startswith(("postproc_", "files_")))
             if os.path.isdir(GOLDEN) else [])
 
 
