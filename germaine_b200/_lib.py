@@ -19,6 +19,8 @@ GM_WARNING_NOT_CONVERGED = 2
 GM_ERROR_OUT_OF_MEMORY = -1
 GM_ERROR_INVALID = -2
 GM_SEIS_KEEP_LAST = 1
+GM_HESS_GREEN = 1
+GM_HESS_SHIN = 2
 GM_ERROR_STATE = -3
 GM_ERROR_CUDA = -4
 GM_ERROR_NONFINITE = -5
@@ -56,7 +58,7 @@ class GmStats(ctypes.Structure):
 EXPORTS = [
     "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats", "gm_engine_stream",
     "gm_set_model", "gm_set_models", "gm_factor", "gm_factor_models", "gm_factor_values", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
-    "gm_get_gradient_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc",
+    "gm_get_gradient_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_hessian", "gm_get_hessian_fp64", "gm_apply_hess",
     "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_cgemm_sub_c64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
@@ -111,6 +113,9 @@ def load() -> ctypes.CDLL:
     lib.gm_get_gradient_fp64.argtypes = [vp, vp, vp]
     f32 = ctypes.c_float
     lib.gm_gauss_filt.argtypes = [i32, i32, i32, f32, f32, f32, f32, f32, vp, vp]
+    lib.gm_hessian.argtypes = [vp, i32, i32, vp, vp, i32, vp, vp, vp, vp]
+    lib.gm_get_hessian_fp64.argtypes = [vp, vp, vp]
+    lib.gm_apply_hess.argtypes = [i32, i32, f32, vp, vp, vp]
     cp = ctypes.c_char_p
     lib.gm_write_seis.argtypes = [cp, i32, i32, i32, i32, vp]
     lib.gm_read_seis.argtypes = [cp, i32, i32, i32, vp]

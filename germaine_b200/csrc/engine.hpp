@@ -82,6 +82,7 @@ struct gm_engine {
     gm::DevBuf d_src_k, d_rec_k, d_seis, d_field, d_res, d_grad, d_frame, d_frame_pass, d_misc;
     gm::DevBuf d_xf, d_xa;   // forward / adjoint solutions kept for the gradient
     std::vector<double> last_grad0, last_grad1;
+    std::vector<double> last_hess0, last_hess1;
 
     gm_stats stats{};
     cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_s0 = nullptr, ev_s1 = nullptr;

@@ -1,6 +1,7 @@
 // gm_forward / gm_grad_obj / gm_obj: the per-frequency drivers of the
 // reference (forward_shot_AC, grad_obj_AC, obj_AC and their TE/SH twins)
 // over every shot and every frequency of the factorised batch at once.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 #include <vector>
@@ -74,13 +75,15 @@ int upload(gm::DevBuf &buf, const std::vector<T> &v, cudaStream_t st) {
     return GM_OK;
 }
 
-// spike right-hand sides of every shot and frequency into e->d_b, forward solve into xout
-int forward_solve(gm_engine *e, int ns, const Geometry &g, double2 *xout) {
+// spike right-hand sides of every shot and frequency into e->d_b, forward solve into xout;
+// the spike amplitude is that of src_physics's source routine (RHS_source_AC / _TE)
+int forward_solve(gm_engine *e, int ns, const Geometry &g, double2 *xout, int src_physics = 0) {
     const int nf = e->nf, n = e->n;
+    if (!src_physics) src_physics = e->cfg.physics;
     std::vector<double2> amp(nf);
     for (int f = 0; f < nf; ++f) {
         double a[2];
-        gmh_source_amp(e->cfg.physics, e->freqs[f], e->cfg.s, e->cfg.dh, a);
+        gmh_source_amp(src_physics, e->freqs[f], e->cfg.s, e->cfg.dh, a);
         amp[f] = make_double2(a[0], a[1]);
     }
     int rc;
@@ -93,6 +96,27 @@ int forward_solve(gm_engine *e, int ns, const Geometry &g, double2 *xout) {
     rc = gm::engine_solve_device(e, GM_SYS_A, ns, xout, e->d_b.as<double2>());
     GM_CUDA(cudaStreamSynchronize(e->st));  // amp_buf is released on return
     return rc;
+}
+
+// cp_grad_frame's taper (coefficient and number of passes per grid point) on the device
+int ensure_frame(gm_engine *e) {
+    if (e->d_frame.p) return GM_OK;
+    const int n = e->n;
+    std::vector<float> coef(n);
+    std::vector<unsigned char> passes(n);
+    gmh_grad_frame(e->cfg.nx, e->cfg.ny, e->cfg.npml, e->cfg.free_surf, coef.data(), passes.data());
+    int rc;
+    if ((rc = upload(e->d_frame, coef, e->st))) return rc;
+    if ((rc = upload(e->d_frame_pass, passes, e->st))) return rc;
+    GM_CUDA(cudaStreamSynchronize(e->st));   // the host vectors are released on return
+    return GM_OK;
+}
+
+int single_model(const gm_engine *e, const char *who) {
+    for (int m : e->models)
+        if (m != e->models[0])
+            return fail(GM_ERROR_STATE, "%s: the factorised matrices come from different models", who);
+    return GM_OK;
 }
 
 int check_ready(const gm_engine *e, int ns, int ntr) {
@@ -227,9 +251,7 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     if (rc) return rc;
     if (!pobs || ntr <= 0) return fail(GM_ERROR_INVALID, "gm_grad_obj: need observed data and receivers");
     if (misfit < 1 || misfit > 3) return fail(GM_ERROR_INVALID, "gm_grad_obj: MISFIT must be 1, 2 or 3");
-    for (int m : e->models)   // one gradient: every matrix of the batch from the same model
-        if (m != e->models[0])
-            return fail(GM_ERROR_STATE, "gm_grad_obj: the factorised matrices come from different models");
+    if ((rc = single_model(e, "gm_grad_obj"))) return rc;   // one gradient: one model
     const bool te = e->cfg.physics == GM_PHYS_TE;
     GM_CUDA(cudaSetDevice(e->device));
     Geometry g;
@@ -256,13 +278,7 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     if (arc > worst) worst = arc;
 
     // gradient stack + PML frame taper
-    if (!e->d_frame.p) {
-        std::vector<float> coef(n);
-        std::vector<unsigned char> passes(n);
-        gmh_grad_frame(e->cfg.nx, e->cfg.ny, e->cfg.npml, e->cfg.free_surf, coef.data(), passes.data());
-        if ((rc = upload(e->d_frame, coef, e->st))) return rc;
-        if ((rc = upload(e->d_frame_pass, passes, e->st))) return rc;
-    }
+    if ((rc = ensure_frame(e))) return rc;
     std::vector<double2> om2(nf), om(nf);
     for (int f = 0; f < nf; ++f) {
         float a[2], b[2];
@@ -309,5 +325,113 @@ extern "C" int gm_get_gradient_fp64(gm_engine *e, double *g0, double *g1) {
     if (e->last_grad0.empty()) return fail(GM_ERROR_STATE, "no gradient computed yet");
     if (g0) std::memcpy(g0, e->last_grad0.data(), e->last_grad0.size() * sizeof(double));
     if (g1 && !e->last_grad1.empty()) std::memcpy(g1, e->last_grad1.data(), e->last_grad1.size() * sizeof(double));
+    return GM_OK;
+}
+
+// Diagonal Hessian estimators of the reference, over every shot and every
+// factorised frequency:
+//   GM_HESS_SHIN   hessian_shin_AC (src/AC/hessian_shin_AC.c:102-132) and
+//                  hessian_shin_TE: sum over shots of |J|^2 with
+//                  J = 2 Omega^2 F / (rho vp^3) (AC), iOmega F and Omega^2 F (TE);
+//   GM_HESS_GREEN  hessian_AC (src/AC/hessian_AC.c:134-165) and hessian_TE:
+//                  J also multiplied by the Green's function G_r of every
+//                  receiver (a spike at the receiver, RHS_source_AC_hess).
+// The reference solves ntr Green's functions for every shot; they do not
+// depend on the shot, so here they are solved once per frequency (in blocks
+// of receivers) and, since |a F_s G_r|^2 = |a|^2 |F_s|^2 |G_r|^2, the double
+// sum over (shot, receiver) is the product of a shot sum and a receiver sum
+// per grid point.  Both sums and the result are FP64; the cp_grad_frame
+// taper follows (src/AC/hessian_AC.c:174-175).
+extern "C" int gm_hessian(gm_engine *e, int mode, int nshots, const float *src_x, const float *src_y, int ntr,
+                          const int32_t *rec_x, const int32_t *rec_y, float *hess0, float *hess1) {
+    int rc = check_ready(e, nshots, ntr);
+    if (rc) return rc;
+    if (mode != GM_HESS_SHIN && mode != GM_HESS_GREEN) return fail(GM_ERROR_INVALID, "gm_hessian: unknown mode %d", mode);
+    if (mode == GM_HESS_GREEN && ntr <= 0) return fail(GM_ERROR_INVALID, "gm_hessian: GM_HESS_GREEN needs receivers");
+    if (e->cfg.physics == GM_PHYS_SH) return fail(GM_ERROR_INVALID, "gm_hessian: the reference has no SH Hessian");
+    if ((rc = single_model(e, "gm_hessian"))) return rc;
+    const bool te = e->cfg.physics == GM_PHYS_TE;
+    GM_CUDA(cudaSetDevice(e->device));
+    Geometry g;
+    if ((rc = make_geometry(e, nshots, src_x, src_y, mode == GM_HESS_GREEN ? ntr : 0, rec_x, rec_y, g))) return rc;
+    const int nf = e->nf, n = e->n;
+
+    // |F|^2 summed over shots.  hessian_shin_TE models its forward fields with
+    // RHS_source_AC (src/TE/hessian_shin_TE.c:108), a spike of amplitude
+    // 1/DH^2 without the -i Omega mu0 of RHS_source_TE; hessian_TE uses
+    // RHS_source_TE (src/TE/hessian_TE.c:113).
+    GM_ALLOC(e->d_xf, (size_t)nf * n * nshots * sizeof(double2));
+    const int src_phys = (te && mode == GM_HESS_SHIN) ? GM_PHYS_AC : e->cfg.physics;
+    int worst = forward_solve(e, nshots, g, e->d_xf.as<double2>(), src_phys);
+    if (worst < 0) return worst;
+    gm::DevBuf sq;
+    GM_ALLOC(sq, 2 * (size_t)nf * n * sizeof(double));
+    double *sqf = sq.as<double>(), *sqg = sqf + (size_t)nf * n;
+    gm::launch_hess_sq(e->d_xf.as<double2>(), n, nf, nshots, sqf, 0, e->st);
+    GM_CUDA(cudaGetLastError());
+
+    // |G|^2 summed over receivers, the Green's functions solved in blocks
+    if (mode == GM_HESS_GREEN) {
+        const int blk = std::min(ntr, std::max(nshots, 32));
+        const double a = gmh_hess_green_amp(e->cfg.physics, e->cfg.dh);
+        std::vector<double2> amp(nf, make_double2(a, 0.0));
+        gm::DevBuf amp_buf;
+        if ((rc = upload(amp_buf, amp, e->st))) return rc;
+        if ((rc = upload(e->d_rec_k, g.kadj, e->st))) return rc;
+        GM_ALLOC(e->d_b, (size_t)nf * n * blk * sizeof(double2));
+        GM_ALLOC(e->d_xa, (size_t)nf * n * blk * sizeof(double2));
+        for (int r0 = 0; r0 < ntr; r0 += blk) {
+            const int nr = std::min(blk, ntr - r0);
+            gm::launch_spikes(e->d_b.as<double2>(), n, nf, nr, e->d_rec_k.as<int>() + r0, amp_buf.as<double2>(), e->st);
+            GM_CUDA(cudaGetLastError());
+            // the reference solves with UMFPACK_A for both physics (src/AC/hessian_AC.c:140, src/TE/hessian_TE.c:140)
+            const int src = gm::engine_solve_device(e, GM_SYS_A, nr, e->d_xa.as<double2>(), e->d_b.as<double2>());
+            if (src < 0) return src;
+            if (src > worst) worst = src;
+            gm::launch_hess_sq(e->d_xa.as<double2>(), n, nf, nr, sqg, r0 > 0, e->st);
+            GM_CUDA(cudaGetLastError());
+        }
+        GM_CUDA(cudaStreamSynchronize(e->st));   // amp_buf is released on return
+    }
+
+    if ((rc = ensure_frame(e))) return rc;
+    std::vector<double> w(2 * nf);
+    for (int f = 0; f < nf; ++f) {
+        float o2[2], o[2];
+        gmh_gradient_scalars(e->cfg.physics, e->freqs[f], e->cfg.s, o2, o);
+        const double a2 = (double)o2[0] * o2[0] + (double)o2[1] * o2[1];   // |Omega^2|^2
+        const double a1 = (double)o[0] * o[0] + (double)o[1] * o[1];       // |Omega|^2 = |i Omega|^2
+        w[f] = te ? a1 : 4.0 * a2;                                          // AC: |2 Omega^2|^2
+        w[nf + f] = te ? a2 : 0.0;
+    }
+    gm::DevBuf wbuf;
+    if ((rc = upload(wbuf, w, e->st))) return rc;
+    GM_ALLOC(e->d_grad, 2 * (size_t)n * sizeof(double));
+    GM_ALLOC(e->d_misc, 2 * (size_t)n * sizeof(float));
+    gm::HessArgs ha{};
+    ha.n = n; ha.nf = nf; ha.te = te;
+    ha.sqf = sqf; ha.sqg = mode == GM_HESS_GREEN ? sqg : nullptr;
+    ha.w0 = wbuf.as<double>(); ha.w1 = ha.w0 + nf;
+    ha.m0 = e->d_m0.as<float>() + (size_t)e->models[0] * n; ha.m1 = e->d_m1.as<float>() + (size_t)e->models[0] * n;
+    ha.frame = e->d_frame.as<float>(); ha.passes = e->d_frame_pass.as<unsigned char>();
+    ha.h0 = e->d_grad.as<double>(); ha.h1 = ha.h0 + n;
+    ha.f0 = e->d_misc.as<float>(); ha.f1 = ha.f0 + n;
+    gm::launch_hess_final(ha, e->st);
+    GM_CUDA(cudaGetLastError());
+    e->last_hess0.resize(n);
+    e->last_hess1.assign(te ? n : 0, 0.0);
+    GM_CUDA(cudaMemcpyAsync(e->last_hess0.data(), ha.h0, n * sizeof(double), cudaMemcpyDeviceToHost, e->st));
+    if (te) GM_CUDA(cudaMemcpyAsync(e->last_hess1.data(), ha.h1, n * sizeof(double), cudaMemcpyDeviceToHost, e->st));
+    if (hess0) GM_CUDA(cudaMemcpyAsync(hess0, ha.f0, n * sizeof(float), cudaMemcpyDefault, e->st));
+    if (hess1 && te) GM_CUDA(cudaMemcpyAsync(hess1, ha.f1, n * sizeof(float), cudaMemcpyDefault, e->st));
+    GM_CUDA(cudaStreamSynchronize(e->st));
+    return worst;
+}
+
+extern "C" int gm_get_hessian_fp64(gm_engine *e, double *h0, double *h1) {
+    if (!e) return fail(GM_ERROR_INVALID, "null engine");
+    if (e->last_hess0.empty()) return fail(GM_ERROR_STATE, "no Hessian computed yet");
+    if (h0) std::memcpy(h0, e->last_hess0.data(), e->last_hess0.size() * sizeof(double));
+    if (h1 && !e->last_hess1.empty()) std::memcpy(h1, e->last_hess1.data(), e->last_hess1.size() * sizeof(double));
     return GM_OK;
 }

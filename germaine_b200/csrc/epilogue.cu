@@ -206,4 +206,68 @@ void launch_gradient(const GradArgs &a, cudaStream_t st) {
     (k_gradient<<<(a.n + 127) / 128, 128, 0, st>>>(a), note_launch());
 }
 
+// sq[f][k] (+)= sum_s |field(k)|^2 over the ns solutions of frequency f, the
+// field read through the vec2mat shift: the |F|^2 (shots) and |G|^2
+// (receiver Green's functions) factors of the diagonal Hessians.
+__global__ void k_hess_sq(const double2 *__restrict__ x, int n, int nf, int ns, double *sq, int accumulate) {
+    const size_t t = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= (size_t)nf * n) return;
+    const int k = (int)(t % n), f = (int)(t / n);
+    double acc = 0.0;
+    if (k + 1 < n) {
+        const double2 *row = x + ((size_t)f * n + k + 1) * ns;
+        for (int s = 0; s < ns; ++s) {
+            const double2 v = __ldg(row + s);
+            acc += v.x * v.x + v.y * v.y;
+        }
+    }
+    sq[t] = accumulate ? sq[t] + acc : acc;
+}
+
+void launch_hess_sq(const double2 *x, int n, int nf, int ns, double *sq, int accumulate, cudaStream_t st) {
+    const size_t tot = (size_t)nf * n;
+    (k_hess_sq<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(x, n, nf, ns, sq, accumulate), note_launch());
+}
+
+// h0/h1[k] = taper^passes * sum_f w_f * sqf[f][k] (* sqg[f][k]) (* mat^2):
+// |J|^2 of hessian_shin_AC / hessian_AC and the TE twins summed over shots
+// (and receivers), with |a F G|^2 = |a|^2 |F|^2 |G|^2 so the shot and
+// receiver sums factor.
+__global__ void k_hess_final(HessArgs a) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n) return;
+    double h0 = 0.0, h1 = 0.0;
+    for (int f = 0; f < a.nf; ++f) {
+        double v = a.sqf[(size_t)f * a.n + k];
+        if (a.sqg) v *= a.sqg[(size_t)f * a.n + k];
+        h0 += a.w0[f] * v;
+        if (a.te) h1 += a.w1[f] * v;
+    }
+    if (!a.te) {
+        const double vp = a.m0[k], rho = a.m1[k];
+        const double mat = 1.0 / (rho * vp * vp * vp);
+        h0 *= mat * mat;
+    }
+    // the float output follows the reference's order: the Hessian is a float
+    // array when cp_grad_frame tapers it, so a frame point whose untapered
+    // sum exceeds the float range is inf there, as in the reference
+    const float c = a.frame[k];
+    const int p = a.passes[k];
+    float v0 = __double2float_rn(h0), v1 = __double2float_rn(h1);
+    for (int q = 0; q < p; ++q) {
+        h0 *= c; h1 *= c;
+        v0 = __fmul_rn(v0, c); v1 = __fmul_rn(v1, c);
+    }
+    a.h0[k] = h0;
+    a.f0[k] = v0;
+    if (a.te) {
+        a.h1[k] = h1;
+        a.f1[k] = v1;
+    }
+}
+
+void launch_hess_final(const HessArgs &a, cudaStream_t st) {
+    (k_hess_final<<<(a.n + 127) / 128, 128, 0, st>>>(a), note_launch());
+}
+
 }  // namespace gm

@@ -108,6 +108,17 @@ void gmh_source_amp(int physics, float freq, float s, float dh, double amp[2])
     amp[1] = ai / (dh * dh);
 }
 
+/* Amplitude of the receiver spike of the Hessian's Green's functions:
+ * AC amp/(DH*DH) with float amp = 1 (src/AC/RHS_source_AC_hess.c:26-33, a
+ * float quotient); TE 1.0/(DH*DH) (src/TE/RHS_source_TE_hess.c:38, a double
+ * quotient). */
+double gmh_hess_green_amp(int physics, float dh)
+{
+    if (physics == 4) return 1.0 / (dh * dh);
+    const float amp = 1.0f;
+    return amp / (dh * dh);
+}
+
 /* Gradient scalars: AC Omega^2 = cpowf((2 pi f) - iS, 2) (ass_grad_AC.c:22);
  * TE Omega = 2 pi (f + iS), Omega^2 = cpowf(2 pi (f + iS), 2)
  * (ass_grad_TE.c:22-23). */

@@ -10,6 +10,7 @@ void gmh_pml(int nx, int ny, float dh, int npml, int free_surf, float a0_pml, fl
 void gmh_assembly_scalars(int physics, float freq, float s, float om2[2], float om[2], float om2mu0[2]);
 void gmh_source_amp(int physics, float freq, float s, float dh, double amp[2]);
 void gmh_gradient_scalars(int physics, float freq, float s, float om2[2], float om[2]);
+double gmh_hess_green_amp(int physics, float dh);
 void gmh_stf_unit(const float stf[2], float unit[2]);
 void gmh_wiener(const float num[2], const float den[2], float wien[2]);
 void gmh_grad_frame(int nx, int ny, int npml, int free_surf, float *coef, unsigned char *passes);

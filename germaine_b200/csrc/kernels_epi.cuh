@@ -17,6 +17,17 @@ struct GradArgs {
     double *g0, *g1;            // [n] outputs (FP64)
 };
 
+struct HessArgs {
+    int n, nf, te;
+    const double *sqf, *sqg;    // [nf][n] sums of |F|^2 over shots, |G|^2 over receivers (sqg NULL: shin)
+    const double *w0, *w1;      // per frequency |coefficient|^2 of J (AC: |2 Omega^2|^2; TE: |Omega|^2, |Omega^2|^2)
+    const float *m0, *m1;       // vp, rho (AC)
+    const float *frame;
+    const unsigned char *passes;
+    double *h0, *h1;            // [n] outputs (FP64)
+    float *f0, *f1;             // [n] float outputs: the sum rounded to float, then tapered in float
+};
+
 void launch_spikes(double2 *b, int n, int nf, int ns, const int *ksrc, const double2 *amp, cudaStream_t st);
 void launch_gather_seis(const double2 *x, int n, int nf, int ns, int ntr, const int *krec, float2 *seis, double2 *cal,
                         cudaStream_t st);
@@ -26,5 +37,7 @@ void launch_residual_shot(const double2 *cal, const float2 *obs, int nfs, int nt
 void launch_adjoint_src(double2 *b, int n, int nf, int ns, int ntr, const int *kadj, const double2 *res, double dh2,
                         cudaStream_t st);
 void launch_gradient(const GradArgs &a, cudaStream_t st);
+void launch_hess_sq(const double2 *x, int n, int nf, int ns, double *sq, int accumulate, cudaStream_t st);
+void launch_hess_final(const HessArgs &a, cudaStream_t st);
 
 }  // namespace gm

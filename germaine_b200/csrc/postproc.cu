@@ -7,6 +7,8 @@
 // separately rounded products and sums, so the result is bit-identical.
 // HBM-bound: the gradient is read through L1 (each value is reused by every
 // output cell whose window covers it), one float per cell written.
+#include <algorithm>
+#include <cstring>
 #include <vector>
 
 #include "common.hpp"
@@ -74,5 +76,69 @@ extern "C" int gm_gauss_filt(int device, int nx, int ny, float dh, float vref, f
     cudaFree(din);
     cudaFree(dout);
     cudaFree(dw);
+    return rc;
+}
+
+// ---- apply_hess_AC (src/AC/apply_hess_AC.c:11-40) ----
+// MAX_HESS = max |hess| (NaN entries never pass the reference's ">" test,
+// fmaxf skips them alike); grad *= 1.0 / (hess + EPS_HESS * MAX_HESS) with
+// the reference's types: the denominator summed in float, the reciprocal and
+// the product in double, the result rounded to float.  The maximum of
+// non-negative floats is the maximum of their bit patterns, so the
+// reduction is an atomicMax on the bits and does not depend on the order.
+namespace gm {
+
+__global__ void __launch_bounds__(256) k_hess_max(const float *__restrict__ hess, size_t n, unsigned *maxbits) {
+    float m = 0.0f;
+    for (size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (size_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, fabsf(hess[k]));
+    for (int o = 16; o > 0; o >>= 1) m = fmaxf(m, __shfl_xor_sync(0xffffffffu, m, o));
+    if ((threadIdx.x & 31) == 0) atomicMax(maxbits, __float_as_uint(m));
+}
+
+__global__ void __launch_bounds__(256) k_apply_hess(float *__restrict__ grad, const float *__restrict__ hess, size_t n,
+                                                    float eps_hess, const unsigned *maxbits) {
+    const size_t k = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float em = __fmul_rn(eps_hess, __uint_as_float(*maxbits));
+    const double q = __ddiv_rn(1.0, (double)__fadd_rn(hess[k], em));
+    grad[k] = __double2float_rn(__dmul_rn((double)grad[k], q));
+}
+
+}  // namespace gm
+
+extern "C" int gm_apply_hess(int device, int n, float eps_hess, float *grad, const float *hess, float *max_hess) {
+    if (n <= 0 || !grad || !hess) return gm::fail(GM_ERROR_INVALID, "gm_apply_hess: bad argument");
+    if (cudaSetDevice(device) != cudaSuccess) return gm::fail(GM_ERROR_CUDA, "gm_apply_hess: bad device %d", device);
+    const size_t bytes = (size_t)n * sizeof(float);
+    float *dg = nullptr, *dh = nullptr;
+    unsigned *dmax = nullptr;
+    int rc = GM_OK;
+    if (cudaMalloc(&dg, bytes) != cudaSuccess || cudaMalloc(&dh, bytes) != cudaSuccess ||
+        cudaMalloc(&dmax, sizeof(unsigned)) != cudaSuccess) {
+        rc = gm::fail(GM_ERROR_OUT_OF_MEMORY, "gm_apply_hess: device allocation failed");
+    } else if (cudaMemcpy(dg, grad, bytes, cudaMemcpyDefault) != cudaSuccess ||
+               cudaMemcpy(dh, hess, bytes, cudaMemcpyDefault) != cudaSuccess ||
+               cudaMemset(dmax, 0, sizeof(unsigned)) != cudaSuccess) {
+        rc = gm::fail(GM_ERROR_CUDA, "gm_apply_hess: upload failed");
+    } else {
+        const int tpb = 256;
+        const unsigned nblk = (unsigned)std::min<size_t>(((size_t)n + tpb - 1) / tpb, 148 * 8);
+        gm::k_hess_max<<<nblk, tpb>>>(dh, (size_t)n, dmax);
+        gm::note_launch();
+        gm::k_apply_hess<<<(unsigned)(((size_t)n + tpb - 1) / tpb), tpb>>>(dg, dh, (size_t)n, eps_hess, dmax);
+        gm::note_launch();
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) e = cudaMemcpy(grad, dg, bytes, cudaMemcpyDefault);
+        unsigned bits = 0;
+        if (e == cudaSuccess && max_hess) {
+            e = cudaMemcpy(&bits, dmax, sizeof(unsigned), cudaMemcpyDeviceToHost);
+            std::memcpy(max_hess, &bits, sizeof(float));
+        }
+        if (e != cudaSuccess) rc = gm::fail(GM_ERROR_CUDA, "gm_apply_hess: %s", cudaGetErrorString(e));
+    }
+    cudaFree(dg);
+    cudaFree(dh);
+    cudaFree(dmax);
     return rc;
 }

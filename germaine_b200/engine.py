@@ -213,6 +213,26 @@ class Engine:
         check(self.lib.gm_get_gradient_fp64(self._h, ptr(g0), ptr(g1)))
         return g0, g1
 
+    def hessian(self, src_x, src_y, rec_x=None, rec_y=None, mode: int = _lib.GM_HESS_SHIN):
+        """Diagonal Hessian (gm_hessian): mode GM_HESS_SHIN (hessian_shin_AC,
+        shots only) or GM_HESS_GREEN (hessian_AC, shots x receivers).
+        Returns (hess0, hess1); hess1 is None for AC and the epsilon Hessian
+        for TE (hess0 = sigma Hessian)."""
+        sx = _c(src_x, np.float32); sy = _c(src_y, np.float32)
+        rx = _c(rec_x if rec_x is not None else [], np.int32)
+        ry = _c(rec_y if rec_y is not None else [], np.int32)
+        h0 = np.zeros(self.n, np.float32)
+        h1 = np.zeros(self.n, np.float32) if self.physics == GM_PHYS_TE else None
+        self.last_status = check(self.lib.gm_hessian(self._h, mode, sx.size, ptr(sx), ptr(sy), rx.size, ptr(rx),
+                                                     ptr(ry), ptr(h0), ptr(h1)))
+        return h0, h1
+
+    def hessian_fp64(self):
+        h0 = np.zeros(self.n)
+        h1 = np.zeros(self.n) if self.physics == GM_PHYS_TE else None
+        check(self.lib.gm_get_hessian_fp64(self._h, ptr(h0), ptr(h1)))
+        return h0, h1
+
     def obj(self, src_x, src_y, rec_x, rec_y, pobs, stf_inv: int = 0, misfit: int = 1) -> float:
         sx = _c(src_x, np.float32); sy = _c(src_y, np.float32)
         rx = _c(rec_x, np.int32); ry = _c(rec_y, np.int32)
@@ -221,6 +241,18 @@ class Engine:
         self.last_status = check(self.lib.gm_obj(self._h, sx.size, ptr(sx), ptr(sy), rx.size, ptr(rx), ptr(ry),
                                                  ptr(obs), stf_inv, misfit, ctypes.byref(l2)))
         return float(l2.value)
+
+
+def apply_hess(grad, hess, eps_hess: float, device: int = 0):
+    """apply_hess_AC on the GPU (gm_apply_hess, bit-identical): returns
+    (preconditioned gradient, MAX_HESS)."""
+    g = np.array(grad, np.float32, copy=True, order="C")
+    h = _c(hess, np.float32)
+    if g.size != h.size:
+        raise ValueError("gradient and Hessian differ in size")
+    mx = ctypes.c_float(0.0)
+    check(_lib.load().gm_apply_hess(device, g.size, eps_hess, ptr(g), ptr(h), ctypes.byref(mx)))
+    return g, float(mx.value)
 
 
 def gauss_filt(grad, dh: float, vref: float, fc_low: float, filt_size_grad: float, filt_size_grad1: float,

@@ -48,6 +48,10 @@ extern "C" {
                           overwrite at src/AC/forward_shot_AC.c:41-48 */
 #define GM_OP_EXACT 1  /* M = A: the assembled stencil rows */
 
+/* ---- diagonal Hessian estimators (the reference's HESSIAN parameter) ---- */
+#define GM_HESS_GREEN 1  /* hessian_AC / hessian_TE: shot and receiver Green's functions */
+#define GM_HESS_SHIN  2  /* hessian_shin_AC / hessian_shin_TE (Shin et al. 2001): shots only */
+
 /* ---- solve system (umfpack_zi_solve sys argument) ---- */
 #define GM_SYS_A   0   /* M x = b   (UMFPACK_A)   */
 #define GM_SYS_AT  1   /* M^T x = b (UMFPACK_Aat, non-conjugate transpose) */
@@ -190,6 +194,30 @@ int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y
  * ([NY][NX] each; g1 ignored for AC).  Either pointer may be NULL. */
 int gm_get_gradient_fp64(gm_engine *e, double *g0, double *g1);
 
+/* Diagonal of the approximate Hessian over all shots of all factorised
+ * frequencies, frame-tapered by cp_grad_frame:
+ *   mode GM_HESS_SHIN   hessian_shin_AC (src/AC/hessian_shin_AC.c:48-141) /
+ *                       hessian_shin_TE: sum over shots of |J|^2,
+ *                       J = 2 Omega^2 F / (rho vp^3) (AC), i Omega F and
+ *                       Omega^2 F (TE), F the forward wavefield;
+ *   mode GM_HESS_GREEN  hessian_AC (src/AC/hessian_AC.c:48-174) /
+ *                       hessian_TE: J further multiplied by the Green's
+ *                       function of each receiver (spike source
+ *                       RHS_source_AC_hess / RHS_source_TE_hess), summed over
+ *                       shots and receivers (rec_x/rec_y as in gm_forward).
+ *   hess0  [NY][NX] AC: vp Hessian; TE: sigma Hessian (hess_sigma);
+ *   hess1  [NY][NX] TE: epsilon Hessian (NULL for AC).
+ * Accumulated in FP64 (gm_get_hessian_fp64), returned as float.  The TE
+ * results are not multiplied by MAT1_NORM^2 / MAT2_NORM^2
+ * (src/TE/hessian_TE.c:187-188): as for the gradient, the caller scales.
+ * One material model for the whole batch; SH has no Hessian in the
+ * reference (GM_ERROR_INVALID). */
+int gm_hessian(gm_engine *e, int mode, int nshots, const float *src_x, const float *src_y,
+               int ntr, const int32_t *rec_x, const int32_t *rec_y, float *hess0, float *hess1);
+
+/* The last gm_hessian results before rounding to float, in FP64. */
+int gm_get_hessian_fp64(gm_engine *e, double *h0, double *h1);
+
 /* Objective only (obj_AC, src/AC/obj_AC.c:10-145). */
 int gm_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y,
            int ntr, const int32_t *rec_x, const int32_t *rec_y,
@@ -212,6 +240,14 @@ int gm_obj_each(gm_engine *e, int nshots, const float *src_x, const float *src_y
  * to the reference's float result. */
 int gm_gauss_filt(int device, int nx, int ny, float dh, float vref, float fc_low, float filt_size_grad,
                   float filt_size_grad1, const float *grad, float *out);
+
+/* Apply the diagonal Hessian to a gradient on the GPU: apply_hess_AC
+ * (src/AC/apply_hess_AC.c:11-40), also used for both TE parameters
+ * (src/TE/fwi_FD_TE.c:287-288).  MAX_HESS = max |hess| (returned in
+ * *max_hess when not NULL), then grad *= 1 / (hess + eps_hess * MAX_HESS)
+ * in the reference's float / double arithmetic: bit-identical.  grad and
+ * hess are n floats in host or device memory; grad is updated in place. */
+int gm_apply_hess(int device, int n, float eps_hess, float *grad, const float *hess, float *max_hess);
 
 /* ---- the reference's file formats (host stdio, no GPU needed) ---- */
 #define GM_SEIS_KEEP_LAST 1  /* gm_write_seis: write the last sample as given */

@@ -107,6 +107,8 @@ def load_port():
         lib.port_cp_grad_frame.argtypes = [P, _f32p]
         lib.port_gradient_scalars.argtypes = [P, ctypes.c_int, ctypes.c_float, _f32p, _f32p]
         lib.port_gauss_filt.argtypes = [P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f32p]
+        lib.port_apply_hess.argtypes = [ctypes.c_int, ctypes.c_float, _f32p, _f32p]
+        lib.port_apply_hess.restype = ctypes.c_float
         _port_lib = lib
     return _port_lib
 
@@ -142,8 +144,23 @@ def load_ref():
         lib.ref_writemod_true.argtypes = [cp, i, i, _f32p]
         lib.ref_writemod.argtypes = [cp, i, i, _f32p]
         lib.ref_readmod.argtypes = [cp, _f32p, _f32p]
+        lib.ref_apply_hess.argtypes = [ctypes.c_float, _f32p, _f32p]
+        lib.ref_apply_hess.restype = ctypes.c_float
         _ref_lib = lib
     return _ref_lib
+
+
+# the reference formats file names into char[STRING_SIZE] buffers (include/fd.h:27)
+REF_STRING_SIZE = 74
+
+
+def _ref_name(path, longest_suffix: str) -> bytes:
+    """A path the reference will extend by at most longest_suffix; refuses
+    names that would overflow its fixed file-name buffers."""
+    b = os.fsencode(path)
+    if len(b) + len(longest_suffix) + 1 > REF_STRING_SIZE:
+        raise ValueError(f"{path!r}{longest_suffix} does not fit the reference's {REF_STRING_SIZE}-byte file names")
+    return b
 
 
 def _f32(a):
@@ -255,6 +272,12 @@ class Port:
         inner = np.frombuffer(data, np.float32, nx0 * ny0).reshape(nx0, ny0).T
         return np.pad(inner, ((fs, g.npml), (g.npml, g.npml)), mode="edge")
 
+    def apply_hess(self, grad, hess, eps_hess):
+        """apply_hess_AC: (preconditioned copy of grad, MAX_HESS)."""
+        out = np.ascontiguousarray(grad, np.float32).copy()
+        mx = self.lib.port_apply_hess(out.size, eps_hess, out.reshape(-1), _f32(hess).reshape(-1))
+        return out, float(mx)
+
     def gradient_scalars(self, physics, freq):
         """(Omega^2, Omega) of ass_grad_AC / ass_grad_TE as complex64 values."""
         a = np.zeros(2, np.float32); b = np.zeros(2, np.float32)
@@ -332,29 +355,35 @@ class Ref:
         self.lib.ref_gauss_filt(vref, fc_low, fsg, fsg1, out.reshape(-1))
         return out
 
+    def apply_hess(self, grad, hess, eps_hess):
+        """apply_hess_AC: (preconditioned copy of grad, MAX_HESS)."""
+        out = np.ascontiguousarray(grad, np.float32).copy()
+        mx = self.lib.ref_apply_hess(eps_hess, out.reshape(-1), _f32(hess).reshape(-1))
+        return out, float(mx)
+
     # ---- file formats: the reference writes / reads the files itself ----
     def write_seis(self, prefix, stage, seis):
         """write_seis_AC: <prefix>_p_stage_<stage>.bin from complex [nf][nshots][ntr]."""
         nf, ns, ntr = seis.shape
-        self.lib.ref_write_seis(os.fsencode(prefix), stage, nf, ns, ntr, _f32(seis.real).ravel(),
+        self.lib.ref_write_seis(_ref_name(prefix, f"_p_stage_{stage}.bin"), stage, nf, ns, ntr, _f32(seis.real).ravel(),
                                 _f32(seis.imag).ravel())
 
     def read_seis(self, prefix, stage, nf, nshots, ntr):
         """read_seis_AC of <prefix>_p_stage_<stage>.bin."""
         re = np.zeros(nf * nshots * ntr, np.float32); im = np.zeros_like(re)
-        self.lib.ref_read_seis(os.fsencode(prefix), stage, nf, nshots, ntr, re, im)
+        self.lib.ref_read_seis(_ref_name(prefix, f"_p_stage_{stage}.bin"), stage, nf, nshots, ntr, re, im)
         return (re + 1j * im).astype(np.complex64).reshape(nf, nshots, ntr)
 
     def writemod_true(self, path, grid, idx=1, idy=1):
-        self.lib.ref_writemod_true(os.fsencode(path), idx, idy, _f32(grid).ravel())
+        self.lib.ref_writemod_true(_ref_name(path, ""), idx, idy, _f32(grid).ravel())
 
     def writemod(self, path, grid, idx=1, idy=1):
-        self.lib.ref_writemod(os.fsencode(path), idx, idy, _f32(grid).ravel())
+        self.lib.ref_writemod(_ref_name(path, ""), idx, idy, _f32(grid).ravel())
 
     def readmod(self, mfile):
         """readmod of <mfile>.vp / <mfile>.rho -> (vp, rho) [NY][NX] with the frame."""
         vp = np.zeros(self.g.n, np.float32); rho = np.zeros_like(vp)
-        self.lib.ref_readmod(os.fsencode(mfile), vp, rho)
+        self.lib.ref_readmod(_ref_name(mfile, ".germaine.rho"), vp, rho)
         return vp.reshape(self.g.ny, self.g.nx), rho.reshape(self.g.ny, self.g.nx)
 
 
@@ -378,6 +407,10 @@ class RefDropin:
         lib.dropin_grad_obj_ac.argtypes = [ctypes.c_int, _f32p, _f32p, _f32p, ctypes.c_int, _f32p, _f32p, ctypes.c_int,
                                            _i32p, _i32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int, _f32p]
         lib.dropin_grad_obj_ac.restype = ctypes.c_float
+        cp, i = ctypes.c_char_p, ctypes.c_int
+        lib.dropin_hessian_ac.argtypes = [i, i, _f32p, _f32p, _f32p, i, _f32p, _f32p, i, _i32p, _i32p, cp, _f32p]
+        lib.dropin_hessian_te.argtypes = [i, i, _f32p, _f32p, _f32p, i, _f32p, _f32p, i, _i32p, _i32p, cp, _f32p,
+                                          _f32p]
         self.lib = lib
         lib.ref_set_grid(g.nx, g.ny, g.dh, g.npml, g.free_surf, g.a0_pml, g.s)
 
@@ -399,3 +432,21 @@ class RefDropin:
                                          np.ascontiguousarray(ry, np.int32), _f32(obs.real).ravel(),
                                          _f32(obs.imag).ravel(), stf_inv, misfit, grad)
         return grad.reshape(self.g.ny, self.g.nx), float(l2)
+
+    def hessian(self, physics, mode, freqs, m0, m1, xs, ys, rx, ry, jacobian):
+        """hessian_shin_{AC,TE} (mode 2) or hessian_{AC,TE} (mode 1) over one
+        stage: (hess0, hess1) [NY][NX] float32 (AC: hess, None; TE: sigma,
+        epsilon with MAT1_NORM = MAT2_NORM = 1).  The drivers write their
+        <jacobian>_hess* files too."""
+        nf, ns, ntr = len(freqs), len(xs), len(rx)
+        args = (mode, nf, _f32(freqs), _f32(m0).ravel(), _f32(m1).ravel(), ns, _f32(xs), _f32(ys), ntr,
+                np.ascontiguousarray(rx, np.int32), np.ascontiguousarray(ry, np.int32),
+                _ref_name(jacobian, "_hess_epsilon"))
+        h0 = np.zeros(self.g.n, np.float32)
+        shape = (self.g.ny, self.g.nx)
+        if physics == PHYS_TE:
+            h1 = np.zeros(self.g.n, np.float32)
+            self.lib.dropin_hessian_te(*args, h0, h1)
+            return h0.reshape(shape), h1.reshape(shape)
+        self.lib.dropin_hessian_ac(*args, h0)
+        return h0.reshape(shape), None

@@ -468,3 +468,22 @@ void port_gauss_filt(const port_grid *g, float vref, float fc_low, float fsg, fl
     free(wt);
     free(src);
 }
+
+/* apply_hess_AC, src/AC/apply_hess_AC.c:11-40: MAX_HESS is the largest
+ * fabs(hess) (a float; entries whose fabs is not > the running maximum, NaN
+ * included, are skipped), then grad *= 1.0 / (hess + EPS_HESS * MAX_HESS):
+ * the denominator in float, the reciprocal and the product in double, the
+ * result stored as float.  Returns MAX_HESS. */
+float port_apply_hess(int n, float eps_hess, float *grad, const float *hess)
+{
+    float max_hess = 0.0f;
+    int k;
+    for (k = 0; k < n; k++)
+        if (fabs(hess[k]) > max_hess) max_hess = fabs(hess[k]);
+    for (k = 0; k < n; k++) {
+        const float den = hess[k] + eps_hess * max_hess;
+        const double q = 1.0 / den;
+        grad[k] = (float)(grad[k] * q);
+    }
+    return max_hess;
+}

@@ -5,6 +5,10 @@
  * Entry points that run the reference's UNMODIFIED per-frequency drivers
  *   forward_shot_AC   src/AC/forward_shot_AC.c:10
  *   grad_obj_AC       src/AC/grad_obj_AC.c:10
+ *   hessian_shin_AC   src/AC/hessian_shin_AC.c:10   (HESSIAN = 2)
+ *   hessian_AC        src/AC/hessian_AC.c:10        (HESSIAN = 1)
+ *   hessian_shin_TE   src/TE/hessian_shin_TE.c:10
+ *   hessian_TE        src/TE/hessian_TE.c:10
  * compiled from the reference tree against include/germaine_umfpack.h (as
  * "umfpack.h") and linked with libgermaine_umfpack.so, so that every
  * UMFPACK call of the drivers lands on the GPU engine.  oracle/Makefile
@@ -19,6 +23,8 @@
 /* the reference's globals (defined by include/globvar.h in ref_harness.c) */
 extern int NX, NY, NXNY, NONZERO, NSHOT1, NSHOT2, NSHOTS, NF, SNAP, SEISMO, INFO, READ_REC, MYID, NP;
 extern int N_STREAMER, STF_INV, MISFIT, INVMAT, NFREQ1, NFREQ2;
+extern float MAT1_NORM, MAT2_NORM;
+extern char JACOBIAN[STRING_SIZE];
 
 /* the drivers' prototypes not declared in fd.h */
 void pml_pro(struct PML_AC *PML_AC, struct waveAC *waveAC);
@@ -141,4 +147,81 @@ float dropin_grad_obj_ac(int nf, const float *freqs, const float *vp, const floa
     free(stage); free(precr); free(preci);
     free_wave(&w, &p, &m);
     return l2;
+}
+
+static void flat_from_nr(float **m, float *flat)
+{
+    int i, j;
+    for (j = 1; j <= NY; j++)
+        for (i = 1; i <= NX; i++) flat[(j - 1) * NX + (i - 1)] = m[j][i];
+}
+
+static float *stage_freqs(struct waveAC *w, int nf, const float *freqs)
+{
+    float *stage = malloc(sizeof(float) * (size_t)nf);
+    int i;
+    for (i = 0; i < nf; i++) stage[i] = freqs[i];
+    w->stage_freq = stage - 1;
+    NFREQ1 = 1; NFREQ2 = nf + 1;
+    return stage;
+}
+
+/* hessian_shin_AC (mode 2) or hessian_AC (mode 1) over freqs[0..nf): the
+ * frame-tapered Hessian (NY x NX) into hess; the drivers also write
+ * <jacobian>_hess (float, x outer). */
+void dropin_hessian_ac(int mode, int nf, const float *freqs, const float *vp, const float *rho, int nshots,
+                       const float *sx, const float *sy, int ntr, const int *rx, const int *ry, const char *jacobian,
+                       float *hess)
+{
+    struct waveAC w; struct PML_AC p; struct matAC m; struct fwiAC f;
+    float **srcpos, *stage;
+    driver_globals(nshots, nf);
+    snprintf(JACOBIAN, STRING_SIZE, "%s", jacobian);
+    alloc_wave(&w, &p, &m, vp, rho);
+    stage = stage_freqs(&w, nf, freqs);
+    f.hess = matrix(1, NY, 1, NX);
+    f.forwardr = matrix(1, NY, 1, NX); f.forwardi = matrix(1, NY, 1, NX);
+    srcpos = srcpos_nr(nshots, sx, sy);
+    acq.recpos = recpos_nr(ntr, rx, ry);
+    if (mode == 2) hessian_shin_AC(&f, &w, &p, &m, srcpos, nshots, acq.recpos, ntr, 1, 1);
+    else hessian_AC(&f, &w, &p, &m, srcpos, nshots, acq.recpos, ntr, 1, 1);
+    flat_from_nr(f.hess, hess);
+    free_imatrix(acq.recpos, 1, 3, 1, ntr);
+    free_matrix(srcpos, 1, 8, 1, nshots);
+    free_matrix(f.hess, 1, NY, 1, NX);
+    free_matrix(f.forwardr, 1, NY, 1, NX); free_matrix(f.forwardi, 1, NY, 1, NX);
+    free(stage);
+    free_wave(&w, &p, &m);
+}
+
+/* hessian_shin_TE (mode 2) or hessian_TE (mode 1) with MAT1_NORM =
+ * MAT2_NORM = 1: hess_sigma, hess_epsilon (NY x NX); the drivers also write
+ * <jacobian>_hess_sigma and <jacobian>_hess_epsilon. */
+void dropin_hessian_te(int mode, int nf, const float *freqs, const float *eps, const float *sig, int nshots,
+                       const float *sx, const float *sy, int ntr, const int *rx, const int *ry, const char *jacobian,
+                       float *hess_sigma, float *hess_epsilon)
+{
+    struct waveAC w; struct PML_AC p; struct matAC unused; struct matTE m; struct fwiTE f;
+    float **srcpos, *stage;
+    driver_globals(nshots, nf);
+    snprintf(JACOBIAN, STRING_SIZE, "%s", jacobian);
+    MAT1_NORM = 1.0f; MAT2_NORM = 1.0f;
+    alloc_wave(&w, &p, &unused, eps, sig);   /* the AC material grids are not read by the TE drivers */
+    m.epsilon = nr_from_flat(eps); m.sigma = nr_from_flat(sig);
+    stage = stage_freqs(&w, nf, freqs);
+    f.hess_sigma = matrix(1, NY, 1, NX); f.hess_epsilon = matrix(1, NY, 1, NX);
+    f.forwardr = matrix(1, NY, 1, NX); f.forwardi = matrix(1, NY, 1, NX);
+    srcpos = srcpos_nr(nshots, sx, sy);
+    acq.recpos = recpos_nr(ntr, rx, ry);
+    if (mode == 2) hessian_shin_TE(&f, &w, &p, &m, srcpos, nshots, acq.recpos, ntr, 1, 1);
+    else hessian_TE(&f, &w, &p, &m, srcpos, nshots, acq.recpos, ntr, 1, 1);
+    flat_from_nr(f.hess_sigma, hess_sigma);
+    flat_from_nr(f.hess_epsilon, hess_epsilon);
+    free_imatrix(acq.recpos, 1, 3, 1, ntr);
+    free_matrix(srcpos, 1, 8, 1, nshots);
+    free_matrix(f.hess_sigma, 1, NY, 1, NX); free_matrix(f.hess_epsilon, 1, NY, 1, NX);
+    free_matrix(f.forwardr, 1, NY, 1, NX); free_matrix(f.forwardi, 1, NY, 1, NX);
+    free_matrix(m.epsilon, 0, NY + 1, 0, NX + 1); free_matrix(m.sigma, 0, NY + 1, 0, NX + 1);
+    free(stage);
+    free_wave(&w, &p, &unused);
 }

@@ -31,6 +31,7 @@
  *   writemod_true        src/writemod_true.c:12
  *   writemod             src/writemod.c:11   (format 3 via writedsk)
  *   readmod              src/readmod.c:10
+ *   apply_hess_AC        src/AC/apply_hess_AC.c:11
  */
 #include "fd.h"
 #include "globvar.h"
@@ -343,4 +344,17 @@ void ref_readmod(const char *mfile, float *vp, float *rho)
     from_nr(m.vp, vp); from_nr(m.rho, rho);
     free_matrix(m.vp, 0, NY + 1, 0, NX + 1);
     free_matrix(m.rho, 0, NY + 1, 0, NX + 1);
+}
+
+/* apply_hess_AC (src/AC/apply_hess_AC.c:11) on flat [NY][NX] arrays; returns MAX_HESS */
+float ref_apply_hess(float eps_hess, float *grad, const float *hess)
+{
+    extern float MAX_HESS, EPS_HESS;
+    float **g = to_nr(grad), **h = to_nr(hess);
+    EPS_HESS = eps_hess;
+    apply_hess_AC(g, h);
+    from_nr(g, grad);
+    free_matrix(g, 0, NY + 1, 0, NX + 1);
+    free_matrix(h, 0, NY + 1, 0, NX + 1);
+    return MAX_HESS;
 }

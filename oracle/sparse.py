@@ -147,3 +147,75 @@ def gradient_fp64(g: Grid, physics: int, freqs, Xf, Xa, stfu, vp=None, rho=None,
     coef, passes = grad_frame(g, port)
     fac = coef ** passes
     return g0 * fac, (g1 * fac if physics == PHYS_TE else None)
+
+
+def hess_green_rhs(g: Grid, physics: int, rx, ry) -> np.ndarray:
+    """[n][ntr] right-hand sides of the Hessian's receiver Green's functions:
+    a spike at the adjoint index (RHS_source_AC_hess, src/AC/RHS_source_AC_hess.c:26-33:
+    float amp 1 over float DH*DH; RHS_source_TE_hess, src/TE/RHS_source_TE_hess.c:34-38:
+    1.0 / (DH*DH) in double)."""
+    dh2 = np.float32(g.dh) * np.float32(g.dh)
+    amp = float(1.0 / np.float64(dh2)) if physics == PHYS_TE else float(np.float32(1.0) / dh2)
+    B = np.zeros((g.n, len(rx)), complex)
+    for t, (a, b) in enumerate(zip(rx, ry)):
+        B[adjoint_index(g, int(a), int(b)), t] = amp
+    return B
+
+
+def hessian_source_physics(physics: int, mode: int) -> int:
+    """The physics whose source routine models the Hessian's forward fields:
+    hessian_shin_TE calls RHS_source_AC (src/TE/hessian_shin_TE.c:108, a
+    1/DH^2 spike without the -i Omega mu0 of RHS_source_TE); every other
+    estimator uses its own physics' source."""
+    return 1 if (physics == PHYS_TE and mode == 2) else physics
+
+
+def hessian_fp64(g: Grid, physics: int, mode: int, freqs, Xf, Xg=None, vp=None, rho=None,
+                 port: Port | None = None, tapered: bool = True):
+    """FP64 diagonal Hessians term by term, then the cp_grad_frame taper:
+    mode 2, hessian_shin_AC (src/AC/hessian_shin_AC.c:117-126):
+        sum_s |J|^2, J = 2 Omega^2 F_s / (rho vp^3);
+    mode 1, hessian_AC (src/AC/hessian_AC.c:152-160):
+        sum_s sum_r |J|^2, J = -2 Omega^2 F_s G_r / (rho vp^3);
+    TE (src/TE/hessian_shin_TE.c:121-128, src/TE/hessian_TE.c:147-158):
+        sigma J = (i Omega) F_s (G_r), epsilon J = Omega^2 F_s (G_r).
+    Xf: [nf][n][ns] forward solutions, Xg: [nf][n][ntr] Green's functions
+    (both before the vec2mat shift).  Returns (h0, h1) [n]; h1 None for AC;
+    tapered=False leaves out the cp_grad_frame taper."""
+    port = port or Port(g)
+    h0 = np.zeros(g.n)
+    h1 = np.zeros(g.n)
+    mat = None
+    if physics != PHYS_TE:
+        vpd = np.asarray(vp, np.float64).reshape(-1)
+        rhod = np.asarray(rho, np.float64).reshape(-1)
+        mat = 1.0 / (rhod * vpd ** 3)
+    for f in range(len(freqs)):
+        om2, om = port.gradient_scalars(physics, float(freqs[f]))
+        F = vec2mat(Xf[f].T)                                   # [ns][n]
+        G = vec2mat(Xg[f].T) if mode == 1 else np.ones((1, g.n))   # [ntr][n]
+        FG = F[:, None, :] * G[None, :, :]                      # [ns][ntr][n], one term per (shot, receiver)
+        if physics != PHYS_TE:
+            J = (-2.0 if mode == 1 else 2.0) * om2 * FG * mat
+            h0 += np.sum(np.abs(J) ** 2, axis=(0, 1))
+        else:
+            h0 += np.sum(np.abs(1j * om * FG) ** 2, axis=(0, 1))
+            h1 += np.sum(np.abs(om2 * FG) ** 2, axis=(0, 1))
+    if not tapered:
+        return h0, (h1 if physics == PHYS_TE else None)
+    coef, passes = grad_frame(g, port)
+    fac = coef ** passes
+    return h0 * fac, (h1 * fac if physics == PHYS_TE else None)
+
+
+def taper_float(g: Grid, h, port: Port | None = None) -> np.ndarray:
+    """cp_grad_frame on a float array (src/cp_grad_frame.c:162-200): the
+    untapered sum rounded to float, then multiplied in float by the taper
+    coefficient once per boundary strip the point lies in."""
+    coef, passes = grad_frame(g, port or Port(g))
+    v = np.asarray(h, np.float64).astype(np.float32)
+    c = np.asarray(coef, np.float32)
+    for q in range(int(np.max(passes)) if np.size(passes) else 0):
+        sel = passes > q
+        v[sel] = v[sel] * c[sel]
+    return v

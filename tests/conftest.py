@@ -1,5 +1,7 @@
 import os
+import shutil
 import sys
+import tempfile
 
 import pytest
 
@@ -19,3 +21,14 @@ def gpu_lib():
     from germaine_b200 import _lib
     lib = _lib.load()
     return lib
+
+
+@pytest.fixture
+def short_tmp():
+    """A temporary directory with a short path: the reference formats file
+    names into 74-byte buffers, which pytest's tmp_path can overflow."""
+    d = tempfile.mkdtemp(prefix="gm", dir="/tmp")
+    try:
+        yield d
+    finally:
+        shutil.rmtree(d, ignore_errors=True)

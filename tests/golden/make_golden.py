@@ -5,8 +5,9 @@ profiles and assembled triplets (init_A_*_9p_pml) and, for the acoustic
 cases, a right-hand side with its FP64 sparse solution on the operator
 UMFPACK factorises (M = A^T; solved with SciPy SuperLU because UMFPACK is
 not part of the reference tree); postproc_gauss_filt.npz holds gauss_filt
-cases and files_formats.npz the bytes of the reference's seismogram and
-model files.  Run:  python tests/golden/make_golden.py [assembly] [gauss] [files]
+cases, postproc_apply_hess.npz apply_hess_AC cases and files_formats.npz
+the bytes of the reference's seismogram and model files.
+Run:  python tests/golden/make_golden.py [assembly] [gauss] [hess] [files]
 (no argument: all).
 """
 import tempfile
@@ -33,11 +34,13 @@ CASES = [
 
 def main():
     out = os.path.dirname(os.path.abspath(__file__))
-    which = set(sys.argv[1:]) or {"assembly", "gauss", "files"}
+    which = set(sys.argv[1:]) or {"assembly", "gauss", "hess", "files"}
     if "assembly" in which:
         assembly_fixtures(out)
     if "gauss" in which:
         gauss_filt_fixture(out)
+    if "hess" in which:
+        apply_hess_fixture(out)
     if "files" in which:
         files_fixture(out)
 
@@ -89,6 +92,31 @@ def gauss_filt_fixture(out):
         d[f"out_{k}"] = O.Ref(g).gauss_filt(grad, vref, fc, fs0, fs1)
     np.savez_compressed(os.path.join(out, "postproc_gauss_filt.npz"), **d)
     print("wrote postproc_gauss_filt")
+
+
+# apply_hess_AC cases: grid, EPS_HESS
+HESS_CASES = [(37, 29, 0.005), (50, 20, 0.1), (16, 16, 0.0)]
+
+
+def apply_hess_fixture(out):
+    """postproc_apply_hess.npz: seeded gradients and Hessians (positive, with
+    zeros and negative entries) and the reference's apply_hess_AC of each:
+    grad_k, hess_k, out_k, max_k (MAX_HESS), case_k = (nx, ny, eps)."""
+    rng = np.random.default_rng(17)
+    d = {"ncases": len(HESS_CASES)}
+    for k, (nx, ny, eps) in enumerate(HESS_CASES):
+        g = O.Grid(nx=nx, ny=ny, dh=10.0, npml=4)
+        grad = rng.standard_normal((ny, nx)).astype(np.float32)
+        hess = (np.exp(rng.uniform(-8, 3, (ny, nx))) * 1e-7).astype(np.float32)
+        hess[rng.random((ny, nx)) < 0.05] = 0
+        hess[rng.random((ny, nx)) < 0.03] *= -1
+        if eps == 0.0:
+            hess[hess == 0] = 1e-12     # EPS_HESS = 0 divides by hess itself
+        o, mx = O.Ref(g).apply_hess(grad, hess, eps)
+        d.update({f"case_{k}": np.array([nx, ny, eps]), f"grad_{k}": grad, f"hess_{k}": hess, f"out_{k}": o,
+                  f"max_{k}": np.float32(mx)})
+    np.savez_compressed(os.path.join(out, "postproc_apply_hess.npz"), **d)
+    print("wrote postproc_apply_hess")
 
 
 # file-format cases: grid nx, ny, npml, free_surf

@@ -116,8 +116,10 @@ def test_errors(tmp_path):
 
 
 @needs_ref
-def test_against_reference_live(tmp_path):
+def test_against_reference_live(short_tmp):
     """Fresh seeded data through the reference's own writers and readers."""
+    import pathlib
+    tmp_path = pathlib.Path(short_tmp)
     rng = np.random.default_rng(31)
     for nx, ny, npml, fs in [(33, 25, 7, 0), (25, 20, 3, 1)]:
         g = O.Grid(nx=nx, ny=ny, dh=10.0, npml=npml, free_surf=fs)

@@ -150,3 +150,35 @@ def test_port_gauss_filt_equals_reference(fs0, fs1):
     a = O.Port(g).gauss_filt(grad, 2500.0, 4.0, fs0, fs1)
     b = O.Ref(g).gauss_filt(grad, 2500.0, 4.0, fs0, fs1)
     assert np.array_equal(_bits(a), _bits(b))
+
+
+def hess_cases():
+    d = np.load(os.path.join(GOLDEN, "postproc_apply_hess.npz"))
+    out = []
+    for k in range(int(d["ncases"])):
+        nx, ny, eps = d[f"case_{k}"]
+        out.append((int(nx), int(ny), float(np.float32(eps)), d[f"grad_{k}"], d[f"hess_{k}"], d[f"out_{k}"],
+                    float(d[f"max_{k}"])))
+    return out
+
+
+def test_port_apply_hess_against_golden():
+    """apply_hess_AC (src/AC/apply_hess_AC.c:11-40): the restatement is
+    bit-identical to the reference's output stored in the fixture (negative
+    and zero Hessian entries, EPS_HESS = 0 included)."""
+    for nx, ny, eps, grad, hess, ref, mx in hess_cases():
+        g = O.Grid(nx=nx, ny=ny, dh=10.0, npml=4)
+        out, m = O.Port(g).apply_hess(grad, hess, eps)
+        assert np.array_equal(_bits(out), _bits(ref)) and m == mx
+
+
+@needs_ref
+@pytest.mark.parametrize("eps", [0.005, 0.3, 1e-7])
+def test_port_apply_hess_equals_reference(eps):
+    g = O.Grid(nx=41, ny=35, dh=10.0, npml=4)
+    rng = np.random.default_rng(9)
+    grad = rng.standard_normal((35, 41)).astype(np.float32)
+    hess = (rng.standard_normal((35, 41)) * 1e-4).astype(np.float32)
+    a, ma = O.Port(g).apply_hess(grad, hess, eps)
+    b, mb = O.Ref(g).apply_hess(grad, hess, eps)
+    assert np.array_equal(_bits(a), _bits(b)) and ma == mb
