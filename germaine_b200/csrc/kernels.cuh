@@ -143,4 +143,11 @@ void launch_convert_down(const double2 *src, void *dst, size_t count, cudaStream
 template <class R>
 void launch_add_up(double2 *x, const void *d, size_t count, cudaStream_t st);
 
+// one ordered float dot product (lbfgs.cu: k_dot_seq): out = sum a[i] * b[i], i = 0..n-1 in order
+struct DotJob {
+    const float *a, *b;
+    long n;
+    float *out;
+};
+
 }  // namespace gm

@@ -243,6 +243,84 @@ class Engine:
         return float(l2.value)
 
 
+class Lbfgs:
+    """The reference's l-BFGS update on the GPU (gm_lbfgs_*): LBFGS
+    (src/LBFGS.c) for nclass = 1, LBFGS_TE (src/TE/LBFGS_TE.c) for
+    nclass = 2, with the history resident on the device.  Grids are
+    [nclass][NY][NX] (or [NY][NX] for one class) float32."""
+
+    def __init__(self, nx: int, ny: int, npml: int, m: int, nclass: int = 1, free_surf: int = 0, device: int = 0):
+        self.lib = _lib.load()
+        self.nx, self.ny, self.nclass, self.m = nx, ny, nclass, m
+        h = ctypes.c_void_p()
+        check(self.lib.gm_lbfgs_create(device, nx, ny, npml, free_surf, nclass, m, ctypes.byref(h)))
+        self._h = h
+
+    def close(self):
+        if self._h:
+            self.lib.gm_lbfgs_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _grid(self, a):
+        g = _c(a, np.float32)
+        if g.size != self.nclass * self.nx * self.ny:
+            raise ValueError("grid size does not match the l-BFGS layout")
+        return g
+
+    def step(self, first: bool, pointer: int, grad, gradm, model, hess=None, eps_hess: float = 0.0):
+        """One LBFGS call; returns Hgrad with the shape of gradm."""
+        g, gm, md = self._grid(grad), self._grid(gradm), self._grid(model)
+        hs = self._grid(hess) if hess is not None else None
+        out = np.empty_like(gm)
+        check(self.lib.gm_lbfgs_step(self._h, int(bool(first)), pointer, ptr(g), ptr(gm), ptr(md), ptr(hs), eps_hess,
+                                     ptr(out)))
+        return out
+
+    def rotate(self):
+        check(self.lib.gm_lbfgs_rotate(self._h))
+
+    def zero(self):
+        check(self.lib.gm_lbfgs_zero(self._h))
+
+    def check_descent(self, hgrad, grad) -> float:
+        """p of check_descent; the history is cleared when p < 0."""
+        p = ctypes.c_float(0.0)
+        check(self.lib.gm_lbfgs_check_descent(self._h, ptr(self._grid(hgrad)), ptr(self._grid(grad)),
+                                              ctypes.byref(p)))
+        return float(p.value)
+
+    def get_old(self):
+        shape = (self.nclass, self.ny, self.nx) if self.nclass > 1 else (self.ny, self.nx)
+        g = np.empty(shape, np.float32)
+        md = np.empty(shape, np.float32)
+        check(self.lib.gm_lbfgs_get_old(self._h, ptr(g), ptr(md)))
+        return g, md
+
+    def set_old(self, grad_old, model_old):
+        check(self.lib.gm_lbfgs_set_old(self._h, ptr(self._grid(grad_old)), ptr(self._grid(model_old))))
+
+
+def mat_change(hgrad, model_old, eps_scale: float, low: float, up: float, mode: int = 0, device: int = 0):
+    """calc_mat_change_wolfe (mode 0) / _multi_para (mode 1) on the GPU."""
+    h = _c(hgrad, np.float32)
+    old = _c(model_old, np.float32)
+    out = np.empty_like(old)
+    check(_lib.load().gm_mat_change(device, old.size, mode, eps_scale, low, up, ptr(h), ptr(old), ptr(out)))
+    return out
+
+
 def apply_hess(grad, hess, eps_hess: float, device: int = 0):
     """apply_hess_AC on the GPU (gm_apply_hess, bit-identical): returns
     (preconditioned gradient, MAX_HESS)."""

@@ -249,6 +249,59 @@ int gm_gauss_filt(int device, int nx, int ny, float dh, float vref, float fc_low
  * hess are n floats in host or device memory; grad is updated in place. */
 int gm_apply_hess(int device, int n, float eps_hess, float *grad, const float *hess, float *max_hess);
 
+/* ---- quasi-Newton l-BFGS on the device ----
+ * The reference's l-BFGS update (LBFGS, src/LBFGS.c:12-250; LBFGS_TE,
+ * src/TE/LBFGS_TE.c:12, for the two TE classes sigma, epsilon) with its
+ * history (y, s of the last m iterations) and the previous gradient and
+ * model (what the "<JACOBIAN>_p.old" / "_p_vp.old" files hold) resident on
+ * one GPU.  Results are bit-identical to the reference's float arithmetic,
+ * including the order of its float dot products (dotp, src/dotp.c).
+ * Grids are [nclass][NY][NX] row-major floats in host or device memory;
+ * only IDX = IDY = 1 layouts are covered. */
+typedef struct gm_lbfgs gm_lbfgs;
+
+/* nclass 1 (AC / SH: NLBFGS_class = 1) or 2 (TE); m = NLBFGS. */
+int gm_lbfgs_create(int device, int nx, int ny, int npml, int free_surf, int nclass, int m, gm_lbfgs **out);
+int gm_lbfgs_destroy(gm_lbfgs *h);
+
+/* One LBFGS call: first != 0 is the reference's iter == 1 (AC) or
+ * LBFGS_RESET == 1 (TE): hgrad = gradm.  Otherwise slot `pointer` (the
+ * reference's LBFGS_pointer, 1..m) receives y = grad - previous grad and
+ * s = model - previous model, and the two-loop recursion gives hgrad from
+ * gradm with the initial Hessian gamma = (y.s)/(y.y) (hess == NULL) or the
+ * diagonal Hessian q / (hess + eps_hess * max|hess|) per class (LBFGS_TE
+ * with HESSIAN != 0).  hgrad is frame-tapered (cp_grad_frame).  grad and
+ * model are kept as the next call's previous gradient and model; model is
+ * what the reference saves (AC: vp; TE: sigma / MAT1_NORM and
+ * epsilon / MAT2_NORM as scale_grad forms them). */
+int gm_lbfgs_step(gm_lbfgs *h, int first, int pointer, const float *grad, const float *gradm,
+                  const float *model, const float *hess, float eps_hess, float *hgrad);
+
+/* rot_LBFGS_vec (src/rot_LBFGS_vec.c:10-24): slots 2..m move to 1..m-1. */
+int gm_lbfgs_rotate(gm_lbfgs *h);
+
+/* zero_LBFGS / zero_LBFGS1 (src/zero_LBFGS.c): clear the history. */
+int gm_lbfgs_zero(gm_lbfgs *h);
+
+/* check_descent (src/check_descent.c:10-31) / check_descent_multi_para_TE:
+ * p = -(hgrad . grad) / (grad . grad) with the reference's float sums; the
+ * history is cleared when p < 0.  *p receives p (may be NULL). */
+int gm_lbfgs_check_descent(gm_lbfgs *h, const float *hgrad, const float *grad, float *p);
+
+/* The previous gradient and model ([nclass][NY][NX]): what the reference's
+ * "*.old" files hold (x outer on disk: gm_write_model writes them), so a run
+ * can stop and resume. */
+int gm_lbfgs_get_old(gm_lbfgs *h, float *grad_old, float *model_old);
+int gm_lbfgs_set_old(gm_lbfgs *h, const float *grad_old, const float *model_old);
+
+/* Model update along the search direction: model = model_old + eps_scale *
+ * hgrad over n floats, then mode 0 = calc_mat_change_wolfe
+ * (src/calc_mat_change_wolfe.c:27-47: values outside [low, up] or below 0
+ * keep model_old), mode 1 = calc_mat_change_wolfe_multi_para (clamped to
+ * [low, up]).  Bit-identical; host or device buffers. */
+int gm_mat_change(int device, int n, int mode, float eps_scale, float low, float up, const float *hgrad,
+                  const float *model_old, float *model);
+
 /* ---- the reference's file formats (host stdio, no GPU needed) ---- */
 #define GM_SEIS_KEEP_LAST 1  /* gm_write_seis: write the last sample as given */
 

@@ -109,6 +109,12 @@ def load_port():
         lib.port_gauss_filt.argtypes = [P, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f32p]
         lib.port_apply_hess.argtypes = [ctypes.c_int, ctypes.c_float, _f32p, _f32p]
         lib.port_apply_hess.restype = ctypes.c_float
+        lib.port_lbfgs.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p,
+                                   _f32p, _f32p, ctypes.c_void_p, ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p,
+                                   _f32p]
+        lib.port_lbfgs_rotate.argtypes = [ctypes.c_int, ctypes.c_int, _f32p, _f32p]
+        lib.port_check_descent.argtypes = [P, ctypes.c_int, _f32p, _f32p]
+        lib.port_check_descent.restype = ctypes.c_float
         _port_lib = lib
     return _port_lib
 
@@ -146,6 +152,13 @@ def load_ref():
         lib.ref_readmod.argtypes = [cp, _f32p, _f32p]
         lib.ref_apply_hess.argtypes = [ctypes.c_float, _f32p, _f32p]
         lib.ref_apply_hess.restype = ctypes.c_float
+        fp = _f32p
+        lib.ref_lbfgs_ac.argtypes = [i, i, i, fp, fp, fp, fp, fp, fp, fp, fp, fp, fp, cp, fp]
+        lib.ref_lbfgs_te.argtypes = [i, i, i, i, ctypes.c_float, ctypes.c_float, ctypes.c_float, fp, fp, fp, fp, fp, fp,
+                                     fp, fp, fp, fp, fp, fp, fp, fp, fp, cp, fp, fp]
+        lib.ref_lbfgs_rotate.argtypes = [i, i, fp, fp]
+        lib.ref_dotp_matrix.argtypes = [fp, fp]
+        lib.ref_dotp_matrix.restype = ctypes.c_float
         _ref_lib = lib
     return _ref_lib
 
@@ -450,3 +463,89 @@ class RefDropin:
             return h0.reshape(shape), h1.reshape(shape)
         self.lib.dropin_hessian_ac(*args, h0)
         return h0.reshape(shape), None
+
+
+class PortLbfgs:
+    """The restated l-BFGS (port.c: port_lbfgs) with its state: history y, s
+    ([m][nvec]) and the previous gradient / model, as the reference keeps
+    them in its LBFGS vectors and "*.old" files."""
+
+    def __init__(self, g: Grid, m: int, nclass: int = 1):
+        self.g, self.m, self.nclass = g, m, nclass
+        self.lib = load_port()
+        self._pg = _pg(g)
+        self.nvec = nclass * g.n
+        self.y = np.zeros(m * self.nvec, np.float32)
+        self.s = np.zeros(m * self.nvec, np.float32)
+        self.old_grad = np.zeros(self.nvec, np.float32)
+        self.old_model = np.zeros(self.nvec, np.float32)
+        self.q = np.zeros(self.nvec, np.float32)
+        self.r = np.zeros(self.nvec, np.float32)
+        self.scal = np.zeros(2 * m + 1, np.float32)
+
+    def step(self, first, pointer, grad, gradm, model, hess=None, eps_hess=0.0):
+        out = np.zeros(self.nvec, np.float32)
+        hs = _f32(hess).ravel() if hess is not None else None
+        self.lib.port_lbfgs(ctypes.byref(self._pg), self.nclass, self.m, pointer, int(bool(first)), self.y, self.s,
+                            _f32(grad).ravel(), _f32(gradm).ravel(), _f32(model).ravel(),
+                            None if hs is None else hs.ctypes.data_as(ctypes.c_void_p), eps_hess, self.old_grad,
+                            self.old_model, self.q, self.r, self.scal, out)
+        return out.reshape(np.shape(gradm))
+
+    def rotate(self):
+        self.lib.port_lbfgs_rotate(self.m, self.nvec, self.y, self.s)
+
+    def zero(self):
+        self.y[:] = 0
+        self.s[:] = 0
+
+    def check_descent(self, hgrad, grad):
+        p = float(self.lib.port_check_descent(ctypes.byref(self._pg), self.nclass, _f32(hgrad).ravel(),
+                                              _f32(grad).ravel()))
+        if p < 0.0:
+            self.zero()
+        return p
+
+
+class RefLbfgs:
+    """The reference's LBFGS / LBFGS_TE (oracle/_ref) with the persistent
+    arrays the reference's FWI loop owns; it reads and writes its "*.old"
+    files under `jacobian` (keep that path short: the reference formats file
+    names into fixed buffers)."""
+
+    def __init__(self, g: Grid, m: int, nclass: int, jacobian: str):
+        self.g, self.m, self.nclass = g, m, nclass
+        self.lib = load_ref()
+        self.lib.ref_set_grid(g.nx, g.ny, g.dh, g.npml, g.free_surf, g.a0_pml, g.s)
+        self.jac = _ref_name(jacobian, "_p_epsilon_grad.old")
+        self.nvec = nclass * g.n
+        self.y = np.zeros(m * self.nvec, np.float32)
+        self.s = np.zeros(m * self.nvec, np.float32)
+        self.rho = np.zeros(m, np.float32)
+        self.alpha = np.zeros(m, np.float32)
+        self.beta = np.zeros(m, np.float32)
+        self.q = np.zeros(self.nvec, np.float32)
+        self.r = np.zeros(self.nvec, np.float32)
+
+    def step_ac(self, iter_, pointer, grad, gradm, vp):
+        out = np.zeros(self.g.n, np.float32)
+        self.lib.ref_lbfgs_ac(iter_, pointer, self.m, self.y, self.s, self.rho, self.alpha, self.q, self.r,
+                              self.beta, _f32(grad).ravel(), _f32(gradm).ravel(), _f32(vp).ravel(), self.jac, out)
+        return out.reshape(self.g.ny, self.g.nx)
+
+    def step_te(self, reset, pointer, grad, gradm, model, norms, hess=None, eps_hess=0.0):
+        """grad, gradm, model, hess: [2][NY][NX] (sigma, epsilon); model is
+        sigma, epsilon before normalisation; norms = (MAT1_NORM, MAT2_NORM)."""
+        n = self.g.n
+        gs, ge = (_f32(a).ravel() for a in grad)
+        ms, me = (_f32(a).ravel() for a in gradm)
+        sg, ep = (_f32(a).ravel() for a in model)
+        hs, he = ((_f32(a).ravel() for a in hess) if hess is not None else (np.zeros(n, np.float32),) * 2)
+        o0 = np.zeros(n, np.float32); o1 = np.zeros(n, np.float32)
+        self.lib.ref_lbfgs_te(int(bool(reset)), pointer, self.m, int(hess is not None), eps_hess, norms[0], norms[1],
+                              self.y, self.s, self.rho, self.alpha, self.q, self.r, self.beta, gs, ge, ms, me, sg, ep,
+                              hs, he, self.jac, o0, o1)
+        return np.stack([o0, o1]).reshape(2, self.g.ny, self.g.nx)
+
+    def rotate(self):
+        self.lib.ref_lbfgs_rotate(self.m, self.nvec, self.y, self.s)

@@ -487,3 +487,121 @@ float port_apply_hess(int n, float eps_hess, float *grad, const float *hess)
     }
     return max_hess;
 }
+
+/* ---- l-BFGS (src/LBFGS.c:12-250 for one parameter class, src/TE/LBFGS_TE.c
+ * for two) on flat arrays.  Vectors of length nvec = nclass * NX * NY are in
+ * the reference's order: class outer, then x (i) outer, y (j) inner, 0-based;
+ * y, s hold m such vectors (slot k at offset (k-1) * nvec).  grad, gradm,
+ * model, hess and hgrad are [nclass][NY][NX] row-major.  old_grad /
+ * old_model hold what the reference's "<JACOBIAN>_p.old" / "_p_vp.old"
+ * files hold (grad and model of the previous call) in vector order and are
+ * overwritten with this call's.  hess == NULL: initial Hessian gamma
+ * (LBFGS.c:124-126, LBFGS_TE.c HESSIAN = 0); else q / (hess + eps *
+ * MAX_HESS) per class (LBFGS_TE.c HESSIAN != 0).  first != 0: Hgrad =
+ * gradm (iter == 1 / LBFGS_RESET == 1).  Float arithmetic and summation
+ * order as the reference (dotp, src/dotp.c:10-35, sums in float). */
+static float port_dotp(const float *v1, const float *v2, int n)
+{
+    float tmp = 0.0f;
+    for (int i = 0; i < n; i++) tmp += v1[i] * v2[i];
+    return tmp;
+}
+
+void port_lbfgs(const port_grid *g, int nclass, int m, int pointer, int first, float *y, float *s,
+                const float *grad, const float *gradm, const float *model, const float *hess, float eps_hess,
+                float *old_grad, float *old_model, float *q, float *r, float *scal, float *hgrad)
+{
+    const int nx = g->nx, ny = g->ny, n = nx * ny, nvec = nclass * n;
+    float *rho = scal, *alpha = scal + m;   /* scal: 2 m + 1 floats, the last = gamma */
+    int c, i, j, k, h;
+    if (!first) {
+        h = nvec * (pointer - 1);
+        for (c = 0; c < nclass; c++)
+            for (i = 0; i < nx; i++)
+                for (j = 0; j < ny; j++, h++) {
+                    const int gi = c * n + j * nx + i, v = h - nvec * (pointer - 1);
+                    y[h] = grad[gi] - old_grad[v];
+                    s[h] = model[gi] - old_model[v];
+                }
+        {
+            const float *yp = y + nvec * (pointer - 1), *sp = s + nvec * (pointer - 1);
+            const float nom = port_dotp(yp, sp, nvec), den = port_dotp(yp, yp, nvec);
+            scal[2 * m] = nom / den;
+        }
+        for (k = 1; k <= m; k++) {
+            const float sum = port_dotp(y + nvec * (k - 1), s + nvec * (k - 1), nvec);
+            rho[k - 1] = (fabs(sum) > 0.0) ? 1.0 / sum : 0.0;
+        }
+        h = 0;
+        for (c = 0; c < nclass; c++)
+            for (i = 0; i < nx; i++)
+                for (j = 0; j < ny; j++) q[h++] = gradm[c * n + j * nx + i];
+        for (k = m; k >= 1; k--) {
+            const float sum = port_dotp(s + nvec * (k - 1), q, nvec);
+            alpha[k - 1] = rho[k - 1] * sum;
+            for (i = 0; i < nvec; i++) q[i] = q[i] - alpha[k - 1] * y[nvec * (k - 1) + i];
+        }
+        if (!hess) {
+            for (i = 0; i < nvec; i++) r[i] = scal[2 * m] * q[i];
+        } else {
+            h = 0;
+            for (c = 0; c < nclass; c++) {
+                float mx = 0.0f;
+                for (k = 0; k < n; k++)
+                    if (fabs(hess[c * n + k]) > mx) mx = fabs(hess[c * n + k]);
+                for (i = 0; i < nx; i++)
+                    for (j = 0; j < ny; j++, h++) r[h] = q[h] / (hess[c * n + j * nx + i] + eps_hess * mx);
+            }
+        }
+        for (k = 1; k <= m; k++) {
+            const float sum = port_dotp(y + nvec * (k - 1), r, nvec);
+            const float beta = rho[k - 1] * sum;
+            for (i = 0; i < nvec; i++) r[i] = r[i] + s[nvec * (k - 1) + i] * (alpha[k - 1] - beta);
+        }
+        h = 0;
+        for (c = 0; c < nclass; c++)
+            for (i = 0; i < nx; i++)
+                for (j = 0; j < ny; j++) hgrad[c * n + j * nx + i] = r[h++];
+    } else {
+        for (k = 0; k < nvec; k++) hgrad[k] = gradm[k];
+    }
+    for (c = 0; c < nclass; c++) port_cp_grad_frame(g, hgrad + c * n);
+    h = 0;
+    for (c = 0; c < nclass; c++)
+        for (i = 0; i < nx; i++)
+            for (j = 0; j < ny; j++, h++) {
+                old_grad[h] = grad[c * n + j * nx + i];
+                old_model[h] = model[c * n + j * nx + i];
+            }
+}
+
+/* rot_LBFGS_vec, src/rot_LBFGS_vec.c:10-24: slots 2..m move to 1..m-1 */
+void port_lbfgs_rotate(int m, int nvec, float *y, float *s)
+{
+    for (int k = 0; k < (m - 1) * nvec; k++) {
+        y[k] = y[k + nvec];
+        s[k] = s[k + nvec];
+    }
+}
+
+/* check_descent (src/check_descent.c:17-19) / check_descent_multi_para_TE
+ * (src/TE/check_descent_multi_para_TE.c:21-26): p = -nom / denom from
+ * per-class dotp_matrix sums (x outer, y inner) added in float.  Grids are
+ * [nclass][NY][NX] row-major. */
+float port_check_descent(const port_grid *g, int nclass, const float *hgrad, const float *grad)
+{
+    const int nx = g->nx, ny = g->ny, n = nx * ny;
+    float nom = 0.0f, den = 0.0f;
+    for (int c = 0; c < nclass; c++) {
+        float a = 0.0f, b = 0.0f;
+        for (int i = 0; i < nx; i++)
+            for (int j = 0; j < ny; j++) {
+                const int k = c * n + j * nx + i;
+                a += hgrad[k] * grad[k];
+                b += grad[k] * grad[k];
+            }
+        if (c == 0) { nom = a; den = b; }
+        else { nom += a; den += b; }
+    }
+    return -nom / den;
+}

@@ -32,6 +32,10 @@
  *   writemod             src/writemod.c:11   (format 3 via writedsk)
  *   readmod              src/readmod.c:10
  *   apply_hess_AC        src/AC/apply_hess_AC.c:11
+ *   LBFGS                src/LBFGS.c:12      (+ dotp, exchange_grad_MPI)
+ *   LBFGS_TE             src/TE/LBFGS_TE.c:12
+ *   rot_LBFGS_vec        src/rot_LBFGS_vec.c:10
+ *   dotp_matrix          src/dotp_matrix.c:8
  */
 #include "fd.h"
 #include "globvar.h"
@@ -357,4 +361,70 @@ float ref_apply_hess(float eps_hess, float *grad, const float *hess)
     free_matrix(g, 0, NY + 1, 0, NX + 1);
     free_matrix(h, 0, NY + 1, 0, NX + 1);
     return MAX_HESS;
+}
+
+/* LBFGS (src/LBFGS.c:12) for one call: y, s ([m * n]), rho, alpha, beta ([m]),
+ * q, r ([n]) are the caller's persistent 0-based arrays (passed 1-based to
+ * the reference); grad, gradm, vp and hgrad are flat [NY][NX].  The
+ * reference reads / writes <jacobian>_p.old, _p_vp.old and _c.old. */
+void ref_lbfgs_ac(int iter, int pointer, int m, float *y, float *s, float *rho, float *alpha, float *q, float *r,
+                  float *beta, const float *grad, const float *gradm, const float *vp, const char *jacobian,
+                  float *hgrad)
+{
+    extern char JACOBIAN[STRING_SIZE];
+    float **hg = to_nr(hgrad), **g = to_nr(grad), **gm = to_nr(gradm), **v = to_nr(vp);
+    snprintf(JACOBIAN, STRING_SIZE, "%s", jacobian);
+    IDX = 1; IDY = 1; MYID = 0;
+    LBFGS(hg, g, gm, iter, y - 1, s - 1, rho - 1, alpha - 1, v, q - 1, r - 1, beta - 1, pointer, m, NX * NY);
+    from_nr(hg, hgrad);
+    free_matrix(hg, 0, NY + 1, 0, NX + 1); free_matrix(g, 0, NY + 1, 0, NX + 1);
+    free_matrix(gm, 0, NY + 1, 0, NX + 1); free_matrix(v, 0, NY + 1, 0, NX + 1);
+}
+
+/* LBFGS_TE (src/TE/LBFGS_TE.c:12): two parameter classes (sigma, epsilon)
+ * normalised by MAT1_NORM / MAT2_NORM; hessian != 0 scales q by the
+ * diagonal Hessians hs / he instead of gamma.  y, s: [m * 2n]; q, r: [2n]. */
+void ref_lbfgs_te(int reset, int pointer, int m, int hessian, float eps_hess, float mat1_norm, float mat2_norm,
+                  float *y, float *s, float *rho, float *alpha, float *q, float *r, float *beta,
+                  const float *gs, const float *ge, const float *gms, const float *gme, const float *sigma,
+                  const float *epsilon, const float *hs, const float *he, const char *jacobian, float *hgs,
+                  float *hge)
+{
+    extern char JACOBIAN[STRING_SIZE];
+    extern int HESSIAN, LBFGS_RESET;
+    extern float EPS_HESS, MAT1_NORM, MAT2_NORM;
+    struct fwiTE f; struct matTE mt;
+    f.grad_sigma = to_nr(gs); f.grad_epsilon = to_nr(ge);
+    f.gradm_sigma = to_nr(gms); f.gradm_epsilon = to_nr(gme);
+    f.Hgrad_sigma = to_nr(gs); f.Hgrad_epsilon = to_nr(ge);
+    f.hess_sigma = to_nr(hs); f.hess_epsilon = to_nr(he);
+    mt.sigma = to_nr(sigma); mt.epsilon = to_nr(epsilon);
+    mt.sigmar = to_nr(sigma); mt.epsilonr = to_nr(epsilon);
+    snprintf(JACOBIAN, STRING_SIZE, "%s", jacobian);
+    IDX = 1; IDY = 1; MYID = 0;
+    HESSIAN = hessian; LBFGS_RESET = reset; EPS_HESS = eps_hess; MAT1_NORM = mat1_norm; MAT2_NORM = mat2_norm;
+    LBFGS_TE(&f, &mt, 1, y - 1, s - 1, rho - 1, alpha - 1, q - 1, r - 1, beta - 1, pointer, m, 2 * NX * NY);
+    from_nr(f.Hgrad_sigma, hgs); from_nr(f.Hgrad_epsilon, hge);
+    free_matrix(f.grad_sigma, 0, NY + 1, 0, NX + 1); free_matrix(f.grad_epsilon, 0, NY + 1, 0, NX + 1);
+    free_matrix(f.gradm_sigma, 0, NY + 1, 0, NX + 1); free_matrix(f.gradm_epsilon, 0, NY + 1, 0, NX + 1);
+    free_matrix(f.Hgrad_sigma, 0, NY + 1, 0, NX + 1); free_matrix(f.Hgrad_epsilon, 0, NY + 1, 0, NX + 1);
+    free_matrix(f.hess_sigma, 0, NY + 1, 0, NX + 1); free_matrix(f.hess_epsilon, 0, NY + 1, 0, NX + 1);
+    free_matrix(mt.sigma, 0, NY + 1, 0, NX + 1); free_matrix(mt.epsilon, 0, NY + 1, 0, NX + 1);
+    free_matrix(mt.sigmar, 0, NY + 1, 0, NX + 1); free_matrix(mt.epsilonr, 0, NY + 1, 0, NX + 1);
+}
+
+/* rot_LBFGS_vec (src/rot_LBFGS_vec.c:10) on 0-based y, s */
+void ref_lbfgs_rotate(int m, int nvec, float *y, float *s)
+{
+    rot_LBFGS_vec(y - 1, s - 1, m, nvec);
+}
+
+/* dotp_matrix (src/dotp_matrix.c:8), the sums of check_descent */
+float ref_dotp_matrix(const float *a, const float *b)
+{
+    float **A = to_nr(a), **B = to_nr(b);
+    const float v = dotp_matrix(A, B, NX, NY);
+    free_matrix(A, 0, NY + 1, 0, NX + 1);
+    free_matrix(B, 0, NY + 1, 0, NX + 1);
+    return v;
 }

@@ -182,3 +182,46 @@ def test_port_apply_hess_equals_reference(eps):
     a, ma = O.Port(g).apply_hess(grad, hess, eps)
     b, mb = O.Ref(g).apply_hess(grad, hess, eps)
     assert np.array_equal(_bits(a), _bits(b)) and ma == mb
+
+
+# ---- l-BFGS (src/LBFGS.c, src/TE/LBFGS_TE.c) ----
+from tests import lbfgs_cases as LC  # noqa: E402
+
+
+@needs_ref
+def test_port_lbfgs_ac_equals_reference(short_tmp):
+    """Six iterations with NLBFGS = 3 (two rotations): every direction bit-identical."""
+    g, m = LC.grid(), 3
+    seq = LC.sequence(g, 1, 6, seed=1)
+    port, ref = O.PortLbfgs(g, m, 1), O.RefLbfgs(g, m, 1, os.path.join(short_tmp, "j"))
+    a = LC.run(lambda f, p, it, gr, gm, md, h: port.step(f, p, gr, gm, md), port.rotate, m, seq)
+    b = LC.run(lambda f, p, it, gr, gm, md, h: ref.step_ac(it, p, gr, gm, md), ref.rotate, m, seq)
+    for x, y in zip(a, b):
+        assert np.array_equal(_bits(x), _bits(y))
+    assert np.array_equal(_bits(port.y), _bits(ref.y)) and np.array_equal(_bits(port.s), _bits(ref.s))
+
+
+@needs_ref
+@pytest.mark.parametrize("with_hess", [False, True], ids=["gamma", "hessian"])
+def test_port_lbfgs_te_equals_reference(short_tmp, with_hess):
+    g, m, norms, eps = LC.grid(free_surf=1), 2, (0.01, 8.85e-11), 0.005
+    seq = LC.sequence(g, 2, 5, seed=2)
+    port, ref = O.PortLbfgs(g, m, 2), O.RefLbfgs(g, m, 2, os.path.join(short_tmp, "j"))
+    hs = (lambda h: h) if with_hess else (lambda h: None)
+    a = LC.run(lambda f, p, it, gr, gm, md, h: port.step(f, p, gr, gm, LC.normalise(md, norms), hs(h), eps),
+               port.rotate, m, seq)
+    b = LC.run(lambda f, p, it, gr, gm, md, h: ref.step_te(f, p, gr, gm, md, norms, hs(h), eps), ref.rotate, m, seq)
+    for x, y in zip(a, b):
+        assert np.array_equal(_bits(x), _bits(y))
+
+
+@needs_ref
+def test_port_check_descent_sums_equal_reference():
+    g = LC.grid()
+    rng = np.random.default_rng(8)
+    hg = rng.standard_normal((g.ny, g.nx)).astype(np.float32)
+    gr = rng.standard_normal((g.ny, g.nx)).astype(np.float32)
+    R = O.Ref(g)
+    nom, den = R.lib.ref_dotp_matrix(hg.ravel(), gr.ravel()), R.lib.ref_dotp_matrix(gr.ravel(), gr.ravel())
+    p = O.PortLbfgs(g, 1, 1).check_descent(hg, gr)
+    assert _bits(np.float32(p)) == _bits(np.float32(-np.float32(nom)) / np.float32(den))
