@@ -337,18 +337,40 @@ static int factor_batch(gm_engine *e, double pivscale) {
     GM_CUDA(cudaMemsetAsync(e->d_tcerr.p, 0, sizeof(int), e->st));
     const GemmProb<R> *probs = e->d_cb_probs.as<GemmProb<R>>();
     const int4 *tiles = e->d_cb_tiles.as<int4>();
-    for (size_t h = 0; h < e->levels.size(); ++h) {
+    // GM_TRACE_LEVELS=1: device time of every level on stderr
+    static const bool trace = std::getenv("GM_TRACE_LEVELS") != nullptr;
+    const int nl = (int)e->levels.size();
+    std::vector<cudaEvent_t> ev;
+    if (trace) {
+        ev.resize(nl + 1);
+        for (auto &x : ev) cudaEventCreate(&x);
+        cudaEventRecord(ev[0], e->st);
+    }
+    for (int h = 0; h < nl; ++h) {
         if (small_factor_level<R>(e->levels[h])) {
             launch_factor_small<R>(a, e->levels[h], e->st);
-            continue;
+        } else {
+            launch_factor_level<R>(a, e->levels[h], e->st);
+            const auto &pl = e->cb_plan[h];
+            if (pl.backend == 1)
+                launch_cgemm_sub(1, reinterpret_cast<const CgemmProb *>(probs + pl.prob_off), tiles + pl.tile_off,
+                                 pl.ntiles, e->d_tcerr.as<int>(), e->st);
+            else
+                launch_gemm_sub_cc<R>(probs + pl.prob_off, tiles + pl.tile_off, pl.ntiles, e->st);
         }
-        launch_factor_level<R>(a, e->levels[h], e->st);
-        const auto &pl = e->cb_plan[h];
-        if (pl.backend == 1)
-            launch_cgemm_sub(1, reinterpret_cast<const CgemmProb *>(probs + pl.prob_off), tiles + pl.tile_off,
-                             pl.ntiles, e->d_tcerr.as<int>(), e->st);
-        else
-            launch_gemm_sub_cc<R>(probs + pl.prob_off, tiles + pl.tile_off, pl.ntiles, e->st);
+        if (trace) cudaEventRecord(ev[1 + h], e->st);
+    }
+    if (trace) {
+        cudaEventSynchronize(ev[nl]);
+        for (int h = 0; h < nl; ++h) {
+            float ms = 0;
+            cudaEventElapsedTime(&ms, ev[h], ev[1 + h]);
+            const LevelInfo &L = e->levels[h];
+            std::fprintf(stderr, "factor %s level %2d: fronts %5d max_front %4d max_piv %4d %s %.3f ms\n",
+                         sizeof(R) == 8 ? "c128" : "c64", h, L.count, L.max_front, L.max_piv,
+                         small_factor_level<R>(L) ? "small" : "tiled", ms);
+        }
+        for (auto &x : ev) cudaEventDestroy(x);
     }
     GM_CUDA(cudaGetLastError());
     return GM_OK;
@@ -486,8 +508,35 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans) {
     const int nchunk = (nrhs + 31) / 32;
     a.rch = (nrhs + nchunk - 1) / nchunk;
     a.trans = trans;
-    for (int h = 0; h < (int)e->levels.size(); ++h) launch_solve_forward_level<R>(a, e->levels[h], e->st);
-    for (int h = (int)e->levels.size() - 1; h >= 0; --h) launch_solve_backward_level<R>(a, e->levels[h], e->st);
+    // GM_TRACE_LEVELS=1: device time of every level of both passes on stderr
+    static const bool trace = std::getenv("GM_TRACE_LEVELS") != nullptr;
+    const int nl = (int)e->levels.size();
+    std::vector<cudaEvent_t> ev;
+    if (trace) {
+        ev.resize(2 * nl + 1);
+        for (auto &x : ev) cudaEventCreate(&x);
+        cudaEventRecord(ev[0], e->st);
+    }
+    for (int h = 0; h < nl; ++h) {
+        launch_solve_forward_level<R>(a, e->levels[h], e->st);
+        if (trace) cudaEventRecord(ev[1 + h], e->st);
+    }
+    for (int h = nl - 1; h >= 0; --h) {
+        launch_solve_backward_level<R>(a, e->levels[h], e->st);
+        if (trace) cudaEventRecord(ev[1 + nl + (nl - 1 - h)], e->st);
+    }
+    if (trace) {
+        cudaEventSynchronize(ev[2 * nl]);
+        for (int h = 0; h < nl; ++h) {
+            float fm = 0, bm = 0;
+            cudaEventElapsedTime(&fm, ev[h], ev[1 + h]);
+            cudaEventElapsedTime(&bm, ev[nl + (nl - 1 - h)], ev[1 + nl + (nl - 1 - h)]);
+            const LevelInfo &L = e->levels[h];
+            std::fprintf(stderr, "subst %s level %2d: fronts %5d max_front %4d max_piv %4d max_ring %4d fwd %.3f ms bwd %.3f ms\n",
+                         sizeof(R) == 8 ? "c128" : "c64", h, L.count, L.max_front, L.max_piv, L.max_ring, fm, bm);
+        }
+        for (auto &x : ev) cudaEventDestroy(x);
+    }
     cudaEventRecord(e->ev_s1, e->st);
     cudaEventSynchronize(e->ev_s1);
     float ms = 0;
