@@ -495,7 +495,7 @@ extern "C" int gm_get_triplets(gm_engine *e, int ifreq, double *Ar, double *Ai, 
 namespace gm {
 
 template <class R>
-static void substitute(gm_engine *e, void *xT, int nrhs, int trans) {
+static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsigned char *mask = nullptr) {
     cudaEventRecord(e->ev_s0, e->st);
     SolveArgs<R> a{};
     a.s = e->dsym;
@@ -508,6 +508,8 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans) {
     const int nchunk = (nrhs + 31) / 32;
     a.rch = (nrhs + nchunk - 1) / nchunk;
     a.trans = trans;
+    a.mask = mask;
+    a.mask_nch = (nrhs + 31) / 32;
     // GM_TRACE_LEVELS=1: device time of every level of both passes on stderr
     static const bool trace = std::getenv("GM_TRACE_LEVELS") != nullptr;
     const int nl = (int)e->levels.size();
@@ -545,8 +547,33 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans) {
     e->stats.n_subst += 1;
 }
 
+// Forward-pass pruning mask from a right-hand-side pattern: node v is live
+// for right-hand-side group g (32 columns) when a column of the group is
+// nonzero on a pivot row of v's subtree -- the owner of every nonzero row
+// and that node's ancestors.  Returns the device mask, or NULL (dense).
+static const unsigned char *build_mask(gm_engine *e, int nrhs, const RhsPattern *pat) {
+    if (!pat || (!pat->per_col && !pat->common) || std::getenv("GM_NO_PRUNE")) return nullptr;
+    const Symbolic &sy = e->sym;
+    const int nch = (nrhs + 31) / 32, nn = sy.nnodes;
+    std::vector<unsigned char> m((size_t)nn * nch, 0);
+    auto mark = [&](int row, int g) {
+        if (row < 0 || row >= sy.n) return;
+        for (int v = sy.owner[row]; v >= 0 && !m[(size_t)v * nch + g]; v = sy.parent[v]) m[(size_t)v * nch + g] = 1;
+    };
+    if (pat->per_col)
+        for (int r = 0; r < std::min(nrhs, pat->ncol); ++r) mark(pat->per_col[r], r / 32);
+    for (int i = 0; i < pat->ncommon; ++i)
+        for (int g = 0; g < nch; ++g) mark(pat->common[i], g);
+    if (e->d_mask.ensure(m.size()) != cudaSuccess) return nullptr;   // fall back to the dense pass
+    if (cudaMemcpyAsync(e->d_mask.p, m.data(), m.size(), cudaMemcpyHostToDevice, e->st) != cudaSuccess) return nullptr;
+    cudaStreamSynchronize(e->st);   // m is released on return
+    return e->d_mask.as<unsigned char>();
+}
+
 // x (device, [nf][n][nrhs] c128) = M'^{-1} b with FP64 refinement; b, x device.
-int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const double2 *d_b) {
+// The first substitution prunes the forward pass by `pattern` when given;
+// the refinement sweeps (dense residuals) do not.
+int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const double2 *d_b, const RhsPattern *pattern) {
     const size_t cnt = (size_t)e->nf * e->n * nrhs;
     const bool fp64 = e->cfg.precision == GM_PREC_FP64;
     GM_ALLOC(e->d_t, cnt * e->csize());
@@ -563,8 +590,9 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     if (fp64) launch_convert_down<double>(d_b, e->d_t.p, cnt, e->st);
     else launch_convert_down<float>(d_b, e->d_t.p, cnt, e->st);
     GM_CUDA(cudaMemsetAsync(d_x, 0, cnt * sizeof(double2), e->st));
-    if (fp64) substitute<double>(e, e->d_t.p, nrhs, sys);
-    else substitute<float>(e, e->d_t.p, nrhs, sys);
+    const unsigned char *mask = build_mask(e, nrhs, pattern);
+    if (fp64) substitute<double>(e, e->d_t.p, nrhs, sys, mask);
+    else substitute<float>(e, e->d_t.p, nrhs, sys, mask);
     if (fp64) launch_add_up<double>(d_x, e->d_t.p, cnt, e->st);
     else launch_add_up<float>(d_x, e->d_t.p, cnt, e->st);
     GM_CUDA(cudaGetLastError());

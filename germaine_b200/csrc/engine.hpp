@@ -81,6 +81,7 @@ struct gm_engine {
     // epilogue state
     gm::DevBuf d_src_k, d_rec_k, d_seis, d_field, d_res, d_grad, d_frame, d_frame_pass, d_misc;
     gm::DevBuf d_xf, d_xa;   // forward / adjoint solutions kept for the gradient
+    gm::DevBuf d_mask;       // forward-pass pruning mask of the current solve
     std::vector<double> last_grad0, last_grad1;
     std::vector<double> last_hess0, last_hess1;
 
@@ -102,6 +103,18 @@ struct gm_engine {
 };
 
 namespace gm {
+// Where the right-hand sides can be nonzero (for pruning the forward pass of
+// the first substitution): right-hand side r is nonzero at most on row
+// per_col[r] (a spike; -1: none) and on the rows in `common`.  Rows are grid
+// indices.  A solve given no pattern treats every right-hand side as dense.
+struct RhsPattern {
+    const int *per_col = nullptr;
+    int ncol = 0;
+    const int *common = nullptr;
+    int ncommon = 0;
+};
+
 // internal entry points shared between translation units
-int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x_out, const double2 *d_b_in);
+int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x_out, const double2 *d_b_in,
+                        const RhsPattern *pattern = nullptr);
 }

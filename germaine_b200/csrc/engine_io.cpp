@@ -93,7 +93,10 @@ int forward_solve(gm_engine *e, int ns, const Geometry &g, double2 *xout, int sr
     GM_ALLOC(e->d_b, (size_t)nf * n * ns * sizeof(double2));
     gm::launch_spikes(e->d_b.as<double2>(), n, nf, ns, e->d_src_k.as<int>(), amp_buf.as<double2>(), e->st);
     GM_CUDA(cudaGetLastError());
-    rc = gm::engine_solve_device(e, GM_SYS_A, ns, xout, e->d_b.as<double2>());
+    gm::RhsPattern pat;   // one spike per shot: prune the forward pass
+    pat.per_col = g.ksrc.data();
+    pat.ncol = ns;
+    rc = gm::engine_solve_device(e, GM_SYS_A, ns, xout, e->d_b.as<double2>(), &pat);
     GM_CUDA(cudaStreamSynchronize(e->st));  // amp_buf is released on return
     return rc;
 }
@@ -273,7 +276,10 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     GM_CUDA(cudaGetLastError());
     GM_ALLOC(e->d_xa, (size_t)nf * n * nshots * sizeof(double2));
     const int sys = te ? GM_SYS_AT : GM_SYS_A;   // grad_obj_TE.c:149 vs grad_obj_AC.c:147
-    const int arc = gm::engine_solve_device(e, sys, nshots, e->d_xa.as<double2>(), e->d_b.as<double2>());
+    gm::RhsPattern pat;   // adjoint sources only at the receivers
+    pat.common = g.kadj.data();
+    pat.ncommon = ntr;
+    const int arc = gm::engine_solve_device(e, sys, nshots, e->d_xa.as<double2>(), e->d_b.as<double2>(), &pat);
     if (arc < 0) return arc;
     if (arc > worst) worst = arc;
 
@@ -385,7 +391,10 @@ extern "C" int gm_hessian(gm_engine *e, int mode, int nshots, const float *src_x
             gm::launch_spikes(e->d_b.as<double2>(), n, nf, nr, e->d_rec_k.as<int>() + r0, amp_buf.as<double2>(), e->st);
             GM_CUDA(cudaGetLastError());
             // the reference solves with UMFPACK_A for both physics (src/AC/hessian_AC.c:140, src/TE/hessian_TE.c:140)
-            const int src = gm::engine_solve_device(e, GM_SYS_A, nr, e->d_xa.as<double2>(), e->d_b.as<double2>());
+            gm::RhsPattern pat;   // one receiver spike per right-hand side
+            pat.per_col = g.kadj.data() + r0;
+            pat.ncol = nr;
+            const int src = gm::engine_solve_device(e, GM_SYS_A, nr, e->d_xa.as<double2>(), e->d_b.as<double2>(), &pat);
             if (src < 0) return src;
             if (src > worst) worst = src;
             gm::launch_hess_sq(e->d_xa.as<double2>(), n, nf, nr, sqg, r0 > 0, e->st);

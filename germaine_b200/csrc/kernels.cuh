@@ -112,6 +112,11 @@ struct SolveArgs {
     int nf, nrhs, ldr;
     int rch;                  // right-hand sides per CTA (<= 32)
     int trans;                // 0: M x = b, 1: M^T x = b
+    // forward-pass pruning (NULL: every front carries data): mask[v * mask_nch + g]
+    // is 0 when right-hand sides 32 g .. 32 g + 31 are zero on every pivot row of
+    // node v's subtree, so that node's y and update vector are zero
+    const unsigned char *mask;
+    int mask_nch;
 };
 
 template <class R>

@@ -4,11 +4,12 @@
 // every frequency).
 //
 // Right-hand sides / solutions are [nf][n][ldr] complex, right-hand side
-// fastest.  Work units are (front, frequency, slice of TC = 32 right-hand
+// fastest.  Work units are (front, frequency, slice of 32 or 40 right-hand
 // sides).  The factorisation stores, in every 32 x 32 diagonal block, the
 // inverses of the block's triangles, so every step below is a small GEMM on
-// CUDA cores: 128 threads, each owning a 4 x 4 complex register tile of a
-// 64-row x 32-right-hand-side output tile, operands staged in shared memory.
+// CUDA cores: 128 threads, each owning a (RT/16) x B complex register tile
+// of an RT-row x 8B-right-hand-side output tile, operands staged in shared
+// memory.
 //
 // Pivot rows are solved in place in x (their rows of x hold the right-hand
 // side, then y, then the solution); the workspace w holds only each front's
@@ -37,17 +38,19 @@
 namespace gm {
 
 constexpr int SNB = 32;   // pivot block (= factorisation block)
-constexpr int TC = 32;    // right-hand sides per CTA
 constexpr int NT = 128;   // threads per CTA
-// RT (output rows per tile, 64 or 32) is a template parameter: 64-row tiles
-// reuse each staged right-hand-side row over more factor rows; 32-row tiles
-// halve the accumulators and the factor tile, so more CTAs fit on an SM --
-// the better trade on the small fronts of the lower tree levels.
+// Template parameters of the kernels:
+//   RT (output rows per tile, 64 or 32): 64-row tiles reuse each staged
+//      right-hand-side row over more factor rows; 32-row tiles halve the
+//      accumulators and the factor tile, so more CTAs fit on an SM -- the
+//      better trade on the small fronts of the lower tree levels;
+//   B (right-hand sides per CTA = 8 B): every slice re-stages the front's
+//      factor tiles, so wider slices read the factors fewer times.
 
-template <class C, int RT>
+template <class C, int RT, int B>
 struct SolveSmem {
-    C L[SNB][RT];    // factor tile, [pivot q][row]
-    C Y[SNB][TC];    // right operand, [pivot q][rhs]
+    C L[SNB][RT];       // factor tile, [pivot q][row]
+    C Y[SNB][8 * B];    // right operand, [pivot q][rhs]
 };
 
 // factor element M'(i, c) of the forward (L') or backward (U') factor:
@@ -61,8 +64,8 @@ __device__ __forceinline__ C elem(const C *F, int f, int i, int c) {
 // outside are left as they are: tile_mma reads only q < qb, and rows >= rows
 // (or right-hand sides >= rn) only feed accumulators that are never stored,
 // so partial tiles stage only what they use.
-template <class C, bool TRANS, int RT>
-__device__ __forceinline__ void stage_factor(SolveSmem<C, RT> &sm, const C *F, int f, int i0, int rows, int c0, int qb) {
+template <class C, bool TRANS, int RT, int B>
+__device__ __forceinline__ void stage_factor(SolveSmem<C, RT, B> &sm, const C *F, int f, int i0, int rows, int c0, int qb) {
     if (!TRANS) {
         for (int t = threadIdx.x; t < RT * qb; t += NT) {
             const int row = t % RT, q = t / RT;
@@ -81,8 +84,8 @@ __device__ __forceinline__ void stage_factor(SolveSmem<C, RT> &sm, const C *F, i
 //   !FWD && !TRANS: U^-1       !FWD && TRANS: (L^-1)^T
 // The stored block holds L^-1 strictly below the diagonal (unit diagonal
 // implied) and U^-1 on and above it.
-template <class C, bool FWD, bool TRANS, int RT>
-__device__ __forceinline__ void stage_dinv(SolveSmem<C, RT> &sm, const C *F, int f, int k0, int kb) {
+template <class C, bool FWD, bool TRANS, int RT, int B>
+__device__ __forceinline__ void stage_dinv(SolveSmem<C, RT, B> &sm, const C *F, int f, int k0, int kb) {
     for (int t = threadIdx.x; t < SNB * kb; t += NT) {
         const int p = t % SNB, q = t / SNB;   // operator entry (p, q) -> sm.L[q][p], q < kb
         if (p >= kb) continue;
@@ -104,49 +107,49 @@ __device__ __forceinline__ void stage_dinv(SolveSmem<C, RT> &sm, const C *F, int
 // groups b that lie entirely outside are skipped warp-uniformly (a warp owns
 // rows 4w..4w+3 of each 16-row group), so small fronts and short slices do
 // not pay for the full 64 x 32 tile.
-template <class C, int RT>
-__device__ __forceinline__ void tile_mma(const SolveSmem<C, RT> &sm, int qb, C (&acc)[RT / 16][4], int tr, int tc,
+template <class C, int RT, int B>
+__device__ __forceinline__ void tile_mma(const SolveSmem<C, RT, B> &sm, int qb, C (&acc)[RT / 16][B], int tr, int tc,
                                          int rows, int rn) {
     constexpr int A = RT / 16;
     const int wrow = (threadIdx.x >> 5) * 4;
     const int na = rows <= wrow ? 0 : min(A, (rows - wrow + 15) / 16);
-    const int nb = min(4, (rn + 7) / 8);
+    const int nb = min(B, (rn + 7) / 8);
     if (na == 0) return;   // warp-uniform: this warp owns no row of the tile
 #pragma unroll 2
     for (int q = 0; q < qb; ++q) {
-        C l[A], y[4];
+        C l[A], y[B];
 #pragma unroll
         for (int a = 0; a < A; ++a) l[a] = a < na ? sm.L[q][tr + 16 * a] : czero<C>();
 #pragma unroll
-        for (int b = 0; b < 4; ++b) y[b] = b < nb ? sm.Y[q][tc + 8 * b] : czero<C>();
+        for (int b = 0; b < B; ++b) y[b] = b < nb ? sm.Y[q][tc + 8 * b] : czero<C>();
 #pragma unroll
         for (int a = 0; a < A; ++a) {
             if (a >= na) break;
 #pragma unroll
-            for (int b = 0; b < 4; ++b)
+            for (int b = 0; b < B; ++b)
                 if (b < nb) cfma(acc[a][b], l[a], y[b]);
         }
     }
 }
 
-template <class C, int A>
-__device__ __forceinline__ void zero_acc(C (&acc)[A][4]) {
+template <class C, int A, int B>
+__device__ __forceinline__ void zero_acc(C (&acc)[A][B]) {
 #pragma unroll
     for (int a = 0; a < A; ++a)
 #pragma unroll
-        for (int b = 0; b < 4; ++b) acc[a][b] = czero<C>();
+        for (int b = 0; b < B; ++b) acc[a][b] = czero<C>();
 }
 
 // row_ptr(row)[col] -= acc for the thread's rows (< rows) and columns (< rn)
-template <class C, int A, class RowPtr>
-__device__ __forceinline__ void sub_acc(RowPtr row_ptr, int rows, int rn, const C (&acc)[A][4], int tr, int tc) {
+template <class C, int A, int B, class RowPtr>
+__device__ __forceinline__ void sub_acc(RowPtr row_ptr, int rows, int rn, const C (&acc)[A][B], int tr, int tc) {
 #pragma unroll
     for (int a = 0; a < A; ++a) {
         const int row = tr + 16 * a;
         if (row >= rows) continue;
         C *v = row_ptr(row);
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < B; ++b) {
             const int col = tc + 8 * b;
             if (col < rn) v[col] = csub(v[col], acc[a][b]);
         }
@@ -154,12 +157,24 @@ __device__ __forceinline__ void sub_acc(RowPtr row_ptr, int rows, int rn, const 
 }
 
 // sm.Y[q][r] = row_ptr(q)[r] for q < qb, r < rn (entries outside: as above)
-template <class C, int RT, class RowPtr>
-__device__ __forceinline__ void stage_rows(SolveSmem<C, RT> &sm, RowPtr row_ptr, int qb, int rn) {
+template <class C, int RT, int B, class RowPtr>
+__device__ __forceinline__ void stage_rows(SolveSmem<C, RT, B> &sm, RowPtr row_ptr, int qb, int rn) {
+    constexpr int TC = 8 * B;
     for (int t = threadIdx.x; t < qb * TC; t += NT) {
         const int q = t / TC, r = t % TC;
         if (r < rn) sm.Y[q][r] = row_ptr(q)[r];
     }
+}
+
+// false when right-hand sides r0 .. r0 + rn - 1 are zero throughout node v's
+// subtree (forward-pass pruning mask; no mask: always true)
+template <class R>
+__device__ __forceinline__ bool live(const SolveArgs<R> &a, int v, int r0, int rn) {
+    if (!a.mask) return true;
+    const unsigned char *m = a.mask + (size_t)v * a.mask_nch;
+    for (int g = r0 >> 5; g <= (r0 + rn - 1) >> 5; ++g)
+        if (m[g]) return true;
+    return false;
 }
 
 template <class R>
@@ -172,7 +187,7 @@ struct Ctx {
     C *W;   // this node's update vector: ring row i (front position s + i)
 };
 
-template <class R>
+template <class R, int TC>
 __device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first, int chunk) {
     using C = cplx<R>;
     Ctx<R> c;
@@ -192,43 +207,47 @@ __device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first,
 // Forward pass, pivot part: add the children's update vectors (gathered by
 // the extend-add inverse maps) into x at this front's pivots, then solve the
 // pivot rows in place in x, 32-pivot block by block.
-template <class R, bool TRANS, int RT>
+template <class R, bool TRANS, int RT, int B>
 __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, int fused) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SolveSmem<C, RT> &sm = *reinterpret_cast<SolveSmem<C, RT> *>(smem_raw);
-    const Ctx<R> c = make_ctx(a, lvl_first, blockIdx.x);
+    SolveSmem<C, RT, B> &sm = *reinterpret_cast<SolveSmem<C, RT, B> *>(smem_raw);
+    constexpr int TC = 8 * B;
+    const Ctx<R> c = make_ctx<R, TC>(a, lvl_first, blockIdx.x);
     if (c.rn <= 0) return;
+    const int r0 = blockIdx.x * TC;
+    if (!live(a, c.node, r0, c.rn)) return;   // y and the update vector are zero
     (void)fused;
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int *inv = a.s.inv + a.s.inv_off[c.node];
     const size_t fz = blockIdx.z;
-    const C *Wall = reinterpret_cast<const C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + blockIdx.x * TC;
+    const C *Wall = reinterpret_cast<const C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + r0;
     const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
-    const C *W0 = c0 >= 0 ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
-    const C *W1 = c1 >= 0 ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
+    const C *W0 = c0 >= 0 && live(a, c0, r0, c.rn) ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
+    const C *W1 = c1 >= 0 && live(a, c1, r0, c.rn) ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
     const size_t ldr = a.ldr;
 
     if (W0 || W1) {   // children's update vectors at the pivots (the ring part is k_fwd_ring's)
         for (int i = warp; i < c.s; i += NT / 32) {
-            if (lane >= c.rn) continue;
             const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
             if (q0 < 0 && q1 < 0) continue;
-            C v = czero<C>();
-            if (q0 >= 0) v = cadd(v, W0[(size_t)q0 * ldr + lane]);
-            if (q1 >= 0) v = cadd(v, W1[(size_t)q1 * ldr + lane]);
-            C &x = c.X[(size_t)c.vars[i] * ldr + lane];
-            x = cadd(x, v);
+            for (int r = lane; r < c.rn; r += 32) {
+                C v = czero<C>();
+                if (q0 >= 0) v = cadd(v, W0[(size_t)q0 * ldr + r]);
+                if (q1 >= 0) v = cadd(v, W1[(size_t)q1 * ldr + r]);
+                C &x = c.X[(size_t)c.vars[i] * ldr + r];
+                x = cadd(x, v);
+            }
         }
         __syncthreads();
     }
 
     auto xrow = [&](int k) { return c.X + (size_t)c.vars[k] * ldr; };
-    C acc[RT / 16][4];
+    C acc[RT / 16][B];
     for (int k0 = 0; k0 < c.s; k0 += SNB) {
         const int kb = min(SNB, c.s - k0);
-        stage_dinv<C, true, TRANS, RT>(sm, c.F, c.f, k0, kb);
+        stage_dinv<C, true, TRANS, RT, B>(sm, c.F, c.f, k0, kb);
         stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
         __syncthreads();
         zero_acc(acc);
@@ -238,7 +257,7 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
         for (int a2 = 0; a2 < 2; ++a2) {
             const int p = tr + 16 * a2;
 #pragma unroll
-            for (int b = 0; b < 4; ++b) sm.Y[p][tc + 8 * b] = acc[a2][b];
+            for (int b = 0; b < B; ++b) sm.Y[p][tc + 8 * b] = acc[a2][b];
         }
         __syncthreads();
         for (int t = threadIdx.x; t < kb * TC; t += NT) {
@@ -247,7 +266,7 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
         }
         for (int i0 = k0 + kb; i0 < c.s; i0 += RT) {
             const int rows = min(RT, c.s - i0);
-            stage_factor<C, TRANS, RT>(sm, c.F, c.f, i0, rows, k0, kb);
+            stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, k0, kb);
             __syncthreads();
             zero_acc(acc);
             tile_mma(sm, kb, acc, tr, tc, rows, c.rn);
@@ -261,23 +280,25 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
 // Forward pass, ring part: update vector = children's update vectors at the
 // ring rows - L'(ring, pivots) y, 64-row tiles of the ring over many CTAs;
 // blockIdx.x = chunk + nchunk * tile
-template <class R, bool TRANS, int RT>
+template <class R, bool TRANS, int RT, int B>
 __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, int nchunk) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SolveSmem<C, RT> &sm = *reinterpret_cast<SolveSmem<C, RT> *>(smem_raw);
+    SolveSmem<C, RT, B> &sm = *reinterpret_cast<SolveSmem<C, RT, B> *>(smem_raw);
+    constexpr int TC = 8 * B;
     const int chunk = blockIdx.x % nchunk, tile = blockIdx.x / nchunk;
-    const Ctx<R> c = make_ctx(a, lvl_first, chunk);
+    const Ctx<R> c = make_ctx<R, TC>(a, lvl_first, chunk);
     const int i0 = c.s + tile * RT;
     if (c.rn <= 0 || i0 >= c.f) return;
+    if (!live(a, c.node, chunk * TC, c.rn)) return;   // the update vector is zero (never read)
     const int rows = min(RT, c.f - i0);
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const size_t ldr = a.ldr;
-    C acc[RT / 16][4];
+    C acc[RT / 16][B];
     zero_acc(acc);
     for (int q0 = 0; q0 < c.s; q0 += SNB) {
         const int qb = min(SNB, c.s - q0);
-        stage_factor<C, TRANS, RT>(sm, c.F, c.f, i0, rows, q0, qb);
+        stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, q0, qb);
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q0 + q] * ldr; }, qb, c.rn);
         __syncthreads();
         tile_mma(sm, qb, acc, tr, tc, rows, c.rn);
@@ -287,17 +308,17 @@ __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, 
     const int *inv = a.s.inv + a.s.inv_off[c.node];
     const C *Wall = reinterpret_cast<const C *>(a.w) + (size_t)blockIdx.z * a.s.rhs_total * a.ldr + chunk * TC;
     const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
-    const C *W0 = c0 >= 0 ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
-    const C *W1 = c1 >= 0 ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
+    const C *W0 = c0 >= 0 && live(a, c0, chunk * TC, c.rn) ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
+    const C *W1 = c1 >= 0 && live(a, c1, chunk * TC, c.rn) ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
 #pragma unroll
-    for (int p = 0; p < 4; ++p) {
+    for (int p = 0; p < RT / 16; ++p) {
         const int row = tr + 16 * p;
         if (row >= rows) continue;
         const int i = i0 + row;
         const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
         C *w = c.W + (size_t)(i - c.s) * ldr;
 #pragma unroll
-        for (int b = 0; b < 4; ++b) {
+        for (int b = 0; b < B; ++b) {
             const int r = tc + 8 * b;
             if (r >= c.rn) continue;
             C g = czero<C>();
@@ -310,23 +331,24 @@ __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, 
 
 // Backward pass, ring part: x[pivots] -= U'(pivots, ring) x[ring]
 // (final values of the ancestors' variables); blockIdx.x = chunk + nchunk * tile
-template <class R, bool TRANS, int RT>
+template <class R, bool TRANS, int RT, int B>
 __global__ void __launch_bounds__(NT) k_bwd_ring(SolveArgs<R> a, int lvl_first, int nchunk) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SolveSmem<C, RT> &sm = *reinterpret_cast<SolveSmem<C, RT> *>(smem_raw);
+    SolveSmem<C, RT, B> &sm = *reinterpret_cast<SolveSmem<C, RT, B> *>(smem_raw);
+    constexpr int TC = 8 * B;
     const int chunk = blockIdx.x % nchunk, tile = blockIdx.x / nchunk;
-    const Ctx<R> c = make_ctx(a, lvl_first, chunk);
+    const Ctx<R> c = make_ctx<R, TC>(a, lvl_first, chunk);
     const int i0 = tile * RT;
     if (c.rn <= 0 || i0 >= c.s || c.f == c.s) return;
     const int rows = min(RT, c.s - i0);
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const size_t ldr = a.ldr;
-    C acc[RT / 16][4];
+    C acc[RT / 16][B];
     zero_acc(acc);
     for (int j0 = c.s; j0 < c.f; j0 += SNB) {
         const int jb = min(SNB, c.f - j0);
-        stage_factor<C, TRANS, RT>(sm, c.F, c.f, i0, rows, j0, jb);
+        stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, j0, jb);
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[j0 + q] * ldr; }, jb, c.rn);
         __syncthreads();
         tile_mma(sm, jb, acc, tr, tc, rows, c.rn);
@@ -337,22 +359,23 @@ __global__ void __launch_bounds__(NT) k_bwd_ring(SolveArgs<R> a, int lvl_first, 
 
 // Backward pass, pivot part: block by block from the last, x_b = Dinv t_b in
 // place in x, then t_above -= U'(above, b) x_b.
-template <class R, bool TRANS, int RT>
+template <class R, bool TRANS, int RT, int B>
 __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, int fused) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
-    SolveSmem<C, RT> &sm = *reinterpret_cast<SolveSmem<C, RT> *>(smem_raw);
-    const Ctx<R> c = make_ctx(a, lvl_first, blockIdx.x);
+    SolveSmem<C, RT, B> &sm = *reinterpret_cast<SolveSmem<C, RT, B> *>(smem_raw);
+    constexpr int TC = 8 * B;
+    const Ctx<R> c = make_ctx<R, TC>(a, lvl_first, blockIdx.x);
     if (c.rn <= 0) return;
     (void)fused;
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const size_t ldr = a.ldr;
     auto xrow = [&](int k) { return c.X + (size_t)c.vars[k] * ldr; };
-    C acc[RT / 16][4];
+    C acc[RT / 16][B];
     const int nblk = (c.s + SNB - 1) / SNB;
     for (int b = nblk - 1; b >= 0; --b) {
         const int k0 = b * SNB, kb = min(SNB, c.s - k0);
-        stage_dinv<C, false, TRANS, RT>(sm, c.F, c.f, k0, kb);
+        stage_dinv<C, false, TRANS, RT, B>(sm, c.F, c.f, k0, kb);
         stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
         __syncthreads();
         zero_acc(acc);
@@ -362,7 +385,7 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
         for (int a2 = 0; a2 < 2; ++a2) {
             const int p = tr + 16 * a2;
 #pragma unroll
-            for (int bb = 0; bb < 4; ++bb) sm.Y[p][tc + 8 * bb] = acc[a2][bb];
+            for (int bb = 0; bb < B; ++bb) sm.Y[p][tc + 8 * bb] = acc[a2][bb];
         }
         __syncthreads();
         for (int t = threadIdx.x; t < kb * TC; t += NT) {
@@ -371,7 +394,7 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
         }
         for (int i0 = 0; i0 < k0; i0 += RT) {
             const int rows = min(RT, k0 - i0);
-            stage_factor<C, TRANS, RT>(sm, c.F, c.f, i0, rows, k0, kb);
+            stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, k0, kb);
             __syncthreads();
             zero_acc(acc);
             tile_mma(sm, kb, acc, tr, tc, rows, c.rn);
@@ -381,23 +404,28 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
     }
 }
 
-template <class R, int RT>
-static size_t solve_smem() { return sizeof(SolveSmem<cplx<R>, RT>); }
+template <class R, int RT, int B>
+static size_t solve_smem() { return sizeof(SolveSmem<cplx<R>, RT, B>); }
 
-template <class R, int RT>
+template <class R, int RT, int B>
 static void set_attrs() {
     static bool done = false;
     if (done) return;
-    const int sm = (int)solve_smem<R, RT>();
-    cudaFuncSetAttribute((const void *)k_fwd_piv<R, false, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute((const void *)k_fwd_piv<R, true, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute((const void *)k_fwd_ring<R, false, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute((const void *)k_fwd_ring<R, true, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute((const void *)k_bwd_ring<R, false, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute((const void *)k_bwd_ring<R, true, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute((const void *)k_bwd_piv<R, false, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
-    cudaFuncSetAttribute((const void *)k_bwd_piv<R, true, RT>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    const int sm = (int)solve_smem<R, RT, B>();
+    cudaFuncSetAttribute((const void *)k_fwd_piv<R, false, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_fwd_piv<R, true, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_fwd_ring<R, false, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_fwd_ring<R, true, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_bwd_ring<R, false, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_bwd_ring<R, true, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_bwd_piv<R, false, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    cudaFuncSetAttribute((const void *)k_bwd_piv<R, true, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     done = true;
+}
+
+static int env_int(const char *name) {
+    const char *v = std::getenv(name);
+    return v ? std::atoi(v) : 0;
 }
 
 // Tile height of a level: 32-row tiles wherever the level has many fronts
@@ -406,58 +434,81 @@ static void set_attrs() {
 // top levels of at most four fronts, where the tiles of one front are the
 // parallelism.  GM_SOLVE_RT=32 / 64 forces one height on every level.
 static int level_rt(const LevelInfo &L) {
-    static const int forced = [] {
-        const char *v = std::getenv("GM_SOLVE_RT");
-        return v ? std::atoi(v) : 0;
-    }();
+    static const int forced = env_int("GM_SOLVE_RT");
     if (forced == 32 || forced == 64) return forced;
     return L.count > 4 ? 32 : 64;
 }
 
-template <class R, int RT>
+// Right-hand-side slice width (8 B).  Measured on 841 x 227 with 100
+// right-hand sides: 32 / 40 / 56 columns give 36.6 / 36.6 / 38.0 ms per
+// complex128 substitution and 19.9 / 19.1 / 19.8 ms per complex64 one, so
+// the lower levels are not bound by re-reading the factors per slice.
+// GM_SOLVE_B=4 / 5 forces 32 / 40.
+template <class R>
+static int slice_b(int nrhs) {
+    static const int forced = env_int("GM_SOLVE_B");
+    if (forced == 4 || forced == 5) return forced;
+    return (sizeof(R) == 4 && nrhs > 32) ? 5 : 4;
+}
+
+template <class R, int RT, int B>
 static void forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
-    set_attrs<R, RT>();
-    const size_t smem = solve_smem<R, RT>();
-    const int nchunk = (a.nrhs + TC - 1) / TC;
+    set_attrs<R, RT, B>();
+    const size_t smem = solve_smem<R, RT, B>();
+    const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
     dim3 g1(nchunk, L.count, a.nf);
     const int fused = 0;   // separate ring kernel: more parallelism per level
-    if (a.trans) (k_fwd_piv<R, true, RT><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
-    else (k_fwd_piv<R, false, RT><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
+    if (a.trans) (k_fwd_piv<R, true, RT, B><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
+    else (k_fwd_piv<R, false, RT, B><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
     if (L.max_ring > 0) {
         dim3 g2(nchunk * ((L.max_ring + RT - 1) / RT), L.count, a.nf);
-        if (a.trans) (k_fwd_ring<R, true, RT><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
-        else (k_fwd_ring<R, false, RT><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
+        if (a.trans) (k_fwd_ring<R, true, RT, B><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
+        else (k_fwd_ring<R, false, RT, B><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
     }
 }
 
-template <class R, int RT>
+template <class R, int RT, int B>
 static void backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
-    set_attrs<R, RT>();
-    const size_t smem = solve_smem<R, RT>();
-    const int nchunk = (a.nrhs + TC - 1) / TC;
+    set_attrs<R, RT, B>();
+    const size_t smem = solve_smem<R, RT, B>();
+    const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
     const int fused = 0;
     if (L.max_ring > 0) {
         dim3 g1(nchunk * ((L.max_piv + RT - 1) / RT), L.count, a.nf);
-        if (a.trans) (k_bwd_ring<R, true, RT><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
-        else (k_bwd_ring<R, false, RT><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
+        if (a.trans) (k_bwd_ring<R, true, RT, B><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
+        else (k_bwd_ring<R, false, RT, B><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
     }
     dim3 g2(nchunk, L.count, a.nf);
-    if (a.trans) (k_bwd_piv<R, true, RT><<<g2, NT, smem, st>>>(a, L.first, fused), note_launch());
-    else (k_bwd_piv<R, false, RT><<<g2, NT, smem, st>>>(a, L.first, fused), note_launch());
+    if (a.trans) (k_bwd_piv<R, true, RT, B><<<g2, NT, smem, st>>>(a, L.first, fused), note_launch());
+    else (k_bwd_piv<R, false, RT, B><<<g2, NT, smem, st>>>(a, L.first, fused), note_launch());
+}
+
+template <class R, int B>
+static void level_pass(bool fwd, const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
+    if (level_rt(L) == 32) {
+        if (fwd) forward_level<R, 32, B>(a, L, st);
+        else backward_level<R, 32, B>(a, L, st);
+    } else {
+        if (fwd) forward_level<R, 64, B>(a, L, st);
+        else backward_level<R, 64, B>(a, L, st);
+    }
+}
+
+template <class R>
+static void dispatch(bool fwd, const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
+    if (L.count == 0) return;
+    if (slice_b<R>(a.nrhs) == 5) level_pass<R, 5>(fwd, a, L, st);
+    else level_pass<R, 4>(fwd, a, L, st);
 }
 
 template <class R>
 void launch_solve_forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
-    if (L.count == 0) return;
-    if (level_rt(L) == 32) forward_level<R, 32>(a, L, st);
-    else forward_level<R, 64>(a, L, st);
+    dispatch<R>(true, a, L, st);
 }
 
 template <class R>
 void launch_solve_backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
-    if (L.count == 0) return;
-    if (level_rt(L) == 32) backward_level<R, 32>(a, L, st);
-    else backward_level<R, 64>(a, L, st);
+    dispatch<R>(false, a, L, st);
 }
 
 template void launch_solve_forward_level<double>(const SolveArgs<double> &, const LevelInfo &, cudaStream_t);

@@ -140,7 +140,8 @@ void build_symbolic(int nx, int ny, int leaf_max, Symbolic &s) {
     }
 
     // owner node of every pivot
-    std::vector<int> owner(s.n, -1);
+    s.owner.assign(s.n, -1);
+    std::vector<int> &owner = s.owner;
     for (int v = 0; v < nn; ++v)
         for (int i = 0; i < s.npiv[v]; ++i) owner[s.vars[s.var_off[v] + i]] = v;
 

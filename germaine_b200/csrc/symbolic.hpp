@@ -29,6 +29,7 @@ struct Symbolic {
 
     // per node (postorder: children before parents)
     std::vector<int> npiv, nfront, parent, height, child0, child1;
+    std::vector<int> owner;          // grid index -> node that eliminates it
     std::vector<int64_t> var_off;    // vars[var_off[v] .. + nfront[v]): pivots first, then ring
     std::vector<int> vars;           // grid indices
     std::vector<int64_t> front_off;  // column-major nfront x nfront block per node
