@@ -47,9 +47,10 @@ sys.path.insert(0, ROOT)
 
 DH, NPML, ROW = 25.0, 20, 2
 METRIC = "shot-solves/s (factor+solve) mixed vs FP64 on B200 at resid<=1e-10; %roofline"
-# DRAM bytes of one complex128 substitution on 4 frequencies (first 50 K5
-# launches of the FP64 engine, ncu dram__bytes_read.sum + write.sum)
-SUBST_TRAFFIC_FP64_4FREQ = 15.221e9
+# DRAM bytes of one complex128 backward substitution pass on 4 frequencies
+# (the first k_bwd_ring / k_bwd_piv launches of the FP64 engine, ncu
+# dram__bytes_read.sum + dram__bytes_write.sum)
+BWD_TRAFFIC_FP64_4FREQ = 6.813e9
 
 # the benchmark workload; --nx0/--ny0/--nfreq/--nshots shrink it for
 # profiling captures (the bench line then names the smaller workload)
@@ -291,18 +292,20 @@ def run_gpu(args):
     head = results[head_name]
     value = units / (head["ms"] * 1e-3)
     st = head["stats"]
-    # roofline of the substitution (K5, the dominant kernel group): factor
-    # entries read once per substitution + right-hand sides read and
-    # written, over the device time of one substitution
+    # roofline of the backward substitution pass (K5 k_bwd_ring + k_bwd_piv,
+    # the dense part of every solve: the forward pass is pruned to the
+    # fronts on the paths from the sources to the root): the stored U
+    # entries read once + the right-hand sides read (y, ancestors' x) and the
+    # solution written, over the device time of the backward passes
     csize = 16 if head_name == "fp64" else 8
-    subst_bytes = nf * (st["factor_entries"] * csize + 2 * st["n"] * ns * csize)
-    subst_ms = st["ms_subst"] / max(1, st["n_subst"])
+    subst_bytes = nf * (st["u_entries"] * csize + 2 * st["n"] * ns * csize)
+    subst_ms = st["ms_subst_bwd"] / max(1, st["n_subst"])
     achieved = subst_bytes / (subst_ms * 1e-3) / 1e9
     # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one
-    # substitution from ncu captures of this workload on 4 frequencies (the
-    # first 50 K5 launches of each engine), scaled by frequency count
-    per4 = {"mixed": 9.697e9, "fp64": SUBST_TRAFFIC_FP64_4FREQ}[head_name]
-    traffic = (per4 / 4 * nf if per4 and (W["nx0"], W["ny0"], W["nshots"], args.leaf) == (801, 187, 100, 64)
+    # backward pass from an ncu capture of this workload on 4 frequencies,
+    # scaled by frequency count
+    per4 = {"mixed": None, "fp64": BWD_TRAFFIC_FP64_4FREQ}[head_name]
+    traffic = (per4 / 4 * nf if per4 and (W["nx0"], W["ny0"], W["nshots"], args.leaf) == (801, 187, 100, 32)
                else None)
     line = {
         "metric": METRIC,
@@ -338,7 +341,7 @@ def run_gpu(args):
                       "gpu_launches_per_step": results[n]["launches"]}
                   for n in ("fp64", "mixed")},
         "mixed_over_fp64": fp64["ms"] / mixed["ms"],
-        "roofline": {"kernel": "K5 multi-RHS substitution (k_fwd + k_bwd, %s)" % ("complex128" if csize == 16 else "complex64"),
+        "roofline": {"kernel": "K5 backward substitution (k_bwd_ring + k_bwd_piv, %s)" % ("complex128" if csize == 16 else "complex64"),
                      "bound": "hbm", "achieved": achieved, "peak": peak_hbm, "unit": "GB/s",
                      "frac": achieved / peak_hbm, "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": subst_bytes, "ms_per_launch_group": subst_ms},
@@ -388,7 +391,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--seed", type=int, default=2024)
-    ap.add_argument("--leaf", type=int, default=64)
+    ap.add_argument("--leaf", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--nx0", type=int, default=W["nx0"], help="model width without PML (profiling cases)")
     ap.add_argument("--ny0", type=int, default=W["ny0"], help="model depth without PML (profiling cases)")

@@ -48,7 +48,8 @@ class GmStats(ctypes.Structure):
                 ("perturbed_pivots", ctypes.c_int64), ("ir_iterations", ctypes.c_int32),
                 ("ir_residual", ctypes.c_double), ("ms_assemble", ctypes.c_double),
                 ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double), ("ms_refine", ctypes.c_double),
-                ("ms_subst", ctypes.c_double), ("n_subst", ctypes.c_int32), ("kernel_launches", ctypes.c_int64)]
+                ("ms_subst", ctypes.c_double), ("n_subst", ctypes.c_int32), ("kernel_launches", ctypes.c_int64),
+                ("u_entries", ctypes.c_int64), ("ms_subst_bwd", ctypes.c_double)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

@@ -86,7 +86,7 @@ struct gm_engine {
     std::vector<double> last_hess0, last_hess1;
 
     gm_stats stats{};
-    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_s0 = nullptr, ev_s1 = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr, ev_s0 = nullptr, ev_s1 = nullptr, ev_sm = nullptr;
 
     gm_engine() = default;
     gm_engine(const gm_engine &) = delete;
@@ -96,6 +96,7 @@ struct gm_engine {
         if (ev1) cudaEventDestroy(ev1);
         if (ev_s0) cudaEventDestroy(ev_s0);
         if (ev_s1) cudaEventDestroy(ev_s1);
+        if (ev_sm) cudaEventDestroy(ev_sm);
         if (st) cudaStreamDestroy(st);
     }
 

@@ -192,7 +192,7 @@ void build_symbolic(int nx, int ny, int leaf_max, Symbolic &s) {
     }
 
     // exact flop and storage counts
-    s.factor_flops = 0; s.solve_flops_per_rhs = 0; s.factor_entries = 0;
+    s.factor_flops = 0; s.solve_flops_per_rhs = 0; s.factor_entries = 0; s.u_entries = 0;
     for (int v = 0; v < nn; ++v) {
         const double f = s.nfront[v], sp = s.npiv[v];
         for (int k = 0; k < s.npiv[v]; ++k) {
@@ -200,6 +200,7 @@ void build_symbolic(int nx, int ny, int leaf_max, Symbolic &s) {
             s.factor_flops += 8.0 * m * m + 6.0 * m;  // rank-1 update + column scaling by 1/pivot
         }
         s.factor_entries += (int64_t)(f * f - (f - sp) * (f - sp));
+        s.u_entries += (int64_t)(sp * (sp + 1) / 2 + sp * (f - sp));
         s.solve_flops_per_rhs += 8.0 * (f * f - (f - sp) * (f - sp));
     }
 }

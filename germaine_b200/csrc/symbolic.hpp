@@ -54,6 +54,7 @@ struct Symbolic {
     double factor_flops = 0;       // partial LU of every front
     double solve_flops_per_rhs = 0;// forward + backward substitution, one RHS
     int64_t factor_entries = 0;    // stored L+U entries (sum f^2 - (f-s)^2)
+    int64_t u_entries = 0;         // stored U entries (pivot rows from the diagonal on: s(s+1)/2 + s(f-s))
 };
 
 // Builds the nested-dissection symbolic structure of an nx x ny 9-point grid.

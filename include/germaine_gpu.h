@@ -70,7 +70,7 @@ typedef struct {
     int32_t physics;         /* GM_PHYS_* */
     int32_t precision;       /* GM_PREC_* */
     int32_t op_mode;         /* GM_OP_* */
-    int32_t leaf_max;        /* nested-dissection leaf size (0 = default 64) */
+    int32_t leaf_max;        /* nested-dissection leaf size (0 = default 32) */
     double ir_tol;           /* refinement target on max_k ||b_k - M x_k|| / ||b_k|| (0 = 1e-10) */
     int32_t ir_max_iter;     /* refinement iteration cap (0 = default 10) */
 } gm_config;
@@ -91,6 +91,8 @@ typedef struct {
     double ms_subst;            /* device time of the substitutions of the last solve */
     int32_t n_subst;            /* substitutions (initial + refinement) of the last solve */
     int64_t kernel_launches;    /* kernels launched by this library in this process */
+    int64_t u_entries;          /* stored U entries (pivot rows) per frequency: the backward pass's factor */
+    double ms_subst_bwd;        /* device time of the backward passes of those substitutions */
 } gm_stats;
 
 const char *gm_last_error(void);
