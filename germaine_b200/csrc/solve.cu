@@ -404,6 +404,63 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
     }
 }
 
+// Backward pass of a whole front whose pivots fit one 32-pivot block (the
+// small fronts of the lower levels): t = y - U'(pivots, ring) x[ring] with
+// the product accumulated in registers over 32-column ring blocks, t placed
+// in shared memory, then x_piv = Dinv t -- k_bwd_ring and k_bwd_piv in one
+// CTA, without writing t to x in between.
+template <class R, bool TRANS, int B>
+__global__ void __launch_bounds__(NT) k_bwd_small(SolveArgs<R> a, int lvl_first) {
+    using C = cplx<R>;
+    constexpr int RT = 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SolveSmem<C, RT, B> &sm = *reinterpret_cast<SolveSmem<C, RT, B> *>(smem_raw);
+    constexpr int TC = 8 * B;
+    const Ctx<R> c = make_ctx<R, TC>(a, lvl_first, blockIdx.x);
+    if (c.rn <= 0 || c.s == 0) return;
+    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
+    const size_t ldr = a.ldr;
+    const int s = c.s;   // <= SNB (launch condition)
+    C acc[RT / 16][B];
+    zero_acc(acc);
+    for (int j0 = s; j0 < c.f; j0 += SNB) {
+        const int jb = min(SNB, c.f - j0);
+        stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, 0, s, j0, jb);
+        stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[j0 + q] * ldr; }, jb, c.rn);
+        __syncthreads();
+        tile_mma(sm, jb, acc, tr, tc, s, c.rn);
+        __syncthreads();
+    }
+    // t = y - acc in sm.Y (row q of the next product's right operand = pivot q)
+    stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q] * ldr; }, s, c.rn);
+    stage_dinv<C, false, TRANS, RT, B>(sm, c.F, c.f, 0, s);
+    __syncthreads();
+#pragma unroll
+    for (int p = 0; p < RT / 16; ++p) {
+        const int row = tr + 16 * p;
+        if (row >= s) continue;
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const int col = tc + 8 * b;
+            if (col < c.rn) sm.Y[row][col] = csub(sm.Y[row][col], acc[p][b]);
+        }
+    }
+    __syncthreads();
+    zero_acc(acc);
+    tile_mma(sm, s, acc, tr, tc, s, c.rn);   // x_piv = Dinv t
+#pragma unroll
+    for (int p = 0; p < RT / 16; ++p) {
+        const int row = tr + 16 * p;
+        if (row >= s) continue;
+        C *x = c.X + (size_t)c.vars[row] * ldr;
+#pragma unroll
+        for (int b = 0; b < B; ++b) {
+            const int col = tc + 8 * b;
+            if (col < c.rn) x[col] = acc[p][b];
+        }
+    }
+}
+
 template <class R, int RT, int B>
 static size_t solve_smem() { return sizeof(SolveSmem<cplx<R>, RT, B>); }
 
@@ -420,6 +477,10 @@ static void set_attrs() {
     cudaFuncSetAttribute((const void *)k_bwd_ring<R, true, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     cudaFuncSetAttribute((const void *)k_bwd_piv<R, false, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     cudaFuncSetAttribute((const void *)k_bwd_piv<R, true, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    if (RT == 32) {
+        cudaFuncSetAttribute((const void *)k_bwd_small<R, false, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute((const void *)k_bwd_small<R, true, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+    }
     done = true;
 }
 
@@ -472,6 +533,13 @@ static void backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream
     set_attrs<R, RT, B>();
     const size_t smem = solve_smem<R, RT, B>();
     const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
+    static const bool no_small = env_int("GM_NO_BWD_SMALL") != 0;
+    if (RT == 32 && L.max_piv <= SNB && !no_small) {   // one pivot block per front: fused ring + pivot kernel
+        dim3 g(nchunk, L.count, a.nf);
+        if (a.trans) (k_bwd_small<R, true, B><<<g, NT, smem, st>>>(a, L.first), note_launch());
+        else (k_bwd_small<R, false, B><<<g, NT, smem, st>>>(a, L.first), note_launch());
+        return;
+    }
     const int fused = 0;
     if (L.max_ring > 0) {
         dim3 g1(nchunk * ((L.max_piv + RT - 1) / RT), L.count, a.nf);
