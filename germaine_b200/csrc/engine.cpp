@@ -592,15 +592,18 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     e->stats.ms_subst_bwd = 0;
     e->stats.n_subst = 0;
     GM_CUDA(cudaEventRecord(t0, e->st));
-    // initial solve in working precision
-    if (fp64) launch_convert_down<double>(d_b, e->d_t.p, cnt, e->st);
-    else launch_convert_down<float>(d_b, e->d_t.p, cnt, e->st);
-    GM_CUDA(cudaMemsetAsync(d_x, 0, cnt * sizeof(double2), e->st));
+    // initial solve in working precision: in FP64 in place in x (b copied
+    // into it), in complex64 in the work buffer and then added into x = 0
     const unsigned char *mask = build_mask(e, nrhs, pattern);
-    if (fp64) substitute<double>(e, e->d_t.p, nrhs, sys, mask);
-    else substitute<float>(e, e->d_t.p, nrhs, sys, mask);
-    if (fp64) launch_add_up<double>(d_x, e->d_t.p, cnt, e->st);
-    else launch_add_up<float>(d_x, e->d_t.p, cnt, e->st);
+    if (fp64) {
+        GM_CUDA(cudaMemcpyAsync(d_x, d_b, cnt * sizeof(double2), cudaMemcpyDeviceToDevice, e->st));
+        substitute<double>(e, d_x, nrhs, sys, mask);
+    } else {
+        launch_convert_down<float>(d_b, e->d_t.p, cnt, e->st);
+        GM_CUDA(cudaMemsetAsync(d_x, 0, cnt * sizeof(double2), e->st));
+        substitute<float>(e, e->d_t.p, nrhs, sys, mask);
+        launch_add_up<float>(d_x, e->d_t.p, cnt, e->st);
+    }
     GM_CUDA(cudaGetLastError());
     GM_CUDA(cudaEventRecord(t1, e->st));
     GM_CUDA(cudaEventSynchronize(t1));
