@@ -622,9 +622,12 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     int it = 0;
     GM_CUDA(cudaEventRecord(t0, e->st));
     for (;; ++it) {
-        // residual straight into the working-precision right-hand side
-        const int nblk = fp64 ? launch_residual_t<double>(ra, e->d_t.p, e->d_part.as<double>(), nblk_max, e->st)
-                              : launch_residual_t<float>(ra, e->d_t.p, e->d_part.as<double>(), nblk_max, e->st);
+        // residual straight into the working-precision right-hand side; the
+        // first check of FP64 factors normally passes, so it computes the
+        // norms only and the residual is formed again if a sweep follows
+        void *rhs = (fp64 && it == 0) ? nullptr : e->d_t.p;
+        const int nblk = fp64 ? launch_residual_t<double>(ra, rhs, e->d_part.as<double>(), nblk_max, e->st)
+                              : launch_residual_t<float>(ra, rhs, e->d_part.as<double>(), nblk_max, e->st);
         launch_reduce_norms(e->d_part.as<double>(), nblk, cntn, e->d_norm.as<double>(), e->st);
         GM_CUDA(cudaGetLastError());
         GM_CUDA(cudaMemcpyAsync(norms.data(), e->d_norm.p, cntn * sizeof(double), cudaMemcpyDeviceToHost, e->st));
@@ -655,6 +658,7 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
             std::fprintf(stderr, "\n");
         }
         if (worst <= e->cfg.ir_tol || it >= e->cfg.ir_max_iter) break;
+        if (!rhs) launch_residual_t<double>(ra, e->d_t.p, e->d_part.as<double>(), nblk_max, e->st);
         if (fp64) substitute<double>(e, e->d_t.p, nrhs, sys);
         else substitute<float>(e, e->d_t.p, nrhs, sys);
         if (fp64) launch_add_up<double>(d_x, e->d_t.p, cnt, e->st);

@@ -139,6 +139,7 @@ struct ResidArgs {
 int launch_residual(const ResidArgs &a, double *part, int max_blocks, cudaStream_t st);
 void launch_reduce_norms(const double *part, int nblk, int cnt, double *out, cudaStream_t st);
 // as launch_residual, but writes (T)(b - M'x) into t [nf][n][ldr] instead of r
+// (t = NULL: the norms only)
 template <class R>
 int launch_residual_t(const ResidArgs &a, void *t, double *part, int max_blocks, cudaStream_t st);
 

@@ -109,3 +109,24 @@ def test_solve_large_fronts(precision):
     assert _rel(x[0], xr) <= (1e-10 if precision == GM_PREC_FP64 else 1e-8)
     if precision == GM_PREC_C64_IR:
         assert st["ir_iterations"] <= 4
+
+
+def test_fp64_refinement_sweeps():
+    """FP64 factors pass the first residual check, which therefore forms only
+    the norms; a target below FP64 rounding forces sweeps, which must form
+    the residual again and keep the solution at the SuperLU reference."""
+    nx, ny, dh, npml = 40, 30, 10.0, 6
+    g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml)
+    m0, m1 = random_smooth(nx, ny, 1500.0, 3500.0, 7), random_smooth(nx, ny, 1000.0, 2500.0, 8)
+    rng = np.random.default_rng(9)
+    b = rng.standard_normal((1, g.n, 5)) + 1j * rng.standard_normal((1, g.n, 5))
+    with Engine(nx, ny, dh, npml, leaf_max=16, ir_tol=1e-30, ir_max_iter=2) as e:
+        e.set_model(m0, m1)
+        e.factor([9.0])
+        x = e.solve(b)
+        st = e.stats()
+    assert st["ir_iterations"] == 2 and st["n_subst"] == 3
+    assert st["ir_residual"] <= 1e-12
+    A = OS.assembled_matrix(g, *O.Port(g).assemble(1, 9.0, m0, m1))
+    xr = OS.DirectSolver(OS.operator(A)).solve(b[0])
+    assert _rel(x[0], xr) <= 1e-10
