@@ -62,7 +62,7 @@ EXPORTS = [
     "gm_get_gradient_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_hessian", "gm_get_hessian_fp64", "gm_apply_hess",
     "gm_lbfgs_create", "gm_lbfgs_destroy", "gm_lbfgs_step", "gm_lbfgs_rotate", "gm_lbfgs_zero",
     "gm_lbfgs_check_descent", "gm_lbfgs_get_old", "gm_lbfgs_set_old", "gm_mat_change",
-    "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_cgemm_sub_c64",
+    "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_read_grid", "gm_cgemm_sub_c64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
 ]
@@ -134,6 +134,7 @@ def load() -> ctypes.CDLL:
     lib.gm_write_model_true.argtypes = [cp, i32, i32, i32, i32, i32, i32, vp]
     lib.gm_write_model.argtypes = [cp, i32, i32, i32, i32, vp]
     lib.gm_read_model.argtypes = [cp, i32, i32, i32, i32, vp]
+    lib.gm_read_grid.argtypes = [cp, i32, i32, vp]
     lib.gm_solve_noalloc.argtypes = [vp, i32, i32, vp, vp]
     lib.gm_cgemm_sub_c64.argtypes = [i32, i32, i32, vp, vp, vp, vp]
     lib.gm_symbolic_create.argtypes = [i32, i32, i32, ctypes.POINTER(vp)]

@@ -16,6 +16,10 @@
 //   models with the frame  writemod (src/writemod.c:24-30) in binary
 //                format 3 (src/writedsk.c:32-40): the full NX x NY grid,
 //                same order and subsampling;
+//   full grids read back  the layout writemod and the reference's l-BFGS
+//                "*.old" files (src/LBFGS.c:183-216) and Hessian files
+//                (src/AC/hessian_AC.c:178-188) are written in: NX x NY
+//                floats, x outer (gm_read_grid);
 //   material models  readmod (src/readmod.c:43-104; readmod_SH, readmod_TE
 //                alike): the interior layout of writemod_true, extended into
 //                the PML frame by copying the nearest interior value (left /
@@ -125,5 +129,18 @@ extern "C" int gm_read_model(const char *path, int nx, int ny, int npml, int fre
         for (int i = 0; i < nx; ++i) at(j, i) = at(yshift, i);
     for (int j = yshift + ny0; j < ny; ++j)
         for (int i = 0; i < nx; ++i) at(j, i) = at(yshift + ny0 - 1, i);
+    return GM_OK;
+}
+
+extern "C" int gm_read_grid(const char *path, int nx, int ny, float *grid) {
+    if (!path || !grid || nx <= 0 || ny <= 0) return gm::fail(GM_ERROR_INVALID, "gm_read_grid: bad argument");
+    File fp(path, "rb");
+    if (!fp.f) return gm::fail(GM_ERROR_INVALID, "gm_read_grid: cannot open %s", path);
+    std::vector<float> col(ny);
+    for (int i = 0; i < nx; ++i) {
+        if (std::fread(col.data(), sizeof(float), ny, fp.f) != (size_t)ny)
+            return gm::fail(GM_ERROR_INVALID, "gm_read_grid: %s holds fewer than %d x %d floats", path, nx, ny);
+        for (int j = 0; j < ny; ++j) grid[(size_t)j * nx + i] = col[j];
+    }
     return GM_OK;
 }

@@ -63,6 +63,14 @@ def write_model(path, grid, idx: int = 1, idy: int = 1) -> None:
     check(_lib.load().gm_write_model(_path(path), nx, ny, idx, idy, ptr(g)))
 
 
+def read_grid(path, nx: int, ny: int) -> np.ndarray:
+    """Read a full [NY][NX] grid written x outer (writemod format 3, the
+    reference's l-BFGS "*.old" and Hessian files)."""
+    g = np.empty((ny, nx), np.float32)
+    check(_lib.load().gm_read_grid(_path(path), nx, ny, ptr(g)))
+    return g
+
+
 def read_model(path, nx: int, ny: int, npml: int, free_surf: int = 0) -> np.ndarray:
     """Read one material file into a [NY][NX] grid (NX, NY include the PML
     frame) and extend it into the frame as readmod does."""

@@ -325,6 +325,11 @@ int gm_write_model_true(const char *path, int nx, int ny, int npml, int free_sur
 /* The full [NY][NX] grid as writemod writes it in binary format 3
  * (src/writemod.c:24-30, src/writedsk.c:32-40): x outer, subsampled. */
 int gm_write_model(const char *path, int nx, int ny, int idx, int idy, const float *grid);
+/* A full [NY][NX] grid from a file in writemod's layout without
+ * subsampling (x outer): the reference's l-BFGS "*.old" files
+ * (src/LBFGS.c:183-216, read back at src/LBFGS.c:44-66) and Hessian files
+ * (src/AC/hessian_AC.c:178-188) -- so that a run can resume from them. */
+int gm_read_grid(const char *path, int nx, int ny, float *grid);
 /* One material file as readmod reads it (src/readmod.c:43-104; readmod_SH
  * and readmod_TE alike): interior floats, x outer, placed into the [NY][NX]
  * grid and extended into the PML frame by the nearest interior value. */

@@ -146,3 +146,27 @@ def test_against_reference_live(short_tmp):
         # readmod's own copy of the extended model (writemod format 3)
         files.write_model(tmp_path / "ours.vp", rvp)
         assert _read(tmp_path / "mm.germaine.vp") == _read(tmp_path / "ours.vp")
+
+
+def test_read_grid_round_trip(tmp_path):
+    rng = np.random.default_rng(12)
+    grid = rng.standard_normal((23, 31)).astype(np.float32)
+    files.write_model(tmp_path / "g", grid)
+    assert np.array_equal(_bits(files.read_grid(tmp_path / "g", 31, 23)), _bits(grid))
+    with pytest.raises(GmError):
+        files.read_grid(tmp_path / "g", 31, 24)   # file too short
+
+
+@needs_ref
+def test_read_grid_of_reference_lbfgs_files(short_tmp):
+    """The reference's l-BFGS state files (src/LBFGS.c:183-216) read back as
+    the grids it was given and returned."""
+    from tests import lbfgs_cases as LC
+    g = LC.grid()
+    (gr, gm, md, _), = LC.sequence(g, 1, 1, seed=13)
+    jac = os.path.join(short_tmp, "j")
+    ref = O.RefLbfgs(g, 2, 1, jac)
+    hgrad = ref.step_ac(1, 1, gr, gm, md)
+    assert np.array_equal(_bits(files.read_grid(jac + "_p.old", g.nx, g.ny)), _bits(gr))
+    assert np.array_equal(_bits(files.read_grid(jac + "_p_vp.old", g.nx, g.ny)), _bits(md))
+    assert np.array_equal(_bits(files.read_grid(jac + "_c.old", g.nx, g.ny)), _bits(hgrad))
