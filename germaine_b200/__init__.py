@@ -10,7 +10,7 @@ per-frequency drivers (``engine.Engine``) and of the reference's file
 formats (``files``).
 """
 from .engine import (GM_OP_EXACT, GM_OP_REF, GM_PHYS_AC, GM_PHYS_SH, GM_PHYS_TE, GM_PREC_C64_IR,  # noqa: F401
-                     GM_PREC_FP64, GM_SYS_A, GM_SYS_AT, Engine, Lbfgs, apply_hess, gauss_filt, mat_change,
+                     GM_PREC_FP64, GM_SYS_A, GM_SYS_AT, Engine, Lbfgs, apply_hess, gauss_filt, mat_change, precond,
                      nonzero)
 from ._lib import GM_HESS_GREEN, GM_HESS_SHIN  # noqa: F401
 from ._lib import GmError  # noqa: F401

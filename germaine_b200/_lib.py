@@ -59,7 +59,7 @@ class GmStats(ctypes.Structure):
 EXPORTS = [
     "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats", "gm_engine_stream",
     "gm_set_model", "gm_set_models", "gm_factor", "gm_factor_models", "gm_factor_values", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
-    "gm_get_gradient_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_hessian", "gm_get_hessian_fp64", "gm_apply_hess",
+    "gm_get_gradient_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_hessian", "gm_get_hessian_fp64", "gm_apply_hess", "gm_precond",
     "gm_lbfgs_create", "gm_lbfgs_destroy", "gm_lbfgs_step", "gm_lbfgs_rotate", "gm_lbfgs_zero",
     "gm_lbfgs_check_descent", "gm_lbfgs_get_old", "gm_lbfgs_set_old", "gm_mat_change",
     "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_read_grid", "gm_cgemm_sub_c64",
@@ -119,6 +119,7 @@ def load() -> ctypes.CDLL:
     lib.gm_hessian.argtypes = [vp, i32, i32, vp, vp, i32, vp, vp, vp, vp]
     lib.gm_get_hessian_fp64.argtypes = [vp, vp, vp]
     lib.gm_apply_hess.argtypes = [i32, i32, f32, vp, vp, vp]
+    lib.gm_precond.argtypes = [i32, i32, i32, i32, i32, f32, i32, f32, f32, f32, f32, i32, i32, vp, vp]
     lib.gm_lbfgs_create.argtypes = [i32, i32, i32, i32, i32, i32, i32, ctypes.POINTER(vp)]
     lib.gm_lbfgs_destroy.argtypes = [vp]
     lib.gm_lbfgs_step.argtypes = [vp, i32, i32, vp, vp, vp, vp, f32, vp]

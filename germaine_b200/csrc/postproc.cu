@@ -142,3 +142,89 @@ extern "C" int gm_apply_hess(int device, int n, float eps_hess, float *grad, con
     cudaFree(dmax);
     return rc;
 }
+
+// ---- precond (src/precond.c:10-24): gauss_filt, taper_grad_hor, taper_grad_file ----
+// taper_grad_hor (src/taper_grad_hor.c:20-31): rows j <= GRADT2 + FSSHIFT
+// (1-based) set to zero.  taper_grad_file (src/taper_grad_file.c:18-70):
+// the interior multiplied by the taper read from "taper.bin" (NX0 x NY0
+// floats, x outer), then the frame filled from the nearest interior column
+// (left, right: every row), the top NPML rows from row NPML+1 when
+// FREE_SURF == 1 (for a free surface those are interior rows -- the
+// reference overwrites them; it leaves the frame rows of FREE_SURF == 0
+// as the column copies left them) and the bottom rows from row
+// FSSHIFT+NY0.  All float multiplications and copies: bit-identical.
+namespace gm {
+
+__global__ void k_taper_hor(float *g, int nx, int rows) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < rows * nx) g[t] = 0.0f;
+}
+
+__global__ void k_taper_file_mul(float *g, const float *__restrict__ tap, int nx, int npml, int fsshift, int nx0,
+                                 int ny0) {
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;   // t = i * ny0 + j: file order
+    if (t >= nx0 * ny0) return;
+    const int i = t / ny0, j = t % ny0;
+    float &v = g[(size_t)(j + fsshift) * nx + (i + npml)];
+    v = __fmul_rn(v, tap[t]);
+}
+
+__global__ void k_taper_file_lr(float *g, int nx, int ny, int npml, int nx0) {
+    const int j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= ny) return;
+    float *row = g + (size_t)j * nx;
+    const float l = row[npml], r = row[npml + nx0 - 1];
+    for (int i = 0; i < npml; ++i) row[i] = l;
+    for (int i = npml + nx0; i < nx; ++i) row[i] = r;
+}
+
+__global__ void k_taper_file_tb(float *g, int nx, int ny, int npml, int free_surf, int fsshift, int ny0) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nx) return;
+    if (free_surf == 1)
+        for (int j = 0; j < npml; ++j) g[(size_t)j * nx + i] = g[(size_t)npml * nx + i];
+    for (int j = fsshift + ny0; j < ny; ++j) g[(size_t)j * nx + i] = g[(size_t)(fsshift + ny0 - 1) * nx + i];
+}
+
+}  // namespace gm
+
+extern "C" int gm_precond(int device, int nx, int ny, int npml, int free_surf, float dh, int spatfilter, float vref,
+                          float fc_low, float filt_size_grad, float filt_size_grad1, int taper_hor, int gradt2,
+                          const float *taper, float *grad) {
+    if (nx <= 0 || ny <= 0 || npml < 0 || !grad) return gm::fail(GM_ERROR_INVALID, "gm_precond: bad argument");
+    const int fsshift = free_surf ? 0 : npml, nx0 = nx - 2 * npml, ny0 = ny - npml - fsshift;
+    if (taper && (nx0 <= 0 || ny0 <= 0)) return gm::fail(GM_ERROR_INVALID, "gm_precond: grid without interior");
+    int rc;
+    if (spatfilter == 1 && (rc = gm_gauss_filt(device, nx, ny, dh, vref, fc_low, filt_size_grad, filt_size_grad1, grad, grad)))
+        return rc;
+    if (!taper_hor && !taper) return GM_OK;
+    if (cudaSetDevice(device) != cudaSuccess) return gm::fail(GM_ERROR_CUDA, "gm_precond: bad device %d", device);
+    const size_t n = (size_t)nx * ny;
+    float *dg = nullptr, *dt = nullptr;
+    rc = GM_OK;
+    cudaError_t e = cudaMalloc(&dg, n * sizeof(float));
+    if (e == cudaSuccess && taper) e = cudaMalloc(&dt, (size_t)nx0 * ny0 * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(dg, grad, n * sizeof(float), cudaMemcpyDefault);
+    if (e == cudaSuccess && taper) e = cudaMemcpy(dt, taper, (size_t)nx0 * ny0 * sizeof(float), cudaMemcpyDefault);
+    if (e == cudaSuccess && taper_hor) {
+        const int rows = std::min(ny, std::max(0, gradt2 + fsshift));
+        if (rows > 0) {
+            gm::k_taper_hor<<<(rows * nx + 255) / 256, 256>>>(dg, nx, rows);
+            gm::note_launch();
+        }
+    }
+    if (e == cudaSuccess && taper) {
+        gm::k_taper_file_mul<<<(nx0 * ny0 + 255) / 256, 256>>>(dg, dt, nx, npml, fsshift, nx0, ny0);
+        gm::k_taper_file_lr<<<(ny + 127) / 128, 128>>>(dg, nx, ny, npml, nx0);
+        gm::k_taper_file_tb<<<(nx + 127) / 128, 128>>>(dg, nx, ny, npml, free_surf, fsshift, ny0);
+        gm::note_launch();
+        gm::note_launch();
+        gm::note_launch();
+    }
+    if (e == cudaSuccess) e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaMemcpy(grad, dg, n * sizeof(float), cudaMemcpyDefault);
+    if (e != cudaSuccess) rc = gm::fail(GM_ERROR_CUDA, "gm_precond: %s", cudaGetErrorString(e));
+    cudaFree(dg);
+    cudaFree(dt);
+    return rc;
+}

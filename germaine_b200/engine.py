@@ -321,6 +321,20 @@ def mat_change(hgrad, model_old, eps_scale: float, low: float, up: float, mode: 
     return out
 
 
+def precond(grad, npml: int, free_surf: int, dh: float, spatfilter: int = 0, vref: float = 0.0,
+            fc_low: float = 1.0, filt_size_grad: float = 0.0, filt_size_grad1: float = 0.0, taper_hor: int = 0,
+            gradt2: int = 0, taper=None, device: int = 0) -> np.ndarray:
+    """precond() on the GPU (gm_precond: gauss_filt, taper_grad_hor,
+    taper_grad_file with the "taper.bin" content given as `taper`,
+    [NX0*NY0] floats x outer); returns the preconditioned copy."""
+    g = np.array(grad, np.float32, copy=True, order="C")
+    ny, nx = g.shape
+    tp = _c(taper, np.float32) if taper is not None else None
+    check(_lib.load().gm_precond(device, nx, ny, npml, free_surf, dh, spatfilter, vref, fc_low, filt_size_grad,
+                                 filt_size_grad1, taper_hor, gradt2, ptr(tp), ptr(g)))
+    return g
+
+
 def apply_hess(grad, hess, eps_hess: float, device: int = 0):
     """apply_hess_AC on the GPU (gm_apply_hess, bit-identical): returns
     (preconditioned gradient, MAX_HESS)."""

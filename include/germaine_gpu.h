@@ -243,6 +243,20 @@ int gm_obj_each(gm_engine *e, int nshots, const float *src_x, const float *src_y
 int gm_gauss_filt(int device, int nx, int ny, float dh, float vref, float fc_low, float filt_size_grad,
                   float filt_size_grad1, const float *grad, float *out);
 
+/* The gradient preconditioning of precond() (src/precond.c:10-24) on the
+ * GPU, in its order: spatfilter == 1 -> gauss_filt (as gm_gauss_filt);
+ * taper_hor != 0 -> taper_grad_hor (src/taper_grad_hor.c:20-31: rows
+ * 1 .. GRADT2 + FSSHIFT set to zero, gradt2 = GRADT2); taper != NULL ->
+ * taper_grad_file (src/taper_grad_file.c:18-70): the interior multiplied
+ * by the NX0 x NY0 taper (x outer, the content of "taper.bin"), the frame
+ * filled from the nearest interior column, the top NPML rows from row
+ * NPML+1 when free_surf == 1 (which overwrites interior rows, as the
+ * reference does) and the bottom rows from the last interior row.
+ * Bit-identical; grad [NY][NX] in place, host or device memory. */
+int gm_precond(int device, int nx, int ny, int npml, int free_surf, float dh, int spatfilter, float vref,
+               float fc_low, float filt_size_grad, float filt_size_grad1, int taper_hor, int gradt2,
+               const float *taper, float *grad);
+
 /* Apply the diagonal Hessian to a gradient on the GPU: apply_hess_AC
  * (src/AC/apply_hess_AC.c:11-40), also used for both TE parameters
  * (src/TE/fwi_FD_TE.c:287-288).  MAX_HESS = max |hess| (returned in

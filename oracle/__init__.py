@@ -115,6 +115,7 @@ def load_port():
         lib.port_lbfgs_rotate.argtypes = [ctypes.c_int, ctypes.c_int, _f32p, _f32p]
         lib.port_check_descent.argtypes = [P, ctypes.c_int, _f32p, _f32p]
         lib.port_check_descent.restype = ctypes.c_float
+        lib.port_precond_tapers.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, _f32p]
         _port_lib = lib
     return _port_lib
 
@@ -159,6 +160,8 @@ def load_ref():
         lib.ref_lbfgs_rotate.argtypes = [i, i, fp, fp]
         lib.ref_dotp_matrix.argtypes = [fp, fp]
         lib.ref_dotp_matrix.restype = ctypes.c_float
+        lib.ref_precond.argtypes = [cp, i, ctypes.c_float, ctypes.c_float, ctypes.c_float, ctypes.c_float, i, i, i, fp]
+        lib.ref_precond.restype = ctypes.c_int
         _ref_lib = lib
     return _ref_lib
 
@@ -291,6 +294,17 @@ class Port:
         mx = self.lib.port_apply_hess(out.size, eps_hess, out.reshape(-1), _f32(hess).reshape(-1))
         return out, float(mx)
 
+    def precond(self, grad, spatfilter=0, vref=0.0, fc_low=1.0, fsg=0.0, fsg1=0.0, taper_hor=0, gradt2=0,
+                taper=None):
+        """precond (src/precond.c:10-24): gauss_filt, taper_grad_hor, taper_grad_file."""
+        out = np.ascontiguousarray(grad, np.float32).copy()
+        if spatfilter == 1:
+            out = self.gauss_filt(out, vref, fc_low, fsg, fsg1)
+        tp = _f32(taper).ravel() if taper is not None else None
+        self.lib.port_precond_tapers(ctypes.byref(self._pg), taper_hor, gradt2,
+                                     None if tp is None else tp.ctypes.data_as(ctypes.c_void_p), out.reshape(-1))
+        return out
+
     def gradient_scalars(self, physics, freq):
         """(Omega^2, Omega) of ass_grad_AC / ass_grad_TE as complex64 values."""
         a = np.zeros(2, np.float32); b = np.zeros(2, np.float32)
@@ -373,6 +387,19 @@ class Ref:
         out = np.ascontiguousarray(grad, np.float32).copy()
         mx = self.lib.ref_apply_hess(eps_hess, out.reshape(-1), _f32(hess).reshape(-1))
         return out, float(mx)
+
+    def precond(self, workdir, grad, spatfilter=0, vref=0.0, fc_low=1.0, fsg=0.0, fsg1=0.0, taper_hor=0, gradt2=0,
+                taper=None):
+        """The reference's precond; `taper` (NX0*NY0, x outer) is written to
+        <workdir>/taper.bin, where taper_grad_file reads it."""
+        if taper is not None:
+            _f32(taper).ravel().tofile(os.path.join(workdir, "taper.bin"))
+        out = np.ascontiguousarray(grad, np.float32).copy()
+        rc = self.lib.ref_precond(os.fsencode(workdir), spatfilter, vref, fc_low, fsg, fsg1, taper_hor, gradt2,
+                                  int(taper is not None), out.reshape(-1))
+        if rc != 0:
+            raise RuntimeError("ref_precond: could not enter " + str(workdir))
+        return out
 
     # ---- file formats: the reference writes / reads the files itself ----
     def write_seis(self, prefix, stage, seis):

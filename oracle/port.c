@@ -605,3 +605,34 @@ float port_check_descent(const port_grid *g, int nclass, const float *hgrad, con
     }
     return -nom / den;
 }
+
+/* precond (src/precond.c:10-24) without its gauss_filt step (restated in
+ * port_gauss_filt): taper_grad_hor (src/taper_grad_hor.c:20-31) when
+ * taper_hor, then taper_grad_file (src/taper_grad_file.c:18-70) when taper
+ * (NX0 x NY0 floats, x outer) is given.  grad [NY][NX] in place. */
+void port_precond_tapers(const port_grid *g, int taper_hor, int gradt2, const float *taper, float *grad)
+{
+    const int nx = g->nx, ny = g->ny, npml = g->npml, fs = g->fsshift;
+    const int nx0 = nx - 2 * npml, ny0 = ny - npml - fs;
+    int i, j;
+#define G(jj, ii) grad[((jj) - 1) * nx + (ii) - 1]
+    if (taper_hor)
+        for (j = 1; j <= ny; j++)
+            for (i = 1; i <= nx; i++)
+                if (j <= gradt2 + fs) G(j, i) = 0.0f;
+    if (taper) {
+        int t = 0;
+        for (i = 1; i <= nx0; i++)
+            for (j = 1; j <= ny0; j++) G(j + fs, i + npml) *= taper[t++];
+        for (i = 1; i <= npml; i++)
+            for (j = 1; j <= ny; j++) G(j, i) = G(j, npml + 1);
+        for (i = npml + nx0 + 1; i <= nx; i++)
+            for (j = 1; j <= ny; j++) G(j, i) = G(j, npml + nx0);
+        if (g->free_surf == 1)
+            for (i = 1; i <= nx; i++)
+                for (j = 1; j <= npml; j++) G(j, i) = G(npml + 1, i);
+        for (i = 1; i <= nx; i++)
+            for (j = fs + ny0 + 1; j <= ny; j++) G(j, i) = G(fs + ny0, i);
+    }
+#undef G
+}

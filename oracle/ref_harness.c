@@ -36,7 +36,10 @@
  *   LBFGS_TE             src/TE/LBFGS_TE.c:12
  *   rot_LBFGS_vec        src/rot_LBFGS_vec.c:10
  *   dotp_matrix          src/dotp_matrix.c:8
+ *   precond              src/precond.c:10   (+ taper_grad_hor, taper_grad_file)
  */
+#include <unistd.h>
+
 #include "fd.h"
 #include "globvar.h"
 
@@ -427,4 +430,26 @@ float ref_dotp_matrix(const float *a, const float *b)
     free_matrix(A, 0, NY + 1, 0, NX + 1);
     free_matrix(B, 0, NY + 1, 0, NX + 1);
     return v;
+}
+
+/* precond (src/precond.c:10) on a flat [NY][NX] gradient in place.  Its
+ * taper_grad_file opens "taper.bin" in the working directory: `dir` must
+ * hold that file when sws_taper_file is set (the working directory is
+ * restored afterwards). */
+int ref_precond(const char *dir, int spatfilter, float vref, float fc_low, float fsg, float fsg1, int taper_hor,
+                int gradt2, int sws_taper_file, float *grad)
+{
+    extern int SPATFILTER, SWS_TAPER_GRAD_HOR, SWS_TAPER_FILE, GRADT2;
+    extern float VREF, FC_low, FILT_SIZE_GRAD, FILT_SIZE_GRAD1;
+    char cwd[4096];
+    float **gr;
+    if (!getcwd(cwd, sizeof cwd)) return -1;
+    if (dir && chdir(dir) != 0) return -1;
+    gr = to_nr(grad);
+    SPATFILTER = spatfilter; VREF = vref; FC_low = fc_low; FILT_SIZE_GRAD = fsg; FILT_SIZE_GRAD1 = fsg1;
+    SWS_TAPER_GRAD_HOR = taper_hor; GRADT2 = gradt2; SWS_TAPER_FILE = sws_taper_file;
+    precond(gr);
+    from_nr(gr, grad);
+    free_matrix(gr, 0, NY + 1, 0, NX + 1);
+    return chdir(cwd) == 0 ? 0 : -1;
 }

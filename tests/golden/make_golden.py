@@ -34,13 +34,15 @@ CASES = [
 
 def main():
     out = os.path.dirname(os.path.abspath(__file__))
-    which = set(sys.argv[1:]) or {"assembly", "gauss", "hess", "files"}
+    which = set(sys.argv[1:]) or {"assembly", "gauss", "hess", "precond", "files"}
     if "assembly" in which:
         assembly_fixtures(out)
     if "gauss" in which:
         gauss_filt_fixture(out)
     if "hess" in which:
         apply_hess_fixture(out)
+    if "precond" in which:
+        precond_fixture(out)
     if "files" in which:
         files_fixture(out)
 
@@ -117,6 +119,31 @@ def apply_hess_fixture(out):
                   f"max_{k}": np.float32(mx)})
     np.savez_compressed(os.path.join(out, "postproc_apply_hess.npz"), **d)
     print("wrote postproc_apply_hess")
+
+
+# precond cases: grid nx, ny, npml, free_surf, SPATFILTER, SWS_TAPER_GRAD_HOR, GRADT2, taper file
+PRECOND_CASES = [(41, 33, 5, 0, 0, 1, 3, False), (41, 33, 5, 0, 0, 0, 0, True), (38, 29, 4, 1, 0, 0, 0, True),
+                 (45, 31, 6, 0, 1, 1, 4, True), (36, 30, 5, 1, 1, 1, 2, True)]
+
+
+def precond_fixture(out):
+    """postproc_precond.npz: per case k the grid / switches (case_k), a
+    seeded gradient (grad_k), the taper file content (taper_k, NX0*NY0 x
+    outer, or empty) and the reference's precond output (out_k); gauss_filt
+    with VREF 2000, FC_low 5, sizes 0.3 / 0.5 where SPATFILTER = 1."""
+    rng = np.random.default_rng(19)
+    d = {"ncases": len(PRECOND_CASES)}
+    with tempfile.TemporaryDirectory() as tmp:
+        for k, (nx, ny, npml, fs, spat, hor, gt2, tfile) in enumerate(PRECOND_CASES):
+            g = O.Grid(nx=nx, ny=ny, dh=10.0, npml=npml, free_surf=fs)
+            nx0, ny0 = nx - 2 * npml, ny - npml - g.fsshift
+            grad = rng.standard_normal((ny, nx)).astype(np.float32)
+            taper = rng.uniform(0.0, 1.0, nx0 * ny0).astype(np.float32) if tfile else None
+            o = O.Ref(g).precond(tmp, grad, spat, 2000.0, 5.0, 0.3, 0.5, hor, gt2, taper)
+            d.update({f"case_{k}": np.array([nx, ny, npml, fs, spat, hor, gt2, int(tfile)]), f"grad_{k}": grad,
+                      f"taper_{k}": taper if taper is not None else np.zeros(0, np.float32), f"out_{k}": o})
+    np.savez_compressed(os.path.join(out, "postproc_precond.npz"), **d)
+    print("wrote postproc_precond")
 
 
 # file-format cases: grid nx, ny, npml, free_surf

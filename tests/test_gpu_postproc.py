@@ -39,3 +39,15 @@ def test_gauss_filt_rejects_bad_arguments():
     g = np.zeros((4, 4), np.float32)
     assert lib.gm_gauss_filt(0, 0, 4, 10.0, 2000.0, 5.0, 0.5, 0.5, _lib.ptr(g), _lib.ptr(g)) == _lib.GM_ERROR_INVALID
     assert lib.gm_gauss_filt(0, 4, 4, 10.0, 2000.0, 0.0, 0.5, 0.5, _lib.ptr(g), _lib.ptr(g)) == _lib.GM_ERROR_INVALID
+
+
+def test_precond_matches_reference_fixture():
+    """gm_precond (precond: gauss_filt, taper_grad_hor, taper_grad_file)
+    bit-identical to the reference's output in the committed fixture."""
+    from germaine_b200 import precond
+    from tests.test_oracle_pin import precond_cases
+    for g, kw, grad, ref in precond_cases():
+        out = precond(grad, g.npml, g.free_surf, g.dh, spatfilter=kw["spatfilter"], vref=kw["vref"],
+                      fc_low=kw["fc_low"], filt_size_grad=kw["fsg"], filt_size_grad1=kw["fsg1"],
+                      taper_hor=kw["taper_hor"], gradt2=kw["gradt2"], taper=kw["taper"])
+        assert np.array_equal(_bits(out), _bits(ref)), (g.nx, g.ny, g.free_surf, kw["spatfilter"])

@@ -225,3 +225,37 @@ def test_port_check_descent_sums_equal_reference():
     nom, den = R.lib.ref_dotp_matrix(hg.ravel(), gr.ravel()), R.lib.ref_dotp_matrix(gr.ravel(), gr.ravel())
     p = O.PortLbfgs(g, 1, 1).check_descent(hg, gr)
     assert _bits(np.float32(p)) == _bits(np.float32(-np.float32(nom)) / np.float32(den))
+
+
+# ---- precond (src/precond.c) ----
+def precond_cases():
+    d = np.load(os.path.join(GOLDEN, "postproc_precond.npz"))
+    out = []
+    for k in range(int(d["ncases"])):
+        nx, ny, npml, fs, spat, hor, gt2, tfile = (int(v) for v in d[f"case_{k}"])
+        g = O.Grid(nx=nx, ny=ny, dh=10.0, npml=npml, free_surf=fs)
+        out.append((g, dict(spatfilter=spat, vref=2000.0, fc_low=5.0, fsg=0.3, fsg1=0.5, taper_hor=hor, gradt2=gt2,
+                            taper=d[f"taper_{k}"] if tfile else None), d[f"grad_{k}"], d[f"out_{k}"]))
+    return out
+
+
+def test_port_precond_against_golden():
+    """precond (src/precond.c:10-24): gauss_filt, taper_grad_hor and
+    taper_grad_file, incl. its overwrite of the top interior rows with a
+    free surface; bit-identical to the reference's output in the fixture."""
+    for g, kw, grad, ref in precond_cases():
+        assert np.array_equal(_bits(O.Port(g).precond(grad, **kw)), _bits(ref))
+
+
+@needs_ref
+def test_port_precond_equals_reference(short_tmp):
+    rng = np.random.default_rng(21)
+    for fs in (0, 1):
+        g = O.Grid(nx=40, ny=28, dh=12.5, npml=5, free_surf=fs)
+        nx0, ny0 = g.nx - 2 * g.npml, g.ny - g.npml - g.fsshift
+        grad = rng.standard_normal((g.ny, g.nx)).astype(np.float32)
+        taper = rng.uniform(0, 1, nx0 * ny0).astype(np.float32)
+        kw = dict(spatfilter=1, vref=2500.0, fc_low=4.0, fsg=0.2, fsg1=0.6, taper_hor=1, gradt2=3, taper=taper)
+        a = O.Port(g).precond(grad, **kw)
+        b = O.Ref(g).precond(short_tmp, grad, **kw)
+        assert np.array_equal(_bits(a), _bits(b))
