@@ -10,6 +10,7 @@
 // At 841 x 227 (n = 190,907) with 10 frequencies x 100 shots this is about
 // 8 GB of fronts in FP64 plus 12 GB of vectors -- resident in one B200.
 #include "engine.hpp"
+#include "kernels_epi.cuh"
 
 #include <algorithm>
 #include <cmath>
@@ -578,7 +579,9 @@ static const unsigned char *build_mask(gm_engine *e, int nrhs, const RhsPattern 
 // x (device, [nf][n][nrhs] c128) = M'^{-1} b with FP64 refinement; b, x device.
 // The first substitution prunes the forward pass by `pattern` when given;
 // the refinement sweeps (dense residuals) do not.
-int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const double2 *d_b, const RhsPattern *pattern) {
+int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const double2 *d_b, const RhsPattern *pattern,
+                        const SpikeRhs *spikes) {
+    if (!d_b && !(spikes && spikes->k && spikes->amp)) return fail(GM_ERROR_INVALID, "solve: no right-hand side");
     const size_t cnt = (size_t)e->nf * e->n * nrhs;
     const bool fp64 = e->cfg.precision == GM_PREC_FP64;
     GM_ALLOC(e->d_t, cnt * e->csize());
@@ -595,11 +598,13 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     // initial solve in working precision: in FP64 in place in x (b copied
     // into it), in complex64 in the work buffer and then added into x = 0
     const unsigned char *mask = build_mask(e, nrhs, pattern);
+    const bool implicit = !d_b;
+    if (implicit) launch_spikes(d_x, e->n, e->nf, nrhs, spikes->k, spikes->amp, e->st);   // x = b
     if (fp64) {
-        GM_CUDA(cudaMemcpyAsync(d_x, d_b, cnt * sizeof(double2), cudaMemcpyDeviceToDevice, e->st));
+        if (!implicit) GM_CUDA(cudaMemcpyAsync(d_x, d_b, cnt * sizeof(double2), cudaMemcpyDeviceToDevice, e->st));
         substitute<double>(e, d_x, nrhs, sys, mask);
     } else {
-        launch_convert_down<float>(d_b, e->d_t.p, cnt, e->st);
+        launch_convert_down<float>(implicit ? d_x : d_b, e->d_t.p, cnt, e->st);
         GM_CUDA(cudaMemsetAsync(d_x, 0, cnt * sizeof(double2), e->st));
         substitute<float>(e, e->d_t.p, nrhs, sys, mask);
         launch_add_up<float>(d_x, e->d_t.p, cnt, e->st);
@@ -616,6 +621,10 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     ra.nx = e->cfg.nx; ra.ny = e->cfg.ny; ra.n = e->n; ra.nf = e->nf; ra.nrhs = nrhs; ra.ldr = nrhs;
     ra.A = e->d_A.as<double2>(); ra.x = d_x; ra.b = d_b; ra.r = nullptr;
     ra.op_mode = e->cfg.op_mode; ra.trans = sys;
+    if (implicit) {
+        ra.spike_k = spikes->k;
+        ra.spike_amp = spikes->amp;
+    }
     const int cntn = e->nf * nrhs * 2;
     std::vector<double> norms(cntn);
     double worst = 0;

@@ -115,7 +115,15 @@ struct RhsPattern {
     int ncommon = 0;
 };
 
+// Spike right-hand sides given implicitly (device arrays): right-hand side r
+// of frequency f is amp[f] at row k[r] and zero elsewhere, so no dense b is
+// formed, copied or read.
+struct SpikeRhs {
+    const int *k = nullptr;         // [nrhs]
+    const double2 *amp = nullptr;   // [nf]
+};
+
 // internal entry points shared between translation units
 int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x_out, const double2 *d_b_in,
-                        const RhsPattern *pattern = nullptr);
+                        const RhsPattern *pattern = nullptr, const SpikeRhs *spikes = nullptr);
 }

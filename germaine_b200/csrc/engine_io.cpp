@@ -90,13 +90,14 @@ int forward_solve(gm_engine *e, int ns, const Geometry &g, double2 *xout, int sr
     if ((rc = upload(e->d_src_k, g.ksrc, e->st))) return rc;
     gm::DevBuf amp_buf;
     if ((rc = upload(amp_buf, amp, e->st))) return rc;
-    GM_ALLOC(e->d_b, (size_t)nf * n * ns * sizeof(double2));
-    gm::launch_spikes(e->d_b.as<double2>(), n, nf, ns, e->d_src_k.as<int>(), amp_buf.as<double2>(), e->st);
-    GM_CUDA(cudaGetLastError());
+    (void)n;
     gm::RhsPattern pat;   // one spike per shot: prune the forward pass
     pat.per_col = g.ksrc.data();
     pat.ncol = ns;
-    rc = gm::engine_solve_device(e, GM_SYS_A, ns, xout, e->d_b.as<double2>(), &pat);
+    gm::SpikeRhs sp;      // and never form the dense right-hand sides
+    sp.k = e->d_src_k.as<int>();
+    sp.amp = amp_buf.as<double2>();
+    rc = gm::engine_solve_device(e, GM_SYS_A, ns, xout, nullptr, &pat, &sp);
     GM_CUDA(cudaStreamSynchronize(e->st));  // amp_buf is released on return
     return rc;
 }
@@ -384,17 +385,17 @@ extern "C" int gm_hessian(gm_engine *e, int mode, int nshots, const float *src_x
         gm::DevBuf amp_buf;
         if ((rc = upload(amp_buf, amp, e->st))) return rc;
         if ((rc = upload(e->d_rec_k, g.kadj, e->st))) return rc;
-        GM_ALLOC(e->d_b, (size_t)nf * n * blk * sizeof(double2));
         GM_ALLOC(e->d_xa, (size_t)nf * n * blk * sizeof(double2));
         for (int r0 = 0; r0 < ntr; r0 += blk) {
             const int nr = std::min(blk, ntr - r0);
-            gm::launch_spikes(e->d_b.as<double2>(), n, nf, nr, e->d_rec_k.as<int>() + r0, amp_buf.as<double2>(), e->st);
-            GM_CUDA(cudaGetLastError());
             // the reference solves with UMFPACK_A for both physics (src/AC/hessian_AC.c:140, src/TE/hessian_TE.c:140)
             gm::RhsPattern pat;   // one receiver spike per right-hand side
             pat.per_col = g.kadj.data() + r0;
             pat.ncol = nr;
-            const int src = gm::engine_solve_device(e, GM_SYS_A, nr, e->d_xa.as<double2>(), e->d_b.as<double2>(), &pat);
+            gm::SpikeRhs sp;
+            sp.k = e->d_rec_k.as<int>() + r0;
+            sp.amp = amp_buf.as<double2>();
+            const int src = gm::engine_solve_device(e, GM_SYS_A, nr, e->d_xa.as<double2>(), nullptr, &pat, &sp);
             if (src < 0) return src;
             if (src > worst) worst = src;
             gm::launch_hess_sq(e->d_xa.as<double2>(), n, nf, nr, sqg, r0 > 0, e->st);

@@ -133,6 +133,10 @@ struct ResidArgs {
     double2 *r;         // [nf][n][ldr] out: b - M x
     int op_mode;        // GM_OP_REF: M = A^T, GM_OP_EXACT: M = A
     int trans;          // 0: M, 1: M^T
+    // spike right-hand sides given implicitly (b == NULL): b[f][k][r] =
+    // spike_amp[f] if k == spike_k[r], else 0
+    const int *spike_k;
+    const double2 *spike_amp;
 };
 // r = b - M x and per-(freq, rhs) partial sums of |r|^2 and |b|^2 into
 // part[nblk][nf][nrhs][2]; returns nblk.

@@ -28,11 +28,13 @@ __global__ void __launch_bounds__(128) k_residual(ResidArgs a, OutC *out, double
     const bool use_row = (a.op_mode == GM_OP_EXACT) != (a.trans != 0);
     const double2 *A9 = a.A + (size_t)f * 9 * a.n;
     const size_t base = (size_t)f * a.n * a.ldr;
+    const double2 amp = a.spike_k ? a.spike_amp[f] : make_double2(0.0, 0.0);
     for (int r = threadIdx.x; r < a.nrhs; r += blockDim.x) {
         double rr = 0.0, bb = 0.0;
+        const int ks = a.spike_k ? a.spike_k[r] : -1;
         for (int k = k0; k < k1; ++k) {
             const int x = k % a.nx, y = k / a.nx;
-            const double2 bv = a.b[base + (size_t)k * a.ldr + r];
+            const double2 bv = a.spike_k ? (k == ks ? amp : make_double2(0.0, 0.0)) : a.b[base + (size_t)k * a.ldr + r];
             double2 acc = bv;
 #pragma unroll
             for (int q = 0; q < 9; ++q) {
