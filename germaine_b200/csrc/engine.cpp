@@ -342,27 +342,68 @@ static int factor_batch(gm_engine *e, double pivscale) {
     const int4 *tiles = e->d_cb_tiles.as<int4>();
     // GM_TRACE_LEVELS=1: device time of every level on stderr
     static const bool trace = std::getenv("GM_TRACE_LEVELS") != nullptr;
+    static const bool no_graph = std::getenv("GM_NO_GRAPH") != nullptr;
     const int nl = (int)e->levels.size();
+    auto launch_levels = [&](cudaEvent_t *evs) {
+        for (int h = 0; h < nl; ++h) {
+            if (small_factor_level<R>(e->levels[h])) {
+                launch_factor_small<R>(a, e->levels[h], e->st);
+            } else {
+                launch_factor_level<R>(a, e->levels[h], e->st);
+                const auto &pl = e->cb_plan[h];
+                if (pl.backend == 1)
+                    launch_cgemm_sub(1, reinterpret_cast<const CgemmProb *>(probs + pl.prob_off), tiles + pl.tile_off,
+                                     pl.ntiles, e->d_tcerr.as<int>(), e->st);
+                else
+                    launch_gemm_sub_cc<R>(probs + pl.prob_off, tiles + pl.tile_off, pl.ntiles, e->st);
+            }
+            if (evs) cudaEventRecord(evs[1 + h], e->st);
+        }
+    };
+    if (!trace && !no_graph && !e->fgraph_broken) {
+        // every level of the factorisation as one CUDA graph, replayed while
+        // the buffers and the batch stay the same.  The first factorisation
+        // with new buffers launches directly (which also sets every kernel's
+        // attributes outside any capture), the second captures the graph.
+        gm_engine::FactorGraphKey key;
+        key.front = e->d_front.p; key.A = e->d_A.p; key.amax = e->d_amax.p; key.npert = e->d_npert.p;
+        key.tcerr = e->d_tcerr.p; key.probs = probs; key.tiles = tiles; key.nf = e->nf; key.fp64 = sizeof(R) == 8;
+        if (!(e->fgraph && key == e->fgraph_key) && key == e->fgraph_seen) {
+            if (e->fgraph) cudaGraphExecDestroy(e->fgraph);
+            e->fgraph = nullptr;
+            cudaGraph_t g = nullptr;
+            const long long before = launch_count();
+            bool ok = cudaStreamBeginCapture(e->st, cudaStreamCaptureModeThreadLocal) == cudaSuccess;
+            if (ok) {
+                launch_levels(nullptr);
+                ok = cudaStreamEndCapture(e->st, &g) == cudaSuccess && g;
+            }
+            if (ok) ok = cudaGraphInstantiate(&e->fgraph, g, 0) == cudaSuccess;
+            if (g) cudaGraphDestroy(g);
+            cudaGetLastError();   // a failed capture leaves its error here
+            if (ok) {
+                e->fgraph_key = key;
+                e->fgraph_kernels = launch_count() - before;
+            } else {
+                e->fgraph = nullptr;
+                e->fgraph_broken = true;   // launch directly from now on
+            }
+        }
+        e->fgraph_seen = key;
+        if (e->fgraph && key == e->fgraph_key) {
+            GM_CUDA(cudaGraphLaunch(e->fgraph, e->st));
+            note_launches(e->fgraph_kernels);
+            GM_CUDA(cudaGetLastError());
+            return GM_OK;
+        }
+    }
     std::vector<cudaEvent_t> ev;
     if (trace) {
         ev.resize(nl + 1);
         for (auto &x : ev) cudaEventCreate(&x);
         cudaEventRecord(ev[0], e->st);
     }
-    for (int h = 0; h < nl; ++h) {
-        if (small_factor_level<R>(e->levels[h])) {
-            launch_factor_small<R>(a, e->levels[h], e->st);
-        } else {
-            launch_factor_level<R>(a, e->levels[h], e->st);
-            const auto &pl = e->cb_plan[h];
-            if (pl.backend == 1)
-                launch_cgemm_sub(1, reinterpret_cast<const CgemmProb *>(probs + pl.prob_off), tiles + pl.tile_off,
-                                 pl.ntiles, e->d_tcerr.as<int>(), e->st);
-            else
-                launch_gemm_sub_cc<R>(probs + pl.prob_off, tiles + pl.tile_off, pl.ntiles, e->st);
-        }
-        if (trace) cudaEventRecord(ev[1 + h], e->st);
-    }
+    launch_levels(trace ? ev.data() : nullptr);
     if (trace) {
         cudaEventSynchronize(ev[nl]);
         for (int h = 0; h < nl; ++h) {

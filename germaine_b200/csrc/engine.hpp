@@ -74,6 +74,21 @@ struct gm_engine {
     gm::DevBuf d_cb_probs, d_cb_tiles, d_tcerr;
     const void *cb_plan_base = nullptr;
     int cb_plan_nf = 0;
+    // the factorisation's launch sequence as a CUDA graph, replayed while
+    // the buffers and the batch it was captured for stay the same
+    struct FactorGraphKey {
+        const void *front = nullptr, *A = nullptr, *amax = nullptr, *npert = nullptr, *tcerr = nullptr;
+        const void *probs = nullptr, *tiles = nullptr;
+        int nf = 0, fp64 = 0;
+        bool operator==(const FactorGraphKey &o) const {
+            return front == o.front && A == o.A && amax == o.amax && npert == o.npert && tcerr == o.tcerr &&
+                   probs == o.probs && tiles == o.tiles && nf == o.nf && fp64 == o.fp64;
+        }
+    };
+    FactorGraphKey fgraph_key, fgraph_seen;
+    cudaGraphExec_t fgraph = nullptr;
+    long long fgraph_kernels = 0;
+    bool fgraph_broken = false;   // capture failed once: launch directly
 
     // solve workspaces
     gm::DevBuf d_x, d_b, d_r, d_t, d_w, d_part, d_norm;
@@ -97,6 +112,7 @@ struct gm_engine {
         if (ev_s0) cudaEventDestroy(ev_s0);
         if (ev_s1) cudaEventDestroy(ev_s1);
         if (ev_sm) cudaEventDestroy(ev_sm);
+        if (fgraph) cudaGraphExecDestroy(fgraph);
         if (st) cudaStreamDestroy(st);
     }
 

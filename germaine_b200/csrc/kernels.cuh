@@ -14,6 +14,7 @@ template <class R> using cplx_any = typename cplx_any_t<R>::type;
 
 // Counts kernel launches of this library (reported in gm_stats).
 void note_launch();
+void note_launches(long long n);   // n kernels launched at once (a CUDA graph replay)
 long long launch_count();
 
 // ---------------- K1 assembly ----------------
