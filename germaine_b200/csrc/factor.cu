@@ -25,13 +25,15 @@ constexpr int NB = 32;       // pivot block width
 constexpr int TILE = 64;     // Schur-update tile
 constexpr int PCHUNK = 128;  // panel rows / columns per CTA
 
+constexpr int GATHER_COLS = 4;   // front columns per CTA of the extend-add gather
+
 template <class R>
 __global__ void k_front_gather(FactorArgs<R> a, int lvl_first) {
     using C = cplx<R>;
     const int node = a.s.lvl_nodes[lvl_first + blockIdx.y];
     const int f = a.s.nfront[node];
-    const int j = blockIdx.x;
-    if (j >= f) return;
+    const int j = blockIdx.x * GATHER_COLS + (threadIdx.x >> 5);   // one warp per front column
+    if (j >= f) return;   // warp-uniform (no barrier below)
     C *base = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.z * a.s.front_total;
     C *F = base + a.s.front_off[node];
     const int *inv = a.s.inv + a.s.inv_off[node];
@@ -48,7 +50,7 @@ __global__ void k_front_gather(FactorArgs<R> a, int lvl_first) {
         const int s1 = a.s.npiv[c1]; f1 = a.s.nfront[c1];
         cb1 = base + a.s.front_off[c1] + s1 + (size_t)(s1 + b1) * f1;
     }
-    for (int i = threadIdx.x; i < f; i += blockDim.x) {
+    for (int i = threadIdx.x & 31; i < f; i += 32) {
         C v = czero<C>();
         if (cb0) { const int r = inv[i]; if (r >= 0) v = cadd(v, cb0[r]); }
         if (cb1) { const int r = inv[f + i]; if (r >= 0) v = cadd(v, cb1[r]); }
@@ -359,7 +361,9 @@ template <class R>
 void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
     using C = cplx<R>;
     if (L.count == 0) return;
-    (k_front_gather<R><<<dim3(L.max_front, L.count, a.nf), 128, 0, st>>>(a, L.first), note_launch());
+    (k_front_gather<R><<<dim3((L.max_front + GATHER_COLS - 1) / GATHER_COLS, L.count, a.nf), 32 * GATHER_COLS, 0,
+                         st>>>(a, L.first),
+     note_launch());
     if (L.ent_count > 0) {
         const int tpb = 256;
         (k_entry_scatter<R><<<dim3((unsigned)((L.ent_count + tpb - 1) / tpb), a.nf), tpb, 0, st>>>(a, L.ent_first,
