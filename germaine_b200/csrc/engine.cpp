@@ -563,15 +563,18 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsign
         for (auto &x : ev) cudaEventCreate(&x);
         cudaEventRecord(ev[0], e->st);
     }
-    for (int h = 0; h < nl; ++h) {
-        launch_solve_forward_level<R>(a, e->levels[h], e->st);
-        if (trace) cudaEventRecord(ev[1 + h], e->st);
-    }
-    cudaEventRecord(e->ev_sm, e->st);
-    for (int h = nl - 1; h >= 0; --h) {
-        launch_solve_backward_level<R>(a, e->levels[h], e->st);
-        if (trace) cudaEventRecord(ev[1 + nl + (nl - 1 - h)], e->st);
-    }
+    auto passes = [&](cudaEvent_t *evs) {
+        for (int h = 0; h < nl; ++h) {
+            launch_solve_forward_level<R>(a, e->levels[h], e->st);
+            if (evs) cudaEventRecord(evs[1 + h], e->st);
+        }
+        cudaEventRecord(e->ev_sm, e->st);
+        for (int h = nl - 1; h >= 0; --h) {
+            launch_solve_backward_level<R>(a, e->levels[h], e->st);
+            if (evs) cudaEventRecord(evs[1 + nl + (nl - 1 - h)], e->st);
+        }
+    };
+    passes(trace ? ev.data() : nullptr);
     if (trace) {
         cudaEventSynchronize(ev[2 * nl]);
         for (int h = 0; h < nl; ++h) {

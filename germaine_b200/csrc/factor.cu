@@ -380,7 +380,10 @@ void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
         const int nchunk = mmax > 0 ? (mmax + PCHUNK - 1) / PCHUNK : 0;
         if (nchunk > 0)
             (k_panel<R><<<dim3(2 * nchunk, L.count, a.nf), PCHUNK, 0, st>>>(a, L.first, k0), note_launch());
-        const int ntmax = mmax > 0 ? (mmax + TILE - 1) / TILE : 0;
+        // the trailing tiles only update pivot rows and columns still to come:
+        // after the level's last pivot block every tile would exit at once,
+        // so only the CTA that writes back the diagonal block is launched
+        const int ntmax = (mmax > 0 && L.max_piv > k0 + NB) ? (mmax + TILE - 1) / TILE : 0;
         (k_update<R><<<dim3(ntmax * ntmax + 1, L.count, a.nf), 256, smem, st>>>(a, L.first, k0, ntmax), note_launch());
     }
 }
