@@ -119,9 +119,11 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
         L.max_front = s.lvl_max_front[h];
         L.max_piv = s.lvl_max_piv[h];
         L.max_ring = 0;
+        L.mid_words = 0;
         for (int t = L.first; t < L.first + L.count; ++t) {
-            const int v = s.lvl_nodes[t];
-            L.max_ring = std::max(L.max_ring, s.nfront[v] - s.npiv[v]);
+            const int v = s.lvl_nodes[t], fv = s.nfront[v], sv = s.npiv[v];
+            L.max_ring = std::max(L.max_ring, fv - sv);
+            L.mid_words = std::max(L.mid_words, (int64_t)(fv + 1) * sv + (int64_t)(sv | 1) * (fv - sv));
         }
         L.ent_first = (int64_t)ent_dst.size();
         for (int t = L.first; t < L.first + L.count; ++t) {
@@ -260,6 +262,15 @@ static int assemble_batch(gm_engine *e) {
 // their output tiles: tcgen05 tiles (128 x 64) for the complex64 path on
 // levels whose blocks are large enough to fill them, CUDA-core tiles
 // (64 x 64) otherwise.
+// Levels of fronts with at most NB pivots that are too large for the small
+// kernel go to the fused mid-level kernel; GM_NO_FACTOR_MID=1 keeps them on
+// the blocked panel / update / contribution-GEMM sequence.
+template <class R>
+static bool use_mid_factor(const LevelInfo &L) {
+    static const bool off = std::getenv("GM_NO_FACTOR_MID") != nullptr;
+    return !off && mid_factor_level<R>(L);
+}
+
 template <class R>
 static int build_cb_plan(gm_engine *e) {
     using C = cplx_any<R>;
@@ -289,7 +300,7 @@ static int build_cb_plan(gm_engine *e) {
         pl.backend = backend;
         pl.prob_off = (int64_t)probs.size();
         pl.tile_off = (int64_t)tiles.size();
-        if (small_factor_level<R>(L)) {   // fused small-front kernel forms the Schur complement itself
+        if (small_factor_level<R>(L) || use_mid_factor<R>(L)) {   // fused kernels form the Schur complement themselves
             pl.ntiles = 0;
             continue;
         }
@@ -348,6 +359,8 @@ static int factor_batch(gm_engine *e, double pivscale) {
         for (int h = 0; h < nl; ++h) {
             if (small_factor_level<R>(e->levels[h])) {
                 launch_factor_small<R>(a, e->levels[h], e->st);
+            } else if (use_mid_factor<R>(e->levels[h])) {
+                launch_factor_mid<R>(a, e->levels[h], e->st);
             } else {
                 launch_factor_level<R>(a, e->levels[h], e->st);
                 const auto &pl = e->cb_plan[h];
@@ -412,7 +425,7 @@ static int factor_batch(gm_engine *e, double pivscale) {
             const LevelInfo &L = e->levels[h];
             std::fprintf(stderr, "factor %s level %2d: fronts %5d max_front %4d max_piv %4d %s %.3f ms\n",
                          sizeof(R) == 8 ? "c128" : "c64", h, L.count, L.max_front, L.max_piv,
-                         small_factor_level<R>(L) ? "small" : "tiled", ms);
+                         small_factor_level<R>(L) ? "small" : use_mid_factor<R>(L) ? "mid" : "tiled", ms);
         }
         for (auto &x : ev) cudaEventDestroy(x);
     }

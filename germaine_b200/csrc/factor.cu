@@ -588,3 +588,254 @@ void launch_pack_split(double2 *dst, const double *re, const double *im, size_t 
 }
 
 }  // namespace gm
+
+
+namespace gm {
+
+// ---------------------------------------------------------------------
+// Mid-level fronts: at most NB pivots and at most MID_FT rows, but too
+// large for the small kernel's whole-front tile.  After the extend-add
+// gather and the operator entries (K2), one CTA per front and frequency
+//   1. factorises the pivot columns (f x s) right-looking with each thread
+//      holding one front row in registers: per pivot, the owner of the next
+//      pivot row applies the static pivoting of diag_lu and publishes the
+//      row and the pivot's reciprocal in shared memory, so one barrier per
+//      pivot and no shared-memory traffic for the update itself;
+//   2. solves L11 U12 = A12 with each thread holding one column of U12;
+//   3. inverts the pivot block's two triangles;
+//   4. writes L, U and the inverses back (the layout the blocked path
+//      leaves);
+//   5. applies the rank-s Schur update to the contribution block,
+//      64 x 64 tiles of 4 x 4 complex per thread, each tile's old values
+//      loaded into the accumulators first.
+// This replaces k_panel / k_update and the level's contribution GEMM.
+// Shared memory: P[i + c * (f + 1)] the pivot columns, then
+// U[r + j * (s | 1)] the U12 rows (odd strides: conflict-free 16-byte
+// accesses).
+// ---------------------------------------------------------------------
+constexpr int MID_FT = 256;   // threads per CTA, also the largest front handled
+
+template <class R>
+__device__ __forceinline__ cplx<R> static_pivot(cplx<R> piv, R pivtol, int &npert) {
+    const R mag = sqrt(cabs2(piv));
+    if (!(mag >= pivtol)) {   // also catches NaN
+        if (mag > R(0)) {
+            const R sc = pivtol / mag;
+            piv = mk(piv.x * sc, piv.y * sc);
+        } else {
+            piv = mk(pivtol, R(0));
+        }
+        ++npert;
+    }
+    return piv;
+}
+
+// one complex element global -> shared without a register round trip
+// (cp.async; completes at cp_async_wait_all)
+__device__ __forceinline__ void cp_async_elem(double2 *dst, const double2 *src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+__device__ __forceinline__ void cp_async_elem(float2 *dst, const float2 *src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
+}
+
+template <class R, int NPR>
+__global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_first) {
+    using C = cplx<R>;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    __shared__ C Dinv[NB][NB + 1];
+    __shared__ C urow[2][NPR];   // pivot row k at columns k .. s-1, alternating buffers
+    __shared__ C rd[NPR];        // reciprocal pivots
+    __shared__ int npert;
+    const int node = a.s.lvl_nodes[lvl_first + blockIdx.x];
+    const int f = a.s.nfront[node], s = a.s.npiv[node], m = f - s;
+    if (s == 0) return;   // the gathered front is already the contribution block
+    const int ldp = f + 1, ldu = s | 1;
+    C *P = reinterpret_cast<C *>(smem_raw);
+    C *U = P + (size_t)ldp * s;
+    const int tid = threadIdx.x;
+    C *F = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.y * a.s.front_total + a.s.front_off[node];
+    const R pivtol = (R)(a.pivscale * __longlong_as_double((long long)*a.amax));
+    if (tid == 0) npert = 0;
+
+    for (int t = tid; t < s * m; t += MID_FT) {   // A12, down each column, landing during step 1
+        const int j = t / s, r = t - j * s;
+        cp_async_elem(U + r + j * ldu, F + r + (size_t)(s + j) * f);
+    }
+
+    // 1. pivot columns, one row per thread
+    const bool own = tid < f;
+    C x[NPR];
+#pragma unroll
+    for (int j = 0; j < NPR; ++j) x[j] = (own && j < s) ? F[tid + (size_t)j * f] : czero<C>();
+    int np = 0;
+    if (tid == 0) {
+        x[0] = static_pivot<R>(x[0], pivtol, np);
+        rd[0] = crcp(x[0]);
+#pragma unroll
+        for (int j = 0; j < NPR; ++j)
+            if (j < s) urow[0][j] = x[j];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < NPR; ++k) {
+        if (k >= s) continue;   // s is the same for the whole CTA
+        if (own && tid > k) {
+            const C l = cmul(x[k], rd[k]);
+            x[k] = l;
+#pragma unroll
+            for (int j = k + 1; j < NPR; ++j)
+                if (j < s) cfms(x[j], l, urow[k & 1][j]);
+            const int k1 = k + 1 < NPR ? k + 1 : NPR - 1;
+            if (k + 1 < NPR && tid == k + 1 && k + 1 < s) {   // owner of the next pivot row
+                x[k1] = static_pivot<R>(x[k1], pivtol, np);
+                rd[k1] = crcp(x[k1]);
+#pragma unroll
+                for (int j = k1; j < NPR; ++j)
+                    if (j < s) urow[k1 & 1][j] = x[j];
+            }
+        }
+        __syncthreads();
+    }
+    if (own) {
+#pragma unroll
+        for (int j = 0; j < NPR; ++j)
+            if (j < s) P[tid + j * ldp] = x[j];
+    }
+    if (np) atomicAdd(&npert, np);
+    asm volatile("cp.async.commit_group;\n" ::: "memory");
+    asm volatile("cp.async.wait_all;\n" ::: "memory");
+    __syncthreads();
+
+    // 2. U12 = L11^-1 A12, one column per thread of warps 2 .. 7, while
+    // warps 0 and 1 invert the pivot block's triangles (3.)
+    for (int j = tid - 64; j >= 0 && j < m; j += MID_FT - 64) {
+        C u[NPR];
+#pragma unroll
+        for (int r = 0; r < NPR; ++r) u[r] = r < s ? U[r + j * ldu] : czero<C>();
+#pragma unroll
+        for (int k = 0; k + 1 < NPR; ++k) {
+            if (k + 1 < s) {
+                const C uk = u[k];
+#pragma unroll
+                for (int r = k + 1; r < NPR; ++r)
+                    if (r < s) cfms(u[r], P[r + k * ldp], uk);
+            }
+        }
+#pragma unroll
+        for (int r = 1; r < NPR; ++r)
+            if (r < s) U[r + j * ldu] = u[r];
+    }
+
+    // 3. inverses of the pivot block's triangles: L^-1 strictly below the
+    // diagonal (unit diagonal implied), U^-1 on and above it
+    if (tid < s) {
+        const int c = tid;
+        for (int r = c + 1; r < s; ++r) {
+            C acc = P[r + c * ldp];
+            for (int q = c + 1; q < r; ++q) cfma(acc, P[r + q * ldp], Dinv[q][c]);
+            Dinv[r][c] = mk(-acc.x, -acc.y);
+        }
+    } else if (tid >= 32 && tid < 32 + s) {
+        const int c = tid - 32;
+        Dinv[c][c] = rd[c];
+        for (int r = c - 1; r >= 0; --r) {
+            C acc = czero<C>();
+            for (int q = r + 1; q <= c; ++q) cfma(acc, P[r + q * ldp], Dinv[q][c]);
+            Dinv[r][c] = cmul(mk(-acc.x, -acc.y), rd[r]);
+        }
+    }
+    __syncthreads();
+
+    // 4. write back: pivot columns (inverses in the pivot block), U12
+    for (int t = tid; t < f * s; t += MID_FT) {
+        const int c = t / f, i = t - c * f;
+        F[t] = i < s ? Dinv[i][c] : P[i + c * ldp];
+    }
+    for (int t = tid; t < s * m; t += MID_FT) {
+        const int j = t / s, r = t - j * s;
+        F[r + (size_t)(s + j) * f] = U[r + j * ldu];
+    }
+    if (tid == 0 && npert) atomicAdd(a.npert, (unsigned long long)npert);
+
+    // 5. contribution block -= L21 U12
+    const int tx = tid % 16, ty = tid / 16;
+    for (int i0 = 0; i0 < m; i0 += 64)
+        for (int j0 = 0; j0 < m; j0 += 64) {
+            C acc[4][4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const int i = i0 + tx + 16 * p, j = j0 + ty + 16 * q;
+                    acc[p][q] = (i < m && j < m) ? F[s + i + (size_t)(s + j) * f] : czero<C>();
+                }
+            for (int k = 0; k < s; ++k) {
+                C lv[4], uv[4];
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const int i = i0 + tx + 16 * p;
+                    lv[p] = i < m ? P[s + i + k * ldp] : czero<C>();
+                }
+#pragma unroll
+                for (int q = 0; q < 4; ++q) {
+                    const int j = j0 + ty + 16 * q;
+                    uv[q] = j < m ? U[k + j * ldu] : czero<C>();
+                }
+#pragma unroll
+                for (int p = 0; p < 4; ++p)
+#pragma unroll
+                    for (int q = 0; q < 4; ++q) cfms(acc[p][q], lv[p], uv[q]);
+            }
+#pragma unroll
+            for (int q = 0; q < 4; ++q)
+#pragma unroll
+                for (int p = 0; p < 4; ++p) {
+                    const int i = i0 + tx + 16 * p, j = j0 + ty + 16 * q;
+                    if (i < m && j < m) F[s + i + (size_t)(s + j) * f] = acc[p][q];
+                }
+        }
+}
+
+constexpr size_t MID_FACTOR_SMEM = 200 << 10;
+
+template <class R>
+bool mid_factor_level(const LevelInfo &L) {
+    return L.count > 0 && L.max_piv <= NB && L.max_front <= MID_FT && !small_factor_level<R>(L) &&
+           (size_t)L.mid_words * sizeof(cplx<R>) <= MID_FACTOR_SMEM;
+}
+
+template <class R, int NPR>
+static void launch_mid(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaFuncSetAttribute(k_factor_mid<R, NPR>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)MID_FACTOR_SMEM);
+        attr_set = true;
+    }
+    (k_factor_mid<R, NPR><<<dim3(L.count, a.nf), MID_FT, (size_t)L.mid_words * sizeof(cplx<R>), st>>>(a, L.first),
+     note_launch());
+}
+
+template <class R>
+void launch_factor_mid(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
+    (k_front_gather<R><<<dim3((L.max_front + GATHER_COLS - 1) / GATHER_COLS, L.count, a.nf), 32 * GATHER_COLS, 0,
+                         st>>>(a, L.first),
+     note_launch());
+    if (L.ent_count > 0) {
+        const int tpb = 256;
+        (k_entry_scatter<R><<<dim3((unsigned)((L.ent_count + tpb - 1) / tpb), a.nf), tpb, 0, st>>>(a, L.ent_first,
+                                                                                                  L.ent_count),
+         note_launch());
+    }
+    if (L.max_piv <= 16)
+        launch_mid<R, 16>(a, L, st);
+    else
+        launch_mid<R, NB>(a, L, st);
+}
+
+template bool mid_factor_level<double>(const LevelInfo &);
+template bool mid_factor_level<float>(const LevelInfo &);
+template void launch_factor_mid<double>(const FactorArgs<double> &, const LevelInfo &, cudaStream_t);
+template void launch_factor_mid<float>(const FactorArgs<float> &, const LevelInfo &, cudaStream_t);
+
+}  // namespace gm

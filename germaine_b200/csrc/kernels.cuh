@@ -53,6 +53,7 @@ struct LevelInfo {
     int count;      // nodes in the level
     int max_front, max_piv, max_ring;
     int64_t ent_first, ent_count;  // level's entry range in ent_dst/ent_src
+    int64_t mid_words;  // largest (f + 1) s + (s | 1)(f - s) of the level's fronts: k_factor_mid's tile
 };
 
 template <class R>
@@ -88,6 +89,14 @@ template <class R>
 bool small_factor_level(const LevelInfo &L);
 template <class R>
 void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st);
+// Levels of fronts with at most NB pivots that do not fit the small kernel:
+// gather, operator entries, then one CTA per front factorises the pivot
+// panel in shared memory and applies the Schur update to the contribution
+// block (replaces k_panel / k_update and the level's contribution GEMM).
+template <class R>
+bool mid_factor_level(const LevelInfo &L);
+template <class R>
+void launch_factor_mid(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st);
 
 
 // one dense product C -= A * B (column-major, complex<R>)
