@@ -98,6 +98,12 @@ struct gm_engine {
     gm::DevBuf d_xf, d_xa;   // forward / adjoint solutions kept for the gradient
     gm::DevBuf d_mask;       // forward-pass pruning mask of the current solve
     std::vector<double> last_grad0, last_grad1;
+    // per-shot gradient taper of ass_grad (SWS_TAPER_CIRCULAR_PER_SHOT 0, 1, 2),
+    // its radius (SRTRADIUS, metres) and square half-width (FILTSIZE)
+    int shot_taper = 0;
+    float srt_radius = 0.0f;
+    int filtsize = 0;
+    gm::DevBuf d_taper;   // the taper's tables for the gradient kernel
     std::vector<double> last_hess0, last_hess1;
 
     gm_stats stats{};

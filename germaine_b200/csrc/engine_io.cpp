@@ -248,6 +248,81 @@ extern "C" int gm_obj_each(gm_engine *e, int nshots, const float *src_x, const f
     return solve_rc;
 }
 
+namespace {
+
+// Tables of the per-shot gradient taper (gm_set_shot_taper) for
+// k_gradient, uploaded into e->d_taper: mode 1 the receivers' product of
+// radial coefficients [n] (double), per shot its source window (int4) and
+// offset (int), then the windows' coefficients (float); mode 2 the squares'
+// mask [n].  Host arithmetic of the reference (host_setup.c).
+int shot_taper_tables(gm_engine *e, int ns, const float *sx, const float *sy, int ntr, const int32_t *rx,
+                      const int32_t *ry, gm::GradArgs &ga) {
+    const gm_config &c = e->cfg;
+    const int n = e->n;
+    ga.nx = c.nx;
+    ga.shot_taper = e->shot_taper;
+    if (e->shot_taper == 0) return GM_OK;
+    std::vector<unsigned char> host;
+    auto put = [&host](const void *p, size_t bytes) {   // 16-byte aligned sections
+        const size_t at = (host.size() + 15) / 16 * 16;
+        host.resize(at + bytes);
+        if (bytes) std::memcpy(host.data() + at, p, bytes);
+        return at;
+    };
+    size_t o_rec = 0, o_win = 0, o_off = 0, o_src = 0, o_mask = 0;
+    if (e->shot_taper == 1) {
+        std::vector<double> prod(n);
+        gmh_srt_receiver_product(c.nx, c.ny, c.dh, e->srt_radius, ntr, rx, ry, prod.data());
+        std::vector<int4> win(ns);
+        std::vector<int> off(ns);
+        std::vector<float> coef;
+        for (int s = 0; s < ns; ++s) {
+            int x0, x1, y0, y1;
+            gmh_srt_range(sx[s], e->srt_radius, c.dh, c.nx, &x0, &x1);
+            gmh_srt_range(sy[s], e->srt_radius, c.dh, c.ny, &y0, &y1);
+            const int w = std::max(0, x1 - x0 + 1), h = std::max(0, y1 - y0 + 1);
+            win[s] = make_int4(x0 - 1, y0 - 1, w, h);
+            off[s] = (int)coef.size();
+            for (int iy = y0; iy <= y1; ++iy)
+                for (int ix = x0; ix <= x1; ++ix) coef.push_back(gmh_srt_coef(ix, iy, c.dh, sx[s], sy[s], e->srt_radius));
+        }
+        o_rec = put(prod.data(), prod.size() * sizeof(double));
+        o_win = put(win.data(), win.size() * sizeof(int4));
+        o_off = put(off.data(), off.size() * sizeof(int));
+        o_src = put(coef.data(), coef.size() * sizeof(float));
+    } else {
+        std::vector<unsigned char> mask(n, 0);
+        gmh_taper_grad_shot1(c.nx, c.ny, c.dh, e->filtsize, ns, sx, sy, ntr, rx, ry, nullptr, mask.data());
+        o_mask = put(mask.data(), mask.size());
+    }
+    GM_ALLOC(e->d_taper, host.size() + 16);
+    GM_CUDA(cudaMemcpyAsync(e->d_taper.p, host.data(), host.size(), cudaMemcpyHostToDevice, e->st));
+    GM_CUDA(cudaStreamSynchronize(e->st));   // host is freed on return
+    const char *base = static_cast<const char *>(e->d_taper.p);
+    if (e->shot_taper == 1) {
+        ga.taper_rec = reinterpret_cast<const double *>(base + o_rec);
+        ga.taper_win = reinterpret_cast<const int4 *>(base + o_win);
+        ga.taper_off = reinterpret_cast<const int *>(base + o_off);
+        ga.taper_src = reinterpret_cast<const float *>(base + o_src);
+    } else {
+        ga.taper_mask = reinterpret_cast<const unsigned char *>(base + o_mask);
+    }
+    return GM_OK;
+}
+
+}  // namespace
+
+extern "C" int gm_set_shot_taper(gm_engine *e, int mode, float srtradius, int filtsize) {
+    if (!e) return fail(GM_ERROR_INVALID, "gm_set_shot_taper: no engine");
+    if (mode < 0 || mode > 2) return fail(GM_ERROR_INVALID, "gm_set_shot_taper: mode must be 0, 1 or 2");
+    if (mode == 1 && !(srtradius > 0.0f)) return fail(GM_ERROR_INVALID, "gm_set_shot_taper: SRTRADIUS must be > 0");
+    if (mode == 2 && filtsize < 0) return fail(GM_ERROR_INVALID, "gm_set_shot_taper: FILTSIZE must be >= 0");
+    e->shot_taper = mode;
+    e->srt_radius = srtradius;
+    e->filtsize = filtsize;
+    return GM_OK;
+}
+
 extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y, int ntr,
                            const int32_t *rec_x, const int32_t *rec_y, const float *pobs, int stf_inv, int misfit,
                            float *grad0, float *grad1, float *l2_out, float *seis) {
@@ -307,6 +382,7 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     ga.m0 = e->d_m0.as<float>() + (size_t)e->models[0] * n; ga.m1 = e->d_m1.as<float>() + (size_t)e->models[0] * n;
     ga.frame = e->d_frame.as<float>(); ga.passes = e->d_frame_pass.as<unsigned char>();
     ga.g0 = e->d_grad.as<double>(); ga.g1 = ga.g0 + n;
+    if ((rc = shot_taper_tables(e, nshots, src_x, src_y, ntr, rec_x, rec_y, ga))) return rc;
     gm::launch_gradient(ga, e->st);
     GM_CUDA(cudaGetLastError());
     e->last_grad0.resize(n);

@@ -178,20 +178,61 @@ __global__ void k_gradient(GradArgs a) {
         const double vp = a.m0[k], rho = a.m1[k];
         mat = 1.0 / (rho * vp * vp * vp);
     }
-    for (int f = 0; f < a.nf; ++f) {
-        const double2 om2 = a.om2[f], om = a.om[f];
-        const double2 *xf = a.xf + (size_t)f * a.n * a.ns;
-        const double2 *xa = a.xa + (size_t)f * a.n * a.ns;
-        for (int s = 0; s < a.ns; ++s) {
-            const double2 u = shifted(xf, a.n, a.ns, k, s);
-            const double2 l = shifted(xa, a.n, a.ns, k, s);
-            const double2 w = a.stfu[(size_t)f * a.ns + s];
-            const double2 wul = cmul(cmul(w, u), l);
-            if (!a.te) {
-                g0 += -2.0 * cmul(om2, wul).x * mat;
-            } else {
-                g0 += cmul(wul, make_double2(-om.y, om.x)).x;   // (i Omega) = (-Om.im, Om.re)
-                g1 += cmul(om2, wul).x;
+    if (a.shot_taper == 0) {
+        for (int f = 0; f < a.nf; ++f) {
+            const double2 om2 = a.om2[f], om = a.om[f];
+            const double2 *xf = a.xf + (size_t)f * a.n * a.ns;
+            const double2 *xa = a.xa + (size_t)f * a.n * a.ns;
+            for (int s = 0; s < a.ns; ++s) {
+                const double2 u = shifted(xf, a.n, a.ns, k, s);
+                const double2 l = shifted(xa, a.n, a.ns, k, s);
+                const double2 w = a.stfu[(size_t)f * a.ns + s];
+                const double2 wul = cmul(cmul(w, u), l);
+                if (!a.te) {
+                    g0 += -2.0 * cmul(om2, wul).x * mat;
+                } else {
+                    g0 += cmul(wul, make_double2(-om.y, om.x)).x;   // (i Omega) = (-Om.im, Om.re)
+                    g1 += cmul(om2, wul).x;
+                }
+            }
+        }
+    } else {
+        // each shot's term times its taper: radial coefficients (the shot's
+        // source window, else 1, times the receivers' product), or 1e-5 in
+        // place of the term on the squares
+        const int ix = k % a.nx, iy = k / a.nx;
+        const double crec = a.shot_taper == 1 ? a.taper_rec[k] : 1.0;
+        const bool square = a.shot_taper == 2 && a.taper_mask[k];
+        for (int f = 0; f < a.nf; ++f) {
+            const double2 om2 = a.om2[f], om = a.om[f];
+            const double2 *xf = a.xf + (size_t)f * a.n * a.ns;
+            const double2 *xa = a.xa + (size_t)f * a.n * a.ns;
+            for (int s = 0; s < a.ns; ++s) {
+                const double2 u = shifted(xf, a.n, a.ns, k, s);
+                const double2 l = shifted(xa, a.n, a.ns, k, s);
+                const double2 w = a.stfu[(size_t)f * a.ns + s];
+                const double2 wul = cmul(cmul(w, u), l);
+                double t0, t1 = 0.0;
+                if (!a.te) {
+                    t0 = -2.0 * cmul(om2, wul).x * mat;
+                } else {
+                    t0 = cmul(wul, make_double2(-om.y, om.x)).x;
+                    t1 = cmul(om2, wul).x;
+                }
+                if (a.shot_taper == 1) {
+                    const int4 win = a.taper_win[s];
+                    const int dx = ix - win.x, dy = iy - win.y;
+                    const double c = (dx >= 0 && dx < win.z && dy >= 0 && dy < win.w)
+                                         ? crec * (double)a.taper_src[a.taper_off[s] + dy * win.z + dx]
+                                         : crec;
+                    t0 *= c;
+                    t1 *= c;
+                } else if (square) {
+                    t0 = (double)1e-5f;
+                    t1 = (double)1e-5f;
+                }
+                g0 += t0;
+                g1 += t1;
             }
         }
     }

@@ -223,3 +223,113 @@ int gmh_gauss_kernel(float dh, float vref, float fc_low, float fsg, float fsg1, 
         for (ii = 0; ii < nwx * nwy; ii++) w[ii] /= sum;
     return nwx * nwy;
 }
+
+/* ---------------------------------------------------------------------
+ * Per-shot gradient tapers of ass_grad_AC / ass_grad_TE
+ * (src/AC/ass_grad_AC.c:37-43, src/TE/ass_grad_TE.c:41-49), selected by
+ * SWS_TAPER_CIRCULAR_PER_SHOT:
+ *   1  taper_grad_shot  (src/taper_grad_shot.c:11-99): the shot's gradient
+ *      times a radial taper around its source and around every receiver,
+ *      f0 + (1 - f0) (1/2 - 1/2 cos(pi r / R))^a inside the radius
+ *      R = SRTRADIUS, 1 outside, f0 = 1e-3, a = -log2((0.1 - f0) / (1 - f0));
+ *   2  taper_grad_shot1 (src/taper_grad_shot1.c:11-60): the shot's gradient
+ *      set to 1e-5 on the (2 FILTSIZE + 1)^2 squares around every source
+ *      of the call and every receiver.
+ * Both read the interior source coordinates (metres) and receiver grid
+ * indices as if they were full-grid ones (x = ix DH over the whole grid, no
+ * NPML / FSSHIFT shift): the tapers sit NPML columns (FSSHIFT rows) away
+ * from the physical positions.  Reproduced.  Grids are row-major [NY][NX];
+ * (ix, iy) are the reference's 1-based indices.
+ * --------------------------------------------------------------------- */
+static float srt_exponent(void)
+{
+    float frh = 0.1, f0 = 1e-3;
+    return -(log(frh - f0) - log(1.0 - f0)) / log(2.0);
+}
+
+/* coefficient of the radial taper at (ix, iy) for a centre (xc, yc) in
+ * metres: the reference's float / double evaluation order */
+float gmh_srt_coef(int ix, int iy, float dh, float xc, float yc, float radius)
+{
+    const float f0 = 1e-3, a = srt_exponent();
+    float x = ix * dh, y = iy * dh, r, taper = 1.0;
+    r = sqrt(pow((x - xc), 2.0) + pow((y - yc), 2.0));
+    if (r <= radius) taper = f0 + (1.0 - f0) * pow((0.5 - 0.5 * cos(3.141592653589793 * r / radius)), a);
+    return taper;
+}
+
+/* 1-based index range [*lo, *hi] of points i with i dh within radius of c,
+ * one point of margin, clamped to [1, n] (*lo > *hi: none) */
+void gmh_srt_range(float c, float radius, float dh, int n, int *lo, int *hi)
+{
+    double l = floor((c - radius) / dh) - 1.0, h = ceil((c + radius) / dh) + 1.0;
+    *lo = l < 1.0 ? 1 : (l > n ? n + 1 : (int)l);
+    *hi = h > n ? n : (h < 1.0 ? 0 : (int)h);
+}
+
+/* radial taper of one centre applied to grid (float products, in place);
+ * outside the window the reference multiplies by 1.0f, which changes nothing */
+static void srt_apply(int nx, int ny, float dh, float xc, float yc, float radius, float *grid)
+{
+    int x0, x1, y0, y1, ix, iy;
+    gmh_srt_range(xc, radius, dh, nx, &x0, &x1);
+    gmh_srt_range(yc, radius, dh, ny, &y0, &y1);
+    for (iy = y0; iy <= y1; iy++)
+        for (ix = x0; ix <= x1; ix++) grid[(size_t)(iy - 1) * nx + ix - 1] *= gmh_srt_coef(ix, iy, dh, xc, yc, radius);
+}
+
+/* taper_grad_shot on one shot's float gradient: the source of shot ishot
+ * (0-based) first, then the receivers in order */
+void gmh_taper_grad_shot(int nx, int ny, float dh, float radius, const float *sx, const float *sy, int ntr,
+                         const int *rx, const int *ry, int ishot, float *grid)
+{
+    int n;
+    srt_apply(nx, ny, dh, sx[ishot], sy[ishot], radius, grid);
+    for (n = 0; n < ntr; n++) srt_apply(nx, ny, dh, rx[n] * dh, ry[n] * dh, radius, grid);
+}
+
+/* square of taper_grad_shot1 around grid point (i1, j1), clipped to the
+ * grid (the reference writes past the array when a square crosses the
+ * edge); value written: mark != NULL sets mark to 1, else grid to 1e-5 */
+static void square_set(int nx, int ny, int i1, int j1, int filtsize, float *grid, unsigned char *mark)
+{
+    int i, j;
+    for (i = i1 - filtsize; i <= i1 + filtsize; i++)
+        for (j = j1 - filtsize; j <= j1 + filtsize; j++) {
+            if (i < 1 || i > nx || j < 1 || j > ny) continue;
+            if (mark)
+                mark[(size_t)(j - 1) * nx + i - 1] = 1;
+            else
+                grid[(size_t)(j - 1) * nx + i - 1] = 1e-5f;
+        }
+}
+
+/* taper_grad_shot1 on one shot's float gradient (grid != NULL), or its
+ * mask of the points it overwrites (mark != NULL, zeroed by the caller) */
+void gmh_taper_grad_shot1(int nx, int ny, float dh, int filtsize, int nshots, const float *sx, const float *sy,
+                          int ntr, const int *rx, const int *ry, float *grid, unsigned char *mark)
+{
+    int n;
+    for (n = 0; n < nshots; n++) {
+        float qx = sx[n] / dh, qy = sy[n] / dh;
+        square_set(nx, ny, (int)floor(qx + 0.5), (int)floor(qy + 0.5), filtsize, grid, mark);
+    }
+    for (n = 0; n < ntr; n++) square_set(nx, ny, rx[n], ry[n], filtsize, grid, mark);
+}
+
+/* product over the receivers of their radial taper coefficients, in double
+ * (prod[n] = 1 where no receiver is within reach) */
+void gmh_srt_receiver_product(int nx, int ny, float dh, float radius, int ntr, const int *rx, const int *ry,
+                              double *prod)
+{
+    int n, x0, x1, y0, y1, ix, iy;
+    for (ix = 0; ix < nx * ny; ix++) prod[ix] = 1.0;
+    for (n = 0; n < ntr; n++) {
+        const float xc = rx[n] * dh, yc = ry[n] * dh;
+        gmh_srt_range(xc, radius, dh, nx, &x0, &x1);
+        gmh_srt_range(yc, radius, dh, ny, &y0, &y1);
+        for (iy = y0; iy <= y1; iy++)
+            for (ix = x0; ix <= x1; ix++)
+                prod[(size_t)(iy - 1) * nx + ix - 1] *= (double)gmh_srt_coef(ix, iy, dh, xc, yc, radius);
+    }
+}

@@ -15,6 +15,14 @@ void gmh_stf_unit(const float stf[2], float unit[2]);
 void gmh_wiener(const float num[2], const float den[2], float wien[2]);
 void gmh_grad_frame(int nx, int ny, int npml, int free_surf, float *coef, unsigned char *passes);
 int gmh_gauss_kernel(float dh, float vref, float fc_low, float fsg, float fsg1, int hfs[2], float *w, int wmax);
+float gmh_srt_coef(int ix, int iy, float dh, float xc, float yc, float radius);
+void gmh_srt_range(float c, float radius, float dh, int n, int *lo, int *hi);
+void gmh_taper_grad_shot(int nx, int ny, float dh, float radius, const float *sx, const float *sy, int ntr,
+                         const int *rx, const int *ry, int ishot, float *grid);
+void gmh_taper_grad_shot1(int nx, int ny, float dh, int filtsize, int nshots, const float *sx, const float *sy,
+                          int ntr, const int *rx, const int *ry, float *grid, unsigned char *mark);
+void gmh_srt_receiver_product(int nx, int ny, float dh, float radius, int ntr, const int *rx, const int *ry,
+                              double *prod);
 #ifdef __cplusplus
 }
 #endif

@@ -15,6 +15,14 @@ struct GradArgs {
     const float *frame;         // PML taper coefficient per grid point
     const unsigned char *passes;
     double *g0, *g1;            // [n] outputs (FP64)
+    // per-shot taper (0 none; 1 radial around the shot's source and every
+    // receiver; 2 the term replaced by 1e-5 on the marked squares)
+    int nx, shot_taper;
+    const double *taper_rec;    // [n] product of the receivers' radial coefficients (1)
+    const int4 *taper_win;      // per shot: first column, first row (0-based), width, height of its source window (1)
+    const int *taper_off;       // per shot: offset of its window's coefficients in taper_src (1)
+    const float *taper_src;     // source-window coefficients, row-major per window (1)
+    const unsigned char *taper_mask;   // [n] 1 on the squares (2)
 };
 
 struct HessArgs {

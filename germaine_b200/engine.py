@@ -207,6 +207,13 @@ class Engine:
                                                       ptr(seis)))
         return g0, g1, float(l2.value), seis
 
+    def set_shot_taper(self, mode: int, srtradius: float = 0.0, filtsize: int = 0) -> None:
+        """Per-shot gradient taper of the following grad_obj calls
+        (SWS_TAPER_CIRCULAR_PER_SHOT): 0 none, 1 taper_grad_shot (radius
+        SRTRADIUS in metres), 2 taper_grad_shot1 (squares of half-width
+        FILTSIZE)."""
+        check(self.lib.gm_set_shot_taper(self._h, mode, srtradius, filtsize))
+
     def gradient_fp64(self):
         g0 = np.zeros(self.n)
         g1 = np.zeros(self.n) if self.physics == GM_PHYS_TE else None
@@ -319,6 +326,30 @@ def mat_change(hgrad, model_old, eps_scale: float, low: float, up: float, mode: 
     out = np.empty_like(old)
     check(_lib.load().gm_mat_change(device, old.size, mode, eps_scale, low, up, ptr(h), ptr(old), ptr(out)))
     return out
+
+
+def taper_grad_shot(grad, dh: float, srtradius: float, src_x, src_y, rec_x, rec_y, ishot: int) -> np.ndarray:
+    """taper_grad_shot on one shot's [NY][NX] float gradient (host,
+    bit-identical): returns the tapered copy; ishot is 0-based."""
+    g = np.array(grad, np.float32, copy=True, order="C")
+    ny, nx = g.shape
+    sx = _c(src_x, np.float32); sy = _c(src_y, np.float32)
+    rx = _c(rec_x, np.int32); ry = _c(rec_y, np.int32)
+    check(_lib.load().gm_taper_grad_shot(nx, ny, dh, srtradius, sx.size, ptr(sx), ptr(sy), rx.size, ptr(rx),
+                                         ptr(ry), ishot, ptr(g)))
+    return g
+
+
+def taper_grad_shot1(grad, dh: float, filtsize: int, src_x, src_y, rec_x, rec_y) -> np.ndarray:
+    """taper_grad_shot1 on one shot's [NY][NX] float gradient (host,
+    bit-identical): returns the tapered copy."""
+    g = np.array(grad, np.float32, copy=True, order="C")
+    ny, nx = g.shape
+    sx = _c(src_x, np.float32); sy = _c(src_y, np.float32)
+    rx = _c(rec_x, np.int32); ry = _c(rec_y, np.int32)
+    check(_lib.load().gm_taper_grad_shot1(nx, ny, dh, filtsize, sx.size, ptr(sx), ptr(sy), rx.size, ptr(rx),
+                                          ptr(ry), ptr(g)))
+    return g
 
 
 def precond(grad, npml: int, free_surf: int, dh: float, spatfilter: int = 0, vref: float = 0.0,

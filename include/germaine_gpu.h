@@ -192,6 +192,22 @@ int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y
                 const float *pobs, int stf_inv, int misfit,
                 float *grad0, float *grad1, float *l2, float *seis);
 
+/* Per-shot gradient taper applied by gm_grad_obj inside its shot stack
+ * (SWS_TAPER_CIRCULAR_PER_SHOT of ass_grad_AC / ass_grad_TE,
+ * src/AC/ass_grad_AC.c:37-43, src/TE/ass_grad_TE.c:41-49):
+ *   mode 0  none (the default);
+ *   mode 1  taper_grad_shot: each shot's term times the radial taper of
+ *           radius srtradius (SRTRADIUS, metres) around its source and
+ *           around every receiver;
+ *   mode 2  taper_grad_shot1: each shot's term replaced by 1e-5 on the
+ *           (2 filtsize + 1)^2 squares (FILTSIZE) around every source of
+ *           the call and every receiver.
+ * As in the reference, the tapers are centred at the interior source
+ * coordinates and receiver indices read as full-grid ones (NPML columns,
+ * FSSHIFT rows away from the physical positions).  The product of a
+ * shot's coefficients is formed in FP64 and applied to the FP64 term. */
+int gm_set_shot_taper(gm_engine *e, int mode, float srtradius, int filtsize);
+
 /* The last gm_grad_obj gradients before rounding to float, in FP64
  * ([NY][NX] each; g1 ignored for AC).  Either pointer may be NULL. */
 int gm_get_gradient_fp64(gm_engine *e, double *g0, double *g1);
@@ -317,6 +333,22 @@ int gm_lbfgs_set_old(gm_lbfgs *h, const float *grad_old, const float *model_old)
  * [low, up]).  Bit-identical; host or device buffers. */
 int gm_mat_change(int device, int n, int mode, float eps_scale, float low, float up, const float *hgrad,
                   const float *model_old, float *model);
+
+/* Host drop-ins for the reference's per-shot tapers, on one shot's float
+ * gradient [NY][NX] (NX, NY with the PML frame) in place, float results
+ * identical to the reference's:
+ *   gm_taper_grad_shot   taper_grad_shot (src/taper_grad_shot.c:11): the
+ *                        radial taper around source ishot (0-based) of
+ *                        src_x/src_y (metres, interior coordinates), then
+ *                        around every receiver (interior grid indices);
+ *   gm_taper_grad_shot1  taper_grad_shot1 (src/taper_grad_shot1.c:11):
+ *                        1e-5 on the squares around all nshots sources and
+ *                        all receivers, clipped to the grid. */
+int gm_taper_grad_shot(int nx, int ny, float dh, float srtradius, int nshots, const float *src_x,
+                       const float *src_y, int ntr, const int32_t *rec_x, const int32_t *rec_y, int ishot,
+                       float *grad);
+int gm_taper_grad_shot1(int nx, int ny, float dh, int filtsize, int nshots, const float *src_x,
+                        const float *src_y, int ntr, const int32_t *rec_x, const int32_t *rec_y, float *grad);
 
 /* ---- the reference's file formats (host stdio, no GPU needed) ---- */
 #define GM_SEIS_KEEP_LAST 1  /* gm_write_seis: write the last sample as given */

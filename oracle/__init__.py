@@ -116,6 +116,9 @@ def load_port():
         lib.port_check_descent.argtypes = [P, ctypes.c_int, _f32p, _f32p]
         lib.port_check_descent.restype = ctypes.c_float
         lib.port_precond_tapers.argtypes = [P, ctypes.c_int, ctypes.c_int, ctypes.c_void_p, _f32p]
+        lib.port_srt_field.argtypes = [P, ctypes.c_float, ctypes.c_float, ctypes.c_float, _f32p]
+        lib.port_taper_grad_shot1.argtypes = [P, ctypes.c_int, ctypes.c_int, _f32p, _f32p, ctypes.c_int, _i32p, _i32p,
+                                              _f32p]
         _port_lib = lib
     return _port_lib
 
@@ -152,6 +155,10 @@ def load_ref():
         lib.ref_writemod.argtypes = [cp, i, i, _f32p]
         lib.ref_readmod.argtypes = [cp, _f32p, _f32p]
         lib.ref_apply_hess.argtypes = [ctypes.c_float, _f32p, _f32p]
+        lib.ref_taper_grad_shot.argtypes = [ctypes.c_float, ctypes.c_int, _f32p, _f32p, ctypes.c_int, _i32p, _i32p,
+                                            ctypes.c_int, _f32p]
+        lib.ref_taper_grad_shot1.argtypes = [ctypes.c_int, ctypes.c_int, _f32p, _f32p, ctypes.c_int, _i32p, _i32p,
+                                             _f32p]
         lib.ref_apply_hess.restype = ctypes.c_float
         fp = _f32p
         lib.ref_lbfgs_ac.argtypes = [i, i, i, fp, fp, fp, fp, fp, fp, fp, fp, fp, fp, cp, fp]
@@ -252,6 +259,27 @@ class Port:
 
     def cp_grad_frame(self, grad):
         self.lib.port_cp_grad_frame(ctypes.byref(self._pg), grad)
+
+    def srt_field(self, xc, yc, radius):
+        """Radial taper coefficients of one centre (metres), [NY*NX] float."""
+        c = np.zeros(self.g.n, np.float32)
+        self.lib.port_srt_field(ctypes.byref(self._pg), xc, yc, radius, c)
+        return c
+
+    def taper_grad_shot(self, grad, radius, sx, sy, rx, ry, ishot):
+        """taper_grad_shot on a [NY*NX] float gradient: the source of shot
+        ishot (0-based), then each receiver, one float product each."""
+        out = _f32(grad).copy()
+        out *= self.srt_field(float(sx[ishot]), float(sy[ishot]), radius)
+        for x, y in zip(rx, ry):
+            out *= self.srt_field(np.float32(x) * np.float32(self.g.dh), np.float32(y) * np.float32(self.g.dh), radius)
+        return out
+
+    def taper_grad_shot1(self, grad, filtsize, sx, sy, rx, ry):
+        out = _f32(grad).copy()
+        self.lib.port_taper_grad_shot1(ctypes.byref(self._pg), filtsize, len(sx), _f32(sx), _f32(sy), len(rx),
+                                       np.asarray(rx, np.int32), np.asarray(ry, np.int32), out)
+        return out
 
     def gauss_filt(self, grad, vref, fc_low, fsg, fsg1):
         """Filtered copy of a [NY][NX] gradient (gauss_filt)."""
@@ -376,6 +404,18 @@ class Ref:
 
     def cp_grad_frame(self, grad):
         self.lib.ref_cp_grad_frame(grad)
+
+    def taper_grad_shot(self, grad, radius, sx, sy, rx, ry, ishot):
+        out = _f32(grad).copy()
+        self.lib.ref_taper_grad_shot(radius, len(sx), _f32(sx), _f32(sy), len(rx), np.asarray(rx, np.int32),
+                                     np.asarray(ry, np.int32), ishot, out)
+        return out
+
+    def taper_grad_shot1(self, grad, filtsize, sx, sy, rx, ry):
+        out = _f32(grad).copy()
+        self.lib.ref_taper_grad_shot1(filtsize, len(sx), _f32(sx), _f32(sy), len(rx), np.asarray(rx, np.int32),
+                                      np.asarray(ry, np.int32), out)
+        return out
 
     def gauss_filt(self, grad, vref, fc_low, fsg, fsg1):
         out = np.ascontiguousarray(grad, np.float32).copy()

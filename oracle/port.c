@@ -636,3 +636,37 @@ void port_precond_tapers(const port_grid *g, int taper_hor, int gradt2, const fl
     }
 #undef G
 }
+
+/* Radial taper field of one centre (xc, yc) in metres, as taper_grad_shot
+ * evaluates it for the shot's source (src/taper_grad_shot.c:33-37, 47-56)
+ * and for each receiver with centre recpos * DH (:66-76):
+ * coef = f0 + (1 - f0) (1/2 - 1/2 cos(pi r / R))^a for r <= R, 1 beyond,
+ * x = i DH and y = j DH over the whole grid (no PML shift). */
+void port_srt_field(const port_grid *g, float xc, float yc, float radius, float *coef)
+{
+    float frh = 0.1, f0 = 1e-3;
+    float a = -(log(frh - f0) - log(1.0 - f0)) / log(2.0);
+    for (int j = 1; j <= g->ny; j++)
+        for (int i = 1; i <= g->nx; i++) {
+            float x = i * g->dh, y = j * g->dh;
+            float r = sqrt(pow((x - xc), 2.0) + pow((y - yc), 2.0));
+            float t = 1.0;
+            if (r <= radius) t = f0 + (1.0 - f0) * pow((0.5 - 0.5 * cos(M_PI * r / radius)), a);
+            coef[(j - 1) * g->nx + i - 1] = t;
+        }
+}
+
+/* taper_grad_shot1 (src/taper_grad_shot1.c:25-57): 1e-5 on the
+ * (2 F + 1)^2 squares around every source (centre iround(x / DH)) and every
+ * receiver (its grid indices); points off the grid are skipped. */
+void port_taper_grad_shot1(const port_grid *g, int filtsize, int nshots, const float *sx, const float *sy, int ntr,
+                           const int *rx, const int *ry, float *grad)
+{
+    for (int n = 0; n < nshots + ntr; n++) {
+        const int i1 = n < nshots ? iround_f(sx[n] / g->dh) : rx[n - nshots];
+        const int j1 = n < nshots ? iround_f(sy[n] / g->dh) : ry[n - nshots];
+        for (int i = i1 - filtsize; i <= i1 + filtsize; i++)
+            for (int j = j1 - filtsize; j <= j1 + filtsize; j++)
+                if (i >= 1 && i <= g->nx && j >= 1 && j <= g->ny) grad[(j - 1) * g->nx + i - 1] = 1e-5f;
+    }
+}

@@ -37,6 +37,8 @@
  *   rot_LBFGS_vec        src/rot_LBFGS_vec.c:10
  *   dotp_matrix          src/dotp_matrix.c:8
  *   precond              src/precond.c:10   (+ taper_grad_hor, taper_grad_file)
+ *   taper_grad_shot      src/taper_grad_shot.c:11
+ *   taper_grad_shot1     src/taper_grad_shot1.c:11
  */
 #include <unistd.h>
 
@@ -452,4 +454,47 @@ int ref_precond(const char *dir, int spatfilter, float vref, float fc_low, float
     from_nr(gr, grad);
     free_matrix(gr, 0, NY + 1, 0, NX + 1);
     return chdir(cwd) == 0 ? 0 : -1;
+}
+
+/* taper_grad_shot / taper_grad_shot1 on one shot's flat [NY][NX] float
+ * gradient, in place; sources in metres (srcpos[1]/[2]), receivers as grid
+ * indices (recpos[1]/[2]), ishot 0-based.  Callers keep every square of
+ * taper_grad_shot1 inside the grid (the reference does not clip them). */
+static float **srcpos_nr(int nshots, const float *sx, const float *sy)
+{
+    float **sp = matrix(1, 8, 1, nshots);
+    int n, q;
+    for (n = 1; n <= nshots; n++) {
+        for (q = 1; q <= 8; q++) sp[q][n] = 0.0f;
+        sp[1][n] = sx[n - 1]; sp[2][n] = sy[n - 1];
+    }
+    return sp;
+}
+
+void ref_taper_grad_shot(float srtradius, int nshots, const float *sx, const float *sy, int ntr, const int *rx,
+                         const int *ry, int ishot, float *grad)
+{
+    extern float SRTRADIUS;
+    float **g = to_nr(grad), **sp = srcpos_nr(nshots, sx, sy);
+    int **rp = recpos_nr(ntr, rx, ry);
+    SRTRADIUS = srtradius;
+    taper_grad_shot(g, sp, nshots, rp, ntr, ishot + 1);
+    from_nr(g, grad);
+    free_matrix(g, 0, NY + 1, 0, NX + 1);
+    free_matrix(sp, 1, 8, 1, nshots);
+    free_imatrix(rp, 1, 3, 1, ntr);
+}
+
+void ref_taper_grad_shot1(int filtsize, int nshots, const float *sx, const float *sy, int ntr, const int *rx,
+                          const int *ry, float *grad)
+{
+    extern int FILTSIZE;
+    float **g = to_nr(grad), **sp = srcpos_nr(nshots, sx, sy);
+    int **rp = recpos_nr(ntr, rx, ry);
+    FILTSIZE = filtsize;
+    taper_grad_shot1(g, sp, nshots, rp, ntr, 1);
+    from_nr(g, grad);
+    free_matrix(g, 0, NY + 1, 0, NX + 1);
+    free_matrix(sp, 1, 8, 1, nshots);
+    free_imatrix(rp, 1, 3, 1, ntr);
 }

@@ -122,9 +122,47 @@ def grad_frame(g: Grid, port: Port | None = None):
     return coef, passes.reshape(-1)
 
 
-def gradient_fp64(g: Grid, physics: int, freqs, Xf, Xa, stfu, vp=None, rho=None, port: Port | None = None):
+def shot_taper(g: Grid, mode: int, sx, sy, rx, ry, radius: float = 0.0, filtsize: int = 0,
+               port: Port | None = None):
+    """The per-shot gradient taper of ass_grad_AC / ass_grad_TE
+    (SWS_TAPER_CIRCULAR_PER_SHOT, src/AC/ass_grad_AC.c:37-43) in the FP64
+    form the gradient stack applies: mode 1 ("radial", C[ns][n]) with
+    C_s = (product over the receivers, in order, of their radial
+    coefficients) * (shot s's source coefficients), the coefficients those
+    of taper_grad_shot (port_srt_field); mode 2 ("squares", mask[n]) with
+    the points taper_grad_shot1 overwrites; mode 0 None."""
+    port = port or Port(g)
+    if mode == 1:
+        dh = np.float32(g.dh)
+        crec = np.ones(g.n)
+        for x, y in zip(rx, ry):
+            crec *= port.srt_field(np.float32(x) * dh, np.float32(y) * dh, radius).astype(np.float64)
+        C = np.stack([crec * port.srt_field(float(sx[s]), float(sy[s]), radius).astype(np.float64)
+                      for s in range(len(sx))])
+        return ("radial", C)
+    if mode == 2:
+        return ("squares", port.taper_grad_shot1(np.zeros(g.n, np.float32), filtsize, sx, sy, rx, ry) != 0)
+    return None
+
+
+def _taper_terms(t, taper):
+    """Per-shot terms [ns][n] of one frequency after the shot taper."""
+    if taper is None:
+        return t
+    kind, val = taper
+    if kind == "radial":
+        return t * val
+    t = t.copy()
+    t[:, val] = float(np.float32(1e-5))
+    return t
+
+
+def gradient_fp64(g: Grid, physics: int, freqs, Xf, Xa, stfu, vp=None, rho=None, port: Port | None = None,
+                  taper=None):
     """FP64 ass_grad_AC / ass_grad_TE summed over frequencies and shots, then
-    the cp_grad_frame taper.  Xf, Xa: [nf][n][ns] solutions; stfu[nf][ns]."""
+    the cp_grad_frame taper.  Xf, Xa: [nf][n][ns] solutions; stfu[nf][ns];
+    taper: the per-shot taper of shot_taper (None: SWS_TAPER_CIRCULAR_PER_SHOT
+    = 0)."""
     port = port or Port(g)
     nf = len(freqs)
     g0 = np.zeros(g.n)
@@ -139,11 +177,16 @@ def gradient_fp64(g: Grid, physics: int, freqs, Xf, Xa, stfu, vp=None, rho=None,
         u = vec2mat(Xf[f].T)  # [ns][n]
         lam = vec2mat(Xa[f].T)
         wul = stfu[f][:, None] * u * lam
-        if physics != PHYS_TE:
+        if taper is None and physics != PHYS_TE:
             g0 += np.sum(-2.0 * (om2 * wul).real * mat[None, :], axis=0)
-        else:
+        elif taper is None:
             g0 += np.sum((wul * (1j * om)).real, axis=0)
             g1 += np.sum((om2 * wul).real, axis=0)
+        elif physics != PHYS_TE:
+            g0 += np.sum(_taper_terms(-2.0 * (om2 * wul).real * mat[None, :], taper), axis=0)
+        else:
+            g0 += np.sum(_taper_terms((wul * (1j * om)).real, taper), axis=0)
+            g1 += np.sum(_taper_terms((om2 * wul).real, taper), axis=0)
     coef, passes = grad_frame(g, port)
     fac = coef ** passes
     return g0 * fac, (g1 * fac if physics == PHYS_TE else None)

@@ -5,9 +5,10 @@ profiles and assembled triplets (init_A_*_9p_pml) and, for the acoustic
 cases, a right-hand side with its FP64 sparse solution on the operator
 UMFPACK factorises (M = A^T; solved with SciPy SuperLU because UMFPACK is
 not part of the reference tree); postproc_gauss_filt.npz holds gauss_filt
-cases, postproc_apply_hess.npz apply_hess_AC cases and files_formats.npz
-the bytes of the reference's seismogram and model files.
-Run:  python tests/golden/make_golden.py [assembly] [gauss] [hess] [files]
+cases, postproc_apply_hess.npz apply_hess_AC cases, postproc_shot_taper.npz
+taper_grad_shot / taper_grad_shot1 cases and files_formats.npz the bytes
+of the reference's seismogram and model files.
+Run:  python tests/golden/make_golden.py [assembly] [gauss] [hess] [precond] [shot] [files]
 (no argument: all).
 """
 import tempfile
@@ -34,7 +35,7 @@ CASES = [
 
 def main():
     out = os.path.dirname(os.path.abspath(__file__))
-    which = set(sys.argv[1:]) or {"assembly", "gauss", "hess", "precond", "files"}
+    which = set(sys.argv[1:]) or {"assembly", "gauss", "hess", "precond", "shot", "files"}
     if "assembly" in which:
         assembly_fixtures(out)
     if "gauss" in which:
@@ -43,6 +44,8 @@ def main():
         apply_hess_fixture(out)
     if "precond" in which:
         precond_fixture(out)
+    if "shot" in which:
+        shot_taper_fixture(out)
     if "files" in which:
         files_fixture(out)
 
@@ -119,6 +122,35 @@ def apply_hess_fixture(out):
                   f"max_{k}": np.float32(mx)})
     np.savez_compressed(os.path.join(out, "postproc_apply_hess.npz"), **d)
     print("wrote postproc_apply_hess")
+
+
+# per-shot taper cases: grid nx, ny, dh, SRTRADIUS, FILTSIZE, shots, receivers
+SHOT_TAPER_CASES = [(61, 47, 12.5, 40.0, 1, 4, 9), (48, 40, 0.05, 0.18, 2, 3, 6), (35, 30, 10.0, 80.0, 0, 2, 5)]
+
+
+def shot_taper_fixture(out):
+    """postproc_shot_taper.npz: seeded one-shot gradients, interior source
+    coordinates (metres, off the grid nodes) and receiver indices kept
+    FILTSIZE + 1 points inside the grid, and the reference's taper_grad_shot
+    of every shot (rad_k [ns][NY*NX]) and taper_grad_shot1 (sq_k);
+    case_k = (nx, ny, dh, SRTRADIUS, FILTSIZE)."""
+    rng = np.random.default_rng(23)
+    d = {"ncases": len(SHOT_TAPER_CASES)}
+    for k, (nx, ny, dh, radius, fs, ns, ntr) in enumerate(SHOT_TAPER_CASES):
+        g = O.Grid(nx=nx, ny=ny, dh=dh, npml=4)
+        grad = rng.standard_normal(ny * nx).astype(np.float32)
+        lo = fs + 2
+        sx = (rng.uniform(lo, nx - lo, ns) * dh).astype(np.float32)
+        sy = (rng.uniform(lo, ny - lo, ns) * dh).astype(np.float32)
+        rx = rng.integers(lo, nx - lo, ntr).astype(np.int32)
+        ry = rng.integers(lo, ny - lo, ntr).astype(np.int32)
+        ref = O.Ref(g)
+        rad = np.stack([ref.taper_grad_shot(grad, radius, sx, sy, rx, ry, s) for s in range(ns)])
+        sq = ref.taper_grad_shot1(grad, fs, sx, sy, rx, ry)
+        d.update({f"case_{k}": np.array([nx, ny, dh, radius, fs]), f"grad_{k}": grad, f"sx_{k}": sx, f"sy_{k}": sy,
+                  f"rx_{k}": rx, f"ry_{k}": ry, f"rad_{k}": rad, f"sq_{k}": sq})
+    np.savez_compressed(os.path.join(out, "postproc_shot_taper.npz"), **d)
+    print("wrote postproc_shot_taper")
 
 
 # precond cases: grid nx, ny, npml, free_surf, SPATFILTER, SWS_TAPER_GRAD_HOR, GRADT2, taper file

@@ -84,7 +84,7 @@ def test_forward_field_layout_matches_reference_vec2mat():
         assert np.array_equal(field[0][s].real, pr) and np.array_equal(field[0][s].imag, pi)
 
 
-def oracle_grad(g, physics, m0, m1, freqs, xs, ys, rx, ry, obs, stf_inv, misfit):
+def oracle_grad(g, physics, m0, m1, freqs, xs, ys, rx, ry, obs, stf_inv, misfit, taper=None):
     X, solvers = oracle_forward(g, physics, m0, m1, freqs, xs, ys)
     idx = [OS.receiver_read_index(g, int(a), int(b)) for a, b in zip(rx, ry)]
     kadj = [OS.adjoint_index(g, int(a), int(b)) for a, b in zip(rx, ry)]
@@ -102,7 +102,7 @@ def oracle_grad(g, physics, m0, m1, freqs, xs, ys, rx, ry, obs, stf_inv, misfit)
             for t, k in enumerate(kadj):
                 Badj[k, s] = np.conj(res[t]) / dh2
         Xa[i] = solvers[i].solve(Badj, trans=(physics == GM_PHYS_TE))
-    g0, g1 = OS.gradient_fp64(g, physics, freqs, X, Xa, stfu, vp=m0, rho=m1)
+    g0, g1 = OS.gradient_fp64(g, physics, freqs, X, Xa, stfu, vp=m0, rho=m1, taper=taper)
     return g0, g1, 0.5 * l2
 
 
@@ -139,6 +139,42 @@ def test_gradient_matches_fp64_oracle(physics, stf_inv, misfit):
         assert _rel(g1, r1) < 1e-8
         assert _rel(g1f, r1) < 2e-6
     assert abs(l2 - rl2) / rl2 < 2e-6 and abs(l2o - rl2) / rl2 < 2e-6
+
+
+@pytest.mark.parametrize("physics", [GM_PHYS_AC, GM_PHYS_TE], ids=["ac", "te"])
+@pytest.mark.parametrize("mode", [1, 2], ids=["radial", "squares"])
+def test_gradient_shot_taper(physics, mode):
+    """SWS_TAPER_CIRCULAR_PER_SHOT = 1 (taper_grad_shot) and 2
+    (taper_grad_shot1) applied per shot inside the gradient stack, against
+    the FP64 oracle with the same per-shot coefficients; the tapered points
+    are checked on their own (the squares' 1e-5 is small against the
+    gradient), the others are the untapered gradient."""
+    g, m0, m1, freqs, xs, ys, rx, ry = _case(physics, seed=3)
+    obs = _observed(g, physics, m0, m1, freqs, xs, ys, rx, ry)
+    radius, filtsize = float(np.float32(3.5 * g.dh)), 1
+    with Engine(g.nx, g.ny, g.dh, g.npml, physics=physics, leaf_max=32) as e:
+        e.set_model(m0, m1)
+        e.factor(freqs)
+        e.set_shot_taper(mode, radius, filtsize)
+        e.grad_obj(xs, ys, rx, ry, obs)
+        t0, t1 = e.gradient_fp64()
+        e.set_shot_taper(0)
+        e.grad_obj(xs, ys, rx, ry, obs)
+        u0, u1 = e.gradient_fp64()
+        with pytest.raises(GmError):
+            e.set_shot_taper(3)
+        with pytest.raises(GmError):
+            e.set_shot_taper(1, 0.0)
+    taper = OS.shot_taper(g, mode, xs, ys, rx, ry, radius, filtsize)
+    r0, r1, _ = oracle_grad(g, physics, m0, m1, freqs, xs, ys, rx, ry, obs, 0, 1, taper=taper)
+    touched = np.any(taper[1] != 1.0, axis=0) if mode == 1 else taper[1]
+    assert 0 < touched.sum() < g.n
+    pairs = [(t0, u0, r0)] + ([(t1, u1, r1)] if physics == GM_PHYS_TE else [])
+    for t, u, r in pairs:
+        assert _rel(t, r) < 1e-8
+        assert _rel(t[touched], r[touched]) < 1e-8
+        assert _rel(t[~touched], u[~touched]) < 1e-12
+        assert _rel(u[touched], t[touched]) > 1e-3       # the taper changed those points
 
 
 def test_gradient_mixed_precision_within_1e6():

@@ -259,3 +259,83 @@ def test_port_precond_equals_reference(short_tmp):
         a = O.Port(g).precond(grad, **kw)
         b = O.Ref(g).precond(short_tmp, grad, **kw)
         assert np.array_equal(_bits(a), _bits(b))
+
+
+# ---- per-shot gradient tapers (src/taper_grad_shot.c, src/taper_grad_shot1.c) ----
+def shot_taper_cases():
+    d = np.load(os.path.join(GOLDEN, "postproc_shot_taper.npz"))
+    out = []
+    for k in range(int(d["ncases"])):
+        nx, ny, dh, radius, fs = d[f"case_{k}"]
+        out.append((int(nx), int(ny), float(np.float32(dh)), float(np.float32(radius)), int(fs), d[f"grad_{k}"],
+                    d[f"sx_{k}"], d[f"sy_{k}"], d[f"rx_{k}"], d[f"ry_{k}"], d[f"rad_{k}"], d[f"sq_{k}"]))
+    return out
+
+
+def test_shot_tapers_against_golden():
+    """taper_grad_shot for every shot and taper_grad_shot1: the restatement
+    (oracle/port.c) and the product's host drop-ins (gm_taper_grad_shot,
+    gm_taper_grad_shot1) are bit-identical to the reference's outputs stored
+    in the fixture."""
+    from germaine_b200 import taper_grad_shot, taper_grad_shot1
+    for nx, ny, dh, radius, fs, grad, sx, sy, rx, ry, rad, sq in shot_taper_cases():
+        g = O.Grid(nx=nx, ny=ny, dh=dh, npml=4)
+        port = O.Port(g)
+        for s in range(len(sx)):
+            assert np.array_equal(_bits(port.taper_grad_shot(grad, radius, sx, sy, rx, ry, s)), _bits(rad[s]))
+            got = taper_grad_shot(grad.reshape(ny, nx), dh, radius, sx, sy, rx, ry, s)
+            assert np.array_equal(_bits(got.ravel()), _bits(rad[s]))
+        assert np.array_equal(_bits(port.taper_grad_shot1(grad, fs, sx, sy, rx, ry)), _bits(sq))
+        got = taper_grad_shot1(grad.reshape(ny, nx), dh, fs, sx, sy, rx, ry)
+        assert np.array_equal(_bits(got.ravel()), _bits(sq))
+        assert np.any(rad != grad[None, :]) and np.any(sq != grad)
+
+
+@needs_ref
+@pytest.mark.parametrize("radius", [25.0, 62.5, 150.0])
+def test_shot_tapers_equal_reference(radius):
+    """Random interior geometries, sources off the grid nodes, overlapping
+    receiver tapers: restatement, product and reference bit-identical."""
+    from germaine_b200 import taper_grad_shot, taper_grad_shot1
+    g = O.Grid(nx=57, ny=43, dh=12.5, npml=6)
+    rng = np.random.default_rng(int(radius))
+    grad = rng.standard_normal(g.n).astype(np.float32)
+    sx = (rng.uniform(4, 53, 3) * g.dh).astype(np.float32)
+    sy = (rng.uniform(4, 39, 3) * g.dh).astype(np.float32)
+    rx = rng.integers(4, 53, 11).astype(np.int32)
+    ry = rng.integers(4, 39, 11).astype(np.int32)
+    ref, port = O.Ref(g), O.Port(g)
+    for s in range(3):
+        want = ref.taper_grad_shot(grad, radius, sx, sy, rx, ry, s)
+        assert np.array_equal(_bits(port.taper_grad_shot(grad, radius, sx, sy, rx, ry, s)), _bits(want))
+        got = taper_grad_shot(grad.reshape(g.ny, g.nx), g.dh, radius, sx, sy, rx, ry, s)
+        assert np.array_equal(_bits(got.ravel()), _bits(want))
+    for fs in (0, 1, 2):
+        want = ref.taper_grad_shot1(grad, fs, sx, sy, rx, ry)
+        assert np.array_equal(_bits(port.taper_grad_shot1(grad, fs, sx, sy, rx, ry)), _bits(want))
+        got = taper_grad_shot1(grad.reshape(g.ny, g.nx), g.dh, fs, sx, sy, rx, ry)
+        assert np.array_equal(_bits(got.ravel()), _bits(want))
+
+
+def test_shot_taper_squares_clipped_at_the_edge():
+    """Squares that cross the grid edge (where the reference writes past its
+    arrays) are clipped: restatement and product agree, nothing outside the
+    grid is touched."""
+    from germaine_b200 import GmError, taper_grad_shot1
+    g = O.Grid(nx=20, ny=16, dh=5.0, npml=3)
+    grad = np.arange(g.n, dtype=np.float32) + 1
+    sx = np.array([0.0, 97.0], np.float32)
+    sy = np.array([2.0, 78.0], np.float32)
+    rx = np.array([1, 20], np.int32)
+    ry = np.array([16, 1], np.int32)
+    a = O.Port(g).taper_grad_shot1(grad, 2, sx, sy, rx, ry)
+    b = taper_grad_shot1(grad.reshape(g.ny, g.nx), g.dh, 2, sx, sy, rx, ry).ravel()
+    assert np.array_equal(_bits(a), _bits(b))
+    assert np.count_nonzero(b == np.float32(1e-5)) > 0
+    with pytest.raises(GmError):
+        taper_grad_shot1(grad.reshape(g.ny, g.nx), g.dh, -1, sx, sy, rx, ry)
+    from germaine_b200 import taper_grad_shot
+    with pytest.raises(GmError):      # shot index out of range
+        taper_grad_shot(grad.reshape(g.ny, g.nx), g.dh, 10.0, sx, sy, rx, ry, 2)
+    with pytest.raises(GmError):      # radius must be positive
+        taper_grad_shot(grad.reshape(g.ny, g.nx), g.dh, 0.0, sx, sy, rx, ry, 0)
