@@ -292,7 +292,8 @@ def run_gpu(args):
     head = results[head_name]
     value = units / (head["ms"] * 1e-3)
     st = head["stats"]
-    # roofline of the backward substitution pass (K5 k_bwd_ring + k_bwd_piv,
+    # roofline of the backward substitution pass (K5 k_bwd_small on the
+    # fronts with at most 32 pivots, k_bwd_ring + k_bwd_piv above them;
     # the dense part of every solve: the forward pass is pruned to the
     # fronts on the paths from the sources to the root): the stored U
     # entries read once + the right-hand sides read (y, ancestors' x) and the
@@ -341,7 +342,7 @@ def run_gpu(args):
                       "gpu_launches_per_step": results[n]["launches"]}
                   for n in ("fp64", "mixed")},
         "mixed_over_fp64": fp64["ms"] / mixed["ms"],
-        "roofline": {"kernel": "K5 backward substitution (k_bwd_ring + k_bwd_piv, %s)" % ("complex128" if csize == 16 else "complex64"),
+        "roofline": {"kernel": "K5 backward substitution (k_bwd_small, k_bwd_ring + k_bwd_piv, %s)" % ("complex128" if csize == 16 else "complex64"),
                      "bound": "hbm", "achieved": achieved, "peak": peak_hbm, "unit": "GB/s",
                      "frac": achieved / peak_hbm, "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": subst_bytes, "ms_per_launch_group": subst_ms},
