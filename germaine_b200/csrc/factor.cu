@@ -16,6 +16,15 @@
 // that each NB x NB diagonal block holds the INVERSES of its two triangles
 // (what the substitution multiplies by) -- and its Schur complement (the
 // contribution block) in the trailing block.
+//
+// Two fused kernels leave the same layout on the levels where they pay:
+//   k_factor_small  fronts that fit shared memory whole (the lower levels):
+//                   extend-add, entries, LU and Schur complement in one CTA;
+//   k_factor_mid    fronts with at most NB pivots and at most 256 rows above
+//                   those: after K2, one CTA factorises the pivot columns
+//                   and applies the Schur update to the contribution block
+//                   once, in place of K3 / K4 and the contribution GEMM.
+// The remaining (upper) levels take the blocked K2-K4 sequence.
 #include "kernels.cuh"
 #include "cplx.cuh"
 
