@@ -11,7 +11,7 @@ formats (``files``).
 """
 from .engine import (GM_OP_EXACT, GM_OP_REF, GM_PHYS_AC, GM_PHYS_SH, GM_PHYS_TE, GM_PREC_C64_IR,  # noqa: F401
                      GM_PREC_FP64, GM_SYS_A, GM_SYS_AT, Engine, Lbfgs, apply_hess, gauss_filt, mat_change, precond,
-                     nonzero, taper_grad_shot, taper_grad_shot1)
+                     nonzero, taper_grad_shot, taper_grad_shot1, tikhonov_cost_te, tikhonov_grad_te)
 from ._lib import GM_HESS_GREEN, GM_HESS_SHIN  # noqa: F401
 from ._lib import GmError  # noqa: F401
 from . import files  # noqa: F401

@@ -62,7 +62,7 @@ EXPORTS = [
     "gm_get_gradient_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_hessian", "gm_get_hessian_fp64", "gm_apply_hess", "gm_precond",
     "gm_lbfgs_create", "gm_lbfgs_destroy", "gm_lbfgs_step", "gm_lbfgs_rotate", "gm_lbfgs_zero",
     "gm_lbfgs_check_descent", "gm_lbfgs_get_old", "gm_lbfgs_set_old", "gm_mat_change",
-    "gm_set_shot_taper", "gm_taper_grad_shot", "gm_taper_grad_shot1",
+    "gm_set_shot_taper", "gm_taper_grad_shot", "gm_taper_grad_shot1", "gm_tikhonov_cost_te", "gm_tikhonov_grad_te",
     "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_read_grid", "gm_cgemm_sub_c64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
@@ -133,6 +133,8 @@ def load() -> ctypes.CDLL:
     lib.gm_set_shot_taper.argtypes = [vp, i32, f32, i32]
     lib.gm_taper_grad_shot.argtypes = [i32, i32, f32, f32, i32, vp, vp, i32, vp, vp, i32, vp]
     lib.gm_taper_grad_shot1.argtypes = [i32, i32, f32, i32, i32, vp, vp, i32, vp, vp, vp]
+    lib.gm_tikhonov_cost_te.argtypes = [i32, i32, i32, i32, f32, f32, f32, f32, f32, f32, f32, vp, vp, f32, vp]
+    lib.gm_tikhonov_grad_te.argtypes = [i32, i32, i32, i32, f32, f32, f32, f32, f32, f32, f32, vp, vp, vp, vp]
     cp = ctypes.c_char_p
     lib.gm_write_seis.argtypes = [cp, i32, i32, i32, i32, vp]
     lib.gm_read_seis.argtypes = [cp, i32, i32, i32, vp]

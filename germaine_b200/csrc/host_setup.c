@@ -333,3 +333,69 @@ void gmh_srt_receiver_product(int nx, int ny, float dh, float radius, int ntr, c
                 prod[(size_t)(iy - 1) * nx + ix - 1] *= (double)gmh_srt_coef(ix, iy, dh, xc, yc, radius);
     }
 }
+
+/* ---------------------------------------------------------------------
+ * Tikhonov regularisation of TE FWI on the normalised models
+ * s = (BETA_MAT1 / MAT1_NORM) sigma and e = (BETA_MAT2 / MAT2_NORM) epsilon
+ * (scale_grad, src/scale_grad.c:10-24): the five-point Laplacian
+ * L(m) = (W + E + N + S - 4 C) / DH^2 at every IDX-th column and IDY-th row
+ * of the points 2 .. NX-1, 2 .. NY-1 (src/TE/Tikhonov_cost_TE.c:27-38,
+ * src/TE/Tikhonov_grad_TE.c:27-36).  The neighbour sum is float, the centre
+ * term double (the 4.0 literal), DH^2 a float product, the quotient stored
+ * as float; the penalty sums 0.5 BETA L^2 in double per point into a float.
+ * Grids are row-major [NY][NX]; (i, j) 1-based.
+ * --------------------------------------------------------------------- */
+static float tikh_laplace(const float *m, int nx, int i, int j, float dh)
+{
+#define M(jj, ii) m[(size_t)((jj) - 1) * nx + (ii) - 1]
+    return (M(j, i - 1) + M(j, i + 1) + M(j - 1, i) + M(j + 1, i) - 4.0 * M(j, i)) / (dh * dh);
+#undef M
+}
+
+static void tikh_normalise(const float *m, float beta, float norm, int n, float *out)
+{
+    const float a = beta / norm;
+    int k;
+    for (k = 0; k < n; k++) out[k] = a * m[k];
+}
+
+/* Tikhonov_cost_TE: returns L2 + LAMBDA_1 tikh_sigma + LAMBDA_2 tikh_epsilon
+ * (L2 itself when both LAMBDAs are <= 0); work holds 2 NX NY floats */
+float gmh_tikhonov_cost_te(int nx, int ny, int idx, int idy, float dh, float norm1, float norm2, float beta1,
+                           float beta2, float lambda1, float lambda2, const float *sigma, const float *epsilon,
+                           float l2, float *work)
+{
+    float *sr = work, *er = work + (size_t)nx * ny, ls, le, ts = 0.0, te = 0.0;
+    int i, j;
+    tikh_normalise(sigma, beta1, norm1, nx * ny, sr);
+    tikh_normalise(epsilon, beta2, norm2, nx * ny, er);
+    for (i = 2; i <= nx - 1; i = i + idx)
+        for (j = 2; j <= ny - 1; j = j + idy) {
+            ls = tikh_laplace(sr, nx, i, j, dh);
+            le = tikh_laplace(er, nx, i, j, dh);
+            ts += 0.5 * beta1 * ls * ls;
+            te += 0.5 * beta2 * le * le;
+        }
+    if ((lambda1 > 0.0) || (lambda2 > 0.0)) return l2 + lambda1 * ts + lambda2 * te;
+    return l2;
+}
+
+/* Tikhonov_grad_TE: grad_sigma += LAMBDA_1 BETA_MAT1 L(s), grad_epsilon +=
+ * LAMBDA_2 BETA_MAT2 L(e) (float), when either LAMBDA is > 0 */
+void gmh_tikhonov_grad_te(int nx, int ny, int idx, int idy, float dh, float norm1, float norm2, float beta1,
+                          float beta2, float lambda1, float lambda2, const float *sigma, const float *epsilon,
+                          float *grad_sigma, float *grad_epsilon, float *work)
+{
+    float *sr = work, *er = work + (size_t)nx * ny, ls, le;
+    int i, j;
+    if (!((lambda1 > 0.0) || (lambda2 > 0.0))) return;
+    tikh_normalise(sigma, beta1, norm1, nx * ny, sr);
+    tikh_normalise(epsilon, beta2, norm2, nx * ny, er);
+    for (i = 2; i <= nx - 1; i = i + idx)
+        for (j = 2; j <= ny - 1; j = j + idy) {
+            ls = tikh_laplace(sr, nx, i, j, dh);
+            le = tikh_laplace(er, nx, i, j, dh);
+            grad_sigma[(size_t)(j - 1) * nx + i - 1] += lambda1 * beta1 * ls;
+            grad_epsilon[(size_t)(j - 1) * nx + i - 1] += lambda2 * beta2 * le;
+        }
+}

@@ -21,6 +21,12 @@ void gmh_taper_grad_shot(int nx, int ny, float dh, float radius, const float *sx
                          const int *rx, const int *ry, int ishot, float *grid);
 void gmh_taper_grad_shot1(int nx, int ny, float dh, int filtsize, int nshots, const float *sx, const float *sy,
                           int ntr, const int *rx, const int *ry, float *grid, unsigned char *mark);
+float gmh_tikhonov_cost_te(int nx, int ny, int idx, int idy, float dh, float norm1, float norm2, float beta1,
+                           float beta2, float lambda1, float lambda2, const float *sigma, const float *epsilon,
+                           float l2, float *work);
+void gmh_tikhonov_grad_te(int nx, int ny, int idx, int idy, float dh, float norm1, float norm2, float beta1,
+                          float beta2, float lambda1, float lambda2, const float *sigma, const float *epsilon,
+                          float *grad_sigma, float *grad_epsilon, float *work);
 void gmh_srt_receiver_product(int nx, int ny, float dh, float radius, int ntr, const int *rx, const int *ry,
                               double *prod);
 #ifdef __cplusplus

@@ -352,6 +352,34 @@ def taper_grad_shot1(grad, dh: float, filtsize: int, src_x, src_y, rec_x, rec_y)
     return g
 
 
+def tikhonov_cost_te(sigma, epsilon, l2: float, dh: float, mat1_norm: float, mat2_norm: float, beta_mat1: float,
+                     beta_mat2: float, lambda_1: float, lambda_2: float, idx: int = 1, idy: int = 1) -> float:
+    """Tikhonov_cost_TE (host, bit-identical): the misfit plus the Laplacian
+    penalty of the normalised [NY][NX] sigma and epsilon models."""
+    s = _c(sigma, np.float32)
+    e = _c(epsilon, np.float32)
+    ny, nx = np.shape(sigma)
+    out = ctypes.c_float(0.0)
+    check(_lib.load().gm_tikhonov_cost_te(nx, ny, idx, idy, dh, mat1_norm, mat2_norm, beta_mat1, beta_mat2, lambda_1,
+                                          lambda_2, ptr(s), ptr(e), l2, ctypes.byref(out)))
+    return float(out.value)
+
+
+def tikhonov_grad_te(grad_sigma, grad_epsilon, sigma, epsilon, dh: float, mat1_norm: float, mat2_norm: float,
+                     beta_mat1: float, beta_mat2: float, lambda_1: float, lambda_2: float, idx: int = 1,
+                     idy: int = 1):
+    """Tikhonov_grad_TE (host, bit-identical): returns the regularised
+    copies of the two [NY][NX] TE gradients."""
+    gs = np.array(grad_sigma, np.float32, copy=True, order="C")
+    ge = np.array(grad_epsilon, np.float32, copy=True, order="C")
+    s = _c(sigma, np.float32)
+    e = _c(epsilon, np.float32)
+    ny, nx = gs.shape
+    check(_lib.load().gm_tikhonov_grad_te(nx, ny, idx, idy, dh, mat1_norm, mat2_norm, beta_mat1, beta_mat2, lambda_1,
+                                          lambda_2, ptr(s), ptr(e), ptr(gs), ptr(ge)))
+    return gs, ge
+
+
 def precond(grad, npml: int, free_surf: int, dh: float, spatfilter: int = 0, vref: float = 0.0,
             fc_low: float = 1.0, filt_size_grad: float = 0.0, filt_size_grad1: float = 0.0, taper_hor: int = 0,
             gradt2: int = 0, taper=None, device: int = 0) -> np.ndarray:

@@ -350,6 +350,25 @@ int gm_taper_grad_shot(int nx, int ny, float dh, float srtradius, int nshots, co
 int gm_taper_grad_shot1(int nx, int ny, float dh, int filtsize, int nshots, const float *src_x,
                         const float *src_y, int ntr, const int32_t *rec_x, const int32_t *rec_y, float *grad);
 
+/* Host drop-ins for the TE inversion's Tikhonov regularisation on the
+ * normalised models (BETA_MAT1 / MAT1_NORM) sigma and (BETA_MAT2 /
+ * MAT2_NORM) epsilon, [NY][NX] with the PML frame, float results identical
+ * to the reference's:
+ *   gm_tikhonov_cost_te  Tikhonov_cost_TE (src/TE/Tikhonov_cost_TE.c:10):
+ *                        *l2_out = l2 + LAMBDA_1 * sum 0.5 BETA_MAT1 L(s)^2
+ *                        + LAMBDA_2 * sum 0.5 BETA_MAT2 L(e)^2 (l2 when
+ *                        both LAMBDAs are <= 0), L the five-point Laplacian
+ *                        at every IDX-th / IDY-th interior point;
+ *   gm_tikhonov_grad_te  Tikhonov_grad_TE (src/TE/Tikhonov_grad_TE.c:10):
+ *                        grad_sigma += LAMBDA_1 BETA_MAT1 L(s),
+ *                        grad_epsilon += LAMBDA_2 BETA_MAT2 L(e). */
+int gm_tikhonov_cost_te(int nx, int ny, int idx, int idy, float dh, float mat1_norm, float mat2_norm,
+                        float beta_mat1, float beta_mat2, float lambda_1, float lambda_2,
+                        const float *sigma, const float *epsilon, float l2, float *l2_out);
+int gm_tikhonov_grad_te(int nx, int ny, int idx, int idy, float dh, float mat1_norm, float mat2_norm,
+                        float beta_mat1, float beta_mat2, float lambda_1, float lambda_2,
+                        const float *sigma, const float *epsilon, float *grad_sigma, float *grad_epsilon);
+
 /* ---- the reference's file formats (host stdio, no GPU needed) ---- */
 #define GM_SEIS_KEEP_LAST 1  /* gm_write_seis: write the last sample as given */
 

@@ -159,6 +159,11 @@ def load_ref():
                                             ctypes.c_int, _f32p]
         lib.ref_taper_grad_shot1.argtypes = [ctypes.c_int, ctypes.c_int, _f32p, _f32p, ctypes.c_int, _i32p, _i32p,
                                              _f32p]
+        f_ = ctypes.c_float
+        lib.ref_tikhonov_cost_te.restype = f_
+        lib.ref_tikhonov_cost_te.argtypes = [ctypes.c_int, ctypes.c_int, f_, f_, f_, f_, f_, f_, _f32p, _f32p, f_]
+        lib.ref_tikhonov_grad_te.argtypes = [ctypes.c_int, ctypes.c_int, f_, f_, f_, f_, f_, f_, _f32p, _f32p, _f32p,
+                                             _f32p]
         lib.ref_apply_hess.restype = ctypes.c_float
         fp = _f32p
         lib.ref_lbfgs_ac.argtypes = [i, i, i, fp, fp, fp, fp, fp, fp, fp, fp, fp, fp, cp, fp]
@@ -410,6 +415,18 @@ class Ref:
         self.lib.ref_taper_grad_shot(radius, len(sx), _f32(sx), _f32(sy), len(rx), np.asarray(rx, np.int32),
                                      np.asarray(ry, np.int32), ishot, out)
         return out
+
+    def tikhonov_cost_te(self, sigma, epsilon, l2, norm1, norm2, beta1, beta2, lambda1, lambda2, idx=1, idy=1):
+        return float(self.lib.ref_tikhonov_cost_te(idx, idy, norm1, norm2, beta1, beta2, lambda1, lambda2,
+                                                   _f32(sigma).ravel(), _f32(epsilon).ravel(), l2))
+
+    def tikhonov_grad_te(self, gsig, geps, sigma, epsilon, norm1, norm2, beta1, beta2, lambda1, lambda2, idx=1,
+                         idy=1):
+        gs = _f32(gsig).ravel().copy()
+        ge = _f32(geps).ravel().copy()
+        self.lib.ref_tikhonov_grad_te(idx, idy, norm1, norm2, beta1, beta2, lambda1, lambda2, _f32(sigma).ravel(),
+                                      _f32(epsilon).ravel(), gs, ge)
+        return gs, ge
 
     def taper_grad_shot1(self, grad, filtsize, sx, sy, rx, ry):
         out = _f32(grad).copy()

@@ -39,6 +39,8 @@
  *   precond              src/precond.c:10   (+ taper_grad_hor, taper_grad_file)
  *   taper_grad_shot      src/taper_grad_shot.c:11
  *   taper_grad_shot1     src/taper_grad_shot1.c:11
+ *   Tikhonov_cost_TE     src/TE/Tikhonov_cost_TE.c:10
+ *   Tikhonov_grad_TE     src/TE/Tikhonov_grad_TE.c:10
  */
 #include <unistd.h>
 
@@ -497,4 +499,45 @@ void ref_taper_grad_shot1(int filtsize, int nshots, const float *sx, const float
     free_matrix(g, 0, NY + 1, 0, NX + 1);
     free_matrix(sp, 1, 8, 1, nshots);
     free_imatrix(rp, 1, 3, 1, ntr);
+}
+
+/* Tikhonov_cost_TE / Tikhonov_grad_TE on flat [NY][NX] models and TE
+ * gradients (the latter in place) */
+static void set_tikhonov(int idx, int idy, float norm1, float norm2, float beta1, float beta2, float lambda1,
+                         float lambda2)
+{
+    extern float MAT1_NORM, MAT2_NORM, BETA_MAT1, BETA_MAT2, LAMBDA_1, LAMBDA_2;
+    IDX = idx; IDY = idy;
+    MAT1_NORM = norm1; MAT2_NORM = norm2; BETA_MAT1 = beta1; BETA_MAT2 = beta2;
+    LAMBDA_1 = lambda1; LAMBDA_2 = lambda2;
+}
+
+float ref_tikhonov_cost_te(int idx, int idy, float norm1, float norm2, float beta1, float beta2, float lambda1,
+                           float lambda2, const float *sigma, const float *epsilon, float l2)
+{
+    struct matTE m; struct fwiTE f;
+    float out;
+    set_tikhonov(idx, idy, norm1, norm2, beta1, beta2, lambda1, lambda2);
+    m.sigma = to_nr(sigma); m.epsilon = to_nr(epsilon);
+    m.sigmar = matrix(1, NY, 1, NX); m.epsilonr = matrix(1, NY, 1, NX);
+    out = Tikhonov_cost_TE(&f, &m, l2, 1);
+    free_matrix(m.sigma, 0, NY + 1, 0, NX + 1); free_matrix(m.epsilon, 0, NY + 1, 0, NX + 1);
+    free_matrix(m.sigmar, 1, NY, 1, NX); free_matrix(m.epsilonr, 1, NY, 1, NX);
+    return out;
+}
+
+void ref_tikhonov_grad_te(int idx, int idy, float norm1, float norm2, float beta1, float beta2, float lambda1,
+                          float lambda2, const float *sigma, const float *epsilon, float *grad_sigma,
+                          float *grad_epsilon)
+{
+    struct matTE m; struct fwiTE f;
+    set_tikhonov(idx, idy, norm1, norm2, beta1, beta2, lambda1, lambda2);
+    m.sigma = to_nr(sigma); m.epsilon = to_nr(epsilon);
+    m.sigmar = matrix(1, NY, 1, NX); m.epsilonr = matrix(1, NY, 1, NX);
+    f.grad_sigma = to_nr(grad_sigma); f.grad_epsilon = to_nr(grad_epsilon);
+    Tikhonov_grad_TE(&f, &m, 1);
+    from_nr(f.grad_sigma, grad_sigma); from_nr(f.grad_epsilon, grad_epsilon);
+    free_matrix(m.sigma, 0, NY + 1, 0, NX + 1); free_matrix(m.epsilon, 0, NY + 1, 0, NX + 1);
+    free_matrix(m.sigmar, 1, NY, 1, NX); free_matrix(m.epsilonr, 1, NY, 1, NX);
+    free_matrix(f.grad_sigma, 0, NY + 1, 0, NX + 1); free_matrix(f.grad_epsilon, 0, NY + 1, 0, NX + 1);
 }

@@ -6,9 +6,10 @@ cases, a right-hand side with its FP64 sparse solution on the operator
 UMFPACK factorises (M = A^T; solved with SciPy SuperLU because UMFPACK is
 not part of the reference tree); postproc_gauss_filt.npz holds gauss_filt
 cases, postproc_apply_hess.npz apply_hess_AC cases, postproc_shot_taper.npz
-taper_grad_shot / taper_grad_shot1 cases and files_formats.npz the bytes
+taper_grad_shot / taper_grad_shot1 cases, postproc_tikhonov_te.npz
+Tikhonov_cost_TE / Tikhonov_grad_TE cases and files_formats.npz the bytes
 of the reference's seismogram and model files.
-Run:  python tests/golden/make_golden.py [assembly] [gauss] [hess] [precond] [shot] [files]
+Run:  python tests/golden/make_golden.py [assembly] [gauss] [hess] [precond] [shot] [tikh] [files]
 (no argument: all).
 """
 import tempfile
@@ -35,7 +36,7 @@ CASES = [
 
 def main():
     out = os.path.dirname(os.path.abspath(__file__))
-    which = set(sys.argv[1:]) or {"assembly", "gauss", "hess", "precond", "shot", "files"}
+    which = set(sys.argv[1:]) or {"assembly", "gauss", "hess", "precond", "shot", "tikh", "files"}
     if "assembly" in which:
         assembly_fixtures(out)
     if "gauss" in which:
@@ -46,6 +47,8 @@ def main():
         precond_fixture(out)
     if "shot" in which:
         shot_taper_fixture(out)
+    if "tikh" in which:
+        tikhonov_fixture(out)
     if "files" in which:
         files_fixture(out)
 
@@ -151,6 +154,36 @@ def shot_taper_fixture(out):
                   f"rx_{k}": rx, f"ry_{k}": ry, f"rad_{k}": rad, f"sq_{k}": sq})
     np.savez_compressed(os.path.join(out, "postproc_shot_taper.npz"), **d)
     print("wrote postproc_shot_taper")
+
+
+# Tikhonov cases: grid nx, ny, dh, IDX, IDY, MAT1_NORM, MAT2_NORM, BETA_MAT1, BETA_MAT2, LAMBDA_1, LAMBDA_2
+TIKH_CASES = [(37, 29, 0.05, 1, 1, 0.01, 8.85e-11, 1.0, 1.0, 0.3, 0.7),
+              (40, 33, 0.025, 2, 3, 0.005, 1.77e-10, 0.5, 2.0, 1e-3, 0.0),
+              (21, 18, 0.1, 1, 1, 0.01, 8.85e-11, 1.0, 1.0, 0.0, 0.0)]
+
+
+def tikhonov_fixture(out):
+    """postproc_tikhonov_te.npz: seeded TE models (sigma in S/m, absolute
+    epsilon) and gradients with the reference's Tikhonov_cost_TE of a misfit
+    (cost_k) and Tikhonov_grad_TE (gs_k, ge_k); case_k = (nx, ny, dh, IDX,
+    IDY, MAT1_NORM, MAT2_NORM, BETA_MAT1, BETA_MAT2, LAMBDA_1, LAMBDA_2, L2)."""
+    rng = np.random.default_rng(29)
+    d = {"ncases": len(TIKH_CASES)}
+    for k, (nx, ny, dh, idx, idy, n1, n2, b1, b2, l1, l2) in enumerate(TIKH_CASES):
+        g = O.Grid(nx=nx, ny=ny, dh=dh, npml=4)
+        sig = rng.uniform(1e-4, 1e-2, (ny, nx)).astype(np.float32)
+        eps = (rng.uniform(3, 25, (ny, nx)) * 8.8541878e-12).astype(np.float32)
+        gsig = rng.standard_normal((ny, nx)).astype(np.float32)
+        geps = rng.standard_normal((ny, nx)).astype(np.float32)
+        misfit = np.float32(rng.uniform(1, 100))
+        ref = O.Ref(g)
+        cost = ref.tikhonov_cost_te(sig, eps, misfit, n1, n2, b1, b2, l1, l2, idx, idy)
+        gs, ge = ref.tikhonov_grad_te(gsig, geps, sig, eps, n1, n2, b1, b2, l1, l2, idx, idy)
+        d.update({f"case_{k}": np.array([nx, ny, dh, idx, idy, n1, n2, b1, b2, l1, l2, misfit]), f"sig_{k}": sig,
+                  f"eps_{k}": eps, f"gsig_{k}": gsig, f"geps_{k}": geps, f"cost_{k}": np.float32(cost),
+                  f"gs_{k}": gs, f"ge_{k}": ge})
+    np.savez_compressed(os.path.join(out, "postproc_tikhonov_te.npz"), **d)
+    print("wrote postproc_tikhonov_te")
 
 
 # precond cases: grid nx, ny, npml, free_surf, SPATFILTER, SWS_TAPER_GRAD_HOR, GRADT2, taper file

@@ -339,3 +339,51 @@ def test_shot_taper_squares_clipped_at_the_edge():
         taper_grad_shot(grad.reshape(g.ny, g.nx), g.dh, 10.0, sx, sy, rx, ry, 2)
     with pytest.raises(GmError):      # radius must be positive
         taper_grad_shot(grad.reshape(g.ny, g.nx), g.dh, 0.0, sx, sy, rx, ry, 0)
+
+
+# ---- Tikhonov regularisation of TE FWI (src/TE/Tikhonov_cost_TE.c, Tikhonov_grad_TE.c) ----
+def tikhonov_cases():
+    d = np.load(os.path.join(GOLDEN, "postproc_tikhonov_te.npz"))
+    out = []
+    for k in range(int(d["ncases"])):
+        c = d[f"case_{k}"]
+        nx, ny, idx, idy = int(c[0]), int(c[1]), int(c[3]), int(c[4])
+        dh, n1, n2, b1, b2, l1, l2, misfit = (float(np.float32(v)) for v in (c[2], *c[5:12]))
+        out.append((nx, ny, dh, idx, idy, n1, n2, b1, b2, l1, l2, misfit, d[f"sig_{k}"], d[f"eps_{k}"],
+                    d[f"gsig_{k}"], d[f"geps_{k}"], float(d[f"cost_{k}"]), d[f"gs_{k}"], d[f"ge_{k}"]))
+    return out
+
+
+def test_tikhonov_te_against_golden():
+    """gm_tikhonov_cost_te / gm_tikhonov_grad_te bit-identical to the
+    reference's outputs stored in the fixture (IDX/IDY subsampling, one
+    LAMBDA zero, both zero)."""
+    from germaine_b200 import tikhonov_cost_te, tikhonov_grad_te
+    for (nx, ny, dh, idx, idy, n1, n2, b1, b2, l1, l2, misfit, sig, eps, gsig, geps, cost, gs,
+         ge) in tikhonov_cases():
+        got = tikhonov_cost_te(sig, eps, misfit, dh, n1, n2, b1, b2, l1, l2, idx, idy)
+        assert np.float32(got).view(np.uint32) == np.float32(cost).view(np.uint32)
+        a, b = tikhonov_grad_te(gsig, geps, sig, eps, dh, n1, n2, b1, b2, l1, l2, idx, idy)
+        assert np.array_equal(_bits(a.ravel()), _bits(gs)) and np.array_equal(_bits(b.ravel()), _bits(ge))
+
+
+@needs_ref
+@pytest.mark.parametrize("idx,idy,lam", [(1, 1, (0.2, 0.9)), (3, 2, (0.0, 5e-4)), (1, 4, (2.0, 0.0))])
+def test_tikhonov_te_equals_reference(idx, idy, lam):
+    from germaine_b200 import GmError, tikhonov_cost_te, tikhonov_grad_te
+    g = O.Grid(nx=45, ny=31, dh=0.04, npml=5)
+    rng = np.random.default_rng(idx * 10 + idy)
+    sig = rng.uniform(1e-4, 2e-2, (g.ny, g.nx)).astype(np.float32)
+    eps = (rng.uniform(2, 30, (g.ny, g.nx)) * 8.8541878e-12).astype(np.float32)
+    gsig = rng.standard_normal((g.ny, g.nx)).astype(np.float32)
+    geps = rng.standard_normal((g.ny, g.nx)).astype(np.float32)
+    args = (0.01, 8.85e-11, 1.0, 0.5, *lam)
+    ref = O.Ref(g)
+    want = ref.tikhonov_cost_te(sig, eps, 12.5, *args, idx, idy)
+    got = tikhonov_cost_te(sig, eps, 12.5, g.dh, *args, idx, idy)
+    assert np.float32(got).view(np.uint32) == np.float32(want).view(np.uint32)
+    ws, we = ref.tikhonov_grad_te(gsig, geps, sig, eps, *args, idx, idy)
+    gs, ge = tikhonov_grad_te(gsig, geps, sig, eps, g.dh, *args, idx, idy)
+    assert np.array_equal(_bits(gs.ravel()), _bits(ws)) and np.array_equal(_bits(ge.ravel()), _bits(we))
+    with pytest.raises(GmError):
+        tikhonov_cost_te(sig, eps, 12.5, g.dh, 0.0, 8.85e-11, 1.0, 0.5, *lam)     # MAT1_NORM = 0
