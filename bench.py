@@ -46,6 +46,7 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 DH, NPML, ROW = 25.0, 20, 2
+RESIDUAL_TARGET = 1e-10
 METRIC = "shot-solves/s (factor+solve) mixed vs FP64 on B200 at resid<=1e-10; %roofline"
 # DRAM bytes of one complex128 backward substitution pass on 4 frequencies
 # (the first k_bwd_ring / k_bwd_piv launches of the FP64 engine, ncu
@@ -220,6 +221,7 @@ def run_gpu(args):
     import torch
 
     from germaine_b200 import GM_PREC_C64_IR, GM_PREC_FP64, Engine
+    from germaine_b200._lib import GM_WARNING_NOT_CONVERGED
 
     rank = int(os.environ.get("RANK", 0))
     world = int(os.environ.get("WORLD_SIZE", 1))
@@ -262,9 +264,18 @@ def run_gpu(args):
         e = Engine(nx, ny, DH, NPML, precision=prec, device=local, leaf_max=args.leaf)
         e.set_model(vp_d, rho_d)
 
+        def check_converged(tag):
+            # every step must meet the residual target: a path that stops
+            # above it (GM_WARNING_NOT_CONVERGED) has no valid number
+            st = e.stats()
+            if e.last_status == GM_WARNING_NOT_CONVERGED or not st["ir_residual"] <= RESIDUAL_TARGET:
+                raise SystemExit(f"bench: {name} path ({tag}) did not reach the residual target: status "
+                                 f"{e.last_status}, max relative residual {st['ir_residual']:.3e}")
+
         def step_dev():
             e.factor(freqs)
             e.forward(xs, ys, rx, ry, seis_out=seis_d)
+            check_converged("device-resident")
 
         clocks = ClockSampler(local)
         clocks.start()
@@ -277,6 +288,7 @@ def run_gpu(args):
             e.set_model(vp_h, rho_h)
             e.factor(freqs)
             e.forward(xs, ys, rx, ry, seis_out=seis_h)
+            check_converged("end-to-end")
         ms_e2e, _ = time_steps(torch, e, step_e2e, max(1, args.steps // 2), 1, dist)
         r["ms_e2e"] = ms_e2e
         results[name] = r

@@ -103,6 +103,7 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
     GM_CUDA(cudaEventCreate(&e->ev_s0));
     GM_CUDA(cudaEventCreate(&e->ev_s1));
     GM_CUDA(cudaEventCreate(&e->ev_sm));
+    if ((rc = gm::noalloc_prepare(device))) return rc;
 
     const gm::Symbolic &s = e->sym;
     // level-ordered entry lists in the configured operator orientation
@@ -551,8 +552,11 @@ extern "C" int gm_get_triplets(gm_engine *e, int ifreq, double *Ar, double *Ai, 
 
 namespace gm {
 
+// One substitution over the right-hand sides in xT; fmap (device, nfz
+// entries) restricts it to those matrices of the batch (NULL: all).
 template <class R>
-static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsigned char *mask = nullptr) {
+static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsigned char *mask = nullptr,
+                       const int *fmap = nullptr, int nfz = 0) {
     cudaEventRecord(e->ev_s0, e->st);
     SolveArgs<R> a{};
     a.s = e->dsym;
@@ -560,6 +564,8 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsign
     a.x = xT;
     a.w = e->d_w.p;
     a.nf = e->nf;
+    a.fmap = fmap;
+    a.nfz = nfz;
     a.nrhs = nrhs;
     a.ldr = nrhs;
     const int nchunk = (nrhs + 31) / 32;
@@ -673,7 +679,11 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     cudaEventElapsedTime(&ms, t0, t1);
     e->stats.ms_solve = ms;
 
-    // refinement: r = b - M' x (FP64), x += M'^{-1} r (working precision)
+    // Refinement, per matrix: r = b - M' x (FP64), x += M'^{-1} r (working
+    // precision), until the matrix's worst right-hand side meets the target.
+    // A matrix that has met it leaves the sweeps: the residual, substitution
+    // and update kernels of the next sweep run over the remaining matrices
+    // only (their list is the launch's fmap).
     ResidArgs ra{};
     ra.nx = e->cfg.nx; ra.ny = e->cfg.ny; ra.n = e->n; ra.nf = e->nf; ra.nrhs = nrhs; ra.ldr = nrhs;
     ra.A = e->d_A.as<double2>(); ra.x = d_x; ra.b = d_b; ra.r = nullptr;
@@ -682,53 +692,79 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
         ra.spike_k = spikes->k;
         ra.spike_amp = spikes->amp;
     }
-    const int cntn = e->nf * nrhs * 2;
-    std::vector<double> norms(cntn);
+    GM_ALLOC(e->d_fmap, 2 * (size_t)e->nf * sizeof(int));
+    int *d_act = e->d_fmap.as<int>();
+    std::vector<int> &act = e->h_fmap;
+    act.resize(e->nf);
+    for (int f = 0; f < e->nf; ++f) act[f] = f;
+    std::vector<double> norms((size_t)e->nf * nrhs * 2);
+    e->refine_info.assign(e->nf, gm_refine_info{0.0, 0.0, 0, GM_REFINE_NONE});
     double worst = 0;
     int it = 0;
     GM_CUDA(cudaEventRecord(t0, e->st));
     for (;; ++it) {
+        const int na = (int)act.size();
+        GM_CUDA(cudaMemcpyAsync(d_act, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, e->st));
+        ra.fmap = d_act;
+        ra.nfz = na;
         // residual straight into the working-precision right-hand side; the
         // first check of FP64 factors normally passes, so it computes the
         // norms only and the residual is formed again if a sweep follows
         void *rhs = (fp64 && it == 0) ? nullptr : e->d_t.p;
         const int nblk = fp64 ? launch_residual_t<double>(ra, rhs, e->d_part.as<double>(), nblk_max, e->st)
                               : launch_residual_t<float>(ra, rhs, e->d_part.as<double>(), nblk_max, e->st);
+        const int cntn = na * nrhs * 2;
         launch_reduce_norms(e->d_part.as<double>(), nblk, cntn, e->d_norm.as<double>(), e->st);
         GM_CUDA(cudaGetLastError());
         GM_CUDA(cudaMemcpyAsync(norms.data(), e->d_norm.p, cntn * sizeof(double), cudaMemcpyDeviceToHost, e->st));
         GM_CUDA(cudaStreamSynchronize(e->st));
-        worst = 0;
         bool finite = true;
-        for (int c = 0; c < e->nf * nrhs; ++c) {
-            const double rr = norms[2 * c], bb = norms[2 * c + 1];
-            if (!std::isfinite(rr)) finite = false;
-            const double rel = bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);
-            worst = std::max(worst, rel);
+        std::vector<int> next;
+        for (int z = 0; z < na; ++z) {
+            const int f = act[z];
+            double wf = 0;
+            for (int r = 0; r < nrhs; ++r) {
+                const double rr = norms[2 * ((size_t)z * nrhs + r)], bb = norms[2 * ((size_t)z * nrhs + r) + 1];
+                if (!std::isfinite(rr)) finite = false;
+                wf = std::max(wf, bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr));
+            }
+            gm_refine_info &ri = e->refine_info[f];
+            if (it == 0) ri.first_residual = wf;
+            ri.final_residual = wf;
+            if (wf > e->cfg.ir_tol) next.push_back(f);
         }
         if (!finite) {
             e->stats.ir_iterations = it;
             e->stats.ir_residual = NAN;
             return fail(GM_ERROR_NONFINITE, "non-finite residual after %d refinement sweeps", it);
         }
+        worst = 0;
+        for (const gm_refine_info &ri : e->refine_info) worst = std::max(worst, ri.final_residual);
         if (std::getenv("GM_TRACE_REFINEMENT")) {
-            std::fprintf(stderr, "refinement sweep %d: max relative residual %.3e; per frequency", it, worst);
-            for (int f = 0; f < e->nf; ++f) {
-                double wf = 0;
-                for (int r = 0; r < nrhs; ++r) {
-                    const double rr = norms[2 * (f * nrhs + r)], bb = norms[2 * (f * nrhs + r) + 1];
-                    wf = std::max(wf, bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr));
-                }
-                std::fprintf(stderr, " %.1e", wf);
-            }
+            std::fprintf(stderr, "refinement sweep %d: max relative residual %.3e; per matrix", it, worst);
+            for (const gm_refine_info &ri : e->refine_info) std::fprintf(stderr, " %.1e", ri.final_residual);
             std::fprintf(stderr, "\n");
         }
-        if (worst <= e->cfg.ir_tol || it >= e->cfg.ir_max_iter) break;
+        if (next.empty() || it >= e->cfg.ir_max_iter) break;
+        // the remaining matrices: their residual is in t (formed again for
+        // the FP64 path, whose first check formed norms only)
+        const int nn = (int)next.size();
+        act.swap(next);
+        GM_CUDA(cudaMemcpyAsync(d_act, act.data(), nn * sizeof(int), cudaMemcpyHostToDevice, e->st));
+        ra.nfz = nn;
         if (!rhs) launch_residual_t<double>(ra, e->d_t.p, e->d_part.as<double>(), nblk_max, e->st);
-        if (fp64) substitute<double>(e, e->d_t.p, nrhs, sys);
-        else substitute<float>(e, e->d_t.p, nrhs, sys);
-        if (fp64) launch_add_up<double>(d_x, e->d_t.p, cnt, e->st);
-        else launch_add_up<float>(d_x, e->d_t.p, cnt, e->st);
+        const size_t per_f = (size_t)e->n * nrhs;
+        if (fp64) {
+            substitute<double>(e, e->d_t.p, nrhs, sys, nullptr, d_act, nn);
+            launch_add_up_f<double>(d_x, e->d_t.p, per_f, d_act, nn, e->st);
+        } else {
+            substitute<float>(e, e->d_t.p, nrhs, sys, nullptr, d_act, nn);
+            launch_add_up_f<float>(d_x, e->d_t.p, per_f, d_act, nn, e->st);
+        }
+        for (int f : act) {
+            e->refine_info[f].sweeps += 1;
+            e->refine_info[f].method = GM_REFINE_IR;
+        }
     }
     GM_CUDA(cudaEventRecord(t1, e->st));
     GM_CUDA(cudaEventSynchronize(t1));
@@ -740,6 +776,15 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
 }
 
 }  // namespace gm
+
+extern "C" int gm_refine_report(const gm_engine *e, int nmat, gm_refine_info *out) {
+    if (!e || !out) return fail(GM_ERROR_INVALID, "gm_refine_report: null argument");
+    if (nmat != (int)e->refine_info.size())
+        return fail(GM_ERROR_INVALID, "gm_refine_report: the last solve covered %d matrices, not %d",
+                    (int)e->refine_info.size(), nmat);
+    for (int f = 0; f < nmat; ++f) out[f] = e->refine_info[f];
+    return GM_OK;
+}
 
 extern "C" int gm_solve(gm_engine *e, int sys, int nrhs, const double *b, double *x) {
     if (!e || !b || !x || nrhs <= 0) return fail(GM_ERROR_INVALID, "gm_solve: bad argument");

@@ -92,10 +92,14 @@ struct gm_engine {
 
     // solve workspaces
     gm::DevBuf d_x, d_b, d_r, d_t, d_w, d_part, d_norm;
+    gm::DevBuf d_fmap;                          // matrices still refined (device list)
+    std::vector<int> h_fmap;                    // its host copy (kept alive for async uploads)
+    std::vector<gm_refine_info> refine_info;    // per matrix, of the last solve
 
     // epilogue state
     gm::DevBuf d_src_k, d_rec_k, d_seis, d_field, d_res, d_grad, d_frame, d_frame_pass, d_misc;
     gm::DevBuf d_xf, d_xa;   // forward / adjoint solutions kept for the gradient
+    int xf_ns = 0, xa_ns = 0; // right-hand sides held in d_xf / d_xa (0: none valid)
     gm::DevBuf d_mask;       // forward-pass pruning mask of the current solve
     std::vector<double> last_grad0, last_grad1;
     // per-shot gradient taper of ass_grad (SWS_TAPER_CIRCULAR_PER_SHOT 0, 1, 2),
@@ -144,6 +148,10 @@ struct SpikeRhs {
     const int *k = nullptr;         // [nrhs]
     const double2 *amp = nullptr;   // [nf]
 };
+
+// once per device at engine creation: the scratch array and kernels of
+// gm_solve_noalloc (noalloc.cu)
+int noalloc_prepare(int device);
 
 // internal entry points shared between translation units
 int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x_out, const double2 *d_b_in,

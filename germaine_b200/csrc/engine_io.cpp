@@ -136,8 +136,11 @@ int check_ready(const gm_engine *e, int ns, int ntr) {
 int forward_and_seis(gm_engine *e, int ns, const Geometry &g, int ntr, float *seis_out) {
     const int nf = e->nf, n = e->n;
     GM_ALLOC(e->d_xf, (size_t)nf * n * ns * sizeof(double2));
+    e->xf_ns = 0;
+    e->xa_ns = 0;
     const int rc = forward_solve(e, ns, g, e->d_xf.as<double2>());
     if (rc < 0) return rc;
+    e->xf_ns = ns;
     if (ntr > 0) {
         int rc2;
         if ((rc2 = upload(e->d_rec_k, g.krec, e->st))) return rc2;
@@ -357,6 +360,7 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     pat.ncommon = ntr;
     const int arc = gm::engine_solve_device(e, sys, nshots, e->d_xa.as<double2>(), e->d_b.as<double2>(), &pat);
     if (arc < 0) return arc;
+    e->xa_ns = nshots;
     if (arc > worst) worst = arc;
 
     // gradient stack + PML frame taper
@@ -403,6 +407,17 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     return worst;
 }
 
+extern "C" int gm_get_wavefield_fp64(gm_engine *e, int which, double *x) {
+    if (!e || !x || (which != 0 && which != 1)) return fail(GM_ERROR_INVALID, "gm_get_wavefield_fp64: bad argument");
+    const int ns = which ? e->xa_ns : e->xf_ns;
+    if (ns <= 0) return fail(GM_ERROR_STATE, "gm_get_wavefield_fp64: no %s solution held", which ? "adjoint" : "forward");
+    GM_CUDA(cudaSetDevice(e->device));
+    const gm::DevBuf &buf = which ? e->d_xa : e->d_xf;
+    GM_CUDA(cudaMemcpyAsync(x, buf.p, (size_t)e->nf * e->n * ns * sizeof(double2), cudaMemcpyDefault, e->st));
+    GM_CUDA(cudaStreamSynchronize(e->st));
+    return GM_OK;
+}
+
 extern "C" int gm_get_gradient_fp64(gm_engine *e, double *g0, double *g1) {
     if (!e) return fail(GM_ERROR_INVALID, "null engine");
     if (e->last_grad0.empty()) return fail(GM_ERROR_STATE, "no gradient computed yet");
@@ -444,9 +459,12 @@ extern "C" int gm_hessian(gm_engine *e, int mode, int nshots, const float *src_x
     // 1/DH^2 without the -i Omega mu0 of RHS_source_TE; hessian_TE uses
     // RHS_source_TE (src/TE/hessian_TE.c:113).
     GM_ALLOC(e->d_xf, (size_t)nf * n * nshots * sizeof(double2));
+    e->xf_ns = 0;
+    e->xa_ns = 0;   // d_xa will hold blocks of receiver Green's functions
     const int src_phys = (te && mode == GM_HESS_SHIN) ? GM_PHYS_AC : e->cfg.physics;
     int worst = forward_solve(e, nshots, g, e->d_xf.as<double2>(), src_phys);
     if (worst < 0) return worst;
+    e->xf_ns = nshots;
     gm::DevBuf sq;
     GM_ALLOC(sq, 2 * (size_t)nf * n * sizeof(double));
     double *sqf = sq.as<double>(), *sqg = sqf + (size_t)nf * n;

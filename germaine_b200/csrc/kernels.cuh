@@ -127,6 +127,9 @@ struct SolveArgs {
     // node v's subtree, so that node's y and update vector are zero
     const unsigned char *mask;
     int mask_nch;
+    // matrices of this launch: fmap[0 .. nfz) (NULL: all nf, in order)
+    const int *fmap;
+    int nfz;
 };
 
 template <class R>
@@ -147,21 +150,37 @@ struct ResidArgs {
     // spike_amp[f] if k == spike_k[r], else 0
     const int *spike_k;
     const double2 *spike_amp;
+    // matrices of this launch: fmap[0 .. nfz) (NULL: all nf, in order);
+    // partial sums and norms are indexed by the position in fmap
+    const int *fmap;
+    int nfz;
 };
 // r = b - M x and per-(freq, rhs) partial sums of |r|^2 and |b|^2 into
-// part[nblk][nf][nrhs][2]; returns nblk.
+// part[nblk][nfz][nrhs][2]; returns nblk.
 int launch_residual(const ResidArgs &a, double *part, int max_blocks, cudaStream_t st);
 void launch_reduce_norms(const double *part, int nblk, int cnt, double *out, cudaStream_t st);
 // as launch_residual, but writes (T)(b - M'x) into t [nf][n][ldr] instead of r
 // (t = NULL: the norms only)
 template <class R>
 int launch_residual_t(const ResidArgs &a, void *t, double *part, int max_blocks, cudaStream_t st);
+// out = M' x (FP64) for x of working precision cplx<R>, with the partial
+// sums of |out|^2 (b ignored; the |b|^2 sums are 0)
+template <class R>
+int launch_matvec(const ResidArgs &a, const void *x, double2 *out, double *part, int max_blocks, cudaStream_t st);
 
 // y(T) <- x(double) and x(double) += d(T) over [nf][n][ldr]
 template <class R>
 void launch_convert_down(const double2 *src, void *dst, size_t count, cudaStream_t st);
 template <class R>
 void launch_add_up(double2 *x, const void *d, size_t count, cudaStream_t st);
+// x[f] += d[f] for the matrices f = fmap[0 .. nfz) (device list), per_f entries each
+template <class R>
+void launch_add_up_f(double2 *x, const void *d, size_t per_f, const int *fmap, int nfz, cudaStream_t st);
+
+// Load every substitution / refinement kernel now (lazy module loading
+// would otherwise load each on its first launch, taking device memory).
+void preload_solve_kernels();
+void preload_refine_kernels();
 
 // one ordered float dot product (lbfgs.cu: k_dot_seq): out = sum a[i] * b[i], i = 0..n-1 in order
 struct DotJob {

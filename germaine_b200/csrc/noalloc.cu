@@ -13,15 +13,20 @@
 // (GM_NOALLOC_SCRATCH_BYTES below), so it serves small problems only and
 // rejects larger ones with GM_ERROR_INVALID.
 //
-// The array exists once per GPU that loads the library and stays resident
-// until the process exits.  Its device address is looked up with
-// cudaGetSymbolAddress the first time the entry point runs on a device, with
-// that device current; that first call should therefore come before any
-// stream capture.  Every call shares the array and leaves its contents
-// behind: nothing in it is read before this call writes it (the solution
-// buffer, which the refinement accumulates into, is the caller's and is
-// cleared first), and two calls whose GPU work overlaps -- from two threads,
-// or two engines on different streams of the same device -- race on it.
+// The array is loaded on a device together with this file's module.  CUDA
+// loads modules lazily (on first use), and loading one takes device memory,
+// so gm_engine_create does that set-up once per device, with the device
+// current: it looks the array's address up with cudaGetSymbolAddress and
+// loads every substitution and refinement kernel the entry point launches
+// (noalloc_prepare below).  From then on the array stays resident on that
+// device until the process exits, and a gm_solve_noalloc call allocates
+// nothing.  Every call shares the array and leaves its contents behind:
+// nothing in it is read before this call writes it (the solution buffer,
+// which the refinement accumulates into, is the caller's and is cleared
+// first), and two calls whose GPU work overlaps -- from two threads, or two
+// engines on different streams of the same device -- race on it.  The
+// refinement loop reads the residual norms back to the host and waits for
+// the engine's stream once per sweep.
 #include <cmath>
 #include <mutex>
 
@@ -55,6 +60,18 @@ int scratch_address(int device, unsigned char **out) {
 
 size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
+// true when p is memory a kernel on the current device can use: device or
+// managed memory (a host pointer would fault there, or on a system with
+// heterogeneous memory access silently read host memory)
+bool device_reachable(const void *p) {
+    cudaPointerAttributes at{};
+    if (cudaPointerGetAttributes(&at, p) != cudaSuccess) {
+        cudaGetLastError();   // clear the error of an unknown pointer
+        return false;
+    }
+    return at.type == cudaMemoryTypeDevice || at.type == cudaMemoryTypeManaged;
+}
+
 template <class R>
 void substitute_into(gm_engine *e, void *xT, void *w, int nrhs, int trans) {
     gm::SolveArgs<R> a{};
@@ -74,6 +91,22 @@ void substitute_into(gm_engine *e, void *xT, void *w, int nrhs, int trans) {
 
 }  // namespace
 
+namespace gm {
+// Once per device, with that device current (gm_engine_create): the scratch
+// array's address and every kernel gm_solve_noalloc launches, so that the
+// entry point itself never triggers a lazy module load.
+int noalloc_prepare(int device) {
+    unsigned char *base = nullptr;
+    const int rc = scratch_address(device, &base);
+    if (rc) return rc;
+    preload_solve_kernels();
+    preload_refine_kernels();
+    const cudaError_t err = cudaGetLastError();
+    if (err != cudaSuccess) return fail(GM_ERROR_CUDA, "loading the solve kernels failed: %s", cudaGetErrorString(err));
+    return GM_OK;
+}
+}  // namespace gm
+
 #define NA_CUDA(call)                                                                                       \
     do {                                                                                                    \
         cudaError_t err_ = (call);                                                                          \
@@ -90,6 +123,13 @@ extern "C" int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d
     const bool fp64 = e->cfg.precision == GM_PREC_FP64;
     const size_t cs = e->csize();
     const size_t cnt = (size_t)e->nf * e->n * nrhs;
+    if (!device_reachable(d_b) || !device_reachable(d_x))
+        return gm::fail(GM_ERROR_INVALID, "gm_solve_noalloc: b and x must be device (or managed) memory");
+    {
+        const uintptr_t b0 = (uintptr_t)d_b, x0 = (uintptr_t)d_x, nb = cnt * sizeof(double2);
+        if (b0 < x0 + nb && x0 < b0 + nb)
+            return gm::fail(GM_ERROR_INVALID, "gm_solve_noalloc: b and x overlap");
+    }
     const int nblk = (e->n + 63) / 64;
     const int npairs = e->nf * nrhs;
     const size_t b_t = align256(cnt * cs);
@@ -115,6 +155,7 @@ extern "C" int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d
     double2 *x = reinterpret_cast<double2 *>(d_x);
 
     // initial solve in working precision, x = 0 + t
+    NA_CUDA(cudaEventRecord(e->ev0, e->st));
     if (fp64) gm::launch_convert_down<double>(b, t, cnt, e->st);
     else gm::launch_convert_down<float>(b, t, cnt, e->st);
     NA_CUDA(cudaMemsetAsync(x, 0, cnt * sizeof(double2), e->st));
@@ -123,6 +164,16 @@ extern "C" int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d
     if (fp64) gm::launch_add_up<double>(x, t, cnt, e->st);
     else gm::launch_add_up<float>(x, t, cnt, e->st);
     NA_CUDA(cudaGetLastError());
+    NA_CUDA(cudaEventRecord(e->ev1, e->st));
+    NA_CUDA(cudaEventSynchronize(e->ev1));
+    float ms = 0;
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    e->stats.ms_solve = ms;
+    e->stats.ms_refine = 0;
+    e->stats.ms_subst = 0;       // substitutions are not timed separately here
+    e->stats.ms_subst_bwd = 0;
+    e->stats.n_subst = 1;
+    NA_CUDA(cudaEventRecord(e->ev0, e->st));
 
     gm::ResidArgs ra{};
     ra.nx = e->cfg.nx; ra.ny = e->cfg.ny; ra.n = e->n; ra.nf = e->nf; ra.nrhs = nrhs; ra.ldr = nrhs;
@@ -141,11 +192,15 @@ extern "C" int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d
         bool finite = true;
         for (int c = 0; c < npairs; ++c) {
             const double rr = h_norm[2 * c], bb = h_norm[2 * c + 1];
-            if (!(rr == rr) || rr > 1e300) finite = false;
+            if (!std::isfinite(rr)) finite = false;
             const double rel = bb > 0 ? std::sqrt(rr / bb) : std::sqrt(rr);
             worst = rel > worst ? rel : worst;
         }
-        if (!finite) return gm::fail(GM_ERROR_NONFINITE, "gm_solve_noalloc: non-finite residual after %d sweeps", it);
+        if (!finite) {
+            e->stats.ir_iterations = it;
+            e->stats.ir_residual = NAN;
+            return gm::fail(GM_ERROR_NONFINITE, "gm_solve_noalloc: non-finite residual after %d sweeps", it);
+        }
         if (worst <= e->cfg.ir_tol || it >= e->cfg.ir_max_iter) break;
         if (fp64) gm::launch_convert_down<double>(r, t, cnt, e->st);
         else gm::launch_convert_down<float>(r, t, cnt, e->st);
@@ -153,8 +208,12 @@ extern "C" int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d
         else substitute_into<float>(e, t, w, nrhs, sys);
         if (fp64) gm::launch_add_up<double>(x, t, cnt, e->st);
         else gm::launch_add_up<float>(x, t, cnt, e->st);
+        e->stats.n_subst += 1;
     }
-    NA_CUDA(cudaStreamSynchronize(e->st));
+    NA_CUDA(cudaEventRecord(e->ev1, e->st));
+    NA_CUDA(cudaEventSynchronize(e->ev1));
+    cudaEventElapsedTime(&ms, e->ev0, e->ev1);
+    e->stats.ms_refine = ms;
     e->stats.ir_iterations = it;
     e->stats.ir_residual = worst;
     return worst <= e->cfg.ir_tol ? GM_OK : GM_WARNING_NOT_CONVERGED;

@@ -177,6 +177,12 @@ __device__ __forceinline__ bool live(const SolveArgs<R> &a, int v, int r0, int r
     return false;
 }
 
+// matrix handled by this CTA: blockIdx.z indexes the launch's matrix list
+template <class R>
+__device__ __forceinline__ size_t solve_matrix(const SolveArgs<R> &a) {
+    return a.fmap ? (size_t)a.fmap[blockIdx.z] : (size_t)blockIdx.z;
+}
+
 template <class R>
 struct Ctx {
     using C = cplx<R>;
@@ -196,7 +202,7 @@ __device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first,
     c.s = a.s.npiv[c.node];
     const int r0 = chunk * TC;
     c.rn = min(TC, a.nrhs - r0);
-    const size_t fz = blockIdx.z;
+    const size_t fz = solve_matrix(a);
     c.F = reinterpret_cast<const C *>(a.front) + fz * a.s.front_total + a.s.front_off[c.node];
     c.vars = a.s.vars + a.s.var_off[c.node];
     c.X = reinterpret_cast<C *>(a.x) + fz * (size_t)a.s.n * a.ldr + r0;
@@ -221,7 +227,7 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int *inv = a.s.inv + a.s.inv_off[c.node];
-    const size_t fz = blockIdx.z;
+    const size_t fz = solve_matrix(a);
     const C *Wall = reinterpret_cast<const C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + r0;
     const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
     const C *W0 = c0 >= 0 && live(a, c0, r0, c.rn) ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
@@ -306,7 +312,7 @@ __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, 
     }
     // w = (children's update vectors at the ring rows) - L'(ring, piv) y
     const int *inv = a.s.inv + a.s.inv_off[c.node];
-    const C *Wall = reinterpret_cast<const C *>(a.w) + (size_t)blockIdx.z * a.s.rhs_total * a.ldr + chunk * TC;
+    const C *Wall = reinterpret_cast<const C *>(a.w) + solve_matrix(a) * a.s.rhs_total * a.ldr + chunk * TC;
     const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
     const C *W0 = c0 >= 0 && live(a, c0, chunk * TC, c.rn) ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
     const C *W1 = c1 >= 0 && live(a, c1, chunk * TC, c.rn) ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
@@ -512,17 +518,20 @@ static int slice_b(int nrhs) {
     return (sizeof(R) == 4 && nrhs > 32) ? 5 : 4;
 }
 
+template <class R>
+static int solve_nfz(const SolveArgs<R> &a) { return a.fmap ? a.nfz : a.nf; }
+
 template <class R, int RT, int B>
 static void forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
     set_attrs<R, RT, B>();
     const size_t smem = solve_smem<R, RT, B>();
     const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
-    dim3 g1(nchunk, L.count, a.nf);
+    dim3 g1(nchunk, L.count, solve_nfz(a));
     const int fused = 0;   // separate ring kernel: more parallelism per level
     if (a.trans) (k_fwd_piv<R, true, RT, B><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
     else (k_fwd_piv<R, false, RT, B><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
     if (L.max_ring > 0) {
-        dim3 g2(nchunk * ((L.max_ring + RT - 1) / RT), L.count, a.nf);
+        dim3 g2(nchunk * ((L.max_ring + RT - 1) / RT), L.count, solve_nfz(a));
         if (a.trans) (k_fwd_ring<R, true, RT, B><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
         else (k_fwd_ring<R, false, RT, B><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
     }
@@ -535,18 +544,18 @@ static void backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream
     const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
     static const bool no_small = env_int("GM_NO_BWD_SMALL") != 0;
     if (RT == 32 && L.max_piv <= SNB && !no_small) {   // one pivot block per front: fused ring + pivot kernel
-        dim3 g(nchunk, L.count, a.nf);
+        dim3 g(nchunk, L.count, solve_nfz(a));
         if (a.trans) (k_bwd_small<R, true, B><<<g, NT, smem, st>>>(a, L.first), note_launch());
         else (k_bwd_small<R, false, B><<<g, NT, smem, st>>>(a, L.first), note_launch());
         return;
     }
     const int fused = 0;
     if (L.max_ring > 0) {
-        dim3 g1(nchunk * ((L.max_piv + RT - 1) / RT), L.count, a.nf);
+        dim3 g1(nchunk * ((L.max_piv + RT - 1) / RT), L.count, solve_nfz(a));
         if (a.trans) (k_bwd_ring<R, true, RT, B><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
         else (k_bwd_ring<R, false, RT, B><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
     }
-    dim3 g2(nchunk, L.count, a.nf);
+    dim3 g2(nchunk, L.count, solve_nfz(a));
     if (a.trans) (k_bwd_piv<R, true, RT, B><<<g2, NT, smem, st>>>(a, L.first, fused), note_launch());
     else (k_bwd_piv<R, false, RT, B><<<g2, NT, smem, st>>>(a, L.first, fused), note_launch());
 }
@@ -564,7 +573,7 @@ static void level_pass(bool fwd, const SolveArgs<R> &a, const LevelInfo &L, cuda
 
 template <class R>
 static void dispatch(bool fwd, const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
-    if (L.count == 0) return;
+    if (L.count == 0 || solve_nfz(a) <= 0) return;
     if (slice_b<R>(a.nrhs) == 5) level_pass<R, 5>(fwd, a, L, st);
     else level_pass<R, 4>(fwd, a, L, st);
 }
@@ -577,6 +586,21 @@ void launch_solve_forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaS
 template <class R>
 void launch_solve_backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
     dispatch<R>(false, a, L, st);
+}
+
+// Sets the shared-memory attribute of every substitution kernel variant,
+// which also loads each kernel (CUDA loads modules and functions lazily, on
+// first use, and a load takes device memory): a caller that must not
+// allocate once solving has begun calls this beforehand.
+void preload_solve_kernels() {
+    set_attrs<double, 32, 4>();
+    set_attrs<double, 64, 4>();
+    set_attrs<double, 32, 5>();
+    set_attrs<double, 64, 5>();
+    set_attrs<float, 32, 4>();
+    set_attrs<float, 64, 4>();
+    set_attrs<float, 32, 5>();
+    set_attrs<float, 64, 5>();
 }
 
 template void launch_solve_forward_level<double>(const SolveArgs<double> &, const LevelInfo &, cudaStream_t);

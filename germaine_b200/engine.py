@@ -130,6 +130,14 @@ class Engine:
         self.freqs = f
         return self.last_status
 
+    def refine_report(self) -> list[dict]:
+        """Per-matrix refinement records of the last solve (gm_refine_report):
+        first / final max relative residual, sweeps, method."""
+        arr = (_lib.GmRefineInfo * self.nf)()
+        check(self.lib.gm_refine_report(self._h, self.nf, arr))
+        return [{"first_residual": a.first_residual, "final_residual": a.final_residual, "sweeps": a.sweeps,
+                 "method": _lib.REFINE_METHOD_NAMES.get(a.method, str(a.method))} for a in arr]
+
     def stats(self) -> dict:
         s = GmStats()
         check(self.lib.gm_engine_stats(self._h, ctypes.byref(s)))
@@ -213,6 +221,16 @@ class Engine:
         SRTRADIUS in metres), 2 taper_grad_shot1 (squares of half-width
         FILTSIZE)."""
         check(self.lib.gm_set_shot_taper(self._h, mode, srtradius, filtsize))
+
+    def wavefield_fp64(self, which: int = 0, nshots: int | None = None) -> np.ndarray:
+        """FP64 solutions of the last forward-type call (which = 0) or of the
+        last grad_obj's adjoint solve (which = 1): [nf][NY*NX][nshots]
+        complex128 in grid order (no vec2mat shift)."""
+        if nshots is None:
+            raise ValueError("nshots is required")
+        x = np.empty((self.nf, self.n, nshots), np.complex128)
+        check(self.lib.gm_get_wavefield_fp64(self._h, which, ptr(x)))
+        return x
 
     def gradient_fp64(self):
         g0 = np.zeros(self.n)

@@ -95,6 +95,20 @@ typedef struct {
     double ms_subst_bwd;        /* device time of the backward passes of those substitutions */
 } gm_stats;
 
+/* Refinement record of one matrix in the last solve (gm_solve and the solves
+ * inside gm_forward, gm_obj, gm_grad_obj -- whose last solve is the adjoint
+ * one -- and gm_hessian).  Residuals are max over the matrix's right-hand
+ * sides of ||b - M x|| / ||b||, formed in FP64. */
+#define GM_REFINE_NONE  0  /* the first (working-precision) solution met the target */
+#define GM_REFINE_IR    1  /* classical iterative refinement sweeps */
+#define GM_REFINE_GMRES 2  /* GMRES on the correction equation, preconditioned by the factors */
+typedef struct {
+    double first_residual;   /* residual of the first solution */
+    double final_residual;   /* residual on return */
+    int32_t sweeps;          /* substitutions after the first one (IR sweeps or GMRES iterations) */
+    int32_t method;          /* GM_REFINE_* */
+} gm_refine_info;
+
 const char *gm_last_error(void);
 int gm_version(void);
 
@@ -152,6 +166,12 @@ int gm_factor_values(gm_engine *e, int nmat, const double *re, const double *im)
  * src/AC/init_A_AC_9p_pml.c:75-80).  Any of the four outputs may be NULL. */
 int gm_get_triplets(gm_engine *e, int ifreq, double *Ar, double *Ai, int32_t *irow, int32_t *icol);
 
+/* Per-matrix refinement records of the last solve: out[0 .. nmat) for the
+ * nmat matrices of the factorised batch (nmat must equal that count).  No
+ * counterpart in the reference (UMFPACK's Info array reports one solve); it
+ * states, per frequency, the error of the mixed-precision path. */
+int gm_refine_report(const gm_engine *e, int nmat, gm_refine_info *out);
+
 /* Solve sys (GM_SYS_A / GM_SYS_AT) for nrhs right-hand sides per frequency
  * with the current factors, followed by FP64 iterative refinement to
  * cfg.ir_tol: umfpack_zi_solve (src/AC/forward_shot_AC.c:88) over a block
@@ -207,6 +227,15 @@ int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y
  * FSSHIFT rows away from the physical positions).  The product of a
  * shot's coefficients is formed in FP64 and applied to the FP64 term. */
 int gm_set_shot_taper(gm_engine *e, int mode, float srtradius, int filtsize);
+
+/* The FP64 solution vectors behind the float outputs: which = 0 the forward
+ * wavefields of the last gm_forward / gm_obj / gm_obj_each / gm_grad_obj /
+ * gm_hessian call (the umfpack_zi_solve result xr/xi of
+ * src/AC/forward_shot_AC.c:88 for every shot), which = 1 the adjoint
+ * wavefields of the last gm_grad_obj (src/AC/grad_obj_AC.c:147).  x is
+ * [nfreq][N][nshots] complex128 (interleaved re/im, shot fastest) in grid
+ * order, before vec2mat's shift.  GM_ERROR_STATE when none is held. */
+int gm_get_wavefield_fp64(gm_engine *e, int which, double *x);
 
 /* The last gm_grad_obj gradients before rounding to float, in FP64
  * ([NY][NX] each; g1 ignored for AC).  Either pointer may be NULL. */
@@ -405,12 +434,16 @@ int gm_read_model(const char *path, int nx, int ny, int npml, int free_surf, flo
  * synchronises the whole device (stalling the caller's own kernels on other
  * streams), and a caller that has reserved its device memory budget up
  * front has none left to give.  Same arguments and result as gm_solve, but
- * b and x must be device pointers, and every workspace comes from one
- * file-scope device array of 32 MiB (held by every GPU that loads the
- * library until exit); problems whose workspaces do not fit return
- * GM_ERROR_INVALID.  The first call on a device looks up the array's
- * address (make it before any stream capture); calls whose GPU work
- * overlaps race on the shared array. */
+ * b and x must be device (or managed) pointers that do not overlap
+ * (GM_ERROR_INVALID otherwise), and every workspace comes from one
+ * file-scope device array of 32 MiB; problems whose workspaces do not fit
+ * return GM_ERROR_INVALID.  gm_engine_create loads that array (and every
+ * kernel this call launches) on the engine's device, where it stays until
+ * the process exits, so the call itself allocates nothing.  Calls whose GPU
+ * work overlaps race on the shared array.  Each refinement sweep copies the
+ * residual norms to the host and waits for the engine's stream, so the call
+ * cannot be recorded into a CUDA graph by stream capture.  Statistics:
+ * ms_solve and ms_refine are timed, ms_subst is not (0). */
 int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d_b, double *d_x);
 
 /* Batched complex64 GEMM C_i -= A_i * B_i on device pointers: the Schur
