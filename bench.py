@@ -261,7 +261,8 @@ def run_gpu(args):
 
     results = {}
     for name, prec in (("mixed", GM_PREC_C64_IR), ("fp64", GM_PREC_FP64)):
-        e = Engine(nx, ny, DH, NPML, precision=prec, device=local, leaf_max=args.leaf)
+        e = Engine(nx, ny, DH, NPML, precision=prec, device=local, leaf_max=args.leaf,
+                   refine={"auto": 0, "ir": 1, "gmres": 2}[args.refine])
         e.set_model(vp_d, rho_d)
 
         def check_converged(tag):
@@ -291,12 +292,29 @@ def run_gpu(args):
             check_converged("end-to-end")
         ms_e2e, _ = time_steps(torch, e, step_e2e, max(1, args.steps // 2), 1, dist)
         r["ms_e2e"] = ms_e2e
+        # per-frequency refinement record of the last step and, outside the
+        # timed region, the FP64 forward wavefields for the error table
+        r["refine"] = e.refine_report()
+        r["x"] = e.wavefield_fp64(0, ns) if args.wavefield_error else None
         results[name] = r
         e.close()
         del e
         torch.cuda.empty_cache()
 
     mixed, fp64 = results["mixed"], results["fp64"]
+    per_freq = []
+    for i, f in enumerate(freqs):
+        row = {"freq_hz": float(f)}
+        for nm in ("mixed", "fp64"):
+            rf = results[nm]["refine"][i]
+            row[nm] = {"first_residual": rf["first_residual"], "final_residual": rf["final_residual"],
+                       "sweeps": rf["sweeps"], "method": rf["method"]}
+        if mixed["x"] is not None:
+            a, b = mixed["x"][i], fp64["x"][i]
+            row["mixed_wavefield_rel_l2_vs_fp64"] = float(np.linalg.norm(a - b) / np.linalg.norm(b))
+        per_freq.append(row)
+    for nm in ("mixed", "fp64"):
+        results[nm]["x"] = None
     units = nf * ns * world
     # headline: the faster of the two paths (both refine to the residual
     # target); the other is reported beside it
@@ -354,6 +372,7 @@ def run_gpu(args):
                       "gpu_launches_per_step": results[n]["launches"]}
                   for n in ("fp64", "mixed")},
         "mixed_over_fp64": fp64["ms"] / mixed["ms"],
+        "per_frequency": per_freq,
         "roofline": {"kernel": "K5 backward substitution (k_bwd_small, k_bwd_ring + k_bwd_piv, %s)" % ("complex128" if csize == 16 else "complex64"),
                      "bound": "hbm", "achieved": achieved, "peak": peak_hbm, "unit": "GB/s",
                      "frac": achieved / peak_hbm, "peak_kind": peak_kind, "traffic": traffic,
@@ -406,6 +425,10 @@ def main():
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--leaf", type=int, default=32)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--refine", choices=["auto", "ir", "gmres"], default="auto",
+                    help="refinement of the mixed path: automatic IR / GMRES-IR choice, IR only, GMRES-IR only")
+    ap.add_argument("--no-wavefield-error", dest="wavefield_error", action="store_false",
+                    help="skip the per-frequency wavefield comparison of the two paths (outside the timed region)")
     ap.add_argument("--nx0", type=int, default=W["nx0"], help="model width without PML (profiling cases)")
     ap.add_argument("--ny0", type=int, default=W["ny0"], help="model depth without PML (profiling cases)")
     ap.add_argument("--nfreq", type=int, default=W["nfreq"], help="frequencies 2, 3, ... Hz (profiling cases)")

@@ -30,6 +30,7 @@ GM_PHYS_AC, GM_PHYS_SH, GM_PHYS_TE = 1, 2, 4
 GM_PREC_FP64, GM_PREC_C64_IR = 0, 1
 GM_OP_REF, GM_OP_EXACT = 0, 1
 GM_SYS_A, GM_SYS_AT = 0, 1
+GM_REFINE_MODE_AUTO, GM_REFINE_MODE_IR, GM_REFINE_MODE_GMRES = 0, 1, 2
 
 
 class GmConfig(ctypes.Structure):
@@ -37,7 +38,7 @@ class GmConfig(ctypes.Structure):
                 ("npml", ctypes.c_int32), ("free_surf", ctypes.c_int32), ("a0_pml", ctypes.c_float),
                 ("s", ctypes.c_float), ("physics", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("op_mode", ctypes.c_int32), ("leaf_max", ctypes.c_int32), ("ir_tol", ctypes.c_double),
-                ("ir_max_iter", ctypes.c_int32)]
+                ("ir_max_iter", ctypes.c_int32), ("refine", ctypes.c_int32), ("gmres_restart", ctypes.c_int32)]
 
 
 class GmStats(ctypes.Structure):
@@ -71,7 +72,7 @@ EXPORTS = [
     "gm_get_gradient_fp64", "gm_get_wavefield_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_hessian", "gm_get_hessian_fp64", "gm_apply_hess", "gm_precond",
     "gm_lbfgs_create", "gm_lbfgs_destroy", "gm_lbfgs_step", "gm_lbfgs_rotate", "gm_lbfgs_zero",
     "gm_lbfgs_check_descent", "gm_lbfgs_get_old", "gm_lbfgs_set_old", "gm_mat_change",
-    "gm_set_shot_taper", "gm_taper_grad_shot", "gm_taper_grad_shot1", "gm_tikhonov_cost_te", "gm_tikhonov_grad_te",
+    "gm_set_shot_taper", "gm_set_invmat", "gm_set_source_wavelet", "gm_stf_dft", "gm_taper_grad_shot", "gm_taper_grad_shot1", "gm_tikhonov_cost_te", "gm_tikhonov_grad_te",
     "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_read_grid", "gm_cgemm_sub_c64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
@@ -142,6 +143,9 @@ def load() -> ctypes.CDLL:
     lib.gm_lbfgs_set_old.argtypes = [vp, vp, vp]
     lib.gm_mat_change.argtypes = [i32, i32, i32, f32, f32, f32, vp, vp, vp]
     lib.gm_set_shot_taper.argtypes = [vp, i32, f32, i32]
+    lib.gm_set_invmat.argtypes = [vp, i32]
+    lib.gm_set_source_wavelet.argtypes = [vp, i32, vp]
+    lib.gm_stf_dft.argtypes = [ctypes.c_char_p, i32, f32, vp]
     lib.gm_taper_grad_shot.argtypes = [i32, i32, f32, f32, i32, vp, vp, i32, vp, vp, i32, vp]
     lib.gm_taper_grad_shot1.argtypes = [i32, i32, f32, i32, i32, vp, vp, i32, vp, vp, vp]
     lib.gm_tikhonov_cost_te.argtypes = [i32, i32, i32, i32, f32, f32, f32, f32, f32, f32, f32, vp, vp, f32, vp]

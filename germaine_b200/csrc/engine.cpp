@@ -14,6 +14,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <complex>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
@@ -62,6 +63,9 @@ int check_config(const gm_config *c) {
     if (c->precision != GM_PREC_FP64 && c->precision != GM_PREC_C64_IR)
         return fail(GM_ERROR_INVALID, "unknown precision %d", c->precision);
     if (c->op_mode != GM_OP_REF && c->op_mode != GM_OP_EXACT) return fail(GM_ERROR_INVALID, "unknown op_mode %d", c->op_mode);
+    if (c->refine < GM_REFINE_MODE_AUTO || c->refine > GM_REFINE_MODE_GMRES)
+        return fail(GM_ERROR_INVALID, "unknown refinement mode %d", c->refine);
+    if (c->gmres_restart < 0) return fail(GM_ERROR_INVALID, "GMRES restart length must be >= 0");
     return GM_OK;
 }
 
@@ -85,6 +89,8 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
         if (e->cfg.leaf_max <= 0) e->cfg.leaf_max = 32;   // measured best at 841 x 227 (24 .. 40 within 6 %)
         if (!(e->cfg.ir_tol > 0)) e->cfg.ir_tol = 1e-10;
         if (e->cfg.ir_max_iter <= 0) e->cfg.ir_max_iter = 10;
+        if (e->cfg.gmres_restart <= 0 || e->cfg.gmres_restart > gm::kGmresMaxRestart)
+            e->cfg.gmres_restart = gm::kGmresMaxRestart;
         e->device = device;
         e->fsshift = cfg->free_surf ? 0 : cfg->npml;
         e->n = cfg->nx * cfg->ny;
@@ -556,7 +562,7 @@ namespace gm {
 // entries) restricts it to those matrices of the batch (NULL: all).
 template <class R>
 static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsigned char *mask = nullptr,
-                       const int *fmap = nullptr, int nfz = 0) {
+                       const int *fmap = nullptr, int nfz = 0, const int *xmap = nullptr) {
     cudaEventRecord(e->ev_s0, e->st);
     SolveArgs<R> a{};
     a.s = e->dsym;
@@ -566,6 +572,7 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsign
     a.nf = e->nf;
     a.fmap = fmap;
     a.nfz = nfz;
+    a.xmap = xmap;
     a.nrhs = nrhs;
     a.ldr = nrhs;
     const int nchunk = (nrhs + 31) / 32;
@@ -639,6 +646,243 @@ static const unsigned char *build_mask(gm_engine *e, int nrhs, const RhsPattern 
     return e->d_mask.as<unsigned char>();
 }
 
+// GMRES-IR for the matrices `gset` of the batch: restarted GMRES(m) on the
+// correction equation M' d = b - M' x, one run per (matrix, right-hand
+// side), in FP64 with the working-precision factors as right
+// preconditioner (flexible form, gmres.cu).  Each cycle starts from the
+// true FP64 residual; a matrix leaves when its worst right-hand side meets
+// the target, a cycle ends for a matrix when the least-squares residual
+// estimate of each of its right-hand sides is below half the target.  At
+// most ir_max_iter iterations per matrix in total.  Updates x in place and
+// the matrices' refinement records.
+template <class R>
+static int gmres_refine(gm_engine *e, int sys, int nrhs, double2 *d_x, const ResidArgs &ra_in,
+                        const std::vector<int> &gset) {
+    using cd = std::complex<double>;
+    const int ng = (int)gset.size();
+    if (ng == 0) return GM_OK;
+    const int m = e->cfg.gmres_restart;
+    const int n = e->n;
+    const double tol = e->cfg.ir_tol;
+    const size_t per = (size_t)n * nrhs;
+    const size_t vstride = (size_t)ng * per;   // one Krylov slot holds all ng matrices
+    GM_ALLOC(e->d_gv, (size_t)(m + 1) * vstride * sizeof(double2));
+    GM_ALLOC(e->d_gz, (size_t)m * vstride * sizeof(cplx_any<R>));
+    const int nblk_r = (n + 63) / 64, nblk_g = (n + 255) / 256;
+    const size_t part_words = std::max((size_t)nblk_r * ng * nrhs * 2, (size_t)nblk_g * ng * nrhs * (m + 1) * 2);
+    GM_ALLOC(e->d_gpart, part_words * sizeof(double));
+    GM_ALLOC(e->d_gnorm, (size_t)ng * nrhs * (m + 1) * 2 * sizeof(double));
+    GM_ALLOC(e->d_gcoef, (size_t)ng * nrhs * kGmresStride * sizeof(double2) + (size_t)ng * nrhs * sizeof(double));
+    GM_ALLOC(e->d_gmap, 2 * (size_t)ng * sizeof(int));
+    double2 *V = e->d_gv.as<double2>();
+    cplx_any<R> *Z = e->d_gz.as<cplx_any<R>>();
+    double *part = e->d_gpart.as<double>(), *nrm = e->d_gnorm.as<double>();
+    double2 *d_coef = e->d_gcoef.as<double2>();
+    double *d_scal = reinterpret_cast<double *>(d_coef + (size_t)ng * nrhs * kGmresStride);
+    int *d_fm = e->d_gmap.as<int>(), *d_zm = d_fm + ng;
+
+    // per (slot, right-hand side) column: Hessenberg columns, rotations, g
+    const int ncol = ng * nrhs;
+    std::vector<double> beta((size_t)ncol * (m + 1)), bnorm(ncol);
+    std::vector<cd> H((size_t)ncol * (m + 1) * m), cs_sn((size_t)ncol * m * 2), g((size_t)ncol * (m + 1));
+    std::vector<char> cdone(ncol);
+    std::vector<int> used(ng, 0), kz(ng, 0);
+    std::vector<int> live_f, live_z;
+    std::vector<double> hn;
+    std::vector<double2> hc;
+    std::vector<double> hs;
+    ResidArgs ra = ra_in;
+    ra.xmap = nullptr;
+
+    auto upload_maps = [&](const std::vector<int> &zl) -> int {
+        std::vector<int> fz(zl.size());
+        for (size_t j = 0; j < zl.size(); ++j) fz[j] = gset[zl[j]];
+        GM_CUDA(cudaMemcpy(d_fm, fz.data(), fz.size() * sizeof(int), cudaMemcpyHostToDevice));
+        GM_CUDA(cudaMemcpy(d_zm, zl.data(), zl.size() * sizeof(int), cudaMemcpyHostToDevice));
+        return GM_OK;
+    };
+    auto fetch = [&](double *src, size_t words, std::vector<double> &dst) -> int {
+        dst.resize(words);
+        GM_CUDA(cudaMemcpyAsync(dst.data(), src, words * sizeof(double), cudaMemcpyDeviceToHost, e->st));
+        GM_CUDA(cudaStreamSynchronize(e->st));
+        return GM_OK;
+    };
+
+    std::vector<int> live;   // slots still refined
+    for (int z = 0; z < ng; ++z) live.push_back(z);
+    for (;;) {
+        // true residual V_0 = b - M' x of the live matrices, FP64
+        const int nl = (int)live.size();
+        int rc;
+        if ((rc = upload_maps(live))) return rc;
+        ra.fmap = d_fm;
+        ra.nfz = nl;
+        ra.omap = d_zm;
+        ra.r = V;
+        const int nb = launch_residual(ra, part, nblk_r, e->st);
+        launch_reduce_norms(part, nb, nl * nrhs * 2, nrm, e->st);
+        GM_CUDA(cudaGetLastError());
+        if ((rc = fetch(nrm, (size_t)nl * nrhs * 2, hn))) return rc;
+        std::vector<int> next;
+        for (int j = 0; j < nl; ++j) {
+            const int z = live[j];
+            double wf = 0;
+            for (int r = 0; r < nrhs; ++r) {
+                const double rr = hn[2 * ((size_t)j * nrhs + r)], bb = hn[2 * ((size_t)j * nrhs + r) + 1];
+                if (!std::isfinite(rr)) return fail(GM_ERROR_NONFINITE, "GMRES-IR: non-finite residual");
+                const int c = z * nrhs + r;
+                beta[(size_t)c * (m + 1)] = std::sqrt(rr);
+                bnorm[c] = bb > 0 ? std::sqrt(bb) : 1.0;
+                wf = std::max(wf, std::sqrt(rr) / bnorm[c]);
+            }
+            gm_refine_info &ri = e->refine_info[gset[z]];
+            ri.final_residual = wf;
+            if (wf > tol && used[z] < e->cfg.ir_max_iter) next.push_back(z);
+        }
+        if (next.empty()) break;
+        if (next.size() != live.size()) {   // V_0 of the remaining slots is in place already
+            live.swap(next);
+            if ((rc = upload_maps(live))) return rc;
+        }
+        // one GMRES cycle over the live slots
+        for (int z : live) {
+            kz[z] = 0;
+            for (int r = 0; r < nrhs; ++r) {
+                const int c = z * nrhs + r;
+                const double b0 = beta[(size_t)c * (m + 1)];
+                cdone[c] = !(b0 > 0.5 * tol * bnorm[c]);
+                std::fill(g.begin() + (size_t)c * (m + 1), g.begin() + (size_t)(c + 1) * (m + 1), cd(0));
+                g[(size_t)c * (m + 1)] = b0;
+            }
+        }
+        std::vector<int> inner = live;
+        const int max_j = std::min(m, e->cfg.ir_max_iter);
+        for (int jj = 0; jj < max_j && !inner.empty(); ++jj) {
+            const int ni = (int)inner.size();
+            if ((rc = upload_maps(inner))) return rc;
+            // Z_jj = (R)(V_jj / beta_jj)
+            hs.assign((size_t)ni * nrhs, 0.0);
+            for (int j = 0; j < ni; ++j)
+                for (int r = 0; r < nrhs; ++r) {
+                    const int c = inner[j] * nrhs + r;
+                    const double b = beta[(size_t)c * (m + 1) + jj];
+                    hs[(size_t)j * nrhs + r] = (!cdone[c] && b > 0) ? 1.0 / b : 0.0;
+                }
+            GM_CUDA(cudaMemcpy(d_scal, hs.data(), hs.size() * sizeof(double), cudaMemcpyHostToDevice));
+            launch_scale_down<R>(V + jj * vstride, Z + jj * vstride, d_scal, d_zm, ni, n, nrhs, e->st);
+            // Z_jj <- M~^-1 Z_jj (working-precision substitution in place)
+            substitute<R>(e, Z + jj * vstride, nrhs, sys, nullptr, d_fm, ni, d_zm);
+            // V_jj+1 = M' Z_jj (FP64)
+            ResidArgs pa = ra;
+            pa.fmap = d_fm; pa.nfz = ni; pa.xmap = d_zm; pa.omap = d_zm;
+            launch_matvec<R>(pa, Z + jj * vstride, V + (jj + 1) * vstride, part, nblk_r, e->st);
+            // h_i = <v_i, w>: dots with the unnormalised V_i
+            const int nv = jj + 1;
+            const int nbd = launch_dots(V, vstride, nv, V + (jj + 1) * vstride, d_zm, ni, n, nrhs, part, e->st);
+            launch_reduce_norms(part, nbd, ni * nrhs * (nv + 1) * 2, nrm, e->st);
+            GM_CUDA(cudaGetLastError());
+            if ((rc = fetch(nrm, (size_t)ni * nrhs * (nv + 1) * 2, hn))) return rc;
+            hc.assign((size_t)ni * nrhs * kGmresStride, make_double2(0.0, 0.0));
+            for (int j = 0; j < ni; ++j)
+                for (int r = 0; r < nrhs; ++r) {
+                    const int c = inner[j] * nrhs + r;
+                    if (cdone[c]) continue;   // its coefficients stay 0: W is left as it is
+                    for (int i = 0; i < nv; ++i) {
+                        const double *p = &hn[(((size_t)j * nrhs + r) * (nv + 1) + i) * 2];
+                        const double bi = beta[(size_t)c * (m + 1) + i];
+                        const cd h = cd(p[0], p[1]) / bi;   // <V_i / beta_i, w>
+                        H[((size_t)c * (m + 1) + i) * m + jj] = h;
+                        const cd co = h / bi;
+                        hc[((size_t)j * nrhs + r) * kGmresStride + i] = make_double2(co.real(), co.imag());
+                    }
+                }
+            GM_CUDA(cudaMemcpy(d_coef, hc.data(), hc.size() * sizeof(double2), cudaMemcpyHostToDevice));
+            const int nbu = launch_gs_update(V, vstride, nv, V + (jj + 1) * vstride, d_coef, d_zm, ni, n, nrhs, part,
+                                             e->st);
+            launch_reduce_norms(part, nbu, ni * nrhs, nrm, e->st);
+            GM_CUDA(cudaGetLastError());
+            if ((rc = fetch(nrm, (size_t)ni * nrhs, hn))) return rc;
+            // Givens rotations of column jj and the residual estimates
+            std::vector<int> still;
+            for (int j = 0; j < ni; ++j) {
+                const int z = inner[j];
+                bool all_done = true;
+                for (int r = 0; r < nrhs; ++r) {
+                    const int c = z * nrhs + r;
+                    if (cdone[c]) continue;
+                    const double hnext = std::sqrt(std::max(hn[(size_t)j * nrhs + r], 0.0));
+                    beta[(size_t)c * (m + 1) + jj + 1] = hnext;
+                    cd *Hc = &H[(size_t)c * (m + 1) * m];
+                    cd *rot = &cs_sn[(size_t)c * m * 2];
+                    for (int i = 0; i < jj; ++i) {   // earlier rotations
+                        const cd cs = rot[2 * i], sn = rot[2 * i + 1];
+                        const cd a = Hc[i * m + jj], b = Hc[(i + 1) * m + jj];
+                        Hc[i * m + jj] = cs * a + sn * b;
+                        Hc[(i + 1) * m + jj] = -std::conj(sn) * a + cs * b;
+                    }
+                    const cd a = Hc[jj * m + jj];
+                    const double t = std::hypot(std::abs(a), hnext);
+                    cd cs, sn;
+                    if (std::abs(a) == 0.0) {
+                        cs = 0.0;
+                        sn = 1.0;
+                    } else {
+                        cs = std::abs(a) / t;
+                        sn = (a / std::abs(a)) * hnext / t;
+                    }
+                    rot[2 * jj] = cs;
+                    rot[2 * jj + 1] = sn;
+                    Hc[jj * m + jj] = cs * a + sn * hnext;
+                    Hc[(jj + 1) * m + jj] = 0.0;
+                    cd *gc = &g[(size_t)c * (m + 1)];
+                    gc[jj + 1] = -std::conj(sn) * gc[jj];
+                    gc[jj] = cs * gc[jj];
+                    if (std::abs(gc[jj + 1]) <= 0.5 * tol * bnorm[c] || !(hnext > 0)) cdone[c] = 1;
+                    else all_done = false;
+                }
+                kz[z] = jj + 1;
+                if (!all_done) still.push_back(z);
+            }
+            inner.swap(still);
+        }
+        // x += sum_i y_i Z_i with R y = g (upper triangular), per matrix
+        for (int z : live) {
+            const int k = kz[z];
+            if (k == 0) continue;
+            hc.assign((size_t)nrhs * kGmresStride, make_double2(0.0, 0.0));
+            for (int r = 0; r < nrhs; ++r) {
+                const int c = z * nrhs + r;
+                const cd *Hc = &H[(size_t)c * (m + 1) * m];
+                const cd *gc = &g[(size_t)c * (m + 1)];
+                // columns that met the estimate early have k_c < k entries;
+                // their trailing rows are 0, so solve over the nonzero part
+                int kc = k;
+                while (kc > 0 && Hc[(kc - 1) * m + (kc - 1)] == cd(0)) --kc;
+                std::vector<cd> y(kc);
+                for (int i = kc - 1; i >= 0; --i) {
+                    cd acc = gc[i];
+                    for (int q = i + 1; q < kc; ++q) acc -= Hc[i * m + q] * y[q];
+                    y[i] = acc / Hc[i * m + i];
+                }
+                for (int i = 0; i < kc; ++i)
+                    hc[(size_t)r * kGmresStride + i] = make_double2(y[i].real(), y[i].imag());
+            }
+            GM_CUDA(cudaMemcpy(d_coef, hc.data(), hc.size() * sizeof(double2), cudaMemcpyHostToDevice));
+            const int fz = gset[z];
+            GM_CUDA(cudaMemcpy(d_fm, &fz, sizeof(int), cudaMemcpyHostToDevice));
+            GM_CUDA(cudaMemcpy(d_zm, &z, sizeof(int), cudaMemcpyHostToDevice));
+            launch_x_update<R>(d_x, Z, vstride, k, d_coef, d_fm, d_zm, 1, n, nrhs, e->st);
+            GM_CUDA(cudaGetLastError());
+            used[z] += k;
+            gm_refine_info &ri = e->refine_info[fz];
+            ri.sweeps += k;
+            ri.method = GM_REFINE_GMRES;
+            GM_CUDA(cudaStreamSynchronize(e->st));   // d_coef / maps are rewritten next
+        }
+    }
+    return GM_OK;
+}
+
 // x (device, [nf][n][nrhs] c128) = M'^{-1} b with FP64 refinement; b, x device.
 // The first substitution prunes the forward pass by `pattern` when given;
 // the refinement sweeps (dense residuals) do not.
@@ -698,6 +942,7 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     act.resize(e->nf);
     for (int f = 0; f < e->nf; ++f) act[f] = f;
     std::vector<double> norms((size_t)e->nf * nrhs * 2);
+    std::vector<double> prev_res(e->nf, 0.0);
     e->refine_info.assign(e->nf, gm_refine_info{0.0, 0.0, 0, GM_REFINE_NONE});
     double worst = 0;
     int it = 0;
@@ -707,6 +952,8 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
         GM_CUDA(cudaMemcpyAsync(d_act, act.data(), na * sizeof(int), cudaMemcpyHostToDevice, e->st));
         ra.fmap = d_act;
         ra.nfz = na;
+        ra.omap = nullptr;
+        ra.xmap = nullptr;
         // residual straight into the working-precision right-hand side; the
         // first check of FP64 factors normally passes, so it computes the
         // norms only and the residual is formed again if a sweep follows
@@ -746,10 +993,44 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
             std::fprintf(stderr, "\n");
         }
         if (next.empty() || it >= e->cfg.ir_max_iter) break;
+        // Matrices that go on with GMRES-IR: all of them in GMRES mode; in
+        // auto mode those whose last sweep contracted too slowly to reach the
+        // target within two more sweeps (the first check has no contraction
+        // yet, so every matrix starts with a plain sweep)
+        std::vector<int> gset, irset;
+        for (int f : next) {
+            const gm_refine_info &ri = e->refine_info[f];
+            bool to_gmres = e->cfg.refine == GM_REFINE_MODE_GMRES;
+            if (e->cfg.refine == GM_REFINE_MODE_AUTO && it > 0) {
+                const double rho = prev_res[f] > 0 ? ri.final_residual / prev_res[f] : 1.0;
+                const double need = std::log(e->cfg.ir_tol / ri.final_residual);
+                to_gmres = !(rho < 1.0) || need / std::log(rho) > 2.0;
+            }
+            (to_gmres ? gset : irset).push_back(f);
+        }
+        for (int f : next) prev_res[f] = e->refine_info[f].final_residual;
+        if (!gset.empty()) {
+            const int grc = fp64 ? gmres_refine<double>(e, sys, nrhs, d_x, ra, gset)
+                                 : gmres_refine<float>(e, sys, nrhs, d_x, ra, gset);
+            if (grc) {
+                e->stats.ir_iterations = it;
+                e->stats.ir_residual = NAN;
+                return grc;
+            }
+        }
+        if (irset.empty()) {
+            worst = 0;
+            for (const gm_refine_info &ri : e->refine_info) worst = std::max(worst, ri.final_residual);
+            ++it;
+            break;
+        }
         // the remaining matrices: their residual is in t (formed again for
         // the FP64 path, whose first check formed norms only)
-        const int nn = (int)next.size();
-        act.swap(next);
+        const int nn = (int)irset.size();
+        act.swap(irset);
+        ra.omap = nullptr;
+        ra.xmap = nullptr;
+        ra.r = nullptr;
         GM_CUDA(cudaMemcpyAsync(d_act, act.data(), nn * sizeof(int), cudaMemcpyHostToDevice, e->st));
         ra.nfz = nn;
         if (!rhs) launch_residual_t<double>(ra, e->d_t.p, e->d_part.as<double>(), nblk_max, e->st);

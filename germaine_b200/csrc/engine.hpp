@@ -93,6 +93,9 @@ struct gm_engine {
     // solve workspaces
     gm::DevBuf d_x, d_b, d_r, d_t, d_w, d_part, d_norm;
     gm::DevBuf d_fmap;                          // matrices still refined (device list)
+    // GMRES-IR: Krylov vectors [m+1][ng][n][nrhs] c128, preconditioned
+    // vectors [m][ng][n][nrhs] (working precision), reductions, coefficients
+    gm::DevBuf d_gv, d_gz, d_gpart, d_gnorm, d_gcoef, d_gmap;
     std::vector<int> h_fmap;                    // its host copy (kept alive for async uploads)
     std::vector<gm_refine_info> refine_info;    // per matrix, of the last solve
 
@@ -104,6 +107,8 @@ struct gm_engine {
     std::vector<double> last_grad0, last_grad1;
     // per-shot gradient taper of ass_grad (SWS_TAPER_CIRCULAR_PER_SHOT 0, 1, 2),
     // its radius (SRTRADIUS, metres) and square half-width (FILTSIZE)
+    int invmat = 1;               // INVMAT of calc_res_AC: 1 FWI residuals, 2 RTM (observed data)
+    std::vector<float> wavelet;   // [nf][2] source amplitudes of READ_WAVELET = 1 (empty: spikes)
     int shot_taper = 0;
     float srt_radius = 0.0f;
     int filtsize = 0;

@@ -81,9 +81,13 @@ int forward_solve(gm_engine *e, int ns, const Geometry &g, double2 *xout, int sr
     const int nf = e->nf, n = e->n;
     if (!src_physics) src_physics = e->cfg.physics;
     std::vector<double2> amp(nf);
+    if (!e->wavelet.empty() && e->wavelet.size() != 2 * (size_t)nf)
+        return fail(GM_ERROR_STATE, "the source wavelet holds %d amplitudes, the batch %d matrices",
+                    (int)(e->wavelet.size() / 2), nf);
     for (int f = 0; f < nf; ++f) {
         double a[2];
-        gmh_source_amp(src_physics, e->freqs[f], e->cfg.s, e->cfg.dh, a);
+        if (e->wavelet.empty()) gmh_source_amp(src_physics, e->freqs[f], e->cfg.s, e->cfg.dh, a);
+        else gmh_wavelet_amp(&e->wavelet[2 * (size_t)f], e->cfg.dh, a);
         amp[f] = make_double2(a[0], a[1]);
     }
     int rc;
@@ -168,7 +172,7 @@ int residuals(gm_engine *e, int ns, int ntr, const float *pobs, int stf_inv, int
     double2 *stf = reinterpret_cast<double2 *>(l2p + nfs + (nfs & 1));
     GM_CUDA(cudaMemcpyAsync(obs, pobs, cnt * sizeof(float2), cudaMemcpyDefault, e->st));
     double2 *cal = e->d_res.as<double2>(), *res = cal + cnt;
-    gm::launch_residual_shot(cal, obs, nfs, ntr, stf_inv, misfit, res, l2p, stf, e->st);
+    gm::launch_residual_shot(cal, obs, nfs, ntr, stf_inv, misfit, e->invmat, res, l2p, stf, e->st);
     GM_CUDA(cudaGetLastError());
     std::vector<double> l2h(nfs);
     std::vector<double2> stfh(nfs);
@@ -314,6 +318,26 @@ int shot_taper_tables(gm_engine *e, int ns, const float *sx, const float *sy, in
 }
 
 }  // namespace
+
+extern "C" int gm_set_invmat(gm_engine *e, int invmat) {
+    if (!e) return fail(GM_ERROR_INVALID, "gm_set_invmat: no engine");
+    if (invmat != 1 && invmat != 2) return fail(GM_ERROR_INVALID, "gm_set_invmat: INVMAT must be 1 (FWI) or 2 (RTM)");
+    e->invmat = invmat;
+    return GM_OK;
+}
+
+extern "C" int gm_set_source_wavelet(gm_engine *e, int nmat, const float *amp) {
+    if (!e) return fail(GM_ERROR_INVALID, "gm_set_source_wavelet: no engine");
+    if (!amp) {
+        e->wavelet.clear();
+        return GM_OK;
+    }
+    if (nmat <= 0) return fail(GM_ERROR_INVALID, "gm_set_source_wavelet: need at least one amplitude");
+    for (int i = 0; i < 2 * nmat; ++i)
+        if (!std::isfinite(amp[i])) return fail(GM_ERROR_INVALID, "gm_set_source_wavelet: amplitude %d is not finite", i / 2);
+    e->wavelet.assign(amp, amp + 2 * (size_t)nmat);
+    return GM_OK;
+}
 
 extern "C" int gm_set_shot_taper(gm_engine *e, int mode, float srtradius, int filtsize) {
     if (!e) return fail(GM_ERROR_INVALID, "gm_set_shot_taper: no engine");

@@ -79,11 +79,13 @@ void launch_field(const double2 *x, int n, int nf, int ns, float2 *field, cudaSt
 }
 
 // Residuals of one (frequency, shot) per CTA: optional Wiener source
-// estimate, MISFIT 1/2/3, the reference's zeroing of the adjoint source
-// where both observed parts are below 1e-20, and the misfit partial sum
-// (counted before the zeroing, as calc_res_AC.c:82-88 does).
+// estimate, MISFIT 1/2/3 (INVMAT = 1) or the observed data itself
+// (INVMAT = 2, the RTM branch of calc_res_AC.c:77), the reference's zeroing
+// of the adjoint source where both observed parts are below 1e-20, and the
+// misfit partial sum (counted before the zeroing, as calc_res_AC.c:82-88
+// does).
 __global__ void k_residual_shot(const double2 *cal, const float2 *obs, int ntr, int stf_inv, int misfit,
-                                double2 *res, double *l2, double2 *stf) {
+                                int invmat, double2 *res, double *l2, double2 *stf) {
     const int fs = blockIdx.x;
     const double2 *c = cal + (size_t)fs * ntr;
     const float2 *o = obs + (size_t)fs * ntr;
@@ -116,7 +118,9 @@ __global__ void k_residual_shot(const double2 *cal, const float2 *obs, int ntr, 
         const double2 cv = c[t];
         const double2 ov = make_double2(o[t].x, o[t].y);
         double2 r;
-        if (misfit == 2) {
+        if (invmat == 2) {
+            r = ov;
+        } else if (misfit == 2) {
             // clog(obs) - clog(cal)
             r = make_double2(log(hypot(ov.x, ov.y)) - log(hypot(cv.x, cv.y)), atan2(ov.y, ov.x) - atan2(cv.y, cv.x));
         } else if (misfit == 3) {
@@ -142,8 +146,8 @@ __global__ void k_residual_shot(const double2 *cal, const float2 *obs, int ntr, 
 }
 
 void launch_residual_shot(const double2 *cal, const float2 *obs, int nfs, int ntr, int stf_inv, int misfit,
-                          double2 *res, double *l2, double2 *stf, cudaStream_t st) {
-    (k_residual_shot<<<nfs, 256, 0, st>>>(cal, obs, ntr, stf_inv, misfit, res, l2, stf), note_launch());
+                          int invmat, double2 *res, double *l2, double2 *stf, cudaStream_t st) {
+    (k_residual_shot<<<nfs, 256, 0, st>>>(cal, obs, ntr, stf_inv, misfit, invmat, res, l2, stf), note_launch());
 }
 
 // Adjoint sources conj(res)/DH^2 at the receivers; receivers sharing a grid

@@ -24,14 +24,20 @@
 //                alike): the interior layout of writemod_true, extended into
 //                the PML frame by copying the nearest interior value (left /
 //                right columns, then top rows unless FREE_SURF, then bottom
-//                rows).
+//                rows);
+//   source wavelet  the SU trace read_stf_dft reads (src/read_stf_dft.c:
+//                24-52): a 240-byte trace header (sample count and
+//                interval as unsigned shorts at bytes 114 and 116), then the
+//                samples as floats (gm_stf_dft).
 // Host code only (plain stdio); grids are flat row-major [NY][NX] over the
 // full grid including the frame.
 #include <cstdio>
+#include <cstring>
 #include <vector>
 
 #include "common.hpp"
 #include "germaine_gpu.h"
+#include "host_setup.h"
 
 namespace {
 
@@ -142,5 +148,24 @@ extern "C" int gm_read_grid(const char *path, int nx, int ny, float *grid) {
             return gm::fail(GM_ERROR_INVALID, "gm_read_grid: %s holds fewer than %d x %d floats", path, nx, ny);
         for (int j = 0; j < ny; ++j) grid[(size_t)j * nx + i] = col[j];
     }
+    return GM_OK;
+}
+
+extern "C" int gm_stf_dft(const char *path, int physics, float freq, float *amp) {
+    if (!path || !amp) return gm::fail(GM_ERROR_INVALID, "gm_stf_dft: bad argument");
+    if (physics < 1 || physics > 4) return gm::fail(GM_ERROR_INVALID, "gm_stf_dft: unknown physics %d", physics);
+    File fp(path, "rb");
+    if (!fp.f) return gm::fail(GM_ERROR_INVALID, "gm_stf_dft: cannot open %s", path);
+    unsigned char hdr[240];
+    if (std::fread(hdr, 1, sizeof hdr, fp.f) != sizeof hdr)
+        return gm::fail(GM_ERROR_INVALID, "gm_stf_dft: %s has no 240-byte SU trace header", path);
+    unsigned short ns = 0, ndt = 0;
+    std::memcpy(&ns, hdr + 114, sizeof ns);
+    std::memcpy(&ndt, hdr + 116, sizeof ndt);
+    if (ns == 0) return gm::fail(GM_ERROR_INVALID, "gm_stf_dft: %s holds no samples", path);
+    std::vector<float> w(ns);
+    if (std::fread(w.data(), sizeof(float), ns, fp.f) != ns)
+        return gm::fail(GM_ERROR_INVALID, "gm_stf_dft: %s holds fewer than %d samples", path, (int)ns);
+    gmh_stf_dft(w.data(), (int)ns, (int)ndt, physics, freq, amp);
     return GM_OK;
 }

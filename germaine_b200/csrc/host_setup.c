@@ -108,6 +108,39 @@ void gmh_source_amp(int physics, float freq, float s, float dh, double amp[2])
     amp[1] = ai / (dh * dh);
 }
 
+/* Spike amplitude of an external source wavelet (READ_WAVELET = 1): the
+ * float amplitude read_stf_dft returns, over DH^2 in float as RHS_source_AC
+ * / RHS_source_TE divide it (src/AC/RHS_source_AC.c:40-55). */
+void gmh_wavelet_amp(const float a[2], float dh, double amp[2])
+{
+    amp[0] = a[0] / (dh * dh);
+    amp[1] = a[1] / (dh * dh);
+}
+
+/* The DFT of read_stf_dft (src/read_stf_dft.c:24-71) at one frequency, in
+ * its float / double evaluation order: t = (j - 1) dt in float, each term
+ * w_j cos(2 t f pi) dt in double added to the float sum.  The reference
+ * copies the trace samples one place down (wavelet[j] = data[j] for
+ * j = 1 .. ns, from data[0 .. ns - 1] read), so the DFT uses samples 1 ..
+ * ns - 1 of the file, at times 0 .. (ns - 2) dt, and a last sample read
+ * from beyond the ones in the file; that sample is taken as 0 here.
+ * dt = sample interval [mus] / 1e6 (PHYSICS <= 3) or [ns] / 1e12 (TE). */
+void gmh_stf_dft(const float *samples, int ns, int ndt, int physics, float freq, float amp[2])
+{
+    float dt, t, w;
+    int j;
+    if (physics <= 3) dt = ndt / 1e6;
+    else dt = ndt / 1e12;
+    amp[0] = 0.0;
+    amp[1] = 0.0;
+    for (j = 1; j <= ns; j++) {
+        w = j < ns ? samples[j] : 0.0f;
+        t = (j - 1) * dt;
+        amp[0] += w * cos(2.0 * t * freq * M_PI) * dt;
+        amp[1] += w * sin(2.0 * t * freq * M_PI) * dt;
+    }
+}
+
 /* Amplitude of the receiver spike of the Hessian's Green's functions:
  * AC amp/(DH*DH) with float amp = 1 (src/AC/RHS_source_AC_hess.c:26-33, a
  * float quotient); TE 1.0/(DH*DH) (src/TE/RHS_source_TE_hess.c:38, a double

@@ -9,6 +9,8 @@ void gmh_pml(int nx, int ny, float dh, int npml, int free_surf, float a0_pml, fl
              float freq, float *out);
 void gmh_assembly_scalars(int physics, float freq, float s, float om2[2], float om[2], float om2mu0[2]);
 void gmh_source_amp(int physics, float freq, float s, float dh, double amp[2]);
+void gmh_wavelet_amp(const float a[2], float dh, double amp[2]);
+void gmh_stf_dft(const float *samples, int ns, int ndt, int physics, float freq, float amp[2]);
 void gmh_gradient_scalars(int physics, float freq, float s, float om2[2], float om[2]);
 double gmh_hess_green_amp(int physics, float dh);
 void gmh_stf_unit(const float stf[2], float unit[2]);

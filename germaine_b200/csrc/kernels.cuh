@@ -127,9 +127,11 @@ struct SolveArgs {
     // node v's subtree, so that node's y and update vector are zero
     const unsigned char *mask;
     int mask_nch;
-    // matrices of this launch: fmap[0 .. nfz) (NULL: all nf, in order)
+    // matrices of this launch: fmap[0 .. nfz) (NULL: all nf, in order);
+    // xmap[j]: slot of x / w for launch position j (NULL: the matrix index)
     const int *fmap;
     int nfz;
+    const int *xmap;
 };
 
 template <class R>
@@ -154,6 +156,10 @@ struct ResidArgs {
     // partial sums and norms are indexed by the position in fmap
     const int *fmap;
     int nfz;
+    // slots of x and of the output for launch position j (NULL: the
+    // matrix index itself): xmap[j], omap[j]
+    const int *xmap;
+    const int *omap;
 };
 // r = b - M x and per-(freq, rhs) partial sums of |r|^2 and |b|^2 into
 // part[nblk][nfz][nrhs][2]; returns nblk.
@@ -176,6 +182,29 @@ void launch_add_up(double2 *x, const void *d, size_t count, cudaStream_t st);
 // x[f] += d[f] for the matrices f = fmap[0 .. nfz) (device list), per_f entries each
 template <class R>
 void launch_add_up_f(double2 *x, const void *d, size_t per_f, const int *fmap, int nfz, cudaStream_t st);
+
+// ---------------- K6b GMRES-IR vector kernels ----------------
+// Vectors [slot][n][nrhs]; j indexes the launch's list (zmap: slots, fmap:
+// matrices of the batch); per-column coefficient arrays are
+// [j][nrhs][kGmresStride] complex.
+constexpr int kGmresMaxRestart = 8;
+constexpr int kGmresStride = kGmresMaxRestart + 1;
+// Z[zmap[j]] = (R)(V[zmap[j]] * s[j][r])
+template <class R>
+void launch_scale_down(const double2 *V, void *Z, const double *s, const int *zmap, int nj, int n, int nrhs,
+                       cudaStream_t st);
+// part[blk][j][r][0 .. nv] = partial sums of conj(V_i) W (i < nv) and |W|^2;
+// V_i = V + i * vstride; returns the number of row blocks
+int launch_dots(const double2 *V, size_t vstride, int nv, const double2 *W, const int *zmap, int nj, int n, int nrhs,
+                double *part, cudaStream_t st);
+// W -= sum_i coef[j][r][i] V_i; part[blk][j][r] = partial sums of |W|^2
+int launch_gs_update(const double2 *V, size_t vstride, int nv, double2 *W, const double2 *coef, const int *zmap,
+                     int nj, int n, int nrhs, double *part, cudaStream_t st);
+// x[fmap[j]] += sum_{i < nz} y[j][r][i] Z_i[zmap[j]]
+template <class R>
+void launch_x_update(double2 *x, const void *Z, size_t zstride, int nz, const double2 *y, const int *fmap,
+                     const int *zmap, int nj, int n, int nrhs, cudaStream_t st);
+void preload_gmres_kernels();
 
 // Load every substitution / refinement kernel now (lazy module loading
 // would otherwise load each on its first launch, taking device memory).

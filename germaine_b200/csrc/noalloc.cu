@@ -101,6 +101,7 @@ int noalloc_prepare(int device) {
     if (rc) return rc;
     preload_solve_kernels();
     preload_refine_kernels();
+    preload_gmres_kernels();
     const cudaError_t err = cudaGetLastError();
     if (err != cudaSuccess) return fail(GM_ERROR_CUDA, "loading the solve kernels failed: %s", cudaGetErrorString(err));
     return GM_OK;

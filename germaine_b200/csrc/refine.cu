@@ -54,8 +54,10 @@ __global__ void __launch_bounds__(RLANES *RGRP, 3) k_residual(ResidArgs a, const
     __syncthreads();
     double rr = 0.0, bb = 0.0;
     if (r < a.nrhs) {
-        const size_t base = (size_t)f * a.n * a.ldr + r;
-        const InC *X = xin + base;
+        const size_t per = (size_t)a.n * a.ldr;
+        const size_t base = (size_t)f * per + r;
+        const InC *X = xin + (size_t)(a.xmap ? a.xmap[fz] : f) * per + r;
+        OutC *O = out ? out + (size_t)(a.omap ? a.omap[fz] : f) * per + r : nullptr;
         const bool spikes = !PRODUCT && a.spike_k;
         const int ks = spikes ? a.spike_k[r] : -1;
         const double2 amp = spikes ? a.spike_amp[f] : make_double2(0.0, 0.0);
@@ -74,7 +76,7 @@ __global__ void __launch_bounds__(RLANES *RGRP, 3) k_residual(ResidArgs a, const
                 cfms(acc, cf[q][i], cto_d(X[(size_t)(k + dx + dy * a.nx) * a.ldr]));
             }
             if (PRODUCT) acc = make_double2(-acc.x, -acc.y);
-            if (WRITE) out[base + (size_t)k * a.ldr] = cconv<OutC>(acc);
+            if (WRITE) O[(size_t)k * a.ldr] = cconv<OutC>(acc);
             rr += acc.x * acc.x + acc.y * acc.y;
             bb += bv.x * bv.x + bv.y * bv.y;
         }

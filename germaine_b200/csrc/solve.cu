@@ -182,6 +182,11 @@ template <class R>
 __device__ __forceinline__ size_t solve_matrix(const SolveArgs<R> &a) {
     return a.fmap ? (size_t)a.fmap[blockIdx.z] : (size_t)blockIdx.z;
 }
+// slot of x and of the workspace w used by this CTA
+template <class R>
+__device__ __forceinline__ size_t solve_slot(const SolveArgs<R> &a) {
+    return a.xmap ? (size_t)a.xmap[blockIdx.z] : solve_matrix(a);
+}
 
 template <class R>
 struct Ctx {
@@ -202,11 +207,11 @@ __device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first,
     c.s = a.s.npiv[c.node];
     const int r0 = chunk * TC;
     c.rn = min(TC, a.nrhs - r0);
-    const size_t fz = solve_matrix(a);
+    const size_t fz = solve_matrix(a), xz = solve_slot(a);
     c.F = reinterpret_cast<const C *>(a.front) + fz * a.s.front_total + a.s.front_off[c.node];
     c.vars = a.s.vars + a.s.var_off[c.node];
-    c.X = reinterpret_cast<C *>(a.x) + fz * (size_t)a.s.n * a.ldr + r0;
-    c.W = reinterpret_cast<C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + r0 + (size_t)a.s.rhs_off[c.node] * a.ldr;
+    c.X = reinterpret_cast<C *>(a.x) + xz * (size_t)a.s.n * a.ldr + r0;
+    c.W = reinterpret_cast<C *>(a.w) + xz * (size_t)a.s.rhs_total * a.ldr + r0 + (size_t)a.s.rhs_off[c.node] * a.ldr;
     return c;
 }
 
@@ -227,8 +232,8 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
     const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int *inv = a.s.inv + a.s.inv_off[c.node];
-    const size_t fz = solve_matrix(a);
-    const C *Wall = reinterpret_cast<const C *>(a.w) + fz * (size_t)a.s.rhs_total * a.ldr + r0;
+    const size_t xz = solve_slot(a);
+    const C *Wall = reinterpret_cast<const C *>(a.w) + xz * (size_t)a.s.rhs_total * a.ldr + r0;
     const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
     const C *W0 = c0 >= 0 && live(a, c0, r0, c.rn) ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
     const C *W1 = c1 >= 0 && live(a, c1, r0, c.rn) ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
@@ -312,7 +317,7 @@ __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, 
     }
     // w = (children's update vectors at the ring rows) - L'(ring, piv) y
     const int *inv = a.s.inv + a.s.inv_off[c.node];
-    const C *Wall = reinterpret_cast<const C *>(a.w) + solve_matrix(a) * a.s.rhs_total * a.ldr + chunk * TC;
+    const C *Wall = reinterpret_cast<const C *>(a.w) + solve_slot(a) * a.s.rhs_total * a.ldr + chunk * TC;
     const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
     const C *W0 = c0 >= 0 && live(a, c0, chunk * TC, c.rn) ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
     const C *W1 = c1 >= 0 && live(a, c1, chunk * TC, c.rn) ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;

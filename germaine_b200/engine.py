@@ -46,10 +46,10 @@ class Engine:
     def __init__(self, nx: int, ny: int, dh: float, npml: int, physics: int = GM_PHYS_AC,
                  precision: int = GM_PREC_FP64, op_mode: int = GM_OP_REF, free_surf: int = 0,
                  a0_pml: float = 90.0, s: float = 0.0, device: int = 0, leaf_max: int = 32,
-                 ir_tol: float = 1e-10, ir_max_iter: int = 10):
+                 ir_tol: float = 1e-10, ir_max_iter: int = 10, refine: int = 0, gmres_restart: int = 0):
         self.lib = _lib.load()
         self.cfg = GmConfig(nx, ny, dh, npml, free_surf, a0_pml, s, physics, precision, op_mode, leaf_max,
-                            ir_tol, ir_max_iter)
+                            ir_tol, ir_max_iter, refine, gmres_restart)
         self.nx, self.ny, self.n = nx, ny, nx * ny
         self.physics = physics
         self._h = ctypes.c_void_p()
@@ -214,6 +214,21 @@ class Engine:
                                                       stf_inv, misfit, ptr(g0), ptr(g1), ctypes.byref(l2),
                                                       ptr(seis)))
         return g0, g1, float(l2.value), seis
+
+    def set_invmat(self, invmat: int) -> None:
+        """INVMAT of the residuals of the following grad_obj / obj calls:
+        1 FWI (default), 2 RTM (residual = observed data)."""
+        check(self.lib.gm_set_invmat(self._h, invmat))
+
+    def set_source_wavelet(self, amp) -> None:
+        """Per-matrix complex source amplitudes of an external wavelet
+        (READ_WAVELET = 1; amp: nmat complex values, e.g. from stf_dft), or
+        None for spike sources."""
+        if amp is None:
+            check(self.lib.gm_set_source_wavelet(self._h, 0, None))
+            return
+        a = _c(np.asarray(amp, np.complex64).reshape(-1).view(np.float32), np.float32)
+        check(self.lib.gm_set_source_wavelet(self._h, a.size // 2, ptr(a)))
 
     def set_shot_taper(self, mode: int, srtradius: float = 0.0, filtsize: int = 0) -> None:
         """Per-shot gradient taper of the following grad_obj calls
@@ -434,3 +449,12 @@ def gauss_filt(grad, dh: float, vref: float, fc_low: float, filt_size_grad: floa
     check(_lib.load().gm_gauss_filt(device, nx, ny, dh, vref, fc_low, filt_size_grad, filt_size_grad1, ptr(g),
                                     ptr(out)))
     return out
+
+
+def stf_dft(path: str, physics: int, freq: float) -> complex:
+    """read_stf_dft on the host (gm_stf_dft): the complex64 amplitude of the
+    SU wavelet at path for frequency freq, float-identical to the
+    reference's."""
+    amp = np.zeros(2, np.float32)
+    check(_lib.load().gm_stf_dft(str(path).encode(), physics, freq, ptr(amp)))
+    return complex(np.complex64(amp[0] + 1j * amp[1]))

@@ -73,7 +73,16 @@ typedef struct {
     int32_t leaf_max;        /* nested-dissection leaf size (0 = default 32) */
     double ir_tol;           /* refinement target on max_k ||b_k - M x_k|| / ||b_k|| (0 = 1e-10) */
     int32_t ir_max_iter;     /* refinement iteration cap (0 = default 10) */
+    int32_t refine;          /* GM_REFINE_MODE_* (0 = auto) */
+    int32_t gmres_restart;   /* GMRES iterations per cycle (0 = default 8, at most 8) */
 } gm_config;
+
+/* ---- refinement of the solves (gm_config.refine) ---- */
+#define GM_REFINE_MODE_AUTO  0  /* iterative refinement; a matrix whose first sweep contracts
+                                   too slowly to meet the target within two more sweeps
+                                   continues with GMRES-IR */
+#define GM_REFINE_MODE_IR    1  /* classical iterative refinement only */
+#define GM_REFINE_MODE_GMRES 2  /* GMRES-IR for every matrix that needs refinement */
 
 /* Statistics of the last factor/solve (host-side copy). */
 typedef struct {
@@ -211,6 +220,35 @@ int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const float *src_y
                 int ntr, const int32_t *rec_x, const int32_t *rec_y,
                 const float *pobs, int stf_inv, int misfit,
                 float *grad0, float *grad1, float *l2, float *seis);
+
+/* INVMAT of calc_res_AC (src/AC/calc_res_AC.c:74-77) for the following
+ * gm_grad_obj / gm_obj / gm_obj_each calls: 1 (the default) forms FWI data
+ * residuals (MISFIT 1/2/3); 2 makes the residual the observed data itself,
+ * the RTM branch that RTM_FD_AC reaches through grad_obj_AC
+ * (src/AC/RTM_FD_AC.c:190), so that gm_grad_obj returns the RTM image.
+ * The adjoint-source zeroing of tiny observed samples and the misfit sum
+ * apply in both modes, as in the reference. */
+int gm_set_invmat(gm_engine *e, int invmat);
+
+/* External source wavelet (READ_WAVELET = 1, src/AC/RHS_source_AC.c:40-42,
+ * src/TE/RHS_source_TE.c:44-46): amp [nmat][2] holds, per factorised matrix,
+ * the complex float amplitude that read_stf_dft returns for its frequency
+ * (gm_stf_dft computes it from the SU file); the spikes of gm_forward,
+ * gm_obj, gm_obj_each, gm_grad_obj and the forward fields of gm_hessian are
+ * then amp / DH^2 instead of 1 / DH^2 (AC, SH) or -i Omega mu0 / DH^2 (TE).
+ * nmat must match the batch at solve time (GM_ERROR_STATE otherwise).
+ * amp = NULL restores the spike wavelet. */
+int gm_set_source_wavelet(gm_engine *e, int nmat, const float *amp);
+
+/* read_stf_dft (src/read_stf_dft.c:12-73) on the host: the SU trace at path
+ * (wavelet samples, interval in microseconds for physics <= 3, in
+ * nanoseconds for TE) Fourier-transformed at freq, amp[0..1] = real and
+ * imaginary part, float results identical to the reference's.  As in the
+ * reference the samples enter one place down: the DFT uses samples 1 .. ns-1
+ * of the file at times 0, dt, ...; the reference's last term reads one
+ * sample past those in the file (whatever its buffer held), taken as 0
+ * here.  No GPU needed. */
+int gm_stf_dft(const char *path, int physics, float freq, float *amp);
 
 /* Per-shot gradient taper applied by gm_grad_obj inside its shot stack
  * (SWS_TAPER_CIRCULAR_PER_SHOT of ass_grad_AC / ass_grad_TE,

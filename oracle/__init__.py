@@ -143,6 +143,7 @@ def load_ref():
         lib.ref_calc_seis.argtypes = [_f32p, _f32p, ctypes.c_int, _i32p, _i32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p]
         lib.ref_calc_res.argtypes = [_f32p, _f32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int, _f32p, _f32p, _f32p]
         lib.ref_calc_res.restype = ctypes.c_float
+        lib.ref_read_stf_dft.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_float, _f32p]
         lib.ref_rhs_adj.argtypes = [_f32p, _f32p, ctypes.c_int, _i32p, _i32p, _f64p, _f64p]
         lib.ref_ass_grad_ac.argtypes = [ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
         lib.ref_ass_grad_te.argtypes = [ctypes.c_float, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p, _f32p]
@@ -504,6 +505,7 @@ class RefDropin:
         lib.dropin_grad_obj_ac.argtypes = [ctypes.c_int, _f32p, _f32p, _f32p, ctypes.c_int, _f32p, _f32p, ctypes.c_int,
                                            _i32p, _i32p, _f32p, _f32p, ctypes.c_int, ctypes.c_int, _f32p]
         lib.dropin_grad_obj_ac.restype = ctypes.c_float
+        lib.dropin_set_invmat.argtypes = [ctypes.c_int]
         cp, i = ctypes.c_char_p, ctypes.c_int
         lib.dropin_hessian_ac.argtypes = [i, i, _f32p, _f32p, _f32p, i, _f32p, _f32p, i, _i32p, _i32p, cp, _f32p]
         lib.dropin_hessian_te.argtypes = [i, i, _f32p, _f32p, _f32p, i, _f32p, _f32p, i, _i32p, _i32p, cp, _f32p,
@@ -519,11 +521,12 @@ class RefDropin:
                                         np.ascontiguousarray(rx, np.int32), np.ascontiguousarray(ry, np.int32), sr, si)
         return (sr + 1j * si).reshape(ns, ntr).astype(np.complex64)
 
-    def grad_obj_ac(self, freqs, vp, rho, xs, ys, rx, ry, obs, stf_inv=0, misfit=1):
+    def grad_obj_ac(self, freqs, vp, rho, xs, ys, rx, ry, obs, stf_inv=0, misfit=1, invmat=1):
         """(gradient [NY][NX] float32, L2) of grad_obj_AC over one stage."""
         nf, ns, ntr = len(freqs), len(xs), len(rx)
         obs = np.asarray(obs, np.complex64).reshape(nf, ns, ntr)
         grad = np.zeros(self.g.n, np.float32)
+        self.lib.dropin_set_invmat(invmat)
         l2 = self.lib.dropin_grad_obj_ac(nf, _f32(freqs), _f32(vp).ravel(), _f32(rho).ravel(), ns, _f32(xs),
                                          _f32(ys), ntr, np.ascontiguousarray(rx, np.int32),
                                          np.ascontiguousarray(ry, np.int32), _f32(obs.real).ravel(),
@@ -633,3 +636,13 @@ class RefLbfgs:
 
     def rotate(self):
         self.lib.ref_lbfgs_rotate(self.m, self.nvec, self.y, self.s)
+
+
+def ref_stf_dft(path: str, physics: int, freq: float) -> complex:
+    """The reference's read_stf_dft (oracle/_ref) on the SU file at path:
+    the complex64 amplitude at freq."""
+    import numpy as np
+    lib = load_ref()
+    amp = np.zeros(2, np.float32)
+    lib.ref_read_stf_dft(str(path).encode(), physics, freq, amp)
+    return complex(np.complex64(amp[0] + 1j * amp[1]))

@@ -110,6 +110,11 @@ void dropin_forward_shot_ac(float freq, const float *vp, const float *rho, int n
     free_wave(&w, &p, &m);
 }
 
+/* INVMAT for the next dropin_grad_obj_ac calls: 1 FWI (default), 2 RTM
+ * (calc_res_AC takes the observed data as residual, as under RTM_FD_AC). */
+static int dropin_invmat = 1;
+void dropin_set_invmat(int invmat) { dropin_invmat = invmat; }
+
 /* grad_obj_AC over the frequencies freqs[0..nf) (one stage): observed data
  * pobs and modelled data prec are [nf][nshots][ntr]; the frame-tapered
  * gradient (NY x NX, row-major) goes to grad, the objective is returned. */
@@ -121,7 +126,7 @@ float dropin_grad_obj_ac(int nf, const float *freqs, const float *vp, const floa
     float **srcpos, l2, *precr, *preci, *stage;
     int i, j;
     driver_globals(nshots, nf);
-    STF_INV = stf_inv; MISFIT = misfit; INVMAT = 1;
+    STF_INV = stf_inv; MISFIT = misfit; INVMAT = dropin_invmat;
     NFREQ1 = 1; NFREQ2 = nf + 1;
     alloc_wave(&w, &p, &m, vp, rho);
     precr = calloc((size_t)nf * nshots * ntr, sizeof(float));

@@ -86,15 +86,18 @@ def spike_rhs(g: Grid, physics: int, freq: float, xs, ys, port: Port | None = No
     return B
 
 
-def residual_fp64(cal, obs, stf_inv: int = 0, misfit: int = 1):
-    """calc_res_AC in double for one shot: returns (l2, res, wien)."""
+def residual_fp64(cal, obs, stf_inv: int = 0, misfit: int = 1, invmat: int = 1):
+    """calc_res_AC in double for one shot: returns (l2, res, wien); invmat 2
+    is the RTM branch (residual = observed data, src/AC/calc_res_AC.c:77)."""
     cal = np.asarray(cal, np.complex128)
     obs_c = np.asarray(obs, np.complex64)
     o = obs_c.astype(np.complex128)
     w = 1.0 + 0j
     if stf_inv:
         w = np.sum(np.conj(cal) * o) / np.sum(np.conj(o) * o)
-    if misfit == 1:
+    if invmat == 2:
+        res = o.copy()
+    elif misfit == 1:
         res = (o - w * cal) / abs(w)
     elif misfit == 2:
         res = np.log(o) - np.log(cal)

@@ -62,3 +62,25 @@ def test_reference_grad_obj_ac_on_gpu(stf_inv):
     assert _rel(grad.ravel(), r0) < 1e-5
     if stf_inv == 1:   # with STF_INV = 0 the reference's misfit accumulator is uninitialised
         assert abs(l2 - rl2) / rl2 < 1e-5
+
+
+def test_reference_grad_obj_ac_rtm_on_gpu():
+    """RTM_FD_AC's call of grad_obj_AC (INVMAT = 2, src/AC/RTM_FD_AC.c:190):
+    the unmodified reference driver through the UMFPACK shim against the
+    engine's own INVMAT = 2 path and the FP64 oracle."""
+    from germaine_b200 import Engine
+    g, vp, rho, xs, ys, rx, ry = _case(seed=2)
+    freqs = [7.0, 13.0]
+    obs = _observed(g, O.PHYS_AC, vp, rho, freqs, xs, ys, rx, ry)
+    d = O.RefDropin(g)
+    grad, l2 = d.grad_obj_ac(freqs, vp, rho, xs, ys, rx, ry, obs, stf_inv=1, invmat=2)
+    d.lib.dropin_set_invmat(1)
+    r0, _, rl2 = oracle_grad(g, O.PHYS_AC, vp, rho, freqs, xs, ys, rx, ry, obs, 1, 1, invmat=2)
+    assert _rel(grad.ravel(), r0) < 1e-5
+    assert abs(l2 - rl2) / rl2 < 1e-5
+    with Engine(g.nx, g.ny, g.dh, g.npml) as e:
+        e.set_model(vp, rho)
+        e.factor(freqs)
+        e.set_invmat(2)
+        g0, _, _, _ = e.grad_obj(xs, ys, rx, ry, obs, stf_inv=1)
+    assert _rel(g0, grad.ravel()) < 1e-5

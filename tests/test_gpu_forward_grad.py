@@ -84,7 +84,7 @@ def test_forward_field_layout_matches_reference_vec2mat():
         assert np.array_equal(field[0][s].real, pr) and np.array_equal(field[0][s].imag, pi)
 
 
-def oracle_grad(g, physics, m0, m1, freqs, xs, ys, rx, ry, obs, stf_inv, misfit, taper=None):
+def oracle_grad(g, physics, m0, m1, freqs, xs, ys, rx, ry, obs, stf_inv, misfit, taper=None, invmat=1):
     X, solvers = oracle_forward(g, physics, m0, m1, freqs, xs, ys)
     idx = [OS.receiver_read_index(g, int(a), int(b)) for a, b in zip(rx, ry)]
     kadj = [OS.adjoint_index(g, int(a), int(b)) for a, b in zip(rx, ry)]
@@ -96,7 +96,7 @@ def oracle_grad(g, physics, m0, m1, freqs, xs, ys, rx, ry, obs, stf_inv, misfit,
         fld = OS.vec2mat(X[i].T)
         Badj = np.zeros((g.n, len(xs)), complex)
         for s in range(len(xs)):
-            li, res, w = OS.residual_fp64(fld[s, idx], obs[i, s], stf_inv, misfit)
+            li, res, w = OS.residual_fp64(fld[s, idx], obs[i, s], stf_inv, misfit, invmat)
             l2 += li
             stfu[i, s] = w / abs(w)
             for t, k in enumerate(kadj):
@@ -234,3 +234,65 @@ def test_state_errors():
             e.forward(xs, ys, rx, ry)                # no factorisation yet
         with pytest.raises(GmError):
             e.factor([-1.0])
+
+
+@pytest.mark.parametrize("physics,stf_inv", [(GM_PHYS_AC, 0), (GM_PHYS_AC, 1), (GM_PHYS_TE, 0)],
+                         ids=["ac", "ac-stf", "te"])
+def test_rtm_image_invmat2(physics, stf_inv):
+    """INVMAT = 2 (RTM_FD_AC's use of grad_obj_AC): the residual is the
+    observed data (src/AC/calc_res_AC.c:77), back-propagated and stacked
+    like a gradient; misfit = 0.5 sum |obs|^2 of the non-zeroed samples."""
+    g, m0, m1, freqs, xs, ys, rx, ry = _case(physics, seed=6)
+    obs = _observed(g, physics, m0, m1, freqs, xs, ys, rx, ry)
+    with Engine(g.nx, g.ny, g.dh, g.npml, physics=physics, leaf_max=32) as e:
+        e.set_model(m0, m1)
+        e.factor(freqs)
+        e.set_invmat(2)
+        _, _, l2, _ = e.grad_obj(xs, ys, rx, ry, obs, stf_inv=stf_inv)
+        g0, g1 = e.gradient_fp64()
+        l2o = e.obj(xs, ys, rx, ry, obs, stf_inv=stf_inv)
+        e.set_invmat(1)
+        e.grad_obj(xs, ys, rx, ry, obs, stf_inv=stf_inv)
+        f0, _ = e.gradient_fp64()
+        with pytest.raises(GmError):
+            e.set_invmat(3)
+    r0, r1, rl2 = oracle_grad(g, physics, m0, m1, freqs, xs, ys, rx, ry, obs, stf_inv, 1, invmat=2)
+    assert _rel(g0, r0) < 1e-8
+    if physics == GM_PHYS_TE:
+        assert _rel(g1, r1) < 1e-8
+    assert abs(l2 - rl2) / rl2 < 2e-6 and abs(l2o - rl2) / rl2 < 2e-6
+    assert _rel(f0, g0) > 1e-3          # the FWI gradient differs
+
+
+@pytest.mark.parametrize("physics", [GM_PHYS_AC, GM_PHYS_TE], ids=["ac", "te"])
+def test_source_wavelet_amplitudes(physics):
+    """READ_WAVELET = 1: each frequency's spike carries the wavelet's DFT
+    amplitude over DH^2 (src/AC/RHS_source_AC.c:40-55), for the forward
+    fields and the gradient."""
+    g, m0, m1, freqs, xs, ys, rx, ry = _case(physics, seed=7)
+    amp = np.array([0.8 - 0.3j, -0.25 + 1.1j], np.complex64)[:len(freqs)]
+    with Engine(g.nx, g.ny, g.dh, g.npml, physics=physics, leaf_max=32) as e:
+        e.set_model(m0, m1)
+        e.factor(freqs)
+        e.set_source_wavelet(amp)
+        seis, _ = e.forward(xs, ys, rx, ry)
+        X = e.wavefield_fp64(0, len(xs))
+        e.set_source_wavelet(amp[:1])                # wrong count for the batch
+        with pytest.raises(GmError):
+            e.forward(xs, ys, rx, ry)
+        e.set_source_wavelet(None)
+        seis1, _ = e.forward(xs, ys, rx, ry)
+    port = O.Port(g)
+    dh2 = np.float32(g.dh) * np.float32(g.dh)
+    idx = [OS.receiver_read_index(g, int(a), int(b)) for a, b in zip(rx, ry)]
+    for i, f in enumerate(freqs):
+        A = OS.assembled_matrix(g, *port.assemble(physics, f, m0, m1))
+        ds = OS.DirectSolver(OS.operator(A))
+        B = np.zeros((g.n, len(xs)), complex)
+        for s in range(len(xs)):
+            k = OS.source_index(g, float(xs[s]), float(ys[s]))
+            B[k, s] = complex(np.float32(amp[i].real) / dh2, np.float32(amp[i].imag) / dh2)
+        Xr = ds.solve(B)
+        assert _rel(X[i], Xr) < 1e-10
+        assert _rel(seis[i], OS.vec2mat(Xr.T)[:, idx]) < 2e-6
+    assert _rel(seis1, seis) > 1e-2

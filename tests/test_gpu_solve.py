@@ -7,6 +7,7 @@ import oracle as O
 from oracle import sparse as OS
 from germaine_b200 import (GM_OP_EXACT, GM_OP_REF, GM_PHYS_AC, GM_PHYS_TE, GM_PREC_C64_IR, GM_PREC_FP64, GM_SYS_A,
                            GM_SYS_AT, Engine)
+from germaine_b200._lib import GM_REFINE_MODE_AUTO, GM_REFINE_MODE_GMRES, GM_REFINE_MODE_IR
 from tests.models import inclusion_ac, random_smooth, te_model
 
 pytestmark = pytest.mark.gpu
@@ -130,3 +131,41 @@ def test_fp64_refinement_sweeps():
     A = OS.assembled_matrix(g, *O.Port(g).assemble(1, 9.0, m0, m1))
     xr = OS.DirectSolver(OS.operator(A)).solve(b[0])
     assert _rel(x[0], xr) <= 1e-10
+
+
+@pytest.mark.parametrize("refine", [GM_REFINE_MODE_AUTO, GM_REFINE_MODE_IR, GM_REFINE_MODE_GMRES],
+                         ids=["auto", "ir", "gmres"])
+@pytest.mark.parametrize("sys_", [GM_SYS_A, GM_SYS_AT], ids=["A", "At"])
+def test_mixed_refinement_modes(refine, sys_):
+    """complex64 factors refined by plain sweeps, by GMRES-IR (FP64 Arnoldi,
+    complex64 factors as right preconditioner) or by the automatic choice;
+    every mode reaches the target and the SuperLU solution, and the
+    per-matrix report names the method and its sweeps."""
+    nx, ny, dh, npml = 90, 64, 10.0, 10
+    freqs = [3.0, 11.0, 24.0]
+    g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml)
+    m0, m1 = _setup(nx, ny, dh, npml, seed=21)
+    rng = np.random.default_rng(5)
+    nrhs = 37
+    b = rng.standard_normal((len(freqs), g.n, nrhs)) + 1j * rng.standard_normal((len(freqs), g.n, nrhs))
+    with Engine(nx, ny, dh, npml, precision=GM_PREC_C64_IR, leaf_max=24, refine=refine, gmres_restart=4) as e:
+        e.set_model(m0, m1)
+        e.factor(freqs)
+        x = e.solve(b, sys=sys_)
+        st = e.stats()
+        rep = e.refine_report()
+    assert st["ir_residual"] <= 1e-10
+    assert len(rep) == len(freqs)
+    port = O.Port(g)
+    for i, f in enumerate(freqs):
+        A = OS.assembled_matrix(g, *port.assemble(1, f, m0, m1))
+        ds = OS.DirectSolver(OS.operator(A))
+        xr = ds.solve(b[i], trans=(sys_ == GM_SYS_AT))
+        assert _rel(x[i], xr) <= 1e-8
+        r = rep[i]
+        assert r["final_residual"] <= 1e-10 < r["first_residual"]
+        assert r["sweeps"] >= 1
+        if refine == GM_REFINE_MODE_IR:
+            assert r["method"] == "ir"
+        if refine == GM_REFINE_MODE_GMRES:
+            assert r["method"] == "gmres"
