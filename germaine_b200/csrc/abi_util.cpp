@@ -46,3 +46,20 @@ extern "C" int gm_cgemm_sub_c64(int device, int backend, int nprob, const int32_
     cudaFree(derr);
     return rc;
 }
+
+extern "C" int gm_wait_probe(int device, long long polls, int *timed_out) {
+    if (!timed_out || polls < 1 || polls > (1ll << 24))
+        return gm::fail(GM_ERROR_INVALID, "gm_wait_probe: polls must be in 1 .. 2^24");
+    if (cudaSetDevice(device) != cudaSuccess) return gm::fail(GM_ERROR_CUDA, "gm_wait_probe: bad device");
+    int *d = nullptr;
+    if (cudaMalloc(&d, sizeof(int)) != cudaSuccess) return gm::fail(GM_ERROR_OUT_OF_MEMORY, "gm_wait_probe: allocation");
+    cudaMemset(d, 0xff, sizeof(int));
+    gm::launch_wait_probe(polls, d, 0);
+    cudaError_t e = cudaDeviceSynchronize();
+    int h = -1;
+    if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+    cudaFree(d);
+    if (e != cudaSuccess) return gm::fail(GM_ERROR_CUDA, "gm_wait_probe: %s", cudaGetErrorString(e));
+    *timed_out = h;
+    return GM_OK;
+}

@@ -464,8 +464,13 @@ static int factor_assembled(gm_engine *e) {
     float ms = 0;
     cudaEventElapsedTime(&ms, e->ev0, e->ev1);
     e->stats.ms_factor = ms;
-    unsigned long long np = 0;
+    unsigned long long np = 0, amax_bits = 0;
     GM_CUDA(cudaMemcpy(&np, e->d_npert.p, sizeof np, cudaMemcpyDeviceToHost));
+    GM_CUDA(cudaMemcpy(&amax_bits, e->d_amax.p, sizeof amax_bits, cudaMemcpyDeviceToHost));
+    double amax = 0;
+    std::memcpy(&amax, &amax_bits, sizeof amax);
+    if (!std::isfinite(amax))   // NaN bits order above every finite value in the max reduction
+        return fail(GM_ERROR_NONFINITE, "factor: the operator holds non-finite values (NaN or Inf material?)");
     int tcerr = 0;
     GM_CUDA(cudaMemcpy(&tcerr, e->d_tcerr.p, sizeof tcerr, cudaMemcpyDeviceToHost));
     if (tcerr) return fail(GM_ERROR_CUDA, "factor: a tensor-core wait timed out in the contribution-block update");

@@ -575,9 +575,12 @@ __global__ void __launch_bounds__(256) k_amax(const double2 *A, size_t cnt, unsi
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += (size_t)gridDim.x * blockDim.x) {
         const double2 v = A[i];
         const double a = hypot(v.x, v.y);
-        m = a > m ? a : m;   // NaN entries are skipped here; they surface as non-finite factors
+        m = (a > m || a != a) ? a : m;   // a NaN entry makes the maximum NaN (reported by the host)
     }
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
+    for (int o = 16; o > 0; o >>= 1) {
+        const double q = __shfl_xor_sync(0xffffffffu, m, o);
+        m = (q > m || q != q) ? q : m;
+    }
     if ((threadIdx.x & 31) == 0) atomicMax(out, (unsigned long long)__double_as_longlong(m));
 }
 

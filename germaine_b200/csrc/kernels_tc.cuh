@@ -14,6 +14,9 @@ using CgemmProb = GemmProb<float>;
 // tensor-core wait timed out.
 void launch_cgemm_sub(int backend, const CgemmProb *d_probs, const int4 *d_tiles, int ntiles, int *d_err,
                       cudaStream_t st);
+// one CTA waits, with the tensor-core kernels' bounded wait, on an mbarrier
+// that nothing signals; *d_status = 1 when the wait ran out (device memory)
+void launch_wait_probe(long long limit, int *d_status, cudaStream_t st);
 int cgemm_tile_rows();
 int cgemm_tile_cols();
 

@@ -102,8 +102,8 @@ __device__ __forceinline__ void mma_tf32(uint32_t d_tmem, uint64_t adesc, uint64
         : "memory");
 }
 
-__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity) {
-    for (long long it = 0; it < WAIT_LIMIT; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint32_t mbar, uint32_t parity, long long limit = WAIT_LIMIT) {
+    for (long long it = 0; it < limit; ++it) {
         uint32_t done;
         asm volatile(
             "{\n\t.reg .pred p;\n\t"
@@ -297,6 +297,27 @@ __global__ void __launch_bounds__(128) k_cgemm_cc(const CgemmProb *__restrict__ 
         c.x -= acc.x;
         c.y -= acc.y;
     }
+}
+
+// The bounded wait of k_cgemm_tc on an mbarrier that no thread ever
+// signals: phase 0 never completes, so the wait gives up after `limit`
+// polls and the kernel reports it in *status (1 = timed out, 0 = the wait
+// returned early, which would be a defect).  Nothing else is in flight:
+// no tensor-core work, no memory copies, no TMEM.
+__global__ void k_wait_probe(long long limit, int *status) {
+    __shared__ __align__(8) unsigned long long bar;
+    if (threadIdx.x == 0) {
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" :: "r"(smem_u32(&bar)), "r"(1) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const bool ok = mbar_wait(smem_u32(&bar), 0u, limit);
+    __syncthreads();
+    if (threadIdx.x == 0) *status = ok ? 0 : 1;
+}
+
+void launch_wait_probe(long long limit, int *d_status, cudaStream_t st) {
+    (k_wait_probe<<<1, 32, 0, st>>>(limit, d_status), note_launch());
 }
 
 size_t cgemm_tc_smem_bytes() { return sizeof(TcSmem) + 1024; }

@@ -492,6 +492,15 @@ int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d_b, double 
 int gm_cgemm_sub_c64(int device, int backend, int nprob, const int32_t *dims, void *const *A, void *const *B,
                      void *const *C);
 
+/* Failure-path check of the tensor-core kernels' bounded waits: one CTA
+ * waits, with the same bounded mbarrier wait as the tcgen05 kernels, on an
+ * mbarrier that nothing signals; the wait gives up after `polls` polls
+ * (1 .. 2^24) and *timed_out is set to 1 (0 would mean the wait returned
+ * without its phase completing).  Where a tcgen05 kernel's wait runs out it
+ * sets an error flag that the factorisation returns as GM_ERROR_CUDA
+ * instead of hanging.  No counterpart in the reference. */
+int gm_wait_probe(int device, long long polls, int *timed_out);
+
 /* ---- symbolic-analysis introspection (host only, no GPU needed) ---- */
 typedef struct gm_symbolic gm_symbolic;
 int gm_symbolic_create(int nx, int ny, int leaf_max, gm_symbolic **out);
