@@ -121,6 +121,7 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
     e->levels.resize(s.nlevels);
     for (int h = 0; h < s.nlevels; ++h) {
         gm::LevelInfo &L = e->levels[h];
+        L.index = h;
         L.first = s.lvl_off[h];
         L.count = s.lvl_off[h + 1] - s.lvl_off[h];
         L.max_front = s.lvl_max_front[h];
@@ -578,6 +579,11 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsign
     a.fmap = fmap;
     a.nfz = nfz;
     a.xmap = xmap;
+    if (mask && e->work_chunk > 0) {   // the pruned pass launches only the live pairs
+        a.work = e->d_work.as<int2>();
+        a.work_off = e->work_off.data();
+        a.work_chunk = e->work_chunk;
+    }
     a.nrhs = nrhs;
     a.ldr = nrhs;
     const int nchunk = (nrhs + 31) / 32;
@@ -647,7 +653,32 @@ static const unsigned char *build_mask(gm_engine *e, int nrhs, const RhsPattern 
         for (int g = 0; g < nch; ++g) mark(pat->common[i], g);
     if (e->d_mask.ensure(m.size()) != cudaSuccess) return nullptr;   // fall back to the dense pass
     if (cudaMemcpyAsync(e->d_mask.p, m.data(), m.size(), cudaMemcpyHostToDevice, e->st) != cudaSuccess) return nullptr;
-    cudaStreamSynchronize(e->st);   // m is released on return
+    // the live (front position, slice) pairs of every level, for slices of
+    // the width the substitution will use
+    const int tcw = solve_slice_width(nrhs, e->cfg.precision == GM_PREC_FP64);
+    const int nslice = (nrhs + tcw - 1) / tcw;
+    std::vector<int2> work;
+    e->work_off.assign(e->levels.size() + 1, 0);
+    for (size_t h = 0; h < e->levels.size(); ++h) {
+        e->work_off[h] = (int)work.size();
+        const LevelInfo &L = e->levels[h];
+        for (int t = 0; t < L.count; ++t) {
+            const int v = sy.lvl_nodes[L.first + t];
+            for (int c = 0; c < nslice; ++c) {
+                const int r0 = c * tcw, r1 = std::min(nrhs, r0 + tcw) - 1;
+                bool lv = false;
+                for (int g = r0 >> 5; g <= (r1 >> 5) && !lv; ++g) lv = m[(size_t)v * nch + g] != 0;
+                if (lv) work.push_back(make_int2(t, c));
+            }
+        }
+    }
+    e->work_off[e->levels.size()] = (int)work.size();
+    e->work_chunk = 0;
+    if (e->d_work.ensure((work.size() + 1) * sizeof(int2)) == cudaSuccess &&
+        cudaMemcpyAsync(e->d_work.p, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice, e->st) ==
+            cudaSuccess)
+        e->work_chunk = tcw;
+    cudaStreamSynchronize(e->st);   // m and work are released on return
     return e->d_mask.as<unsigned char>();
 }
 
@@ -757,6 +788,7 @@ static int gmres_refine(gm_engine *e, int sys, int nrhs, double2 *d_x, const Res
                 const double b0 = beta[(size_t)c * (m + 1)];
                 cdone[c] = !(b0 > 0.5 * tol * bnorm[c]);
                 std::fill(g.begin() + (size_t)c * (m + 1), g.begin() + (size_t)(c + 1) * (m + 1), cd(0));
+                std::fill(H.begin() + (size_t)c * (m + 1) * m, H.begin() + (size_t)(c + 1) * (m + 1) * m, cd(0));
                 g[(size_t)c * (m + 1)] = b0;
             }
         }
@@ -847,6 +879,18 @@ static int gmres_refine(gm_engine *e, int sys, int nrhs, double2 *d_x, const Res
                 }
                 kz[z] = jj + 1;
                 if (!all_done) still.push_back(z);
+            }
+            if (std::getenv("GM_TRACE_REFINEMENT")) {
+                std::fprintf(stderr, "GMRES iteration %d: largest estimated relative residual per matrix", jj + 1);
+                for (int j = 0; j < ni; ++j) {
+                    double w = 0;
+                    for (int r = 0; r < nrhs; ++r) {
+                        const int c = inner[j] * nrhs + r;
+                        w = std::max(w, std::abs(g[(size_t)c * (m + 1) + jj + 1]) / bnorm[c]);
+                    }
+                    std::fprintf(stderr, " [%d] %.2e", gset[inner[j]], w);
+                }
+                std::fprintf(stderr, "\n");
             }
             inner.swap(still);
         }
@@ -1006,7 +1050,7 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
         for (int f : next) {
             const gm_refine_info &ri = e->refine_info[f];
             bool to_gmres = e->cfg.refine == GM_REFINE_MODE_GMRES;
-            if (e->cfg.refine == GM_REFINE_MODE_AUTO && it > 0) {
+            if (e->cfg.refine == GM_REFINE_MODE_AUTO && it > 0 && !fp64) {   // FP64 factors: plain sweeps
                 const double rho = prev_res[f] > 0 ? ri.final_residual / prev_res[f] : 1.0;
                 const double need = std::log(e->cfg.ir_tol / ri.final_residual);
                 to_gmres = !(rho < 1.0) || need / std::log(rho) > 2.0;

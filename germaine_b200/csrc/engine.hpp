@@ -104,6 +104,9 @@ struct gm_engine {
     gm::DevBuf d_xf, d_xa;   // forward / adjoint solutions kept for the gradient
     int xf_ns = 0, xa_ns = 0; // right-hand sides held in d_xf / d_xa (0: none valid)
     gm::DevBuf d_mask;       // forward-pass pruning mask of the current solve
+    gm::DevBuf d_work;       // its live (front position, slice) pairs per level
+    std::vector<int> work_off;
+    int work_chunk = 0;      // slice width the pairs were built for (0: no list)
     std::vector<double> last_grad0, last_grad1;
     // per-shot gradient taper of ass_grad (SWS_TAPER_CIRCULAR_PER_SHOT 0, 1, 2),
     // its radius (SRTRADIUS, metres) and square half-width (FILTSIZE)

@@ -54,6 +54,7 @@ struct LevelInfo {
     int max_front, max_piv, max_ring;
     int64_t ent_first, ent_count;  // level's entry range in ent_dst/ent_src
     int64_t mid_words;  // largest (f + 1) s + (s | 1)(f - s) of the level's fronts: k_factor_mid's tile
+    int index;          // the level's height
 };
 
 template <class R>
@@ -132,7 +133,16 @@ struct SolveArgs {
     const int *fmap;
     int nfz;
     const int *xmap;
+    // live (front position in its level, slice) pairs of a pruned forward
+    // pass (device), level h at work[work_off[h] .. work_off[h + 1]) (host
+    // offsets), for slices of work_chunk right-hand sides; NULL: no list
+    const int2 *work;
+    const int *work_off;
+    int work_chunk;
 };
+
+// right-hand sides per substitution slice for nrhs right-hand sides
+int solve_slice_width(int nrhs, bool fp64);
 
 template <class R>
 void launch_solve_forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st);

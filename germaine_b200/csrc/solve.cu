@@ -199,10 +199,10 @@ struct Ctx {
 };
 
 template <class R, int TC>
-__device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first, int chunk) {
+__device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first, int chunk, int pos = -1) {
     using C = cplx<R>;
     Ctx<R> c;
-    c.node = a.s.lvl_nodes[lvl_first + blockIdx.y];
+    c.node = a.s.lvl_nodes[lvl_first + (pos < 0 ? (int)blockIdx.y : pos)];
     c.f = a.s.nfront[c.node];
     c.s = a.s.npiv[c.node];
     const int r0 = chunk * TC;
@@ -415,6 +415,99 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
     }
 }
 
+// Forward pass of a whole front whose pivots fit one 32-pivot block (the
+// small fronts of the lower levels): the children's update vectors are added
+// into x at the pivots, y = Dinv x_piv is formed in shared memory and written
+// back to x, and the update vector w = (children's update vectors at the
+// ring rows) - L'(ring, pivots) y follows tile by tile with y kept in shared
+// memory -- k_fwd_piv and k_fwd_ring in one CTA, y read once.
+// wofs >= 0: the CTA's (front position, slice) is work[wofs + blockIdx.x],
+// the live pairs of a pruned pass; wofs < 0: (blockIdx.y, blockIdx.x).
+template <class R, bool TRANS, int B>
+__global__ void __launch_bounds__(NT) k_fwd_small(SolveArgs<R> a, int lvl_first, int wofs) {
+    using C = cplx<R>;
+    constexpr int RT = 32;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    SolveSmem<C, RT, B> &sm = *reinterpret_cast<SolveSmem<C, RT, B> *>(smem_raw);
+    constexpr int TC = 8 * B;
+    const int2 wk = wofs >= 0 ? a.work[wofs + blockIdx.x] : make_int2((int)blockIdx.y, (int)blockIdx.x);
+    const Ctx<R> c = make_ctx<R, TC>(a, lvl_first, wk.y, wk.x);
+    if (c.rn <= 0) return;
+    const int r0 = wk.y * TC;
+    if (!live(a, c.node, r0, c.rn)) return;   // y and the update vector are zero
+    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int *inv = a.s.inv + a.s.inv_off[c.node];
+    const size_t xz = solve_slot(a);
+    const C *Wall = reinterpret_cast<const C *>(a.w) + xz * (size_t)a.s.rhs_total * a.ldr + r0;
+    const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
+    const C *W0 = c0 >= 0 && live(a, c0, r0, c.rn) ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
+    const C *W1 = c1 >= 0 && live(a, c1, r0, c.rn) ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
+    const size_t ldr = a.ldr;
+    const int s = c.s;   // <= SNB (launch condition)
+
+    if (W0 || W1) {   // children's update vectors at the pivots
+        for (int i = warp; i < s; i += NT / 32) {
+            const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
+            if (q0 < 0 && q1 < 0) continue;
+            for (int r = lane; r < c.rn; r += 32) {
+                C v = czero<C>();
+                if (q0 >= 0) v = cadd(v, W0[(size_t)q0 * ldr + r]);
+                if (q1 >= 0) v = cadd(v, W1[(size_t)q1 * ldr + r]);
+                C &x = c.X[(size_t)c.vars[i] * ldr + r];
+                x = cadd(x, v);
+            }
+        }
+        __syncthreads();
+    }
+    C acc[RT / 16][B];
+    if (s > 0) {
+        stage_dinv<C, true, TRANS, RT, B>(sm, c.F, c.f, 0, s);
+        stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q] * ldr; }, s, c.rn);
+        __syncthreads();
+        zero_acc(acc);
+        tile_mma(sm, s, acc, tr, tc, s, c.rn);   // y = Dinv x_piv
+        __syncthreads();
+#pragma unroll
+        for (int a2 = 0; a2 < RT / 16; ++a2) {
+            const int p = tr + 16 * a2;
+#pragma unroll
+            for (int b = 0; b < B; ++b) sm.Y[p][tc + 8 * b] = acc[a2][b];
+        }
+        __syncthreads();
+        for (int t = threadIdx.x; t < s * TC; t += NT) {
+            const int q = t / TC, r = t % TC;
+            if (r < c.rn) c.X[(size_t)c.vars[q] * ldr + r] = sm.Y[q][r];
+        }
+    }
+    // w over the ring rows, 32-row tiles, y staying in sm.Y
+    for (int i0 = s; i0 < c.f; i0 += RT) {
+        const int rows = min(RT, c.f - i0);
+        stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, 0, s);
+        __syncthreads();
+        zero_acc(acc);
+        tile_mma(sm, s, acc, tr, tc, rows, c.rn);
+#pragma unroll
+        for (int p = 0; p < RT / 16; ++p) {
+            const int row = tr + 16 * p;
+            if (row >= rows) continue;
+            const int i = i0 + row;
+            const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
+            C *w = c.W + (size_t)(i - s) * ldr;
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                const int r = tc + 8 * b;
+                if (r >= c.rn) continue;
+                C g = czero<C>();
+                if (q0 >= 0) g = cadd(g, W0[(size_t)q0 * ldr + r]);
+                if (q1 >= 0) g = cadd(g, W1[(size_t)q1 * ldr + r]);
+                w[r] = csub(g, acc[p][b]);
+            }
+        }
+        __syncthreads();   // sm.L is staged again for the next tile
+    }
+}
+
 // Backward pass of a whole front whose pivots fit one 32-pivot block (the
 // small fronts of the lower levels): t = y - U'(pivots, ring) x[ring] with
 // the product accumulated in registers over 32-column ring blocks, t placed
@@ -491,6 +584,8 @@ static void set_attrs() {
     if (RT == 32) {
         cudaFuncSetAttribute((const void *)k_bwd_small<R, false, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
         cudaFuncSetAttribute((const void *)k_bwd_small<R, true, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute((const void *)k_fwd_small<R, false, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
+        cudaFuncSetAttribute((const void *)k_fwd_small<R, true, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     }
     done = true;
 }
@@ -531,6 +626,20 @@ static void forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_
     set_attrs<R, RT, B>();
     const size_t smem = solve_smem<R, RT, B>();
     const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
+    static const bool no_small = env_int("GM_NO_FWD_SMALL") != 0;
+    if (RT == 32 && L.max_piv <= SNB && !no_small) {   // one pivot block per front: fused pivot + ring kernel
+        int wofs = -1;
+        dim3 g(nchunk, L.count, solve_nfz(a));
+        if (a.work && a.work_chunk == 8 * B) {   // pruned pass: only the live (front, slice) pairs
+            wofs = a.work_off[L.index];
+            const int nlive = a.work_off[L.index + 1] - wofs;
+            if (nlive == 0) return;
+            g = dim3(nlive, 1, solve_nfz(a));
+        }
+        if (a.trans) (k_fwd_small<R, true, B><<<g, NT, smem, st>>>(a, L.first, wofs), note_launch());
+        else (k_fwd_small<R, false, B><<<g, NT, smem, st>>>(a, L.first, wofs), note_launch());
+        return;
+    }
     dim3 g1(nchunk, L.count, solve_nfz(a));
     const int fused = 0;   // separate ring kernel: more parallelism per level
     if (a.trans) (k_fwd_piv<R, true, RT, B><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
@@ -607,6 +716,8 @@ void preload_solve_kernels() {
     set_attrs<float, 32, 5>();
     set_attrs<float, 64, 5>();
 }
+
+int solve_slice_width(int nrhs, bool fp64) { return 8 * (fp64 ? slice_b<double>(nrhs) : slice_b<float>(nrhs)); }
 
 template void launch_solve_forward_level<double>(const SolveArgs<double> &, const LevelInfo &, cudaStream_t);
 template void launch_solve_forward_level<float>(const SolveArgs<float> &, const LevelInfo &, cudaStream_t);
