@@ -298,6 +298,17 @@ def time_steps(torch, e, step, steps: int, warmup: int, dist=None):
     return ms, int(launches)
 
 
+def measure_fp64_peak(device: int) -> float:
+    """FP64 FMA rate of the CUDA cores (TFLOP/s), measured by the library's
+    DFMA microbenchmark before any timed step."""
+    import ctypes
+
+    from germaine_b200 import _lib
+    out = ctypes.c_double(0.0)
+    _lib.check(_lib.load().gm_peak_fp64(device, ctypes.byref(out)))
+    return float(out.value)
+
+
 def load_peaks():
     try:
         with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
@@ -348,6 +359,7 @@ def run_gpu(args):
     rho_h = torch.from_numpy(rho.reshape(-1)).pin_memory()
     seis_h = torch.empty((nf, ns, ntr, 2), dtype=torch.float32).pin_memory()
     peak_hbm, peak_bf16, peak_kind = load_peaks()
+    fp64_peak = measure_fp64_peak(local)
 
     results = {}
     for name, prec in (("mixed", GM_PREC_C64_IR), ("fp64", GM_PREC_FP64)):
@@ -428,6 +440,25 @@ def run_gpu(args):
     per4 = {"mixed": None, "fp64": BWD_TRAFFIC_FP64_4FREQ}[head_name]
     traffic = (per4 / 4 * nf if per4 and (W["nx0"], W["ny0"], W["nshots"], args.leaf) == (801, 187, 100, 32)
                else None)
+    # the same pass against the FP64 (complex64: FP32) CUDA-core rate -- at
+    # 100 right-hand sides its arithmetic intensity (8 flops per stored U
+    # entry per right-hand side) is above the HBM ridge -- and the
+    # factorisation against it: exact flop counts of the symbolic analysis
+    # over the device time of the phase
+    subst_flops = 8.0 * st["u_entries"] * ns * nf
+    factor_flops = st["factor_flops"] * nf
+    peak_fp = fp64_peak * (2.0 if head_name == "mixed" else 1.0)
+    roofline_compute = [
+        {"kernel": "K5 backward substitution (same launch group)", "bound": "fp64" if csize == 16 else "fp32",
+         "achieved": subst_flops / (subst_ms * 1e-3) / 1e12, "peak": peak_fp, "unit": "TFLOP/s",
+         "frac": subst_flops / (subst_ms * 1e-3) / 1e12 / peak_fp, "algorithmic_flops": subst_flops,
+         "arithmetic_intensity_flop_per_byte": subst_flops / subst_bytes,
+         "peak_kind": "measured FP64 DFMA rate (gm_peak_fp64)" + (" x 2 for FP32" if csize == 8 else "")},
+        {"kernel": "K2-K4 factorisation, all levels", "bound": "fp64" if csize == 16 else "fp32",
+         "achieved": factor_flops / (st["ms_factor"] * 1e-3) / 1e12, "peak": peak_fp, "unit": "TFLOP/s",
+         "frac": factor_flops / (st["ms_factor"] * 1e-3) / 1e12 / peak_fp, "algorithmic_flops": factor_flops,
+         "ms": st["ms_factor"], "peak_kind": "measured FP64 DFMA rate (gm_peak_fp64)" + (" x 2 for FP32" if csize == 8 else "")},
+    ]
     line = {
         "metric": METRIC,
         "value": value,
@@ -467,6 +498,8 @@ def run_gpu(args):
                      "bound": "hbm", "achieved": achieved, "peak": peak_hbm, "unit": "GB/s",
                      "frac": achieved / peak_hbm, "peak_kind": peak_kind, "traffic": traffic,
                      "algorithmic_bytes": subst_bytes, "ms_per_launch_group": subst_ms},
+        "roofline_compute": roofline_compute,
+        "fp64_peak_tflops": fp64_peak,
         "gpu_launches": head["launches"] * args.steps,
         "clocks": head["clocks"],
         "cpu_baseline": cpu,

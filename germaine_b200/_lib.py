@@ -69,11 +69,11 @@ REFINE_METHOD_NAMES = {GM_REFINE_NONE: "none", GM_REFINE_IR: "ir", GM_REFINE_GMR
 EXPORTS = [
     "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats", "gm_engine_stream",
     "gm_refine_report", "gm_set_model", "gm_set_models", "gm_factor", "gm_factor_models", "gm_factor_values", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
-    "gm_get_gradient_fp64", "gm_get_wavefield_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_hessian", "gm_get_hessian_fp64", "gm_apply_hess", "gm_precond",
+    "gm_get_gradient_fp64", "gm_get_wavefield_fp64", "gm_get_misfit_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_hessian", "gm_get_hessian_fp64", "gm_apply_hess", "gm_precond",
     "gm_lbfgs_create", "gm_lbfgs_destroy", "gm_lbfgs_step", "gm_lbfgs_rotate", "gm_lbfgs_zero",
     "gm_lbfgs_check_descent", "gm_lbfgs_get_old", "gm_lbfgs_set_old", "gm_mat_change",
     "gm_set_shot_taper", "gm_set_invmat", "gm_set_source_wavelet", "gm_stf_dft", "gm_taper_grad_shot", "gm_taper_grad_shot1", "gm_tikhonov_cost_te", "gm_tikhonov_grad_te",
-    "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_read_grid", "gm_cgemm_sub_c64", "gm_wait_probe",
+    "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_read_grid", "gm_cgemm_sub_c64", "gm_wait_probe", "gm_peak_fp64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
 ]
@@ -127,6 +127,7 @@ def load() -> ctypes.CDLL:
     lib.gm_obj.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, i32, i32, vp]
     lib.gm_get_gradient_fp64.argtypes = [vp, vp, vp]
     lib.gm_get_wavefield_fp64.argtypes = [vp, i32, vp]
+    lib.gm_get_misfit_fp64.argtypes = [vp, i32, vp, vp]
     f32 = ctypes.c_float
     lib.gm_gauss_filt.argtypes = [i32, i32, i32, f32, f32, f32, f32, f32, vp, vp]
     lib.gm_hessian.argtypes = [vp, i32, i32, vp, vp, i32, vp, vp, vp, vp]
@@ -160,6 +161,7 @@ def load() -> ctypes.CDLL:
     lib.gm_solve_noalloc.argtypes = [vp, i32, i32, vp, vp]
     lib.gm_cgemm_sub_c64.argtypes = [i32, i32, i32, vp, vp, vp, vp]
     lib.gm_wait_probe.argtypes = [i32, ctypes.c_longlong, ctypes.POINTER(i32)]
+    lib.gm_peak_fp64.argtypes = [i32, ctypes.POINTER(f64)]
     lib.gm_symbolic_create.argtypes = [i32, i32, i32, ctypes.POINTER(vp)]
     lib.gm_symbolic_destroy.argtypes = [vp]
     lib.gm_symbolic_sizes.argtypes = [vp, vp]

@@ -172,7 +172,9 @@ int residuals(gm_engine *e, int ns, int ntr, const float *pobs, int stf_inv, int
     double2 *stf = reinterpret_cast<double2 *>(l2p + nfs + (nfs & 1));
     GM_CUDA(cudaMemcpyAsync(obs, pobs, cnt * sizeof(float2), cudaMemcpyDefault, e->st));
     double2 *cal = e->d_res.as<double2>(), *res = cal + cnt;
-    gm::launch_residual_shot(cal, obs, nfs, ntr, stf_inv, misfit, e->invmat, res, l2p, stf, e->st);
+    // GM_OP_EXACT forms the exact residual: no zeroing of tiny observed samples
+    const int zeroing = e->cfg.op_mode == GM_OP_EXACT ? 0 : 1;
+    gm::launch_residual_shot(cal, obs, nfs, ntr, stf_inv, misfit, e->invmat, zeroing, res, l2p, stf, e->st);
     GM_CUDA(cudaGetLastError());
     std::vector<double> l2h(nfs);
     std::vector<double2> stfh(nfs);
@@ -181,6 +183,9 @@ int residuals(gm_engine *e, int ns, int ntr, const float *pobs, int stf_inv, int
     GM_CUDA(cudaStreamSynchronize(e->st));
     l2 = 0;
     for (double v : l2h) l2 += v;
+    e->last_l2 = 0.5 * l2;
+    e->last_l2_each.assign(nf, 0.0);
+    for (int i = 0; i < nfs; ++i) e->last_l2_each[i / ns] += 0.5 * l2h[i];
     if (l2_each) {
         l2_each->assign(nf, 0.0);
         for (int i = 0; i < nfs; ++i) (*l2_each)[i / ns] += l2h[i];
@@ -359,6 +364,10 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     if (misfit < 1 || misfit > 3) return fail(GM_ERROR_INVALID, "gm_grad_obj: MISFIT must be 1, 2 or 3");
     if ((rc = single_model(e, "gm_grad_obj"))) return rc;   // one gradient: one model
     const bool te = e->cfg.physics == GM_PHYS_TE;
+    const bool exact = e->cfg.op_mode == GM_OP_EXACT;
+    if (exact && (e->cfg.physics != GM_PHYS_AC || stf_inv || misfit != 1 || e->invmat != 1))
+        return fail(GM_ERROR_INVALID, "gm_grad_obj: the exact gradient (GM_OP_EXACT) covers acoustic FWI with "
+                                      "MISFIT 1, no source estimate and INVMAT 1");
     GM_CUDA(cudaSetDevice(e->device));
     Geometry g;
     if ((rc = make_geometry(e, nshots, src_x, src_y, ntr, rec_x, rec_y, g))) return rc;
@@ -372,13 +381,15 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     // adjoint sources and the adjoint solve with the same factors
     if ((rc = upload(e->d_rec_k, g.kadj, e->st))) return rc;
     const size_t cnt = (size_t)nf * nshots * ntr;
-    const double dh2 = (double)(e->cfg.dh * e->cfg.dh);
+    // the reference's adjoint source is conj(res) / DH^2; the exact gradient's is conj(res)
+    const double dh2 = exact ? 1.0 : (double)(e->cfg.dh * e->cfg.dh);
     GM_ALLOC(e->d_b, (size_t)nf * n * nshots * sizeof(double2));
     gm::launch_adjoint_src(e->d_b.as<double2>(), n, nf, nshots, ntr, e->d_rec_k.as<int>(), e->d_res.as<double2>() + cnt,
                            dh2, e->st);
     GM_CUDA(cudaGetLastError());
     GM_ALLOC(e->d_xa, (size_t)nf * n * nshots * sizeof(double2));
-    const int sys = te ? GM_SYS_AT : GM_SYS_A;   // grad_obj_TE.c:149 vs grad_obj_AC.c:147
+    // grad_obj_TE.c:149 vs grad_obj_AC.c:147; the exact adjoint solves with M^T
+    const int sys = (te || exact) ? GM_SYS_AT : GM_SYS_A;
     gm::RhsPattern pat;   // adjoint sources only at the receivers
     pat.common = g.kadj.data();
     pat.ncommon = ntr;
@@ -393,6 +404,12 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     for (int f = 0; f < nf; ++f) {
         float a[2], b[2];
         gmh_gradient_scalars(e->cfg.physics, e->freqs[f], e->cfg.s, a, b);
+        if (exact) {   // the derivative of the assembled operator: the assembly's Omega^2
+            float o2[2], o[2], o2mu0[2];
+            gmh_assembly_scalars(e->cfg.physics, e->freqs[f], e->cfg.s, o2, o, o2mu0);
+            a[0] = o2[0];
+            a[1] = o2[1];
+        }
         om2[f] = make_double2(a[0], a[1]);
         om[f] = make_double2(b[0], b[1]);
     }
@@ -411,7 +428,14 @@ extern "C" int gm_grad_obj(gm_engine *e, int nshots, const float *src_x, const f
     ga.frame = e->d_frame.as<float>(); ga.passes = e->d_frame_pass.as<unsigned char>();
     ga.g0 = e->d_grad.as<double>(); ga.g1 = ga.g0 + n;
     if ((rc = shot_taper_tables(e, nshots, src_x, src_y, ntr, rec_x, rec_y, ga))) return rc;
-    gm::launch_gradient(ga, e->st);
+    if (exact) {
+        if (e->shot_taper) return fail(GM_ERROR_INVALID, "gm_grad_obj: the exact gradient takes no per-shot taper");
+        float w[6];
+        gmh_fd_weights(e->cfg.dh, w);
+        gm::launch_gradient_exact(ga, w, e->st);
+    } else {
+        gm::launch_gradient(ga, e->st);
+    }
     GM_CUDA(cudaGetLastError());
     e->last_grad0.resize(n);
     e->last_grad1.assign(te ? n : 0, 0.0);
@@ -439,6 +463,17 @@ extern "C" int gm_get_wavefield_fp64(gm_engine *e, int which, double *x) {
     const gm::DevBuf &buf = which ? e->d_xa : e->d_xf;
     GM_CUDA(cudaMemcpyAsync(x, buf.p, (size_t)e->nf * e->n * ns * sizeof(double2), cudaMemcpyDefault, e->st));
     GM_CUDA(cudaStreamSynchronize(e->st));
+    return GM_OK;
+}
+
+extern "C" int gm_get_misfit_fp64(gm_engine *e, int nmat, double *l2, double *l2_each) {
+    if (!e) return fail(GM_ERROR_INVALID, "null engine");
+    if (e->last_l2_each.empty()) return fail(GM_ERROR_STATE, "no misfit computed yet");
+    if (l2_each && nmat != (int)e->last_l2_each.size())
+        return fail(GM_ERROR_INVALID, "gm_get_misfit_fp64: the last misfit covered %d matrices, not %d",
+                    (int)e->last_l2_each.size(), nmat);
+    if (l2) *l2 = e->last_l2;
+    if (l2_each) std::memcpy(l2_each, e->last_l2_each.data(), e->last_l2_each.size() * sizeof(double));
     return GM_OK;
 }
 

@@ -85,7 +85,7 @@ void launch_field(const double2 *x, int n, int nf, int ns, float2 *field, cudaSt
 // misfit partial sum (counted before the zeroing, as calc_res_AC.c:82-88
 // does).
 __global__ void k_residual_shot(const double2 *cal, const float2 *obs, int ntr, int stf_inv, int misfit,
-                                int invmat, double2 *res, double *l2, double2 *stf) {
+                                int invmat, int zeroing, double2 *res, double *l2, double2 *stf) {
     const int fs = blockIdx.x;
     const double2 *c = cal + (size_t)fs * ntr;
     const float2 *o = obs + (size_t)fs * ntr;
@@ -130,7 +130,7 @@ __global__ void k_residual_shot(const double2 *cal, const float2 *obs, int ntr, 
             r = make_double2((ov.x - wc.x) / wabs, (ov.y - wc.y) / wabs);
         }
         acc += r.x * r.x + r.y * r.y;
-        if (o[t].x < 1e-20f && o[t].y < 1e-20f) r = make_double2(0.0, 0.0);
+        if (zeroing && o[t].x < 1e-20f && o[t].y < 1e-20f) r = make_double2(0.0, 0.0);
         rs[t] = r;
     }
     red[0][threadIdx.x] = acc;
@@ -146,8 +146,9 @@ __global__ void k_residual_shot(const double2 *cal, const float2 *obs, int ntr, 
 }
 
 void launch_residual_shot(const double2 *cal, const float2 *obs, int nfs, int ntr, int stf_inv, int misfit,
-                          int invmat, double2 *res, double *l2, double2 *stf, cudaStream_t st) {
-    (k_residual_shot<<<nfs, 256, 0, st>>>(cal, obs, ntr, stf_inv, misfit, invmat, res, l2, stf), note_launch());
+                          int invmat, int zeroing, double2 *res, double *l2, double2 *stf, cudaStream_t st) {
+    (k_residual_shot<<<nfs, 256, 0, st>>>(cal, obs, ntr, stf_inv, misfit, invmat, zeroing, res, l2, stf),
+     note_launch());
 }
 
 // Adjoint sources conj(res)/DH^2 at the receivers; receivers sharing a grid
@@ -249,6 +250,51 @@ __global__ void k_gradient(GradArgs a) {
 
 void launch_gradient(const GradArgs &a, cudaStream_t st) {
     (k_gradient<<<(a.n + 127) / 128, 128, 0, st>>>(a), note_launch());
+}
+
+// Exact discrete FWI gradient of the acoustic engine (GM_OP_EXACT): the
+// derivative of J = 0.5 sum |d - u(rec)|^2 over all shots and frequencies,
+// with A u = s and A^T lambda = sum_rec conj(r) e_rec, with respect to vp at
+// grid point c.  vp enters A only through the mass term of column c,
+// A[c - off(q)][c] += w_q Omega^2 ivp2[c] (w_q = a, b, c of
+// init_A_AC_9p_pml for the centre, edge and corner neighbours), so
+//   dJ/divp2_c = Re(Omega^2 u_c sum_q w_q lambda_{c - off(q)}),
+//   dJ/dvp_c   = dJ/divp2_c * (-2 / (rho_c vp_c^3)),
+// read without the vec2mat shift; then the PML frame taper.  om2 holds the
+// assembly's Omega^2 per frequency, w the three mass weights.
+__global__ void k_gradient_exact(GradArgs a, double wa, double wb, double wc) {
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n) return;
+    const int nx = a.nx, ny = a.n / nx, x = k % nx, y = k / nx;
+    double g = 0.0;
+    for (int f = 0; f < a.nf; ++f) {
+        const double2 om2 = a.om2[f];
+        const double2 *xf = a.xf + (size_t)f * a.n * a.ns;
+        const double2 *xa = a.xa + (size_t)f * a.n * a.ns;
+        for (int s = 0; s < a.ns; ++s) {
+            double2 ls = make_double2(0.0, 0.0);
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                const int xx = x - (q % 3 - 1), yy = y - (q / 3 - 1);   // row k' with k' + off(q) = k
+                if (xx < 0 || xx >= nx || yy < 0 || yy >= ny) continue;
+                const double w = q == 4 ? wa : (q & 1) ? wb : wc;
+                const double2 l = xa[(size_t)(yy * nx + xx) * a.ns + s];
+                ls.x += w * l.x;
+                ls.y += w * l.y;
+            }
+            g += cmul(cmul(om2, xf[(size_t)k * a.ns + s]), ls).x;
+        }
+    }
+    const double vp = a.m0[k], rho = a.m1[k];
+    g *= -2.0 / (rho * vp * vp * vp);
+    const float c = a.frame[k];
+    const int p = a.passes[k];
+    for (int q = 0; q < p; ++q) g *= c;
+    a.g0[k] = g;
+}
+
+void launch_gradient_exact(const GradArgs &a, const float w[3], cudaStream_t st) {
+    (k_gradient_exact<<<(a.n + 127) / 128, 128, 0, st>>>(a, w[0], w[1], w[2]), note_launch());
 }
 
 // sq[f][k] (+)= sum_s |field(k)|^2 over the ns solutions of frequency f, the

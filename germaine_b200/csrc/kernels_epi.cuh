@@ -41,10 +41,12 @@ void launch_gather_seis(const double2 *x, int n, int nf, int ns, int ntr, const 
                         cudaStream_t st);
 void launch_field(const double2 *x, int n, int nf, int ns, float2 *field, cudaStream_t st);
 void launch_residual_shot(const double2 *cal, const float2 *obs, int nfs, int ntr, int stf_inv, int misfit,
-                          int invmat, double2 *res, double *l2, double2 *stf, cudaStream_t st);
+                          int invmat, int zeroing, double2 *res, double *l2, double2 *stf, cudaStream_t st);
 void launch_adjoint_src(double2 *b, int n, int nf, int ns, int ntr, const int *kadj, const double2 *res, double dh2,
                         cudaStream_t st);
 void launch_gradient(const GradArgs &a, cudaStream_t st);
+// exact discrete AC gradient of GM_OP_EXACT (w: mass weights a, b, c)
+void launch_gradient_exact(const GradArgs &a, const float w[3], cudaStream_t st);
 void launch_hess_sq(const double2 *x, int n, int nf, int ns, double *sq, int accumulate, cudaStream_t st);
 void launch_hess_final(const HessArgs &a, cudaStream_t st);
 

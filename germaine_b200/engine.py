@@ -247,6 +247,14 @@ class Engine:
         check(self.lib.gm_get_wavefield_fp64(self._h, which, ptr(x)))
         return x
 
+    def misfit_fp64(self):
+        """(0.5 * misfit sum, per-matrix misfits) of the last obj / obj_each /
+        grad_obj, in FP64."""
+        each = np.zeros(self.nf)
+        l2 = ctypes.c_double(0.0)
+        check(self.lib.gm_get_misfit_fp64(self._h, self.nf, ctypes.byref(l2), ptr(each)))
+        return float(l2.value), each
+
     def gradient_fp64(self):
         g0 = np.zeros(self.n)
         g1 = np.zeros(self.n) if self.physics == GM_PHYS_TE else None

@@ -46,7 +46,12 @@ extern "C" {
 /* ---- operator orientation ---- */
 #define GM_OP_REF   0  /* M = A^T: what UMFPACK factorises after the value
                           overwrite at src/AC/forward_shot_AC.c:41-48 */
-#define GM_OP_EXACT 1  /* M = A: the assembled stencil rows */
+#define GM_OP_EXACT 1  /* M = A: the assembled stencil rows; gm_grad_obj then gives
+                          the exact discrete gradient of the misfit (acoustic,
+                          MISFIT 1, no source estimate): residuals not zeroed,
+                          adjoint source conj(res), adjoint solve with M^T, the
+                          mass term's 9-point spread of init_A_AC_9p_pml
+                          differentiated, no vec2mat shift in the stack */
 
 /* ---- diagonal Hessian estimators (the reference's HESSIAN parameter) ---- */
 #define GM_HESS_GREEN 1  /* hessian_AC / hessian_TE: shot and receiver Green's functions */
@@ -275,6 +280,12 @@ int gm_set_shot_taper(gm_engine *e, int mode, float srtradius, int filtsize);
  * order, before vec2mat's shift.  GM_ERROR_STATE when none is held. */
 int gm_get_wavefield_fp64(gm_engine *e, int which, double *x);
 
+/* The last misfit in FP64 before rounding to float: *l2 = 0.5 * sum of
+ * |res|^2 over every matrix, shot and receiver of the last gm_obj /
+ * gm_obj_each / gm_grad_obj, l2_each[m] the same per matrix (nmat = the
+ * batch's matrix count).  Either pointer may be NULL. */
+int gm_get_misfit_fp64(gm_engine *e, int nmat, double *l2, double *l2_each);
+
 /* The last gm_grad_obj gradients before rounding to float, in FP64
  * ([NY][NX] each; g1 ignored for AC).  Either pointer may be NULL. */
 int gm_get_gradient_fp64(gm_engine *e, double *g0, double *g1);
@@ -500,6 +511,12 @@ int gm_cgemm_sub_c64(int device, int backend, int nprob, const int32_t *dims, vo
  * sets an error flag that the factorisation returns as GM_ERROR_CUDA
  * instead of hanging.  No counterpart in the reference. */
 int gm_wait_probe(int device, long long polls, int *timed_out);
+
+/* Measured FP64 FMA throughput of the device's CUDA cores in TFLOP/s (a DFMA
+ * chain kernel timed with CUDA events, best of four launches after two
+ * warm-up launches): the denominator of the FP64 roofline fractions.  No
+ * counterpart in the reference. */
+int gm_peak_fp64(int device, double *tflops);
 
 /* ---- symbolic-analysis introspection (host only, no GPU needed) ---- */
 typedef struct gm_symbolic gm_symbolic;
