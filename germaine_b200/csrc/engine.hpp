@@ -111,6 +111,7 @@ struct gm_engine {
     // per-shot gradient taper of ass_grad (SWS_TAPER_CIRCULAR_PER_SHOT 0, 1, 2),
     // its radius (SRTRADIUS, metres) and square half-width (FILTSIZE)
     int invmat = 1;               // INVMAT of calc_res_AC: 1 FWI residuals, 2 RTM (observed data)
+    int shot_block = 0;           // gm_forward's cap on shots per block solve (0: memory decides)
     double last_l2 = 0;           // 0.5 * misfit sum of the last gm_obj / gm_obj_each / gm_grad_obj, FP64
     std::vector<double> last_l2_each;   // the same per matrix
     std::vector<float> wavelet;   // [nf][2] source amplitudes of READ_WAVELET = 1 (empty: spikes)

@@ -200,6 +200,55 @@ int residuals(gm_engine *e, int ns, int ntr, const float *pobs, int stf_inv, int
 
 }  // namespace
 
+namespace {
+
+// Device bytes per shot of one block solve over the batch: the FP64
+// solutions, the working-precision copy, the front update vectors and the
+// residual partial sums.
+size_t bytes_per_shot(const gm_engine *e) {
+    const size_t n = (size_t)e->n, nf = (size_t)e->nf;
+    return nf * (n * sizeof(double2) + n * e->csize() + (size_t)e->sym.rhs_total * e->csize() +
+                 ((n + 63) / 64) * 2 * sizeof(double) + 2 * sizeof(double));
+}
+
+// Shots per block solve of gm_forward: all of them unless their workspaces
+// exceed the device memory left (free now plus what the engine's solve
+// workspaces already hold, less a reserve of 5 % of the device and 1 GB),
+// or the caller's cap (gm_set_shot_block).
+int shot_block(const gm_engine *e, int nshots) {
+    size_t fr = 0, tot = 0;
+    if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return nshots;
+    const size_t held = e->d_xf.bytes + e->d_t.bytes + e->d_w.bytes + e->d_part.bytes;
+    const size_t reserve = tot / 20 + ((size_t)1 << 30);
+    const size_t avail = fr + held > reserve ? fr + held - reserve : 0;
+    size_t blk = avail / std::max<size_t>(1, bytes_per_shot(e));
+    if (e->shot_block > 0) blk = std::min<size_t>(blk, (size_t)e->shot_block);
+    return (int)std::max<size_t>(1, std::min<size_t>(blk, (size_t)nshots));
+}
+
+}  // namespace
+
+extern "C" int gm_set_shot_block(gm_engine *e, int max_shots) {
+    if (!e || max_shots < 0) return fail(GM_ERROR_INVALID, "gm_set_shot_block: bad argument");
+    e->shot_block = max_shots;
+    return GM_OK;
+}
+
+extern "C" int gm_memory_estimate(gm_engine *e, int nmat, size_t *factor_bytes, size_t *shot_bytes) {
+    if (!e || nmat <= 0) return fail(GM_ERROR_INVALID, "gm_memory_estimate: bad argument");
+    const size_t n = (size_t)e->n, m = (size_t)nmat;
+    if (factor_bytes)   // fronts, assembled stencils, mass / stiffness, PML profiles
+        *factor_bytes = m * ((size_t)e->sym.front_total * e->csize() + 9 * n * sizeof(double2) + n * sizeof(float2) +
+                             n * sizeof(float) + (4 * ((size_t)e->cfg.nx + 2) + 4 * ((size_t)e->cfg.ny + 2)) * 4);
+    if (shot_bytes) {
+        const int nf = e->nf;
+        e->nf = nmat;
+        *shot_bytes = bytes_per_shot(e);
+        e->nf = nf;
+    }
+    return GM_OK;
+}
+
 extern "C" int gm_forward(gm_engine *e, int nshots, const float *src_x, const float *src_y, int ntr,
                           const int32_t *rec_x, const int32_t *rec_y, float *seis, float *field) {
     int rc = check_ready(e, nshots, ntr);
@@ -208,6 +257,39 @@ extern "C" int gm_forward(gm_engine *e, int nshots, const float *src_x, const fl
     GM_CUDA(cudaSetDevice(e->device));
     Geometry g;
     if ((rc = make_geometry(e, nshots, src_x, src_y, ntr, rec_x, rec_y, g))) return rc;
+    const int blk = shot_block(e, nshots);
+    if (blk < nshots) {
+        // block solves of at most blk shots each: seismograms and fields are
+        // copied out per frequency into the [nf][nshots][...] outputs
+        int worst = GM_OK;
+        Geometry gb = g;
+        for (int s0 = 0; s0 < nshots; s0 += blk) {
+            const int nb = std::min(blk, nshots - s0);
+            gb.ksrc.assign(g.ksrc.begin() + s0, g.ksrc.begin() + s0 + nb);
+            const int brc = forward_and_seis(e, nb, gb, ntr, nullptr);
+            if (brc < 0) return brc;
+            worst = std::max(worst, brc);
+            for (int f = 0; f < e->nf; ++f) {
+                if (seis && ntr > 0)
+                    GM_CUDA(cudaMemcpyAsync(seis + 2 * ((size_t)f * nshots + s0) * ntr,
+                                            e->d_seis.as<float2>() + (size_t)f * nb * ntr,
+                                            (size_t)nb * ntr * sizeof(float2), cudaMemcpyDefault, e->st));
+            }
+            if (field) {
+                const size_t cnt = (size_t)e->nf * nb * e->n;
+                GM_ALLOC(e->d_field, cnt * sizeof(float2));
+                gm::launch_field(e->d_xf.as<double2>(), e->n, e->nf, nb, e->d_field.as<float2>(), e->st);
+                GM_CUDA(cudaGetLastError());
+                for (int f = 0; f < e->nf; ++f)
+                    GM_CUDA(cudaMemcpyAsync(field + 2 * ((size_t)f * nshots + s0) * e->n,
+                                            e->d_field.as<float2>() + (size_t)f * nb * e->n,
+                                            (size_t)nb * e->n * sizeof(float2), cudaMemcpyDefault, e->st));
+            }
+            GM_CUDA(cudaStreamSynchronize(e->st));
+        }
+        e->xf_ns = 0;   // only the last block's solutions are held
+        return worst;
+    }
     const int solve_rc = forward_and_seis(e, nshots, g, ntr, seis);
     if (solve_rc < 0) return solve_rc;
     if (field) {

@@ -57,6 +57,15 @@ struct LevelInfo {
     int index;          // the level's height
 };
 
+// Launches that put a level's fronts on grid.y are split into pieces of at
+// most kMaxGridY fronts (the hardware limit of gridDim.y); each piece passes
+// its own first level position.
+constexpr int kMaxGridY = 65535;
+template <class F>
+inline void for_level_pieces(const LevelInfo &L, F fn) {
+    for (int c0 = 0; c0 < L.count; c0 += kMaxGridY) fn(L.first + c0, L.count - c0 < kMaxGridY ? L.count - c0 : kMaxGridY);
+}
+
 template <class R>
 struct FactorArgs {
     DevSym s;

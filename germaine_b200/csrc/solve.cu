@@ -628,26 +628,34 @@ static void forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_
     const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
     static const bool no_small = env_int("GM_NO_FWD_SMALL") != 0;
     if (RT == 32 && L.max_piv <= SNB && !no_small) {   // one pivot block per front: fused pivot + ring kernel
-        int wofs = -1;
-        dim3 g(nchunk, L.count, solve_nfz(a));
         if (a.work && a.work_chunk == 8 * B) {   // pruned pass: only the live (front, slice) pairs
-            wofs = a.work_off[L.index];
+            const int wofs = a.work_off[L.index];
             const int nlive = a.work_off[L.index + 1] - wofs;
             if (nlive == 0) return;
-            g = dim3(nlive, 1, solve_nfz(a));
+            dim3 g(nlive, 1, solve_nfz(a));
+            if (a.trans) (k_fwd_small<R, true, B><<<g, NT, smem, st>>>(a, L.first, wofs), note_launch());
+            else (k_fwd_small<R, false, B><<<g, NT, smem, st>>>(a, L.first, wofs), note_launch());
+            return;
         }
-        if (a.trans) (k_fwd_small<R, true, B><<<g, NT, smem, st>>>(a, L.first, wofs), note_launch());
-        else (k_fwd_small<R, false, B><<<g, NT, smem, st>>>(a, L.first, wofs), note_launch());
+        for_level_pieces(L, [&](int first, int count) {
+            dim3 g(nchunk, count, solve_nfz(a));
+            if (a.trans) (k_fwd_small<R, true, B><<<g, NT, smem, st>>>(a, first, -1), note_launch());
+            else (k_fwd_small<R, false, B><<<g, NT, smem, st>>>(a, first, -1), note_launch());
+        });
         return;
     }
-    dim3 g1(nchunk, L.count, solve_nfz(a));
     const int fused = 0;   // separate ring kernel: more parallelism per level
-    if (a.trans) (k_fwd_piv<R, true, RT, B><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
-    else (k_fwd_piv<R, false, RT, B><<<g1, NT, smem, st>>>(a, L.first, fused), note_launch());
+    for_level_pieces(L, [&](int first, int count) {
+        dim3 g1(nchunk, count, solve_nfz(a));
+        if (a.trans) (k_fwd_piv<R, true, RT, B><<<g1, NT, smem, st>>>(a, first, fused), note_launch());
+        else (k_fwd_piv<R, false, RT, B><<<g1, NT, smem, st>>>(a, first, fused), note_launch());
+    });
     if (L.max_ring > 0) {
-        dim3 g2(nchunk * ((L.max_ring + RT - 1) / RT), L.count, solve_nfz(a));
-        if (a.trans) (k_fwd_ring<R, true, RT, B><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
-        else (k_fwd_ring<R, false, RT, B><<<g2, NT, smem, st>>>(a, L.first, nchunk), note_launch());
+        for_level_pieces(L, [&](int first, int count) {
+            dim3 g2(nchunk * ((L.max_ring + RT - 1) / RT), count, solve_nfz(a));
+            if (a.trans) (k_fwd_ring<R, true, RT, B><<<g2, NT, smem, st>>>(a, first, nchunk), note_launch());
+            else (k_fwd_ring<R, false, RT, B><<<g2, NT, smem, st>>>(a, first, nchunk), note_launch());
+        });
     }
 }
 
@@ -658,20 +666,26 @@ static void backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream
     const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
     static const bool no_small = env_int("GM_NO_BWD_SMALL") != 0;
     if (RT == 32 && L.max_piv <= SNB && !no_small) {   // one pivot block per front: fused ring + pivot kernel
-        dim3 g(nchunk, L.count, solve_nfz(a));
-        if (a.trans) (k_bwd_small<R, true, B><<<g, NT, smem, st>>>(a, L.first), note_launch());
-        else (k_bwd_small<R, false, B><<<g, NT, smem, st>>>(a, L.first), note_launch());
+        for_level_pieces(L, [&](int first, int count) {
+            dim3 g(nchunk, count, solve_nfz(a));
+            if (a.trans) (k_bwd_small<R, true, B><<<g, NT, smem, st>>>(a, first), note_launch());
+            else (k_bwd_small<R, false, B><<<g, NT, smem, st>>>(a, first), note_launch());
+        });
         return;
     }
     const int fused = 0;
     if (L.max_ring > 0) {
-        dim3 g1(nchunk * ((L.max_piv + RT - 1) / RT), L.count, solve_nfz(a));
-        if (a.trans) (k_bwd_ring<R, true, RT, B><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
-        else (k_bwd_ring<R, false, RT, B><<<g1, NT, smem, st>>>(a, L.first, nchunk), note_launch());
+        for_level_pieces(L, [&](int first, int count) {
+            dim3 g1(nchunk * ((L.max_piv + RT - 1) / RT), count, solve_nfz(a));
+            if (a.trans) (k_bwd_ring<R, true, RT, B><<<g1, NT, smem, st>>>(a, first, nchunk), note_launch());
+            else (k_bwd_ring<R, false, RT, B><<<g1, NT, smem, st>>>(a, first, nchunk), note_launch());
+        });
     }
-    dim3 g2(nchunk, L.count, solve_nfz(a));
-    if (a.trans) (k_bwd_piv<R, true, RT, B><<<g2, NT, smem, st>>>(a, L.first, fused), note_launch());
-    else (k_bwd_piv<R, false, RT, B><<<g2, NT, smem, st>>>(a, L.first, fused), note_launch());
+    for_level_pieces(L, [&](int first, int count) {
+        dim3 g2(nchunk, count, solve_nfz(a));
+        if (a.trans) (k_bwd_piv<R, true, RT, B><<<g2, NT, smem, st>>>(a, first, fused), note_launch());
+        else (k_bwd_piv<R, false, RT, B><<<g2, NT, smem, st>>>(a, first, fused), note_launch());
+    });
 }
 
 template <class R, int B>

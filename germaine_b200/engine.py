@@ -215,6 +215,27 @@ class Engine:
                                                       ptr(seis)))
         return g0, g1, float(l2.value), seis
 
+    def set_shot_block(self, max_shots: int) -> None:
+        """Cap on shots per block solve of forward() (0: device memory decides)."""
+        check(self.lib.gm_set_shot_block(self._h, max_shots))
+
+    def memory_estimate(self, nmat: int):
+        """(bytes to factorise nmat matrices at once, bytes per shot of a block
+        solve over them)."""
+        fb, sb = ctypes.c_size_t(0), ctypes.c_size_t(0)
+        check(self.lib.gm_memory_estimate(self._h, nmat, ctypes.byref(fb), ctypes.byref(sb)))
+        return int(fb.value), int(sb.value)
+
+    def plan(self, nfreq: int, nshots: int, budget: int):
+        """Frequencies per factorisation batch and shots per block solve so that
+        one batch (its factors plus one block's workspaces) fits `budget`
+        device bytes; raises if even one frequency with one shot does not."""
+        for nb in range(nfreq, 0, -1):
+            fb, sb = self.memory_estimate(nb)
+            if fb + sb <= budget:
+                return nb, int(max(1, min(nshots, (budget - fb) // sb)))
+        raise ValueError(f"one frequency needs {sum(self.memory_estimate(1))} bytes, more than {budget}")
+
     def set_invmat(self, invmat: int) -> None:
         """INVMAT of the residuals of the following grad_obj / obj calls:
         1 FWI (default), 2 RTM (residual = observed data)."""

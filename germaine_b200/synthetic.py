@@ -8,6 +8,8 @@ external benchmark collection that is not part of the reference tree).
   the PML frame the way readmod() does (src/readmod.c:60-92).
 * ``inclusion_model`` -- homogeneous 2000 m/s / 1000 kg/m^3 with one circular
   2400 m/s inclusion of radius 150 m at the centre.
+* ``gpr_model``      -- georadar (TE) model: layered relative permittivity
+  3-25 with elliptical anomalies, conductivity 0.1-10 mS/m.
 * ``line_acquisition`` -- shots and receivers along one model row.
 """
 from __future__ import annotations
@@ -58,6 +60,38 @@ def inclusion_model(nx0: int = 201, ny0: int = 101, dh: float = 10.0, npml: int 
     vp[(X - nx0 * dh / 2) ** 2 + (Y - ny0 * dh / 2) ** 2 <= radius ** 2] = v1
     vp_full = extend_into_pml(vp, npml)
     return vp_full, np.full_like(vp_full, rho)
+
+
+def gpr_model(nx0: int = 4000, ny0: int = 2000, dh: float = 0.025, npml: int = 30, seed: int = 2025,
+              nlayers: int = 6, nellipses: int = 12):
+    """Georadar (TE) model: seeded random layers of relative permittivity
+    3-25 with elliptical anomalies, conductivity 0.1-10 mS/m; returns the
+    absolute permittivity (eps_r * eps0, F/m) and the conductivity (S/m),
+    [NY][NX] with the PML frame."""
+    eps0 = 8.854187817e-12
+    rng = np.random.default_rng(seed)
+    x = (np.arange(nx0) * dh)[None, :]
+    y = (np.arange(ny0) * dh)[:, None]
+    depth = ny0 * dh
+    tops = np.sort(rng.uniform(0.05, 0.95, nlayers - 1)) * depth
+    eps = np.full((ny0, nx0), rng.uniform(3.0, 25.0), np.float64)
+    sig = np.full((ny0, nx0), 10 ** rng.uniform(-4.0, -2.0), np.float64)
+    for t in tops:
+        amp = rng.uniform(0.0, 0.03) * depth
+        lam = rng.uniform(0.3, 1.0) * nx0 * dh
+        surf = t + amp * np.sin(2 * np.pi * x / lam + rng.uniform(0, 2 * np.pi))
+        below = y >= surf
+        eps = np.where(below, rng.uniform(3.0, 25.0), eps)
+        sig = np.where(below, 10 ** rng.uniform(-4.0, -2.0), sig)
+    for _ in range(nellipses):
+        cx, cy = rng.uniform(0.1, 0.9) * nx0 * dh, rng.uniform(0.1, 0.9) * depth
+        ax, ay = rng.uniform(0.01, 0.08) * nx0 * dh, rng.uniform(0.01, 0.08) * depth
+        inside = ((x - cx) / ax) ** 2 + ((y - cy) / ay) ** 2 <= 1.0
+        eps = np.where(inside, rng.uniform(3.0, 25.0), eps)
+        sig = np.where(inside, 10 ** rng.uniform(-4.0, -2.0), sig)
+    eps_full = extend_into_pml((eps * eps0).astype(np.float32), npml)
+    sig_full = extend_into_pml(sig.astype(np.float32), npml)
+    return eps_full, sig_full
 
 
 def line_acquisition(nx0: int, dh: float, nshots: int, row: int, nrec: int | None = None):

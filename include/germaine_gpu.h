@@ -209,6 +209,18 @@ int gm_forward(gm_engine *e, int nshots, const float *src_x, const float *src_y,
                int ntr, const int32_t *rec_x, const int32_t *rec_y,
                float *seis, float *field);
 
+/* Memory plan of large problems.  gm_forward solves its shots in blocks
+ * when the workspaces of all of them would not fit the device memory left
+ * (free memory plus the engine's solve workspaces, less a reserve), or when
+ * max_shots > 0 caps the block (0 = memory alone decides); the outputs are
+ * the same, and gm_get_wavefield_fp64 then holds no solutions.
+ * gm_memory_estimate returns the device bytes of factorising nmat matrices
+ * at once and of one shot of a block solve over nmat matrices, so that a
+ * caller can choose how many frequencies to factorise together.  No
+ * counterpart in the reference (one frequency and one shot at a time). */
+int gm_set_shot_block(gm_engine *e, int max_shots);
+int gm_memory_estimate(gm_engine *e, int nmat, size_t *factor_bytes, size_t *shot_bytes);
+
 /* FWI objective + gradient of all factorised frequencies (grad_obj_AC,
  * src/AC/grad_obj_AC.c:10-194; grad_obj_TE for GM_PHYS_TE): forward solve,
  * residual (calc_res_AC, MISFIT 1/2/3, optional Wiener source estimate

@@ -17,15 +17,20 @@ def _model(nx, ny, seed=1):
     return random_smooth(nx, ny, 1500.0, 3500.0, seed), np.full((ny, nx), 1000.0, np.float32)
 
 
-@pytest.mark.parametrize("bad", [np.nan, np.inf, 0.0], ids=["nan-vp", "inf-vp", "zero-rho"])
+@pytest.mark.parametrize("bad", ["nan-vp", "zero-vp", "zero-rho"])
 @pytest.mark.parametrize("precision", [GM_PREC_FP64, GM_PREC_C64_IR], ids=["fp64", "c64"])
 def test_nonfinite_material_is_reported(bad, precision):
+    """NaN material, or material whose operator coefficients overflow
+    (1/(rho vp^2) or 1/rho infinite), stops the factorisation with
+    GM_ERROR_NONFINITE."""
     nx, ny = 40, 30
     vp, rho = _model(nx, ny)
-    if bad == 0.0:
+    if bad == "zero-rho":
         rho[12, 17] = 0.0               # b = 1/rho = inf
+    elif bad == "zero-vp":
+        vp[12, 17] = 0.0                # ivp2 = 1/(rho vp^2) = inf
     else:
-        vp[12, 17] = bad
+        vp[12, 17] = np.nan
     with Engine(nx, ny, 10.0, 6, precision=precision, leaf_max=16) as e:
         e.set_model(vp, rho)
         with pytest.raises(GmError) as ex:
@@ -66,7 +71,7 @@ def test_zero_pivot_is_perturbed_and_counted():
         assert e.stats()["perturbed_pivots"] >= 1
         b = np.zeros((1, n, 2), complex)
         b[0, 100, 0] = 1.0
-        b[0, 300, 1] = 1.0j
+        b[0, row, 1] = 1.0j              # the zeroed row's equation 0 = 1j has no solution
         x = e.solve(b)
         assert e.last_status == _lib.GM_WARNING_NOT_CONVERGED
         assert np.all(np.isfinite(x))
