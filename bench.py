@@ -49,9 +49,10 @@ DH, NPML, ROW = 25.0, 20, 2
 RESIDUAL_TARGET = 1e-10
 METRIC = "shot-solves/s (factor+solve) mixed vs FP64 on B200 at resid<=1e-10; %roofline"
 # DRAM bytes of one complex128 backward substitution pass on 4 frequencies
-# (the first k_bwd_ring / k_bwd_piv launches of the FP64 engine, ncu
-# dram__bytes_read.sum + dram__bytes_write.sum)
-BWD_TRAFFIC_FP64_4FREQ = 6.813e9
+# (the first k_bwd_small / k_bwd_ring / k_bwd_piv launches of the FP64
+# engine, ncu dram__bytes_read.sum + dram__bytes_write.sum;
+# profiles/bwd_substitution_dram_fp64_thrust841x227_leaf32_4freq.md)
+BWD_TRAFFIC_FP64_4FREQ = 4.805e9
 
 # the benchmark workload; --nx0/--ny0/--nfreq/--nshots shrink it for
 # profiling captures (the bench line then names the smaller workload)

@@ -546,201 +546,6 @@ __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int 
     if (tid == 0 && npert) atomicAdd(a.npert, (unsigned long long)npert);
 }
 
-// The same front factorisation with the LU steps in registers: the front
-// is gathered into shared memory as above, then each of the 256 threads
-// holds a T x T tile of it (rows ty + 16 a, columns tx + 16 b: a strided
-// mapping that keeps the shrinking trailing block spread over all threads)
-// and the right-looking LU runs on the tiles.  Per pivot only the pivot
-// column and row pass through shared memory (double-buffered, one barrier
-// per pivot); every thread forms the reciprocal pivot itself.  The
-// arithmetic of every entry is that of k_factor_small (same scaling and
-// update operations in the same order), so the factors are identical.
-// Fronts of at most 16 T rows.
-constexpr int RT_GRID = 16;
-
-template <class R, int T>
-__global__ void __launch_bounds__(SMALL_FT, (T <= 4 ? 2 : 1)) k_factor_small_rt(FactorArgs<R> a, int lvl_first, int ld) {
-    using C = cplx<R>;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C *S = reinterpret_cast<C *>(smem_raw);
-    __shared__ C Dinv[NB][NB + 1];
-    __shared__ C colb[2][RT_GRID * T], rowb[2][RT_GRID * T], pivb[2];
-    __shared__ int npert;
-    const int pos = lvl_first + blockIdx.x;
-    const int node = a.s.lvl_nodes[pos];
-    const int f = a.s.nfront[node], s = a.s.npiv[node];
-    C *rd = S + (size_t)ld * f;   // reciprocal pivots
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nw = SMALL_FT / 32;
-    const int tx = tid % RT_GRID, ty = tid / RT_GRID;
-    const size_t fz = blockIdx.y;
-    C *base = reinterpret_cast<C *>(a.front) + fz * a.s.front_total;
-    C *F = base + a.s.front_off[node];
-
-    // extend-add of the children's contribution blocks (zero for leaves)
-    const int *inv = a.s.inv + a.s.inv_off[node];
-    const int c0 = a.s.child0[node], c1 = a.s.child1[node];
-    const C *cb0 = nullptr, *cb1 = nullptr;
-    int f0 = 0, f1 = 0;
-    if (c0 >= 0) { const int s0 = a.s.npiv[c0]; f0 = a.s.nfront[c0]; cb0 = base + a.s.front_off[c0] + s0 + (size_t)s0 * f0; }
-    if (c1 >= 0) { const int s1 = a.s.npiv[c1]; f1 = a.s.nfront[c1]; cb1 = base + a.s.front_off[c1] + s1 + (size_t)s1 * f1; }
-    for (int j = warp; j < f; j += nw) {
-        const int j0 = cb0 ? inv[j] : -1, j1 = cb1 ? inv[f + j] : -1;
-        for (int i = lane; i < f; i += 32) {
-            C v = czero<C>();
-            if (j0 >= 0) { const int r = inv[i]; if (r >= 0) v = cadd(v, cb0[r + (size_t)j0 * f0]); }
-            if (j1 >= 0) { const int r = inv[f + i]; if (r >= 0) v = cadd(v, cb1[r + (size_t)j1 * f1]); }
-            S[i + j * ld] = v;
-        }
-    }
-    if (tid == 0) npert = 0;
-    __syncthreads();
-    {   // operator entries owned by the front (positions are distinct)
-        const int64_t e0 = a.ent_lvl_off[pos], e1 = a.ent_lvl_off[pos + 1];
-        const int64_t fo = a.s.front_off[node];
-        const double2 *A = a.A + fz * 9 * (size_t)a.s.n;
-        for (int64_t e = e0 + tid; e < e1; e += SMALL_FT) {
-            const int p = (int)(a.ent_dst[e] - fo);
-            const int i = p % f, j = p / f;
-            C &d = S[i + j * ld];
-            d = cadd(d, cconv<C>(A[a.ent_src[e]]));
-        }
-    }
-    __syncthreads();
-
-    // the tiles into registers
-    C t[T][T];
-#pragma unroll
-    for (int ia = 0; ia < T; ++ia)
-#pragma unroll
-        for (int jb = 0; jb < T; ++jb) {
-            const int i = ty + RT_GRID * ia, j = tx + RT_GRID * jb;
-            t[ia][jb] = (i < f && j < f) ? S[i + j * ld] : czero<C>();
-        }
-    const R pivtol = (R)(a.pivscale * __longlong_as_double((long long)*a.amax));
-    // publish pivot column / row k (values after step k - 1) into buffer k & 1
-    auto publish = [&](int k) {
-        const int b = k & 1;
-        if (tx == k % RT_GRID) {
-            const int jb = k / RT_GRID;
-#pragma unroll
-            for (int ia = 0; ia < T; ++ia) {
-                const int i = ty + RT_GRID * ia;
-                if (jb < T && i < f) {
-                    C v = czero<C>();
-#pragma unroll
-                    for (int q = 0; q < T; ++q)
-                        if (q == jb) v = t[ia][q];
-                    if (i > k) colb[b][i] = v;
-                    else if (i == k) pivb[b] = v;
-                }
-            }
-        }
-        if (ty == k % RT_GRID) {
-            const int ia = k / RT_GRID;
-#pragma unroll
-            for (int jb = 0; jb < T; ++jb) {
-                const int j = tx + RT_GRID * jb;
-                if (ia < T && j > k && j < f) {
-                    C v = czero<C>();
-#pragma unroll
-                    for (int q = 0; q < T; ++q)
-                        if (q == ia) v = t[q][jb];
-                    rowb[b][j] = v;
-                }
-            }
-        }
-    };
-    if (s > 0) publish(0);
-    __syncthreads();
-    for (int k = 0; k < s; ++k) {
-        const int b = k & 1;
-        C piv = pivb[b];
-        const R mag = sqrt(cabs2(piv));
-        bool pert = false;
-        if (!(mag >= pivtol)) {   // static pivoting as in k_factor_small (also catches NaN)
-            if (mag > R(0)) {
-                const R sc = pivtol / mag;
-                piv = mk(piv.x * sc, piv.y * sc);
-            } else {
-                piv = mk(pivtol, R(0));
-            }
-            pert = true;
-        }
-        const C rk = crcp(piv);
-        C u[T];
-#pragma unroll
-        for (int jb = 0; jb < T; ++jb) {
-            const int j = tx + RT_GRID * jb;
-            u[jb] = (j > k && j < f) ? rowb[b][j] : czero<C>();
-        }
-#pragma unroll
-        for (int ia = 0; ia < T; ++ia) {
-            const int i = ty + RT_GRID * ia;
-            if (i < k || i >= f) continue;
-            if (i == k) {
-                if (tx == k % RT_GRID) {   // the (static) pivot, in the tile of its owner
-#pragma unroll
-                    for (int jb = 0; jb < T; ++jb)
-                        if (tx + RT_GRID * jb == k) t[ia][jb] = piv;
-                    rd[k] = rk;
-                    if (pert) ++npert;
-                }
-                continue;
-            }
-            const C l = cmul(colb[b][i], rk);
-#pragma unroll
-            for (int jb = 0; jb < T; ++jb) {
-                const int j = tx + RT_GRID * jb;
-                if (j == k) t[ia][jb] = l;                              // L column k
-                else if (j > k && j < f) cfms(t[ia][jb], l, u[jb]);
-            }
-        }
-        if (k + 1 < s) publish(k + 1);
-        __syncthreads();
-    }
-    // the tiles back to shared memory
-#pragma unroll
-    for (int ia = 0; ia < T; ++ia)
-#pragma unroll
-        for (int jb = 0; jb < T; ++jb) {
-            const int i = ty + RT_GRID * ia, j = tx + RT_GRID * jb;
-            if (i < f && j < f) S[i + j * ld] = t[ia][jb];
-        }
-    __syncthreads();
-
-    // inverses of the NB x NB diagonal blocks (as k_factor_small)
-    for (int k0 = 0; k0 < s; k0 += NB) {
-        const int kb = min(NB, s - k0);
-        auto D = [&](int r, int q) { return S[(k0 + r) + (k0 + q) * ld]; };
-        if (tid < kb) {
-            const int c = tid;
-            for (int r = c + 1; r < kb; ++r) {
-                C acc = D(r, c);
-                for (int q = c + 1; q < r; ++q) cfma(acc, D(r, q), Dinv[q][c]);
-                Dinv[r][c] = mk(-acc.x, -acc.y);
-            }
-        } else if (tid >= 32 && tid < 32 + kb) {
-            const int c = tid - 32;
-            Dinv[c][c] = rd[k0 + c];
-            for (int r = c - 1; r >= 0; --r) {
-                C acc = czero<C>();
-                for (int q = r + 1; q <= c; ++q) cfma(acc, D(r, q), Dinv[q][c]);
-                Dinv[r][c] = cmul(mk(-acc.x, -acc.y), rd[k0 + r]);
-            }
-        }
-        __syncthreads();
-        for (int tt = tid; tt < kb * kb; tt += SMALL_FT) {
-            const int r = tt % kb, c = tt / kb;
-            S[(k0 + r) + (k0 + c) * ld] = Dinv[r][c];
-        }
-        __syncthreads();
-    }
-
-    for (int j = warp; j < f; j += nw)
-        for (int i = lane; i < f; i += 32) F[i + (size_t)j * f] = S[i + j * ld];
-    if (tid == 0 && npert) atomicAdd(a.npert, (unsigned long long)npert);
-}
-
 constexpr size_t SMALL_FACTOR_SMEM = 100 << 10;
 
 template <class R>
@@ -759,19 +564,10 @@ void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_factor_small<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
-        cudaFuncSetAttribute(k_factor_small_rt<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
-        cudaFuncSetAttribute(k_factor_small_rt<R, 5>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
         attr_set = true;
     }
     const size_t smem = small_factor_smem<R>(L.max_front);
-    // register-tiled LU for fronts of at most 80 rows (GM_NO_FACTOR_RT=1: the shared-memory one)
-    static const bool no_rt = std::getenv("GM_NO_FACTOR_RT") != nullptr;
-    if (!no_rt && L.max_front <= RT_GRID * 4)
-        (k_factor_small_rt<R, 4><<<dim3(L.count, a.nf), SMALL_FT, smem, st>>>(a, L.first, L.max_front + 1), note_launch());
-    else if (!no_rt && L.max_front <= RT_GRID * 5)
-        (k_factor_small_rt<R, 5><<<dim3(L.count, a.nf), SMALL_FT, smem, st>>>(a, L.first, L.max_front + 1), note_launch());
-    else
-        (k_factor_small<R><<<dim3(L.count, a.nf), SMALL_FT, smem, st>>>(a, L.first, L.max_front + 1), note_launch());
+    (k_factor_small<R><<<dim3(L.count, a.nf), SMALL_FT, smem, st>>>(a, L.first, L.max_front + 1), note_launch());
 }
 
 template bool small_factor_level<double>(const LevelInfo &);
