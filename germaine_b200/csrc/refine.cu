@@ -35,6 +35,7 @@ template <class InC, class OutC, bool WRITE, bool PRODUCT>
 __global__ void __launch_bounds__(RLANES *RGRP, 3) k_residual(ResidArgs a, const InC *__restrict__ xin, OutC *out,
                                                             double *part) {
     __shared__ double2 cf[9][RROWS];
+    __shared__ unsigned short nbm[RROWS];   // per row: bit q set when neighbour q lies inside the grid
     __shared__ double red[2][RGRP][RLANES];
     const int fz = blockIdx.z;
     const int f = a.fmap ? a.fmap[fz] : fz;
@@ -42,14 +43,24 @@ __global__ void __launch_bounds__(RLANES *RGRP, 3) k_residual(ResidArgs a, const
     const int r = blockIdx.y * RLANES + threadIdx.x;
     const bool use_row = (a.op_mode == GM_OP_EXACT) != (a.trans != 0);
     const double2 *A9 = a.A + (size_t)f * 9 * a.n;
-    for (int t = threadIdx.y * RLANES + threadIdx.x; t < 9 * RROWS; t += RLANES * RGRP) {
-        const int q = t / RROWS, i = t % RROWS, k = k0 + i;
-        double2 v = make_double2(0.0, 0.0);
+    const int tid = threadIdx.y * RLANES + threadIdx.x;
+    if (tid < RROWS) {   // the grid-edge tests once per row, not per right-hand side
+        const int k = k0 + tid;
+        unsigned m = 0;
         if (k < a.n) {
-            const int xx = k % a.nx + q % 3 - 1, yy = k / a.nx + q / 3 - 1;
-            if (xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny) v = op_coef(A9, a.n, a.nx, use_row, q, k);
+            const int x = k % a.nx, y = k / a.nx;
+#pragma unroll
+            for (int q = 0; q < 9; ++q) {
+                const int xx = x + q % 3 - 1, yy = y + q / 3 - 1;
+                if (xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny) m |= 1u << q;
+            }
         }
-        cf[q][i] = v;
+        nbm[tid] = (unsigned short)m;
+    }
+    __syncthreads();
+    for (int t = tid; t < 9 * RROWS; t += RLANES * RGRP) {
+        const int q = t / RROWS, i = t % RROWS;
+        cf[q][i] = (nbm[i] >> q) & 1 ? op_coef(A9, a.n, a.nx, use_row, q, k0 + i) : make_double2(0.0, 0.0);
     }
     __syncthreads();
     double rr = 0.0, bb = 0.0;
@@ -61,20 +72,22 @@ __global__ void __launch_bounds__(RLANES *RGRP, 3) k_residual(ResidArgs a, const
         const bool spikes = !PRODUCT && a.spike_k;
         const int ks = spikes ? a.spike_k[r] : -1;
         const double2 amp = spikes ? a.spike_amp[f] : make_double2(0.0, 0.0);
+        // neighbour q of row k is row k + dq[q]: offsets in elements of x
+        int dq[9];
+#pragma unroll
+        for (int q = 0; q < 9; ++q) dq[q] = ((q % 3 - 1) + (q / 3 - 1) * a.nx) * a.ldr;
 #pragma unroll 2
         for (int i = threadIdx.y; i < RROWS; i += RGRP) {
             const int k = k0 + i;
             if (k >= a.n) break;
-            const int x = k % a.nx, y = k / a.nx;
+            const unsigned m = nbm[i];
             double2 bv = make_double2(0.0, 0.0);
             if (!PRODUCT) bv = spikes ? (k == ks ? amp : bv) : a.b[base + (size_t)k * a.ldr];
             double2 acc = bv;
+            const InC *Xk = X + (size_t)k * a.ldr;
 #pragma unroll
-            for (int q = 0; q < 9; ++q) {
-                const int dx = q % 3 - 1, dy = q / 3 - 1;
-                if (x + dx < 0 || x + dx >= a.nx || y + dy < 0 || y + dy >= a.ny) continue;
-                cfms(acc, cf[q][i], cto_d(X[(size_t)(k + dx + dy * a.nx) * a.ldr]));
-            }
+            for (int q = 0; q < 9; ++q)
+                if ((m >> q) & 1) cfms(acc, cf[q][i], cto_d(Xk[dq[q]]));
             if (PRODUCT) acc = make_double2(-acc.x, -acc.y);
             if (WRITE) O[(size_t)k * a.ldr] = cconv<OutC>(acc);
             rr += acc.x * acc.x + acc.y * acc.y;
