@@ -697,11 +697,22 @@ static int gmres_refine(gm_engine *e, int sys, int nrhs, double2 *d_x, const Res
     using cd = std::complex<double>;
     const int ng = (int)gset.size();
     if (ng == 0) return GM_OK;
-    const int m = e->cfg.gmres_restart;
     const int n = e->n;
     const double tol = e->cfg.ir_tol;
     const size_t per = (size_t)n * nrhs;
     const size_t vstride = (size_t)ng * per;   // one Krylov slot holds all ng matrices
+    // restart length: the configured one, shortened while the Krylov and
+    // preconditioned vectors would not fit 80 % of the device memory left
+    int m = e->cfg.gmres_restart;
+    {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
+            const size_t avail = (fr + e->d_gv.bytes + e->d_gz.bytes) / 10 * 8;
+            while (m >= 2 && (size_t)(m + 1) * vstride * sizeof(double2) + (size_t)m * vstride * sizeof(cplx_any<R>) > avail)
+                --m;
+        }
+        if (m < 2) return GM_WARNING_NOT_CONVERGED;   // no room: the caller refines with plain sweeps
+    }
     GM_ALLOC(e->d_gv, (size_t)(m + 1) * vstride * sizeof(double2));
     GM_ALLOC(e->d_gz, (size_t)m * vstride * sizeof(cplx_any<R>));
     const int nblk_r = (n + 63) / 64, nblk_g = (n + 255) / 256;
@@ -1061,7 +1072,11 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
         if (!gset.empty()) {
             const int grc = fp64 ? gmres_refine<double>(e, sys, nrhs, d_x, ra, gset)
                                  : gmres_refine<float>(e, sys, nrhs, d_x, ra, gset);
-            if (grc) {
+            if (grc == GM_WARNING_NOT_CONVERGED) {   // no room for the Krylov vectors: plain sweeps
+                irset.insert(irset.end(), gset.begin(), gset.end());
+                std::sort(irset.begin(), irset.end());
+                gset.clear();
+            } else if (grc) {
                 e->stats.ir_iterations = it;
                 e->stats.ir_residual = NAN;
                 return grc;

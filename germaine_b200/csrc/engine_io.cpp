@@ -216,12 +216,14 @@ size_t bytes_per_shot(const gm_engine *e) {
 // workspaces already hold, less a reserve of 5 % of the device and 1 GB),
 // or the caller's cap (gm_set_shot_block).
 int shot_block(const gm_engine *e, int nshots) {
+    const size_t held = e->d_xf.bytes + e->d_t.bytes + e->d_w.bytes + e->d_part.bytes + e->d_norm.bytes;
+    const size_t per = std::max<size_t>(1, bytes_per_shot(e));
+    if (e->shot_block <= 0 && per * (size_t)nshots <= held) return nshots;   // workspaces in place already
     size_t fr = 0, tot = 0;
     if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) return nshots;
-    const size_t held = e->d_xf.bytes + e->d_t.bytes + e->d_w.bytes + e->d_part.bytes;
     const size_t reserve = tot / 20 + ((size_t)1 << 30);
     const size_t avail = fr + held > reserve ? fr + held - reserve : 0;
-    size_t blk = avail / std::max<size_t>(1, bytes_per_shot(e));
+    size_t blk = avail / per;
     if (e->shot_block > 0) blk = std::min<size_t>(blk, (size_t)e->shot_block);
     return (int)std::max<size_t>(1, std::min<size_t>(blk, (size_t)nshots));
 }
