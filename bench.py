@@ -367,6 +367,10 @@ def run_gpu(args):
         e = Engine(nx, ny, DH, NPML, precision=prec, device=local, leaf_max=args.leaf,
                    refine={"auto": 0, "ir": 1, "gmres": 2}[args.refine])
         e.set_model(vp_d, rho_d)
+        tuned = None
+        if args.autotune:   # substitution tiles per level, timed on this workload's factors (untimed set-up)
+            e.factor(freqs)
+            tuned = e.autotune(ns)
 
         def check_converged(tag):
             # every step must meet the residual target: a path that stops
@@ -386,7 +390,7 @@ def run_gpu(args):
         ms, launches = time_steps(torch, e, step_dev, args.steps, args.warmup, dist)
         ck = clocks.stop()
         st = e.stats()
-        r = {"ms": ms, "launches": launches, "stats": st, "clocks": ck}
+        r = {"ms": ms, "launches": launches, "stats": st, "clocks": ck, "tuned": tuned}
 
         def step_e2e():
             e.set_model(vp_h, rho_h)
@@ -491,7 +495,8 @@ def run_gpu(args):
                                    "refine": results[n]["stats"]["ms_refine"],
                                    "substitutions": results[n]["stats"]["ms_subst"],
                                    "n_subst": results[n]["stats"]["n_subst"]},
-                      "gpu_launches_per_step": results[n]["launches"]}
+                      "gpu_launches_per_step": results[n]["launches"],
+                      "autotuned_tiles": results[n]["tuned"]}
                   for n in ("fp64", "mixed")},
         "mixed_over_fp64": fp64["ms"] / mixed["ms"],
         "per_frequency": per_freq,
@@ -551,6 +556,8 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--refine", choices=["auto", "ir", "gmres"], default="auto",
                     help="refinement of the mixed path: automatic IR / GMRES-IR choice, IR only, GMRES-IR only")
+    ap.add_argument("--no-autotune", dest="autotune", action="store_false",
+                    help="keep the default substitution tiles instead of the per-level autotuned ones")
     ap.add_argument("--no-wavefield-error", dest="wavefield_error", action="store_false",
                     help="skip the per-frequency wavefield comparison of the two paths (outside the timed region)")
     ap.add_argument("--nx0", type=int, default=W["nx0"], help="model width without PML (profiling cases)")

@@ -68,7 +68,7 @@ REFINE_METHOD_NAMES = {GM_REFINE_NONE: "none", GM_REFINE_IR: "ir", GM_REFINE_GMR
 # every C-ABI symbol declared in include/germaine_gpu.h
 EXPORTS = [
     "gm_last_error", "gm_version", "gm_engine_create", "gm_engine_destroy", "gm_engine_stats", "gm_engine_stream",
-    "gm_refine_report", "gm_set_model", "gm_set_models", "gm_factor", "gm_factor_models", "gm_factor_values", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
+    "gm_refine_report", "gm_autotune", "gm_autotune_table", "gm_set_model", "gm_set_models", "gm_factor", "gm_factor_models", "gm_factor_values", "gm_get_triplets", "gm_solve", "gm_forward", "gm_grad_obj", "gm_obj",
     "gm_get_gradient_fp64", "gm_get_wavefield_fp64", "gm_get_misfit_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_hessian", "gm_get_hessian_fp64", "gm_apply_hess", "gm_precond",
     "gm_lbfgs_create", "gm_lbfgs_destroy", "gm_lbfgs_step", "gm_lbfgs_rotate", "gm_lbfgs_zero",
     "gm_lbfgs_check_descent", "gm_lbfgs_get_old", "gm_lbfgs_set_old", "gm_mat_change",
@@ -122,6 +122,8 @@ def load() -> ctypes.CDLL:
     lib.gm_get_triplets.argtypes = [vp, i32, vp, vp, vp, vp]
     lib.gm_solve.argtypes = [vp, i32, i32, vp, vp]
     lib.gm_refine_report.argtypes = [vp, i32, ctypes.POINTER(GmRefineInfo)]
+    lib.gm_autotune.argtypes = [vp, i32, i32]
+    lib.gm_autotune_table.argtypes = [vp, ctypes.POINTER(i32), vp, i32]
     lib.gm_forward.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, vp]
     lib.gm_grad_obj.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, i32, i32, vp, vp, vp, vp]
     lib.gm_obj.argtypes = [vp, i32, vp, vp, i32, vp, vp, vp, i32, i32, vp]

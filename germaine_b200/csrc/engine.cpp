@@ -579,10 +579,11 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsign
     a.fmap = fmap;
     a.nfz = nfz;
     a.xmap = xmap;
-    if (mask && e->work_chunk > 0) {   // the pruned pass launches only the live pairs
+    if (!e->lvl_cfg.empty() && e->tuned_nrhs == nrhs) a.lvl_cfg = e->lvl_cfg.data();
+    if (mask && e->have_work) {   // the pruned pass launches only the live pairs
         a.work = e->d_work.as<int2>();
         a.work_off = e->work_off.data();
-        a.work_chunk = e->work_chunk;
+        a.work_w = e->work_w.data();
     }
     a.nrhs = nrhs;
     a.ldr = nrhs;
@@ -654,13 +655,17 @@ static const unsigned char *build_mask(gm_engine *e, int nrhs, const RhsPattern 
     if (e->d_mask.ensure(m.size()) != cudaSuccess) return nullptr;   // fall back to the dense pass
     if (cudaMemcpyAsync(e->d_mask.p, m.data(), m.size(), cudaMemcpyHostToDevice, e->st) != cudaSuccess) return nullptr;
     // the live (front position, slice) pairs of every level, for slices of
-    // the width the substitution will use
-    const int tcw = solve_slice_width(nrhs, e->cfg.precision == GM_PREC_FP64);
-    const int nslice = (nrhs + tcw - 1) / tcw;
+    // the width the level's forward pass will use (tuned or default)
+    const int tcw_default = solve_slice_width(nrhs, e->cfg.precision == GM_PREC_FP64);
+    const bool tuned = !e->lvl_cfg.empty() && e->tuned_nrhs == nrhs;
     std::vector<int2> work;
     e->work_off.assign(e->levels.size() + 1, 0);
+    e->work_w.assign(e->levels.size(), tcw_default);
     for (size_t h = 0; h < e->levels.size(); ++h) {
         e->work_off[h] = (int)work.size();
+        const int tcw = tuned && e->lvl_cfg[4 * h + 1] ? 8 * e->lvl_cfg[4 * h + 1] : tcw_default;
+        e->work_w[h] = tcw;
+        const int nslice = (nrhs + tcw - 1) / tcw;
         const LevelInfo &L = e->levels[h];
         for (int t = 0; t < L.count; ++t) {
             const int v = sy.lvl_nodes[L.first + t];
@@ -673,11 +678,9 @@ static const unsigned char *build_mask(gm_engine *e, int nrhs, const RhsPattern 
         }
     }
     e->work_off[e->levels.size()] = (int)work.size();
-    e->work_chunk = 0;
-    if (e->d_work.ensure((work.size() + 1) * sizeof(int2)) == cudaSuccess &&
-        cudaMemcpyAsync(e->d_work.p, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice, e->st) ==
-            cudaSuccess)
-        e->work_chunk = tcw;
+    e->have_work = e->d_work.ensure((work.size() + 1) * sizeof(int2)) == cudaSuccess &&
+                   cudaMemcpyAsync(e->d_work.p, work.data(), work.size() * sizeof(int2), cudaMemcpyHostToDevice,
+                                   e->st) == cudaSuccess;
     cudaStreamSynchronize(e->st);   // m and work are released on return
     return e->d_mask.as<unsigned char>();
 }
@@ -1121,6 +1124,100 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
 }
 
 }  // namespace gm
+
+namespace gm {
+
+// Device time of every level of one forward and one backward pass over
+// right-hand sides held in xT (all dense), with the engine's current
+// per-level tile table.
+template <class R>
+static void time_levels(gm_engine *e, void *xT, int nrhs, std::vector<float> &fwd, std::vector<float> &bwd) {
+    const int nl = (int)e->levels.size();
+    SolveArgs<R> a{};
+    a.s = e->dsym;
+    a.front = e->d_front.p;
+    a.x = xT;
+    a.w = e->d_w.p;
+    a.nf = e->nf;
+    a.nrhs = nrhs;
+    a.ldr = nrhs;
+    const int nchunk = (nrhs + 31) / 32;
+    a.rch = (nrhs + nchunk - 1) / nchunk;
+    a.lvl_cfg = e->lvl_cfg.data();
+    std::vector<cudaEvent_t> ev(2 * nl + 1);
+    for (auto &x : ev) cudaEventCreate(&x);
+    cudaEventRecord(ev[0], e->st);
+    for (int h = 0; h < nl; ++h) {
+        launch_solve_forward_level<R>(a, e->levels[h], e->st);
+        cudaEventRecord(ev[1 + h], e->st);
+    }
+    for (int h = nl - 1; h >= 0; --h) {
+        launch_solve_backward_level<R>(a, e->levels[h], e->st);
+        cudaEventRecord(ev[1 + nl + (nl - 1 - h)], e->st);
+    }
+    cudaEventSynchronize(ev[2 * nl]);
+    fwd.assign(nl, 0.f);
+    bwd.assign(nl, 0.f);
+    for (int h = 0; h < nl; ++h) {
+        cudaEventElapsedTime(&fwd[h], ev[h], ev[1 + h]);
+        cudaEventElapsedTime(&bwd[h], ev[nl + (nl - 1 - h)], ev[1 + nl + (nl - 1 - h)]);
+    }
+    for (auto &x : ev) cudaEventDestroy(x);
+}
+
+}  // namespace gm
+
+extern "C" int gm_autotune(gm_engine *e, int nrhs, int reps) {
+    if (!e || nrhs <= 0) return fail(GM_ERROR_INVALID, "gm_autotune: bad argument");
+    if (!e->factored) return fail(GM_ERROR_STATE, "gm_autotune: no factorisation (gm_factor)");
+    GM_CUDA(cudaSetDevice(e->device));
+    if (reps <= 0) reps = 2;
+    const bool fp64 = e->cfg.precision == GM_PREC_FP64;
+    const size_t cnt = (size_t)e->nf * e->n * nrhs;
+    GM_ALLOC(e->d_t, cnt * e->csize());
+    GM_ALLOC(e->d_w, (size_t)e->nf * e->sym.rhs_total * nrhs * e->csize());
+    GM_CUDA(cudaMemsetAsync(e->d_t.p, 0, cnt * e->csize(), e->st));   // the pass's cost does not depend on the values
+    const int nl = (int)e->levels.size();
+    // candidate tiles: row height 32 / 64 x slice width 32 / 40 columns
+    const int cand[4][2] = {{32, 4}, {64, 4}, {32, 5}, {64, 5}};
+    std::vector<float> best_f(nl, 1e30f), best_b(nl, 1e30f);
+    std::vector<int> pick(4 * nl, 0);
+    std::vector<float> tf, tb;
+    for (const auto &c : cand) {
+        e->lvl_cfg.assign(4 * nl, 0);
+        for (int h = 0; h < nl; ++h) {
+            e->lvl_cfg[4 * h + 0] = c[0]; e->lvl_cfg[4 * h + 1] = c[1];
+            e->lvl_cfg[4 * h + 2] = c[0]; e->lvl_cfg[4 * h + 3] = c[1];
+        }
+        std::vector<float> sf(nl, 1e30f), sb(nl, 1e30f);
+        for (int r = 0; r < reps; ++r) {   // best of reps (the first run also loads the kernels)
+            if (fp64) gm::time_levels<double>(e, e->d_t.p, nrhs, tf, tb);
+            else gm::time_levels<float>(e, e->d_t.p, nrhs, tf, tb);
+            for (int h = 0; h < nl; ++h) { sf[h] = std::min(sf[h], tf[h]); sb[h] = std::min(sb[h], tb[h]); }
+        }
+        for (int h = 0; h < nl; ++h) {
+            if (sf[h] < best_f[h]) { best_f[h] = sf[h]; pick[4 * h + 0] = c[0]; pick[4 * h + 1] = c[1]; }
+            if (sb[h] < best_b[h]) { best_b[h] = sb[h]; pick[4 * h + 2] = c[0]; pick[4 * h + 3] = c[1]; }
+        }
+    }
+    GM_CUDA(cudaGetLastError());
+    e->lvl_cfg = pick;
+    e->tuned_nrhs = nrhs;
+    if (std::getenv("GM_TRACE_LEVELS"))
+        for (int h = 0; h < nl; ++h)
+            std::fprintf(stderr, "autotune level %2d: forward rt %d slice %d (%.3f ms), backward rt %d slice %d (%.3f ms)\n",
+                         h, pick[4 * h], 8 * pick[4 * h + 1], best_f[h], pick[4 * h + 2], 8 * pick[4 * h + 3], best_b[h]);
+    return GM_OK;
+}
+
+extern "C" int gm_autotune_table(const gm_engine *e, int *nrhs, int *table, int nlevels) {
+    if (!e || !nrhs) return fail(GM_ERROR_INVALID, "gm_autotune_table: bad argument");
+    *nrhs = e->tuned_nrhs;
+    if (table && nlevels > 0)
+        for (int i = 0; i < 4 * std::min(nlevels, (int)e->levels.size()); ++i)
+            table[i] = i < (int)e->lvl_cfg.size() ? e->lvl_cfg[i] : 0;
+    return GM_OK;
+}
 
 extern "C" int gm_refine_report(const gm_engine *e, int nmat, gm_refine_info *out) {
     if (!e || !out) return fail(GM_ERROR_INVALID, "gm_refine_report: null argument");

@@ -105,8 +105,13 @@ struct gm_engine {
     int xf_ns = 0, xa_ns = 0; // right-hand sides held in d_xf / d_xa (0: none valid)
     gm::DevBuf d_mask;       // forward-pass pruning mask of the current solve
     gm::DevBuf d_work;       // its live (front position, slice) pairs per level
+    // substitution tiles per level chosen by gm_autotune for tuned_nrhs
+    // right-hand sides and this precision: {fwd rt, fwd B, bwd rt, bwd B}
+    std::vector<int> lvl_cfg;
+    int tuned_nrhs = 0;
     std::vector<int> work_off;
-    int work_chunk = 0;      // slice width the pairs were built for (0: no list)
+    std::vector<int> work_w; // per level: slice width the pairs were built for
+    bool have_work = false;
     std::vector<double> last_grad0, last_grad1;
     // per-shot gradient taper of ass_grad (SWS_TAPER_CIRCULAR_PER_SHOT 0, 1, 2),
     // its radius (SRTRADIUS, metres) and square half-width (FILTSIZE)

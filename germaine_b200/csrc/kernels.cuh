@@ -144,10 +144,13 @@ struct SolveArgs {
     const int *xmap;
     // live (front position in its level, slice) pairs of a pruned forward
     // pass (device), level h at work[work_off[h] .. work_off[h + 1]) (host
-    // offsets), for slices of work_chunk right-hand sides; NULL: no list
+    // offsets), for slices of work_w[h] right-hand sides (host); NULL: no list
     const int2 *work;
     const int *work_off;
-    int work_chunk;
+    const int *work_w;
+    // host: per level {forward rt, forward B, backward rt, backward B} chosen
+    // by the autotuner (gm_autotune; 0 entries keep the default rule), or NULL
+    const int *lvl_cfg;
 };
 
 // right-hand sides per substitution slice for nrhs right-hand sides

@@ -628,7 +628,7 @@ static void forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_
     const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
     static const bool no_small = env_int("GM_NO_FWD_SMALL") != 0;
     if (RT == 32 && L.max_piv <= SNB && !no_small) {   // one pivot block per front: fused pivot + ring kernel
-        if (a.work && a.work_chunk == 8 * B) {   // pruned pass: only the live (front, slice) pairs
+        if (a.work && a.work_w[L.index] == 8 * B) {   // pruned pass: only the live (front, slice) pairs
             const int wofs = a.work_off[L.index];
             const int nlive = a.work_off[L.index + 1] - wofs;
             if (nlive == 0) return;
@@ -699,9 +699,30 @@ static void level_pass(bool fwd, const SolveArgs<R> &a, const LevelInfo &L, cuda
     }
 }
 
+template <class R, int B>
+static void level_pass_rt(bool fwd, int rt, const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
+    if (rt == 32) {
+        if (fwd) forward_level<R, 32, B>(a, L, st);
+        else backward_level<R, 32, B>(a, L, st);
+    } else {
+        if (fwd) forward_level<R, 64, B>(a, L, st);
+        else backward_level<R, 64, B>(a, L, st);
+    }
+}
+
+// The level's tile height and slice width: the autotuned choice when the
+// engine holds one (a.lvl_cfg, per level: forward rt, forward B, backward
+// rt, backward B; 0 = the default rule), else the default rules above.
 template <class R>
 static void dispatch(bool fwd, const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
     if (L.count == 0 || solve_nfz(a) <= 0) return;
+    if (a.lvl_cfg) {
+        const int *c = a.lvl_cfg + 4 * L.index + (fwd ? 0 : 2);
+        const int rt = c[0] ? c[0] : level_rt(L), b = c[1] ? c[1] : slice_b<R>(a.nrhs);
+        if (b == 5) level_pass_rt<R, 5>(fwd, rt, a, L, st);
+        else level_pass_rt<R, 4>(fwd, rt, a, L, st);
+        return;
+    }
     if (slice_b<R>(a.nrhs) == 5) level_pass<R, 5>(fwd, a, L, st);
     else level_pass<R, 4>(fwd, a, L, st);
 }

@@ -130,6 +130,17 @@ class Engine:
         self.freqs = f
         return self.last_status
 
+    def autotune(self, nrhs: int, reps: int = 2):
+        """Choose the substitution tiles of every level for nrhs right-hand
+        sides by timing the candidates on the current factors (gm_autotune);
+        returns the table [level] -> (fwd rows, fwd slice, bwd rows, bwd slice)."""
+        check(self.lib.gm_autotune(self._h, nrhs, reps))
+        nl = self.stats()["nlevels"]
+        tab = np.zeros(4 * nl, np.int32)
+        n = ctypes.c_int(0)
+        check(self.lib.gm_autotune_table(self._h, ctypes.byref(n), ptr(tab), nl))
+        return [(int(a), 8 * int(b), int(c), 8 * int(d)) for a, b, c, d in tab.reshape(nl, 4)]
+
     def refine_report(self) -> list[dict]:
         """Per-matrix refinement records of the last solve (gm_refine_report):
         first / final max relative residual, sweeps, method."""

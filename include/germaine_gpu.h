@@ -180,6 +180,18 @@ int gm_factor_values(gm_engine *e, int nmat, const double *re, const double *im)
  * src/AC/init_A_AC_9p_pml.c:75-80).  Any of the four outputs may be NULL. */
 int gm_get_triplets(gm_engine *e, int ifreq, double *Ar, double *Ai, int32_t *irow, int32_t *icol);
 
+/* Autotuner of the substitution's tiles: on the current factors, times one
+ * forward and one backward pass over nrhs dense right-hand sides for every
+ * candidate tile (32- or 64-row output tiles x 32- or 40-column
+ * right-hand-side slices; best of `reps` runs each, 0 = 2) level by level,
+ * and keeps per level and pass the fastest.  Solves with nrhs right-hand
+ * sides use that table from then on (other counts keep the default
+ * rules).  gm_autotune_table returns the tuned right-hand-side count and,
+ * for nlevels levels, {forward rows, forward slice/8, backward rows,
+ * backward slice/8} per level.  No counterpart in the reference. */
+int gm_autotune(gm_engine *e, int nrhs, int reps);
+int gm_autotune_table(const gm_engine *e, int *nrhs, int *table, int nlevels);
+
 /* Per-matrix refinement records of the last solve: out[0 .. nmat) for the
  * nmat matrices of the factorised batch (nmat must equal that count).  No
  * counterpart in the reference (UMFPACK's Info array reports one solve); it

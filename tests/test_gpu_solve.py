@@ -169,3 +169,32 @@ def test_mixed_refinement_modes(refine, sys_):
             assert r["method"] == "ir"
         if refine == GM_REFINE_MODE_GMRES:
             assert r["method"] == "gmres"
+
+
+@pytest.mark.parametrize("precision", [GM_PREC_FP64, GM_PREC_C64_IR], ids=["fp64", "c64ir"])
+def test_autotuned_tiles_keep_the_solution(precision):
+    """The autotuner picks, per level and pass, the fastest of the
+    candidate substitution tiles; solves with the tuned table give the
+    SuperLU solution, and other right-hand-side counts keep the defaults."""
+    nx, ny, dh, npml = 90, 64, 10.0, 10
+    g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml)
+    m0, m1 = _setup(nx, ny, dh, npml, seed=13)
+    rng = np.random.default_rng(2)
+    nrhs = 45
+    b = rng.standard_normal((2, g.n, nrhs)) + 1j * rng.standard_normal((2, g.n, nrhs))
+    with Engine(nx, ny, dh, npml, precision=precision, leaf_max=24) as e:
+        e.set_model(m0, m1)
+        e.factor([8.0, 19.0])
+        table = e.autotune(nrhs)
+        assert len(table) == e.stats()["nlevels"]
+        for fr, fs, br, bs in table:
+            assert fr in (32, 64) and br in (32, 64) and fs in (32, 40) and bs in (32, 40)
+        x = e.solve(b)
+        x7 = e.solve(b[:, :, :7])
+        assert e.stats()["ir_residual"] <= 1e-10
+    port = O.Port(g)
+    for i, f in enumerate([8.0, 19.0]):
+        ds = OS.DirectSolver(OS.operator(OS.assembled_matrix(g, *port.assemble(1, f, m0, m1))))
+        tol = 1e-10 if precision == GM_PREC_FP64 else 1e-8
+        assert _rel(x[i], ds.solve(b[i])) <= tol
+        assert _rel(x7[i], ds.solve(b[i][:, :7])) <= tol
