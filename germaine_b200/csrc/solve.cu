@@ -415,6 +415,10 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
     }
 }
 
+// (The complex128 small-front kernels are held to 80 registers, six CTAs per
+// SM: measured on the leaf levels they stall on global loads first, so more
+// resident warps pay; the complex64 ones need fewer registers anyway.)
+//
 // Forward pass of a whole front whose pivots fit one 32-pivot block (the
 // small fronts of the lower levels): the children's update vectors are added
 // into x at the pivots, y = Dinv x_piv is formed in shared memory and written
@@ -424,7 +428,7 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
 // wofs >= 0: the CTA's (front position, slice) is work[wofs + blockIdx.x],
 // the live pairs of a pruned pass; wofs < 0: (blockIdx.y, blockIdx.x).
 template <class R, bool TRANS, int B>
-__global__ void __launch_bounds__(NT) k_fwd_small(SolveArgs<R> a, int lvl_first, int wofs) {
+__global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_fwd_small(SolveArgs<R> a, int lvl_first, int wofs) {
     using C = cplx<R>;
     constexpr int RT = 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -514,7 +518,7 @@ __global__ void __launch_bounds__(NT) k_fwd_small(SolveArgs<R> a, int lvl_first,
 // in shared memory, then x_piv = Dinv t -- k_bwd_ring and k_bwd_piv in one
 // CTA, without writing t to x in between.
 template <class R, bool TRANS, int B>
-__global__ void __launch_bounds__(NT) k_bwd_small(SolveArgs<R> a, int lvl_first) {
+__global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_bwd_small(SolveArgs<R> a, int lvl_first) {
     using C = cplx<R>;
     constexpr int RT = 32;
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -82,10 +82,12 @@ def smooth_random_model(extent_x: float, extent_y: float, dh: float, nx0: int, n
 
 
 def run_multigrid(cases, nshots: int, seed: int = 7, precision: int = 1, workers: int | None = None,
-                  row: int = 2):
+                  row: int = 2, refine: int = 1):
     """Factorise and solve every grid's frequency for nshots shots along
     model row `row`, all grids concurrently.  Returns (shot-solves/s over
-    the whole set, wall seconds, per-grid records)."""
+    the whole set, wall seconds, per-grid records).  refine defaults to
+    plain refinement sweeps: with every grid's workspaces resident at once
+    there is no room for GMRES-IR's Krylov vectors."""
     extent_x = max(c.nx0 * c.dh for c in cases)
     extent_y = max(c.ny0 * c.dh for c in cases)
     engines, setups = [], []
@@ -96,7 +98,7 @@ def run_multigrid(cases, nshots: int, seed: int = 7, precision: int = 1, workers
         ys = np.full(nshots, row * c.dh, np.float32)
         rx = np.arange(1, c.nx0, max(1, c.nx0 // 200), dtype=np.int32)
         ry = np.full(rx.size, row, np.int32)
-        e = Engine(nx, ny, c.dh, c.npml, precision=precision)
+        e = Engine(nx, ny, c.dh, c.npml, precision=precision, refine=refine)
         e.set_model(vp, rho)
         engines.append(e)
         setups.append((xs, ys, rx, ry))
