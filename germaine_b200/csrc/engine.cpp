@@ -284,15 +284,19 @@ static int build_cb_plan(gm_engine *e) {
     using C = cplx_any<R>;
     const Symbolic &s = e->sym;
     const bool c64 = e->cfg.precision == GM_PREC_C64_IR;
-    // Smallest contribution block routed to the tcgen05 kernel.  Off by
-    // default: the kernel's accumulation keeps a ~1e-7 relative bias on
-    // same-sign sums (truncation inside each MMA) that costs the refinement
-    // two extra sweeps on the 841 x 227 benchmark, while the block GEMM is a
-    // small part of the factorisation time; GM_TC_MIN_BLOCK=<rows> enables it.
-    int kTcMinBlock = 1 << 30;
+    // Smallest contribution block routed to the tcgen05 kernel
+    // (gm_config.tc_min_block; GM_TC_MIN_BLOCK=<rows> overrides it).  Off by
+    // default: measured on 841 x 227 with 10 frequencies x 100 shots, routing
+    // the blocks of >= 128 rows makes the complex64 factorisation slower
+    // (14.72 vs 14.24 ms: the kernel keeps its tensor pipe 15-20 % busy) and
+    // its truncating accumulation costs the 3 Hz matrix a fourth sweep
+    // (92.5 -> 110 ms per step), while the block GEMM is ~1.4 % of the GPU
+    // time of a step.
+    int kTcMinBlock = e->cfg.tc_min_block > 0 ? e->cfg.tc_min_block : 1 << 30;
     if (const char *v = std::getenv("GM_TC_MIN_BLOCK")) kTcMinBlock = std::atoi(v);
     std::vector<GemmProb<R>> probs;
     std::vector<int4> tiles;
+    e->stats.tc_tiles = 0;
     e->cb_plan.assign(e->levels.size(), {});
     C *base = e->d_front.as<C>();
     for (size_t h = 0; h < e->levels.size(); ++h) {
@@ -325,6 +329,7 @@ static int build_cb_plan(gm_engine *e) {
                     for (int b = 0; b < (m + tc - 1) / tc; ++b) tiles.push_back(make_int4(id, a, b, 0));
             }
         pl.ntiles = (int)(tiles.size() - pl.tile_off);
+        if (backend == 1) e->stats.tc_tiles += pl.ntiles;
     }
     GM_ALLOC(e->d_cb_probs, probs.size() * sizeof(GemmProb<R>) + 16);
     GM_ALLOC(e->d_cb_tiles, tiles.size() * sizeof(int4) + 16);

@@ -80,6 +80,8 @@ typedef struct {
     int32_t ir_max_iter;     /* refinement iteration cap (0 = default 10) */
     int32_t refine;          /* GM_REFINE_MODE_* (0 = auto) */
     int32_t gmres_restart;   /* GMRES iterations per cycle (0 = default 8, at most 8) */
+    int32_t tc_min_block;    /* complex64: contribution blocks of at least this many rows
+                                update on the tcgen05 tensor cores (0 = none) */
 } gm_config;
 
 /* ---- refinement of the solves (gm_config.refine) ---- */
@@ -107,6 +109,7 @@ typedef struct {
     int64_t kernel_launches;    /* kernels launched by this library in this process */
     int64_t u_entries;          /* stored U entries (pivot rows) per frequency: the backward pass's factor */
     double ms_subst_bwd;        /* device time of the backward passes of those substitutions */
+    int64_t tc_tiles;           /* output tiles of the factorisation routed to tcgen05 */
 } gm_stats;
 
 /* Refinement record of one matrix in the last solve (gm_solve and the solves

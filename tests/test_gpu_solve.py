@@ -87,20 +87,23 @@ def test_te_transpose_solve():
     assert _rel(x[0], xr) <= 1e-10
 
 
-@pytest.mark.parametrize("precision", [GM_PREC_FP64, GM_PREC_C64_IR], ids=["fp64", "c64ir"])
-def test_solve_large_fronts(precision):
-    """A grid whose upper fronts have contribution blocks above 96 rows, so
-    the complex64 path runs its contribution-block updates on tcgen05."""
+@pytest.mark.parametrize("precision,tc", [(GM_PREC_FP64, 0), (GM_PREC_C64_IR, 0), (GM_PREC_C64_IR, 96)],
+                         ids=["fp64", "c64ir", "c64ir-tcgen05"])
+def test_solve_large_fronts(precision, tc):
+    """A grid whose upper fronts have contribution blocks above 96 rows; with
+    tc_min_block = 96 the complex64 factorisation routes those blocks'
+    updates to the tcgen05 kernel (counted in the statistics)."""
     nx, ny, dh, npml = 230, 170, 10.0, 12
     g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml)
     m0, m1 = _setup(nx, ny, dh, npml, seed=8)
     rng = np.random.default_rng(12)
     b = rng.standard_normal((1, g.n, 6)) + 1j * rng.standard_normal((1, g.n, 6))
-    with Engine(nx, ny, dh, npml, precision=precision) as e:
+    with Engine(nx, ny, dh, npml, precision=precision, tc_min_block=tc) as e:
         e.set_model(m0, m1)
         e.factor([18.0])
         x = e.solve(b)
         st = e.stats()
+    assert (st["tc_tiles"] > 0) == (tc > 0)
     A = OS.assembled_matrix(g, *O.Port(g).assemble(1, 18.0, m0, m1))
     ds = OS.DirectSolver(OS.operator(A))
     xr = ds.solve(b[0])
