@@ -73,7 +73,7 @@ EXPORTS = [
     "gm_get_gradient_fp64", "gm_get_wavefield_fp64", "gm_get_misfit_fp64", "gm_obj_each", "gm_gauss_filt", "gm_solve_noalloc", "gm_hessian", "gm_get_hessian_fp64", "gm_apply_hess", "gm_precond",
     "gm_lbfgs_create", "gm_lbfgs_destroy", "gm_lbfgs_step", "gm_lbfgs_rotate", "gm_lbfgs_zero",
     "gm_lbfgs_check_descent", "gm_lbfgs_get_old", "gm_lbfgs_set_old", "gm_mat_change",
-    "gm_set_shot_taper", "gm_set_shot_block", "gm_memory_estimate", "gm_set_invmat", "gm_set_source_wavelet", "gm_stf_dft", "gm_taper_grad_shot", "gm_taper_grad_shot1", "gm_tikhonov_cost_te", "gm_tikhonov_grad_te",
+    "gm_set_shot_taper", "gm_set_shot_block", "gm_set_refine", "gm_memory_estimate", "gm_set_invmat", "gm_set_source_wavelet", "gm_stf_dft", "gm_taper_grad_shot", "gm_taper_grad_shot1", "gm_tikhonov_cost_te", "gm_tikhonov_grad_te",
     "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_read_grid", "gm_cgemm_sub_c64", "gm_wait_probe", "gm_peak_fp64",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
@@ -149,6 +149,7 @@ def load() -> ctypes.CDLL:
     lib.gm_set_shot_taper.argtypes = [vp, i32, f32, i32]
     lib.gm_set_invmat.argtypes = [vp, i32]
     lib.gm_set_shot_block.argtypes = [vp, i32]
+    lib.gm_set_refine.argtypes = [vp, i32, i32]
     lib.gm_memory_estimate.argtypes = [vp, i32, ctypes.POINTER(ctypes.c_size_t), ctypes.POINTER(ctypes.c_size_t)]
     lib.gm_set_source_wavelet.argtypes = [vp, i32, vp]
     lib.gm_stf_dft.argtypes = [ctypes.c_char_p, i32, f32, vp]

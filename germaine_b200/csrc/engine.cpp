@@ -19,6 +19,7 @@
 #include <cstdlib>
 #include <cstring>
 #include <memory>
+#include <mutex>
 #include <new>
 
 #include "host_setup.h"
@@ -690,6 +691,12 @@ static const unsigned char *build_mask(gm_engine *e, int nrhs, const RhsPattern 
     return e->d_mask.as<unsigned char>();
 }
 
+// serialises the GMRES workspace sizing of engines on different host threads
+static std::mutex &gmres_alloc_mutex() {
+    static std::mutex mu;
+    return mu;
+}
+
 // GMRES-IR for the matrices `gset` of the batch: restarted GMRES(m) on the
 // correction equation M' d = b - M' x, one run per (matrix, right-hand
 // side), in FP64 with the working-precision factors as right
@@ -709,21 +716,31 @@ static int gmres_refine(gm_engine *e, int sys, int nrhs, double2 *d_x, const Res
     const double tol = e->cfg.ir_tol;
     const size_t per = (size_t)n * nrhs;
     const size_t vstride = (size_t)ng * per;   // one Krylov slot holds all ng matrices
-    // restart length: the configured one, shortened while the Krylov and
-    // preconditioned vectors would not fit 80 % of the device memory left
+    // restart length: the configured one when the Krylov and preconditioned
+    // vectors already held fit it; otherwise shortened while they would not
+    // fit 80 % of the device memory left, and again while their allocation
+    // fails (engines on other host threads allocate at the same time).  The
+    // query and the allocation hold a process-wide lock, so concurrent
+    // engines see each other's workspaces.
     int m = e->cfg.gmres_restart;
-    {
+    const auto v_bytes = [&](int mm) { return (size_t)(mm + 1) * vstride * sizeof(double2); };
+    const auto z_bytes = [&](int mm) { return (size_t)mm * vstride * sizeof(cplx_any<R>); };
+    if (!(e->d_gv.p && e->d_gz.p && e->d_gv.bytes >= v_bytes(m) && e->d_gz.bytes >= z_bytes(m))) {
+        std::lock_guard<std::mutex> lock(gmres_alloc_mutex());
         size_t fr = 0, tot = 0;
         if (cudaMemGetInfo(&fr, &tot) == cudaSuccess) {
             const size_t avail = (fr + e->d_gv.bytes + e->d_gz.bytes) / 10 * 8;
-            while (m >= 2 && (size_t)(m + 1) * vstride * sizeof(double2) + (size_t)m * vstride * sizeof(cplx_any<R>) > avail)
-                --m;
+            while (m >= 2 && v_bytes(m) + z_bytes(m) > avail) --m;
+        }
+        for (; m >= 2; --m) {
+            if (e->d_gv.ensure(v_bytes(m)) == cudaSuccess && e->d_gz.ensure(z_bytes(m)) == cudaSuccess) break;
+            e->d_gv.release();
+            e->d_gz.release();
+            (void)cudaGetLastError();   // the failed allocation is not an error of this solve
         }
         if (m < 2) return GM_WARNING_NOT_CONVERGED;   // no room: the caller refines with plain sweeps
     }
-    GM_ALLOC(e->d_gv, (size_t)(m + 1) * vstride * sizeof(double2));
-    GM_ALLOC(e->d_gz, (size_t)m * vstride * sizeof(cplx_any<R>));
-    const int nblk_r = (n + 63) / 64, nblk_g = (n + 255) / 256;
+    const int nblk_r = residual_blocks(n), nblk_g = (n + 255) / 256;
     const size_t part_words = std::max((size_t)nblk_r * ng * nrhs * 2, (size_t)nblk_g * ng * nrhs * (m + 1) * 2);
     GM_ALLOC(e->d_gpart, part_words * sizeof(double));
     GM_ALLOC(e->d_gnorm, (size_t)ng * nrhs * (m + 1) * 2 * sizeof(double));
@@ -961,7 +978,7 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     const bool fp64 = e->cfg.precision == GM_PREC_FP64;
     GM_ALLOC(e->d_t, cnt * e->csize());
     GM_ALLOC(e->d_w, (size_t)e->nf * e->sym.rhs_total * nrhs * e->csize());
-    const int nblk_max = (e->n + 63) / 64;
+    const int nblk_max = residual_blocks(e->n);
     GM_ALLOC(e->d_part, (size_t)nblk_max * e->nf * nrhs * 2 * sizeof(double));
     GM_ALLOC(e->d_norm, (size_t)e->nf * nrhs * 2 * sizeof(double));
 
@@ -1183,28 +1200,71 @@ extern "C" int gm_autotune(gm_engine *e, int nrhs, int reps) {
     GM_ALLOC(e->d_w, (size_t)e->nf * e->sym.rhs_total * nrhs * e->csize());
     GM_CUDA(cudaMemsetAsync(e->d_t.p, 0, cnt * e->csize(), e->st));   // the pass's cost does not depend on the values
     const int nl = (int)e->levels.size();
-    // candidate tiles: row height 32 / 64 x slice width 32 / 40 columns
-    const int cand[4][2] = {{32, 4}, {64, 4}, {32, 5}, {64, 5}};
+    // per level, each pass direction: the fastest of the candidate tiles
+    // (row height 32 / 64 x slice width 32 / 40 columns), best of reps
+    // timings; a candidate replaces the built-in choice (lvl_cfg 0) only
+    // when it is at least 3 % faster, so timing noise keeps the default
+    const int cand[5][2] = {{0, 0}, {32, 4}, {64, 4}, {32, 5}, {64, 5}};
     std::vector<float> best_f(nl, 1e30f), best_b(nl, 1e30f);
     std::vector<int> pick(4 * nl, 0);
     std::vector<float> tf, tb;
+    auto time_pass = [&](std::vector<float> &sf, std::vector<float> &sb) {
+        sf.assign(nl, 1e30f);
+        sb.assign(nl, 1e30f);
+        for (int r = 0; r < reps; ++r) {   // best of reps (the first run also loads the kernels)
+            if (fp64) gm::time_levels<double>(e, e->d_t.p, nrhs, tf, tb);
+            else gm::time_levels<float>(e, e->d_t.p, nrhs, tf, tb);
+            for (int h = 0; h < nl; ++h) { sf[h] = std::min(sf[h], tf[h]); sb[h] = std::min(sb[h], tb[h]); }
+        }
+    };
     for (const auto &c : cand) {
         e->lvl_cfg.assign(4 * nl, 0);
         for (int h = 0; h < nl; ++h) {
             e->lvl_cfg[4 * h + 0] = c[0]; e->lvl_cfg[4 * h + 1] = c[1];
             e->lvl_cfg[4 * h + 2] = c[0]; e->lvl_cfg[4 * h + 3] = c[1];
         }
-        std::vector<float> sf(nl, 1e30f), sb(nl, 1e30f);
-        for (int r = 0; r < reps; ++r) {   // best of reps (the first run also loads the kernels)
-            if (fp64) gm::time_levels<double>(e, e->d_t.p, nrhs, tf, tb);
-            else gm::time_levels<float>(e, e->d_t.p, nrhs, tf, tb);
-            for (int h = 0; h < nl; ++h) { sf[h] = std::min(sf[h], tf[h]); sb[h] = std::min(sb[h], tb[h]); }
-        }
+        std::vector<float> sf, sb;
+        time_pass(sf, sb);
+        const float margin = c[0] ? 0.97f : 1.0f;
         for (int h = 0; h < nl; ++h) {
-            if (sf[h] < best_f[h]) { best_f[h] = sf[h]; pick[4 * h + 0] = c[0]; pick[4 * h + 1] = c[1]; }
-            if (sb[h] < best_b[h]) { best_b[h] = sb[h]; pick[4 * h + 2] = c[0]; pick[4 * h + 3] = c[1]; }
+            // forward levels of fronts with at most 32 pivots keep 32-row
+            // tiles: only that kernel runs the pruned first pass of
+            // spike right-hand sides from a work list
+            const bool fwd_ok = !(c[0] == 64 && e->levels[h].max_piv <= 32);
+            if (fwd_ok && sf[h] < margin * best_f[h]) {
+                best_f[h] = sf[h]; pick[4 * h + 0] = c[0]; pick[4 * h + 1] = c[1];
+            }
+            if (sb[h] < margin * best_b[h]) { best_b[h] = sb[h]; pick[4 * h + 2] = c[0]; pick[4 * h + 3] = c[1]; }
         }
     }
+    // the per-level picks must also win over whole passes (a level's tiles
+    // change what the next level finds in L2): interleaved timings of the
+    // picked table against the built-in choice, the faster total kept
+    {
+        std::vector<float> sf, sb;
+        float t_pick = 1e30f, t_def = 1e30f;
+        for (int r = 0; r < 2; ++r) {
+            e->lvl_cfg = pick;
+            time_pass(sf, sb);
+            float t = 0;
+            for (int h = 0; h < nl; ++h) t += sf[h] + sb[h];
+            t_pick = std::min(t_pick, t);
+            e->lvl_cfg.assign(4 * nl, 0);
+            time_pass(sf, sb);
+            t = 0;
+            for (int h = 0; h < nl; ++h) t += sf[h] + sb[h];
+            t_def = std::min(t_def, t);
+        }
+        if (!(t_pick < t_def)) pick.assign(4 * nl, 0);
+    }
+    // the table names every level's tiles: built-in choices resolved
+    const int b_def = gm::solve_slice_width(nrhs, fp64) / 8;
+    for (int h = 0; h < nl; ++h)
+        for (int d = 0; d < 2; ++d)
+            if (pick[4 * h + 2 * d] == 0) {
+                pick[4 * h + 2 * d] = gm::solve_level_rt(e->levels[h]);
+                pick[4 * h + 2 * d + 1] = b_def;
+            }
     GM_CUDA(cudaGetLastError());
     e->lvl_cfg = pick;
     e->tuned_nrhs = nrhs;
@@ -1221,6 +1281,17 @@ extern "C" int gm_autotune_table(const gm_engine *e, int *nrhs, int *table, int 
     if (table && nlevels > 0)
         for (int i = 0; i < 4 * std::min(nlevels, (int)e->levels.size()); ++i)
             table[i] = i < (int)e->lvl_cfg.size() ? e->lvl_cfg[i] : 0;
+    return GM_OK;
+}
+
+extern "C" int gm_set_refine(gm_engine *e, int refine, int gmres_restart) {
+    if (!e) return fail(GM_ERROR_INVALID, "gm_set_refine: null engine");
+    if (refine < GM_REFINE_MODE_AUTO || refine > GM_REFINE_MODE_GMRES)
+        return fail(GM_ERROR_INVALID, "unknown refinement mode %d", refine);
+    if (gmres_restart < 0) return fail(GM_ERROR_INVALID, "GMRES restart length must be >= 0");
+    e->cfg.refine = refine;
+    e->cfg.gmres_restart = gmres_restart == 0 || gmres_restart > gm::kGmresMaxRestart ? gm::kGmresMaxRestart
+                                                                                        : gmres_restart;
     return GM_OK;
 }
 

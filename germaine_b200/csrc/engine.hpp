@@ -30,8 +30,12 @@ struct DevBuf {
         if (nb <= bytes && p) return cudaSuccess;
         release();
         cudaError_t e = cudaMalloc(&p, nb ? nb : 16);
-        if (e == cudaSuccess) bytes = nb;
-        else p = nullptr;
+        if (e == cudaSuccess) {
+            bytes = nb;
+        } else {
+            p = nullptr;
+            (void)cudaGetLastError();   // reported through the return value, not left for later checks
+        }
         return e;
     }
     template <class T> T *as() const { return reinterpret_cast<T *>(p); }

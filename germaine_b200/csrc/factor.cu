@@ -28,6 +28,7 @@
 #include <cstdlib>
 #include "kernels.cuh"
 #include "cplx.cuh"
+#include "async_copy.cuh"
 
 namespace gm {
 
@@ -649,15 +650,6 @@ __device__ __forceinline__ cplx<R> static_pivot(cplx<R> piv, R pivtol, int &nper
     return piv;
 }
 
-// one complex element global -> shared without a register round trip
-// (cp.async; completes at cp_async_wait_all)
-__device__ __forceinline__ void cp_async_elem(double2 *dst, const double2 *src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
-}
-__device__ __forceinline__ void cp_async_elem(float2 *dst, const float2 *src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src));
-}
-
 template <class R, int NPR>
 __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_first) {
     using C = cplx<R>;
@@ -722,9 +714,7 @@ __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_
             if (j < s) P[tid + j * ldp] = x[j];
     }
     if (np) atomicAdd(&npert, np);
-    asm volatile("cp.async.commit_group;\n" ::: "memory");
-    asm volatile("cp.async.wait_all;\n" ::: "memory");
-    __syncthreads();
+    staged_sync();
 
     // 2. U12 = L11^-1 A12, one column per thread of warps 2 .. 7, while
     // warps 0 and 1 invert the pivot block's triangles (3.)

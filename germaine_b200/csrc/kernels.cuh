@@ -155,6 +155,8 @@ struct SolveArgs {
 
 // right-hand sides per substitution slice for nrhs right-hand sides
 int solve_slice_width(int nrhs, bool fp64);
+// the built-in tile height of a level's substitution kernels (32 or 64)
+int solve_level_rt(const LevelInfo &L);
 
 template <class R>
 void launch_solve_forward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st);
@@ -183,6 +185,8 @@ struct ResidArgs {
     const int *xmap;
     const int *omap;
 };
+// row blocks of the residual kernel for n unknowns (the partial-sum count)
+int residual_blocks(int n);
 // r = b - M x and per-(freq, rhs) partial sums of |r|^2 and |b|^2 into
 // part[nblk][nfz][nrhs][2]; returns nblk.
 int launch_residual(const ResidArgs &a, double *part, int max_blocks, cudaStream_t st);

@@ -99,6 +99,7 @@ int noalloc_prepare(int device) {
     unsigned char *base = nullptr;
     const int rc = scratch_address(device, &base);
     if (rc) return rc;
+    (void)cudaGetLastError();   // an earlier call's error is not this load's
     preload_solve_kernels();
     preload_refine_kernels();
     preload_gmres_kernels();
@@ -131,7 +132,7 @@ extern "C" int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d
         if (b0 < x0 + nb && x0 < b0 + nb)
             return gm::fail(GM_ERROR_INVALID, "gm_solve_noalloc: b and x overlap");
     }
-    const int nblk = (e->n + 63) / 64;
+    const int nblk = gm::residual_blocks(e->n);
     const int npairs = e->nf * nrhs;
     const size_t b_t = align256(cnt * cs);
     const size_t b_w = align256((size_t)e->nf * e->sym.rhs_total * nrhs * cs);

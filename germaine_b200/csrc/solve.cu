@@ -34,6 +34,7 @@
 
 #include "kernels.cuh"
 #include "cplx.cuh"
+#include "async_copy.cuh"
 
 namespace gm {
 
@@ -60,6 +61,10 @@ __device__ __forceinline__ C elem(const C *F, int f, int i, int c) {
     return TRANS ? F[c + (size_t)i * f] : F[i + (size_t)c * f];
 }
 
+// The staging helpers below issue asynchronous copies (every load of the
+// tile in flight at once, no register round trip); the tile is complete
+// after staged_sync().
+//
 // sm.L[q][row] = M'(i0 + row, c0 + q) for row < rows, q < qb.  Entries
 // outside are left as they are: tile_mma reads only q < qb, and rows >= rows
 // (or right-hand sides >= rn) only feed accumulators that are never stored,
@@ -69,12 +74,12 @@ __device__ __forceinline__ void stage_factor(SolveSmem<C, RT, B> &sm, const C *F
     if (!TRANS) {
         for (int t = threadIdx.x; t < RT * qb; t += NT) {
             const int row = t % RT, q = t / RT;
-            if (row < rows) sm.L[q][row] = F[(i0 + row) + (size_t)(c0 + q) * f];
+            if (row < rows) cp_async_elem(&sm.L[q][row], F + (i0 + row) + (size_t)(c0 + q) * f);
         }
     } else {
         for (int t = threadIdx.x; t < SNB * rows; t += NT) {
             const int q = t % SNB, row = t / SNB;
-            if (q < qb) sm.L[q][row] = F[(c0 + q) + (size_t)(i0 + row) * f];
+            if (q < qb) cp_async_elem(&sm.L[q][row], F + (c0 + q) + (size_t)(i0 + row) * f);
         }
     }
 }
@@ -89,16 +94,15 @@ __device__ __forceinline__ void stage_dinv(SolveSmem<C, RT, B> &sm, const C *F, 
     for (int t = threadIdx.x; t < SNB * kb; t += NT) {
         const int p = t % SNB, q = t / SNB;   // operator entry (p, q) -> sm.L[q][p], q < kb
         if (p >= kb) continue;
-        C v = czero<C>();
         const bool lower_src = FWD != TRANS;         // L^-1 (or its transpose) wanted
         const int r = TRANS ? q : p, c = TRANS ? p : q;  // position in the stored block
-        if (lower_src) {
-            if (r > c) v = F[(k0 + r) + (size_t)(k0 + c) * f];
-            else if (r == c) v = mk(decltype(v.x)(1), decltype(v.x)(0));
-        } else if (r <= c) {
-            v = F[(k0 + r) + (size_t)(k0 + c) * f];
+        const bool stored = lower_src ? r > c : r <= c;
+        if (stored) {
+            cp_async_elem(&sm.L[q][p], F + (k0 + r) + (size_t)(k0 + c) * f);
+        } else {
+            using RR = decltype(sm.L[0][0].x);
+            sm.L[q][p] = (lower_src && r == c) ? mk(RR(1), RR(0)) : czero<C>();
         }
-        sm.L[q][p] = v;
     }
 }
 
@@ -162,7 +166,7 @@ __device__ __forceinline__ void stage_rows(SolveSmem<C, RT, B> &sm, RowPtr row_p
     constexpr int TC = 8 * B;
     for (int t = threadIdx.x; t < qb * TC; t += NT) {
         const int q = t / TC, r = t % TC;
-        if (r < rn) sm.Y[q][r] = row_ptr(q)[r];
+        if (r < rn) cp_async_elem(&sm.Y[q][r], row_ptr(q) + r);
     }
 }
 
@@ -260,7 +264,7 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
         const int kb = min(SNB, c.s - k0);
         stage_dinv<C, true, TRANS, RT, B>(sm, c.F, c.f, k0, kb);
         stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
-        __syncthreads();
+        staged_sync();
         zero_acc(acc);
         tile_mma(sm, kb, acc, tr, tc, kb, c.rn);   // y_b = Dinv w_b
         __syncthreads();
@@ -278,7 +282,7 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
         for (int i0 = k0 + kb; i0 < c.s; i0 += RT) {
             const int rows = min(RT, c.s - i0);
             stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, k0, kb);
-            __syncthreads();
+            staged_sync();
             zero_acc(acc);
             tile_mma(sm, kb, acc, tr, tc, rows, c.rn);
             sub_acc(
@@ -311,7 +315,7 @@ __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, 
         const int qb = min(SNB, c.s - q0);
         stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, q0, qb);
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q0 + q] * ldr; }, qb, c.rn);
-        __syncthreads();
+        staged_sync();
         tile_mma(sm, qb, acc, tr, tc, rows, c.rn);
         __syncthreads();
     }
@@ -361,7 +365,7 @@ __global__ void __launch_bounds__(NT) k_bwd_ring(SolveArgs<R> a, int lvl_first, 
         const int jb = min(SNB, c.f - j0);
         stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, j0, jb);
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[j0 + q] * ldr; }, jb, c.rn);
-        __syncthreads();
+        staged_sync();
         tile_mma(sm, jb, acc, tr, tc, rows, c.rn);
         __syncthreads();
     }
@@ -388,7 +392,7 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
         const int k0 = b * SNB, kb = min(SNB, c.s - k0);
         stage_dinv<C, false, TRANS, RT, B>(sm, c.F, c.f, k0, kb);
         stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
-        __syncthreads();
+        staged_sync();
         zero_acc(acc);
         tile_mma(sm, kb, acc, tr, tc, kb, c.rn);   // x_b = Dinv t_b
         __syncthreads();
@@ -406,7 +410,7 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
         for (int i0 = 0; i0 < k0; i0 += RT) {
             const int rows = min(RT, k0 - i0);
             stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, k0, kb);
-            __syncthreads();
+            staged_sync();
             zero_acc(acc);
             tile_mma(sm, kb, acc, tr, tc, rows, c.rn);
             sub_acc([&](int row) { return xrow(i0 + row); }, rows, c.rn, acc, tr, tc);
@@ -468,7 +472,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_fwd_small(SolveA
     if (s > 0) {
         stage_dinv<C, true, TRANS, RT, B>(sm, c.F, c.f, 0, s);
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q] * ldr; }, s, c.rn);
-        __syncthreads();
+        staged_sync();
         zero_acc(acc);
         tile_mma(sm, s, acc, tr, tc, s, c.rn);   // y = Dinv x_piv
         __syncthreads();
@@ -488,7 +492,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_fwd_small(SolveA
     for (int i0 = s; i0 < c.f; i0 += RT) {
         const int rows = min(RT, c.f - i0);
         stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, 0, s);
-        __syncthreads();
+        staged_sync();
         zero_acc(acc);
         tile_mma(sm, s, acc, tr, tc, rows, c.rn);
 #pragma unroll
@@ -535,14 +539,14 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_bwd_small(SolveA
         const int jb = min(SNB, c.f - j0);
         stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, 0, s, j0, jb);
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[j0 + q] * ldr; }, jb, c.rn);
-        __syncthreads();
+        staged_sync();
         tile_mma(sm, jb, acc, tr, tc, s, c.rn);
         __syncthreads();
     }
     // t = y - acc in sm.Y (row q of the next product's right operand = pivot q)
     stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q] * ldr; }, s, c.rn);
     stage_dinv<C, false, TRANS, RT, B>(sm, c.F, c.f, 0, s);
-    __syncthreads();
+    staged_sync();
 #pragma unroll
     for (int p = 0; p < RT / 16; ++p) {
         const int row = tr + 16 * p;
@@ -757,6 +761,7 @@ void preload_solve_kernels() {
 }
 
 int solve_slice_width(int nrhs, bool fp64) { return 8 * (fp64 ? slice_b<double>(nrhs) : slice_b<float>(nrhs)); }
+int solve_level_rt(const LevelInfo &L) { return level_rt(L); }
 
 template void launch_solve_forward_level<double>(const SolveArgs<double> &, const LevelInfo &, cudaStream_t);
 template void launch_solve_forward_level<float>(const SolveArgs<float> &, const LevelInfo &, cudaStream_t);

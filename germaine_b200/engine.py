@@ -231,6 +231,11 @@ class Engine:
         """Cap on shots per block solve of forward() (0: device memory decides)."""
         check(self.lib.gm_set_shot_block(self._h, max_shots))
 
+    def set_refine(self, refine: int, gmres_restart: int = 0) -> None:
+        """Refinement mode (GM_REFINE_MODE_*) and GMRES restart length of the
+        following solves (0 = default)."""
+        check(self.lib.gm_set_refine(self._h, refine, gmres_restart))
+
     def memory_estimate(self, nmat: int):
         """(bytes to factorise nmat matrices at once, bytes per shot of a block
         solve over them)."""

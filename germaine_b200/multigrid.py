@@ -19,6 +19,7 @@ from dataclasses import dataclass
 
 import numpy as np
 
+from ._lib import GM_REFINE_MODE_IR
 from .engine import Engine
 from .synthetic import extend_into_pml
 
@@ -82,12 +83,20 @@ def smooth_random_model(extent_x: float, extent_y: float, dh: float, nx0: int, n
 
 
 def run_multigrid(cases, nshots: int, seed: int = 7, precision: int = 1, workers: int | None = None,
-                  row: int = 2, refine: int = 1):
+                  row: int = 2, refine: int = 0):
     """Factorise and solve every grid's frequency for nshots shots along
     model row `row`, all grids concurrently.  Returns (shot-solves/s over
-    the whole set, wall seconds, per-grid records).  refine defaults to
-    plain refinement sweeps: with every grid's workspaces resident at once
-    there is no room for GMRES-IR's Krylov vectors."""
+    the whole set, wall seconds, per-grid records).
+
+    refine defaults to the engine's automatic choice (plain sweeps, GMRES-IR
+    for a grid whose sweeps contract too slowly: at 5 points per wavelength
+    the complex64 factors of the highest frequencies stall plain sweeps).
+    Two untimed passes place the buffers: the first, with plain sweeps
+    only, allocates every grid's fronts and solve workspaces; the second,
+    with the requested refinement, runs the grids one after another,
+    smallest first, so that GMRES-IR sizes its Krylov vectors from the
+    device memory all the grids leave.  The timed pass then runs every grid
+    concurrently on the resident buffers."""
     extent_x = max(c.nx0 * c.dh for c in cases)
     extent_y = max(c.ny0 * c.dh for c in cases)
     engines, setups = [], []
@@ -98,7 +107,7 @@ def run_multigrid(cases, nshots: int, seed: int = 7, precision: int = 1, workers
         ys = np.full(nshots, row * c.dh, np.float32)
         rx = np.arange(1, c.nx0, max(1, c.nx0 // 200), dtype=np.int32)
         ry = np.full(rx.size, row, np.int32)
-        e = Engine(nx, ny, c.dh, c.npml, precision=precision, refine=refine)
+        e = Engine(nx, ny, c.dh, c.npml, precision=precision, refine=GM_REFINE_MODE_IR)
         e.set_model(vp, rho)
         engines.append(e)
         setups.append((xs, ys, rx, ry))
@@ -115,7 +124,11 @@ def run_multigrid(cases, nshots: int, seed: int = 7, precision: int = 1, workers
     import torch
     try:
         with ThreadPoolExecutor(max_workers=workers or len(cases)) as pool:
-            list(pool.map(one, range(len(cases))))      # first pass: every engine allocates its buffers
+            list(pool.map(one, range(len(cases))))              # fronts and solve workspaces
+            torch.cuda.synchronize()
+            for i in sorted(range(len(cases)), key=lambda i: engines[i].n):   # Krylov workspaces
+                engines[i].set_refine(refine)
+                one(i)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
             recs = list(pool.map(one, range(len(cases))))

@@ -236,6 +236,12 @@ int gm_forward(gm_engine *e, int nshots, const float *src_x, const float *src_y,
 int gm_set_shot_block(gm_engine *e, int max_shots);
 int gm_memory_estimate(gm_engine *e, int nmat, size_t *factor_bytes, size_t *shot_bytes);
 
+/* Refinement mode (GM_REFINE_MODE_*) and GMRES restart length (0 = the
+ * default 8, at most 8) of the following solves: gm_config.refine and
+ * gm_config.gmres_restart changed on a live engine.  No counterpart in the
+ * reference (its UMFPACK solves are not refined). */
+int gm_set_refine(gm_engine *e, int refine, int gmres_restart);
+
 /* FWI objective + gradient of all factorised frequencies (grad_obj_AC,
  * src/AC/grad_obj_AC.c:10-194; grad_obj_TE for GM_PHYS_TE): forward solve,
  * residual (calc_res_AC, MISFIT 1/2/3, optional Wiener source estimate

@@ -176,9 +176,10 @@ def test_mixed_refinement_modes(refine, sys_):
 
 @pytest.mark.parametrize("precision", [GM_PREC_FP64, GM_PREC_C64_IR], ids=["fp64", "c64ir"])
 def test_autotuned_tiles_keep_the_solution(precision):
-    """The autotuner picks, per level and pass, the fastest of the
-    candidate substitution tiles; solves with the tuned table give the
-    SuperLU solution, and other right-hand-side counts keep the defaults."""
+    """The autotuner picks, per level and pass, a candidate substitution
+    tile where it beats the built-in one (the table names the resolved
+    choice either way); solves with the tuned table give the SuperLU
+    solution, and other right-hand-side counts keep the defaults."""
     nx, ny, dh, npml = 90, 64, 10.0, 10
     g = O.Grid(nx=nx, ny=ny, dh=dh, npml=npml)
     m0, m1 = _setup(nx, ny, dh, npml, seed=13)
