@@ -738,9 +738,11 @@ static int gmres_refine(gm_engine *e, int sys, int nrhs, double2 *d_x, const Res
             e->d_gz.release();
             (void)cudaGetLastError();   // the failed allocation is not an error of this solve
         }
+        if (std::getenv("GM_TRACE_REFINEMENT"))
+            std::fprintf(stderr, "GMRES workspace: restart %d for %d matrices (%.2f GB free)\n", m, ng, fr / 1e9);
         if (m < 2) return GM_WARNING_NOT_CONVERGED;   // no room: the caller refines with plain sweeps
     }
-    const int nblk_r = residual_blocks(n), nblk_g = (n + 255) / 256;
+    const int nblk_r = residual_blocks(e->cfg.nx, e->cfg.ny), nblk_g = (n + 255) / 256;
     const size_t part_words = std::max((size_t)nblk_r * ng * nrhs * 2, (size_t)nblk_g * ng * nrhs * (m + 1) * 2);
     GM_ALLOC(e->d_gpart, part_words * sizeof(double));
     GM_ALLOC(e->d_gnorm, (size_t)ng * nrhs * (m + 1) * 2 * sizeof(double));
@@ -978,7 +980,7 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     const bool fp64 = e->cfg.precision == GM_PREC_FP64;
     GM_ALLOC(e->d_t, cnt * e->csize());
     GM_ALLOC(e->d_w, (size_t)e->nf * e->sym.rhs_total * nrhs * e->csize());
-    const int nblk_max = residual_blocks(e->n);
+    const int nblk_max = residual_blocks(e->cfg.nx, e->cfg.ny);
     GM_ALLOC(e->d_part, (size_t)nblk_max * e->nf * nrhs * 2 * sizeof(double));
     GM_ALLOC(e->d_norm, (size_t)e->nf * nrhs * 2 * sizeof(double));
 

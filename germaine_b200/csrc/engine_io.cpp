@@ -208,7 +208,7 @@ namespace {
 size_t bytes_per_shot(const gm_engine *e) {
     const size_t n = (size_t)e->n, nf = (size_t)e->nf;
     return nf * (n * sizeof(double2) + n * e->csize() + (size_t)e->sym.rhs_total * e->csize() +
-                 (size_t)gm::residual_blocks((int)n) * 2 * sizeof(double) + 2 * sizeof(double));
+                 (size_t)gm::residual_blocks(e->cfg.nx, e->cfg.ny) * 2 * sizeof(double) + 2 * sizeof(double));
 }
 
 // Shots per block solve of gm_forward: all of them unless their workspaces

@@ -257,13 +257,16 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
     C *Ls = reinterpret_cast<C *>(smem_raw);   // [NB][TILE]: Ls[c*TILE + r]
     C *Us = Ls + NB * TILE;                    // [NB][TILE]: Us[c*TILE + col]
     const int r0 = i0 + ti * TILE, c0 = i0 + tj * TILE;
+    // asynchronous copies, all in flight at once; entries outside the
+    // front or beyond kb are not staged (the pivot loop reads c < kb only,
+    // and rows / columns outside the front feed accumulators never stored)
     for (int t = threadIdx.x; t < NB * TILE; t += blockDim.x) {
         const int r = t % TILE, c = t / TILE;
-        Ls[t] = (c < kb && r0 + r < f) ? F[(r0 + r) + (size_t)(k0 + c) * f] : czero<C>();
+        if (c < kb && r0 + r < f) cp_async_elem(Ls + t, F + (r0 + r) + (size_t)(k0 + c) * f);
         const int col = t / NB, cc = t % NB;   // U: contiguous along the pivot index
-        Us[cc * TILE + col] = (cc < kb && c0 + col < f) ? F[(k0 + cc) + (size_t)(c0 + col) * f] : czero<C>();
+        if (cc < kb && c0 + col < f) cp_async_elem(Us + cc * TILE + col, F + (k0 + cc) + (size_t)(c0 + col) * f);
     }
-    __syncthreads();
+    staged_sync();
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
     C acc[4][4];
 #pragma unroll
@@ -296,9 +299,15 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
     }
 }
 
-// Batched C -= A * B on CUDA cores (64 x 64 output tiles, K in chunks of NB
-// staged through shared memory, 4 x 4 complex register tile per thread):
-// the contribution-block update of every front of a level in one launch.
+// Batched C -= A * B on CUDA cores (64 x 64 output tiles, 4 x 4 complex
+// register tile per thread): the contribution-block update of every front
+// of a level in one launch.  K runs in chunks of GKC staged through shared
+// memory by asynchronous copies, two buffers: the next chunk's loads are in
+// flight while the current one is multiplied.  Tile entries outside A's
+// rows or B's columns are not staged (they only feed accumulators that are
+// never stored); the chunk loop reads only the k < kb part.
+constexpr int GKC = 16;
+
 template <class R>
 __global__ void __launch_bounds__(256) k_gemm_sub_cc(const GemmProb<R> *__restrict__ probs,
                                                      const int4 *__restrict__ tiles) {
@@ -307,36 +316,50 @@ __global__ void __launch_bounds__(256) k_gemm_sub_cc(const GemmProb<R> *__restri
     const GemmProb<R> p = probs[tl.x];
     const int r0 = tl.y * TILE, c0 = tl.z * TILE;
     extern __shared__ unsigned char smem_raw[];
-    C *As = reinterpret_cast<C *>(smem_raw);   // [NB][TILE]
-    C *Bs = As + NB * TILE;                    // [NB][TILE]
+    C *As = reinterpret_cast<C *>(smem_raw);   // [2][GKC][TILE]: As[c * TILE + r]
+    C *Bs = As + 2 * GKC * TILE;               // [2][GKC][TILE]: Bs[c * TILE + col]
     const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    auto stage = [&](int buf, int k0) {
+        const int kb = min(GKC, p.k - k0);
+        C *Ab = As + buf * GKC * TILE, *Bb = Bs + buf * GKC * TILE;
+        for (int t = threadIdx.x; t < GKC * TILE; t += blockDim.x) {
+            const int r = t % TILE, c = t / TILE;
+            if (c < kb && r0 + r < p.m) cp_async_elem(Ab + t, p.A + (size_t)(r0 + r) + (size_t)(k0 + c) * p.lda);
+            const int col = t / GKC, cc = t % GKC;   // B: contiguous along k
+            if (cc < kb && c0 + col < p.n)
+                cp_async_elem(Bb + cc * TILE + col, p.B + (size_t)(k0 + cc) + (size_t)(c0 + col) * p.ldb);
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
     C acc[4][4];
 #pragma unroll
     for (int i = 0; i < 4; ++i)
 #pragma unroll
         for (int j = 0; j < 4; ++j) acc[i][j] = czero<C>();
-    for (int k0 = 0; k0 < p.k; k0 += NB) {
-        const int kb = min(NB, p.k - k0);
-        for (int t = threadIdx.x; t < NB * TILE; t += blockDim.x) {
-            const int r = t % TILE, c = t / TILE;
-            As[t] = (c < kb && r0 + r < p.m) ? p.A[(size_t)(r0 + r) + (size_t)(k0 + c) * p.lda] : czero<C>();
-            const int col = t / NB, cc = t % NB;
-            Bs[cc * TILE + col] = (cc < kb && c0 + col < p.n) ? p.B[(size_t)(k0 + cc) + (size_t)(c0 + col) * p.ldb]
-                                                              : czero<C>();
+    const int nk = (p.k + GKC - 1) / GKC;
+    if (nk > 0) stage(0, 0);
+    for (int kc = 0; kc < nk; ++kc) {
+        if (kc + 1 < nk) {
+            stage((kc + 1) & 1, (kc + 1) * GKC);
+            asm volatile("cp.async.wait_group 1;\n" ::: "memory");   // chunk kc has landed
+        } else {
+            asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         }
         __syncthreads();
+        const int kb = min(GKC, p.k - kc * GKC);
+        const C *Ab = As + (kc & 1) * GKC * TILE, *Bb = Bs + (kc & 1) * GKC * TILE;
         for (int c = 0; c < kb; ++c) {
             C lv[4], uv[4];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) lv[i] = As[c * TILE + tx + 16 * i];
+            for (int i = 0; i < 4; ++i) lv[i] = Ab[c * TILE + tx + 16 * i];
 #pragma unroll
-            for (int j = 0; j < 4; ++j) uv[j] = Bs[c * TILE + ty + 16 * j];
+            for (int j = 0; j < 4; ++j) uv[j] = Bb[c * TILE + ty + 16 * j];
 #pragma unroll
             for (int i = 0; i < 4; ++i)
 #pragma unroll
                 for (int j = 0; j < 4; ++j) cfma(acc[i][j], lv[i], uv[j]);
         }
-        __syncthreads();
+        __syncthreads();   // this buffer is staged again for chunk kc + 2
     }
 #pragma unroll
     for (int j = 0; j < 4; ++j) {
@@ -356,7 +379,7 @@ __global__ void __launch_bounds__(256) k_gemm_sub_cc(const GemmProb<R> *__restri
 template <class R>
 void launch_gemm_sub_cc(const GemmProb<R> *d_probs, const int4 *d_tiles, int ntiles, cudaStream_t st) {
     if (ntiles <= 0) return;
-    const size_t smem = 2 * NB * TILE * sizeof(cplx<R>);
+    const size_t smem = 4 * GKC * TILE * sizeof(cplx<R>);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_gemm_sub_cc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);

@@ -186,7 +186,7 @@ struct ResidArgs {
     const int *omap;
 };
 // row blocks of the residual kernel for n unknowns (the partial-sum count)
-int residual_blocks(int n);
+int residual_blocks(int nx, int ny);
 // r = b - M x and per-(freq, rhs) partial sums of |r|^2 and |b|^2 into
 // part[nblk][nfz][nrhs][2]; returns nblk.
 int launch_residual(const ResidArgs &a, double *part, int max_blocks, cudaStream_t st);

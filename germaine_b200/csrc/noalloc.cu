@@ -132,7 +132,7 @@ extern "C" int gm_solve_noalloc(gm_engine *e, int sys, int nrhs, const double *d
         if (b0 < x0 + nb && x0 < b0 + nb)
             return gm::fail(GM_ERROR_INVALID, "gm_solve_noalloc: b and x overlap");
     }
-    const int nblk = gm::residual_blocks(e->n);
+    const int nblk = gm::residual_blocks(e->cfg.nx, e->cfg.ny);
     const int npairs = e->nf * nrhs;
     const size_t b_t = align256(cnt * cs);
     const size_t b_w = align256((size_t)e->nf * e->sym.rhs_total * nrhs * cs);

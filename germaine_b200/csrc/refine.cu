@@ -8,18 +8,25 @@
 
 namespace gm {
 
-// Residual tile: RROWS consecutive unknowns of one matrix x RLANES
-// right-hand sides, one warp per row at a time (the branch on the stencil's
-// grid edges is warp-uniform, the 32 lanes read 32 consecutive right-hand
-// sides of each neighbour row: one 512-byte load per neighbour), RGRP warps
-// over the tile's rows.  The tile's operator values (9 per row, shared by
-// every right-hand side) are staged in shared memory once.
-constexpr int RROWS = 64;   // measured on 841 x 227: 32-row tiles took 15 % longer
-constexpr int RLANES = 32;
-constexpr int RGRP = 8;
+// Residual tile: a patch of PL grid lines x PW grid columns of one matrix x
+// RLANES right-hand sides.  Warp w walks grid line y0 + w of the patch from
+// left to right, one grid point per step, with the 3 x 3 stencil window of
+// x in registers: each step loads only the window's new right-hand column
+// (the points above, at and below the next grid point: three 512-byte
+// loads per step, U steps' loads issued together), so every x value is
+// loaded by three warps of the patch or its neighbours instead of nine
+// times.  The vertical neighbours of a warp's line are the centre lines of
+// the warps above and below it, so most of them come from L1.  The
+// patch's operator values (9 per grid point, shared by every right-hand
+// side) and grid-edge masks are staged in shared memory once.
+constexpr int PW = 32;      // grid columns per patch (steps per warp)
+constexpr int PL = 8;       // grid lines per patch (warps per CTA)
+constexpr int RLANES = 32;  // right-hand sides per CTA
+constexpr int RSTEP = 3;    // window steps whose loads are in flight together
+static_assert(PW == RLANES, "one patch point per thread when the patch is staged");
 
-// row tiles of the residual kernel for n unknowns (partial-sum blocks)
-int residual_blocks(int n) { return (n + RROWS - 1) / RROWS; }
+// patches of the residual kernel on an nx x ny grid (partial-sum blocks)
+int residual_blocks(int nx, int ny) { return ((nx + PW - 1) / PW) * ((ny + PL - 1) / PL); }
 
 // Operator value M'[k][k+off(q)] for the selected orientation (M' = M or M^T,
 // M = A^T in GM_OP_REF, M = A in GM_OP_EXACT); A[k][k+off(q)] = A9[q][k].
@@ -35,75 +42,101 @@ __device__ __forceinline__ double2 op_coef(const double2 *A9, int n, int nx, boo
 // OutC = float2 writes the refinement right-hand side directly in the
 // working precision of the substitution; WRITE = false forms the norms only.
 template <class InC, class OutC, bool WRITE, bool PRODUCT>
-__global__ void __launch_bounds__(RLANES *RGRP, 3) k_residual(ResidArgs a, const InC *__restrict__ xin, OutC *out,
-                                                            double *part) {
-    __shared__ double2 cf[9][RROWS];
-    __shared__ unsigned short nbm[RROWS];   // per row: bit q set when neighbour q lies inside the grid
-    __shared__ double red[2][RGRP][RLANES];
+__global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const InC *__restrict__ xin, OutC *out,
+                                                          double *part) {
+    __shared__ double2 cf[9][PL][PW];
+    __shared__ unsigned short nbm[PL][PW];   // per grid point: bit q set when neighbour q lies inside the grid
+    __shared__ double red[2][PL][RLANES];
     const int fz = blockIdx.z;
     const int f = a.fmap ? a.fmap[fz] : fz;
-    const int k0 = blockIdx.x * RROWS;
+    const int ncb = (a.nx + PW - 1) / PW;
+    const int x0 = (int)(blockIdx.x % ncb) * PW, y0 = (int)(blockIdx.x / ncb) * PL;
     const int r = blockIdx.y * RLANES + threadIdx.x;
     const bool use_row = (a.op_mode == GM_OP_EXACT) != (a.trans != 0);
     const double2 *A9 = a.A + (size_t)f * 9 * a.n;
-    const int tid = threadIdx.y * RLANES + threadIdx.x;
-    if (tid < RROWS) {   // the grid-edge tests once per row, not per right-hand side
-        const int k = k0 + tid;
+    {   // one grid point of the patch per thread: its edge mask and operator values
+        const int ly = threadIdx.y, lx = threadIdx.x;
+        const int x = x0 + lx, y = y0 + ly;
         unsigned m = 0;
-        if (k < a.n) {
-            const int x = k % a.nx, y = k / a.nx;
+        if (x < a.nx && y < a.ny) {
 #pragma unroll
             for (int q = 0; q < 9; ++q) {
                 const int xx = x + q % 3 - 1, yy = y + q / 3 - 1;
                 if (xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny) m |= 1u << q;
             }
         }
-        nbm[tid] = (unsigned short)m;
-    }
-    __syncthreads();
-    for (int t = tid; t < 9 * RROWS; t += RLANES * RGRP) {
-        const int q = t / RROWS, i = t % RROWS;
-        cf[q][i] = (nbm[i] >> q) & 1 ? op_coef(A9, a.n, a.nx, use_row, q, k0 + i) : make_double2(0.0, 0.0);
+        nbm[ly][lx] = (unsigned short)m;
+        const int k = y * a.nx + x;
+#pragma unroll
+        for (int q = 0; q < 9; ++q)
+            cf[q][ly][lx] = (m >> q) & 1 ? op_coef(A9, a.n, a.nx, use_row, q, k) : make_double2(0.0, 0.0);
     }
     __syncthreads();
     double rr = 0.0, bb = 0.0;
-    if (r < a.nrhs) {
+    const int w = threadIdx.y, y = y0 + w;
+    const int xe = min(PW, a.nx - x0);   // grid columns of this patch
+    if (r < a.nrhs && y < a.ny) {
         const size_t per = (size_t)a.n * a.ldr;
         const size_t base = (size_t)f * per + r;
+        const size_t ldr = a.ldr;
         const InC *X = xin + (size_t)(a.xmap ? a.xmap[fz] : f) * per + r;
         OutC *O = out ? out + (size_t)(a.omap ? a.omap[fz] : f) * per + r : nullptr;
         const bool spikes = !PRODUCT && a.spike_k;
         const int ks = spikes ? a.spike_k[r] : -1;
         const double2 amp = spikes ? a.spike_amp[f] : make_double2(0.0, 0.0);
-        // neighbour q of row k is row k + dq[q]: offsets in elements of x
-        int dq[9];
+        const int n = a.n, nx = a.nx;
+        // x at flat index i, zero outside the array (such values are masked)
+        auto ld = [&](int i) { return (i >= 0 && i < n) ? cto_d(X[(size_t)i * ldr]) : make_double2(0.0, 0.0); };
+        const int kb = y * nx + x0;   // flat index of the line segment's first point
+        // window: wl[d] / wc[d] = x left of / at the current point on the
+        // line above (d = 0), the same line (1) and the line below (2)
+        double2 wl[3], wc[3];
 #pragma unroll
-        for (int q = 0; q < 9; ++q) dq[q] = ((q % 3 - 1) + (q / 3 - 1) * a.nx) * a.ldr;
-#pragma unroll 2
-        for (int i = threadIdx.y; i < RROWS; i += RGRP) {
-            const int k = k0 + i;
-            if (k >= a.n) break;
-            const unsigned m = nbm[i];
-            double2 bv = make_double2(0.0, 0.0);
-            if (!PRODUCT) bv = spikes ? (k == ks ? amp : bv) : a.b[base + (size_t)k * a.ldr];
-            double2 acc = bv;
-            const InC *Xk = X + (size_t)k * a.ldr;
+        for (int d = 0; d < 3; ++d) {
+            wl[d] = ld(kb - 1 + (d - 1) * nx);
+            wc[d] = ld(kb + (d - 1) * nx);
+        }
+        for (int c0 = 0; c0 < xe; c0 += RSTEP) {
+            double2 wr[RSTEP][3];   // the right-hand columns of the next RSTEP points
 #pragma unroll
-            for (int q = 0; q < 9; ++q)
-                if ((m >> q) & 1) cfms(acc, cf[q][i], cto_d(Xk[dq[q]]));
-            if (PRODUCT) acc = make_double2(-acc.x, -acc.y);
-            if (WRITE) O[(size_t)k * a.ldr] = cconv<OutC>(acc);
-            rr += acc.x * acc.x + acc.y * acc.y;
-            bb += bv.x * bv.x + bv.y * bv.y;
+            for (int u = 0; u < RSTEP; ++u)
+#pragma unroll
+                for (int d = 0; d < 3; ++d)
+                    wr[u][d] = c0 + u < xe ? ld(kb + c0 + u + 1 + (d - 1) * nx) : make_double2(0.0, 0.0);
+#pragma unroll
+            for (int u = 0; u < RSTEP; ++u) {
+                const int lx = c0 + u;
+                if (lx >= xe) break;
+                const int k = kb + lx;
+                const unsigned m = nbm[w][lx];
+                double2 bv = make_double2(0.0, 0.0);
+                if (!PRODUCT) bv = spikes ? (k == ks ? amp : bv) : a.b[base + (size_t)k * ldr];
+                double2 acc = bv;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    if ((m >> (3 * d)) & 1) cfms(acc, cf[3 * d][w][lx], wl[d]);
+                    if ((m >> (3 * d + 1)) & 1) cfms(acc, cf[3 * d + 1][w][lx], wc[d]);
+                    if ((m >> (3 * d + 2)) & 1) cfms(acc, cf[3 * d + 2][w][lx], wr[u][d]);
+                }
+                if (PRODUCT) acc = make_double2(-acc.x, -acc.y);
+                if (WRITE) O[(size_t)k * ldr] = cconv<OutC>(acc);
+                rr += acc.x * acc.x + acc.y * acc.y;
+                bb += bv.x * bv.x + bv.y * bv.y;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    wl[d] = wc[d];
+                    wc[d] = wr[u][d];
+                }
+            }
         }
     }
-    red[0][threadIdx.y][threadIdx.x] = rr;
-    red[1][threadIdx.y][threadIdx.x] = bb;
+    red[0][w][threadIdx.x] = rr;
+    red[1][w][threadIdx.x] = bb;
     __syncthreads();
     if (threadIdx.y == 0 && r < a.nrhs) {
         double s0 = 0.0, s1 = 0.0;
 #pragma unroll
-        for (int g = 0; g < RGRP; ++g) {
+        for (int g = 0; g < PL; ++g) {
             s0 += red[0][g][threadIdx.x];
             s1 += red[1][g][threadIdx.x];
         }
@@ -117,12 +150,12 @@ static int resid_nfz(const ResidArgs &a) { return a.fmap ? a.nfz : a.nf; }
 
 template <class InC, class OutC, bool WRITE, bool PRODUCT>
 static int launch_k6(const ResidArgs &a, const void *x, void *out, double *part, int max_blocks, cudaStream_t st) {
-    const int nblk = residual_blocks(a.n);
+    const int nblk = residual_blocks(a.nx, a.ny);
     const int nfz = resid_nfz(a);
     if (nblk > max_blocks) return -1;
     if (nfz <= 0) return nblk;
     dim3 grid(nblk, (a.nrhs + RLANES - 1) / RLANES, nfz);
-    (k_residual<InC, OutC, WRITE, PRODUCT><<<grid, dim3(RLANES, RGRP), 0, st>>>(
+    (k_residual<InC, OutC, WRITE, PRODUCT><<<grid, dim3(RLANES, PL), 0, st>>>(
          a, reinterpret_cast<const InC *>(x), reinterpret_cast<OutC *>(out), part),
      note_launch());
     return nblk;
