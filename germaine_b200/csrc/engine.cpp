@@ -1081,9 +1081,11 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
         }
         if (next.empty() || it >= e->cfg.ir_max_iter) break;
         // Matrices that go on with GMRES-IR: all of them in GMRES mode; in
-        // auto mode those whose last sweep contracted too slowly to reach the
-        // target within two more sweeps (the first check has no contraction
-        // yet, so every matrix starts with a plain sweep)
+        // auto mode those whose plain sweeps cannot reach the target within
+        // the sweeps left at the contraction of the last one (or did not
+        // contract at all).  The first check has no contraction yet, so
+        // every matrix starts with a plain sweep; plain sweeps need no
+        // Krylov vectors, which matters when many engines share the device.
         std::vector<int> gset, irset;
         for (int f : next) {
             const gm_refine_info &ri = e->refine_info[f];
@@ -1091,7 +1093,7 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
             if (e->cfg.refine == GM_REFINE_MODE_AUTO && it > 0 && !fp64) {   // FP64 factors: plain sweeps
                 const double rho = prev_res[f] > 0 ? ri.final_residual / prev_res[f] : 1.0;
                 const double need = std::log(e->cfg.ir_tol / ri.final_residual);
-                to_gmres = !(rho < 1.0) || need / std::log(rho) > 2.0;
+                to_gmres = !(rho < 1.0) || need / std::log(rho) > (double)(e->cfg.ir_max_iter - it);
             }
             (to_gmres ? gset : irset).push_back(f);
         }

@@ -86,8 +86,9 @@ typedef struct {
 
 /* ---- refinement of the solves (gm_config.refine) ---- */
 #define GM_REFINE_MODE_AUTO  0  /* iterative refinement; with complex64 factors a matrix whose
-                                   last sweep contracted too slowly to meet the target
-                                   within two more sweeps continues with GMRES-IR */
+                                   last sweep did not contract, or contracted too slowly to
+                                   meet the target within the sweeps left (ir_max_iter),
+                                   continues with GMRES-IR */
 #define GM_REFINE_MODE_IR    1  /* classical iterative refinement only */
 #define GM_REFINE_MODE_GMRES 2  /* GMRES-IR for every matrix that needs refinement */
 
