@@ -444,23 +444,9 @@ template void launch_factor_level<float>(const FactorArgs<float> &, const LevelI
 // sequence.  S[i + j * ld] holds front entry (i, j).
 // ---------------------------------------------------------------------
 constexpr int SMALL_FT = 256;   // threads per CTA
-// Register-tiled LU of fronts of at most 64 rows (RTILE = true): the front
-// is spread cyclically over a 16 x 16 grid of threads, thread (tr, tc)
-// holding entries (tr + 16 ii, tc + 16 jj), ii, jj < 4, in registers.  Per
-// pivot k the owners of column k and row k publish them to shared memory
-// (alternating buffers: one barrier per pivot), every thread takes the pivot
-// (static pivoting as diag_lu, evaluated redundantly), scales its rows of
-// the column and applies the rank-1 update to its entries.  Shared memory
-// then carries two vectors per pivot instead of the whole trailing block.
-// The cyclic layout keeps every thread busy to the last pivot; 4 x 4 blocks
-// of rows or columns that are all finished are skipped.
-constexpr int SRT_T = 16;   // thread grid side (SRT_T * SRT_T = SMALL_FT)
-constexpr int SRT_N = 4;    // entries per thread along each dimension
-constexpr int SRT_MAXF = SRT_T * SRT_N;
-static_assert(SRT_T * SRT_T == SMALL_FT, "one thread per grid position");
 
-template <class R, bool RTILE>
-__global__ void __launch_bounds__(SMALL_FT, RTILE ? 2 : 1) k_factor_small(FactorArgs<R> a, int lvl_first, int ld) {
+template <class R>
+__global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int lvl_first, int ld) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *S = reinterpret_cast<C *>(smem_raw);
@@ -507,45 +493,15 @@ __global__ void __launch_bounds__(SMALL_FT, RTILE ? 2 : 1) k_factor_small(Factor
     }
     __syncthreads();
 
+    // right-looking LU of the pivot columns; the trailing update covers the
+    // contribution block too (its Schur complement).  Warp 0 updates column
+    // k + 1 first in step k, so it can take the next pivot (static pivoting
+    // as in diag_lu) and scale the next L column while the other warps are
+    // still updating: one barrier per pivot.
     const R pivtol = (R)(a.pivscale * __longlong_as_double((long long)*a.amax));
-    if constexpr (RTILE) {
-        __shared__ C colbuf[2][SRT_MAXF], rowbuf[2][SRT_MAXF];
-        const int tr = tid % SRT_T, tc = tid / SRT_T;
-        C t[SRT_N][SRT_N];
-#pragma unroll
-        for (int ii = 0; ii < SRT_N; ++ii)
-#pragma unroll
-            for (int jj = 0; jj < SRT_N; ++jj) {
-                const int i = tr + SRT_T * ii, j = tc + SRT_T * jj;
-                t[ii][jj] = (i < f && j < f) ? S[i + j * ld] : czero<C>();
-            }
-        for (int k = 0; k < s; ++k) {
-            const int b = k & 1, kq = k / SRT_T, kr = k % SRT_T;
-            // publish column k (rows >= k) and row k (columns > k)
-            if (tc == kr) {
-#pragma unroll
-                for (int jj = 0; jj < SRT_N; ++jj)
-                    if (jj == kq) {
-#pragma unroll
-                        for (int ii = 0; ii < SRT_N; ++ii) {
-                            const int i = tr + SRT_T * ii;
-                            if (i >= k && i < f) colbuf[b][i] = t[ii][jj];
-                        }
-                    }
-            }
-            if (tr == kr) {
-#pragma unroll
-                for (int ii = 0; ii < SRT_N; ++ii)
-                    if (ii == kq) {
-#pragma unroll
-                        for (int jj = 0; jj < SRT_N; ++jj) {
-                            const int j = tc + SRT_T * jj;
-                            if (j > k && j < f) rowbuf[b][j] = t[ii][jj];
-                        }
-                    }
-            }
-            __syncthreads();
-            C piv = colbuf[b][k];
+    auto take_pivot = [&](int k) {   // warp 0 only: pivot k, reciprocal, L column k scaled
+        if (lane == 0) {
+            C piv = S[k + k * ld];
             const R mag = sqrt(cabs2(piv));
             if (!(mag >= pivtol)) {   // also catches NaN
                 if (mag > R(0)) {
@@ -554,85 +510,30 @@ __global__ void __launch_bounds__(SMALL_FT, RTILE ? 2 : 1) k_factor_small(Factor
                 } else {
                     piv = mk(pivtol, R(0));
                 }
-                if (tid == 0) ++npert;
+                S[k + k * ld] = piv;
+                ++npert;
             }
-            const C rk = crcp(piv);
-            if (tid == 0) rd[k] = rk;
-            C l[SRT_N], u[SRT_N];
-#pragma unroll
-            for (int ii = 0; ii < SRT_N; ++ii) {
-                const int i = tr + SRT_T * ii;
-                l[ii] = i > k ? cmul(colbuf[b][i], rk) : czero<C>();
-            }
-#pragma unroll
-            for (int jj = 0; jj < SRT_N; ++jj) {
-                const int j = tc + SRT_T * jj;
-                u[jj] = j > k ? rowbuf[b][j] : czero<C>();
-            }
-#pragma unroll
-            for (int ii = 0; ii < SRT_N; ++ii) {
-                if (SRT_T * ii + SRT_T - 1 < k) continue;   // rows of this block all finished
-#pragma unroll
-                for (int jj = 0; jj < SRT_N; ++jj) {
-                    if (SRT_T * jj + SRT_T - 1 < k) continue;
-                    const int i = tr + SRT_T * ii, j = tc + SRT_T * jj;
-                    if (j == k && i > k) t[ii][jj] = l[ii];                      // L column k, scaled
-                    else if (i == k && j == k) t[ii][jj] = piv;                  // the (perturbed) pivot
-                    else if (i > k && j > k) cfms(t[ii][jj], l[ii], u[jj]);      // Schur update
-                }
+            rd[k] = crcp(piv);
+        }
+        __syncwarp();
+        const C rk = rd[k];
+        for (int i = k + 1 + lane; i < f; i += 32) S[i + k * ld] = cmul(S[i + k * ld], rk);
+        __syncwarp();
+    };
+    if (warp == 0 && s > 0) take_pivot(0);
+    __syncthreads();
+    for (int k = 0; k < s; ++k) {
+        const int m = f - k - 1;
+        for (int jj = warp; jj < m; jj += nw) {
+            C *col = S + (k + 1 + jj) * ld;
+            const C u = col[k];
+            for (int ii = lane; ii < m; ii += 32) cfms(col[k + 1 + ii], S[k + 1 + ii + k * ld], u);
+            if (jj == 0 && k + 1 < s) {   // warp 0 just finished column k + 1
+                __syncwarp();
+                take_pivot(k + 1);
             }
         }
-        __syncthreads();   // rd complete; nothing reads the buffers any more
-#pragma unroll
-        for (int ii = 0; ii < SRT_N; ++ii)
-#pragma unroll
-            for (int jj = 0; jj < SRT_N; ++jj) {
-                const int i = tr + SRT_T * ii, j = tc + SRT_T * jj;
-                if (i < f && j < f) S[i + j * ld] = t[ii][jj];
-            }
         __syncthreads();
-    } else {
-        // right-looking LU of the pivot columns; the trailing update covers the
-        // contribution block too (its Schur complement).  Warp 0 updates column
-        // k + 1 first in step k, so it can take the next pivot (static pivoting
-        // as in diag_lu) and scale the next L column while the other warps are
-        // still updating: one barrier per pivot.
-        auto take_pivot = [&](int k) {   // warp 0 only: pivot k, reciprocal, L column k scaled
-            if (lane == 0) {
-                C piv = S[k + k * ld];
-                const R mag = sqrt(cabs2(piv));
-                if (!(mag >= pivtol)) {   // also catches NaN
-                    if (mag > R(0)) {
-                        const R sc = pivtol / mag;
-                        piv = mk(piv.x * sc, piv.y * sc);
-                    } else {
-                        piv = mk(pivtol, R(0));
-                    }
-                    S[k + k * ld] = piv;
-                    ++npert;
-                }
-                rd[k] = crcp(piv);
-            }
-            __syncwarp();
-            const C rk = rd[k];
-            for (int i = k + 1 + lane; i < f; i += 32) S[i + k * ld] = cmul(S[i + k * ld], rk);
-            __syncwarp();
-        };
-        if (warp == 0 && s > 0) take_pivot(0);
-        __syncthreads();
-        for (int k = 0; k < s; ++k) {
-            const int m = f - k - 1;
-            for (int jj = warp; jj < m; jj += nw) {
-                C *col = S + (k + 1 + jj) * ld;
-                const C u = col[k];
-                for (int ii = lane; ii < m; ii += 32) cfms(col[k + 1 + ii], S[k + 1 + ii + k * ld], u);
-                if (jj == 0 && k + 1 < s) {   // warp 0 just finished column k + 1
-                    __syncwarp();
-                    take_pivot(k + 1);
-                }
-            }
-            __syncthreads();
-        }
     }
 
     // inverses of the NB x NB diagonal blocks: L^-1 strictly below the
@@ -686,16 +587,11 @@ template <class R>
 void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_factor_small<R, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
-        cudaFuncSetAttribute(k_factor_small<R, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
+        cudaFuncSetAttribute(k_factor_small<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
         attr_set = true;
     }
     const size_t smem = small_factor_smem<R>(L.max_front);
-    static const bool no_rtile = std::getenv("GM_NO_FACTOR_RTILE") != nullptr;
-    if (L.max_front <= SRT_MAXF && !no_rtile)
-        (k_factor_small<R, true><<<dim3(L.count, a.nf), SMALL_FT, smem, st>>>(a, L.first, L.max_front + 1), note_launch());
-    else
-        (k_factor_small<R, false><<<dim3(L.count, a.nf), SMALL_FT, smem, st>>>(a, L.first, L.max_front + 1), note_launch());
+    (k_factor_small<R><<<dim3(L.count, a.nf), SMALL_FT, smem, st>>>(a, L.first, L.max_front + 1), note_launch());
 }
 
 template bool small_factor_level<double>(const LevelInfo &);

@@ -1,0 +1,54 @@
+"""Known-answer check at the level of the discretisation (not parity): in a
+homogeneous medium the FP64 wavefield of a point source must decay and turn
+in phase like the outgoing 2-D Green's function, a Hankel function of k r
+(the first or the second kind, depending on the time convention of the
+operator: the reference forms Omega = 2 pi (f - S i), S = 0 here, and the
+PML makes the outgoing kind the one that fits).  Ratios u(r) / u(r0) remove
+the source scaling; they are compared along the source's grid line and
+along a diagonal (the 9-point mixed-grid stencil is nearly isotropic), at
+40 grid points per wavelength and 1 to 2.25 wavelengths from the source,
+at least 10 points from the PML."""
+import numpy as np
+import pytest
+from scipy.special import hankel1, hankel2
+
+from germaine_b200 import Engine
+
+pytestmark = pytest.mark.gpu
+
+
+def test_homogeneous_wavefield_follows_the_2d_greens_function():
+    nx0 = ny0 = 201
+    npml, dh, f, v = 20, 10.0, 5.0, 2000.0
+    nx, ny = nx0 + 2 * npml, ny0 + 2 * npml
+    vp = np.full((ny, nx), v, np.float32)
+    rho = np.full((ny, nx), 1000.0, np.float32)
+    xs = np.array([100 * dh], np.float32)          # the middle of the interior
+    ys = np.array([100 * dh], np.float32)
+    rx = np.array([1], np.int32)
+    ry = np.array([1], np.int32)
+    with Engine(nx, ny, dh, npml) as e:
+        e.set_model(vp, rho)
+        e.factor([f])
+        e.forward(xs, ys, rx, ry)
+        assert e.stats()["ir_residual"] <= 1e-10
+        u = e.wavefield_fp64(0, 1)[0, :, 0].reshape(ny, nx)
+    r0, c0 = np.unravel_index(np.argmax(np.abs(u)), u.shape)   # the source point
+    assert abs(c0 - (npml + 100)) <= 1 and abs(r0 - (npml + 100)) <= 1
+    k = 2.0 * np.pi * f / v                         # 40 points per wavelength
+    steps = np.arange(40, 91, 5)                    # 1 .. 2.25 wavelengths
+    ref = 40
+    errs = {}
+    for name, H in (("first", hankel1), ("second", hankel2)):
+        worst = 0.0
+        for dr, dc, scale in ((0, 1, 1.0), (1, 1, np.sqrt(2.0))):
+            d = (steps / scale).round().astype(int) if scale != 1.0 else steps
+            dref = int(round(ref / scale))
+            got = u[r0 + dr * d, c0 + dc * d] / u[r0 + dr * dref, c0 + dc * dref]
+            want = H(0, k * dh * d * scale) / H(0, k * dh * dref * scale)
+            worst = max(worst, float(np.max(np.abs(got - want) / np.abs(want))))
+        errs[name] = worst
+    best = min(errs, key=errs.get)
+    other = "second" if best == "first" else "first"
+    assert errs[best] < 0.05, errs          # decay and phase of the outgoing wave
+    assert errs[other] > 0.5, errs          # the incoming kind does not fit
