@@ -13,12 +13,13 @@ namespace gm {
 // left to right, one grid point per step, with the 3 x 3 stencil window of
 // x in registers: each step loads only the window's new right-hand column
 // (the points above, at and below the next grid point: three 512-byte
-// loads per step, U steps' loads issued together), so every x value is
+// loads per step, RSTEP steps' loads issued together), so every x value is
 // loaded by three warps of the patch or its neighbours instead of nine
 // times.  The vertical neighbours of a warp's line are the centre lines of
 // the warps above and below it, so most of them come from L1.  The
 // patch's operator values (9 per grid point, shared by every right-hand
-// side) and grid-edge masks are staged in shared memory once.
+// side; zero for neighbours outside the grid, so the stencil needs no
+// edge branches) are staged in shared memory once.
 constexpr int PW = 32;      // grid columns per patch (steps per warp)
 constexpr int PL = 8;       // grid lines per patch (warps per CTA)
 constexpr int RLANES = 32;  // right-hand sides per CTA
@@ -44,8 +45,7 @@ __device__ __forceinline__ double2 op_coef(const double2 *A9, int n, int nx, boo
 template <class InC, class OutC, bool WRITE, bool PRODUCT>
 __global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const InC *__restrict__ xin, OutC *out,
                                                           double *part) {
-    __shared__ double2 cf[9][PL][PW];
-    __shared__ unsigned short nbm[PL][PW];   // per grid point: bit q set when neighbour q lies inside the grid
+    __shared__ double2 cf[9][PL][PW];   // operator values, zero for neighbours outside the grid
     __shared__ double red[2][PL][RLANES];
     const int fz = blockIdx.z;
     const int f = a.fmap ? a.fmap[fz] : fz;
@@ -54,10 +54,10 @@ __global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const I
     const int r = blockIdx.y * RLANES + threadIdx.x;
     const bool use_row = (a.op_mode == GM_OP_EXACT) != (a.trans != 0);
     const double2 *A9 = a.A + (size_t)f * 9 * a.n;
-    {   // one grid point of the patch per thread: its edge mask and operator values
+    {   // one grid point of the patch per thread: its operator values
         const int ly = threadIdx.y, lx = threadIdx.x;
         const int x = x0 + lx, y = y0 + ly;
-        unsigned m = 0;
+        unsigned m = 0;   // bit q: neighbour q lies inside the grid
         if (x < a.nx && y < a.ny) {
 #pragma unroll
             for (int q = 0; q < 9; ++q) {
@@ -65,7 +65,6 @@ __global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const I
                 if (xx >= 0 && xx < a.nx && yy >= 0 && yy < a.ny) m |= 1u << q;
             }
         }
-        nbm[ly][lx] = (unsigned short)m;
         const int k = y * a.nx + x;
 #pragma unroll
         for (int q = 0; q < 9; ++q)
@@ -108,15 +107,16 @@ __global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const I
                 const int lx = c0 + u;
                 if (lx >= xe) break;
                 const int k = kb + lx;
-                const unsigned m = nbm[w][lx];
                 double2 bv = make_double2(0.0, 0.0);
                 if (!PRODUCT) bv = spikes ? (k == ks ? amp : bv) : a.b[base + (size_t)k * ldr];
                 double2 acc = bv;
+                // no branches on the grid edges: a neighbour outside the grid
+                // has a zero operator value, and acc - 0 x is acc exactly
 #pragma unroll
                 for (int d = 0; d < 3; ++d) {
-                    if ((m >> (3 * d)) & 1) cfms(acc, cf[3 * d][w][lx], wl[d]);
-                    if ((m >> (3 * d + 1)) & 1) cfms(acc, cf[3 * d + 1][w][lx], wc[d]);
-                    if ((m >> (3 * d + 2)) & 1) cfms(acc, cf[3 * d + 2][w][lx], wr[u][d]);
+                    cfms(acc, cf[3 * d][w][lx], wl[d]);
+                    cfms(acc, cf[3 * d + 1][w][lx], wc[d]);
+                    cfms(acc, cf[3 * d + 2][w][lx], wr[u][d]);
                 }
                 if (PRODUCT) acc = make_double2(-acc.x, -acc.y);
                 if (WRITE) O[(size_t)k * ldr] = cconv<OutC>(acc);

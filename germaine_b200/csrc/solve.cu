@@ -69,19 +69,26 @@ __device__ __forceinline__ C elem(const C *F, int f, int i, int c) {
 // outside are left as they are: tile_mma reads only q < qb, and rows >= rows
 // (or right-hand sides >= rn) only feed accumulators that are never stored,
 // so partial tiles stage only what they use.
-template <class C, bool TRANS, int RT, int B>
-__device__ __forceinline__ void stage_factor(SolveSmem<C, RT, B> &sm, const C *F, int f, int i0, int rows, int c0, int qb) {
+// (the _p forms take the tile by pointer and the participating threads as
+// lt = 0 .. nt - 1; the SolveSmem forms are the CTA-wide ones)
+template <class C, bool TRANS, int RT>
+__device__ __forceinline__ void stage_factor_p(C (*L)[RT], const C *F, int f, int i0, int rows, int c0, int qb, int lt,
+                                               int nt) {
     if (!TRANS) {
-        for (int t = threadIdx.x; t < RT * qb; t += NT) {
+        for (int t = lt; t < RT * qb; t += nt) {
             const int row = t % RT, q = t / RT;
-            if (row < rows) cp_async_elem(&sm.L[q][row], F + (i0 + row) + (size_t)(c0 + q) * f);
+            if (row < rows) cp_async_elem(&L[q][row], F + (i0 + row) + (size_t)(c0 + q) * f);
         }
     } else {
-        for (int t = threadIdx.x; t < SNB * rows; t += NT) {
+        for (int t = lt; t < SNB * rows; t += nt) {
             const int q = t % SNB, row = t / SNB;
-            if (q < qb) cp_async_elem(&sm.L[q][row], F + (c0 + q) + (size_t)(i0 + row) * f);
+            if (q < qb) cp_async_elem(&L[q][row], F + (c0 + q) + (size_t)(i0 + row) * f);
         }
     }
+}
+template <class C, bool TRANS, int RT, int B>
+__device__ __forceinline__ void stage_factor(SolveSmem<C, RT, B> &sm, const C *F, int f, int i0, int rows, int c0, int qb) {
+    stage_factor_p<C, TRANS, RT>(sm.L, F, f, i0, rows, c0, qb, threadIdx.x, NT);
 }
 
 // sm.L[q][p] = the inverse diagonal-block operator of pivot block k0:
@@ -89,21 +96,25 @@ __device__ __forceinline__ void stage_factor(SolveSmem<C, RT, B> &sm, const C *F
 //   !FWD && !TRANS: U^-1       !FWD && TRANS: (L^-1)^T
 // The stored block holds L^-1 strictly below the diagonal (unit diagonal
 // implied) and U^-1 on and above it.
-template <class C, bool FWD, bool TRANS, int RT, int B>
-__device__ __forceinline__ void stage_dinv(SolveSmem<C, RT, B> &sm, const C *F, int f, int k0, int kb) {
-    for (int t = threadIdx.x; t < SNB * kb; t += NT) {
-        const int p = t % SNB, q = t / SNB;   // operator entry (p, q) -> sm.L[q][p], q < kb
+template <class C, bool FWD, bool TRANS, int RT>
+__device__ __forceinline__ void stage_dinv_p(C (*L)[RT], const C *F, int f, int k0, int kb, int lt, int nt) {
+    for (int t = lt; t < SNB * kb; t += nt) {
+        const int p = t % SNB, q = t / SNB;   // operator entry (p, q) -> L[q][p], q < kb
         if (p >= kb) continue;
         const bool lower_src = FWD != TRANS;         // L^-1 (or its transpose) wanted
         const int r = TRANS ? q : p, c = TRANS ? p : q;  // position in the stored block
         const bool stored = lower_src ? r > c : r <= c;
         if (stored) {
-            cp_async_elem(&sm.L[q][p], F + (k0 + r) + (size_t)(k0 + c) * f);
+            cp_async_elem(&L[q][p], F + (k0 + r) + (size_t)(k0 + c) * f);
         } else {
-            using RR = decltype(sm.L[0][0].x);
-            sm.L[q][p] = (lower_src && r == c) ? mk(RR(1), RR(0)) : czero<C>();
+            using RR = decltype(L[0][0].x);
+            L[q][p] = (lower_src && r == c) ? mk(RR(1), RR(0)) : czero<C>();
         }
     }
+}
+template <class C, bool FWD, bool TRANS, int RT, int B>
+__device__ __forceinline__ void stage_dinv(SolveSmem<C, RT, B> &sm, const C *F, int f, int k0, int kb) {
+    stage_dinv_p<C, FWD, TRANS, RT>(sm.L, F, f, k0, kb, threadIdx.x, NT);
 }
 
 // acc[a][b] += sum_q sm.L[q][tr + 16a] * sm.Y[q][tc + 8b] for the output rows
@@ -112,10 +123,10 @@ __device__ __forceinline__ void stage_dinv(SolveSmem<C, RT, B> &sm, const C *F, 
 // rows 4w..4w+3 of each 16-row group), so small fronts and short slices do
 // not pay for the full 64 x 32 tile.
 template <class C, int RT, int B>
-__device__ __forceinline__ void tile_mma(const SolveSmem<C, RT, B> &sm, int qb, C (&acc)[RT / 16][B], int tr, int tc,
-                                         int rows, int rn) {
+__device__ __forceinline__ void tile_mma_p(const C (*L)[RT], const C (*Y)[8 * B], int qb, C (&acc)[RT / 16][B], int tr,
+                                           int tc, int rows, int rn, int lwarp) {
     constexpr int A = RT / 16;
-    const int wrow = (threadIdx.x >> 5) * 4;
+    const int wrow = lwarp * 4;
     const int na = rows <= wrow ? 0 : min(A, (rows - wrow + 15) / 16);
     const int nb = min(B, (rn + 7) / 8);
     if (na == 0) return;   // warp-uniform: this warp owns no row of the tile
@@ -123,9 +134,9 @@ __device__ __forceinline__ void tile_mma(const SolveSmem<C, RT, B> &sm, int qb, 
     for (int q = 0; q < qb; ++q) {
         C l[A], y[B];
 #pragma unroll
-        for (int a = 0; a < A; ++a) l[a] = a < na ? sm.L[q][tr + 16 * a] : czero<C>();
+        for (int a = 0; a < A; ++a) l[a] = a < na ? L[q][tr + 16 * a] : czero<C>();
 #pragma unroll
-        for (int b = 0; b < B; ++b) y[b] = b < nb ? sm.Y[q][tc + 8 * b] : czero<C>();
+        for (int b = 0; b < B; ++b) y[b] = b < nb ? Y[q][tc + 8 * b] : czero<C>();
 #pragma unroll
         for (int a = 0; a < A; ++a) {
             if (a >= na) break;
@@ -134,6 +145,12 @@ __device__ __forceinline__ void tile_mma(const SolveSmem<C, RT, B> &sm, int qb, 
                 if (b < nb) cfma(acc[a][b], l[a], y[b]);
         }
     }
+}
+
+template <class C, int RT, int B>
+__device__ __forceinline__ void tile_mma(const SolveSmem<C, RT, B> &sm, int qb, C (&acc)[RT / 16][B], int tr, int tc,
+                                         int rows, int rn) {
+    tile_mma_p<C, RT, B>(sm.L, sm.Y, qb, acc, tr, tc, rows, rn, threadIdx.x >> 5);
 }
 
 template <class C, int A, int B>
@@ -160,14 +177,17 @@ __device__ __forceinline__ void sub_acc(RowPtr row_ptr, int rows, int rn, const 
     }
 }
 
-// sm.Y[q][r] = row_ptr(q)[r] for q < qb, r < rn (entries outside: as above)
+// Y[q][r] = row_ptr(q)[r] for q < qb, r < rn (entries outside: as above)
+template <class C, int TC, class RowPtr>
+__device__ __forceinline__ void stage_rows_p(C (*Y)[TC], RowPtr row_ptr, int qb, int rn, int lt, int nt) {
+    for (int t = lt; t < qb * TC; t += nt) {
+        const int q = t / TC, r = t % TC;
+        if (r < rn) cp_async_elem(&Y[q][r], row_ptr(q) + r);
+    }
+}
 template <class C, int RT, int B, class RowPtr>
 __device__ __forceinline__ void stage_rows(SolveSmem<C, RT, B> &sm, RowPtr row_ptr, int qb, int rn) {
-    constexpr int TC = 8 * B;
-    for (int t = threadIdx.x; t < qb * TC; t += NT) {
-        const int q = t / TC, r = t % TC;
-        if (r < rn) cp_async_elem(&sm.Y[q][r], row_ptr(q) + r);
-    }
+    stage_rows_p<C, 8 * B>(sm.Y, row_ptr, qb, rn, threadIdx.x, NT);
 }
 
 // false when right-hand sides r0 .. r0 + rn - 1 are zero throughout node v's
@@ -573,6 +593,81 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_bwd_small(SolveA
     }
 }
 
+// Backward pass of whole fronts with at most 32 pivots and at most 32 ring
+// variables (the leaf levels), every right-hand side in one CTA: the
+// front's U'(pivots, ring) block and its diagonal-block inverse are staged
+// once and stay in shared memory while the CTA's two halves (128 threads
+// each, the k_bwd_small thread layout) take the RHS slices two at a time.
+// The factor entries are read once per front instead of once per slice,
+// and each half's x rows (ring and pivot rows together) arrive in one wave
+// of asynchronous copies per slice pair.
+constexpr int FRONT_NT = 2 * NT;
+
+template <class R, int B>
+static size_t bwd_front_smem() {
+    return (2 * SNB * 32 + 4 * SNB * 8 * B) * sizeof(cplx<R>);
+}
+
+template <class R, bool TRANS, int B>
+__global__ void __launch_bounds__(FRONT_NT, 2) k_bwd_front(SolveArgs<R> a, int lvl_first) {
+    using C = cplx<R>;
+    constexpr int RT = 32, TC = 8 * B;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    C(*U)[RT] = reinterpret_cast<C(*)[RT]>(smem_raw);   // U[q][row] = U'(row, s + q)
+    C(*D)[RT] = U + SNB;                                 // the diagonal block's inverse operator
+    C(*Y)[TC] = reinterpret_cast<C(*)[TC]>(D + SNB);    // [2][SNB][TC]: ring x rows of each half
+    C(*P)[TC] = Y + 2 * SNB;                             // [2][SNB][TC]: pivot x rows of each half
+    const Ctx<R> c = make_ctx<R, TC>(a, lvl_first, 0);  // slice 0: X at the first right-hand side
+    const int s = c.s, r = c.f - s;                       // s, r <= SNB (launch condition)
+    if (s == 0) return;
+    const int half = threadIdx.x / NT, lt = threadIdx.x % NT;
+    const int tr = lt / 8, tc = lt % 8, lwarp = lt >> 5;
+    const size_t ldr = a.ldr;
+    stage_factor_p<C, TRANS, RT>(U, c.F, c.f, 0, s, s, r, threadIdx.x, FRONT_NT);
+    stage_dinv_p<C, false, TRANS, RT>(D, c.F, c.f, 0, s, threadIdx.x, FRONT_NT);
+    C(*Yh)[TC] = Y + half * SNB;
+    C(*Ph)[TC] = P + half * SNB;
+    const int nsl = (a.nrhs + TC - 1) / TC;
+    for (int p0 = 0; p0 < nsl; p0 += 2) {   // the same trip count for both halves (barriers below)
+        const int sl = p0 + half;
+        const int rn = sl < nsl ? min(TC, a.nrhs - sl * TC) : 0;
+        C *Xs = c.X + (size_t)sl * TC;
+        if (rn > 0) {
+            stage_rows_p<C, TC>(Yh, [&](int q) { return Xs + (size_t)c.vars[s + q] * ldr; }, r, rn, lt, NT);
+            stage_rows_p<C, TC>(Ph, [&](int q) { return Xs + (size_t)c.vars[q] * ldr; }, s, rn, lt, NT);
+        }
+        staged_sync();   // (the first pass also completes U and D)
+        C acc[RT / 16][B];
+        zero_acc(acc);
+        if (rn > 0) tile_mma_p<C, RT, B>(U, Yh, r, acc, tr, tc, s, rn, lwarp);
+#pragma unroll
+        for (int pp = 0; pp < RT / 16; ++pp) {   // t = y - U'(pivots, ring) x_ring, in place of y
+            const int row = tr + 16 * pp;
+            if (row >= s) continue;
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                const int col = tc + 8 * b;
+                if (col < rn) Ph[row][col] = csub(Ph[row][col], acc[pp][b]);
+            }
+        }
+        __syncthreads();
+        zero_acc(acc);
+        if (rn > 0) tile_mma_p<C, RT, B>(D, Ph, s, acc, tr, tc, s, rn, lwarp);   // x_piv = Dinv t
+#pragma unroll
+        for (int pp = 0; pp < RT / 16; ++pp) {
+            const int row = tr + 16 * pp;
+            if (row >= s) continue;
+            C *x = Xs + (size_t)c.vars[row] * ldr;
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                const int col = tc + 8 * b;
+                if (col < rn) x[col] = acc[pp][b];
+            }
+        }
+        __syncthreads();   // Y and P are staged again
+    }
+}
+
 template <class R, int RT, int B>
 static size_t solve_smem() { return sizeof(SolveSmem<cplx<R>, RT, B>); }
 
@@ -590,6 +685,9 @@ static void set_attrs() {
     cudaFuncSetAttribute((const void *)k_bwd_piv<R, false, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     cudaFuncSetAttribute((const void *)k_bwd_piv<R, true, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (RT == 32) {
+        const int fsm = (int)bwd_front_smem<R, B>();
+        cudaFuncSetAttribute((const void *)k_bwd_front<R, false, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm);
+        cudaFuncSetAttribute((const void *)k_bwd_front<R, true, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm);
         cudaFuncSetAttribute((const void *)k_bwd_small<R, false, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
         cudaFuncSetAttribute((const void *)k_bwd_small<R, true, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
         cudaFuncSetAttribute((const void *)k_fwd_small<R, false, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
@@ -673,6 +771,16 @@ static void backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream
     const size_t smem = solve_smem<R, RT, B>();
     const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
     static const bool no_small = env_int("GM_NO_BWD_SMALL") != 0;
+    static const bool no_front = env_int("GM_NO_BWD_FRONT") != 0;
+    if (RT == 32 && L.max_piv <= SNB && L.max_ring <= SNB && !no_small && !no_front) {   // whole fronts, all slices
+        const size_t fsm = bwd_front_smem<R, B>();
+        for_level_pieces(L, [&](int first, int count) {
+            dim3 g(1, count, solve_nfz(a));
+            if (a.trans) (k_bwd_front<R, true, B><<<g, FRONT_NT, fsm, st>>>(a, first), note_launch());
+            else (k_bwd_front<R, false, B><<<g, FRONT_NT, fsm, st>>>(a, first), note_launch());
+        });
+        return;
+    }
     if (RT == 32 && L.max_piv <= SNB && !no_small) {   // one pivot block per front: fused ring + pivot kernel
         for_level_pieces(L, [&](int first, int count) {
             dim3 g(nchunk, count, solve_nfz(a));

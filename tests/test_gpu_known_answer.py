@@ -3,11 +3,14 @@ homogeneous medium the FP64 wavefield of a point source must decay and turn
 in phase like the outgoing 2-D Green's function, a Hankel function of k r
 (the first or the second kind, depending on the time convention of the
 operator: the reference forms Omega = 2 pi (f - S i), S = 0 here, and the
-PML makes the outgoing kind the one that fits).  Ratios u(r) / u(r0) remove
-the source scaling; they are compared along the source's grid line and
-along a diagonal (the 9-point mixed-grid stencil is nearly isotropic), at
-40 grid points per wavelength and 1 to 2.25 wavelengths from the source,
-at least 10 points from the PML."""
+PML makes the outgoing kind the one that fits -- the second).  Ratios
+u(r) / u(r0) remove the source scaling; they are compared along the
+source's grid line and along a diagonal (the 9-point mixed-grid stencil is
+nearly isotropic), at 25 grid points per wavelength and 1 to 3 wavelengths
+from the source.  The PML is 40 points (1.6 wavelengths) wide: with 20
+points (half a wavelength at 5 Hz) its reflections alone put 7.5 % into the
+ratios (the same solve through the SuperLU oracle on the CPU shows it);
+with 40 points the ratios agree to 0.5 %."""
 import numpy as np
 import pytest
 from scipy.special import hankel1, hankel2
@@ -19,7 +22,7 @@ pytestmark = pytest.mark.gpu
 
 def test_homogeneous_wavefield_follows_the_2d_greens_function():
     nx0 = ny0 = 201
-    npml, dh, f, v = 20, 10.0, 5.0, 2000.0
+    npml, dh, f, v = 40, 10.0, 8.0, 2000.0
     nx, ny = nx0 + 2 * npml, ny0 + 2 * npml
     vp = np.full((ny, nx), v, np.float32)
     rho = np.full((ny, nx), 1000.0, np.float32)
@@ -35,9 +38,9 @@ def test_homogeneous_wavefield_follows_the_2d_greens_function():
         u = e.wavefield_fp64(0, 1)[0, :, 0].reshape(ny, nx)
     r0, c0 = np.unravel_index(np.argmax(np.abs(u)), u.shape)   # the source point
     assert abs(c0 - (npml + 100)) <= 1 and abs(r0 - (npml + 100)) <= 1
-    k = 2.0 * np.pi * f / v                         # 40 points per wavelength
-    steps = np.arange(40, 91, 5)                    # 1 .. 2.25 wavelengths
-    ref = 40
+    k = 2.0 * np.pi * f / v                         # 25 points per wavelength
+    steps = np.arange(25, 76, 5)                    # 1 .. 3 wavelengths
+    ref = 25
     errs = {}
     for name, H in (("first", hankel1), ("second", hankel2)):
         worst = 0.0
@@ -50,5 +53,5 @@ def test_homogeneous_wavefield_follows_the_2d_greens_function():
         errs[name] = worst
     best = min(errs, key=errs.get)
     other = "second" if best == "first" else "first"
-    assert errs[best] < 0.05, errs          # decay and phase of the outgoing wave
+    assert best == "second" and errs[best] < 0.02, errs   # decay and phase of the outgoing wave
     assert errs[other] > 0.5, errs          # the incoming kind does not fit
