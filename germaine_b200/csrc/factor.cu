@@ -522,12 +522,26 @@ __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int 
     };
     if (warp == 0 && s > 0) take_pivot(0);
     __syncthreads();
+    // Each lane holds its rows of the scaled L column k in registers for the
+    // whole step (fronts of at most 4 x 32 rows fit the shared-memory tile),
+    // so an entry's update reads shared memory once, not twice.
+    constexpr int SROWS = 4;
     for (int k = 0; k < s; ++k) {
         const int m = f - k - 1;
+        C lk[SROWS];
+#pragma unroll
+        for (int q = 0; q < SROWS; ++q) {
+            const int ii = lane + 32 * q;
+            lk[q] = ii < m ? S[k + 1 + ii + k * ld] : czero<C>();
+        }
         for (int jj = warp; jj < m; jj += nw) {
             C *col = S + (k + 1 + jj) * ld;
             const C u = col[k];
-            for (int ii = lane; ii < m; ii += 32) cfms(col[k + 1 + ii], S[k + 1 + ii + k * ld], u);
+#pragma unroll
+            for (int q = 0; q < SROWS; ++q) {
+                const int ii = lane + 32 * q;
+                if (ii < m) cfms(col[k + 1 + ii], lk[q], u);
+            }
             if (jj == 0 && k + 1 < s) {   // warp 0 just finished column k + 1
                 __syncwarp();
                 take_pivot(k + 1);
@@ -579,8 +593,8 @@ static size_t small_factor_smem(int fmax) {
 }
 
 template <class R>
-bool small_factor_level(const LevelInfo &L) {
-    return L.count > 0 && small_factor_smem<R>(L.max_front) <= SMALL_FACTOR_SMEM;
+bool small_factor_level(const LevelInfo &L) {   // (the shared-memory bound keeps fronts below 4 x 32 rows)
+    return L.count > 0 && L.max_front <= 128 && small_factor_smem<R>(L.max_front) <= SMALL_FACTOR_SMEM;
 }
 
 template <class R>

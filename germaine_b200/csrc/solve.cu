@@ -121,8 +121,13 @@ __device__ __forceinline__ void stage_dinv(SolveSmem<C, RT, B> &sm, const C *F, 
 // below `rows` and right-hand sides below `rn`; row groups a and column
 // groups b that lie entirely outside are skipped warp-uniformly (a warp owns
 // rows 4w..4w+3 of each 16-row group), so small fronts and short slices do
-// not pay for the full 64 x 32 tile.
-template <class C, int RT, int B>
+// not pay for the full 64 x 32 tile.  TRI: 0 a full operator; TRI_LOWER /
+// TRI_UPPER a triangular one (the diagonal-block inverses), whose column q
+// has no entries above / below row q: 16-row groups that column q does not
+// reach are skipped for that q.
+constexpr int TRI_LOWER = 1, TRI_UPPER = 2;
+
+template <class C, int RT, int B, int TRI = 0>
 __device__ __forceinline__ void tile_mma_p(const C (*L)[RT], const C (*Y)[8 * B], int qb, C (&acc)[RT / 16][B], int tr,
                                            int tc, int rows, int rn, int lwarp) {
     constexpr int A = RT / 16;
@@ -132,14 +137,17 @@ __device__ __forceinline__ void tile_mma_p(const C (*L)[RT], const C (*Y)[8 * B]
     if (na == 0) return;   // warp-uniform: this warp owns no row of the tile
 #pragma unroll 2
     for (int q = 0; q < qb; ++q) {
+        const int alo = TRI == TRI_LOWER ? q / 16 : 0;       // rows >= q only
+        const int ahi = TRI == TRI_UPPER ? q / 16 : A - 1;   // rows <= q only
         C l[A], y[B];
 #pragma unroll
-        for (int a = 0; a < A; ++a) l[a] = a < na ? L[q][tr + 16 * a] : czero<C>();
+        for (int a = 0; a < A; ++a) l[a] = a < na && a >= alo && a <= ahi ? L[q][tr + 16 * a] : czero<C>();
 #pragma unroll
         for (int b = 0; b < B; ++b) y[b] = b < nb ? Y[q][tc + 8 * b] : czero<C>();
 #pragma unroll
         for (int a = 0; a < A; ++a) {
             if (a >= na) break;
+            if (a < alo || a > ahi) continue;
 #pragma unroll
             for (int b = 0; b < B; ++b)
                 if (b < nb) cfma(acc[a][b], l[a], y[b]);
@@ -147,10 +155,10 @@ __device__ __forceinline__ void tile_mma_p(const C (*L)[RT], const C (*Y)[8 * B]
     }
 }
 
-template <class C, int RT, int B>
+template <class C, int RT, int B, int TRI = 0>
 __device__ __forceinline__ void tile_mma(const SolveSmem<C, RT, B> &sm, int qb, C (&acc)[RT / 16][B], int tr, int tc,
                                          int rows, int rn) {
-    tile_mma_p<C, RT, B>(sm.L, sm.Y, qb, acc, tr, tc, rows, rn, threadIdx.x >> 5);
+    tile_mma_p<C, RT, B, TRI>(sm.L, sm.Y, qb, acc, tr, tc, rows, rn, threadIdx.x >> 5);
 }
 
 template <class C, int A, int B>
@@ -286,7 +294,7 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
         stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
         staged_sync();
         zero_acc(acc);
-        tile_mma(sm, kb, acc, tr, tc, kb, c.rn);   // y_b = Dinv w_b
+        tile_mma<C, RT, B, TRI_LOWER>(sm, kb, acc, tr, tc, kb, c.rn);   // y_b = Dinv w_b
         __syncthreads();
 #pragma unroll
         for (int a2 = 0; a2 < 2; ++a2) {
@@ -414,7 +422,7 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
         stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
         staged_sync();
         zero_acc(acc);
-        tile_mma(sm, kb, acc, tr, tc, kb, c.rn);   // x_b = Dinv t_b
+        tile_mma<C, RT, B, TRI_UPPER>(sm, kb, acc, tr, tc, kb, c.rn);   // x_b = Dinv t_b
         __syncthreads();
 #pragma unroll
         for (int a2 = 0; a2 < 2; ++a2) {
@@ -494,7 +502,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_fwd_small(SolveA
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q] * ldr; }, s, c.rn);
         staged_sync();
         zero_acc(acc);
-        tile_mma(sm, s, acc, tr, tc, s, c.rn);   // y = Dinv x_piv
+        tile_mma<C, RT, B, TRI_LOWER>(sm, s, acc, tr, tc, s, c.rn);   // y = Dinv x_piv
         __syncthreads();
 #pragma unroll
         for (int a2 = 0; a2 < RT / 16; ++a2) {
@@ -579,7 +587,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_bwd_small(SolveA
     }
     __syncthreads();
     zero_acc(acc);
-    tile_mma(sm, s, acc, tr, tc, s, c.rn);   // x_piv = Dinv t
+    tile_mma<C, RT, B, TRI_UPPER>(sm, s, acc, tr, tc, s, c.rn);   // x_piv = Dinv t
 #pragma unroll
     for (int p = 0; p < RT / 16; ++p) {
         const int row = tr + 16 * p;
@@ -590,81 +598,6 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_bwd_small(SolveA
             const int col = tc + 8 * b;
             if (col < c.rn) x[col] = acc[p][b];
         }
-    }
-}
-
-// Backward pass of whole fronts with at most 32 pivots and at most 32 ring
-// variables (the leaf levels), every right-hand side in one CTA: the
-// front's U'(pivots, ring) block and its diagonal-block inverse are staged
-// once and stay in shared memory while the CTA's two halves (128 threads
-// each, the k_bwd_small thread layout) take the RHS slices two at a time.
-// The factor entries are read once per front instead of once per slice,
-// and each half's x rows (ring and pivot rows together) arrive in one wave
-// of asynchronous copies per slice pair.
-constexpr int FRONT_NT = 2 * NT;
-
-template <class R, int B>
-static size_t bwd_front_smem() {
-    return (2 * SNB * 32 + 4 * SNB * 8 * B) * sizeof(cplx<R>);
-}
-
-template <class R, bool TRANS, int B>
-__global__ void __launch_bounds__(FRONT_NT, 2) k_bwd_front(SolveArgs<R> a, int lvl_first) {
-    using C = cplx<R>;
-    constexpr int RT = 32, TC = 8 * B;
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    C(*U)[RT] = reinterpret_cast<C(*)[RT]>(smem_raw);   // U[q][row] = U'(row, s + q)
-    C(*D)[RT] = U + SNB;                                 // the diagonal block's inverse operator
-    C(*Y)[TC] = reinterpret_cast<C(*)[TC]>(D + SNB);    // [2][SNB][TC]: ring x rows of each half
-    C(*P)[TC] = Y + 2 * SNB;                             // [2][SNB][TC]: pivot x rows of each half
-    const Ctx<R> c = make_ctx<R, TC>(a, lvl_first, 0);  // slice 0: X at the first right-hand side
-    const int s = c.s, r = c.f - s;                       // s, r <= SNB (launch condition)
-    if (s == 0) return;
-    const int half = threadIdx.x / NT, lt = threadIdx.x % NT;
-    const int tr = lt / 8, tc = lt % 8, lwarp = lt >> 5;
-    const size_t ldr = a.ldr;
-    stage_factor_p<C, TRANS, RT>(U, c.F, c.f, 0, s, s, r, threadIdx.x, FRONT_NT);
-    stage_dinv_p<C, false, TRANS, RT>(D, c.F, c.f, 0, s, threadIdx.x, FRONT_NT);
-    C(*Yh)[TC] = Y + half * SNB;
-    C(*Ph)[TC] = P + half * SNB;
-    const int nsl = (a.nrhs + TC - 1) / TC;
-    for (int p0 = 0; p0 < nsl; p0 += 2) {   // the same trip count for both halves (barriers below)
-        const int sl = p0 + half;
-        const int rn = sl < nsl ? min(TC, a.nrhs - sl * TC) : 0;
-        C *Xs = c.X + (size_t)sl * TC;
-        if (rn > 0) {
-            stage_rows_p<C, TC>(Yh, [&](int q) { return Xs + (size_t)c.vars[s + q] * ldr; }, r, rn, lt, NT);
-            stage_rows_p<C, TC>(Ph, [&](int q) { return Xs + (size_t)c.vars[q] * ldr; }, s, rn, lt, NT);
-        }
-        staged_sync();   // (the first pass also completes U and D)
-        C acc[RT / 16][B];
-        zero_acc(acc);
-        if (rn > 0) tile_mma_p<C, RT, B>(U, Yh, r, acc, tr, tc, s, rn, lwarp);
-#pragma unroll
-        for (int pp = 0; pp < RT / 16; ++pp) {   // t = y - U'(pivots, ring) x_ring, in place of y
-            const int row = tr + 16 * pp;
-            if (row >= s) continue;
-#pragma unroll
-            for (int b = 0; b < B; ++b) {
-                const int col = tc + 8 * b;
-                if (col < rn) Ph[row][col] = csub(Ph[row][col], acc[pp][b]);
-            }
-        }
-        __syncthreads();
-        zero_acc(acc);
-        if (rn > 0) tile_mma_p<C, RT, B>(D, Ph, s, acc, tr, tc, s, rn, lwarp);   // x_piv = Dinv t
-#pragma unroll
-        for (int pp = 0; pp < RT / 16; ++pp) {
-            const int row = tr + 16 * pp;
-            if (row >= s) continue;
-            C *x = Xs + (size_t)c.vars[row] * ldr;
-#pragma unroll
-            for (int b = 0; b < B; ++b) {
-                const int col = tc + 8 * b;
-                if (col < rn) x[col] = acc[pp][b];
-            }
-        }
-        __syncthreads();   // Y and P are staged again
     }
 }
 
@@ -685,9 +618,6 @@ static void set_attrs() {
     cudaFuncSetAttribute((const void *)k_bwd_piv<R, false, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     cudaFuncSetAttribute((const void *)k_bwd_piv<R, true, RT, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
     if (RT == 32) {
-        const int fsm = (int)bwd_front_smem<R, B>();
-        cudaFuncSetAttribute((const void *)k_bwd_front<R, false, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm);
-        cudaFuncSetAttribute((const void *)k_bwd_front<R, true, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, fsm);
         cudaFuncSetAttribute((const void *)k_bwd_small<R, false, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
         cudaFuncSetAttribute((const void *)k_bwd_small<R, true, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
         cudaFuncSetAttribute((const void *)k_fwd_small<R, false, B>, cudaFuncAttributeMaxDynamicSharedMemorySize, sm);
@@ -771,16 +701,6 @@ static void backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream
     const size_t smem = solve_smem<R, RT, B>();
     const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
     static const bool no_small = env_int("GM_NO_BWD_SMALL") != 0;
-    static const bool no_front = env_int("GM_NO_BWD_FRONT") != 0;
-    if (RT == 32 && L.max_piv <= SNB && L.max_ring <= SNB && !no_small && !no_front) {   // whole fronts, all slices
-        const size_t fsm = bwd_front_smem<R, B>();
-        for_level_pieces(L, [&](int first, int count) {
-            dim3 g(1, count, solve_nfz(a));
-            if (a.trans) (k_bwd_front<R, true, B><<<g, FRONT_NT, fsm, st>>>(a, first), note_launch());
-            else (k_bwd_front<R, false, B><<<g, FRONT_NT, fsm, st>>>(a, first), note_launch());
-        });
-        return;
-    }
     if (RT == 32 && L.max_piv <= SNB && !no_small) {   // one pivot block per front: fused ring + pivot kernel
         for_level_pieces(L, [&](int first, int count) {
             dim3 g(nchunk, count, solve_nfz(a));
