@@ -74,7 +74,7 @@ EXPORTS = [
     "gm_lbfgs_create", "gm_lbfgs_destroy", "gm_lbfgs_step", "gm_lbfgs_rotate", "gm_lbfgs_zero",
     "gm_lbfgs_check_descent", "gm_lbfgs_get_old", "gm_lbfgs_set_old", "gm_mat_change",
     "gm_set_shot_taper", "gm_set_shot_block", "gm_set_refine", "gm_memory_estimate", "gm_set_invmat", "gm_set_source_wavelet", "gm_stf_dft", "gm_taper_grad_shot", "gm_taper_grad_shot1", "gm_tikhonov_cost_te", "gm_tikhonov_grad_te",
-    "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_read_grid", "gm_cgemm_sub_c64", "gm_wait_probe", "gm_peak_fp64",
+    "gm_write_seis", "gm_read_seis", "gm_write_model_true", "gm_write_model", "gm_read_model", "gm_read_grid", "gm_cgemm_sub_c64", "gm_wait_probe", "gm_peak_fp64", "gm_peak_fp64_mma",
     "gm_symbolic_create", "gm_symbolic_destroy", "gm_symbolic_sizes", "gm_symbolic_export",
     "gm_symbolic_flops",
 ]
@@ -168,6 +168,7 @@ def load() -> ctypes.CDLL:
     lib.gm_cgemm_sub_c64.argtypes = [i32, i32, i32, vp, vp, vp, vp]
     lib.gm_wait_probe.argtypes = [i32, ctypes.c_longlong, ctypes.POINTER(i32)]
     lib.gm_peak_fp64.argtypes = [i32, ctypes.POINTER(f64)]
+    lib.gm_peak_fp64_mma.argtypes = [i32, ctypes.POINTER(f64)]
     lib.gm_symbolic_create.argtypes = [i32, i32, i32, ctypes.POINTER(vp)]
     lib.gm_symbolic_destroy.argtypes = [vp]
     lib.gm_symbolic_sizes.argtypes = [vp, vp]

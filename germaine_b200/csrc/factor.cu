@@ -445,7 +445,7 @@ template void launch_factor_level<float>(const FactorArgs<float> &, const LevelI
 // ---------------------------------------------------------------------
 constexpr int SMALL_FT = 256;   // threads per CTA
 
-template <class R>
+template <class R, int SROWS>
 __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int lvl_first, int ld) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -523,9 +523,8 @@ __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int 
     if (warp == 0 && s > 0) take_pivot(0);
     __syncthreads();
     // Each lane holds its rows of the scaled L column k in registers for the
-    // whole step (fronts of at most 4 x 32 rows fit the shared-memory tile),
-    // so an entry's update reads shared memory once, not twice.
-    constexpr int SROWS = 4;
+    // whole step (SROWS x 32 >= the level's largest front), so an entry's
+    // update reads shared memory once, not twice.
     for (int k = 0; k < s; ++k) {
         const int m = f - k - 1;
         C lk[SROWS];
@@ -601,11 +600,17 @@ template <class R>
 void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_factor_small<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
+        cudaFuncSetAttribute(k_factor_small<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
+        cudaFuncSetAttribute(k_factor_small<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
+        cudaFuncSetAttribute(k_factor_small<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
         attr_set = true;
     }
     const size_t smem = small_factor_smem<R>(L.max_front);
-    (k_factor_small<R><<<dim3(L.count, a.nf), SMALL_FT, smem, st>>>(a, L.first, L.max_front + 1), note_launch());
+    const dim3 grid(L.count, a.nf);
+    const int ld = L.max_front + 1;
+    if (L.max_front <= 64) (k_factor_small<R, 2><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
+    else if (L.max_front <= 96) (k_factor_small<R, 3><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
+    else (k_factor_small<R, 4><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
 }
 
 template bool small_factor_level<double>(const LevelInfo &);

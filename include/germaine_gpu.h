@@ -551,6 +551,8 @@ int gm_wait_probe(int device, long long polls, int *timed_out);
  * warm-up launches): the denominator of the FP64 roofline fractions.  No
  * counterpart in the reference. */
 int gm_peak_fp64(int device, double *tflops);
+/* The same for FP64 matrix instructions (mma.sync m8n8k4 f64). */
+int gm_peak_fp64_mma(int device, double *tflops);
 
 /* ---- symbolic-analysis introspection (host only, no GPU needed) ---- */
 typedef struct gm_symbolic gm_symbolic;
