@@ -48,10 +48,15 @@ constexpr int NT = 128;   // threads per CTA
 //   B (right-hand sides per CTA = 8 B): every slice re-stages the front's
 //      factor tiles, so wider slices read the factors fewer times.
 
+// Tile rows are padded by SPAD elements: the complex128 tile product reads
+// 8 x 4 fragments (4 pivots x 8 rows), which a stride of RT + 2 spreads over
+// distinct shared-memory banks.
+constexpr int SPAD = 2;
+
 template <class C, int RT, int B>
 struct SolveSmem {
-    C L[SNB][RT];       // factor tile, [pivot q][row]
-    C Y[SNB][8 * B];    // right operand, [pivot q][rhs]
+    C L[SNB][RT + SPAD];       // factor tile, [pivot q][row]
+    C Y[SNB][8 * B + SPAD];    // right operand, [pivot q][rhs]
 };
 
 // factor element M'(i, c) of the forward (L') or backward (U') factor:
@@ -72,8 +77,8 @@ __device__ __forceinline__ C elem(const C *F, int f, int i, int c) {
 // (the _p forms take the tile by pointer and the participating threads as
 // lt = 0 .. nt - 1; the SolveSmem forms are the CTA-wide ones)
 template <class C, bool TRANS, int RT>
-__device__ __forceinline__ void stage_factor_p(C (*L)[RT], const C *F, int f, int i0, int rows, int c0, int qb, int lt,
-                                               int nt) {
+__device__ __forceinline__ void stage_factor_p(C (*L)[RT + SPAD], const C *F, int f, int i0, int rows, int c0, int qb,
+                                               int lt, int nt) {
     if (!TRANS) {
         for (int t = lt; t < RT * qb; t += nt) {
             const int row = t % RT, q = t / RT;
@@ -97,7 +102,7 @@ __device__ __forceinline__ void stage_factor(SolveSmem<C, RT, B> &sm, const C *F
 // The stored block holds L^-1 strictly below the diagonal (unit diagonal
 // implied) and U^-1 on and above it.
 template <class C, bool FWD, bool TRANS, int RT>
-__device__ __forceinline__ void stage_dinv_p(C (*L)[RT], const C *F, int f, int k0, int kb, int lt, int nt) {
+__device__ __forceinline__ void stage_dinv_p(C (*L)[RT + SPAD], const C *F, int f, int k0, int kb, int lt, int nt) {
     for (int t = lt; t < SNB * kb; t += nt) {
         const int p = t % SNB, q = t / SNB;   // operator entry (p, q) -> L[q][p], q < kb
         if (p >= kb) continue;
@@ -117,21 +122,74 @@ __device__ __forceinline__ void stage_dinv(SolveSmem<C, RT, B> &sm, const C *F, 
     stage_dinv_p<C, FWD, TRANS, RT>(sm.L, F, f, k0, kb, threadIdx.x, NT);
 }
 
-// acc[a][b] += sum_q sm.L[q][tr + 16a] * sm.Y[q][tc + 8b] for the output rows
-// below `rows` and right-hand sides below `rn`; row groups a and column
-// groups b that lie entirely outside are skipped warp-uniformly (a warp owns
-// rows 4w..4w+3 of each 16-row group), so small fronts and short slices do
-// not pay for the full 64 x 32 tile.  TRI: 0 a full operator; TRI_LOWER /
-// TRI_UPPER a triangular one (the diagonal-block inverses), whose column q
-// has no entries above / below row q: 16-row groups that column q does not
-// reach are skipped for that q.
+// Per-thread accumulators of an RT x 8B complex output tile (128 threads,
+// lt = 0 .. 127), in the layout of the tile product that fills them.
+template <class C, int RT, int B>
+struct TileAcc;
+
+// complex64: CUDA-core FMAs; thread (tr, tc) = (lt / 8, lt % 8) owns rows
+// tr + 16 i and columns tc + 8 j
+template <int RT, int B>
+struct TileAcc<float2, RT, B> {
+    static constexpr int NR = RT / 16, NC = B;
+    float2 v[NR][NC];
+    __device__ __forceinline__ static int row(int i, int lt) { return lt / 8 + 16 * i; }
+    __device__ __forceinline__ static int col(int j, int lt) { return lt % 8 + 8 * j; }
+};
+
+// complex128: FP64 matrix instructions (mma.sync m8n8k4 f64) on 8 x 8
+// blocks; warp w owns row blocks w + 4 i, lane l row 8 (w + 4 i) + l / 4 of
+// them and columns 8 c + 2 (l % 4) + {0, 1} of every column block c
+template <int RT, int B>
+struct TileAcc<double2, RT, B> {
+    static constexpr int NR = RT / 32, NC = 2 * B;
+    double2 v[NR][NC];
+    __device__ __forceinline__ static int row(int i, int lt) { return 8 * ((lt >> 5) + 4 * i) + ((lt & 31) >> 2); }
+    __device__ __forceinline__ static int col(int j, int lt) { return 8 * (j >> 1) + 2 * (lt & 3) + (j & 1); }
+};
+
+template <class C, int RT, int B>
+__device__ __forceinline__ void zero_acc(TileAcc<C, RT, B> &acc) {
+#pragma unroll
+    for (int i = 0; i < TileAcc<C, RT, B>::NR; ++i)
+#pragma unroll
+        for (int j = 0; j < TileAcc<C, RT, B>::NC; ++j) acc.v[i][j] = czero<C>();
+}
+
+// f(row, col, value) for the thread's accumulators with row < rows, col < rn
+template <class C, int RT, int B, class F>
+__device__ __forceinline__ void for_acc(const TileAcc<C, RT, B> &acc, int rows, int rn, int lt, F f) {
+    using A = TileAcc<C, RT, B>;
+#pragma unroll
+    for (int i = 0; i < A::NR; ++i) {
+        const int row = A::row(i, lt);
+        if (row >= rows) continue;
+#pragma unroll
+        for (int j = 0; j < A::NC; ++j) {
+            const int col = A::col(j, lt);
+            if (col < rn) f(row, col, acc.v[i][j]);
+        }
+    }
+}
+
+// acc += L'[rows x qb] Y[qb x rn]: L[q][row] holds operator entry (row, q),
+// Y[q][col] the right operand.  Rows >= `rows` and columns >= rn of the
+// tile only feed accumulators that are never stored; row and column groups
+// that lie entirely outside are skipped warp-uniformly, so small fronts and
+// short slices do not pay for the full tile.  TRI: 0 a full operator;
+// TRI_LOWER / TRI_UPPER a triangular one (the diagonal-block inverses),
+// whose column q has no entries above / below row q: row groups that column
+// q does not reach are skipped for that q.
 constexpr int TRI_LOWER = 1, TRI_UPPER = 2;
 
-template <class C, int RT, int B, int TRI = 0>
-__device__ __forceinline__ void tile_mma_p(const C (*L)[RT], const C (*Y)[8 * B], int qb, C (&acc)[RT / 16][B], int tr,
-                                           int tc, int rows, int rn, int lwarp) {
+// complex64: each thread accumulates its 16-row-strided rows x 8-column-
+// strided columns with CUDA-core FMAs, one pivot q at a time
+template <int TRI, int RT, int B>
+__device__ __forceinline__ void tile_mma_p(const float2 (*L)[RT + SPAD], const float2 (*Y)[8 * B + SPAD], int qb,
+                                           TileAcc<float2, RT, B> &acc, int rows, int rn, int lt) {
     constexpr int A = RT / 16;
-    const int wrow = lwarp * 4;
+    const int tr = lt / 8, tc = lt % 8;
+    const int wrow = (lt >> 5) * 4;   // a warp owns rows 4w .. 4w + 3 of each 16-row group
     const int na = rows <= wrow ? 0 : min(A, (rows - wrow + 15) / 16);
     const int nb = min(B, (rn + 7) / 8);
     if (na == 0) return;   // warp-uniform: this warp owns no row of the tile
@@ -139,55 +197,85 @@ __device__ __forceinline__ void tile_mma_p(const C (*L)[RT], const C (*Y)[8 * B]
     for (int q = 0; q < qb; ++q) {
         const int alo = TRI == TRI_LOWER ? q / 16 : 0;       // rows >= q only
         const int ahi = TRI == TRI_UPPER ? q / 16 : A - 1;   // rows <= q only
-        C l[A], y[B];
+        float2 l[A], y[B];
 #pragma unroll
-        for (int a = 0; a < A; ++a) l[a] = a < na && a >= alo && a <= ahi ? L[q][tr + 16 * a] : czero<C>();
+        for (int a = 0; a < A; ++a) l[a] = a < na && a >= alo && a <= ahi ? L[q][tr + 16 * a] : czero<float2>();
 #pragma unroll
-        for (int b = 0; b < B; ++b) y[b] = b < nb ? Y[q][tc + 8 * b] : czero<C>();
+        for (int b = 0; b < B; ++b) y[b] = b < nb ? Y[q][tc + 8 * b] : czero<float2>();
 #pragma unroll
         for (int a = 0; a < A; ++a) {
             if (a >= na) break;
             if (a < alo || a > ahi) continue;
 #pragma unroll
             for (int b = 0; b < B; ++b)
-                if (b < nb) cfma(acc[a][b], l[a], y[b]);
+                if (b < nb) cfma(acc.v[a][b], l[a], y[b]);
         }
     }
 }
 
-template <class C, int RT, int B, int TRI = 0>
-__device__ __forceinline__ void tile_mma(const SolveSmem<C, RT, B> &sm, int qb, C (&acc)[RT / 16][B], int tr, int tc,
-                                         int rows, int rn) {
-    tile_mma_p<C, RT, B, TRI>(sm.L, sm.Y, qb, acc, tr, tc, rows, rn, threadIdx.x >> 5);
+// d = a b + d on one 8 x 8 x 4 FP64 block (warp-wide; a: this lane's entry
+// of the 8 x 4 row-major left block, b: of the 4 x 8 column-major right
+// block, d: this lane's two entries of the 8 x 8 result)
+__device__ __forceinline__ void dmma_884(double a, double b, double &d0, double &d1) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
 }
 
-template <class C, int A, int B>
-__device__ __forceinline__ void zero_acc(C (&acc)[A][B]) {
+// complex128: per 4 pivots and per 8 x 8 block, four FP64 matrix
+// instructions (Re += Ar Br - Ai Bi, Im += Ar Bi + Ai Br); a lane loads one
+// complex entry of each left and right fragment.  Pivots q >= qb enter as
+// zeros.
+template <int TRI, int RT, int B>
+__device__ __forceinline__ void tile_mma_p(const double2 (*L)[RT + SPAD], const double2 (*Y)[8 * B + SPAD], int qb,
+                                           TileAcc<double2, RT, B> &acc, int rows, int rn, int lt) {
+    constexpr int NRB = RT / 32;
+    const int w = lt >> 5, lane = lt & 31;
+    const int nb = min(B, (rn + 7) / 8);
+    for (int k0 = 0; k0 < qb; k0 += 4) {
+        const int kk = k0 + (lane & 3);
+        const bool kin = kk < qb;
+        double2 bf[B];
 #pragma unroll
-    for (int a = 0; a < A; ++a)
+        for (int b = 0; b < B; ++b) bf[b] = kin && b < nb ? Y[kk][8 * b + (lane >> 2)] : czero<double2>();
 #pragma unroll
-        for (int b = 0; b < B; ++b) acc[a][b] = czero<C>();
+        for (int i = 0; i < NRB; ++i) {
+            const int rb = w + 4 * i;   // row block: rows 8 rb .. 8 rb + 7
+            if (8 * rb >= rows) break;   // warp-uniform
+            if (TRI == TRI_UPPER && 8 * rb > k0 + 3) continue;   // rows <= q only
+            if (TRI == TRI_LOWER && 8 * rb + 7 < k0) continue;   // rows >= q only
+            const double2 af = kin ? L[kk][8 * rb + (lane >> 2)] : czero<double2>();
+#pragma unroll
+            for (int b = 0; b < B; ++b) {
+                if (b >= nb) break;
+                double2 &d0 = acc.v[i][2 * b], &d1 = acc.v[i][2 * b + 1];
+                dmma_884(af.x, bf[b].x, d0.x, d1.x);
+                dmma_884(-af.y, bf[b].y, d0.x, d1.x);
+                dmma_884(af.x, bf[b].y, d0.y, d1.y);
+                dmma_884(af.y, bf[b].x, d0.y, d1.y);
+            }
+        }
+    }
+}
+
+template <int TRI = 0, class C, int RT, int B>
+__device__ __forceinline__ void tile_mma(const SolveSmem<C, RT, B> &sm, int qb, TileAcc<C, RT, B> &acc, int rows,
+                                         int rn) {
+    tile_mma_p<TRI, RT, B>(sm.L, sm.Y, qb, acc, rows, rn, threadIdx.x);
 }
 
 // row_ptr(row)[col] -= acc for the thread's rows (< rows) and columns (< rn)
-template <class C, int A, int B, class RowPtr>
-__device__ __forceinline__ void sub_acc(RowPtr row_ptr, int rows, int rn, const C (&acc)[A][B], int tr, int tc) {
-#pragma unroll
-    for (int a = 0; a < A; ++a) {
-        const int row = tr + 16 * a;
-        if (row >= rows) continue;
-        C *v = row_ptr(row);
-#pragma unroll
-        for (int b = 0; b < B; ++b) {
-            const int col = tc + 8 * b;
-            if (col < rn) v[col] = csub(v[col], acc[a][b]);
-        }
-    }
+template <class C, int RT, int B, class RowPtr>
+__device__ __forceinline__ void sub_acc(RowPtr row_ptr, int rows, int rn, const TileAcc<C, RT, B> &acc) {
+    for_acc(acc, rows, rn, threadIdx.x, [&](int row, int col, const C &v) {
+        C *x = row_ptr(row);
+        x[col] = csub(x[col], v);
+    });
 }
 
 // Y[q][r] = row_ptr(q)[r] for q < qb, r < rn (entries outside: as above)
 template <class C, int TC, class RowPtr>
-__device__ __forceinline__ void stage_rows_p(C (*Y)[TC], RowPtr row_ptr, int qb, int rn, int lt, int nt) {
+__device__ __forceinline__ void stage_rows_p(C (*Y)[TC + SPAD], RowPtr row_ptr, int qb, int rn, int lt, int nt) {
     for (int t = lt; t < qb * TC; t += nt) {
         const int q = t / TC, r = t % TC;
         if (r < rn) cp_async_elem(&Y[q][r], row_ptr(q) + r);
@@ -261,7 +349,6 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
     const int r0 = blockIdx.x * TC;
     if (!live(a, c.node, r0, c.rn)) return;   // y and the update vector are zero
     (void)fused;
-    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int *inv = a.s.inv + a.s.inv_off[c.node];
     const size_t xz = solve_slot(a);
@@ -287,21 +374,16 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
     }
 
     auto xrow = [&](int k) { return c.X + (size_t)c.vars[k] * ldr; };
-    C acc[RT / 16][B];
+    TileAcc<C, RT, B> acc;
     for (int k0 = 0; k0 < c.s; k0 += SNB) {
         const int kb = min(SNB, c.s - k0);
         stage_dinv<C, true, TRANS, RT, B>(sm, c.F, c.f, k0, kb);
         stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
         staged_sync();
         zero_acc(acc);
-        tile_mma<C, RT, B, TRI_LOWER>(sm, kb, acc, tr, tc, kb, c.rn);   // y_b = Dinv w_b
+        tile_mma<TRI_LOWER>(sm, kb, acc, kb, c.rn);   // y_b = Dinv w_b
         __syncthreads();
-#pragma unroll
-        for (int a2 = 0; a2 < 2; ++a2) {
-            const int p = tr + 16 * a2;
-#pragma unroll
-            for (int b = 0; b < B; ++b) sm.Y[p][tc + 8 * b] = acc[a2][b];
-        }
+        for_acc(acc, kb, c.rn, threadIdx.x, [&](int row, int col, const C &v) { sm.Y[row][col] = v; });
         __syncthreads();
         for (int t = threadIdx.x; t < kb * TC; t += NT) {
             const int q = t / TC, r = t % TC;
@@ -312,9 +394,8 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
             stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, k0, kb);
             staged_sync();
             zero_acc(acc);
-            tile_mma(sm, kb, acc, tr, tc, rows, c.rn);
-            sub_acc(
-                [&](int row) { return xrow(i0 + row); }, rows, c.rn, acc, tr, tc);
+            tile_mma(sm, kb, acc, rows, c.rn);
+            sub_acc([&](int row) { return xrow(i0 + row); }, rows, c.rn, acc);
             __syncthreads();
         }
     }
@@ -335,16 +416,15 @@ __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, 
     if (c.rn <= 0 || i0 >= c.f) return;
     if (!live(a, c.node, chunk * TC, c.rn)) return;   // the update vector is zero (never read)
     const int rows = min(RT, c.f - i0);
-    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const size_t ldr = a.ldr;
-    C acc[RT / 16][B];
+    TileAcc<C, RT, B> acc;
     zero_acc(acc);
     for (int q0 = 0; q0 < c.s; q0 += SNB) {
         const int qb = min(SNB, c.s - q0);
         stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, q0, qb);
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q0 + q] * ldr; }, qb, c.rn);
         staged_sync();
-        tile_mma(sm, qb, acc, tr, tc, rows, c.rn);
+        tile_mma(sm, qb, acc, rows, c.rn);
         __syncthreads();
     }
     // w = (children's update vectors at the ring rows) - L'(ring, piv) y
@@ -353,23 +433,14 @@ __global__ void __launch_bounds__(NT) k_fwd_ring(SolveArgs<R> a, int lvl_first, 
     const int c0 = a.s.child0[c.node], c1 = a.s.child1[c.node];
     const C *W0 = c0 >= 0 && live(a, c0, chunk * TC, c.rn) ? Wall + (size_t)a.s.rhs_off[c0] * a.ldr : nullptr;
     const C *W1 = c1 >= 0 && live(a, c1, chunk * TC, c.rn) ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
-#pragma unroll
-    for (int p = 0; p < RT / 16; ++p) {
-        const int row = tr + 16 * p;
-        if (row >= rows) continue;
+    for_acc(acc, rows, c.rn, threadIdx.x, [&](int row, int r, const C &v) {
         const int i = i0 + row;
         const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
-        C *w = c.W + (size_t)(i - c.s) * ldr;
-#pragma unroll
-        for (int b = 0; b < B; ++b) {
-            const int r = tc + 8 * b;
-            if (r >= c.rn) continue;
-            C g = czero<C>();
-            if (q0 >= 0) g = cadd(g, W0[(size_t)q0 * ldr + r]);
-            if (q1 >= 0) g = cadd(g, W1[(size_t)q1 * ldr + r]);
-            w[r] = csub(g, acc[p][b]);
-        }
-    }
+        C g = czero<C>();
+        if (q0 >= 0) g = cadd(g, W0[(size_t)q0 * ldr + r]);
+        if (q1 >= 0) g = cadd(g, W1[(size_t)q1 * ldr + r]);
+        c.W[(size_t)(i - c.s) * ldr + r] = csub(g, v);
+    });
 }
 
 // Backward pass, ring part: x[pivots] -= U'(pivots, ring) x[ring]
@@ -385,19 +456,18 @@ __global__ void __launch_bounds__(NT) k_bwd_ring(SolveArgs<R> a, int lvl_first, 
     const int i0 = tile * RT;
     if (c.rn <= 0 || i0 >= c.s || c.f == c.s) return;
     const int rows = min(RT, c.s - i0);
-    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const size_t ldr = a.ldr;
-    C acc[RT / 16][B];
+    TileAcc<C, RT, B> acc;
     zero_acc(acc);
     for (int j0 = c.s; j0 < c.f; j0 += SNB) {
         const int jb = min(SNB, c.f - j0);
         stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, j0, jb);
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[j0 + q] * ldr; }, jb, c.rn);
         staged_sync();
-        tile_mma(sm, jb, acc, tr, tc, rows, c.rn);
+        tile_mma(sm, jb, acc, rows, c.rn);
         __syncthreads();
     }
-    sub_acc([&](int row) { return c.X + (size_t)c.vars[i0 + row] * ldr; }, rows, c.rn, acc, tr, tc);
+    sub_acc([&](int row) { return c.X + (size_t)c.vars[i0 + row] * ldr; }, rows, c.rn, acc);
 }
 
 // Backward pass, pivot part: block by block from the last, x_b = Dinv t_b in
@@ -411,10 +481,9 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
     const Ctx<R> c = make_ctx<R, TC>(a, lvl_first, blockIdx.x);
     if (c.rn <= 0) return;
     (void)fused;
-    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const size_t ldr = a.ldr;
     auto xrow = [&](int k) { return c.X + (size_t)c.vars[k] * ldr; };
-    C acc[RT / 16][B];
+    TileAcc<C, RT, B> acc;
     const int nblk = (c.s + SNB - 1) / SNB;
     for (int b = nblk - 1; b >= 0; --b) {
         const int k0 = b * SNB, kb = min(SNB, c.s - k0);
@@ -422,14 +491,9 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
         stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
         staged_sync();
         zero_acc(acc);
-        tile_mma<C, RT, B, TRI_UPPER>(sm, kb, acc, tr, tc, kb, c.rn);   // x_b = Dinv t_b
+        tile_mma<TRI_UPPER>(sm, kb, acc, kb, c.rn);   // x_b = Dinv t_b
         __syncthreads();
-#pragma unroll
-        for (int a2 = 0; a2 < 2; ++a2) {
-            const int p = tr + 16 * a2;
-#pragma unroll
-            for (int bb = 0; bb < B; ++bb) sm.Y[p][tc + 8 * bb] = acc[a2][bb];
-        }
+        for_acc(acc, kb, c.rn, threadIdx.x, [&](int row, int col, const C &v) { sm.Y[row][col] = v; });
         __syncthreads();
         for (int t = threadIdx.x; t < kb * TC; t += NT) {
             const int q = t / TC, r = t % TC;
@@ -440,8 +504,8 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
             stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, k0, kb);
             staged_sync();
             zero_acc(acc);
-            tile_mma(sm, kb, acc, tr, tc, rows, c.rn);
-            sub_acc([&](int row) { return xrow(i0 + row); }, rows, c.rn, acc, tr, tc);
+            tile_mma(sm, kb, acc, rows, c.rn);
+            sub_acc([&](int row) { return xrow(i0 + row); }, rows, c.rn, acc);
             __syncthreads();
         }
     }
@@ -471,7 +535,6 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_fwd_small(SolveA
     if (c.rn <= 0) return;
     const int r0 = wk.y * TC;
     if (!live(a, c.node, r0, c.rn)) return;   // y and the update vector are zero
-    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int *inv = a.s.inv + a.s.inv_off[c.node];
     const size_t xz = solve_slot(a);
@@ -496,20 +559,15 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_fwd_small(SolveA
         }
         __syncthreads();
     }
-    C acc[RT / 16][B];
+    TileAcc<C, RT, B> acc;
     if (s > 0) {
         stage_dinv<C, true, TRANS, RT, B>(sm, c.F, c.f, 0, s);
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q] * ldr; }, s, c.rn);
         staged_sync();
         zero_acc(acc);
-        tile_mma<C, RT, B, TRI_LOWER>(sm, s, acc, tr, tc, s, c.rn);   // y = Dinv x_piv
+        tile_mma<TRI_LOWER>(sm, s, acc, s, c.rn);   // y = Dinv x_piv
         __syncthreads();
-#pragma unroll
-        for (int a2 = 0; a2 < RT / 16; ++a2) {
-            const int p = tr + 16 * a2;
-#pragma unroll
-            for (int b = 0; b < B; ++b) sm.Y[p][tc + 8 * b] = acc[a2][b];
-        }
+        for_acc(acc, s, c.rn, threadIdx.x, [&](int row, int col, const C &v) { sm.Y[row][col] = v; });
         __syncthreads();
         for (int t = threadIdx.x; t < s * TC; t += NT) {
             const int q = t / TC, r = t % TC;
@@ -522,24 +580,15 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_fwd_small(SolveA
         stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, i0, rows, 0, s);
         staged_sync();
         zero_acc(acc);
-        tile_mma(sm, s, acc, tr, tc, rows, c.rn);
-#pragma unroll
-        for (int p = 0; p < RT / 16; ++p) {
-            const int row = tr + 16 * p;
-            if (row >= rows) continue;
+        tile_mma(sm, s, acc, rows, c.rn);
+        for_acc(acc, rows, c.rn, threadIdx.x, [&](int row, int r, const C &v) {
             const int i = i0 + row;
             const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
-            C *w = c.W + (size_t)(i - s) * ldr;
-#pragma unroll
-            for (int b = 0; b < B; ++b) {
-                const int r = tc + 8 * b;
-                if (r >= c.rn) continue;
-                C g = czero<C>();
-                if (q0 >= 0) g = cadd(g, W0[(size_t)q0 * ldr + r]);
-                if (q1 >= 0) g = cadd(g, W1[(size_t)q1 * ldr + r]);
-                w[r] = csub(g, acc[p][b]);
-            }
-        }
+            C g = czero<C>();
+            if (q0 >= 0) g = cadd(g, W0[(size_t)q0 * ldr + r]);
+            if (q1 >= 0) g = cadd(g, W1[(size_t)q1 * ldr + r]);
+            c.W[(size_t)(i - s) * ldr + r] = csub(g, v);
+        });
         __syncthreads();   // sm.L is staged again for the next tile
     }
 }
@@ -558,47 +607,27 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_bwd_small(SolveA
     constexpr int TC = 8 * B;
     const Ctx<R> c = make_ctx<R, TC>(a, lvl_first, blockIdx.x);
     if (c.rn <= 0 || c.s == 0) return;
-    const int tr = threadIdx.x / 8, tc = threadIdx.x % 8;
     const size_t ldr = a.ldr;
     const int s = c.s;   // <= SNB (launch condition)
-    C acc[RT / 16][B];
+    TileAcc<C, RT, B> acc;
     zero_acc(acc);
     for (int j0 = s; j0 < c.f; j0 += SNB) {
         const int jb = min(SNB, c.f - j0);
         stage_factor<C, TRANS, RT, B>(sm, c.F, c.f, 0, s, j0, jb);
         stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[j0 + q] * ldr; }, jb, c.rn);
         staged_sync();
-        tile_mma(sm, jb, acc, tr, tc, s, c.rn);
+        tile_mma(sm, jb, acc, s, c.rn);
         __syncthreads();
     }
     // t = y - acc in sm.Y (row q of the next product's right operand = pivot q)
     stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q] * ldr; }, s, c.rn);
     stage_dinv<C, false, TRANS, RT, B>(sm, c.F, c.f, 0, s);
     staged_sync();
-#pragma unroll
-    for (int p = 0; p < RT / 16; ++p) {
-        const int row = tr + 16 * p;
-        if (row >= s) continue;
-#pragma unroll
-        for (int b = 0; b < B; ++b) {
-            const int col = tc + 8 * b;
-            if (col < c.rn) sm.Y[row][col] = csub(sm.Y[row][col], acc[p][b]);
-        }
-    }
+    for_acc(acc, s, c.rn, threadIdx.x, [&](int row, int col, const C &v) { sm.Y[row][col] = csub(sm.Y[row][col], v); });
     __syncthreads();
     zero_acc(acc);
-    tile_mma<C, RT, B, TRI_UPPER>(sm, s, acc, tr, tc, s, c.rn);   // x_piv = Dinv t
-#pragma unroll
-    for (int p = 0; p < RT / 16; ++p) {
-        const int row = tr + 16 * p;
-        if (row >= s) continue;
-        C *x = c.X + (size_t)c.vars[row] * ldr;
-#pragma unroll
-        for (int b = 0; b < B; ++b) {
-            const int col = tc + 8 * b;
-            if (col < c.rn) x[col] = acc[p][b];
-        }
-    }
+    tile_mma<TRI_UPPER>(sm, s, acc, s, c.rn);   // x_piv = Dinv t
+    for_acc(acc, s, c.rn, threadIdx.x, [&](int row, int col, const C &v) { c.X[(size_t)c.vars[row] * ldr + col] = v; });
 }
 
 template <class R, int RT, int B>
