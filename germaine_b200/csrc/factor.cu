@@ -37,6 +37,95 @@ constexpr int TILE = 64;     // Schur-update tile
 constexpr int PCHUNK = 128;  // panel rows / columns per CTA
 
 constexpr int GATHER_COLS = 4;   // front columns per CTA of the extend-add gather
+constexpr int TSTR = TILE + 2;   // padded row stride of staged 64-wide tiles (conflict-free 8 x 4 fragments)
+
+// 64 x 64 complex output tile of a 256-thread CTA, in the layout of the
+// product that fills it: complex64 with CUDA-core FMAs, thread t owning
+// rows t % 16 + 16 i and columns t / 16 + 16 j (v[i][j]); complex128 on FP64
+// matrix instructions (mma.sync m8n8k4 f64), warp w owning row block w
+// (rows 8 w .. 8 w + 7) of all eight column blocks, lane l row 8 w + l / 4
+// and columns 8 i + 2 (l % 4) + j (v[i][j]).
+template <class C>
+struct Tile64;
+template <>
+struct Tile64<float2> {
+    static constexpr int NI = 4, NJ = 4;
+    float2 v[NI][NJ];
+    __device__ __forceinline__ static int row(int i, int, int t) { return t % 16 + 16 * i; }
+    __device__ __forceinline__ static int col(int, int j, int t) { return t / 16 + 16 * j; }
+};
+template <>
+struct Tile64<double2> {
+    static constexpr int NI = 8, NJ = 2;
+    double2 v[NI][NJ];
+    __device__ __forceinline__ static int row(int, int, int t) { return 8 * (t >> 5) + ((t & 31) >> 2); }
+    __device__ __forceinline__ static int col(int i, int j, int t) { return 8 * i + 2 * (t & 3) + j; }
+};
+
+// f(row, col, value) over the thread's entries of the tile
+template <class C, class F>
+__device__ __forceinline__ void for_tile64(Tile64<C> &acc, int t, F f) {
+#pragma unroll
+    for (int i = 0; i < Tile64<C>::NI; ++i)
+#pragma unroll
+        for (int j = 0; j < Tile64<C>::NJ; ++j) f(Tile64<C>::row(i, j, t), Tile64<C>::col(i, j, t), acc.v[i][j]);
+}
+
+// acc += A B (NEG: acc -= A B) over k < kb, A(r, k) = As[k * ak + r * ar]
+// for rows r < mrows, B(k, c) = Bs[k * bk + c * bc] for columns c < ncols
+// (entries outside read as zero)
+template <bool NEG>
+__device__ __forceinline__ void mma64(const float2 *As, int ak, int ar, const float2 *Bs, int bk, int bc, int kb,
+                                      int mrows, int ncols, Tile64<float2> &acc, int t) {
+    const int tx = t % 16, ty = t / 16;
+    for (int k = 0; k < kb; ++k) {
+        float2 lv[4], uv[4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            lv[i] = tx + 16 * i < mrows ? As[(size_t)k * ak + (size_t)(tx + 16 * i) * ar] : czero<float2>();
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            uv[j] = ty + 16 * j < ncols ? Bs[(size_t)k * bk + (size_t)(ty + 16 * j) * bc] : czero<float2>();
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+                if (NEG) cfms(acc.v[i][j], lv[i], uv[j]);
+                else cfma(acc.v[i][j], lv[i], uv[j]);
+            }
+    }
+}
+
+__device__ __forceinline__ void dmma_884(double a, double b, double &d0, double &d1) {
+    asm volatile("mma.sync.aligned.m8n8k4.row.col.f64.f64.f64.f64 {%0, %1}, {%2}, {%3}, {%0, %1};\n"
+                 : "+d"(d0), "+d"(d1)
+                 : "d"(a), "d"(b));
+}
+
+template <bool NEG>
+__device__ __forceinline__ void mma64(const double2 *As, int ak, int ar, const double2 *Bs, int bk, int bc, int kb,
+                                      int mrows, int ncols, Tile64<double2> &acc, int t) {
+    const int w = t >> 5, lane = t & 31, g = lane >> 2;
+    const int r = 8 * w + g;
+    if (8 * w >= mrows) return;   // warp-uniform: no row of this block is used
+    for (int k0 = 0; k0 < kb; k0 += 4) {
+        const int kk = k0 + (lane & 3);
+        const bool kin = kk < kb;
+        double2 af = kin && r < mrows ? As[(size_t)kk * ak + (size_t)r * ar] : czero<double2>();
+        if (NEG) af = make_double2(-af.x, -af.y);
+#pragma unroll
+        for (int i = 0; i < 8; ++i) {
+            if (8 * i >= ncols) break;   // warp-uniform
+            const int c = 8 * i + g;
+            const double2 bf = kin && c < ncols ? Bs[(size_t)kk * bk + (size_t)c * bc] : czero<double2>();
+            double2 &d0 = acc.v[i][0], &d1 = acc.v[i][1];
+            dmma_884(af.x, bf.x, d0.x, d1.x);    // Re += Ar Br
+            dmma_884(-af.y, bf.y, d0.x, d1.x);   //     - Ai Bi
+            dmma_884(af.x, bf.y, d0.y, d1.y);    // Im += Ar Bi
+            dmma_884(af.y, bf.x, d0.y, d1.y);    //     + Ai Br
+        }
+    }
+}
 
 template <class R>
 __global__ void k_front_gather(FactorArgs<R> a, int lvl_first) {
@@ -254,49 +343,29 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
     if (i0 + ti * TILE >= s && i0 + tj * TILE >= s) return;   // tile inside the contribution block
 
     extern __shared__ unsigned char smem_raw[];
-    C *Ls = reinterpret_cast<C *>(smem_raw);   // [NB][TILE]: Ls[c*TILE + r]
-    C *Us = Ls + NB * TILE;                    // [NB][TILE]: Us[c*TILE + col]
+    C *Ls = reinterpret_cast<C *>(smem_raw);   // [NB][TSTR]: Ls[c * TSTR + r]
+    C *Us = Ls + NB * TSTR;                    // [NB][TSTR]: Us[c * TSTR + col]
     const int r0 = i0 + ti * TILE, c0 = i0 + tj * TILE;
     // asynchronous copies, all in flight at once; entries outside the
-    // front or beyond kb are not staged (the pivot loop reads c < kb only,
-    // and rows / columns outside the front feed accumulators never stored)
+    // front or beyond kb are not staged (the product reads k < kb only and
+    // treats rows / columns outside the front as zero)
     for (int t = threadIdx.x; t < NB * TILE; t += blockDim.x) {
         const int r = t % TILE, c = t / TILE;
-        if (c < kb && r0 + r < f) cp_async_elem(Ls + t, F + (r0 + r) + (size_t)(k0 + c) * f);
+        if (c < kb && r0 + r < f) cp_async_elem(Ls + c * TSTR + r, F + (r0 + r) + (size_t)(k0 + c) * f);
         const int col = t / NB, cc = t % NB;   // U: contiguous along the pivot index
-        if (cc < kb && c0 + col < f) cp_async_elem(Us + cc * TILE + col, F + (k0 + cc) + (size_t)(c0 + col) * f);
+        if (cc < kb && c0 + col < f) cp_async_elem(Us + cc * TSTR + col, F + (k0 + cc) + (size_t)(c0 + col) * f);
     }
     staged_sync();
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
-    C acc[4][4];
-#pragma unroll
-    for (int p = 0; p < 4; ++p)
-#pragma unroll
-        for (int q = 0; q < 4; ++q) acc[p][q] = czero<C>();
-    for (int c = 0; c < kb; ++c) {
-        C lv[4], uv[4];
-#pragma unroll
-        for (int p = 0; p < 4; ++p) lv[p] = Ls[c * TILE + tx + 16 * p];
-#pragma unroll
-        for (int q = 0; q < 4; ++q) uv[q] = Us[c * TILE + ty + 16 * q];
-#pragma unroll
-        for (int p = 0; p < 4; ++p)
-#pragma unroll
-            for (int q = 0; q < 4; ++q) cfma(acc[p][q], lv[p], uv[q]);
-    }
-#pragma unroll
-    for (int q = 0; q < 4; ++q) {
-        const int col = c0 + ty + 16 * q;
-        if (col >= f) continue;
-#pragma unroll
-        for (int p = 0; p < 4; ++p) {
-            const int row = r0 + tx + 16 * p;
-            if (row < f && (row < s || col < s)) {
-                C &d = F[row + (size_t)col * f];
-                d = csub(d, acc[p][q]);
-            }
+    Tile64<C> acc;
+    for_tile64(acc, threadIdx.x, [](int, int, C &v) { v = czero<C>(); });
+    mma64<false>(Ls, TSTR, 1, Us, TSTR, 1, kb, min(TILE, f - r0), min(TILE, f - c0), acc, threadIdx.x);
+    for_tile64(acc, threadIdx.x, [&](int rr, int cc, C &v) {
+        const int row = r0 + rr, col = c0 + cc;
+        if (row < f && col < f && (row < s || col < s)) {
+            C &d = F[row + (size_t)col * f];
+            d = csub(d, v);
         }
-    }
+    });
 }
 
 // Batched C -= A * B on CUDA cores (64 x 64 output tiles, 4 x 4 complex
@@ -316,26 +385,23 @@ __global__ void __launch_bounds__(256) k_gemm_sub_cc(const GemmProb<R> *__restri
     const GemmProb<R> p = probs[tl.x];
     const int r0 = tl.y * TILE, c0 = tl.z * TILE;
     extern __shared__ unsigned char smem_raw[];
-    C *As = reinterpret_cast<C *>(smem_raw);   // [2][GKC][TILE]: As[c * TILE + r]
-    C *Bs = As + 2 * GKC * TILE;               // [2][GKC][TILE]: Bs[c * TILE + col]
-    const int tx = threadIdx.x % 16, ty = threadIdx.x / 16;
+    C *As = reinterpret_cast<C *>(smem_raw);   // [2][GKC][TSTR]: As[c * TSTR + r]
+    C *Bs = As + 2 * GKC * TSTR;               // [2][GKC][TSTR]: Bs[c * TSTR + col]
     auto stage = [&](int buf, int k0) {
         const int kb = min(GKC, p.k - k0);
-        C *Ab = As + buf * GKC * TILE, *Bb = Bs + buf * GKC * TILE;
+        C *Ab = As + buf * GKC * TSTR, *Bb = Bs + buf * GKC * TSTR;
         for (int t = threadIdx.x; t < GKC * TILE; t += blockDim.x) {
             const int r = t % TILE, c = t / TILE;
-            if (c < kb && r0 + r < p.m) cp_async_elem(Ab + t, p.A + (size_t)(r0 + r) + (size_t)(k0 + c) * p.lda);
+            if (c < kb && r0 + r < p.m) cp_async_elem(Ab + c * TSTR + r, p.A + (size_t)(r0 + r) + (size_t)(k0 + c) * p.lda);
             const int col = t / GKC, cc = t % GKC;   // B: contiguous along k
             if (cc < kb && c0 + col < p.n)
-                cp_async_elem(Bb + cc * TILE + col, p.B + (size_t)(k0 + cc) + (size_t)(c0 + col) * p.ldb);
+                cp_async_elem(Bb + cc * TSTR + col, p.B + (size_t)(k0 + cc) + (size_t)(c0 + col) * p.ldb);
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
-    C acc[4][4];
-#pragma unroll
-    for (int i = 0; i < 4; ++i)
-#pragma unroll
-        for (int j = 0; j < 4; ++j) acc[i][j] = czero<C>();
+    Tile64<C> acc;
+    for_tile64(acc, threadIdx.x, [](int, int, C &v) { v = czero<C>(); });
+    const int mrows = min(TILE, p.m - r0), ncols = min(TILE, p.n - c0);
     const int nk = (p.k + GKC - 1) / GKC;
     if (nk > 0) stage(0, 0);
     for (int kc = 0; kc < nk; ++kc) {
@@ -347,39 +413,23 @@ __global__ void __launch_bounds__(256) k_gemm_sub_cc(const GemmProb<R> *__restri
         }
         __syncthreads();
         const int kb = min(GKC, p.k - kc * GKC);
-        const C *Ab = As + (kc & 1) * GKC * TILE, *Bb = Bs + (kc & 1) * GKC * TILE;
-        for (int c = 0; c < kb; ++c) {
-            C lv[4], uv[4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i) lv[i] = Ab[c * TILE + tx + 16 * i];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) uv[j] = Bb[c * TILE + ty + 16 * j];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int j = 0; j < 4; ++j) cfma(acc[i][j], lv[i], uv[j]);
-        }
+        mma64<false>(As + (kc & 1) * GKC * TSTR, TSTR, 1, Bs + (kc & 1) * GKC * TSTR, TSTR, 1, kb, mrows, ncols, acc,
+                     threadIdx.x);
         __syncthreads();   // this buffer is staged again for chunk kc + 2
     }
-#pragma unroll
-    for (int j = 0; j < 4; ++j) {
-        const int col = c0 + ty + 16 * j;
-        if (col >= p.n) continue;
-#pragma unroll
-        for (int i = 0; i < 4; ++i) {
-            const int row = r0 + tx + 16 * i;
-            if (row < p.m) {
-                C &d = p.C[(size_t)row + (size_t)col * p.ldc];
-                d = csub(d, acc[i][j]);
-            }
+    for_tile64(acc, threadIdx.x, [&](int rr, int cc, C &v) {
+        const int row = r0 + rr, col = c0 + cc;
+        if (row < p.m && col < p.n) {
+            C &d = p.C[(size_t)row + (size_t)col * p.ldc];
+            d = csub(d, v);
         }
-    }
+    });
 }
 
 template <class R>
 void launch_gemm_sub_cc(const GemmProb<R> *d_probs, const int4 *d_tiles, int ntiles, cudaStream_t st) {
     if (ntiles <= 0) return;
-    const size_t smem = 4 * GKC * TILE * sizeof(cplx<R>);
+    const size_t smem = 4 * GKC * TSTR * sizeof(cplx<R>);
     static bool attr = false;
     if (!attr) {
         cudaFuncSetAttribute(k_gemm_sub_cc<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -405,7 +455,7 @@ void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
         (k_entry_scatter<R><<<dim3((unsigned)((L.ent_count + tpb - 1) / tpb), a.nf), tpb, 0, st>>>(a, L.ent_first,
                                                                                                   L.ent_count), note_launch());
     }
-    const size_t smem = 2 * NB * TILE * sizeof(C);
+    const size_t smem = 2 * NB * TSTR * sizeof(C);
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
@@ -809,42 +859,21 @@ __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_
     }
     if (tid == 0 && npert) atomicAdd(a.npert, (unsigned long long)npert);
 
-    // 5. contribution block -= L21 U12
-    const int tx = tid % 16, ty = tid / 16;
+    // 5. contribution block -= L21 U12, 64 x 64 tiles, each tile's old
+    // values loaded into the accumulators first
     for (int i0 = 0; i0 < m; i0 += 64)
         for (int j0 = 0; j0 < m; j0 += 64) {
-            C acc[4][4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int p = 0; p < 4; ++p) {
-                    const int i = i0 + tx + 16 * p, j = j0 + ty + 16 * q;
-                    acc[p][q] = (i < m && j < m) ? F[s + i + (size_t)(s + j) * f] : czero<C>();
-                }
-            for (int k = 0; k < s; ++k) {
-                C lv[4], uv[4];
-#pragma unroll
-                for (int p = 0; p < 4; ++p) {
-                    const int i = i0 + tx + 16 * p;
-                    lv[p] = i < m ? P[s + i + k * ldp] : czero<C>();
-                }
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const int j = j0 + ty + 16 * q;
-                    uv[q] = j < m ? U[k + j * ldu] : czero<C>();
-                }
-#pragma unroll
-                for (int p = 0; p < 4; ++p)
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) cfms(acc[p][q], lv[p], uv[q]);
-            }
-#pragma unroll
-            for (int q = 0; q < 4; ++q)
-#pragma unroll
-                for (int p = 0; p < 4; ++p) {
-                    const int i = i0 + tx + 16 * p, j = j0 + ty + 16 * q;
-                    if (i < m && j < m) F[s + i + (size_t)(s + j) * f] = acc[p][q];
-                }
+            Tile64<C> acc;
+            for_tile64(acc, tid, [&](int rr, int cc, C &v) {
+                const int i = i0 + rr, j = j0 + cc;
+                v = (i < m && j < m) ? F[s + i + (size_t)(s + j) * f] : czero<C>();
+            });
+            mma64<true>(P + s + i0, ldp, 1, U + (size_t)j0 * ldu, 1, ldu, s, min(64, m - i0), min(64, m - j0), acc,
+                        tid);
+            for_tile64(acc, tid, [&](int rr, int cc, C &v) {
+                const int i = i0 + rr, j = j0 + cc;
+                if (i < m && j < m) F[s + i + (size_t)(s + j) * f] = v;
+            });
         }
 }
 
