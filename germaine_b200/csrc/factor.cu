@@ -42,9 +42,11 @@ constexpr int TSTR = TILE + 2;   // padded row stride of staged 64-wide tiles (c
 // 64 x 64 complex output tile of a 256-thread CTA, in the layout of the
 // product that fills it: complex64 with CUDA-core FMAs, thread t owning
 // rows t % 16 + 16 i and columns t / 16 + 16 j (v[i][j]); complex128 on FP64
-// matrix instructions (mma.sync m8n8k4 f64), warp w owning row block w
-// (rows 8 w .. 8 w + 7) of all eight column blocks, lane l row 8 w + l / 4
-// and columns 8 i + 2 (l % 4) + j (v[i][j]).
+// matrix instructions (mma.sync m8n8k4 f64) on 8 x 8 blocks, warp w owning
+// row blocks w % 4 and w % 4 + 4 of column blocks 4 (w / 4) .. 4 (w / 4) + 3
+// (so a tile with few rows still keeps six of the eight warps busy), lane l
+// row 8 rb + l / 4 and columns 8 cb + 2 (l % 4) + j of each owned block;
+// v[4 rbi + cbi][j] for row block w % 4 + 4 rbi, column block 4 (w / 4) + cbi.
 template <class C>
 struct Tile64;
 template <>
@@ -58,8 +60,12 @@ template <>
 struct Tile64<double2> {
     static constexpr int NI = 8, NJ = 2;
     double2 v[NI][NJ];
-    __device__ __forceinline__ static int row(int, int, int t) { return 8 * (t >> 5) + ((t & 31) >> 2); }
-    __device__ __forceinline__ static int col(int i, int j, int t) { return 8 * i + 2 * (t & 3) + j; }
+    __device__ __forceinline__ static int row(int i, int, int t) {
+        return 8 * ((t >> 5) % 4 + 4 * (i / 4)) + ((t & 31) >> 2);
+    }
+    __device__ __forceinline__ static int col(int i, int j, int t) {
+        return 8 * (4 * ((t >> 5) / 4) + i % 4) + 2 * (t & 3) + j;
+    }
 };
 
 // f(row, col, value) over the thread's entries of the tile
@@ -106,23 +112,33 @@ template <bool NEG>
 __device__ __forceinline__ void mma64(const double2 *As, int ak, int ar, const double2 *Bs, int bk, int bc, int kb,
                                       int mrows, int ncols, Tile64<double2> &acc, int t) {
     const int w = t >> 5, lane = t & 31, g = lane >> 2;
-    const int r = 8 * w + g;
-    if (8 * w >= mrows) return;   // warp-uniform: no row of this block is used
+    const int rb0 = w % 4, cb0 = 4 * (w / 4);
+    if (8 * rb0 >= mrows || 8 * cb0 >= ncols) return;   // warp-uniform: none of this warp's blocks is used
     for (int k0 = 0; k0 < kb; k0 += 4) {
         const int kk = k0 + (lane & 3);
         const bool kin = kk < kb;
-        double2 af = kin && r < mrows ? As[(size_t)kk * ak + (size_t)r * ar] : czero<double2>();
-        if (NEG) af = make_double2(-af.x, -af.y);
+        double2 bf[4];
 #pragma unroll
-        for (int i = 0; i < 8; ++i) {
-            if (8 * i >= ncols) break;   // warp-uniform
-            const int c = 8 * i + g;
-            const double2 bf = kin && c < ncols ? Bs[(size_t)kk * bk + (size_t)c * bc] : czero<double2>();
-            double2 &d0 = acc.v[i][0], &d1 = acc.v[i][1];
-            dmma_884(af.x, bf.x, d0.x, d1.x);    // Re += Ar Br
-            dmma_884(-af.y, bf.y, d0.x, d1.x);   //     - Ai Bi
-            dmma_884(af.x, bf.y, d0.y, d1.y);    // Im += Ar Bi
-            dmma_884(af.y, bf.x, d0.y, d1.y);    //     + Ai Br
+        for (int ci = 0; ci < 4; ++ci) {
+            const int c = 8 * (cb0 + ci) + g;
+            bf[ci] = kin && c < ncols ? Bs[(size_t)kk * bk + (size_t)c * bc] : czero<double2>();
+        }
+#pragma unroll
+        for (int ri = 0; ri < 2; ++ri) {
+            const int rb = rb0 + 4 * ri;
+            if (8 * rb >= mrows) break;   // warp-uniform
+            const int r = 8 * rb + g;
+            double2 af = kin && r < mrows ? As[(size_t)kk * ak + (size_t)r * ar] : czero<double2>();
+            if (NEG) af = make_double2(-af.x, -af.y);
+#pragma unroll
+            for (int ci = 0; ci < 4; ++ci) {
+                if (8 * (cb0 + ci) >= ncols) break;   // warp-uniform
+                double2 &d0 = acc.v[4 * ri + ci][0], &d1 = acc.v[4 * ri + ci][1];
+                dmma_884(af.x, bf[ci].x, d0.x, d1.x);    // Re += Ar Br
+                dmma_884(-af.y, bf[ci].y, d0.x, d1.x);   //     - Ai Bi
+                dmma_884(af.x, bf[ci].y, d0.y, d1.y);    // Im += Ar Bi
+                dmma_884(af.y, bf[ci].x, d0.y, d1.y);    //     + Ai Br
+            }
         }
     }
 }
@@ -570,33 +586,82 @@ __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int 
         for (int i = k + 1 + lane; i < f; i += 32) S[i + k * ld] = cmul(S[i + k * ld], rk);
         __syncwarp();
     };
-    if (warp == 0 && s > 0) take_pivot(0);
-    __syncthreads();
-    // Each lane holds its rows of the scaled L column k in registers for the
-    // whole step (SROWS x 32 >= the level's largest front), so an entry's
-    // update reads shared memory once, not twice.
-    for (int k = 0; k < s; ++k) {
-        const int m = f - k - 1;
-        C lk[SROWS];
-#pragma unroll
-        for (int q = 0; q < SROWS; ++q) {
-            const int ii = lane + 32 * q;
-            lk[q] = ii < m ? S[k + 1 + ii + k * ld] : czero<C>();
+    if constexpr (sizeof(R) == 8) {
+        // complex128: blocked by 4-pivot panels.  Warp 0 factors a panel's
+        // columns (static pivoting, L columns scaled) and applies each pivot
+        // to the panel rows right of the panel (the U rows); then every warp
+        // applies the rank-4 update to the trailing block on FP64 matrix
+        // instructions, one 8 x 8 block per warp at a time.  Two barriers per
+        // panel instead of one per pivot.
+        constexpr int PW = 4;
+        const int g = lane >> 2, kq = lane & 3;
+        for (int kb0 = 0; kb0 < s; kb0 += PW) {
+            const int kend = min(s, kb0 + PW);
+            if (warp == 0) {
+                for (int k = kb0; k < kend; ++k) {
+                    take_pivot(k);
+                    for (int j = k + 1; j < kend; ++j) {   // panel columns, rows below k
+                        const C u = S[k + j * ld];
+                        for (int i = k + 1 + lane; i < f; i += 32) cfms(S[i + j * ld], S[i + k * ld], u);
+                    }
+                    for (int j = kend + lane; j < f; j += 32) {   // panel rows, columns right of the panel
+                        const C u = S[k + j * ld];
+                        for (int i = k + 1; i < kend; ++i) cfms(S[i + j * ld], S[i + k * ld], u);
+                    }
+                    __syncwarp();
+                }
+            }
+            __syncthreads();
+            const int mt = f - kend, nbt = (mt + 7) / 8;
+            for (int bi = warp; bi < nbt * nbt; bi += nw) {   // trailing block -= L(:, panel) U(panel, :)
+                const int r = kend + 8 * (bi % nbt) + g, c0 = kend + 8 * (bi / nbt);
+                const int cl = c0 + 2 * kq;
+                double2 d0 = r < f && cl < f ? S[r + cl * ld] : czero<C>();
+                double2 d1 = r < f && cl + 1 < f ? S[r + (cl + 1) * ld] : czero<C>();
+                const int kk = kb0 + kq;
+                const bool kin = kk < kend;
+                double2 af = kin && r < f ? S[r + kk * ld] : czero<C>();
+                af = make_double2(-af.x, -af.y);
+                const int cb = c0 + g;
+                const double2 bf = kin && cb < f ? S[kk + cb * ld] : czero<C>();
+                dmma_884(af.x, bf.x, d0.x, d1.x);
+                dmma_884(-af.y, bf.y, d0.x, d1.x);
+                dmma_884(af.x, bf.y, d0.y, d1.y);
+                dmma_884(af.y, bf.x, d0.y, d1.y);
+                if (r < f && cl < f) S[r + cl * ld] = d0;
+                if (r < f && cl + 1 < f) S[r + (cl + 1) * ld] = d1;
+            }
+            __syncthreads();
         }
-        for (int jj = warp; jj < m; jj += nw) {
-            C *col = S + (k + 1 + jj) * ld;
-            const C u = col[k];
+    } else {
+        if (warp == 0 && s > 0) take_pivot(0);
+        __syncthreads();
+        // Each lane holds its rows of the scaled L column k in registers for the
+        // whole step (SROWS x 32 >= the level's largest front), so an entry's
+        // update reads shared memory once, not twice.
+        for (int k = 0; k < s; ++k) {
+            const int m = f - k - 1;
+            C lk[SROWS];
 #pragma unroll
             for (int q = 0; q < SROWS; ++q) {
                 const int ii = lane + 32 * q;
-                if (ii < m) cfms(col[k + 1 + ii], lk[q], u);
+                lk[q] = ii < m ? S[k + 1 + ii + k * ld] : czero<C>();
             }
-            if (jj == 0 && k + 1 < s) {   // warp 0 just finished column k + 1
-                __syncwarp();
-                take_pivot(k + 1);
+            for (int jj = warp; jj < m; jj += nw) {
+                C *col = S + (k + 1 + jj) * ld;
+                const C u = col[k];
+#pragma unroll
+                for (int q = 0; q < SROWS; ++q) {
+                    const int ii = lane + 32 * q;
+                    if (ii < m) cfms(col[k + 1 + ii], lk[q], u);
+                }
+                if (jj == 0 && k + 1 < s) {   // warp 0 just finished column k + 1
+                    __syncwarp();
+                    take_pivot(k + 1);
+                }
             }
+            __syncthreads();
         }
-        __syncthreads();
     }
 
     // inverses of the NB x NB diagonal blocks: L^-1 strictly below the
