@@ -274,7 +274,10 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- GPU arm
-def time_steps(torch, e, step, steps: int, warmup: int, dist=None):
+def time_steps(torch, e, step, steps: int, warmup: int, dist=None, tag: str = "timed"):
+    """Device time per step over `steps` steps after `warmup` untimed ones;
+    the timed steps sit in an NVTX range named `tag` (profilers can select
+    them, e.g. ncu --nvtx --nvtx-include "timed_fp64/")."""
     for _ in range(warmup):
         step()
     stream = torch.cuda.ExternalStream(e.stream())
@@ -283,11 +286,13 @@ def time_steps(torch, e, step, steps: int, warmup: int, dist=None):
     if dist is not None:
         dist.barrier()
     l0 = e.stats()["kernel_launches"]
+    torch.cuda.nvtx.range_push(tag)
     ev0.record(stream)
     for _ in range(steps):
         step()
     ev1.record(stream)
     torch.cuda.synchronize()
+    torch.cuda.nvtx.range_pop()
     if dist is not None:
         dist.barrier()
     ms = ev0.elapsed_time(ev1) / steps
@@ -387,7 +392,7 @@ def run_gpu(args):
 
         clocks = ClockSampler(local)
         clocks.start()
-        ms, launches = time_steps(torch, e, step_dev, args.steps, args.warmup, dist)
+        ms, launches = time_steps(torch, e, step_dev, args.steps, args.warmup, dist, tag=f"timed_{name}")
         ck = clocks.stop()
         st = e.stats()
         r = {"ms": ms, "launches": launches, "stats": st, "clocks": ck, "tuned": tuned}
@@ -397,7 +402,7 @@ def run_gpu(args):
             e.factor(freqs)
             e.forward(xs, ys, rx, ry, seis_out=seis_h)
             check_converged("end-to-end")
-        ms_e2e, _ = time_steps(torch, e, step_e2e, max(1, args.steps // 2), 1, dist)
+        ms_e2e, _ = time_steps(torch, e, step_e2e, max(1, args.steps // 2), 1, dist, tag=f"e2e_{name}")
         r["ms_e2e"] = ms_e2e
         # per-frequency refinement record of the last step and, outside the
         # timed region, the FP64 forward wavefields for the error table

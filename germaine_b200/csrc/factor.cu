@@ -47,17 +47,17 @@ constexpr int TSTR = TILE + 2;   // padded row stride of staged 64-wide tiles (c
 // (so a tile with few rows still keeps six of the eight warps busy), lane l
 // row 8 rb + l / 4 and columns 8 cb + 2 (l % 4) + j of each owned block;
 // v[4 rbi + cbi][j] for row block w % 4 + 4 rbi, column block 4 (w / 4) + cbi.
-template <class C>
+template <class C, bool MMA>
 struct Tile64;
-template <>
-struct Tile64<float2> {
+template <class C>
+struct Tile64<C, false> {   // CUDA-core FMAs (complex64, or complex128 where short K suits them better)
     static constexpr int NI = 4, NJ = 4;
-    float2 v[NI][NJ];
+    C v[NI][NJ];
     __device__ __forceinline__ static int row(int i, int, int t) { return t % 16 + 16 * i; }
     __device__ __forceinline__ static int col(int, int j, int t) { return t / 16 + 16 * j; }
 };
 template <>
-struct Tile64<double2> {
+struct Tile64<double2, true> {   // FP64 matrix instructions
     static constexpr int NI = 8, NJ = 2;
     double2 v[NI][NJ];
     __device__ __forceinline__ static int row(int i, int, int t) {
@@ -69,29 +69,30 @@ struct Tile64<double2> {
 };
 
 // f(row, col, value) over the thread's entries of the tile
-template <class C, class F>
-__device__ __forceinline__ void for_tile64(Tile64<C> &acc, int t, F f) {
+template <class C, bool MMA, class F>
+__device__ __forceinline__ void for_tile64(Tile64<C, MMA> &acc, int t, F f) {
+    using T = Tile64<C, MMA>;
 #pragma unroll
-    for (int i = 0; i < Tile64<C>::NI; ++i)
+    for (int i = 0; i < T::NI; ++i)
 #pragma unroll
-        for (int j = 0; j < Tile64<C>::NJ; ++j) f(Tile64<C>::row(i, j, t), Tile64<C>::col(i, j, t), acc.v[i][j]);
+        for (int j = 0; j < T::NJ; ++j) f(T::row(i, j, t), T::col(i, j, t), acc.v[i][j]);
 }
 
 // acc += A B (NEG: acc -= A B) over k < kb, A(r, k) = As[k * ak + r * ar]
 // for rows r < mrows, B(k, c) = Bs[k * bk + c * bc] for columns c < ncols
 // (entries outside read as zero)
-template <bool NEG>
-__device__ __forceinline__ void mma64(const float2 *As, int ak, int ar, const float2 *Bs, int bk, int bc, int kb,
-                                      int mrows, int ncols, Tile64<float2> &acc, int t) {
+template <bool NEG, class C>
+__device__ __forceinline__ void mma64(const C *As, int ak, int ar, const C *Bs, int bk, int bc, int kb, int mrows,
+                                      int ncols, Tile64<C, false> &acc, int t) {
     const int tx = t % 16, ty = t / 16;
     for (int k = 0; k < kb; ++k) {
-        float2 lv[4], uv[4];
+        C lv[4], uv[4];
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-            lv[i] = tx + 16 * i < mrows ? As[(size_t)k * ak + (size_t)(tx + 16 * i) * ar] : czero<float2>();
+            lv[i] = tx + 16 * i < mrows ? As[(size_t)k * ak + (size_t)(tx + 16 * i) * ar] : czero<C>();
 #pragma unroll
         for (int j = 0; j < 4; ++j)
-            uv[j] = ty + 16 * j < ncols ? Bs[(size_t)k * bk + (size_t)(ty + 16 * j) * bc] : czero<float2>();
+            uv[j] = ty + 16 * j < ncols ? Bs[(size_t)k * bk + (size_t)(ty + 16 * j) * bc] : czero<C>();
 #pragma unroll
         for (int i = 0; i < 4; ++i)
 #pragma unroll
@@ -110,7 +111,7 @@ __device__ __forceinline__ void dmma_884(double a, double b, double &d0, double 
 
 template <bool NEG>
 __device__ __forceinline__ void mma64(const double2 *As, int ak, int ar, const double2 *Bs, int bk, int bc, int kb,
-                                      int mrows, int ncols, Tile64<double2> &acc, int t) {
+                                      int mrows, int ncols, Tile64<double2, true> &acc, int t) {
     const int w = t >> 5, lane = t & 31, g = lane >> 2;
     const int rb0 = w % 4, cb0 = 4 * (w / 4);
     if (8 * rb0 >= mrows || 8 * cb0 >= ncols) return;   // warp-uniform: none of this warp's blocks is used
@@ -372,7 +373,7 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
         if (cc < kb && c0 + col < f) cp_async_elem(Us + cc * TSTR + col, F + (k0 + cc) + (size_t)(c0 + col) * f);
     }
     staged_sync();
-    Tile64<C> acc;
+    Tile64<C, sizeof(R) == 8> acc;
     for_tile64(acc, threadIdx.x, [](int, int, C &v) { v = czero<C>(); });
     mma64<false>(Ls, TSTR, 1, Us, TSTR, 1, kb, min(TILE, f - r0), min(TILE, f - c0), acc, threadIdx.x);
     for_tile64(acc, threadIdx.x, [&](int rr, int cc, C &v) {
@@ -415,7 +416,7 @@ __global__ void __launch_bounds__(256) k_gemm_sub_cc(const GemmProb<R> *__restri
         }
         asm volatile("cp.async.commit_group;\n" ::: "memory");
     };
-    Tile64<C> acc;
+    Tile64<C, sizeof(R) == 8> acc;
     for_tile64(acc, threadIdx.x, [](int, int, C &v) { v = czero<C>(); });
     const int mrows = min(TILE, p.m - r0), ncols = min(TILE, p.n - c0);
     const int nk = (p.k + GKC - 1) / GKC;
@@ -511,7 +512,7 @@ template void launch_factor_level<float>(const FactorArgs<float> &, const LevelI
 // ---------------------------------------------------------------------
 constexpr int SMALL_FT = 256;   // threads per CTA
 
-template <class R, int SROWS>
+template <class R, int SROWS, bool BLOCKED>
 __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int lvl_first, int ld) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -586,8 +587,8 @@ __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int 
         for (int i = k + 1 + lane; i < f; i += 32) S[i + k * ld] = cmul(S[i + k * ld], rk);
         __syncwarp();
     };
-    if constexpr (sizeof(R) == 8) {
-        // complex128: blocked by 4-pivot panels.  Warp 0 factors a panel's
+    if constexpr (BLOCKED) {
+        // complex128, fronts with many pivots: blocked by 4-pivot panels.  Warp 0 factors a panel's
         // columns (static pivoting, L columns scaled) and applies each pivot
         // to the panel rows right of the panel (the U rows); then every warp
         // applies the rank-4 update to the trailing block on FP64 matrix
@@ -715,17 +716,24 @@ template <class R>
 void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaFuncSetAttribute(k_factor_small<R, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
-        cudaFuncSetAttribute(k_factor_small<R, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
-        cudaFuncSetAttribute(k_factor_small<R, 4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
+        cudaFuncSetAttribute(k_factor_small<R, 2, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
+        cudaFuncSetAttribute(k_factor_small<R, 3, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
+        cudaFuncSetAttribute(k_factor_small<R, 4, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMALL_FACTOR_SMEM);
+        if (sizeof(R) == 8)
+            cudaFuncSetAttribute(k_factor_small<R, 2, sizeof(R) == 8>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)SMALL_FACTOR_SMEM);
         attr_set = true;
     }
     const size_t smem = small_factor_smem<R>(L.max_front);
     const dim3 grid(L.count, a.nf);
     const int ld = L.max_front + 1;
-    if (L.max_front <= 64) (k_factor_small<R, 2><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
-    else if (L.max_front <= 96) (k_factor_small<R, 3><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
-    else (k_factor_small<R, 4><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
+    // the blocked complex128 LU pays on fronts with many pivots (the leaf
+    // level: 5.4 -> 4.6 ms); with 7-13 pivots its one-warp panels are slower
+    if (sizeof(R) == 8 && L.max_piv >= 16)
+        (k_factor_small<R, 2, sizeof(R) == 8><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
+    else if (L.max_front <= 64) (k_factor_small<R, 2, false><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
+    else if (L.max_front <= 96) (k_factor_small<R, 3, false><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
+    else (k_factor_small<R, 4, false><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
 }
 
 template bool small_factor_level<double>(const LevelInfo &);
@@ -928,7 +936,7 @@ __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_
     // values loaded into the accumulators first
     for (int i0 = 0; i0 < m; i0 += 64)
         for (int j0 = 0; j0 < m; j0 += 64) {
-            Tile64<C> acc;
+            Tile64<C, (sizeof(R) == 8 && NPR > 16)> acc;   // short K (<= 16 pivots): CUDA-core FMAs
             for_tile64(acc, tid, [&](int rr, int cc, C &v) {
                 const int i = i0 + rr, j = j0 + cc;
                 v = (i < m && j < m) ? F[s + i + (size_t)(s + j) * f] : czero<C>();
