@@ -574,7 +574,8 @@ namespace gm {
 // entries) restricts it to those matrices of the batch (NULL: all).
 template <class R>
 static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsigned char *mask = nullptr,
-                       const int *fmap = nullptr, int nfz = 0, const int *xmap = nullptr) {
+                       const int *fmap = nullptr, int nfz = 0, const int *xmap = nullptr,
+                       const SpikeRhs *spikes = nullptr) {
     cudaEventRecord(e->ev_s0, e->st);
     SolveArgs<R> a{};
     a.s = e->dsym;
@@ -598,6 +599,10 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsign
     a.trans = trans;
     a.mask = mask;
     a.mask_nch = (nrhs + 31) / 32;
+    if (spikes && mask) {   // implicit right-hand sides: x not cleared beforehand
+        a.spike_k = spikes->k;
+        a.spike_amp = spikes->amp;
+    }
     // GM_TRACE_LEVELS=1: device time of every level of both passes on stderr
     static const bool trace = std::getenv("GM_TRACE_LEVELS") != nullptr;
     const int nl = (int)e->levels.size();
@@ -993,10 +998,13 @@ int engine_solve_device(gm_engine *e, int sys, int nrhs, double2 *d_x, const dou
     // into it), in complex64 in the work buffer and then added into x = 0
     const unsigned char *mask = build_mask(e, nrhs, pattern);
     const bool implicit = !d_b;
-    if (implicit) launch_spikes(d_x, e->n, e->nf, nrhs, spikes->k, spikes->amp, e->st);   // x = b
+    // FP64 with implicit spikes and a pruning mask: x is not cleared, the
+    // passes take b from the spike list (pruned fronts: y = 0)
+    const bool lazy_b = implicit && fp64 && mask;
+    if (implicit && !lazy_b) launch_spikes(d_x, e->n, e->nf, nrhs, spikes->k, spikes->amp, e->st);   // x = b
     if (fp64) {
         if (!implicit) GM_CUDA(cudaMemcpyAsync(d_x, d_b, cnt * sizeof(double2), cudaMemcpyDeviceToDevice, e->st));
-        substitute<double>(e, d_x, nrhs, sys, mask);
+        substitute<double>(e, d_x, nrhs, sys, mask, nullptr, 0, nullptr, lazy_b ? spikes : nullptr);
     } else {
         launch_convert_down<float>(implicit ? d_x : d_b, e->d_t.p, cnt, e->st);
         GM_CUDA(cudaMemsetAsync(d_x, 0, cnt * sizeof(double2), e->st));

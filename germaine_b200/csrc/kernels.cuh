@@ -151,6 +151,13 @@ struct SolveArgs {
     // host: per level {forward rt, forward B, backward rt, backward B} chosen
     // by the autotuner (gm_autotune; 0 entries keep the default rule), or NULL
     const int *lvl_cfg;
+    // implicit spike right-hand sides (with a pruning mask only; NULL: x
+    // holds b on entry): column r is spike_amp[matrix] on row spike_k[r] and
+    // zero elsewhere.  x is not cleared beforehand: the forward pass writes
+    // b + the children's updates at the pivot rows of every live front, and
+    // the backward pass takes y = 0 at the pivot rows of pruned fronts.
+    const int *spike_k;
+    const double2 *spike_amp;
 };
 
 // right-hand sides per substitution slice for nrhs right-hand sides

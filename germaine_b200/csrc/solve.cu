@@ -297,6 +297,12 @@ __device__ __forceinline__ bool live(const SolveArgs<R> &a, int v, int r0, int r
     return false;
 }
 
+// false when right-hand side `col` is zero throughout node v's subtree
+template <class R>
+__device__ __forceinline__ bool col_live(const SolveArgs<R> &a, int v, int col) {
+    return !a.mask || a.mask[(size_t)v * a.mask_nch + (col >> 5)];
+}
+
 // matrix handled by this CTA: blockIdx.z indexes the launch's matrix list
 template <class R>
 __device__ __forceinline__ size_t solve_matrix(const SolveArgs<R> &a) {
@@ -335,6 +341,33 @@ __device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first,
     return c;
 }
 
+// The pivot rows of this front's slice of x receive the children's update
+// vectors (W0, W1: NULL for a child that is absent or pruned); with implicit
+// spike right-hand sides they become b + the updates, x not being read
+// (it is not cleared before the solve).
+template <class R>
+__device__ __forceinline__ void pivot_rhs(const SolveArgs<R> &a, const Ctx<R> &c, const int *inv, const cplx<R> *W0,
+                                          const cplx<R> *W1, int r0, size_t ldr) {
+    using C = cplx<R>;
+    const bool implicit = a.spike_k != nullptr;
+    if (!(W0 || W1 || implicit)) return;   // CTA-uniform
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const C amp = implicit ? cconv<C>(a.spike_amp[solve_matrix(a)]) : czero<C>();
+    for (int i = warp; i < c.s; i += NT / 32) {
+        const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
+        if (!implicit && q0 < 0 && q1 < 0) continue;
+        const int row = c.vars[i];
+        for (int r = lane; r < c.rn; r += 32) {
+            C v = czero<C>();
+            if (q0 >= 0) v = cadd(v, W0[(size_t)q0 * ldr + r]);
+            if (q1 >= 0) v = cadd(v, W1[(size_t)q1 * ldr + r]);
+            C &x = c.X[(size_t)row * ldr + r];
+            x = implicit ? (a.spike_k[r0 + r] == row ? cadd(amp, v) : v) : cadd(x, v);
+        }
+    }
+    __syncthreads();
+}
+
 // Forward pass, pivot part: add the children's update vectors (gathered by
 // the extend-add inverse maps) into x at this front's pivots, then solve the
 // pivot rows in place in x, 32-pivot block by block.
@@ -349,7 +382,6 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
     const int r0 = blockIdx.x * TC;
     if (!live(a, c.node, r0, c.rn)) return;   // y and the update vector are zero
     (void)fused;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int *inv = a.s.inv + a.s.inv_off[c.node];
     const size_t xz = solve_slot(a);
     const C *Wall = reinterpret_cast<const C *>(a.w) + xz * (size_t)a.s.rhs_total * a.ldr + r0;
@@ -358,20 +390,7 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
     const C *W1 = c1 >= 0 && live(a, c1, r0, c.rn) ? Wall + (size_t)a.s.rhs_off[c1] * a.ldr : nullptr;
     const size_t ldr = a.ldr;
 
-    if (W0 || W1) {   // children's update vectors at the pivots (the ring part is k_fwd_ring's)
-        for (int i = warp; i < c.s; i += NT / 32) {
-            const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
-            if (q0 < 0 && q1 < 0) continue;
-            for (int r = lane; r < c.rn; r += 32) {
-                C v = czero<C>();
-                if (q0 >= 0) v = cadd(v, W0[(size_t)q0 * ldr + r]);
-                if (q1 >= 0) v = cadd(v, W1[(size_t)q1 * ldr + r]);
-                C &x = c.X[(size_t)c.vars[i] * ldr + r];
-                x = cadd(x, v);
-            }
-        }
-        __syncthreads();
-    }
+    pivot_rhs(a, c, inv, W0, W1, r0, ldr);   // (the ring part is k_fwd_ring's)
 
     auto xrow = [&](int k) { return c.X + (size_t)c.vars[k] * ldr; };
     TileAcc<C, RT, B> acc;
@@ -467,7 +486,13 @@ __global__ void __launch_bounds__(NT) k_bwd_ring(SolveArgs<R> a, int lvl_first, 
         tile_mma(sm, jb, acc, rows, c.rn);
         __syncthreads();
     }
-    sub_acc([&](int row) { return c.X + (size_t)c.vars[i0 + row] * ldr; }, rows, c.rn, acc);
+    // y = 0 at the pivot rows in the right-hand sides the pruned forward
+    // pass skipped for this front (x is not cleared there when the
+    // right-hand sides are implicit spikes)
+    for_acc(acc, rows, c.rn, threadIdx.x, [&](int row, int col, const C &v) {
+        C &x = c.X[(size_t)c.vars[i0 + row] * ldr + col];
+        x = csub(a.spike_k && !col_live(a, c.node, chunk * TC + col) ? czero<C>() : x, v);
+    });
 }
 
 // Backward pass, pivot part: block by block from the last, x_b = Dinv t_b in
@@ -483,6 +508,15 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
     (void)fused;
     const size_t ldr = a.ldr;
     auto xrow = [&](int k) { return c.X + (size_t)c.vars[k] * ldr; };
+    if (c.f == c.s && a.spike_k) {
+        // no ring (k_bwd_ring did not set y): y = 0 at the pivot rows in the
+        // right-hand sides the pruned forward pass skipped for this front
+        for (int t = threadIdx.x; t < c.s * TC; t += NT) {
+            const int q = t / TC, r = t % TC;
+            if (r < c.rn && !col_live(a, c.node, blockIdx.x * TC + r)) xrow(q)[r] = czero<C>();
+        }
+        __syncthreads();
+    }
     TileAcc<C, RT, B> acc;
     const int nblk = (c.s + SNB - 1) / SNB;
     for (int b = nblk - 1; b >= 0; --b) {
@@ -535,7 +569,6 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_fwd_small(SolveA
     if (c.rn <= 0) return;
     const int r0 = wk.y * TC;
     if (!live(a, c.node, r0, c.rn)) return;   // y and the update vector are zero
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
     const int *inv = a.s.inv + a.s.inv_off[c.node];
     const size_t xz = solve_slot(a);
     const C *Wall = reinterpret_cast<const C *>(a.w) + xz * (size_t)a.s.rhs_total * a.ldr + r0;
@@ -545,20 +578,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_fwd_small(SolveA
     const size_t ldr = a.ldr;
     const int s = c.s;   // <= SNB (launch condition)
 
-    if (W0 || W1) {   // children's update vectors at the pivots
-        for (int i = warp; i < s; i += NT / 32) {
-            const int q0 = W0 ? inv[i] : -1, q1 = W1 ? inv[c.f + i] : -1;
-            if (q0 < 0 && q1 < 0) continue;
-            for (int r = lane; r < c.rn; r += 32) {
-                C v = czero<C>();
-                if (q0 >= 0) v = cadd(v, W0[(size_t)q0 * ldr + r]);
-                if (q1 >= 0) v = cadd(v, W1[(size_t)q1 * ldr + r]);
-                C &x = c.X[(size_t)c.vars[i] * ldr + r];
-                x = cadd(x, v);
-            }
-        }
-        __syncthreads();
-    }
+    pivot_rhs(a, c, inv, W0, W1, r0, ldr);
     TileAcc<C, RT, B> acc;
     if (s > 0) {
         stage_dinv<C, true, TRANS, RT, B>(sm, c.F, c.f, 0, s);
@@ -619,8 +639,19 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_bwd_small(SolveA
         tile_mma(sm, jb, acc, s, c.rn);
         __syncthreads();
     }
-    // t = y - acc in sm.Y (row q of the next product's right operand = pivot q)
-    stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q] * ldr; }, s, c.rn);
+    // t = y - acc in sm.Y (row q of the next product's right operand = pivot
+    // q); y = 0 where the pruned forward pass skipped the front (its rows of
+    // x are not cleared when the right-hand sides are implicit spikes)
+    if (a.spike_k) {   // y = 0 in the right-hand sides the pruned forward pass skipped
+        for (int t = threadIdx.x; t < s * TC; t += NT) {
+            const int q = t / TC, r = t % TC;
+            if (r >= c.rn) continue;
+            if (col_live(a, c.node, blockIdx.x * TC + r)) cp_async_elem(&sm.Y[q][r], c.X + (size_t)c.vars[q] * ldr + r);
+            else sm.Y[q][r] = czero<C>();
+        }
+    } else {
+        stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q] * ldr; }, s, c.rn);
+    }
     stage_dinv<C, false, TRANS, RT, B>(sm, c.F, c.f, 0, s);
     staged_sync();
     for_acc(acc, s, c.rn, threadIdx.x, [&](int row, int col, const C &v) { sm.Y[row][col] = csub(sm.Y[row][col], v); });
