@@ -186,6 +186,26 @@ __global__ void k_entry_scatter(FactorArgs<R> a, int64_t e0, int64_t cnt) {
     d = cadd(d, cconv<C>(v));
 }
 
+// Static pivoting: a pivot of magnitude below pivtol (or NaN) is replaced by
+// itself scaled to magnitude pivtol (pivtol when it is zero) and counted.
+// The test compares squares, so the common case takes no square root.
+template <class R>
+__device__ __forceinline__ cplx<R> static_pivot(cplx<R> piv, R pivtol, int &npert) {
+    const R m2 = cabs2(piv), tol2 = pivtol * pivtol;
+    const bool small = tol2 > R(0) ? !(m2 >= tol2) : !(sqrt(m2) >= pivtol);   // also catches NaN
+    if (small) {
+        const R mag = sqrt(m2);
+        if (mag > R(0)) {
+            const R sc = pivtol / mag;
+            piv = mk(piv.x * sc, piv.y * sc);
+        } else {
+            piv = mk(pivtol, R(0));
+        }
+        ++npert;
+    }
+    return piv;
+}
+
 // Factor the kb x kb diagonal block D (shared memory, column stride NB+1)
 // in place: unit-lower L and upper U, static pivoting.  Returns (through
 // shared memory) the reciprocals of the pivots.
@@ -195,18 +215,8 @@ __device__ void diag_lu(cplx<R> (*D)[NB + 1], cplx<R> *rdiag, int kb, R pivtol, 
     const int tid = threadIdx.x, nt = blockDim.x;
     for (int p = 0; p < kb; ++p) {
         if (tid == 0) {
-            C piv = D[p][p];
-            const R mag = sqrt(cabs2(piv));
-            if (!(mag >= pivtol)) {   // also catches NaN
-                if (mag > R(0)) {
-                    const R sc = pivtol / mag;
-                    piv = mk(piv.x * sc, piv.y * sc);
-                } else {
-                    piv = mk(pivtol, R(0));
-                }
-                D[p][p] = piv;
-                ++*nperturbed;
-            }
+            const C piv = static_pivot<R>(D[p][p], pivtol, *nperturbed);
+            D[p][p] = piv;
             rdiag[p] = crcp(piv);
         }
         __syncthreads();
@@ -568,18 +578,8 @@ __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int 
     const R pivtol = (R)(a.pivscale * __longlong_as_double((long long)*a.amax));
     auto take_pivot = [&](int k) {   // warp 0 only: pivot k, reciprocal, L column k scaled
         if (lane == 0) {
-            C piv = S[k + k * ld];
-            const R mag = sqrt(cabs2(piv));
-            if (!(mag >= pivtol)) {   // also catches NaN
-                if (mag > R(0)) {
-                    const R sc = pivtol / mag;
-                    piv = mk(piv.x * sc, piv.y * sc);
-                } else {
-                    piv = mk(pivtol, R(0));
-                }
-                S[k + k * ld] = piv;
-                ++npert;
-            }
+            const C piv = static_pivot<R>(S[k + k * ld], pivtol, npert);
+            S[k + k * ld] = piv;
             rd[k] = crcp(piv);
         }
         __syncwarp();
@@ -799,21 +799,6 @@ namespace gm {
 // accesses).
 // ---------------------------------------------------------------------
 constexpr int MID_FT = 256;   // threads per CTA, also the largest front handled
-
-template <class R>
-__device__ __forceinline__ cplx<R> static_pivot(cplx<R> piv, R pivtol, int &npert) {
-    const R mag = sqrt(cabs2(piv));
-    if (!(mag >= pivtol)) {   // also catches NaN
-        if (mag > R(0)) {
-            const R sc = pivtol / mag;
-            piv = mk(piv.x * sc, piv.y * sc);
-        } else {
-            piv = mk(pivtol, R(0));
-        }
-        ++npert;
-    }
-    return piv;
-}
 
 template <class R, int NPR>
 __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_first) {
