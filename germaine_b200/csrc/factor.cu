@@ -208,28 +208,34 @@ __device__ __forceinline__ cplx<R> static_pivot(cplx<R> piv, R pivtol, int &nper
 
 // Factor the kb x kb diagonal block D (shared memory, column stride NB+1)
 // in place: unit-lower L and upper U, static pivoting.  Returns (through
-// shared memory) the reciprocals of the pivots.
+// shared memory) the reciprocals of the pivots.  Warp 0 alone, lane r
+// owning row r: per pivot every lane evaluates the (same) static pivot and
+// its reciprocal, rows below it scale their entry of the pivot column and
+// update the rest of their row with the pivot row -- warp-synchronous, so
+// no block barrier per pivot; one block barrier at the end.
 template <class R>
 __device__ void diag_lu(cplx<R> (*D)[NB + 1], cplx<R> *rdiag, int kb, R pivtol, int *nperturbed) {
     using C = cplx<R>;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int p = 0; p < kb; ++p) {
-        if (tid == 0) {
-            const C piv = static_pivot<R>(D[p][p], pivtol, *nperturbed);
-            D[p][p] = piv;
-            rdiag[p] = crcp(piv);
+    if (threadIdx.x < 32) {
+        const int r = threadIdx.x;
+        int np = 0;
+        for (int p = 0; p < kb; ++p) {
+            const C piv = static_pivot<R>(D[p][p], pivtol, np);
+            const C rp = crcp(piv);
+            __syncwarp();   // every lane has read D[p][p]
+            if (r == p) {
+                D[p][p] = piv;
+                rdiag[p] = rp;
+            } else if (r > p && r < kb) {
+                const C l = cmul(D[r][p], rp);
+                D[r][p] = l;
+                for (int c = p + 1; c < kb; ++c) cfms(D[r][c], l, D[p][c]);
+            }
+            __syncwarp();
         }
-        __syncthreads();
-        const C rp = rdiag[p];
-        for (int r = p + 1 + tid; r < kb; r += nt) D[r][p] = cmul(D[r][p], rp);
-        __syncthreads();
-        const int m = kb - p - 1;
-        for (int t = tid; t < m * m; t += nt) {
-            const int r = p + 1 + t % m, c = p + 1 + t / m;
-            cfms(D[r][c], D[r][p], D[p][c]);
-        }
-        __syncthreads();
+        if (r == 0 && np) *nperturbed += np;   // every lane counted the same perturbations
     }
+    __syncthreads();
 }
 
 template <class R>
@@ -270,11 +276,11 @@ __global__ void __launch_bounds__(PCHUNK) k_panel(FactorArgs<R> a, int lvl_first
             for (int c = 0; c < NB; ++c) x[c] = c < kb ? F[i + (size_t)(k0 + c) * f] : czero<C>();
 #pragma unroll
             for (int c = 0; c < NB; ++c) {
-                if (c < kb) {
-                    C acc = x[c];
+                if (c < kb) {   // two accumulation chains: half the dependent latency
+                    C acc0 = x[c], acc1 = czero<C>();
 #pragma unroll
-                    for (int l = 0; l < c; ++l) cfms(acc, x[l], D[l][c]);
-                    x[c] = cmul(acc, rdiag[c]);
+                    for (int l = 0; l < c; ++l) cfms(l & 1 ? acc1 : acc0, x[l], D[l][c]);
+                    x[c] = cmul(cadd(acc0, acc1), rdiag[c]);
                 }
             }
 #pragma unroll
@@ -292,10 +298,10 @@ __global__ void __launch_bounds__(PCHUNK) k_panel(FactorArgs<R> a, int lvl_first
 #pragma unroll
             for (int r = 0; r < NB; ++r) {
                 if (r < kb) {
-                    C acc = y[r];
+                    C acc0 = y[r], acc1 = czero<C>();
 #pragma unroll
-                    for (int l = 0; l < r; ++l) cfms(acc, D[r][l], y[l]);
-                    y[r] = acc;
+                    for (int l = 0; l < r; ++l) cfms(l & 1 ? acc1 : acc0, D[r][l], y[l]);
+                    y[r] = cadd(acc0, acc1);
                 }
             }
 #pragma unroll
