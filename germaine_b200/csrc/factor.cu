@@ -208,34 +208,30 @@ __device__ __forceinline__ cplx<R> static_pivot(cplx<R> piv, R pivtol, int &nper
 
 // Factor the kb x kb diagonal block D (shared memory, column stride NB+1)
 // in place: unit-lower L and upper U, static pivoting.  Returns (through
-// shared memory) the reciprocals of the pivots.  Warp 0 alone, lane r
-// owning row r: per pivot every lane evaluates the (same) static pivot and
-// its reciprocal, rows below it scale their entry of the pivot column and
-// update the rest of their row with the pivot row -- warp-synchronous, so
-// no block barrier per pivot; one block barrier at the end.
+// shared memory) the reciprocals of the pivots.  (A warp-synchronous form,
+// one row per lane and no block barrier per pivot, measured slower on every
+// tiled level: the rank-1 update is then serial within a lane.)
 template <class R>
 __device__ void diag_lu(cplx<R> (*D)[NB + 1], cplx<R> *rdiag, int kb, R pivtol, int *nperturbed) {
     using C = cplx<R>;
-    if (threadIdx.x < 32) {
-        const int r = threadIdx.x;
-        int np = 0;
-        for (int p = 0; p < kb; ++p) {
-            const C piv = static_pivot<R>(D[p][p], pivtol, np);
-            const C rp = crcp(piv);
-            __syncwarp();   // every lane has read D[p][p]
-            if (r == p) {
-                D[p][p] = piv;
-                rdiag[p] = rp;
-            } else if (r > p && r < kb) {
-                const C l = cmul(D[r][p], rp);
-                D[r][p] = l;
-                for (int c = p + 1; c < kb; ++c) cfms(D[r][c], l, D[p][c]);
-            }
-            __syncwarp();
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int p = 0; p < kb; ++p) {
+        if (tid == 0) {
+            const C piv = static_pivot<R>(D[p][p], pivtol, *nperturbed);
+            D[p][p] = piv;
+            rdiag[p] = crcp(piv);
         }
-        if (r == 0 && np) *nperturbed += np;   // every lane counted the same perturbations
+        __syncthreads();
+        const C rp = rdiag[p];
+        for (int r = p + 1 + tid; r < kb; r += nt) D[r][p] = cmul(D[r][p], rp);
+        __syncthreads();
+        const int m = kb - p - 1;
+        for (int t = tid; t < m * m; t += nt) {
+            const int r = p + 1 + t % m, c = p + 1 + t / m;
+            cfms(D[r][c], D[r][p], D[p][c]);
+        }
+        __syncthreads();
     }
-    __syncthreads();
 }
 
 template <class R>
