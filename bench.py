@@ -51,7 +51,7 @@ METRIC = "shot-solves/s (factor+solve) mixed vs FP64 on B200 at resid<=1e-10; %r
 # DRAM bytes of one complex128 backward substitution pass on 4 frequencies
 # (the k_bwd_small / k_bwd_ring / k_bwd_piv launches of the FP64 engine's
 # timed step, ncu dram__bytes_read.sum + dram__bytes_write.sum, summed)
-BWD_TRAFFIC_FP64_4FREQ = 4.805e9
+BWD_TRAFFIC_FP64_4FREQ = 3.585e9
 PEAK_KIND = "measured FP64 rate, the higher of CUDA-core DFMA (gm_peak_fp64) and FP64 MMA (gm_peak_fp64_mma)"
 
 # the benchmark workload; --nx0/--ny0/--nfreq/--nshots shrink it for
