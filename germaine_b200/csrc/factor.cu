@@ -525,7 +525,7 @@ template void launch_factor_level<float>(const FactorArgs<float> &, const LevelI
 constexpr int SMALL_FT = 256;   // threads per CTA
 
 template <class R, int SROWS, bool BLOCKED>
-__global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int lvl_first, int ld) {
+__global__ void __launch_bounds__(SMALL_FT, BLOCKED ? 3 : 1) k_factor_small(FactorArgs<R> a, int lvl_first, int ld) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *S = reinterpret_cast<C *>(smem_raw);
@@ -601,17 +601,71 @@ __global__ void __launch_bounds__(SMALL_FT) k_factor_small(FactorArgs<R> a, int 
         for (int kb0 = 0; kb0 < s; kb0 += PW) {
             const int kend = min(s, kb0 + PW);
             if (warp == 0) {
-                for (int k = kb0; k < kend; ++k) {
-                    take_pivot(k);
-                    for (int j = k + 1; j < kend; ++j) {   // panel columns, rows below k
-                        const C u = S[k + j * ld];
-                        for (int i = k + 1 + lane; i < f; i += 32) cfms(S[i + j * ld], S[i + k * ld], u);
+                // the panel in registers: lane l holds rows l and l + 32
+                // (fronts of at most 64 rows) of the panel's columns; the
+                // pivot row's entries come from their owner by shuffles, so
+                // each pivot costs shuffles and FMAs, no shared-memory round
+                // trip or warp barrier
+                C pv[2][PW];
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int j = 0; j < PW; ++j) {
+                        const int i = lane + 32 * q;
+                        pv[q][j] = i < f && kb0 + j < kend ? S[i + (kb0 + j) * ld] : czero<C>();
                     }
-                    for (int j = kend + lane; j < f; j += 32) {   // panel rows, columns right of the panel
-                        const C u = S[k + j * ld];
-                        for (int i = k + 1; i < kend; ++i) cfms(S[i + j * ld], S[i + k * ld], u);
+#pragma unroll
+                for (int jk = 0; jk < PW; ++jk) {
+                    const int k = kb0 + jk;
+                    if (k >= kend) break;   // warp-uniform
+                    const int owner = k & 31;
+                    C prow[PW];   // row k of the panel
+#pragma unroll
+                    for (int j = 0; j < PW; ++j) {
+                        const C v = k >= 32 ? pv[1][j] : pv[0][j];
+                        prow[j] = make_double2(__shfl_sync(0xffffffffu, v.x, owner), __shfl_sync(0xffffffffu, v.y, owner));
                     }
-                    __syncwarp();
+                    int np = 0;
+                    const C piv = static_pivot<R>(prow[jk], pivtol, np);   // every lane: the same pivot
+                    const C rk = crcp(piv);
+                    if (lane == 0) {
+                        rd[k] = rk;
+                        npert += np;
+                    }
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        const int i = lane + 32 * q;
+                        if (i == k) pv[q][jk] = piv;   // the (perturbed) pivot
+                        if (i > k && i < f) {
+                            const C l = cmul(pv[q][jk], rk);
+                            pv[q][jk] = l;
+#pragma unroll
+                            for (int j = jk + 1; j < PW; ++j) cfms(pv[q][j], l, prow[j]);
+                        }
+                    }
+                }
+#pragma unroll
+                for (int q = 0; q < 2; ++q)
+#pragma unroll
+                    for (int j = 0; j < PW; ++j) {
+                        const int i = lane + 32 * q;
+                        if (i < f && kb0 + j < kend) S[i + (kb0 + j) * ld] = pv[q][j];
+                    }
+                __syncwarp();
+                // the panel's U rows right of the panel: unit lower solve with
+                // the panel's diagonal block, one column per lane
+                const int pw = kend - kb0;
+                for (int j = kend + lane; j < f; j += 32) {
+                    C u[PW];
+#pragma unroll
+                    for (int r = 0; r < PW; ++r) {
+                        if (r >= pw) break;
+                        C v = S[kb0 + r + j * ld];
+#pragma unroll
+                        for (int t = 0; t < r; ++t) cfms(v, S[kb0 + r + (kb0 + t) * ld], u[t]);
+                        u[r] = v;
+                        S[kb0 + r + j * ld] = v;
+                    }
                 }
             }
             __syncthreads();
@@ -731,7 +785,7 @@ void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
     const int ld = L.max_front + 1;
     // the blocked complex128 LU pays on fronts with many pivots (the leaf
     // level: 5.4 -> 4.6 ms); with 7-13 pivots its one-warp panels are slower
-    if (sizeof(R) == 8 && L.max_piv >= 16)
+    if (sizeof(R) == 8 && L.max_piv >= 16 && L.max_front <= 64)   // (the blocked panel holds 64 rows)
         (k_factor_small<R, 2, sizeof(R) == 8><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
     else if (L.max_front <= 64) (k_factor_small<R, 2, false><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
     else if (L.max_front <= 96) (k_factor_small<R, 3, false><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
