@@ -524,8 +524,12 @@ template void launch_factor_level<float>(const FactorArgs<float> &, const LevelI
 // ---------------------------------------------------------------------
 constexpr int SMALL_FT = 256;   // threads per CTA
 
+// (register bounds: three CTAs per SM for the blocked form, whose panel
+// registers would otherwise cost one; four for the per-pivot form, which the
+// smaller fronts of levels 1-2 fit in shared memory -- without a bound the
+// compiler takes 88 registers and two CTAs, and those levels run 2x slower)
 template <class R, int SROWS, bool BLOCKED>
-__global__ void __launch_bounds__(SMALL_FT, BLOCKED ? 3 : 1) k_factor_small(FactorArgs<R> a, int lvl_first, int ld) {
+__global__ void __launch_bounds__(SMALL_FT, BLOCKED ? 3 : 4) k_factor_small(FactorArgs<R> a, int lvl_first, int ld) {
     using C = cplx<R>;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     C *S = reinterpret_cast<C *>(smem_raw);
@@ -785,7 +789,13 @@ void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
     const int ld = L.max_front + 1;
     // the blocked complex128 LU pays on fronts with many pivots (the leaf
     // level: 5.4 -> 4.6 ms); with 7-13 pivots its one-warp panels are slower
-    if (sizeof(R) == 8 && L.max_piv >= 16 && L.max_front <= 64)   // (the blocked panel holds 64 rows)
+    // GM_BLOCKED_LU_MIN_PIV=<n> moves the threshold (a large n: the
+    // per-pivot kernel everywhere)
+    static const int min_piv = [] {
+        const char *v = std::getenv("GM_BLOCKED_LU_MIN_PIV");
+        return v ? std::atoi(v) : 16;
+    }();
+    if (sizeof(R) == 8 && L.max_piv >= min_piv && L.max_front <= 64)   // (the blocked panel holds 64 rows)
         (k_factor_small<R, 2, sizeof(R) == 8><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
     else if (L.max_front <= 64) (k_factor_small<R, 2, false><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
     else if (L.max_front <= 96) (k_factor_small<R, 3, false><<<grid, SMALL_FT, smem, st>>>(a, L.first, ld), note_launch());
