@@ -7,10 +7,14 @@
 //   K2 gather   -- each front pulls its children's contribution blocks
 //                  (extend-add by inverse maps: deterministic, no atomics),
 //   K2 scatter  -- adds the operator entries owned by the front,
-//   K3 panel    -- per NB-wide pivot block: LU of the diagonal block with
-//                  static pivoting (each CTA factors it redundantly in shared
-//                  memory) and the triangular solves of the L and U panels,
-//   K4 update   -- rank-NB Schur update of the trailing front, 64x64 tiles.
+//   K3 diag     -- per NB-wide pivot block: LU of the diagonal block with
+//                  static pivoting and the inverses of its two triangles,
+//                  factored once per front (the first block by k_diag, each
+//                  later one by the first CTA of the preceding K4),
+//   K3 panels   -- L21 = A21 U11^-1 and U12 = L11^-1 A12 as products with
+//                  those inverses (FP64 matrix instructions in complex128),
+//   K4 update   -- rank-NB Schur update of the pivot rows and columns still
+//                  to come, 64x64 tiles.
 // K3/K4 alternate ceil(max_piv/NB) times per level.  After the last step a
 // front holds L (unit lower) and U in its first npiv rows/columns -- except
 // that each NB x NB diagonal block holds the INVERSES of its two triangles
@@ -34,7 +38,6 @@ namespace gm {
 
 constexpr int NB = 32;       // pivot block width
 constexpr int TILE = 64;     // Schur-update tile
-constexpr int PCHUNK = 128;  // panel rows / columns per CTA
 
 constexpr int GATHER_COLS = 4;   // front columns per CTA of the extend-add gather
 constexpr int TSTR = TILE + 2;   // padded row stride of staged 64-wide tiles (conflict-free 8 x 4 fragments)
@@ -234,26 +237,20 @@ __device__ void diag_lu(cplx<R> (*D)[NB + 1], cplx<R> *rdiag, int kb, R pivtol, 
     }
 }
 
-template <class R>
-__global__ void __launch_bounds__(PCHUNK) k_panel(FactorArgs<R> a, int lvl_first, int k0) {
-    using C = cplx<R>;
-    const int node = a.s.lvl_nodes[lvl_first + blockIdx.y];
-    const int s = a.s.npiv[node];
-    if (k0 >= s) return;
-    const int f = a.s.nfront[node];
-    const int kb = min(NB, s - k0);
-    const int i0 = k0 + kb;            // first trailing index
-    const int m = f - i0;              // trailing size
-    const int nchunk = (m + PCHUNK - 1) / PCHUNK;
-    const int bx = blockIdx.x;
-    if (bx >= 2 * nchunk) return;
-    C *F = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.z * a.s.front_total + a.s.front_off[node];
+// LU of the kb x kb diagonal block at (k0, k0) of the front F (leading
+// dimension f) with static pivoting; the inverses of its two triangles are
+// written back in its place (what the panel products and the substitution
+// multiply by): L^-1 in the strict lower part (unit diagonal implied), U^-1
+// in the upper part with the diagonal.  The whole CTA (at least 64 threads)
+// takes part; sm is shared scratch of DIAG_SCRATCH complex values.
+constexpr int DIAG_SCRATCH = 2 * NB * (NB + 1) + NB;
 
-    // Every CTA factors the diagonal block redundantly from the unmodified
-    // front; the factored block is written back by k_update's last CTA, after
-    // this kernel has finished reading it.
-    __shared__ C D[NB][NB + 1];
-    __shared__ C rdiag[NB];
+template <class R>
+__device__ void factor_diag_block(const FactorArgs<R> &a, cplx<R> *F, int f, int k0, int kb, cplx<R> *sm) {
+    using C = cplx<R>;
+    auto D = reinterpret_cast<C (*)[NB + 1]>(sm);
+    auto Dinv = reinterpret_cast<C (*)[NB + 1]>(sm + NB * (NB + 1));
+    C *rdiag = sm + 2 * NB * (NB + 1);
     __shared__ int npert;
     if (threadIdx.x == 0) npert = 0;
     for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
@@ -262,49 +259,103 @@ __global__ void __launch_bounds__(PCHUNK) k_panel(FactorArgs<R> a, int lvl_first
     }
     __syncthreads();
     diag_lu<R>(D, rdiag, kb, (R)(a.pivscale * __longlong_as_double((long long)*a.amax)), &npert);
-
-    if (bx < nchunk) {
-        // L panel: row i solves x U = a  (U = upper triangle of D incl. diagonal)
-        const int i = i0 + bx * PCHUNK + threadIdx.x;
-        if (i < f) {
-            C x[NB];
-#pragma unroll
-            for (int c = 0; c < NB; ++c) x[c] = c < kb ? F[i + (size_t)(k0 + c) * f] : czero<C>();
-#pragma unroll
-            for (int c = 0; c < NB; ++c) {
-                if (c < kb) {   // two accumulation chains: half the dependent latency
-                    C acc0 = x[c], acc1 = czero<C>();
-#pragma unroll
-                    for (int l = 0; l < c; ++l) cfms(l & 1 ? acc1 : acc0, x[l], D[l][c]);
-                    x[c] = cmul(cadd(acc0, acc1), rdiag[c]);
-                }
-            }
-#pragma unroll
-            for (int c = 0; c < NB; ++c)
-                if (c < kb) F[i + (size_t)(k0 + c) * f] = x[c];
+    // thread c < kb inverts column c of L, thread 32 + c column c of U
+    const int t = threadIdx.x;
+    if (t < kb) {   // the unit diagonal of L^-1 is implied: only U^-1 owns Dinv[c][c]
+        const int c = t;
+        for (int r = c + 1; r < kb; ++r) {
+            C acc = D[r][c];
+            for (int q = c + 1; q < r; ++q) cfma(acc, D[r][q], Dinv[q][c]);
+            Dinv[r][c] = mk(-acc.x, -acc.y);
         }
-    } else if (bx < 2 * nchunk) {
-        // U panel: column j solves L y = a (unit lower triangle of D)
-        const int j = i0 + (bx - nchunk) * PCHUNK + threadIdx.x;
-        if (j < f) {
-            C y[NB];
-            C *col = F + (size_t)j * f + k0;
-#pragma unroll
-            for (int r = 0; r < NB; ++r) y[r] = r < kb ? col[r] : czero<C>();
-#pragma unroll
-            for (int r = 0; r < NB; ++r) {
-                if (r < kb) {
-                    C acc0 = y[r], acc1 = czero<C>();
-#pragma unroll
-                    for (int l = 0; l < r; ++l) cfms(l & 1 ? acc1 : acc0, D[r][l], y[l]);
-                    y[r] = cadd(acc0, acc1);
-                }
-            }
-#pragma unroll
-            for (int r = 0; r < NB; ++r)
-                if (r < kb) col[r] = y[r];
+    } else if (t >= 32 && t < 32 + kb) {
+        const int c = t - 32;
+        Dinv[c][c] = rdiag[c];
+        for (int r = c - 1; r >= 0; --r) {
+            C acc = czero<C>();
+            for (int q = r + 1; q <= c; ++q) cfma(acc, D[r][q], Dinv[q][c]);
+            Dinv[r][c] = cmul(mk(-acc.x, -acc.y), rdiag[r]);
         }
     }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kb * kb; i += blockDim.x) {
+        const int r = i % kb, c = i / kb;
+        F[(k0 + r) + (size_t)(k0 + c) * f] = Dinv[r][c];
+    }
+    if (threadIdx.x == 0 && npert) atomicAdd(a.npert, (unsigned long long)npert);
+}
+
+// K3a: the first diagonal block of every front of the level (the later
+// ones are factored by the first CTA of the preceding trailing update)
+template <class R>
+__global__ void __launch_bounds__(256) k_diag(FactorArgs<R> a, int lvl_first) {
+    using C = cplx<R>;
+    const int node = a.s.lvl_nodes[lvl_first + blockIdx.x];
+    const int s = a.s.npiv[node];
+    if (s <= 0) return;
+    const int f = a.s.nfront[node];
+    C *F = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.y * a.s.front_total + a.s.front_off[node];
+    extern __shared__ unsigned char smem_raw[];
+    factor_diag_block<R>(a, F, f, 0, min(NB, s), reinterpret_cast<C *>(smem_raw));
+}
+
+// K3b: the L and U panels of pivot block k0 as products with the inverted
+// triangles of its (already factored) diagonal block: L21 = A21 U11^-1 and
+// U12 = L11^-1 A12, one 64-row (L) or 64-column (U) slice per CTA, 256
+// threads.  Both are formed with kb rows of output (the L slice as its
+// transpose U11^-T A21^T), so all eight warps of the matrix-instruction
+// tile layout hold work.  Each CTA reads and writes only its own slice;
+// the diagonal block is read-only here.
+template <class R>
+__global__ void __launch_bounds__(256) k_panel_mm(FactorArgs<R> a, int lvl_first, int k0, int ntmax) {
+    using C = cplx<R>;
+    const int node = a.s.lvl_nodes[lvl_first + blockIdx.y];
+    const int s = a.s.npiv[node];
+    if (k0 >= s) return;
+    const int f = a.s.nfront[node];
+    const int kb = min(NB, s - k0);
+    const int i0 = k0 + kb;
+    const bool upper = blockIdx.x >= (unsigned)ntmax;
+    const int x0 = i0 + (upper ? blockIdx.x - ntmax : blockIdx.x) * TILE;   // first row (L) / column (U)
+    if (x0 >= f) return;
+    const int nx = min(TILE, f - x0);
+    C *F = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.z * a.s.front_total + a.s.front_off[node];
+
+    extern __shared__ unsigned char smem_raw[];
+    C *Is = reinterpret_cast<C *>(smem_raw);   // [NB][TSTR]: Is[k * TSTR + r] = triangle-inverse factor (r, k)
+    C *Ps = Is + NB * TSTR;                    // [NB][TSTR]: Ps[k * TSTR + x] = panel entry (k, x)
+    const C *Dg = F + k0 + (size_t)k0 * f;    // the inverted diagonal block
+    for (int t = threadIdx.x; t < NB * NB; t += blockDim.x) {
+        const int r = t % NB, k = t / NB;      // Is(r, k): U^-T (r, k) = U^-1 (k, r), or L^-1 (r, k)
+        if (r < kb && k < kb) {
+            if (upper) {
+                if (k < r) cp_async_elem(Is + k * TSTR + r, Dg + r + (size_t)k * f);
+                else Is[k * TSTR + r] = k == r ? mk(R(1), R(0)) : czero<C>();
+            } else {
+                if (k <= r) cp_async_elem(Is + k * TSTR + r, Dg + k + (size_t)r * f);
+                else Is[k * TSTR + r] = czero<C>();
+            }
+        }
+    }
+    for (int t = threadIdx.x; t < NB * TILE; t += blockDim.x) {
+        if (upper) {   // A12 columns: contiguous along the pivot index
+            const int x = t / NB, k = t % NB;
+            if (k < kb && x < nx) cp_async_elem(Ps + k * TSTR + x, F + (k0 + k) + (size_t)(x0 + x) * f);
+        } else {       // A21 rows: contiguous along the row index
+            const int x = t % TILE, k = t / TILE;
+            if (k < kb && x < nx) cp_async_elem(Ps + k * TSTR + x, F + (x0 + x) + (size_t)(k0 + k) * f);
+        }
+    }
+    staged_sync();
+    Tile64<C, sizeof(R) == 8> acc;
+    for_tile64(acc, threadIdx.x, [](int, int, C &v) { v = czero<C>(); });
+    mma64<false>(Is, TSTR, 1, Ps, TSTR, 1, kb, kb, nx, acc, threadIdx.x);
+    for_tile64(acc, threadIdx.x, [&](int k, int x, C &v) {
+        if (k < kb && x < nx) {
+            if (upper) F[(k0 + k) + (size_t)(x0 + x) * f] = v;
+            else F[(x0 + x) + (size_t)(k0 + k) * f] = v;
+        }
+    });
 }
 
 // Trailing update C -= Lp * Up on one TILE x TILE tile; 256 threads, each
@@ -324,49 +375,6 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
     const int i0 = k0 + kb, m = f - i0;
     const int nt = (m + TILE - 1) / TILE;
     C *F = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.z * a.s.front_total + a.s.front_off[node];
-    if (blockIdx.x == (unsigned)(ntmax * ntmax)) {
-        // write back the factored diagonal block of this step (k_panel only
-        // read it); the tiles of this kernel never touch that block.
-        __shared__ C D[NB][NB + 1];
-        __shared__ C rdiag[NB];
-        __shared__ int npert;
-        if (threadIdx.x == 0) npert = 0;
-        for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-            const int r = t % kb, c = t / kb;
-            D[r][c] = F[(k0 + r) + (size_t)(k0 + c) * f];
-        }
-        __syncthreads();
-        diag_lu<R>(D, rdiag, kb, (R)(a.pivscale * __longlong_as_double((long long)*a.amax)), &npert);
-        // The substitution only needs the inverses of the block's triangles:
-        // store L^-1 (strict lower part; unit diagonal implied) and U^-1
-        // (upper part with diagonal) in place of L and U.  Thread c < kb
-        // inverts column c of L, thread 32 + c column c of U.
-        __shared__ C Dinv[NB][NB + 1];
-        const int t = threadIdx.x;
-        if (t < kb) {   // the unit diagonal of L^-1 is implied: only U^-1 owns Dinv[c][c]
-            const int c = t;
-            for (int r = c + 1; r < kb; ++r) {
-                C acc = D[r][c];
-                for (int q = c + 1; q < r; ++q) cfma(acc, D[r][q], Dinv[q][c]);
-                Dinv[r][c] = mk(-acc.x, -acc.y);
-            }
-        } else if (t >= 32 && t < 32 + kb) {
-            const int c = t - 32;
-            Dinv[c][c] = rdiag[c];
-            for (int r = c - 1; r >= 0; --r) {
-                C acc = czero<C>();
-                for (int q = r + 1; q <= c; ++q) cfma(acc, D[r][q], Dinv[q][c]);
-                Dinv[r][c] = cmul(mk(-acc.x, -acc.y), rdiag[r]);
-            }
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < kb * kb; i += blockDim.x) {
-            const int r = i % kb, c = i / kb;
-            F[(k0 + r) + (size_t)(k0 + c) * f] = Dinv[r][c];
-        }
-        if (threadIdx.x == 0 && npert) atomicAdd(a.npert, (unsigned long long)npert);
-        return;
-    }
     const int ti = blockIdx.x / ntmax, tj = blockIdx.x % ntmax;
     if (ti >= nt || tj >= nt) return;
     if (i0 + ti * TILE >= s && i0 + tj * TILE >= s) return;   // tile inside the contribution block
@@ -395,6 +403,12 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
             d = csub(d, v);
         }
     });
+    if (blockIdx.x == 0) {
+        // the first tile holds the next diagonal block, now final: factor it
+        // here (the first CTA starts first, so this overlaps the other tiles)
+        __syncthreads();   // the tile's global writes are visible; Ls / Us are free
+        factor_diag_block<R>(a, F, f, i0, min(NB, s - i0), Ls);
+    }
 }
 
 // Batched C -= A * B on CUDA cores (64 x 64 output tiles, 4 x 4 complex
@@ -488,22 +502,27 @@ void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
     static bool attr_set = false;
     if (!attr_set) {
         cudaFuncSetAttribute(k_update<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_panel_mm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr_set = true;
     }
+    for_level_pieces(L, [&](int first, int count) {
+        (k_diag<R><<<dim3(count, a.nf), 256, DIAG_SCRATCH * sizeof(C), st>>>(a, first), note_launch());
+    });
     for (int k0 = 0; k0 < L.max_piv; k0 += NB) {
         const int mmax = L.max_front - k0 - 1;   // largest trailing size (kb >= 1)
-        const int nchunk = mmax > 0 ? (mmax + PCHUNK - 1) / PCHUNK : 0;
-        if (nchunk > 0)
+        const int ntmax = mmax > 0 ? (mmax + TILE - 1) / TILE : 0;
+        if (ntmax > 0)
             for_level_pieces(L, [&](int first, int count) {
-                (k_panel<R><<<dim3(2 * nchunk, count, a.nf), PCHUNK, 0, st>>>(a, first, k0), note_launch());
+                (k_panel_mm<R><<<dim3(2 * ntmax, count, a.nf), 256, smem, st>>>(a, first, k0, ntmax), note_launch());
             });
-        // the trailing tiles only update pivot rows and columns still to come:
-        // after the level's last pivot block every tile would exit at once,
-        // so only the CTA that writes back the diagonal block is launched
-        const int ntmax = (mmax > 0 && L.max_piv > k0 + NB) ? (mmax + TILE - 1) / TILE : 0;
-        for_level_pieces(L, [&](int first, int count) {
-            (k_update<R><<<dim3(ntmax * ntmax + 1, count, a.nf), 256, smem, st>>>(a, first, k0, ntmax), note_launch());
-        });
+        // the trailing tiles only update pivot rows and columns still to
+        // come (and factor the next diagonal block): after the level's last
+        // pivot block there is nothing left for them
+        if (ntmax > 0 && L.max_piv > k0 + NB)
+            for_level_pieces(L, [&](int first, int count) {
+                (k_update<R><<<dim3(ntmax * ntmax, count, a.nf), 256, smem, st>>>(a, first, k0, ntmax),
+                 note_launch());
+            });
     }
 }
 

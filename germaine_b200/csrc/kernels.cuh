@@ -102,7 +102,7 @@ void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
 // Levels of fronts with at most NB pivots that do not fit the small kernel:
 // gather, operator entries, then one CTA per front factorises the pivot
 // panel in shared memory and applies the Schur update to the contribution
-// block (replaces k_panel / k_update and the level's contribution GEMM).
+// block (replaces the K3 / K4 steps and the level's contribution GEMM).
 template <class R>
 bool mid_factor_level(const LevelInfo &L);
 template <class R>
