@@ -209,86 +209,92 @@ __device__ __forceinline__ cplx<R> static_pivot(cplx<R> piv, R pivtol, int &nper
     return piv;
 }
 
-// Factor the kb x kb diagonal block D (shared memory, column stride NB+1)
-// in place: unit-lower L and upper U, static pivoting.  Returns (through
-// shared memory) the reciprocals of the pivots.  (A warp-synchronous form,
-// one row per lane and no block barrier per pivot, measured slower on every
-// tiled level: the rank-1 update is then serial within a lane.)
-template <class R>
-__device__ void diag_lu(cplx<R> (*D)[NB + 1], cplx<R> *rdiag, int kb, R pivtol, int *nperturbed) {
-    using C = cplx<R>;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    for (int p = 0; p < kb; ++p) {
-        if (tid == 0) {
-            const C piv = static_pivot<R>(D[p][p], pivtol, *nperturbed);
-            D[p][p] = piv;
-            rdiag[p] = crcp(piv);
-        }
-        __syncthreads();
-        const C rp = rdiag[p];
-        for (int r = p + 1 + tid; r < kb; r += nt) D[r][p] = cmul(D[r][p], rp);
-        __syncthreads();
-        const int m = kb - p - 1;
-        for (int t = tid; t < m * m; t += nt) {
-            const int r = p + 1 + t % m, c = p + 1 + t / m;
-            cfms(D[r][c], D[r][p], D[p][c]);
-        }
-        __syncthreads();
-    }
-}
-
 // LU of the kb x kb diagonal block at (k0, k0) of the front F (leading
 // dimension f) with static pivoting; the inverses of its two triangles are
-// written back in its place (what the panel products and the substitution
-// multiply by): L^-1 in the strict lower part (unit diagonal implied), U^-1
-// in the upper part with the diagonal.  The whole CTA (at least 64 threads)
-// takes part; sm is shared scratch of DIAG_SCRATCH complex values.
+// written back in its place (all that the panel products and the
+// substitution use): L^-1 in the strict lower part (unit diagonal implied),
+// U^-1 in the upper part with the diagonal.
+//
+// The inverses are built during the elimination, one rank-1 step per pivot
+// p over every entry outside the leading (p+1) x (p+1) block, with l = the
+// scaled column p of L and u = row p of U over the pivot:
+//   trailing   D(r, c) -= l_r D(p, c)             r, c > p
+//   L^-1       X(r, c) -= l_r X(p, c)             r > p >= c   (X = I initially)
+//   unit U^-1  Z(r, c) -= Z(r, p) D(p, c) / piv   r <= p < c   (Z = I initially)
+// (X = L_p^-1 ... L_0^-1 and Z = M_0^-1 ... M_p^-1 for the elementary
+// factors L = L_0 L_1 ... and unit U = ... M_1 M_0), and U^-1 = Z diag(1/piv).
+// All three are T(r, c) -= (a_r / piv) b_c with a = column p and b = row p
+// of D where they lie beyond p, of X / Z otherwise; X and Z share one array
+// (strict lower / upper part).  The regions are disjoint and read only row
+// and column p, so one barrier per pivot suffices; thread 0 forms the next
+// pivot from the same row and column first, applies the static pivot test
+// and publishes its reciprocal.  Each thread owns the entries (t % NB,
+// t / NB + 8 k), k < 4 (256 threads), updated without branches.  (With
+// three barriers per pivot and the inverses as column recurrences
+// afterwards the block took about twice as long; the chain is the serial
+// part of every pivot step of the upper levels.)  The CTA has DIAG_THREADS
+// threads; sm is shared scratch of DIAG_SCRATCH complex values.
 constexpr int DIAG_SCRATCH = 2 * NB * (NB + 1) + NB;
+constexpr int DIAG_THREADS = 256;
 
 template <class R>
 __device__ void factor_diag_block(const FactorArgs<R> &a, cplx<R> *F, int f, int k0, int kb, cplx<R> *sm) {
     using C = cplx<R>;
+    constexpr int NE = NB * NB / DIAG_THREADS;   // entries per thread
     auto D = reinterpret_cast<C (*)[NB + 1]>(sm);
-    auto Dinv = reinterpret_cast<C (*)[NB + 1]>(sm + NB * (NB + 1));
+    auto W = reinterpret_cast<C (*)[NB + 1]>(sm + NB * (NB + 1));   // X (strict lower) and Z (upper)
     C *rdiag = sm + 2 * NB * (NB + 1);
-    __shared__ int npert;
-    if (threadIdx.x == 0) npert = 0;
-    for (int t = threadIdx.x; t < kb * kb; t += blockDim.x) {
-        const int r = t % kb, c = t / kb;
-        D[r][c] = F[(k0 + r) + (size_t)(k0 + c) * f];
-    }
-    __syncthreads();
-    diag_lu<R>(D, rdiag, kb, (R)(a.pivscale * __longlong_as_double((long long)*a.amax)), &npert);
-    // thread c < kb inverts column c of L, thread 32 + c column c of U
-    const int t = threadIdx.x;
-    if (t < kb) {   // the unit diagonal of L^-1 is implied: only U^-1 owns Dinv[c][c]
-        const int c = t;
-        for (int r = c + 1; r < kb; ++r) {
-            C acc = D[r][c];
-            for (int q = c + 1; q < r; ++q) cfma(acc, D[r][q], Dinv[q][c]);
-            Dinv[r][c] = mk(-acc.x, -acc.y);
-        }
-    } else if (t >= 32 && t < 32 + kb) {
-        const int c = t - 32;
-        Dinv[c][c] = rdiag[c];
-        for (int r = c - 1; r >= 0; --r) {
-            C acc = czero<C>();
-            for (int q = r + 1; q <= c; ++q) cfma(acc, D[r][q], Dinv[q][c]);
-            Dinv[r][c] = cmul(mk(-acc.x, -acc.y), rdiag[r]);
+    const R pivtol = (R)(a.pivscale * __longlong_as_double((long long)*a.amax));
+    int np = 0;   // pivots this thread perturbed
+    const int r = threadIdx.x % NB, cb = threadIdx.x / NB;
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        const int c = cb + (DIAG_THREADS / NB) * e;
+        if (r < kb && c < kb) {
+            C v = F[(k0 + r) + (size_t)(k0 + c) * f];
+            if (r == 0 && c == 0) {
+                v = static_pivot<R>(v, pivtol, np);
+                rdiag[0] = crcp(v);
+            }
+            D[r][c] = v;
+            W[r][c] = r == c ? mk(R(1), R(0)) : czero<C>();
         }
     }
     __syncthreads();
-    for (int i = threadIdx.x; i < kb * kb; i += blockDim.x) {
-        const int r = i % kb, c = i / kb;
-        F[(k0 + r) + (size_t)(k0 + c) * f] = Dinv[r][c];
+    for (int p = 0; p + 1 < kb; ++p) {
+        const C rp = rdiag[p];
+        if (threadIdx.x == 0) {
+            C v = D[p + 1][p + 1];
+            cfms(v, cmul(D[p + 1][p], rp), D[p][p + 1]);
+            v = static_pivot<R>(v, pivtol, np);
+            rdiag[p + 1] = crcp(v);
+        }
+#pragma unroll
+        for (int e = 0; e < NE; ++e) {
+            const int c = cb + (DIAG_THREADS / NB) * e;
+            if (r < kb && c < kb && (r > p || c > p) && !(r == p + 1 && c == p + 1)) {
+                const C av = r > p ? D[r][p] : W[r][p];
+                const C bv = c > p ? D[p][c] : W[p][c];
+                C &T = (r > p && c > p) ? D[r][c] : W[r][c];
+                C v = T;
+                cfms(v, cmul(av, rp), bv);
+                T = v;
+            }
+        }
+        __syncthreads();
     }
-    if (threadIdx.x == 0 && npert) atomicAdd(a.npert, (unsigned long long)npert);
+#pragma unroll
+    for (int e = 0; e < NE; ++e) {
+        const int c = cb + (DIAG_THREADS / NB) * e;
+        if (r < kb && c < kb) F[(k0 + r) + (size_t)(k0 + c) * f] = r > c ? W[r][c] : cmul(W[r][c], rdiag[c]);
+    }
+    if (np) atomicAdd(a.npert, (unsigned long long)np);
 }
 
 // K3a: the first diagonal block of every front of the level (the later
 // ones are factored by the first CTA of the preceding trailing update)
 template <class R>
-__global__ void __launch_bounds__(256) k_diag(FactorArgs<R> a, int lvl_first) {
+__global__ void __launch_bounds__(DIAG_THREADS) k_diag(FactorArgs<R> a, int lvl_first) {
     using C = cplx<R>;
     const int node = a.s.lvl_nodes[lvl_first + blockIdx.x];
     const int s = a.s.npiv[node];
@@ -364,6 +370,7 @@ __global__ void __launch_bounds__(256) k_panel_mm(FactorArgs<R> a, int lvl_first
 // pivot columns is updated here; the contribution block (rows and columns
 // >= npiv) receives all pivot steps at once in one K = npiv GEMM at the end
 // of the level (launch_cb_gemm).
+static_assert(DIAG_THREADS == 256, "k_update's first CTA factors the next diagonal block");
 template <class R>
 __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, int k0, int ntmax) {
     using C = cplx<R>;
@@ -383,22 +390,26 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
     C *Ls = reinterpret_cast<C *>(smem_raw);   // [NB][TSTR]: Ls[c * TSTR + r]
     C *Us = Ls + NB * TSTR;                    // [NB][TSTR]: Us[c * TSTR + col]
     const int r0 = i0 + ti * TILE, c0 = i0 + tj * TILE;
-    // asynchronous copies, all in flight at once; entries outside the
-    // front or beyond kb are not staged (the product reads k < kb only and
-    // treats rows / columns outside the front as zero)
+    // a tile whose columns all lie in the contribution block needs only its
+    // pivot rows (and the other way round): the product is cut to them
+    const int mrows = c0 >= s ? min(TILE, s - r0) : min(TILE, f - r0);
+    const int ncols = r0 >= s ? min(TILE, s - c0) : min(TILE, f - c0);
+    // asynchronous copies, all in flight at once; entries outside those rows
+    // and columns or beyond kb are not staged (the product reads k < kb only
+    // and treats rows / columns outside them as zero)
     for (int t = threadIdx.x; t < NB * TILE; t += blockDim.x) {
         const int r = t % TILE, c = t / TILE;
-        if (c < kb && r0 + r < f) cp_async_elem(Ls + c * TSTR + r, F + (r0 + r) + (size_t)(k0 + c) * f);
+        if (c < kb && r < mrows) cp_async_elem(Ls + c * TSTR + r, F + (r0 + r) + (size_t)(k0 + c) * f);
         const int col = t / NB, cc = t % NB;   // U: contiguous along the pivot index
-        if (cc < kb && c0 + col < f) cp_async_elem(Us + cc * TSTR + col, F + (k0 + cc) + (size_t)(c0 + col) * f);
+        if (cc < kb && col < ncols) cp_async_elem(Us + cc * TSTR + col, F + (k0 + cc) + (size_t)(c0 + col) * f);
     }
     staged_sync();
     Tile64<C, sizeof(R) == 8> acc;
     for_tile64(acc, threadIdx.x, [](int, int, C &v) { v = czero<C>(); });
-    mma64<false>(Ls, TSTR, 1, Us, TSTR, 1, kb, min(TILE, f - r0), min(TILE, f - c0), acc, threadIdx.x);
+    mma64<false>(Ls, TSTR, 1, Us, TSTR, 1, kb, mrows, ncols, acc, threadIdx.x);
     for_tile64(acc, threadIdx.x, [&](int rr, int cc, C &v) {
         const int row = r0 + rr, col = c0 + cc;
-        if (row < f && col < f && (row < s || col < s)) {
+        if (rr < mrows && cc < ncols && (row < s || col < s)) {
             C &d = F[row + (size_t)col * f];
             d = csub(d, v);
         }
@@ -506,7 +517,7 @@ void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
         attr_set = true;
     }
     for_level_pieces(L, [&](int first, int count) {
-        (k_diag<R><<<dim3(count, a.nf), 256, DIAG_SCRATCH * sizeof(C), st>>>(a, first), note_launch());
+        (k_diag<R><<<dim3(count, a.nf), DIAG_THREADS, DIAG_SCRATCH * sizeof(C), st>>>(a, first), note_launch());
     });
     for (int k0 = 0; k0 < L.max_piv; k0 += NB) {
         const int mmax = L.max_front - k0 - 1;   // largest trailing size (kb >= 1)
@@ -533,7 +544,7 @@ template void launch_factor_level<float>(const FactorArgs<float> &, const LevelI
 // Small fronts (the lower levels of the tree): one CTA assembles and
 // factorises a whole front in shared memory -- extend-add of the children's
 // contribution blocks, the operator entries, right-looking LU of the npiv
-// pivot columns with the same static pivoting as diag_lu, the Schur
+// pivot columns with the same static pivoting as factor_diag_block, the Schur
 // complement of the contribution block, and the inverses of the NB x NB
 // diagonal blocks -- and writes the front back once.  The result has the
 // layout the blocked path leaves (L below, U above, diagonal-block inverses,
@@ -598,7 +609,7 @@ __global__ void __launch_bounds__(SMALL_FT, BLOCKED ? 3 : 4) k_factor_small(Fact
     // right-looking LU of the pivot columns; the trailing update covers the
     // contribution block too (its Schur complement).  Warp 0 updates column
     // k + 1 first in step k, so it can take the next pivot (static pivoting
-    // as in diag_lu) and scale the next L column while the other warps are
+    // as in factor_diag_block) and scale the next L column while the other warps are
     // still updating: one barrier per pivot.
     const R pivtol = (R)(a.pivscale * __longlong_as_double((long long)*a.amax));
     auto take_pivot = [&](int k) {   // warp 0 only: pivot k, reciprocal, L column k scaled
@@ -868,7 +879,7 @@ namespace gm {
 // gather and the operator entries (K2), one CTA per front and frequency
 //   1. factorises the pivot columns (f x s) right-looking with each thread
 //      holding one front row in registers: per pivot, the owner of the next
-//      pivot row applies the static pivoting of diag_lu and publishes the
+//      pivot row applies the static pivoting of factor_diag_block and publishes the
 //      row and the pivot's reciprocal in shared memory, so one barrier per
 //      pivot and no shared-memory traffic for the update itself;
 //   2. solves L11 U12 = A12 with each thread holding one column of U12;
