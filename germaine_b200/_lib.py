@@ -39,7 +39,7 @@ class GmConfig(ctypes.Structure):
                 ("s", ctypes.c_float), ("physics", ctypes.c_int32), ("precision", ctypes.c_int32),
                 ("op_mode", ctypes.c_int32), ("leaf_max", ctypes.c_int32), ("ir_tol", ctypes.c_double),
                 ("ir_max_iter", ctypes.c_int32), ("refine", ctypes.c_int32), ("gmres_restart", ctypes.c_int32),
-                ("tc_min_block", ctypes.c_int32)]
+                ("tc_min_block", ctypes.c_int32), ("pivot_tol", ctypes.c_double)]
 
 
 class GmStats(ctypes.Structure):
@@ -51,7 +51,8 @@ class GmStats(ctypes.Structure):
                 ("ir_residual", ctypes.c_double), ("ms_assemble", ctypes.c_double),
                 ("ms_factor", ctypes.c_double), ("ms_solve", ctypes.c_double), ("ms_refine", ctypes.c_double),
                 ("ms_subst", ctypes.c_double), ("n_subst", ctypes.c_int32), ("kernel_launches", ctypes.c_int64),
-                ("u_entries", ctypes.c_int64), ("ms_subst_bwd", ctypes.c_double), ("tc_tiles", ctypes.c_int64)]
+                ("u_entries", ctypes.c_int64), ("ms_subst_bwd", ctypes.c_double), ("tc_tiles", ctypes.c_int64),
+                ("pivot_swaps", ctypes.c_int64)]
 
     def as_dict(self) -> dict:
         return {k: getattr(self, k) for k, _ in self._fields_}

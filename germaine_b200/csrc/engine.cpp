@@ -89,6 +89,7 @@ extern "C" int gm_engine_create(int device, const gm_config *cfg, gm_engine **ou
         e->cfg = *cfg;
         if (e->cfg.leaf_max <= 0) e->cfg.leaf_max = 32;   // measured best at 841 x 227 (24 .. 40 within 6 %)
         if (!(e->cfg.ir_tol > 0)) e->cfg.ir_tol = 1e-10;
+        if (e->cfg.pivot_tol == 0) e->cfg.pivot_tol = 0.1;
         if (e->cfg.ir_max_iter <= 0) e->cfg.ir_max_iter = 10;
         if (e->cfg.gmres_restart <= 0 || e->cfg.gmres_restart > gm::kGmresMaxRestart)
             e->cfg.gmres_restart = gm::kGmresMaxRestart;
@@ -358,6 +359,9 @@ static int factor_batch(gm_engine *e, double pivscale) {
     a.amax = e->d_amax.as<unsigned long long>();
     a.pivscale = pivscale;
     a.npert = e->d_npert.as<unsigned long long>();
+    a.nswap = a.npert + 1;
+    a.pivtau2 = e->cfg.pivot_tol > 0 ? e->cfg.pivot_tol * e->cfg.pivot_tol : 0.0;
+    a.pivsrc = e->cfg.pivot_tol > 0 ? e->d_pivsrc.as<unsigned char>() : nullptr;
     if (e->cb_plan_base != e->d_front.p || e->cb_plan_nf != e->nf) {
         const int rc = build_cb_plan<R>(e);
         if (rc) return rc;
@@ -394,6 +398,7 @@ static int factor_batch(gm_engine *e, double pivscale) {
         // attributes outside any capture), the second captures the graph.
         gm_engine::FactorGraphKey key;
         key.front = e->d_front.p; key.A = e->d_A.p; key.amax = e->d_amax.p; key.npert = e->d_npert.p;
+        key.pivsrc = e->d_pivsrc.p;
         key.tcerr = e->d_tcerr.p; key.probs = probs; key.tiles = tiles; key.nf = e->nf; key.fp64 = sizeof(R) == 8;
         if (!(e->fgraph && key == e->fgraph_key) && key == e->fgraph_seen) {
             if (e->fgraph) cudaGraphExecDestroy(e->fgraph);
@@ -451,6 +456,28 @@ static int factor_batch(gm_engine *e, double pivscale) {
 
 namespace gm {
 
+// The threshold-pivoting record starts as the identity: pivot k of a front
+// takes row k % 32 of its 32-pivot block.  The factorisation rewrites the
+// entries of the pivoted levels each time and never touches the others, so
+// a slot is initialised once per buffer.
+static int init_pivsrc(gm_engine *e) {
+    if (e->pivsrc_ready != e->d_pivsrc.p) {
+        e->pivsrc_ready = e->d_pivsrc.p;
+        e->pivsrc_ready_nf = 0;
+    }
+    if (e->pivsrc_ready_nf >= e->nf) return GM_OK;
+    const gm::Symbolic &s = e->sym;
+    std::vector<unsigned char> ident((size_t)e->n, 0);
+    for (int v = 0; v < s.nnodes; ++v)
+        for (int k = 0; k < s.npiv[v]; ++k) ident[s.vars[s.var_off[v] + k]] = (unsigned char)(k % 32);
+    for (int f = e->pivsrc_ready_nf; f < e->nf; ++f)
+        GM_CUDA(cudaMemcpyAsync(e->d_pivsrc.as<unsigned char>() + (size_t)f * e->n, ident.data(), e->n,
+                                cudaMemcpyHostToDevice, e->st));
+    GM_CUDA(cudaStreamSynchronize(e->st));   // the host vector goes out of scope
+    e->pivsrc_ready_nf = e->nf;
+    return GM_OK;
+}
+
 // Numeric factorisation of the nf operators in e->d_A (assembled or given
 // by value).  The static-pivot threshold is relative to max |A| over the
 // whole batch, reduced on the device.
@@ -458,10 +485,15 @@ static int factor_assembled(gm_engine *e) {
     const bool fp64 = e->cfg.precision == GM_PREC_FP64;
     const size_t fbytes = (size_t)e->nf * e->sym.front_total * e->csize();
     GM_ALLOC(e->d_front, fbytes);
-    GM_ALLOC(e->d_npert, sizeof(unsigned long long));
+    GM_ALLOC(e->d_npert, 2 * sizeof(unsigned long long));   // perturbed pivots, row exchanges
     GM_ALLOC(e->d_amax, sizeof(unsigned long long));
+    if (e->cfg.pivot_tol > 0) {
+        GM_ALLOC(e->d_pivsrc, (size_t)e->nf * e->n);
+        const int rc = init_pivsrc(e);
+        if (rc) return rc;
+    }
     GM_CUDA(cudaEventRecord(e->ev0, e->st));
-    GM_CUDA(cudaMemsetAsync(e->d_npert.p, 0, sizeof(unsigned long long), e->st));
+    GM_CUDA(cudaMemsetAsync(e->d_npert.p, 0, 2 * sizeof(unsigned long long), e->st));
     GM_CUDA(cudaMemsetAsync(e->d_amax.p, 0, sizeof(unsigned long long), e->st));
     launch_amax(e->d_A.as<double2>(), (size_t)e->nf * 9 * e->n, e->d_amax.as<unsigned long long>(), e->st);
     const int rc = fp64 ? factor_batch<double>(e, 1e-13) : factor_batch<float>(e, 1e-6);
@@ -471,8 +503,10 @@ static int factor_assembled(gm_engine *e) {
     float ms = 0;
     cudaEventElapsedTime(&ms, e->ev0, e->ev1);
     e->stats.ms_factor = ms;
-    unsigned long long np = 0, amax_bits = 0;
+    unsigned long long np = 0, amax_bits = 0, nsw = 0;
     GM_CUDA(cudaMemcpy(&np, e->d_npert.p, sizeof np, cudaMemcpyDeviceToHost));
+    GM_CUDA(cudaMemcpy(&nsw, e->d_npert.as<unsigned long long>() + 1, sizeof nsw, cudaMemcpyDeviceToHost));
+    e->stats.pivot_swaps = (int64_t)nsw;
     GM_CUDA(cudaMemcpy(&amax_bits, e->d_amax.p, sizeof amax_bits, cudaMemcpyDeviceToHost));
     double amax = 0;
     std::memcpy(&amax, &amax_bits, sizeof amax);
@@ -580,6 +614,7 @@ static void substitute(gm_engine *e, void *xT, int nrhs, int trans, const unsign
     SolveArgs<R> a{};
     a.s = e->dsym;
     a.front = e->d_front.p;
+    a.pivsrc = e->cfg.pivot_tol > 0 ? e->d_pivsrc.as<unsigned char>() : nullptr;
     a.x = xT;
     a.w = e->d_w.p;
     a.nf = e->nf;
@@ -1170,6 +1205,7 @@ static void time_levels(gm_engine *e, void *xT, int nrhs, std::vector<float> &fw
     SolveArgs<R> a{};
     a.s = e->dsym;
     a.front = e->d_front.p;
+    a.pivsrc = e->cfg.pivot_tol > 0 ? e->d_pivsrc.as<unsigned char>() : nullptr;
     a.x = xT;
     a.w = e->d_w.p;
     a.nf = e->nf;

@@ -68,6 +68,12 @@ struct gm_engine {
     std::vector<float> freqs;
     std::vector<int> models;    // material model of each matrix of the batch
     gm::DevBuf d_A, d_mass, d_pml, d_fq, d_front, d_npert, d_amax;
+    // threshold pivoting record [nf][n] (FactorArgs::pivsrc): every slot up
+    // to pivsrc_ready_nf of the buffer at pivsrc_ready holds the identity
+    // outside the pivoted levels
+    gm::DevBuf d_pivsrc;
+    const void *pivsrc_ready = nullptr;
+    int pivsrc_ready_nf = 0;
     bool factored = false;
     bool values_only = false;   // operator given by gm_factor_values (no frequencies / model)
 
@@ -82,11 +88,11 @@ struct gm_engine {
     // the buffers and the batch it was captured for stay the same
     struct FactorGraphKey {
         const void *front = nullptr, *A = nullptr, *amax = nullptr, *npert = nullptr, *tcerr = nullptr;
-        const void *probs = nullptr, *tiles = nullptr;
+        const void *probs = nullptr, *tiles = nullptr, *pivsrc = nullptr;
         int nf = 0, fp64 = 0;
         bool operator==(const FactorGraphKey &o) const {
             return front == o.front && A == o.A && amax == o.amax && npert == o.npert && tcerr == o.tcerr &&
-                   probs == o.probs && tiles == o.tiles && nf == o.nf && fp64 == o.fp64;
+                   probs == o.probs && tiles == o.tiles && pivsrc == o.pivsrc && nf == o.nf && fp64 == o.fp64;
         }
     };
     FactorGraphKey fgraph_key, fgraph_seen;

@@ -226,33 +226,47 @@ __device__ __forceinline__ cplx<R> static_pivot(cplx<R> piv, R pivtol, int &nper
 // All three are T(r, c) -= (a_r / piv) b_c with a = column p and b = row p
 // of D where they lie beyond p, of X / Z otherwise; X and Z share one array
 // (strict lower / upper part).  The regions are disjoint and read only row
-// and column p, so one barrier per pivot suffices; thread 0 forms the next
-// pivot from the same row and column first, applies the static pivot test
-// and publishes its reciprocal.  Each thread owns the entries (t % NB,
-// t / NB + 8 k), k < 4 (256 threads), updated without branches.  (With
-// three barriers per pivot and the inverses as column recurrences
-// afterwards the block took about twice as long; the chain is the serial
-// part of every pivot step of the upper levels.)  The CTA has DIAG_THREADS
-// threads; sm is shared scratch of DIAG_SCRATCH complex values.
+// and column p, so one barrier per pivot suffices.  Each thread owns the
+// entries (t % NB, t / NB + 8 k), k < 4 (256 threads), updated without
+// branches.  (With three barriers per pivot and the inverses as column
+// recurrences afterwards the block took about twice as long; the chain is
+// the serial part of every pivot step of the upper levels.)
+//
+// Without row exchanges (PIV false) thread 0 forms the next pivot from row
+// and column p before the step and publishes its reciprocal.  With them,
+// warp 0 picks pivot p after step p - 1 (a second barrier): the row r >= p
+// of largest |D(r, p)| is exchanged with row p when |D(p, p)|^2 <
+// pivtau2 |D(r, p)|^2 -- the whole row of D (its multipliers included) and
+// the finished part of X (columns < p: X' = P X P for the exchange P);
+// Z only holds finished rows < p.  The block's permutation goes to
+// pivsrc[vars[k0 + q]] (q: pivot position, value: block row in equation
+// order); columns right of the block are exchanged when the U panel is
+// staged, columns left of it (earlier blocks' multipliers) stay in equation
+// order -- the forward substitution gathers the block's rows at the same
+// point of the elimination.  The CTA has DIAG_THREADS threads; sm is shared
+// scratch of DIAG_SCRATCH complex values.
 constexpr int DIAG_SCRATCH = 2 * NB * (NB + 1) + NB;
 constexpr int DIAG_THREADS = 256;
 
-template <class R>
-__device__ void factor_diag_block(const FactorArgs<R> &a, cplx<R> *F, int f, int k0, int kb, cplx<R> *sm) {
+template <class R, bool PIV>
+__device__ void factor_diag_block(const FactorArgs<R> &a, cplx<R> *F, int f, int k0, int kb, cplx<R> *sm,
+                                  unsigned char *src, const int *vars) {
     using C = cplx<R>;
     constexpr int NE = NB * NB / DIAG_THREADS;   // entries per thread
     auto D = reinterpret_cast<C (*)[NB + 1]>(sm);
     auto W = reinterpret_cast<C (*)[NB + 1]>(sm + NB * (NB + 1));   // X (strict lower) and Z (upper)
     C *rdiag = sm + 2 * NB * (NB + 1);
+    __shared__ int rowof[NB];   // PIV: block row (equation order) at pivot position q
     const R pivtol = (R)(a.pivscale * __longlong_as_double((long long)*a.amax));
-    int np = 0;   // pivots this thread perturbed
+    int np = 0, nsw = 0;   // pivots this thread perturbed / exchanged
     const int r = threadIdx.x % NB, cb = threadIdx.x / NB;
+    if (PIV && threadIdx.x < NB) rowof[threadIdx.x] = threadIdx.x;
 #pragma unroll
     for (int e = 0; e < NE; ++e) {
         const int c = cb + (DIAG_THREADS / NB) * e;
         if (r < kb && c < kb) {
             C v = F[(k0 + r) + (size_t)(k0 + c) * f];
-            if (r == 0 && c == 0) {
+            if (!PIV && r == 0 && c == 0) {
                 v = static_pivot<R>(v, pivtol, np);
                 rdiag[0] = crcp(v);
             }
@@ -261,9 +275,52 @@ __device__ void factor_diag_block(const FactorArgs<R> &a, cplx<R> *F, int f, int
         }
     }
     __syncthreads();
-    for (int p = 0; p + 1 < kb; ++p) {
+    for (int p = 0; p < kb; ++p) {
+        if (PIV) {
+            if (threadIdx.x < 32) {   // warp 0: pivot p
+                const int lane = threadIdx.x;
+                R m2 = lane >= p && lane < kb ? cabs2(D[lane][p]) : R(-1);
+                int arg = lane;
+#pragma unroll
+                for (int o = 16; o; o >>= 1) {
+                    const R om = __shfl_xor_sync(0xffffffffu, m2, o);
+                    const int oa = __shfl_xor_sync(0xffffffffu, arg, o);
+                    if (om > m2 || (om == m2 && oa < arg)) {
+                        m2 = om;
+                        arg = oa;
+                    }
+                }
+                m2 = __shfl_sync(0xffffffffu, m2, 0);   // lane 0's result for all (NaN entries
+                arg = __shfl_sync(0xffffffffu, arg, 0);  // could leave the lanes disagreeing)
+                const bool swap = arg != p && cabs2(D[p][p]) < (R)a.pivtau2 * m2;   // warp-uniform
+                if (swap) {
+                    if (lane < kb) {
+                        const C t = D[p][lane];
+                        D[p][lane] = D[arg][lane];
+                        D[arg][lane] = t;
+                        if (lane < p) {
+                            const C u = W[p][lane];
+                            W[p][lane] = W[arg][lane];
+                            W[arg][lane] = u;
+                        }
+                    }
+                    if (lane == 0) {
+                        const int t = rowof[p];
+                        rowof[p] = rowof[arg];
+                        rowof[arg] = t;
+                        ++nsw;
+                    }
+                    __syncwarp();
+                }
+                if (lane == 0) rdiag[p] = crcp(static_pivot<R>(D[p][p], pivtol, np));
+            }
+            __syncthreads();
+            if (p + 1 == kb) break;
+        } else if (p + 1 == kb) {
+            break;
+        }
         const C rp = rdiag[p];
-        if (threadIdx.x == 0) {
+        if (!PIV && threadIdx.x == 0) {
             C v = D[p + 1][p + 1];
             cfms(v, cmul(D[p + 1][p], rp), D[p][p + 1]);
             v = static_pivot<R>(v, pivtol, np);
@@ -272,7 +329,7 @@ __device__ void factor_diag_block(const FactorArgs<R> &a, cplx<R> *F, int f, int
 #pragma unroll
         for (int e = 0; e < NE; ++e) {
             const int c = cb + (DIAG_THREADS / NB) * e;
-            if (r < kb && c < kb && (r > p || c > p) && !(r == p + 1 && c == p + 1)) {
+            if (r < kb && c < kb && (r > p || c > p) && (PIV || !(r == p + 1 && c == p + 1))) {
                 const C av = r > p ? D[r][p] : W[r][p];
                 const C bv = c > p ? D[p][c] : W[p][c];
                 C &T = (r > p && c > p) ? D[r][c] : W[r][c];
@@ -288,21 +345,35 @@ __device__ void factor_diag_block(const FactorArgs<R> &a, cplx<R> *F, int f, int
         const int c = cb + (DIAG_THREADS / NB) * e;
         if (r < kb && c < kb) F[(k0 + r) + (size_t)(k0 + c) * f] = r > c ? W[r][c] : cmul(W[r][c], rdiag[c]);
     }
+    if (PIV && threadIdx.x < kb) src[vars[k0 + threadIdx.x]] = (unsigned char)rowof[threadIdx.x];
     if (np) atomicAdd(a.npert, (unsigned long long)np);
+    if (PIV && nsw) atomicAdd(a.nswap, (unsigned long long)nsw);
+}
+
+// the diagonal block (k0, kb) of front `node` in matrix z, with row
+// exchanges when piv (the level's fronts have more than NB pivots)
+template <class R>
+__device__ __forceinline__ void diag_block(const FactorArgs<R> &a, cplx<R> *F, int node, int z, int k0, int kb,
+                                           cplx<R> *sm, bool piv) {
+    const int f = a.s.nfront[node];
+    if (piv) {
+        factor_diag_block<R, true>(a, F, f, k0, kb, sm, a.pivsrc + (size_t)z * a.s.n, a.s.vars + a.s.var_off[node]);
+    } else {
+        factor_diag_block<R, false>(a, F, f, k0, kb, sm, nullptr, nullptr);
+    }
 }
 
 // K3a: the first diagonal block of every front of the level (the later
 // ones are factored by the first CTA of the preceding trailing update)
 template <class R>
-__global__ void __launch_bounds__(DIAG_THREADS) k_diag(FactorArgs<R> a, int lvl_first) {
+__global__ void __launch_bounds__(DIAG_THREADS) k_diag(FactorArgs<R> a, int lvl_first, int piv) {
     using C = cplx<R>;
     const int node = a.s.lvl_nodes[lvl_first + blockIdx.x];
     const int s = a.s.npiv[node];
     if (s <= 0) return;
-    const int f = a.s.nfront[node];
     C *F = reinterpret_cast<C *>(a.front) + (size_t)blockIdx.y * a.s.front_total + a.s.front_off[node];
     extern __shared__ unsigned char smem_raw[];
-    factor_diag_block<R>(a, F, f, 0, min(NB, s), reinterpret_cast<C *>(smem_raw));
+    diag_block<R>(a, F, node, blockIdx.y, 0, min(NB, s), reinterpret_cast<C *>(smem_raw), piv != 0);
 }
 
 // K3b: the L and U panels of pivot block k0 as products with the inverted
@@ -313,7 +384,7 @@ __global__ void __launch_bounds__(DIAG_THREADS) k_diag(FactorArgs<R> a, int lvl_
 // tile layout hold work.  Each CTA reads and writes only its own slice;
 // the diagonal block is read-only here.
 template <class R>
-__global__ void __launch_bounds__(256) k_panel_mm(FactorArgs<R> a, int lvl_first, int k0, int ntmax) {
+__global__ void __launch_bounds__(256) k_panel_mm(FactorArgs<R> a, int lvl_first, int k0, int ntmax, int piv) {
     using C = cplx<R>;
     const int node = a.s.lvl_nodes[lvl_first + blockIdx.y];
     const int s = a.s.npiv[node];
@@ -343,10 +414,18 @@ __global__ void __launch_bounds__(256) k_panel_mm(FactorArgs<R> a, int lvl_first
             }
         }
     }
+    __shared__ unsigned char rsrc[NB];   // U slice: block row of pivot position k (row exchanges)
+    if (upper) {
+        if (threadIdx.x < NB)
+            rsrc[threadIdx.x] = piv && threadIdx.x < kb
+                                    ? a.pivsrc[(size_t)blockIdx.z * a.s.n + a.s.vars[a.s.var_off[node] + k0 + threadIdx.x]]
+                                    : (unsigned char)threadIdx.x;
+        __syncthreads();
+    }
     for (int t = threadIdx.x; t < NB * TILE; t += blockDim.x) {
-        if (upper) {   // A12 columns: contiguous along the pivot index
+        if (upper) {   // A12 columns: contiguous along the pivot index; rows in pivot order
             const int x = t / NB, k = t % NB;
-            if (k < kb && x < nx) cp_async_elem(Ps + k * TSTR + x, F + (k0 + k) + (size_t)(x0 + x) * f);
+            if (k < kb && x < nx) cp_async_elem(Ps + k * TSTR + x, F + (k0 + rsrc[k]) + (size_t)(x0 + x) * f);
         } else {       // A21 rows: contiguous along the row index
             const int x = t % TILE, k = t / TILE;
             if (k < kb && x < nx) cp_async_elem(Ps + k * TSTR + x, F + (x0 + x) + (size_t)(k0 + k) * f);
@@ -372,7 +451,7 @@ __global__ void __launch_bounds__(256) k_panel_mm(FactorArgs<R> a, int lvl_first
 // of the level (launch_cb_gemm).
 static_assert(DIAG_THREADS == 256, "k_update's first CTA factors the next diagonal block");
 template <class R>
-__global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, int k0, int ntmax) {
+__global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, int k0, int ntmax, int piv) {
     using C = cplx<R>;
     const int node = a.s.lvl_nodes[lvl_first + blockIdx.y];
     const int s = a.s.npiv[node];
@@ -418,7 +497,7 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
         // the first tile holds the next diagonal block, now final: factor it
         // here (the first CTA starts first, so this overlaps the other tiles)
         __syncthreads();   // the tile's global writes are visible; Ls / Us are free
-        factor_diag_block<R>(a, F, f, i0, min(NB, s - i0), Ls);
+        diag_block<R>(a, F, node, blockIdx.z, i0, min(NB, s - i0), Ls, piv != 0);
     }
 }
 
@@ -516,22 +595,24 @@ void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
         cudaFuncSetAttribute(k_panel_mm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr_set = true;
     }
+    // row exchanges on the levels the substitution solves by 32-pivot blocks
+    const int piv = a.pivsrc && a.pivtau2 > 0 && L.max_piv > NB;
     for_level_pieces(L, [&](int first, int count) {
-        (k_diag<R><<<dim3(count, a.nf), DIAG_THREADS, DIAG_SCRATCH * sizeof(C), st>>>(a, first), note_launch());
+        (k_diag<R><<<dim3(count, a.nf), DIAG_THREADS, DIAG_SCRATCH * sizeof(C), st>>>(a, first, piv), note_launch());
     });
     for (int k0 = 0; k0 < L.max_piv; k0 += NB) {
         const int mmax = L.max_front - k0 - 1;   // largest trailing size (kb >= 1)
         const int ntmax = mmax > 0 ? (mmax + TILE - 1) / TILE : 0;
         if (ntmax > 0)
             for_level_pieces(L, [&](int first, int count) {
-                (k_panel_mm<R><<<dim3(2 * ntmax, count, a.nf), 256, smem, st>>>(a, first, k0, ntmax), note_launch());
+                (k_panel_mm<R><<<dim3(2 * ntmax, count, a.nf), 256, smem, st>>>(a, first, k0, ntmax, piv), note_launch());
             });
         // the trailing tiles only update pivot rows and columns still to
         // come (and factor the next diagonal block): after the level's last
         // pivot block there is nothing left for them
         if (ntmax > 0 && L.max_piv > k0 + NB)
             for_level_pieces(L, [&](int first, int count) {
-                (k_update<R><<<dim3(ntmax * ntmax, count, a.nf), 256, smem, st>>>(a, first, k0, ntmax),
+                (k_update<R><<<dim3(ntmax * ntmax, count, a.nf), 256, smem, st>>>(a, first, k0, ntmax, piv),
                  note_launch());
             });
     }

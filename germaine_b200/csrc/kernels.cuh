@@ -80,6 +80,13 @@ struct FactorArgs {
     const unsigned long long *amax;
     double pivscale;
     unsigned long long *npert;  // perturbed-pivot counter
+    // threshold partial pivoting inside the 32-pivot blocks of the tiled
+    // levels (fronts with more than NB pivots): pivtau2 = tolerance^2 (0 =
+    // off); pivsrc[matrix * n + vars[k]] = the row of pivot k's block (0 ..
+    // 31, equation order) that pivot position k took; nswap counts exchanges
+    double pivtau2;
+    unsigned char *pivsrc;
+    unsigned long long *nswap;
     const int64_t *ent_lvl_off; // entries of level position t (index into lvl_nodes):
                                 // ent_dst/ent_src[ent_lvl_off[t] .. ent_lvl_off[t + 1])
 };
@@ -158,6 +165,12 @@ struct SolveArgs {
     // the backward pass takes y = 0 at the pivot rows of pruned fronts.
     const int *spike_k;
     const double2 *spike_amp;
+    // row exchanges of the factorisation's threshold pivoting (FactorArgs::
+    // pivsrc; NULL: none): within each 32-pivot block of the fronts solved
+    // by the ring / pivot kernels, the forward pass of M x = b gathers the
+    // block's right-hand-side rows through it, the backward pass of
+    // M^T x = b scatters the block's solution rows through it
+    const unsigned char *pivsrc;
 };
 
 // right-hand sides per substitution slice for nrhs right-hand sides

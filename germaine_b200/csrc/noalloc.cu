@@ -77,6 +77,7 @@ void substitute_into(gm_engine *e, void *xT, void *w, int nrhs, int trans) {
     gm::SolveArgs<R> a{};
     a.s = e->dsym;
     a.front = e->d_front.p;
+    a.pivsrc = e->cfg.pivot_tol > 0 ? e->d_pivsrc.as<unsigned char>() : nullptr;
     a.x = xT;
     a.w = w;
     a.nf = e->nf;

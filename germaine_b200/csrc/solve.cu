@@ -393,11 +393,22 @@ __global__ void __launch_bounds__(NT) k_fwd_piv(SolveArgs<R> a, int lvl_first, i
     pivot_rhs(a, c, inv, W0, W1, r0, ldr);   // (the ring part is k_fwd_ring's)
 
     auto xrow = [&](int k) { return c.X + (size_t)c.vars[k] * ldr; };
+    // M x = b with row exchanges: block k0's right-hand-side rows are taken
+    // in pivot order (prow[q]: the block row at pivot position q), y is
+    // written in pivot order (rows of L' below the block stay in equation
+    // order until their own block)
+    __shared__ unsigned char prow[SNB];
+    const bool pv = !TRANS && a.pivsrc;
+    const unsigned char *psrc = pv ? a.pivsrc + solve_matrix(a) * (size_t)a.s.n : nullptr;
     TileAcc<C, RT, B> acc;
     for (int k0 = 0; k0 < c.s; k0 += SNB) {
         const int kb = min(SNB, c.s - k0);
+        if (pv) {   // the previous block's reads of prow ended before its staged_sync
+            if (threadIdx.x < kb) prow[threadIdx.x] = psrc[c.vars[k0 + threadIdx.x]];
+            __syncthreads();
+        }
         stage_dinv<C, true, TRANS, RT, B>(sm, c.F, c.f, k0, kb);
-        stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
+        stage_rows(sm, [&](int q) { return xrow(k0 + (pv ? prow[q] : q)); }, kb, c.rn);
         staged_sync();
         zero_acc(acc);
         tile_mma<TRI_LOWER>(sm, kb, acc, kb, c.rn);   // y_b = Dinv w_b
@@ -517,17 +528,24 @@ __global__ void __launch_bounds__(NT) k_bwd_piv(SolveArgs<R> a, int lvl_first, i
         }
         __syncthreads();
     }
+    // M^T x = b with row exchanges: the block's result comes out in pivot
+    // order and is scattered to equation order (prow[q]: the block row at
+    // pivot position q), where the updates of the blocks above read it
+    __shared__ unsigned char prow[SNB];
+    const bool pv = TRANS && a.pivsrc;
+    const unsigned char *psrc = pv ? a.pivsrc + solve_matrix(a) * (size_t)a.s.n : nullptr;
     TileAcc<C, RT, B> acc;
     const int nblk = (c.s + SNB - 1) / SNB;
     for (int b = nblk - 1; b >= 0; --b) {
         const int k0 = b * SNB, kb = min(SNB, c.s - k0);
+        if (pv && threadIdx.x < kb) prow[threadIdx.x] = psrc[c.vars[k0 + threadIdx.x]];   // read after staged_sync
         stage_dinv<C, false, TRANS, RT, B>(sm, c.F, c.f, k0, kb);
         stage_rows(sm, [&](int q) { return xrow(k0 + q); }, kb, c.rn);
         staged_sync();
         zero_acc(acc);
         tile_mma<TRI_UPPER>(sm, kb, acc, kb, c.rn);   // x_b = Dinv t_b
         __syncthreads();
-        for_acc(acc, kb, c.rn, threadIdx.x, [&](int row, int col, const C &v) { sm.Y[row][col] = v; });
+        for_acc(acc, kb, c.rn, threadIdx.x, [&](int row, int col, const C &v) { sm.Y[pv ? prow[row] : row][col] = v; });
         __syncthreads();
         for (int t = threadIdx.x; t < kb * TC; t += NT) {
             const int q = t / TC, r = t % TC;

@@ -47,10 +47,10 @@ class Engine:
                  precision: int = GM_PREC_FP64, op_mode: int = GM_OP_REF, free_surf: int = 0,
                  a0_pml: float = 90.0, s: float = 0.0, device: int = 0, leaf_max: int = 32,
                  ir_tol: float = 1e-10, ir_max_iter: int = 10, refine: int = 0, gmres_restart: int = 0,
-                 tc_min_block: int = 0):
+                 tc_min_block: int = 0, pivot_tol: float = 0.0):
         self.lib = _lib.load()
         self.cfg = GmConfig(nx, ny, dh, npml, free_surf, a0_pml, s, physics, precision, op_mode, leaf_max,
-                            ir_tol, ir_max_iter, refine, gmres_restart, tc_min_block)
+                            ir_tol, ir_max_iter, refine, gmres_restart, tc_min_block, pivot_tol)
         self.nx, self.ny, self.n = nx, ny, nx * ny
         self.physics = physics
         self._h = ctypes.c_void_p()

@@ -82,6 +82,12 @@ typedef struct {
     int32_t gmres_restart;   /* GMRES iterations per cycle (0 = default 8, at most 8) */
     int32_t tc_min_block;    /* complex64: contribution blocks of at least this many rows
                                 update on the tcgen05 tensor cores (0 = none) */
+    double pivot_tol;        /* threshold partial pivoting on the levels factorised in
+                                32-pivot blocks (fronts with more than 32 pivots): within
+                                each block, row p is exchanged with the row of largest
+                                |entry| in column p when |pivot| < pivot_tol x that entry
+                                (0 = default 0.1, UMFPACK's default relative pivot
+                                tolerance; < 0 = static pivots only) */
 } gm_config;
 
 /* ---- refinement of the solves (gm_config.refine) ---- */
@@ -111,6 +117,7 @@ typedef struct {
     int64_t u_entries;          /* stored U entries (pivot rows) per frequency: the backward pass's factor */
     double ms_subst_bwd;        /* device time of the backward passes of those substitutions */
     int64_t tc_tiles;           /* output tiles of the factorisation routed to tcgen05 */
+    int64_t pivot_swaps;        /* row exchanges of the threshold pivoting since the last factor */
 } gm_stats;
 
 /* Refinement record of one matrix in the last solve (gm_solve and the solves
