@@ -595,8 +595,7 @@ void launch_factor_level(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
         cudaFuncSetAttribute(k_panel_mm<R>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         attr_set = true;
     }
-    // row exchanges on the levels the substitution solves by 32-pivot blocks
-    const int piv = a.pivsrc && a.pivtau2 > 0 && L.max_piv > NB;
+    const int piv = a.pivsrc && a.pivtau2 > 0;   // row exchanges (every level of this route)
     for_level_pieces(L, [&](int first, int count) {
         (k_diag<R><<<dim3(count, a.nf), DIAG_THREADS, DIAG_SCRATCH * sizeof(C), st>>>(a, first, piv), note_launch());
     });
@@ -977,6 +976,37 @@ namespace gm {
 // ---------------------------------------------------------------------
 constexpr int MID_FT = 256;   // threads per CTA, also the largest front handled
 
+// Warp 0 of k_factor_mid (which holds every pivot row): pivot position kp
+// goes to the row of largest |x[kp]| among the rows at positions >= kp when
+// the row there has |x[kp]|^2 < tau2 times that (c2: this lane's
+// |x[kp]|^2, pos: the pivot position of this lane's row; the two rows swap
+// positions).  Only scalars: the caller's row stays in registers.
+template <class R>
+__device__ __forceinline__ void mid_select_pivot(R c2, int &pos, int kp, int s, R tau2, int &nsw) {
+    const int lane = threadIdx.x & 31;
+    R m2 = pos >= kp && pos < s ? c2 : R(-1);
+    int arg = lane;
+#pragma unroll
+    for (int o = 16; o; o >>= 1) {
+        const R om = __shfl_xor_sync(0xffffffffu, m2, o);
+        const int oa = __shfl_xor_sync(0xffffffffu, arg, o);
+        if (om > m2 || (om == m2 && oa < arg)) {
+            m2 = om;
+            arg = oa;
+        }
+    }
+    m2 = __shfl_sync(0xffffffffu, m2, 0);     // lane 0's result for all (NaN entries
+    arg = __shfl_sync(0xffffffffu, arg, 0);   // could leave the lanes disagreeing)
+    const int cur = __ffs(__ballot_sync(0xffffffffu, pos == kp)) - 1;   // the lane at position kp
+    const R d2 = __shfl_sync(0xffffffffu, c2, cur);
+    if (arg != cur && d2 < tau2 * m2) {   // warp-uniform
+        const int pa = __shfl_sync(0xffffffffu, pos, arg);
+        if (lane == cur) pos = pa;
+        if (lane == arg) pos = kp;
+        ++nsw;
+    }
+}
+
 template <class R, int NPR>
 __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_first) {
     using C = cplx<R>;
@@ -984,6 +1014,7 @@ __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_
     __shared__ C Dinv[NB][NB + 1];
     __shared__ C urow[2][NPR];   // pivot row k at columns k .. s-1, alternating buffers
     __shared__ C rd[NPR];        // reciprocal pivots
+    __shared__ int perm[NB];     // front row at pivot position q (row exchanges)
     __shared__ int npert;
     const int node = a.s.lvl_nodes[lvl_first + blockIdx.x];
     const int f = a.s.nfront[node], s = a.s.npiv[node], m = f - s;
@@ -1001,13 +1032,23 @@ __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_
         cp_async_elem(U + r + j * ldu, F + r + (size_t)(s + j) * f);
     }
 
-    // 1. pivot columns, one row per thread
+    // 1. pivot columns, one row per thread.  Iteration k applies pivot k
+    // and publishes pivot k + 1: the row at pivot position k + 1 and the
+    // reciprocal.  Rows stay with their threads; pos is the pivot position
+    // of the thread's row (its own index but for exchanged pivot rows).
+    // With row exchanges (piv), warp 0 -- which holds every pivot row,
+    // s <= 32 -- first gives position k + 1 to the row r of largest
+    // |x_r[k+1]| among those at positions > k when the row there has
+    // |x[k+1]|^2 < pivtau2 |x_r[k+1]|^2 (the two rows swap positions); the
+    // rows go to shared memory at their positions afterwards.
     const bool own = tid < f;
+    const bool piv = a.pivsrc != nullptr && a.pivtau2 > 0;
     C x[NPR];
 #pragma unroll
     for (int j = 0; j < NPR; ++j) x[j] = (own && j < s) ? F[tid + (size_t)j * f] : czero<C>();
-    int np = 0;
-    if (tid == 0) {
+    int np = 0, nsw = 0, pos = tid;
+    if (piv && tid < 32) mid_select_pivot<R>(cabs2(x[0]), pos, 0, s, (R)a.pivtau2, nsw);
+    if (pos == 0) {
         x[0] = static_pivot<R>(x[0], pivtol, np);
         rd[0] = crcp(x[0]);
 #pragma unroll
@@ -1018,14 +1059,17 @@ __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_
 #pragma unroll
     for (int k = 0; k < NPR; ++k) {
         if (k >= s) continue;   // s is the same for the whole CTA
-        if (own && tid > k) {
+        if (own && pos > k) {
             const C l = cmul(x[k], rd[k]);
             x[k] = l;
 #pragma unroll
             for (int j = k + 1; j < NPR; ++j)
                 if (j < s) cfms(x[j], l, urow[k & 1][j]);
-            const int k1 = k + 1 < NPR ? k + 1 : NPR - 1;
-            if (k + 1 < NPR && tid == k + 1 && k + 1 < s) {   // owner of the next pivot row
+        }
+        const int k1 = k + 1 < NPR ? k + 1 : NPR - 1;   // pivot published by this iteration
+        if (k + 1 < NPR && k + 1 < s) {
+            if (piv && tid < 32) mid_select_pivot<R>(cabs2(x[k1]), pos, k1, s, (R)a.pivtau2, nsw);
+            if (pos == k1 && own) {   // the row at the next pivot position
                 x[k1] = static_pivot<R>(x[k1], pivtol, np);
                 rd[k1] = crcp(x[k1]);
 #pragma unroll
@@ -1038,17 +1082,20 @@ __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_
     if (own) {
 #pragma unroll
         for (int j = 0; j < NPR; ++j)
-            if (j < s) P[tid + j * ldp] = x[j];
+            if (j < s) P[pos + j * ldp] = x[j];
+        if (pos < s) perm[pos] = tid;
     }
     if (np) atomicAdd(&npert, np);
+    if (tid == 0 && nsw) atomicAdd(a.nswap, (unsigned long long)nsw);
     staged_sync();
+    if (piv && tid < s) a.pivsrc[(size_t)blockIdx.y * a.s.n + a.s.vars[a.s.var_off[node] + tid]] = (unsigned char)perm[tid];
 
     // 2. U12 = L11^-1 A12, one column per thread of warps 2 .. 7, while
     // warps 0 and 1 invert the pivot block's triangles (3.)
     for (int j = tid - 64; j >= 0 && j < m; j += MID_FT - 64) {
-        C u[NPR];
+        C u[NPR];   // A12's rows in pivot order
 #pragma unroll
-        for (int r = 0; r < NPR; ++r) u[r] = r < s ? U[r + j * ldu] : czero<C>();
+        for (int r = 0; r < NPR; ++r) u[r] = r < s ? U[(piv ? perm[r] : r) + j * ldu] : czero<C>();
 #pragma unroll
         for (int k = 0; k + 1 < NPR; ++k) {
             if (k + 1 < s) {
@@ -1059,7 +1106,7 @@ __global__ void __launch_bounds__(MID_FT) k_factor_mid(FactorArgs<R> a, int lvl_
             }
         }
 #pragma unroll
-        for (int r = 1; r < NPR; ++r)
+        for (int r = 0; r < NPR; ++r)
             if (r < s) U[r + j * ldu] = u[r];
     }
 
@@ -1119,6 +1166,15 @@ bool mid_factor_level(const LevelInfo &L) {
     return L.count > 0 && L.max_piv <= NB && L.max_front <= MID_FT && !small_factor_level<R>(L) &&
            (size_t)L.mid_words * sizeof(cplx<R>) <= MID_FACTOR_SMEM;
 }
+
+// Row exchanges happen on every level but those of the small-front kernel
+// (whose fronts fit shared memory whole: the lower levels)
+template <class R>
+bool level_pivots(const LevelInfo &L) {
+    return L.count > 0 && !small_factor_level<R>(L);
+}
+template bool level_pivots<double>(const LevelInfo &);
+template bool level_pivots<float>(const LevelInfo &);
 
 template <class R, int NPR>
 static void launch_mid(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st) {

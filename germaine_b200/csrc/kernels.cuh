@@ -112,6 +112,10 @@ void launch_factor_small(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_
 // block (replaces the K3 / K4 steps and the level's contribution GEMM).
 template <class R>
 bool mid_factor_level(const LevelInfo &L);
+// the level's factorisation exchanges rows (FactorArgs::pivsrc) when
+// pivoting is on: every level but the small-front kernel's
+template <class R>
+bool level_pivots(const LevelInfo &L);
 template <class R>
 void launch_factor_mid(const FactorArgs<R> &a, const LevelInfo &L, cudaStream_t st);
 

@@ -597,10 +597,18 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_fwd_small(SolveA
     const int s = c.s;   // <= SNB (launch condition)
 
     pivot_rhs(a, c, inv, W0, W1, r0, ldr);
+    // M x = b with row exchanges: the pivot rows' right-hand sides are taken
+    // in pivot order (prow[q]: the front row at pivot position q)
+    __shared__ unsigned char prow[SNB];
+    const bool pv = !TRANS && a.pivsrc;
+    if (pv) {
+        if (threadIdx.x < s) prow[threadIdx.x] = a.pivsrc[solve_matrix(a) * (size_t)a.s.n + c.vars[threadIdx.x]];
+        __syncthreads();
+    }
     TileAcc<C, RT, B> acc;
     if (s > 0) {
         stage_dinv<C, true, TRANS, RT, B>(sm, c.F, c.f, 0, s);
-        stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[q] * ldr; }, s, c.rn);
+        stage_rows(sm, [&](int q) { return c.X + (size_t)c.vars[pv ? prow[q] : q] * ldr; }, s, c.rn);
         staged_sync();
         zero_acc(acc);
         tile_mma<TRI_LOWER>(sm, s, acc, s, c.rn);   // y = Dinv x_piv
@@ -647,6 +655,12 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_bwd_small(SolveA
     if (c.rn <= 0 || c.s == 0) return;
     const size_t ldr = a.ldr;
     const int s = c.s;   // <= SNB (launch condition)
+    // M^T x = b with row exchanges: the result comes out in pivot order and
+    // is scattered to equation order (prow[q]: the front row at pivot
+    // position q; read after the staged_sync below)
+    __shared__ unsigned char prow[SNB];
+    const bool pv = TRANS && a.pivsrc;
+    if (pv && threadIdx.x < s) prow[threadIdx.x] = a.pivsrc[solve_matrix(a) * (size_t)a.s.n + c.vars[threadIdx.x]];
     TileAcc<C, RT, B> acc;
     zero_acc(acc);
     for (int j0 = s; j0 < c.f; j0 += SNB) {
@@ -676,7 +690,8 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_bwd_small(SolveA
     __syncthreads();
     zero_acc(acc);
     tile_mma<TRI_UPPER>(sm, s, acc, s, c.rn);   // x_piv = Dinv t
-    for_acc(acc, s, c.rn, threadIdx.x, [&](int row, int col, const C &v) { c.X[(size_t)c.vars[row] * ldr + col] = v; });
+    for_acc(acc, s, c.rn, threadIdx.x,
+            [&](int row, int col, const C &v) { c.X[(size_t)c.vars[pv ? prow[row] : row] * ldr + col] = v; });
 }
 
 template <class R, int RT, int B>
@@ -828,8 +843,10 @@ static void level_pass_rt(bool fwd, int rt, const SolveArgs<R> &a, const LevelIn
 // engine holds one (a.lvl_cfg, per level: forward rt, forward B, backward
 // rt, backward B; 0 = the default rule), else the default rules above.
 template <class R>
-static void dispatch(bool fwd, const SolveArgs<R> &a, const LevelInfo &L, cudaStream_t st) {
-    if (L.count == 0 || solve_nfz(a) <= 0) return;
+static void dispatch(bool fwd, const SolveArgs<R> &a_in, const LevelInfo &L, cudaStream_t st) {
+    if (L.count == 0 || solve_nfz(a_in) <= 0) return;
+    SolveArgs<R> a = a_in;
+    if (!level_pivots<R>(L)) a.pivsrc = nullptr;   // no row exchanges on this level
     if (a.lvl_cfg) {
         const int *c = a.lvl_cfg + 4 * L.index + (fwd ? 0 : 2);
         const int rt = c[0] ? c[0] : level_rt(L), b = c[1] ? c[1] : slice_b<R>(a.nrhs);
