@@ -82,12 +82,12 @@ typedef struct {
     int32_t gmres_restart;   /* GMRES iterations per cycle (0 = default 8, at most 8) */
     int32_t tc_min_block;    /* complex64: contribution blocks of at least this many rows
                                 update on the tcgen05 tensor cores (0 = none) */
-    double pivot_tol;        /* threshold partial pivoting on the levels factorised in
-                                32-pivot blocks (fronts with more than 32 pivots): within
-                                each block, row p is exchanged with the row of largest
-                                |entry| in column p when |pivot| < pivot_tol x that entry
-                                (0 = default 0.1, UMFPACK's default relative pivot
-                                tolerance; < 0 = static pivots only) */
+    double pivot_tol;        /* threshold partial pivoting inside the 32-pivot blocks of
+                                every front too large for the small-front kernel: row p
+                                is exchanged with the row of largest |entry| in column p
+                                (among the block's rows not yet pivoted) when |pivot| <
+                                pivot_tol x that entry (0 = default 0.1, UMFPACK's default
+                                relative pivot tolerance; < 0 = static pivots only) */
 } gm_config;
 
 /* ---- refinement of the solves (gm_config.refine) ---- */
