@@ -3,6 +3,7 @@
 // partial sums of |r|^2 and |b|^2, and the precision conversions of the
 // mixed-precision refinement loop.  HBM-bound: per row 9 operator values
 // (amortised over the right-hand sides) and x, b, r for each right-hand side.
+#include <cstdlib>
 #include "kernels.cuh"
 #include "cplx.cuh"
 
@@ -42,16 +43,24 @@ __device__ __forceinline__ double2 op_coef(const double2 *A9, int n, int nx, boo
 // into part[blockIdx.x][blockIdx.z][r][2].  OutC = double2 writes FP64;
 // OutC = float2 writes the refinement right-hand side directly in the
 // working precision of the substitution; WRITE = false forms the norms only.
-template <class InC, class OutC, bool WRITE, bool PRODUCT>
+// SEG = 1: lane = right-hand side r0 + lane, each warp walking its whole
+// line segment of the patch.  SEG > 1 (the last few right-hand sides, when
+// fewer than RLANES are left): lane = (segment, right-hand side), 32 / SEG
+// right-hand sides from r0, each lane walking PW / SEG points of its line
+// -- a warp instruction then serves SEG times the points where one lane per
+// right-hand side would leave most of the warp idle.
+template <class InC, class OutC, bool WRITE, bool PRODUCT, int SEG>
 __global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const InC *__restrict__ xin, OutC *out,
-                                                          double *part) {
+                                                          double *part, int r0) {
+    constexpr int RL = RLANES / SEG, SW = PW / SEG;   // right-hand sides per warp, points per lane
     __shared__ double2 cf[9][PL][PW];   // operator values, zero for neighbours outside the grid
     __shared__ double red[2][PL][RLANES];
     const int fz = blockIdx.z;
     const int f = a.fmap ? a.fmap[fz] : fz;
     const int ncb = (a.nx + PW - 1) / PW;
     const int x0 = (int)(blockIdx.x % ncb) * PW, y0 = (int)(blockIdx.x / ncb) * PL;
-    const int r = blockIdx.y * RLANES + threadIdx.x;
+    const int r = r0 + blockIdx.y * RL + threadIdx.x % RL;
+    const int seg = threadIdx.x / RL;
     const bool use_row = (a.op_mode == GM_OP_EXACT) != (a.trans != 0);
     const double2 *A9 = a.A + (size_t)f * 9 * a.n;
     {   // one grid point of the patch per thread: its operator values
@@ -73,8 +82,8 @@ __global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const I
     __syncthreads();
     double rr = 0.0, bb = 0.0;
     const int w = threadIdx.y, y = y0 + w;
-    const int xe = min(PW, a.nx - x0);   // grid columns of this patch
-    if (r < a.nrhs && y < a.ny) {
+    const int xs = seg * SW, xe = min(xs + SW, a.nx - x0);   // this lane's columns of the patch
+    if (r < a.nrhs && y < a.ny && xs < xe) {
         const size_t per = (size_t)a.n * a.ldr;
         const size_t base = (size_t)f * per + r;
         const size_t ldr = a.ldr;
@@ -86,7 +95,7 @@ __global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const I
         const int n = a.n, nx = a.nx;
         // x at flat index i, zero outside the array (such values are masked)
         auto ld = [&](int i) { return (i >= 0 && i < n) ? cto_d(X[(size_t)i * ldr]) : make_double2(0.0, 0.0); };
-        const int kb = y * nx + x0;   // flat index of the line segment's first point
+        const int kb = y * nx + x0 + xs;   // flat index of the lane's first point
         // window: wl[d] / wc[d] = x left of / at the current point on the
         // line above (d = 0), the same line (1) and the line below (2)
         double2 wl[3], wc[3];
@@ -95,18 +104,19 @@ __global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const I
             wl[d] = ld(kb - 1 + (d - 1) * nx);
             wc[d] = ld(kb + (d - 1) * nx);
         }
-        for (int c0 = 0; c0 < xe; c0 += RSTEP) {
+        const int ne = xe - xs;   // points of this lane
+        for (int c0 = 0; c0 < ne; c0 += RSTEP) {
             double2 wr[RSTEP][3];   // the right-hand columns of the next RSTEP points
 #pragma unroll
             for (int u = 0; u < RSTEP; ++u)
 #pragma unroll
                 for (int d = 0; d < 3; ++d)
-                    wr[u][d] = c0 + u < xe ? ld(kb + c0 + u + 1 + (d - 1) * nx) : make_double2(0.0, 0.0);
+                    wr[u][d] = c0 + u < ne ? ld(kb + c0 + u + 1 + (d - 1) * nx) : make_double2(0.0, 0.0);
 #pragma unroll
             for (int u = 0; u < RSTEP; ++u) {
-                const int lx = c0 + u;
-                if (lx >= xe) break;
-                const int k = kb + lx;
+                const int lx = xs + c0 + u;   // column in the patch
+                if (c0 + u >= ne) break;
+                const int k = kb + c0 + u;
                 double2 bv = make_double2(0.0, 0.0);
                 if (!PRODUCT) bv = spikes ? (k == ks ? amp : bv) : a.b[base + (size_t)k * ldr];
                 double2 acc = bv;
@@ -133,13 +143,15 @@ __global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const I
     red[0][w][threadIdx.x] = rr;
     red[1][w][threadIdx.x] = bb;
     __syncthreads();
-    if (threadIdx.y == 0 && r < a.nrhs) {
+    if (threadIdx.y == 0 && threadIdx.x < RL && r < a.nrhs) {   // fixed order: deterministic
         double s0 = 0.0, s1 = 0.0;
 #pragma unroll
-        for (int g = 0; g < PL; ++g) {
-            s0 += red[0][g][threadIdx.x];
-            s1 += red[1][g][threadIdx.x];
-        }
+        for (int g = 0; g < PL; ++g)
+#pragma unroll
+            for (int q = 0; q < SEG; ++q) {
+                s0 += red[0][g][q * RL + threadIdx.x];
+                s1 += red[1][g][q * RL + threadIdx.x];
+            }
         double *p = part + (((size_t)blockIdx.x * gridDim.z + fz) * a.nrhs + r) * 2;
         p[0] = s0;
         p[1] = s1;
@@ -148,16 +160,34 @@ __global__ void __launch_bounds__(RLANES *PL, 2) k_residual(ResidArgs a, const I
 
 static int resid_nfz(const ResidArgs &a) { return a.fmap ? a.nfz : a.nf; }
 
+// Full groups of RLANES right-hand sides, then the rest (at most 8) by the
+// segmented form; the partial sums land in the same slots either way.
 template <class InC, class OutC, bool WRITE, bool PRODUCT>
 static int launch_k6(const ResidArgs &a, const void *x, void *out, double *part, int max_blocks, cudaStream_t st) {
     const int nblk = residual_blocks(a.nx, a.ny);
     const int nfz = resid_nfz(a);
     if (nblk > max_blocks) return -1;
     if (nfz <= 0) return nblk;
-    dim3 grid(nblk, (a.nrhs + RLANES - 1) / RLANES, nfz);
-    (k_residual<InC, OutC, WRITE, PRODUCT><<<grid, dim3(RLANES, PL), 0, st>>>(
-         a, reinterpret_cast<const InC *>(x), reinterpret_cast<OutC *>(out), part),
-     note_launch());
+    static const bool no_tail = [] {   // GM_NO_TAIL_SLICE=1: one lane per right-hand side throughout
+        const char *v = std::getenv("GM_NO_TAIL_SLICE");
+        return v && std::atoi(v) != 0;
+    }();
+    const int rem = a.nrhs % RLANES;
+    const int tail = no_tail || rem == 0 || rem > 8 ? 0 : rem;
+    const int nfull = (a.nrhs - tail + RLANES - 1) / RLANES;
+    const InC *xi = reinterpret_cast<const InC *>(x);
+    OutC *o = reinterpret_cast<OutC *>(out);
+    if (nfull > 0)
+        (k_residual<InC, OutC, WRITE, PRODUCT, 1><<<dim3(nblk, nfull, nfz), dim3(RLANES, PL), 0, st>>>(a, xi, o, part, 0),
+         note_launch());
+    if (tail > 4)
+        (k_residual<InC, OutC, WRITE, PRODUCT, 4><<<dim3(nblk, 1, nfz), dim3(RLANES, PL), 0, st>>>(
+             a, xi, o, part, RLANES * nfull),
+         note_launch());
+    else if (tail > 0)
+        (k_residual<InC, OutC, WRITE, PRODUCT, 8><<<dim3(nblk, 1, nfz), dim3(RLANES, PL), 0, st>>>(
+             a, xi, o, part, RLANES * nfull),
+         note_launch());
     return nblk;
 }
 
@@ -261,10 +291,18 @@ template void launch_add_up_f<float>(double2 *, const void *, size_t, const int 
 // Loads the residual / conversion kernels (see preload_solve_kernels).
 void preload_refine_kernels() {
     cudaFuncAttributes fa;
-    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, double2, true, false>);
-    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, double2, false, false>);
-    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, float2, true, false>);
-    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, float2, false, false>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, double2, true, false, 1>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, double2, false, false, 1>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, float2, true, false, 1>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, float2, false, false, 1>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, double2, true, false, 4>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, double2, false, false, 4>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, float2, true, false, 4>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, float2, false, false, 4>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, double2, true, false, 8>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, double2, false, false, 8>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, float2, true, false, 8>);
+    cudaFuncGetAttributes(&fa, (const void *)k_residual<double2, float2, false, false, 8>);
     cudaFuncGetAttributes(&fa, (const void *)k_reduce_norms);
     cudaFuncGetAttributes(&fa, (const void *)k_convert_down<double>);
     cudaFuncGetAttributes(&fa, (const void *)k_convert_down<float>);
