@@ -175,9 +175,6 @@ struct SolveArgs {
     // block's right-hand-side rows through it, the backward pass of
     // M^T x = b scatters the block's solution rows through it
     const unsigned char *pivsrc;
-    // first right-hand side of slice 0 (a launch covering only the last
-    // columns; 0 otherwise)
-    int col0;
 };
 
 // right-hand sides per substitution slice for nrhs right-hand sides

@@ -331,7 +331,7 @@ __device__ __forceinline__ Ctx<R> make_ctx(const SolveArgs<R> &a, int lvl_first,
     c.node = a.s.lvl_nodes[lvl_first + (pos < 0 ? (int)blockIdx.y : pos)];
     c.f = a.s.nfront[c.node];
     c.s = a.s.npiv[c.node];
-    const int r0 = a.col0 + chunk * TC;
+    const int r0 = chunk * TC;
     c.rn = min(TC, a.nrhs - r0);
     const size_t fz = solve_matrix(a), xz = solve_slot(a);
     c.F = reinterpret_cast<const C *>(a.front) + fz * a.s.front_total + a.s.front_off[c.node];
@@ -678,8 +678,7 @@ __global__ void __launch_bounds__(NT, sizeof(R) == 8 ? 6 : 1) k_bwd_small(SolveA
         for (int t = threadIdx.x; t < s * TC; t += NT) {
             const int q = t / TC, r = t % TC;
             if (r >= c.rn) continue;
-            if (col_live(a, c.node, a.col0 + blockIdx.x * TC + r))
-                cp_async_elem(&sm.Y[q][r], c.X + (size_t)c.vars[q] * ldr + r);
+            if (col_live(a, c.node, blockIdx.x * TC + r)) cp_async_elem(&sm.Y[q][r], c.X + (size_t)c.vars[q] * ldr + r);
             else sm.Y[q][r] = czero<C>();
         }
     } else {
@@ -795,32 +794,11 @@ static void backward_level(const SolveArgs<R> &a, const LevelInfo &L, cudaStream
     const size_t smem = solve_smem<R, RT, B>();
     const int nchunk = (a.nrhs + 8 * B - 1) / (8 * B);
     static const bool no_small = env_int("GM_NO_BWD_SMALL") != 0;
-    static const bool no_tail = env_int("GM_NO_TAIL_SLICE") != 0;
     if (RT == 32 && L.max_piv <= SNB && !no_small) {   // one pivot block per front: fused ring + pivot kernel
-        // A last 32-column slice holding at most 8 right-hand sides (100
-        // shots: 4) costs a CTA as long as a full one -- these kernels are
-        // latency-bound -- so on the wide levels the last 32 + rem columns go
-        // to one 40-wide slice instead.  Measured at 841 x 227, 100 shots:
-        // levels 0-3 (1024-6680 fronts) 5.11 -> 4.90 ms, level 4 (512)
-        // 0.393 -> 0.384 ms; on the levels of 256 and 128 fronts slower.
-        const int rem = a.nrhs % 32;
-        const bool tail = B == 4 && !no_tail && L.count >= 512 && a.nrhs > 32 && rem > 0 && rem <= 8;
-        const int nfull = tail ? a.nrhs / 32 - 1 : nchunk;
         for_level_pieces(L, [&](int first, int count) {
-            if (nfull > 0) {
-                dim3 g(nfull, count, solve_nfz(a));
-                if (a.trans) (k_bwd_small<R, true, B><<<g, NT, smem, st>>>(a, first), note_launch());
-                else (k_bwd_small<R, false, B><<<g, NT, smem, st>>>(a, first), note_launch());
-            }
-            if (tail) {
-                SolveArgs<R> t = a;
-                t.col0 = 32 * nfull;
-                set_attrs<R, 32, 5>();
-                const size_t smem5 = solve_smem<R, 32, 5>();
-                dim3 g(1, count, solve_nfz(a));
-                if (a.trans) (k_bwd_small<R, true, 5><<<g, NT, smem5, st>>>(t, first), note_launch());
-                else (k_bwd_small<R, false, 5><<<g, NT, smem5, st>>>(t, first), note_launch());
-            }
+            dim3 g(nchunk, count, solve_nfz(a));
+            if (a.trans) (k_bwd_small<R, true, B><<<g, NT, smem, st>>>(a, first), note_launch());
+            else (k_bwd_small<R, false, B><<<g, NT, smem, st>>>(a, first), note_launch());
         });
         return;
     }
