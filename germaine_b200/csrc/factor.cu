@@ -8,10 +8,12 @@
 //                  (extend-add by inverse maps: deterministic, no atomics),
 //   K2 scatter  -- adds the operator entries owned by the front,
 //   K3 diag     -- per NB-wide pivot block: LU of the diagonal block with
-//                  static pivoting and the inverses of its two triangles,
-//                  factored once per front (the first block by k_diag, each
-//                  later one by the first CTA of the preceding K4),
-//   K3 panels   -- L21 = A21 U11^-1 and U12 = L11^-1 A12 as products with
+//                  threshold partial pivoting inside the block (static
+//                  pivots as the last resort) and the inverses of its two
+//                  triangles, factored once per front (the first block by
+//                  k_diag, each later one by the first CTA of the preceding
+//                  K4),
+//   K3 panels   -- L21 = A21 U11^-1 and U12 = L11^-1 P A12 as products with
 //                  those inverses (FP64 matrix instructions in complex128),
 //   K4 update   -- rank-NB Schur update of the pivot rows and columns still
 //                  to come, 64x64 tiles.
@@ -19,7 +21,10 @@
 // front holds L (unit lower) and U in its first npiv rows/columns -- except
 // that each NB x NB diagonal block holds the INVERSES of its two triangles
 // (what the substitution multiplies by) -- and its Schur complement (the
-// contribution block) in the trailing block.
+// contribution block) in the trailing block.  With row exchanges, the rows
+// of a block's diagonal block and U part are in pivot order, its rows'
+// multipliers of earlier blocks in equation order, and the block's
+// permutation is in FactorArgs::pivsrc.
 //
 // Two fused kernels leave the same layout on the levels where they pay:
 //   k_factor_small  fronts that fit shared memory whole (the lower levels):
@@ -969,7 +974,7 @@ namespace gm {
 //   5. applies the rank-s Schur update to the contribution block,
 //      64 x 64 tiles of 4 x 4 complex per thread, each tile's old values
 //      loaded into the accumulators first.
-// This replaces k_panel / k_update and the level's contribution GEMM.
+// This replaces the K3 / K4 steps and the level's contribution GEMM.
 // Shared memory: P[i + c * (f + 1)] the pivot columns, then
 // U[r + j * (s | 1)] the U12 rows (odd strides: conflict-free 16-byte
 // accesses).
