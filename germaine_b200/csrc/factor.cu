@@ -487,16 +487,17 @@ __global__ void __launch_bounds__(256) k_update(FactorArgs<R> a, int lvl_first, 
         const int col = t / NB, cc = t % NB;   // U: contiguous along the pivot index
         if (cc < kb && col < ncols) cp_async_elem(Us + cc * TSTR + col, F + (k0 + cc) + (size_t)(c0 + col) * f);
     }
-    staged_sync();
+    // the tile's current values go into the accumulators while the staged
+    // operands land (read after the products, their latency was exposed)
     Tile64<C, sizeof(R) == 8> acc;
-    for_tile64(acc, threadIdx.x, [](int, int, C &v) { v = czero<C>(); });
-    mma64<false>(Ls, TSTR, 1, Us, TSTR, 1, kb, mrows, ncols, acc, threadIdx.x);
+    auto mine = [&](int rr, int cc) { return rr < mrows && cc < ncols && (r0 + rr < s || c0 + cc < s); };
     for_tile64(acc, threadIdx.x, [&](int rr, int cc, C &v) {
-        const int row = r0 + rr, col = c0 + cc;
-        if (rr < mrows && cc < ncols && (row < s || col < s)) {
-            C &d = F[row + (size_t)col * f];
-            d = csub(d, v);
-        }
+        v = mine(rr, cc) ? F[(r0 + rr) + (size_t)(c0 + cc) * f] : czero<C>();
+    });
+    staged_sync();
+    mma64<true>(Ls, TSTR, 1, Us, TSTR, 1, kb, mrows, ncols, acc, threadIdx.x);
+    for_tile64(acc, threadIdx.x, [&](int rr, int cc, C &v) {
+        if (mine(rr, cc)) F[(r0 + rr) + (size_t)(c0 + cc) * f] = v;
     });
     if (blockIdx.x == 0) {
         // the first tile holds the next diagonal block, now final: factor it
