@@ -272,13 +272,22 @@ static int assemble_batch(gm_engine *e) {
 // their output tiles: tcgen05 tiles (128 x 64) for the complex64 path on
 // levels whose blocks are large enough to fill them, CUDA-core tiles
 // (64 x 64) otherwise.
-// Levels of fronts with at most NB pivots that are too large for the small
+// Levels of fronts with at most 16 pivots that are too large for the small
 // kernel go to the fused mid-level kernel; GM_NO_FACTOR_MID=1 keeps them on
-// the blocked panel / update / contribution-GEMM sequence.
+// the blocked diagonal / panel / contribution-GEMM sequence.  With 17-32
+// pivots the fused kernel holds 32-entry pivot rows in registers and fits
+// one CTA per SM; measured at 841 x 227 (10 frequencies) the blocked
+// sequence is faster there (levels 5-6, 26-28 pivots: 1.64 -> 1.26 and
+// 1.22 -> 1.10 ms) and slower with 14 pivots (level 4: 1.05 vs 1.39 ms).
+// GM_MID_MAX_PIV=<n> moves the limit (32: every level the kernel takes).
 template <class R>
 static bool use_mid_factor(const LevelInfo &L) {
     static const bool off = std::getenv("GM_NO_FACTOR_MID") != nullptr;
-    return !off && mid_factor_level<R>(L);
+    static const int max_piv = [] {
+        const char *v = std::getenv("GM_MID_MAX_PIV");
+        return v ? std::atoi(v) : 16;
+    }();
+    return !off && L.max_piv <= max_piv && mid_factor_level<R>(L);
 }
 
 template <class R>
