@@ -25,7 +25,7 @@ extern "C" {
 
 /* ---- status codes (UMFPACK_OK / _WARNING_singular_matrix / _ERROR_*) ---- */
 #define GM_OK                     0
-#define GM_WARNING_PERTURBED      1  /* static pivots were perturbed (tiny or zero pivot) */
+#define GM_WARNING_PERTURBED      1  /* pivots were perturbed (tiny or zero pivot) */
 #define GM_WARNING_NOT_CONVERGED  2  /* refinement stopped above the residual target */
 #define GM_ERROR_OUT_OF_MEMORY   -1
 #define GM_ERROR_INVALID         -2  /* bad argument */
@@ -107,7 +107,7 @@ typedef struct {
     int64_t factor_entries;     /* stored L+U entries per frequency */
     double factor_flops;        /* real flops per frequency (complex FMA = 8) */
     double solve_flops_per_rhs; /* real flops per right-hand side (fwd + bwd) */
-    int64_t perturbed_pivots;   /* static pivots replaced since the last factor */
+    int64_t perturbed_pivots;   /* tiny pivots replaced since the last factor */
     int32_t ir_iterations;      /* refinement sweeps of the last solve */
     double ir_residual;         /* max relative residual after the last solve */
     double ms_assemble, ms_factor, ms_solve, ms_refine;  /* device time of the last calls */
@@ -163,7 +163,7 @@ int gm_set_models(gm_engine *e, int nmod, const float *mat0, const float *mat1);
 /* Assemble and factorise the impedance matrices of nfreq frequencies as one
  * batch: init_A_{AC,SH,TE}_9p_pml (src/AC/init_A_AC_9p_pml.c:17) +
  * umfpack_zi_numeric (src/AC/forward_shot_AC.c:61), all frequencies at once.
- * Returns GM_WARNING_PERTURBED if static pivots had to be replaced. */
+ * Returns GM_WARNING_PERTURBED if tiny pivots had to be replaced. */
 int gm_factor(gm_engine *e, int nfreq, const float *h_freqs);
 
 /* gm_factor over nmat matrices, matrix m assembled at frequency h_freqs[m]

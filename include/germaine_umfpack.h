@@ -26,9 +26,12 @@
  *    {0, 1, NX, NX+1}; any other pattern returns
  *    UMFPACK_ERROR_invalid_matrix.  The ordering is the engine's geometric
  *    nested dissection, not AMD/COLAMD.
- *  - umfpack_zi_numeric factorises with static pivoting (no row
- *    interchanges); a replaced tiny pivot returns
- *    UMFPACK_WARNING_singular_matrix, like UMFPACK's zero-pivot warning.
+ *  - umfpack_zi_numeric factorises with threshold partial pivoting at
+ *    UMFPACK's default relative tolerance 0.1, restricted to row exchanges
+ *    inside each front's 32-pivot blocks (the smallest fronts, at the
+ *    leaves of the tree, keep static pivots); a pivot that is still tiny is
+ *    replaced and returns UMFPACK_WARNING_singular_matrix, like UMFPACK's
+ *    zero-pivot warning.
  *  - umfpack_zi_solve supports sys = UMFPACK_A, UMFPACK_At (conjugate
  *    transpose) and UMFPACK_Aat (array transpose); the partial systems
  *    (L, U, P...) return UMFPACK_ERROR_invalid_system.  Every solve ends
