@@ -215,10 +215,11 @@ __device__ __forceinline__ cplx<R> static_pivot(cplx<R> piv, R pivtol, int &nper
 }
 
 // LU of the kb x kb diagonal block at (k0, k0) of the front F (leading
-// dimension f) with static pivoting; the inverses of its two triangles are
-// written back in its place (all that the panel products and the
-// substitution use): L^-1 in the strict lower part (unit diagonal implied),
-// U^-1 in the upper part with the diagonal.
+// dimension f), with threshold row exchanges inside the block or without
+// (below), a pivot that stays tiny replaced as static_pivot does; the
+// inverses of its two triangles are written back in its place (all that
+// the panel products and the substitution use): L^-1 in the strict lower
+// part (unit diagonal implied), U^-1 in the upper part with the diagonal.
 //
 // The inverses are built during the elimination, one rank-1 step per pivot
 // p over every entry outside the leading (p+1) x (p+1) block, with l = the
@@ -964,11 +965,13 @@ namespace gm {
 // large for the small kernel's whole-front tile.  After the extend-add
 // gather and the operator entries (K2), one CTA per front and frequency
 //   1. factorises the pivot columns (f x s) right-looking with each thread
-//      holding one front row in registers: per pivot, the owner of the next
-//      pivot row applies the static pivoting of factor_diag_block and publishes the
-//      row and the pivot's reciprocal in shared memory, so one barrier per
-//      pivot and no shared-memory traffic for the update itself;
-//   2. solves L11 U12 = A12 with each thread holding one column of U12;
+//      holding one front row in registers: per pivot, warp 0 picks the
+//      pivot row by the threshold rule (mid_select_pivot: rows keep their
+//      threads and trade pivot positions), and the row's owner replaces a
+//      pivot that stays tiny as static_pivot does and publishes the row and
+//      the pivot's reciprocal in shared memory, so no shared-memory traffic
+//      for the update itself;
+//   2. solves L11 U12 = P A12 with each thread holding one column of U12;
 //   3. inverts the pivot block's two triangles;
 //   4. writes L, U and the inverses back (the layout the blocked path
 //      leaves);
