@@ -1,7 +1,9 @@
-"""Frequency sharding with one gradient all-reduce (germaine_b200/sharding.py):
-the rank shares follow init_MPIfreq (src/init_MPIfreq.c:20-31), and the
-sharded misfit / FP64 gradient over gloo ranks on CPU equals the
-single-process result.  The per-rank evaluation in the CPU tests is the FP64
+"""Frequency sharding with one gradient all-reduce or one seismogram gather
+(germaine_b200/sharding.py): the rank shares follow init_MPIfreq
+(src/init_MPIfreq.c:20-31), the sharded misfit / FP64 gradient over gloo
+ranks on CPU equals the single-process result, and the gathered
+seismograms equal write_seis_AC's sum of zero-filled arrays
+(src/AC/write_seis_AC.c:33-45) and the single-process forward.  The per-rank evaluation in the CPU tests is the FP64
 oracle (SuperLU + FP64 restatements); on the GPU it is the engine, with the
 all-reduce over NCCL."""
 import os
@@ -11,7 +13,8 @@ import tempfile
 import numpy as np
 import pytest
 
-from germaine_b200.sharding import frequency_range, local_frequencies, sharded_grad_obj
+from germaine_b200.sharding import (frequency_range, gather_seismograms, local_frequencies, sharded_forward,
+                                    sharded_grad_obj)
 
 
 def init_mpifreq(nf, nprocfreq, myid_shot):
@@ -145,3 +148,119 @@ def test_sharded_engine_gradient_over_nccl():
     r0, _, rl2 = _oracle_local(g, vp, rho, xs, ys, rx, ry, obs)(freqs)
     assert np.linalg.norm(g0 - r0) <= 1e-8 * np.linalg.norm(r0)
     assert abs(l2 - rl2) <= 2e-6 * abs(rl2)
+
+
+def _seis_block(f, nshots, ntr):
+    """Seeded seismograms of frequency index f, with a few signed zeros."""
+    rng = np.random.default_rng(100 + f)
+    s = (rng.standard_normal((nshots, ntr)) + 1j * rng.standard_normal((nshots, ntr))).astype(np.complex64)
+    s[0, 0] = np.complex64(complex(-0.0, -0.0))
+    s[-1, -1] = np.complex64(complex(0.0, -0.0))
+    return s
+
+
+def _gather_worker(rank, world, port, out_dir, nf, nshots, ntr):
+    import torch.distributed as dist
+    import datetime
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        lo, hi = frequency_range(nf, world, rank)
+        loc = np.stack([_seis_block(f, nshots, ntr) for f in range(lo, hi)]) if hi > lo else None
+        out = gather_seismograms(loc, nf, nshots, ntr, dist)
+        np.save(os.path.join(out_dir, f"s{rank}.npy"), out)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world,nf", [(2, 3), (3, 4), (4, 3)], ids=["w2-nf3", "w3-nf4", "w4-nf3-idle-rank"])
+def test_gather_seismograms_gloo_equals_reference_sum(world, nf):
+    """Uneven shares and a rank without frequencies; every rank ends with
+    what summing zero-filled full arrays over the ranks gives, bit for bit
+    (signed zeros included)."""
+    import torch.multiprocessing as tmp
+    nshots, ntr = 3, 5
+    with tempfile.TemporaryDirectory() as d:
+        tmp.spawn(_gather_worker, args=(world, _free_port(), d, nf, nshots, ntr), nprocs=world, join=True)
+        res = [np.load(os.path.join(d, f"s{r}.npy")) for r in range(world)]
+    ref = np.zeros((nf, nshots, ntr), np.complex64)   # write_seis_AC: sum of each rank's zero-filled array
+    for r in range(world):
+        lo, hi = frequency_range(nf, world, r)
+        part = np.zeros_like(ref)
+        for f in range(lo, hi):
+            part[f] = _seis_block(f, nshots, ntr)
+        ref = ref + part
+    for out in res:
+        assert out.shape == (nf, nshots, ntr)
+        assert out.view(np.uint32).tobytes() == ref.view(np.uint32).tobytes()
+
+
+def _oracle_forward_local(g, vp, rho, xs, ys, rx, ry):
+    from tests.test_gpu_forward_grad import oracle_forward
+    from oracle import sparse as OS
+    idx = [OS.receiver_read_index(g, int(a), int(b)) for a, b in zip(rx, ry)]
+
+    def run(local):
+        if not local:
+            return None
+        X, _ = oracle_forward(g, 1, vp, rho, local, xs, ys)
+        return np.stack([OS.vec2mat(X[i].T)[:, idx] for i in range(len(local))]).astype(np.complex64)
+    return run
+
+
+def _forward_worker(rank, world, port, out_dir):
+    import torch.distributed as dist
+    import datetime
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
+    try:
+        g, vp, rho, xs, ys, rx, ry, freqs = _case()
+        seis = sharded_forward(freqs, _oracle_forward_local(g, vp, rho, xs, ys, rx, ry), xs.size, rx.size, dist)
+        np.save(os.path.join(out_dir, f"f{rank}.npy"), seis)
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 4])
+def test_sharded_forward_gloo_equals_single_process(world):
+    """world 2: shares of 2 and 1 frequencies; world 4: one rank has none."""
+    import torch.multiprocessing as tmp
+    with tempfile.TemporaryDirectory() as d:
+        tmp.spawn(_forward_worker, args=(world, _free_port(), d), nprocs=world, join=True)
+        res = [np.load(os.path.join(d, f"f{r}.npy")) for r in range(world)]
+    g, vp, rho, xs, ys, rx, ry, freqs = _case()
+    ref = _oracle_forward_local(g, vp, rho, xs, ys, rx, ry)(freqs) + np.complex64(0)
+    for out in res:
+        assert np.array_equal(out, ref)
+
+
+@pytest.mark.gpu
+def test_sharded_engine_forward_over_nccl():
+    """One rank over NCCL on cuda:0: the gathered seismograms (device
+    buffers) are the engine's own block, bit for bit, and match the
+    oracle."""
+    import datetime
+    import torch
+    import torch.distributed as dist
+    from germaine_b200 import Engine
+    from germaine_b200.sharding import engine_forward
+    g, vp, rho, xs, ys, rx, ry, freqs = _case()
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(_free_port())
+    dist.init_process_group("nccl", rank=0, world_size=1, timeout=datetime.timedelta(seconds=60))
+    try:
+        with Engine(g.nx, g.ny, g.dh, g.npml, leaf_max=32) as e:
+            e.set_model(vp, rho)
+            run, blocks = engine_forward(e, xs, ys, rx, ry), []
+
+            def local(fs):
+                blocks.append(run(fs))
+                return blocks[-1]
+            seis = sharded_forward(freqs, local, xs.size, rx.size, dist, device=torch.device("cuda", 0))
+    finally:
+        dist.destroy_process_group()
+    assert np.array_equal(seis, blocks[0])
+    ref = _oracle_forward_local(g, vp, rho, xs, ys, rx, ry)(freqs)
+    assert np.linalg.norm(seis - ref) <= 2e-6 * np.linalg.norm(ref)
