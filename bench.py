@@ -107,30 +107,18 @@ def _cpu_rank(args):
     return time.perf_counter() - t0, tf, ts, len(freqs) * len(shots)
 
 
-def split_range(count: int, parts: int, me: int) -> range:
-    """The reference's block split of `count` items over `parts` ranks
-    (init_MPIfreq.c:20-31, init_MPIshot.c:20-31), 0-based."""
-    lo = (count // parts) * me
-    if count % parts > me:
-        lo += me
-        hi = lo + count // parts + 1
-    else:
-        lo += count % parts
-        hi = lo + count // parts
-    return range(lo, hi)
-
-
 def rank_work(nprocfreq: int, nprocshot: int, nshots: int):
     """Per-rank (frequencies, shots) of the reference's layout: rank MYID in
     colour MYID / NPROCFREQ takes the shot block of its colour and the
-    frequency block of its rank in the colour (fwi_FD_AC.c:201-211)."""
+    frequency block of its rank in the colour (fwi_FD_AC.c:201-211,
+    init_MPIfreq.c:20-31, init_MPIshot.c:20-31)."""
+    from germaine_b200.sharding import rank_blocks
     fl = freqs_hz()
+    world = nprocfreq * nprocshot
     work = []
-    for myid in range(nprocfreq * nprocshot):
-        color, myid_shot = myid // nprocfreq, myid % nprocfreq
-        fr = [fl[i] for i in split_range(len(fl), nprocfreq, myid_shot)]
-        sh = list(split_range(nshots, nprocshot, color))
-        work.append((fr, sh))
+    for myid in range(world):
+        (flo, fhi), (slo, shi) = rank_blocks(len(fl), nshots, world, myid, nprocfreq)
+        work.append((fl[flo:fhi], list(range(slo, shi))))
     return work
 
 

@@ -13,8 +13,8 @@ import tempfile
 import numpy as np
 import pytest
 
-from germaine_b200.sharding import (frequency_range, gather_seismograms, local_frequencies, sharded_forward,
-                                    sharded_grad_obj)
+from germaine_b200.sharding import (frequency_range, gather_seismograms, local_frequencies, rank_blocks,
+                                    sharded_forward, sharded_grad_obj)
 
 
 def init_mpifreq(nf, nprocfreq, myid_shot):
@@ -46,6 +46,42 @@ def test_frequency_range_rejects_bad_rank():
         frequency_range(4, 2, 2)
 
 
+def init_mpishot(nshots, nprocshot, color):
+    """NSHOT1, NSHOT2 (1-based, half-open) as src/init_MPIshot.c:20-31 computes them."""
+    nshot1 = (nshots // nprocshot) * color
+    if nshots % nprocshot > color:
+        nshot1 += color
+        nshot2 = nshot1 + nshots // nprocshot + 1
+    else:
+        nshot1 += nshots % nprocshot
+        nshot2 = nshot1 + nshots // nprocshot
+    return nshot1 + 1, nshot2 + 1
+
+
+@pytest.mark.parametrize("world,nprocfreq", [(1, 1), (4, 2), (6, 3), (6, 1), (8, 8), (8, 2)])
+@pytest.mark.parametrize("nf,nshots", [(10, 100), (3, 7), (1, 5)])
+def test_rank_blocks_is_reference_layout(world, nprocfreq, nf, nshots):
+    """COLOR = MYID / NPROCFREQ, MYID_SHOT = MYID % NPROCFREQ
+    (src/AC/fwi_FD_AC.c:201-211); every (frequency, shot) pair on exactly
+    one rank."""
+    seen = np.zeros((nf, nshots), int)
+    for myid in range(world):
+        (flo, fhi), (slo, shi) = rank_blocks(nf, nshots, world, myid, nprocfreq)
+        color, myid_shot = myid // nprocfreq, myid % nprocfreq
+        n1, n2 = init_mpifreq(nf, nprocfreq, myid_shot)
+        s1, s2 = init_mpishot(nshots, world // nprocfreq, color)
+        assert (flo, fhi, slo, shi) == (n1 - 1, n2 - 1, s1 - 1, s2 - 1)
+        seen[flo:fhi, slo:shi] += 1
+    assert np.all(seen == 1)
+
+
+def test_rank_blocks_rejects_uneven_layout():
+    with pytest.raises(ValueError):
+        rank_blocks(10, 100, 6, 0, 4)
+    with pytest.raises(ValueError):
+        rank_blocks(10, 100, 4, 4, 2)
+
+
 def _free_port():
     with socket.socket() as s:
         s.bind(("127.0.0.1", 0))
@@ -71,11 +107,12 @@ def _case():
 def _oracle_local(g, vp, rho, xs, ys, rx, ry, obs_by_freq):
     from tests.test_gpu_forward_grad import oracle_grad
 
-    def run(local):
-        if not local:
+    def run(local, shots=None):
+        sel = slice(None) if shots is None else slice(shots.start, shots.stop)
+        if not local or (shots is not None and len(shots) == 0):
             return np.zeros(g.n), None, 0.0
-        obs = np.stack([obs_by_freq[f] for f in local])
-        g0, _, l2 = oracle_grad(g, 1, vp, rho, local, xs, ys, rx, ry, obs, 0, 1)
+        obs = np.stack([obs_by_freq[f][sel] for f in local])
+        g0, _, l2 = oracle_grad(g, 1, vp, rho, local, xs[sel], ys[sel], rx, ry, obs, 0, 1)
         return g0, None, l2
     return run
 
@@ -86,7 +123,7 @@ def _observed(g, vp, rho, xs, ys, rx, ry, freqs):
     return {f: obs[i] for i, f in enumerate(freqs)}
 
 
-def _worker(rank, world, port, out_dir):
+def _worker(rank, world, port, out_dir, npf=None):
     import torch.distributed as dist
     import datetime
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -95,18 +132,22 @@ def _worker(rank, world, port, out_dir):
     try:
         g, vp, rho, xs, ys, rx, ry, freqs = _case()
         obs = _observed(g, vp, rho, xs, ys, rx, ry, freqs)
-        g0, _, l2 = sharded_grad_obj(freqs, _oracle_local(g, vp, rho, xs, ys, rx, ry, obs), dist)
+        g0, _, l2 = sharded_grad_obj(freqs, _oracle_local(g, vp, rho, xs, ys, rx, ry, obs), dist,
+                                     nshots=xs.size, nprocfreq=npf)
         np.save(os.path.join(out_dir, f"g{rank}.npy"), np.append(g0, l2))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_sharded_gradient_gloo_equals_single_process(world):
-    """world 2: shares of 2 and 1 frequencies; world 4: one rank has none."""
+@pytest.mark.parametrize("world,npf", [(2, None), (4, None), (4, 2), (6, 2)],
+                         ids=["w2", "w4-idle-rank", "w4-2x2-shots", "w6-2x3-shots"])
+def test_sharded_gradient_gloo_equals_single_process(world, npf):
+    """world 2: shares of 2 and 1 frequencies; world 4: one rank has none;
+    2 x 2 and 2 x 3: two frequency blocks with their 3 shots split over 2 or
+    3 ranks (the reference's NPROCSHOT)."""
     import torch.multiprocessing as tmp
     with tempfile.TemporaryDirectory() as d:
-        tmp.spawn(_worker, args=(world, _free_port(), d), nprocs=world, join=True)
+        tmp.spawn(_worker, args=(world, _free_port(), d, npf), nprocs=world, join=True)
         res = [np.load(os.path.join(d, f"g{r}.npy")) for r in range(world)]
     g, vp, rho, xs, ys, rx, ry, freqs = _case()
     obs = _observed(g, vp, rho, xs, ys, rx, ry, freqs)
@@ -127,7 +168,9 @@ def test_local_frequencies_slices():
 @pytest.mark.gpu
 def test_sharded_engine_gradient_over_nccl():
     """One rank over NCCL on cuda:0: the all-reduce of the engine's FP64
-    gradient (device buffer) returns it unchanged and equals the oracle."""
+    gradient (device buffer) returns it unchanged and equals the oracle; the
+    engine's share over two shot blocks (what two ranks of one frequency
+    block evaluate) sums to the whole."""
     import datetime
     import torch
     import torch.distributed as dist
@@ -141,10 +184,14 @@ def test_sharded_engine_gradient_over_nccl():
     try:
         with Engine(g.nx, g.ny, g.dh, g.npml, leaf_max=32) as e:
             e.set_model(vp, rho)
-            g0, _, l2 = sharded_grad_obj(freqs, engine_grad_obj(e, xs, ys, rx, ry, obs), dist,
-                                         device=torch.device("cuda", 0))
+            run = engine_grad_obj(e, xs, ys, rx, ry, obs)
+            g0, _, l2 = sharded_grad_obj(freqs, run, dist, device=torch.device("cuda", 0))
+            ga, _, la = run(freqs, range(0, 2))
+            gb, _, lb = run(freqs, range(2, 3))
     finally:
         dist.destroy_process_group()
+    assert np.linalg.norm(ga + gb - g0) <= 1e-10 * np.linalg.norm(g0)
+    assert abs(la + lb - l2) <= 1e-5 * abs(l2)
     r0, _, rl2 = _oracle_local(g, vp, rho, xs, ys, rx, ry, obs)(freqs)
     assert np.linalg.norm(g0 - r0) <= 1e-8 * np.linalg.norm(r0)
     assert abs(l2 - rl2) <= 2e-6 * abs(rl2)
@@ -159,37 +206,39 @@ def _seis_block(f, nshots, ntr):
     return s
 
 
-def _gather_worker(rank, world, port, out_dir, nf, nshots, ntr):
+def _gather_worker(rank, world, port, out_dir, nf, nshots, ntr, npf):
     import torch.distributed as dist
     import datetime
     os.environ["MASTER_ADDR"] = "127.0.0.1"
     os.environ["MASTER_PORT"] = str(port)
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
-        lo, hi = frequency_range(nf, world, rank)
-        loc = np.stack([_seis_block(f, nshots, ntr) for f in range(lo, hi)]) if hi > lo else None
-        out = gather_seismograms(loc, nf, nshots, ntr, dist)
+        (lo, hi), (slo, shi) = rank_blocks(nf, nshots, world, rank, npf)
+        loc = np.stack([_seis_block(f, nshots, ntr)[slo:shi] for f in range(lo, hi)]) if hi > lo else None
+        out = gather_seismograms(loc, nf, nshots, ntr, dist, nprocfreq=npf)
         np.save(os.path.join(out_dir, f"s{rank}.npy"), out)
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world,nf", [(2, 3), (3, 4), (4, 3)], ids=["w2-nf3", "w3-nf4", "w4-nf3-idle-rank"])
-def test_gather_seismograms_gloo_equals_reference_sum(world, nf):
-    """Uneven shares and a rank without frequencies; every rank ends with
-    what summing zero-filled full arrays over the ranks gives, bit for bit
-    (signed zeros included)."""
+@pytest.mark.parametrize("world,nf,nshots,npf", [(2, 3, 3, None), (3, 4, 3, None), (4, 3, 3, None), (4, 3, 5, 2),
+                                                 (6, 2, 7, 3)],
+                         ids=["w2-nf3", "w3-nf4", "w4-nf3-idle-rank", "w4-2x2-shots", "w6-3x2-idle-freq"])
+def test_gather_seismograms_gloo_equals_reference_sum(world, nf, nshots, npf):
+    """Uneven shares, ranks without frequencies, and split shots
+    (NPROCFREQ = npf); every rank ends with what summing zero-filled full
+    arrays over the ranks gives, bit for bit (signed zeros included)."""
     import torch.multiprocessing as tmp
-    nshots, ntr = 3, 5
+    ntr = 5
     with tempfile.TemporaryDirectory() as d:
-        tmp.spawn(_gather_worker, args=(world, _free_port(), d, nf, nshots, ntr), nprocs=world, join=True)
+        tmp.spawn(_gather_worker, args=(world, _free_port(), d, nf, nshots, ntr, npf), nprocs=world, join=True)
         res = [np.load(os.path.join(d, f"s{r}.npy")) for r in range(world)]
     ref = np.zeros((nf, nshots, ntr), np.complex64)   # write_seis_AC: sum of each rank's zero-filled array
     for r in range(world):
-        lo, hi = frequency_range(nf, world, r)
+        (lo, hi), (slo, shi) = rank_blocks(nf, nshots, world, r, npf)
         part = np.zeros_like(ref)
         for f in range(lo, hi):
-            part[f] = _seis_block(f, nshots, ntr)
+            part[f, slo:shi] = _seis_block(f, nshots, ntr)[slo:shi]
         ref = ref + part
     for out in res:
         assert out.shape == (nf, nshots, ntr)
@@ -201,15 +250,16 @@ def _oracle_forward_local(g, vp, rho, xs, ys, rx, ry):
     from oracle import sparse as OS
     idx = [OS.receiver_read_index(g, int(a), int(b)) for a, b in zip(rx, ry)]
 
-    def run(local):
-        if not local:
+    def run(local, shots=None):
+        sel = slice(None) if shots is None else slice(shots.start, shots.stop)
+        if not local or (shots is not None and len(shots) == 0):
             return None
-        X, _ = oracle_forward(g, 1, vp, rho, local, xs, ys)
+        X, _ = oracle_forward(g, 1, vp, rho, local, xs[sel], ys[sel])
         return np.stack([OS.vec2mat(X[i].T)[:, idx] for i in range(len(local))]).astype(np.complex64)
     return run
 
 
-def _forward_worker(rank, world, port, out_dir):
+def _forward_worker(rank, world, port, out_dir, npf):
     import torch.distributed as dist
     import datetime
     os.environ["MASTER_ADDR"] = "127.0.0.1"
@@ -217,30 +267,38 @@ def _forward_worker(rank, world, port, out_dir):
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=120))
     try:
         g, vp, rho, xs, ys, rx, ry, freqs = _case()
-        seis = sharded_forward(freqs, _oracle_forward_local(g, vp, rho, xs, ys, rx, ry), xs.size, rx.size, dist)
+        seis = sharded_forward(freqs, _oracle_forward_local(g, vp, rho, xs, ys, rx, ry), xs.size, rx.size, dist,
+                               nprocfreq=npf)
         np.save(os.path.join(out_dir, f"f{rank}.npy"), seis)
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 4])
-def test_sharded_forward_gloo_equals_single_process(world):
-    """world 2: shares of 2 and 1 frequencies; world 4: one rank has none."""
+@pytest.mark.parametrize("world,npf", [(2, None), (4, None), (4, 2)], ids=["w2", "w4-idle-rank", "w4-2x2-shots"])
+def test_sharded_forward_gloo_equals_single_process(world, npf):
+    """world 2: shares of 2 and 1 frequencies; world 4: one rank has none;
+    2 x 2: two frequency blocks, each with its shots split over two ranks
+    (their solves take fewer right-hand sides at once, so equal to the
+    float32 rounding of the seismograms)."""
     import torch.multiprocessing as tmp
     with tempfile.TemporaryDirectory() as d:
-        tmp.spawn(_forward_worker, args=(world, _free_port(), d), nprocs=world, join=True)
+        tmp.spawn(_forward_worker, args=(world, _free_port(), d, npf), nprocs=world, join=True)
         res = [np.load(os.path.join(d, f"f{r}.npy")) for r in range(world)]
     g, vp, rho, xs, ys, rx, ry, freqs = _case()
     ref = _oracle_forward_local(g, vp, rho, xs, ys, rx, ry)(freqs) + np.complex64(0)
     for out in res:
-        assert np.array_equal(out, ref)
+        assert out.tobytes() == res[0].tobytes()
+        if npf is None:
+            assert np.array_equal(out, ref)
+        else:
+            assert np.linalg.norm(out - ref) <= 1e-6 * np.linalg.norm(ref)
 
 
 @pytest.mark.gpu
 def test_sharded_engine_forward_over_nccl():
     """One rank over NCCL on cuda:0: the gathered seismograms (device
-    buffers) are the engine's own block, bit for bit, and match the
-    oracle."""
+    buffers) are the engine's own block, bit for bit, and match the oracle;
+    the engine's share for a shot block is that block of the whole."""
     import datetime
     import torch
     import torch.distributed as dist
@@ -255,12 +313,14 @@ def test_sharded_engine_forward_over_nccl():
             e.set_model(vp, rho)
             run, blocks = engine_forward(e, xs, ys, rx, ry), []
 
-            def local(fs):
-                blocks.append(run(fs))
+            def local(fs, shots):
+                blocks.append(run(fs, shots))
                 return blocks[-1]
             seis = sharded_forward(freqs, local, xs.size, rx.size, dist, device=torch.device("cuda", 0))
+            part = run(freqs, range(1, 3))
     finally:
         dist.destroy_process_group()
     assert np.array_equal(seis, blocks[0])
+    assert np.linalg.norm(part - seis[:, 1:3]) <= 1e-6 * np.linalg.norm(seis[:, 1:3])
     ref = _oracle_forward_local(g, vp, rho, xs, ys, rx, ry)(freqs)
     assert np.linalg.norm(seis - ref) <= 2e-6 * np.linalg.norm(ref)
