@@ -27,6 +27,12 @@ of MYID / NPROCFREQ (src/AC/fwi_FD_AC.c:201-211, init_MPIshot at
 src/init_MPIshot.c:20-31), factorising its frequencies redundantly with the
 other ranks of its frequency block.  ``nprocfreq`` selects that layout
 (default: every rank a frequency block of its own, all shots).
+
+Failures: a rank whose local evaluation raises still takes every
+collective step.  One small all-reduce of a failure count precedes the
+exchange; the failing rank then re-raises its own exception and the others
+raise :class:`RankFailure`, so no rank waits for a peer that will not come.
+A rank that stalls or dies is caught by the process group's timeout.
 """
 from __future__ import annotations
 
@@ -36,8 +42,38 @@ import numpy as np
 
 from ._lib import GM_PHYS_TE
 
-__all__ = ["frequency_range", "shot_range", "rank_blocks", "local_frequencies", "allreduce_gradient",
+__all__ = ["RankFailure", "frequency_range", "shot_range", "rank_blocks", "local_frequencies", "allreduce_gradient",
            "sharded_grad_obj", "engine_grad_obj", "gather_seismograms", "sharded_forward", "engine_forward"]
+
+
+class RankFailure(RuntimeError):
+    """Another rank's local evaluation failed; raised on every rank that
+    did not fail itself, after the failure-count step."""
+
+
+def _failures(ok: bool, dist, group, device) -> int:
+    """Number of ranks whose local evaluation failed: one all-reduce that
+    every rank takes, failed or not."""
+    import torch
+    t = torch.tensor([0.0 if ok else 1.0], dtype=torch.float64)
+    if device is not None:
+        t = t.to(device)
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return int(t.item())
+
+
+def _run_local(fn, args, dist, group, device):
+    """fn(*args) on this rank, then the failure-count step."""
+    try:
+        res, err = fn(*args), None
+    except Exception as ex:   # the exchange must still be taken
+        res, err = None, ex
+    failed = _failures(err is None, dist, group, device)
+    if err is not None:
+        raise err
+    if failed:
+        raise RankFailure(f"{failed} rank(s) failed their local evaluation")
+    return res
 
 
 def _block(count: int, parts: int, me: int) -> Tuple[int, int]:
@@ -115,11 +151,12 @@ def sharded_grad_obj(freqs: Sequence[float],
     of shot indices, or None for all shots (NPROCSHOT = 1); a rank without
     frequencies or shots is still called (with an empty list or range) and
     returns zeros.  `nshots` is needed only with `nprocfreq`.  Every rank
-    takes the same collective step, whatever its share."""
+    takes the same collective steps, whatever its share and whether or not
+    its evaluation fails (see the module's notes on failures)."""
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
     local, shots = _share(freqs, nshots, world, rank, nprocfreq)
-    g0, g1, l2 = local_grad_obj(local, shots)
+    g0, g1, l2 = _run_local(local_grad_obj, (local, shots), dist, group, device)
     return allreduce_gradient(g0, g1, l2, dist, group=group, device=device)
 
 
@@ -198,12 +235,19 @@ def sharded_forward(freqs: Sequence[float], local_forward: Callable[[list, Optio
     each rank modelling only its share with `local_forward(local_freqs,
     shots) -> [len(local_freqs)][len(shots)][ntr]` (`shots` None = all
     shots; called with an empty list or range on a rank without work), then
-    gathered.  Every rank takes the same collective step, whatever its
-    share."""
+    gathered.  Every rank takes the same collective steps, whatever its
+    share and whether or not its evaluation fails."""
     world = dist.get_world_size(group)
     rank = dist.get_rank(group)
     local, shots = _share(freqs, nshots, world, rank, nprocfreq)
-    seis = local_forward(local, shots)
+    (flo, fhi), (slo, shi) = rank_blocks(len(freqs), nshots, world, rank, nprocfreq)
+
+    def checked(local, shots):   # a block of the wrong shape fails before the exchange, like any other error
+        seis = local_forward(local, shots)
+        if fhi > flo and shi > slo and np.shape(seis) != (fhi - flo, shi - slo, ntr):
+            raise ValueError(f"rank {rank}: seismograms {np.shape(seis)}, expected {(fhi - flo, shi - slo, ntr)}")
+        return seis
+    seis = _run_local(checked, (local, shots), dist, group, device)
     return gather_seismograms(seis, len(freqs), nshots, ntr, dist, group=group, device=device,
                               nprocfreq=nprocfreq)
 

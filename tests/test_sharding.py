@@ -324,3 +324,74 @@ def test_sharded_engine_forward_over_nccl():
     assert np.linalg.norm(part - seis[:, 1:3]) <= 1e-6 * np.linalg.norm(seis[:, 1:3])
     ref = _oracle_forward_local(g, vp, rho, xs, ys, rx, ry)(freqs)
     assert np.linalg.norm(seis - ref) <= 2e-6 * np.linalg.norm(ref)
+
+
+def _failure_worker(rank, world, port, out_dir, mode):
+    """Rank 1 fails its local step (mode "raise"), returns seismograms of
+    the wrong shape (mode "shape"), or stalls past the process group's
+    timeout before it (mode "stall"); every rank records what it raised and
+    when."""
+    import time
+    import torch.distributed as dist
+    import datetime
+    from germaine_b200.sharding import RankFailure
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=3))
+    freqs = [2.0, 3.0, 4.0]
+
+    def local(fs, shots):
+        if rank == 1 and mode == "raise":
+            raise FloatingPointError("singular front")
+        if rank == 1 and mode == "stall":
+            time.sleep(8)
+        return np.zeros(16), None, float(len(fs))
+    def local_seis(fs, shots):   # rank 1 returns a block of the wrong shape
+        return np.zeros((len(fs), 4 if rank == 1 else 3, 5), np.complex64)
+    t0 = time.monotonic()
+    try:
+        if mode == "shape":
+            sharded_forward(freqs, local_seis, 3, 5, dist)
+        else:
+            sharded_grad_obj(freqs, local, dist)
+        what = "ok"
+    except RankFailure:
+        what = "RankFailure"
+    except (FloatingPointError, ValueError):
+        what = "own"
+    except RuntimeError:   # the process group's timeout or a closed peer
+        what = "timeout"
+    took = time.monotonic() - t0
+    with open(os.path.join(out_dir, f"r{rank}.txt"), "w") as f:
+        f.write(f"{what} {took:.2f}")
+    if mode != "stall":
+        dist.destroy_process_group()
+
+
+def _outcomes(world, mode):
+    import torch.multiprocessing as tmp
+    with tempfile.TemporaryDirectory() as d:
+        tmp.spawn(_failure_worker, args=(world, _free_port(), d, mode), nprocs=world, join=True)
+        out = []
+        for r in range(world):
+            what, took = open(os.path.join(d, f"r{r}.txt")).read().split()
+            out.append((what, float(took)))
+    return out
+
+
+@pytest.mark.parametrize("mode", ["raise", "shape"])
+def test_sharded_rank_failure_reaches_every_rank(mode):
+    """A rank whose evaluation raises (or returns seismograms of the wrong
+    shape) still takes the failure-count step: it re-raises its own error,
+    every other rank raises RankFailure at the same step, and none waits
+    for the timeout."""
+    out = _outcomes(3, mode)
+    assert [w for w, _ in out] == ["RankFailure", "own", "RankFailure"]
+    assert all(t < 2.5 for _, t in out), out
+
+
+def test_sharded_stalled_rank_ends_in_the_timeout():
+    """A rank that stalls past the process group's timeout: the waiting
+    rank's collective ends with an error instead of hanging."""
+    out = _outcomes(2, "stall")
+    assert out[0][0] == "timeout" and out[0][1] < 7.5, out
