@@ -1,5 +1,5 @@
-"""Frequency sharding over ranks with one exchange step: the gradient sum
-(FWI) or the seismogram gather (forward modelling).
+"""Frequency (and shot) sharding over ranks with one data exchange: the
+gradient sum (FWI) or the seismogram gather (forward modelling).
 
 The reference distributes the frequencies of a stage over MPI ranks
 (``init_MPIfreq``, src/init_MPIfreq.c:20-31: contiguous blocks, the first
