@@ -199,7 +199,9 @@ def gather_seismograms(local_seis, nf: int, nshots: int, ntr: int, dist, group=N
     (src/AC/write_seis_AC.c:33-45); every entry has one contributor, so the
     blocks put side by side hold the same values, except that the sum turns
     a -0.0 into +0.0 when more than one rank takes part, which the last
-    step repeats.  One all_gather of the blocks as float32 pairs, each block
+    step repeats.  (Its sum starts one element early and so leaves the last
+    sample 0; that is a property of the file it writes, which
+    files.write_seis reproduces, not of the data.)  One all_gather of the blocks as float32 pairs, each block
     padded to the largest share (the shares differ by at most one frequency
     and one shot).  `device` is where the buffers live for the collective."""
     import torch
