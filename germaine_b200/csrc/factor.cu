@@ -969,8 +969,8 @@ namespace gm {
 //      pivot row by the threshold rule (mid_select_pivot: rows keep their
 //      threads and trade pivot positions), and the row's owner replaces a
 //      pivot that stays tiny as static_pivot does and publishes the row and
-//      the pivot's reciprocal in shared memory, so no shared-memory traffic
-//      for the update itself;
+//      the pivot's reciprocal in shared memory: one barrier per pivot, and
+//      no shared-memory traffic for the update itself;
 //   2. solves L11 U12 = P A12 with each thread holding one column of U12;
 //   3. inverts the pivot block's two triangles;
 //   4. writes L, U and the inverses back (the layout the blocked path
